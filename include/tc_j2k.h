@@ -1,0 +1,278 @@
+/*
+ * tc_j2k.h -- C ABI of the B200 (sm_100a) JPEG 2000 decode pipeline.
+ *
+ * This is the drop-in boundary for kgmoore/ThousandthChicken's device stages.
+ * Each entry point names the reference interface it replaces (paths relative
+ * to the reference project's ThousandthChicken/ directory).  Plain pointers
+ * and sizes only: no C++ or framework types cross this boundary, and no C++
+ * exception escapes it.
+ *
+ * Conventions
+ *  - Status codes: TC_OK (0) or a negative TC_E_* value.  They replace the
+ *    reference's tDeviceRC/cl_int (platform.h:9-11) and its thrown Error
+ *    objects (basic.h:95-104).
+ *  - A tc_ctx is bound to one CUDA device and one CUDA stream; every call on
+ *    a ctx is stream-ordered on that stream.  A ctx may be used from one host
+ *    thread at a time; distinct contexts are independent (no global mutable
+ *    state apart from the read-only tables each kernel builds for itself).
+ *  - Pointers named d_* are device pointers; h_* are host pointers.
+ *  - Geometry: tile origin at (0,0); Mallat layout means the multi-level
+ *    subbands sit in place in one plane (LL_N top-left; at each level the HL
+ *    band right of LL, LH below it, HH diagonal).
+ */
+#ifndef TC_J2K_H
+#define TC_J2K_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+#define TC_OK              0
+#define TC_E_ARG          -1  /* invalid argument */
+#define TC_E_OOM          -2  /* host or device allocation failed */
+#define TC_E_CODESTREAM   -3  /* malformed codestream or code-block data */
+#define TC_E_DEVICE       -4  /* CUDA error */
+#define TC_E_TIMEOUT      -5  /* a bounded device wait gave up */
+#define TC_E_UNSUPPORTED  -6  /* valid JPEG 2000 outside the supported subset */
+#define TC_E_NOFILE       -7  /* file missing (Decoder.cpp:103-107 returns -2) */
+
+/* ---- sample types -------------------------------------------------------- */
+#define TC_U8     1
+#define TC_U16    2
+#define TC_INT32  3
+#define TC_FLOAT32 4
+
+/* ---- context ------------------------------------------------------------- */
+typedef struct tc_ctx tc_ctx;
+
+/* Create a context on `device` that issues work on `cuda_stream` (a
+ * cudaStream_t; NULL = the legacy default stream).  Replaces the OpenCL
+ * set-up of InitOpenCL (ocl_util.cpp:425-466) and KernelInitInfoBase
+ * (platform.h:21-34). */
+int tc_ctx_create(int device, void *cuda_stream, tc_ctx **out);
+int tc_ctx_destroy(tc_ctx *ctx);
+/* Wait for all work on the ctx's stream, then read and clear the device
+ * error word; returns TC_E_CODESTREAM when a kernel flagged bad block data. */
+int tc_ctx_synchronize(tc_ctx *ctx);
+/* Message for the last failing call on this ctx ("" if none). */
+const char *tc_ctx_last_error(const tc_ctx *ctx);
+const char *tc_status_string(int status);
+/* Library version: major*10000 + minor*100 + patch. */
+int tc_version(void);
+/* Number of kernel launches this ctx issued since creation (diagnostics). */
+uint64_t tc_ctx_launch_count(const tc_ctx *ctx);
+
+/* ---- Tier-1 code-block decode (CoefficientCoder) ------------------------- */
+
+/* One code-block as Tier-2 leaves it.  Filled by the parser below, or by a
+ * caller's own parser from the reference's type_codeblock in its
+ * codeBlockCallback (codestream.h:12-14, codestream.c:465-466; fields from
+ * codestream_image_types.h:30-120 and CodeBlockAdditionalInfo,
+ * coefficientcoder_common.h:5-24). */
+typedef struct tc_cblk_desc {
+    uint64_t seg_off;        /* byte offset of the block's codeword in the pool */
+    uint64_t out_off;        /* element offset (4-byte elements) of sample (0,0) */
+    uint32_t seg_len;        /* codeword bytes (cblk->length) */
+    uint32_t out_pitch;      /* output row pitch in elements */
+    float    step;           /* dequantisation step, irreversible blocks only */
+    uint16_t w, h;           /* block size, 1..64 each */
+    uint8_t  passes;         /* coding passes included (cblk->num_coding_passes) */
+    uint8_t  mb;             /* magnitude bit-planes Mb of the subband (1..31) */
+    uint8_t  zero_bitplanes; /* Mb - significant_bits */
+    uint8_t  orient;         /* 0 LL, 1 HL, 2 LH, 3 HH (type_orient) */
+    uint8_t  flags;          /* TC_CBLK_* */
+    uint8_t  reserved[3];
+} tc_cblk_desc;
+
+#define TC_CBLK_IRREVERSIBLE 0x01  /* float output, multiply by step */
+
+/* Output modes of tc_t1_decode. */
+#define TC_T1_OUT_DEQUANT 0  /* int32 (reversible) or float (irreversible) values */
+#define TC_T1_OUT_RAW     1  /* uint32 sign-magnitude, sign at bit 31, magnitude
+                                bit b at bit b+31-Mb: the reference g_decode
+                                output (coefficient_coder.cl:605-626,805-816) */
+
+/* Decode n code-blocks in one persistent launch (one warp per code-block,
+ * blocks taken from a device work queue in the order d_order gives; NULL =
+ * descriptor order; the host-side tc_t1_sort_order() produces a
+ * longest-first order).  With TC_T1_OUT_DEQUANT the inverse quantiser is
+ * fused in: reconstruction point recon_r in [0,1) for truncated blocks
+ * (ISO E.1.1.2; 0 = truncated value).  Replaces
+ * CoefficientCoder::decode_tile/decodeInit/decode (CoefficientCoder.cpp:62-252)
+ * plus Quantizer::dequantize_tile (Quantizer.cpp:181-216). */
+int tc_t1_decode(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint32_t *d_order,
+                 int n, const uint8_t *d_pool, uint64_t pool_len, void *d_out,
+                 int out_mode, float recon_r);
+
+/* Host helper: write into h_order a permutation of 0..n-1 sorted by
+ * decreasing estimated work (passes x area, then codeword length). */
+int tc_t1_sort_order(const tc_cblk_desc *h_desc, int n, uint32_t *h_order);
+
+/* Standalone inverse quantiser over TC_T1_OUT_RAW output: reads the raw word
+ * of every block sample at the descriptor's out_off/out_pitch in d_raw and
+ * writes int32 or float at the same place in d_out.  The number of decoded
+ * bit-planes is taken from the pass count.  Replaces Quantizer::dequantization
+ * and the subband_dequantization_lossless/lossy kernels
+ * (Quantizer.cpp:126-175, quantizer_*_inverse.cl:16-44), with the sign
+ * handled (defect D4 fixed). */
+int tc_dequantize_raw(tc_ctx *ctx, const tc_cblk_desc *d_desc, int n,
+                      const uint32_t *d_raw, void *d_out, float recon_r);
+
+/* ---- DWT (DWTForward53/97, DWTReverse53/97, DWTKernel<T>::run) ----------- */
+
+#define TC_ROUND_FLOOR 0  /* ISO F.3/F.4 floor lifting (conformant) */
+#define TC_ROUND_TRUNC 1  /* C truncating division, as the reference kernels
+                             (dwt_transform_buffer.cl:124-269) */
+
+/* Multi-level forward transform of a w x h plane into Mallat layout.
+ * Replaces DWTForward53::dwt / DWTForward97::dwt (DWTForward53.cpp:20-43,
+ * DWTForward97.cpp:20-43) and DWTKernel<T>::run(in, out, sx, sy, levels)
+ * (DWTKernel.cpp:158-178).  d_in is not modified. */
+int tc_dwt_forward53(tc_ctx *ctx, const int32_t *d_in, int in_pitch,
+                     int32_t *d_out, int out_pitch, int w, int h, int levels,
+                     int rounding);
+int tc_dwt_forward97(tc_ctx *ctx, const float *d_in, int in_pitch,
+                     float *d_out, int out_pitch, int w, int h, int levels);
+
+/* Multi-level reverse transform from Mallat layout back to samples.
+ * Replaces DWTReverse53::dwt / DWTReverse97::dwt (DWTReverse53.cpp:23-43,
+ * DWTReverse97.cpp:24-44) and DWT::iwt (DWT.cpp:57-114).  d_in is not
+ * modified; d_out must not alias d_in. */
+int tc_dwt_reverse53(tc_ctx *ctx, const int32_t *d_in, int in_pitch,
+                     int32_t *d_out, int out_pitch, int w, int h, int levels,
+                     int rounding);
+int tc_dwt_reverse97(tc_ctx *ctx, const float *d_in, int in_pitch,
+                     float *d_out, int out_pitch, int w, int h, int levels);
+
+/* ---- colour transform + DC level shift (Preprocessor) -------------------- */
+
+#define TC_COLOR_DC  0  /* DC level shift only, per component */
+#define TC_COLOR_RCT 1  /* reversible component transform (components 0-2) */
+#define TC_COLOR_ICT 2  /* irreversible component transform (components 0-2) */
+
+/* Inverse: planes of in_type (TC_INT32 or TC_FLOAT32) -> inverse colour
+ * transform, DC shift, rounding (float input: to nearest even) and clamp to
+ * [0, 2^bits-1] -> planes of out_type (TC_U8, TC_U16 or TC_INT32).
+ * Replaces Preprocessor::color_decoder_lossless/color_decoder_lossy/
+ * idc_level_shifting (Preprocessor.cpp:44-180) and the tcr_kernel,
+ * tci_kernel and idc_level_shift_kernel kernels; the ICT uses the ISO G.2
+ * inverse (defect D9 fixed) and the dispatch follows the transform asked for
+ * (defects D7/D8 fixed). */
+int tc_color_inverse(tc_ctx *ctx, int kind, int ncomp,
+                     void *const *d_in, int in_type, int in_pitch,
+                     void *const *d_out, int out_type, int out_pitch,
+                     int w, int h, int bits);
+
+/* Forward: unsigned samples of in_type (TC_U8, TC_U16 or TC_INT32) -> DC
+ * shift and forward colour transform -> TC_INT32 (RCT/DC) or TC_FLOAT32
+ * (ICT, or DC to float) planes.  Replaces the rct_kernel, ict_kernel and
+ * fdc_level_shift_kernel kernels (preprocess_rct.cl, preprocess_ict.cl,
+ * preprocess_dc_level_shift.cl) and Preprocessor::dc_level_shifting. */
+int tc_color_forward(tc_ctx *ctx, int kind, int ncomp,
+                     const void *const *d_in, int in_type, int in_pitch,
+                     void *const *d_out, int out_type, int out_pitch,
+                     int w, int h, int bits);
+
+/* ---- codestream parsing (the Tier-2 hand-off) ---------------------------- */
+
+typedef struct tc_image_info {
+    int32_t width, height, ncomp, bits;    /* all components share size/depth */
+    int32_t is_signed;
+    int32_t levels;                        /* decomposition levels NL */
+    int32_t reversible;                    /* 1 = 5/3, 0 = 9/7 */
+    int32_t mct;                           /* multiple component transform */
+    int32_t cblk_w, cblk_h;
+    int32_t layers, progression;
+    int32_t guard_bits, quant_style;
+    uint32_t ncblk;                        /* code-blocks over all components */
+    uint32_t reserved;
+} tc_image_info;
+
+/* Read the main header only.  Replaces read_main_header (codestream.c:233-258). */
+int tc_j2k_read_header(const uint8_t *h_cs, size_t len, tc_image_info *info);
+
+/* Parse a whole codestream into code-block descriptors.  Segment offsets
+ * refer to h_pool: for single-layer streams h_pool is the codestream itself
+ * (zero copy) and *pool_is_cs is set; otherwise the parser gathers each
+ * block's layers into a contiguous pool it owns.  Output offsets address a
+ * plane set of ncomp planes of width*height elements (plane c at element
+ * c*width*height).  Replaces decode_codestream / decode_tiles /
+ * decode_packet_header / decode_packet_body (codestream.c:336-536) and the
+ * codeBlockCallback hand-off.  Free with tc_j2k_parsed_free. */
+typedef struct tc_j2k_parsed {
+    tc_image_info info;
+    tc_cblk_desc *desc;      /* info.ncblk entries */
+    const uint8_t *pool;     /* segment pool (host) */
+    uint64_t pool_len;
+    int32_t pool_is_cs;
+    int32_t reserved;
+} tc_j2k_parsed;
+int tc_j2k_parse(const uint8_t *h_cs, size_t len, tc_j2k_parsed **out);
+void tc_j2k_parsed_free(tc_j2k_parsed *p);
+
+/* ---- whole-image decode (Decoder) ---------------------------------------- */
+
+/* Decode a codestream held in host memory into host memory: planar
+ * components, TC_U8 samples when bits <= 8 else TC_U16, component c at
+ * h_out + c*width*height*bytes.  Runs Tier-1 with fused dequantisation, the
+ * reverse DWT and the fused inverse colour transform / DC shift on the GPU.
+ * Replaces Decoder::decode (Decoder.cpp:94-217). */
+int tc_decode_j2k(tc_ctx *ctx, const uint8_t *h_cs, size_t len,
+                  void *h_out, size_t out_bytes, tc_image_info *info);
+
+/* Same, reading the codestream from a file (Decoder::decode(fileName)). */
+int tc_decode_j2k_file(tc_ctx *ctx, const char *path, void *h_out,
+                       size_t out_bytes, tc_image_info *info);
+
+/* Device-resident plans: parse and upload once, execute many times.  A batch
+ * plan merges the code-blocks of all images into one Tier-1 launch and the
+ * DWT levels of all images into one launch per level. */
+typedef struct tc_plan tc_plan;
+int tc_plan_create(tc_ctx *ctx, const uint8_t *const *h_cs, const size_t *lens,
+                   int nimages, tc_plan **out);
+int tc_plan_destroy(tc_plan *plan);
+/* Bytes of output for image i (planar, sample type as tc_decode_j2k). */
+int tc_plan_output_bytes(const tc_plan *plan, int image, size_t *bytes);
+int tc_plan_image_info(const tc_plan *plan, int image, tc_image_info *info);
+/* Run the decode of every image in the plan; image i goes to d_out[i]
+ * (device memory of tc_plan_output_bytes bytes).  Stream-ordered. */
+int tc_plan_execute(tc_plan *plan, void *const *d_out);
+
+/* ---- harness encoder (test and benchmark input generation) --------------- */
+
+typedef struct tc_encode_params {
+    int32_t width, height, ncomp, bits;
+    int32_t levels;        /* decomposition levels */
+    int32_t reversible;    /* 1 = 5/3 lossless, 0 = 9/7 */
+    int32_t mct;           /* RCT/ICT on components 0-2 */
+    int32_t cblk_log2;     /* code-block size 2^cblk_log2 (2..6) */
+    double  base_step;     /* irreversible: step relative to 2^bits, divided
+                              by the subband's synthesis L2 norm */
+    int32_t guard_bits;    /* 0 = choose automatically */
+    int32_t progression;   /* 0 = LRCP, 1 = RLCP */
+    int32_t threads;       /* <= 0: all cores */
+    int32_t reserved;
+} tc_encode_params;
+
+/* Encode planar unsigned samples (TC_U8 when bits <= 8, else TC_U16) into a
+ * single-tile, single-layer codestream with all coding passes. */
+int tc_encode_j2k(const tc_encode_params *p, const void *h_planes,
+                  uint8_t *h_out, size_t cap, size_t *out_len);
+
+/* Encode one code-block of quantised coefficients (row-major int32, w x h)
+ * with the MQ coder, keeping the first `passes` coding passes (0 or more
+ * than available = all) and terminating the codeword there.  Returns the
+ * codeword length in *len, the pass count in *passes_out and the leading
+ * zero bit-planes relative to mb in *zero_bitplanes. */
+int tc_t1_encode_block(const int32_t *h_coef, int w, int h, int orient, int mb,
+                       int passes, uint8_t *h_out, int cap, int *len,
+                       int *passes_out, int *zero_bitplanes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TC_J2K_H */

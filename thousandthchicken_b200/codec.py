@@ -1,0 +1,96 @@
+"""Host-side codestream helpers over libtc_j2k: header reading, Tier-2 parsing
+into code-block descriptors, and the harness encoder.  No GPU is needed for
+anything in this module."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib as L
+
+# numpy view of tc_cblk_desc (include/tc_j2k.h)
+DESC_DTYPE = np.dtype([("seg_off", "<u8"), ("out_off", "<u8"), ("seg_len", "<u4"), ("out_pitch", "<u4"),
+                       ("step", "<f4"), ("w", "<u2"), ("h", "<u2"), ("passes", "u1"), ("mb", "u1"),
+                       ("zero_bitplanes", "u1"), ("orient", "u1"), ("flags", "u1"), ("reserved", "u1", (3,))])
+assert DESC_DTYPE.itemsize == 40
+
+INFO_FIELDS = ("width", "height", "ncomp", "bits", "is_signed", "levels", "reversible", "mct", "cblk_w",
+               "cblk_h", "layers", "progression", "guard_bits", "quant_style", "ncblk")
+
+
+def _info_dict(info: L.ImageInfo) -> dict:
+    return {k: int(getattr(info, k)) for k in INFO_FIELDS}
+
+
+def _buf(data) -> np.ndarray:
+    return np.frombuffer(bytes(data), np.uint8) if not isinstance(data, np.ndarray) else \
+        np.ascontiguousarray(data, np.uint8)
+
+
+def read_header(cs) -> dict:
+    a = _buf(cs)
+    info = L.ImageInfo()
+    L.check(L.lib().tc_j2k_read_header(a.ctypes.data, a.size, C.byref(info)), what="tc_j2k_read_header")
+    return _info_dict(info)
+
+
+def parse(cs):
+    """Parse a codestream: returns (info dict, descriptor array, segment pool)."""
+    a = _buf(cs)
+    out = C.POINTER(L.Parsed)()
+    L.check(L.lib().tc_j2k_parse(a.ctypes.data, a.size, C.byref(out)), what="tc_j2k_parse")
+    try:
+        p = out.contents
+        info = _info_dict(p.info)
+        n = info["ncblk"]
+        desc = np.empty(n, DESC_DTYPE)
+        if n:
+            C.memmove(desc.ctypes.data, p.desc, n * DESC_DTYPE.itemsize)
+        if p.pool_is_cs:
+            pool = a.copy()
+        else:
+            pool = np.empty(p.pool_len, np.uint8)
+            if p.pool_len:
+                C.memmove(pool.ctypes.data, p.pool, p.pool_len)
+    finally:
+        L.lib().tc_j2k_parsed_free(out)
+    return info, desc, pool
+
+
+def encode(planes: np.ndarray, bits: int, levels: int = 5, reversible: bool = True, mct: bool = True,
+           cblk_log2: int = 6, base_step: float = 1.0 / 128, guard_bits: int = 0, progression: int = 0,
+           threads: int = 0) -> bytes:
+    """Harness encoder: planar unsigned samples [ncomp, h, w] -> codestream."""
+    planes = np.ascontiguousarray(planes, np.uint8 if bits <= 8 else np.uint16)
+    if planes.ndim == 2:
+        planes = planes[None]
+    ncomp, h, w = planes.shape
+    p = L.EncodeParams(width=w, height=h, ncomp=ncomp, bits=bits, levels=levels, reversible=int(reversible),
+                       mct=int(mct), cblk_log2=cblk_log2, base_step=base_step, guard_bits=guard_bits,
+                       progression=progression, threads=threads)
+    cap = planes.nbytes * 3 + 65536
+    out = np.empty(cap, np.uint8)
+    n = C.c_size_t(0)
+    L.check(L.lib().tc_encode_j2k(C.byref(p), planes.ctypes.data, out.ctypes.data, cap, C.byref(n)),
+            what="tc_encode_j2k")
+    return out[: n.value].tobytes()
+
+
+def t1_encode_block(coef: np.ndarray, orient: int, mb: int, passes: int = 0):
+    """Encode one code-block; returns (codeword bytes, passes, zero_bitplanes)."""
+    coef = np.ascontiguousarray(coef, np.int32)
+    h, w = coef.shape
+    cap = 16 * w * h + 1024
+    out = np.empty(cap, np.uint8)
+    n, np_, zb = C.c_int(0), C.c_int(0), C.c_int(0)
+    L.check(L.lib().tc_t1_encode_block(coef.ctypes.data, w, h, orient, mb, passes, out.ctypes.data, cap,
+                                       C.byref(n), C.byref(np_), C.byref(zb)), what="tc_t1_encode_block")
+    return out[: n.value].tobytes(), np_.value, zb.value
+
+
+def sort_order(desc: np.ndarray) -> np.ndarray:
+    desc = np.ascontiguousarray(desc, DESC_DTYPE)
+    order = np.empty(len(desc), np.uint32)
+    L.check(L.lib().tc_t1_sort_order(desc.ctypes.data, len(desc), order.ctypes.data), what="tc_t1_sort_order")
+    return order

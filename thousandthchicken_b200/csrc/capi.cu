@@ -1,0 +1,706 @@
+// capi.cu -- the extern "C" boundary of libtc_j2k (see include/tc_j2k.h).
+//
+// Orchestrates the decode the reference's Decoder::decode performs
+// (Decoder.cpp:94-217) on one CUDA stream per context:
+//   parse (host) -> H2D segment pool + descriptors -> Tier-1 with fused
+//   dequantisation (one persistent launch over every code-block of every
+//   image) -> reverse DWT levels (ping-pong scratch, no LL copies) -> last
+//   level fused with inverse colour / DC shift / clamp -> D2H.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <vector>
+
+#include "j2k_host.h"
+#include "tc_internal.cuh"
+
+namespace tc {
+
+cudaError_t DevBuf::ensure(size_t bytes)
+{
+    if (bytes <= size && ptr) return cudaSuccess;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    size = 0;
+    const size_t want = std::max<size_t>(bytes, 256);
+    cudaError_t e = cudaMalloc(&ptr, want);
+    if (e == cudaSuccess) size = want;
+    else ptr = nullptr;
+    return e;
+}
+
+void DevBuf::release()
+{
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    size = 0;
+}
+
+int fail(tc_ctx *ctx, int status, const std::string &msg)
+{
+    if (ctx) ctx->err = msg;
+    return status;
+}
+
+int cuda_status(tc_ctx *ctx, cudaError_t e, const char *what)
+{
+    if (e == cudaSuccess) return TC_OK;
+    if (e == cudaErrorMemoryAllocation) return fail(ctx, TC_E_OOM, std::string(what) + ": out of device memory");
+    return fail(ctx, TC_E_DEVICE, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// Pinned host staging buffer (grow-only).
+struct PinBuf {
+    void *ptr = nullptr;
+    size_t size = 0;
+    cudaError_t ensure(size_t bytes)
+    {
+        if (bytes <= size && ptr) return cudaSuccess;
+        if (ptr) cudaFreeHost(ptr);
+        ptr = nullptr;
+        size = 0;
+        cudaError_t e = cudaHostAlloc(&ptr, std::max<size_t>(bytes, 4096), cudaHostAllocDefault);
+        if (e == cudaSuccess) size = std::max<size_t>(bytes, 4096);
+        return e;
+    }
+    void release()
+    {
+        if (ptr) cudaFreeHost(ptr);
+        ptr = nullptr;
+        size = 0;
+    }
+};
+
+static int check_ctx(tc_ctx *ctx)
+{
+    if (!ctx) return TC_E_ARG;
+    cudaError_t e = cudaSetDevice(ctx->device);
+    return cuda_status(ctx, e, "cudaSetDevice");
+}
+
+static int sample_bytes(int bits) { return bits <= 8 ? 1 : 2; }
+
+// Reverse DWT of ncomp components from Mallat planes coef[c] (pitch cp)
+// through levels >= 2 into ping-pong scratch, and the last level either into
+// T planes (out_color < 0) or fused with colour into out_type samples.
+static int run_reverse(tc_ctx *ctx, int wavelet, int rounding, const void *const *coef, int cp, int w, int h,
+                       int levels, int ncomp, char *scratch, void *const *out, int out_pitch, int color,
+                       int out_type, int bits)
+{
+    std::vector<int> ws, hs;
+    level_sizes(w, h, levels, ws, hs);
+    const size_t esz = 4;
+    const size_t sw = levels >= 1 ? ws[1] : 0, sh = levels >= 1 ? hs[1] : 0;
+    const size_t slab = sw * sh * esz;  // one intermediate plane
+    const void *src[4];
+    int src_pitch = cp;
+    for (int c = 0; c < ncomp; c++) src[c] = coef[c];
+    for (int l = levels; l >= 1; l--) {
+        LevelIO io{};
+        io.w = ws[l - 1];
+        io.h = hs[l - 1];
+        io.ncomp = ncomp;
+        io.ll_pitch = src_pitch;
+        io.coef_pitch = cp;
+        for (int c = 0; c < ncomp; c++) {
+            io.ll[c] = src[c];
+            io.coef[c] = coef[c];
+        }
+        if (l == 1) {
+            io.out_pitch = out_pitch;
+            for (int c = 0; c < ncomp; c++) io.out[c] = out[c];
+            cudaError_t e = color >= 0 ? launch_idwt_last_color(ctx, io, wavelet, color, out_type, bits, true)
+                                       : launch_idwt_level(ctx, io, wavelet, rounding);
+            if (e != cudaSuccess) return cuda_status(ctx, e, "reverse DWT (last level)");
+        } else {
+            const int buf = (levels - l) & 1;
+            io.out_pitch = (int)sw;
+            for (int c = 0; c < ncomp; c++) io.out[c] = scratch + ((size_t)c * 2 + buf) * slab;
+            cudaError_t e = launch_idwt_level(ctx, io, wavelet, rounding);
+            if (e != cudaSuccess) return cuda_status(ctx, e, "reverse DWT");
+            for (int c = 0; c < ncomp; c++) src[c] = io.out[c];
+            src_pitch = (int)sw;
+        }
+    }
+    return TC_OK;
+}
+
+static size_t reverse_scratch_bytes(int w, int h, int levels, int ncomp)
+{
+    if (levels < 2) return 0;
+    return (size_t)ncomp * 2 * (size_t)((w + 1) / 2) * (size_t)((h + 1) / 2) * 4;
+}
+
+}  // namespace tc
+
+using namespace tc;
+
+// ============================ plan ===========================================
+
+struct tc_plan {
+    tc_ctx *ctx = nullptr;
+    struct Img {
+        tc_image_info info{};
+        uint64_t coef_off = 0;     // byte offset in the coefficient arena
+        size_t out_bytes = 0;
+    };
+    std::vector<Img> imgs;
+    DevBuf pool, desc, order, coef, scratch;
+    int ncblk = 0;
+    uint64_t pool_len = 0;
+    size_t scratch_per_img = 0;
+    float recon_r = 0.5f;
+};
+
+static int plan_build(tc_ctx *ctx, const uint8_t *const *cs, const size_t *lens, int n, tc_plan *P)
+{
+    P->ctx = ctx;
+    std::vector<Parsed> parsed(n);
+    std::string err;
+    uint64_t pool_total = 0, coef_total = 0;
+    size_t scratch_max = 0;
+    for (int i = 0; i < n; i++) {
+        if (!cs[i] || !lens[i]) return fail(ctx, TC_E_ARG, "empty codestream");
+        const int rc = parse_codestream(cs[i], lens[i], parsed[i], err);
+        if (rc) return fail(ctx, rc, "image " + std::to_string(i) + ": " + err);
+        const tc_image_info &inf = parsed[i].info;
+        tc_plan::Img im;
+        im.info = inf;
+        im.coef_off = coef_total;
+        coef_total += (uint64_t)inf.ncomp * inf.width * inf.height * 4;
+        coef_total = (coef_total + 255) & ~uint64_t(255);
+        im.out_bytes = (size_t)inf.ncomp * inf.width * inf.height * sample_bytes(inf.bits);
+        scratch_max = std::max(scratch_max, reverse_scratch_bytes(inf.width, inf.height, inf.levels, inf.ncomp));
+        P->imgs.push_back(im);
+        const uint64_t pl = parsed[i].pool_is_cs ? lens[i] : parsed[i].own_pool.size();
+        pool_total += (pl + 15) & ~uint64_t(15);
+        P->ncblk += (int)parsed[i].desc.size();
+    }
+    // Host staging: pool and rebased descriptors.
+    std::vector<uint8_t> hpool(pool_total ? pool_total : 16);
+    std::vector<tc_cblk_desc> hdesc;
+    hdesc.reserve(P->ncblk);
+    uint64_t po = 0;
+    for (int i = 0; i < n; i++) {
+        const uint8_t *src = parsed[i].pool_is_cs ? cs[i] : parsed[i].own_pool.data();
+        const uint64_t pl = parsed[i].pool_is_cs ? lens[i] : parsed[i].own_pool.size();
+        if (pl) std::memcpy(hpool.data() + po, src, pl);
+        const uint64_t elem_base = P->imgs[i].coef_off / 4;
+        for (tc_cblk_desc d : parsed[i].desc) {
+            d.seg_off += po;
+            d.out_off += elem_base;
+            hdesc.push_back(d);
+        }
+        po += (pl + 15) & ~uint64_t(15);
+    }
+    std::vector<uint32_t> horder(P->ncblk);
+    tc_t1_sort_order(hdesc.data(), P->ncblk, horder.data());
+    P->pool_len = pool_total;
+    P->scratch_per_img = scratch_max;
+    cudaError_t e;
+    if ((e = P->pool.ensure(hpool.size())) != cudaSuccess ||
+        (e = P->desc.ensure(sizeof(tc_cblk_desc) * std::max(1, P->ncblk))) != cudaSuccess ||
+        (e = P->order.ensure(sizeof(uint32_t) * std::max(1, P->ncblk))) != cudaSuccess ||
+        (e = P->coef.ensure(std::max<uint64_t>(coef_total, 256))) != cudaSuccess ||
+        (e = P->scratch.ensure(std::max<size_t>(scratch_max, 256))) != cudaSuccess)
+        return cuda_status(ctx, e, "plan allocation");
+    if ((e = cudaMemcpyAsync(P->pool.ptr, hpool.data(), hpool.size(), cudaMemcpyHostToDevice, ctx->stream)) ||
+        (e = cudaMemcpyAsync(P->desc.ptr, hdesc.data(), sizeof(tc_cblk_desc) * P->ncblk, cudaMemcpyHostToDevice,
+                             ctx->stream)) ||
+        (e = cudaMemcpyAsync(P->order.ptr, horder.data(), sizeof(uint32_t) * P->ncblk, cudaMemcpyHostToDevice,
+                             ctx->stream)))
+        return cuda_status(ctx, e, "plan upload");
+    if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return cuda_status(ctx, e, "plan upload");
+    return TC_OK;
+}
+
+static int plan_run(tc_plan *P, void *const *d_out)
+{
+    tc_ctx *ctx = P->ctx;
+    cudaError_t e = launch_t1_decode(ctx, static_cast<tc_cblk_desc *>(P->desc.ptr),
+                                     static_cast<uint32_t *>(P->order.ptr), P->ncblk,
+                                     static_cast<uint8_t *>(P->pool.ptr), P->pool_len, P->coef.ptr,
+                                     TC_T1_OUT_DEQUANT, P->recon_r);
+    if (e != cudaSuccess) return cuda_status(ctx, e, "Tier-1 launch");
+    for (size_t i = 0; i < P->imgs.size(); i++) {
+        const tc_image_info &inf = P->imgs[i].info;
+        char *coef = static_cast<char *>(P->coef.ptr) + P->imgs[i].coef_off;
+        const size_t plane = (size_t)inf.width * inf.height;
+        const int ob = sample_bytes(inf.bits);
+        void *cptr[4], *optr[4];
+        for (int c = 0; c < inf.ncomp; c++) {
+            cptr[c] = coef + (size_t)c * plane * 4;
+            optr[c] = static_cast<char *>(d_out[i]) + (size_t)c * plane * ob;
+        }
+        const int color = inf.mct && inf.ncomp >= 3 ? (inf.reversible ? TC_COLOR_RCT : TC_COLOR_ICT) : TC_COLOR_DC;
+        const int wavelet = inf.reversible ? 0 : 1;
+        const int otype = ob == 1 ? TC_U8 : TC_U16;
+        int rc;
+        if (inf.levels == 0) {
+            e = launch_color_inverse(ctx, color, inf.ncomp, cptr, inf.reversible ? TC_INT32 : TC_FLOAT32,
+                                     inf.width, optr, otype, inf.width, inf.width, inf.height, inf.bits);
+            rc = cuda_status(ctx, e, "colour");
+        } else {
+            rc = run_reverse(ctx, wavelet, TC_ROUND_FLOOR, cptr, inf.width, inf.width, inf.height, inf.levels,
+                             inf.ncomp, static_cast<char *>(P->scratch.ptr), optr, inf.width, color, otype,
+                             inf.bits);
+        }
+        if (rc) return rc;
+    }
+    return TC_OK;
+}
+
+// ============================ C ABI ==========================================
+
+extern "C" {
+
+int tc_version(void) { return 10000; }
+
+const char *tc_status_string(int s)
+{
+    switch (s) {
+    case TC_OK: return "ok";
+    case TC_E_ARG: return "invalid argument";
+    case TC_E_OOM: return "out of memory";
+    case TC_E_CODESTREAM: return "malformed codestream";
+    case TC_E_DEVICE: return "CUDA error";
+    case TC_E_TIMEOUT: return "device wait timed out";
+    case TC_E_UNSUPPORTED: return "unsupported codestream feature";
+    case TC_E_NOFILE: return "file not found";
+    default: return "unknown status";
+    }
+}
+
+int tc_ctx_create(int device, void *cuda_stream, tc_ctx **out)
+{
+    if (!out) return TC_E_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) return TC_E_DEVICE;
+    tc_ctx *ctx = new (std::nothrow) tc_ctx;
+    if (!ctx) return TC_E_OOM;
+    ctx->device = device;
+    ctx->stream = static_cast<cudaStream_t>(cuda_stream);
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaMalloc(&ctx->d_words, 4 * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMemset(ctx->d_words, 0, 4 * sizeof(uint32_t));
+    if (e != cudaSuccess) {
+        delete ctx;
+        return e == cudaErrorMemoryAllocation ? TC_E_OOM : TC_E_DEVICE;
+    }
+    *out = ctx;
+    return TC_OK;
+}
+
+int tc_ctx_destroy(tc_ctx *ctx)
+{
+    if (!ctx) return TC_E_ARG;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    ctx->scratch.release();
+    ctx->tmp_pool.release();
+    ctx->tmp_desc.release();
+    ctx->tmp_order.release();
+    ctx->tmp_coef.release();
+    ctx->tmp_out.release();
+    if (ctx->d_words) cudaFree(ctx->d_words);
+    delete ctx;
+    return TC_OK;
+}
+
+int tc_ctx_synchronize(tc_ctx *ctx)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_status(ctx, e, "synchronize");
+    uint32_t w = 0;
+    e = cudaMemcpy(&w, ctx->d_words, sizeof w, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_status(ctx, e, "read device error word");
+    if (w) {
+        cudaMemset(ctx->d_words, 0, sizeof w);
+        return fail(ctx, TC_E_CODESTREAM,
+                    (w & TC_DERR_POOL) ? "a code-block codeword runs past the segment pool"
+                                       : "a code-block descriptor is out of range");
+    }
+    return TC_OK;
+}
+
+const char *tc_ctx_last_error(const tc_ctx *ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+uint64_t tc_ctx_launch_count(const tc_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+int tc_t1_decode(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint32_t *d_order, int n, const uint8_t *d_pool,
+                 uint64_t pool_len, void *d_out, int out_mode, float recon_r)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (n < 0 || (n > 0 && (!d_desc || !d_out || (!d_pool && pool_len))) ||
+        (out_mode != TC_T1_OUT_DEQUANT && out_mode != TC_T1_OUT_RAW) || !(recon_r >= 0.0f && recon_r < 1.0f))
+        return fail(ctx, TC_E_ARG, "tc_t1_decode: bad argument");
+    return cuda_status(ctx, launch_t1_decode(ctx, d_desc, d_order, n, d_pool, pool_len, d_out, out_mode, recon_r),
+                       "tc_t1_decode");
+}
+
+int tc_t1_sort_order(const tc_cblk_desc *h_desc, int n, uint32_t *h_order)
+{
+    if (n < 0 || (n > 0 && (!h_desc || !h_order))) return TC_E_ARG;
+    std::vector<std::pair<uint64_t, uint32_t>> key(n);
+    for (int i = 0; i < n; i++) {
+        const tc_cblk_desc &d = h_desc[i];
+        const uint64_t work = (uint64_t)d.passes * d.w * d.h;
+        key[i] = {(work << 24) | std::min<uint64_t>(d.seg_len, (1u << 24) - 1), (uint32_t)i};
+    }
+    std::stable_sort(key.begin(), key.end(), [](const auto &a, const auto &b) { return a.first > b.first; });
+    for (int i = 0; i < n; i++) h_order[i] = key[i].second;
+    return TC_OK;
+}
+
+int tc_dequantize_raw(tc_ctx *ctx, const tc_cblk_desc *d_desc, int n, const uint32_t *d_raw, void *d_out,
+                      float recon_r)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (n < 0 || (n > 0 && (!d_desc || !d_raw || !d_out)) || !(recon_r >= 0.0f && recon_r < 1.0f))
+        return fail(ctx, TC_E_ARG, "tc_dequantize_raw: bad argument");
+    return cuda_status(ctx, launch_dequant_raw(ctx, d_desc, n, d_raw, d_out, recon_r), "tc_dequantize_raw");
+}
+
+static int dwt_args_ok(const void *in, int ip, const void *out, int op, int w, int h, int levels)
+{
+    return in && out && w > 0 && h > 0 && ip >= w && op >= w && levels >= 0 && levels <= 32;
+}
+
+static int dwt_forward(tc_ctx *ctx, int wavelet, int rounding, const void *d_in, int ip, void *d_out, int op, int w,
+                       int h, int levels)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!dwt_args_ok(d_in, ip, d_out, op, w, h, levels) || d_in == d_out)
+        return fail(ctx, TC_E_ARG, "forward DWT: bad argument");
+    if (levels == 0) {
+        cudaError_t e = cudaMemcpy2DAsync(d_out, (size_t)op * 4, d_in, (size_t)ip * 4, (size_t)w * 4, h,
+                                          cudaMemcpyDeviceToDevice, ctx->stream);
+        return cuda_status(ctx, e, "forward DWT copy");
+    }
+    // Level l reads the previous LL (the input for l = 1) and writes its LL
+    // into a ping-pong scratch plane; the deepest LL lands in the output.
+    std::vector<int> ws, hs;
+    level_sizes(w, h, levels, ws, hs);
+    const size_t slab = (size_t)ws[1] * hs[1] * 4;
+    cudaError_t e = ctx->scratch.ensure(2 * slab);
+    if (e != cudaSuccess) return cuda_status(ctx, e, "forward DWT scratch");
+    const void *src = d_in;
+    int sp = ip;
+    for (int l = 1; l <= levels; l++) {
+        LevelIO io{};
+        io.w = ws[l - 1];
+        io.h = hs[l - 1];
+        io.ncomp = 1;
+        io.ll[0] = src;
+        io.ll_pitch = sp;
+        io.bands[0] = d_out;
+        io.bands_pitch = op;
+        if (l == levels) {
+            io.out[0] = d_out;
+            io.out_pitch = op;
+        } else {
+            io.out[0] = static_cast<char *>(ctx->scratch.ptr) + ((l - 1) & 1) * slab;
+            io.out_pitch = ws[1];
+        }
+        e = launch_fdwt_level(ctx, io, wavelet, rounding);
+        if (e != cudaSuccess) return cuda_status(ctx, e, "forward DWT");
+        src = io.out[0];
+        sp = io.out_pitch;
+    }
+    return TC_OK;
+}
+
+static int dwt_reverse(tc_ctx *ctx, int wavelet, int rounding, const void *d_in, int ip, void *d_out, int op, int w,
+                       int h, int levels)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!dwt_args_ok(d_in, ip, d_out, op, w, h, levels) || d_in == d_out)
+        return fail(ctx, TC_E_ARG, "reverse DWT: bad argument");
+    if (levels == 0) {
+        cudaError_t e = cudaMemcpy2DAsync(d_out, (size_t)op * 4, d_in, (size_t)ip * 4, (size_t)w * 4, h,
+                                          cudaMemcpyDeviceToDevice, ctx->stream);
+        return cuda_status(ctx, e, "reverse DWT copy");
+    }
+    cudaError_t e = ctx->scratch.ensure(std::max<size_t>(reverse_scratch_bytes(w, h, levels, 1), 256));
+    if (e != cudaSuccess) return cuda_status(ctx, e, "reverse DWT scratch");
+    const void *in[1] = {d_in};
+    void *out[1] = {d_out};
+    return run_reverse(ctx, wavelet, rounding, in, ip, w, h, levels, 1, static_cast<char *>(ctx->scratch.ptr), out,
+                       op, -1, 0, 0);
+}
+
+int tc_dwt_forward53(tc_ctx *ctx, const int32_t *d_in, int in_pitch, int32_t *d_out, int out_pitch, int w, int h,
+                     int levels, int rounding)
+{
+    if (rounding != TC_ROUND_FLOOR && rounding != TC_ROUND_TRUNC) return fail(ctx, TC_E_ARG, "bad rounding");
+    return dwt_forward(ctx, 0, rounding, d_in, in_pitch, d_out, out_pitch, w, h, levels);
+}
+
+int tc_dwt_forward97(tc_ctx *ctx, const float *d_in, int in_pitch, float *d_out, int out_pitch, int w, int h,
+                     int levels)
+{
+    return dwt_forward(ctx, 1, 0, d_in, in_pitch, d_out, out_pitch, w, h, levels);
+}
+
+int tc_dwt_reverse53(tc_ctx *ctx, const int32_t *d_in, int in_pitch, int32_t *d_out, int out_pitch, int w, int h,
+                     int levels, int rounding)
+{
+    if (rounding != TC_ROUND_FLOOR && rounding != TC_ROUND_TRUNC) return fail(ctx, TC_E_ARG, "bad rounding");
+    return dwt_reverse(ctx, 0, rounding, d_in, in_pitch, d_out, out_pitch, w, h, levels);
+}
+
+int tc_dwt_reverse97(tc_ctx *ctx, const float *d_in, int in_pitch, float *d_out, int out_pitch, int w, int h,
+                     int levels)
+{
+    return dwt_reverse(ctx, 1, 0, d_in, in_pitch, d_out, out_pitch, w, h, levels);
+}
+
+static int color_args_ok(int kind, int ncomp, const void *const *in, const void *const *out, int ip, int op, int w,
+                         int h, int bits)
+{
+    if (kind < TC_COLOR_DC || kind > TC_COLOR_ICT || ncomp < 1 || ncomp > 4 || !in || !out) return 0;
+    if ((kind != TC_COLOR_DC) && ncomp < 3) return 0;
+    if (w <= 0 || h <= 0 || ip < w || op < w || bits < 1 || bits > 16) return 0;
+    for (int c = 0; c < ncomp; c++)
+        if (!in[c] || !out[c]) return 0;
+    return 1;
+}
+
+int tc_color_inverse(tc_ctx *ctx, int kind, int ncomp, void *const *d_in, int in_type, int in_pitch,
+                     void *const *d_out, int out_type, int out_pitch, int w, int h, int bits)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!color_args_ok(kind, ncomp, d_in, d_out, in_pitch, out_pitch, w, h, bits) ||
+        (in_type != TC_INT32 && in_type != TC_FLOAT32) ||
+        (out_type != TC_U8 && out_type != TC_U16 && out_type != TC_INT32) || (out_type == TC_U8 && bits > 8))
+        return fail(ctx, TC_E_ARG, "tc_color_inverse: bad argument");
+    return cuda_status(ctx,
+                       launch_color_inverse(ctx, kind, ncomp, d_in, in_type, in_pitch, d_out, out_type, out_pitch,
+                                            w, h, bits),
+                       "tc_color_inverse");
+}
+
+int tc_color_forward(tc_ctx *ctx, int kind, int ncomp, const void *const *d_in, int in_type, int in_pitch,
+                     void *const *d_out, int out_type, int out_pitch, int w, int h, int bits)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!color_args_ok(kind, ncomp, d_in, d_out, in_pitch, out_pitch, w, h, bits) ||
+        (in_type != TC_U8 && in_type != TC_U16 && in_type != TC_INT32) ||
+        (out_type != TC_INT32 && out_type != TC_FLOAT32))
+        return fail(ctx, TC_E_ARG, "tc_color_forward: bad argument");
+    return cuda_status(ctx,
+                       launch_color_forward(ctx, kind, ncomp, d_in, in_type, in_pitch, d_out, out_type, out_pitch,
+                                            w, h, bits),
+                       "tc_color_forward");
+}
+
+int tc_j2k_read_header(const uint8_t *h_cs, size_t len, tc_image_info *info)
+{
+    if (!h_cs || !info || len < 2) return TC_E_ARG;
+    std::string err;
+    return read_header(h_cs, len, *info, err);
+}
+
+int tc_j2k_parse(const uint8_t *h_cs, size_t len, tc_j2k_parsed **out)
+{
+    if (!h_cs || !out || len < 2) return TC_E_ARG;
+    *out = nullptr;
+    auto *holder = new (std::nothrow) Parsed;
+    if (!holder) return TC_E_OOM;
+    std::string err;
+    const int rc = parse_codestream(h_cs, len, *holder, err);
+    if (rc) {
+        delete holder;
+        return rc;
+    }
+    // The public struct is followed in memory by nothing we own; keep the
+    // Parsed object alive through a side allocation.
+    struct Box {
+        tc_j2k_parsed pub;
+        Parsed *own;
+    };
+    Box *b = new (std::nothrow) Box;
+    if (!b) {
+        delete holder;
+        return TC_E_OOM;
+    }
+    std::memset(&b->pub, 0, sizeof b->pub);
+    b->own = holder;
+    b->pub.info = holder->info;
+    b->pub.desc = holder->desc.data();
+    b->pub.pool_is_cs = holder->pool_is_cs ? 1 : 0;
+    b->pub.pool = holder->pool_is_cs ? h_cs : holder->own_pool.data();
+    b->pub.pool_len = holder->pool_is_cs ? len : holder->own_pool.size();
+    *out = &b->pub;
+    return TC_OK;
+}
+
+void tc_j2k_parsed_free(tc_j2k_parsed *p)
+{
+    if (!p) return;
+    struct Box {
+        tc_j2k_parsed pub;
+        Parsed *own;
+    };
+    Box *b = reinterpret_cast<Box *>(p);
+    delete b->own;
+    delete b;
+}
+
+int tc_plan_create(tc_ctx *ctx, const uint8_t *const *h_cs, const size_t *lens, int nimages, tc_plan **out)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!h_cs || !lens || nimages < 1 || !out) return fail(ctx, TC_E_ARG, "tc_plan_create: bad argument");
+    *out = nullptr;
+    auto *P = new (std::nothrow) tc_plan;
+    if (!P) return fail(ctx, TC_E_OOM, "tc_plan_create");
+    rc = plan_build(ctx, h_cs, lens, nimages, P);
+    if (rc) {
+        tc_plan_destroy(P);
+        return rc;
+    }
+    *out = P;
+    return TC_OK;
+}
+
+int tc_plan_destroy(tc_plan *P)
+{
+    if (!P) return TC_E_ARG;
+    if (P->ctx) {
+        cudaSetDevice(P->ctx->device);
+        cudaStreamSynchronize(P->ctx->stream);
+    }
+    P->pool.release();
+    P->desc.release();
+    P->order.release();
+    P->coef.release();
+    P->scratch.release();
+    delete P;
+    return TC_OK;
+}
+
+int tc_plan_output_bytes(const tc_plan *P, int image, size_t *bytes)
+{
+    if (!P || !bytes || image < 0 || image >= (int)P->imgs.size()) return TC_E_ARG;
+    *bytes = P->imgs[image].out_bytes;
+    return TC_OK;
+}
+
+int tc_plan_image_info(const tc_plan *P, int image, tc_image_info *info)
+{
+    if (!P || !info || image < 0 || image >= (int)P->imgs.size()) return TC_E_ARG;
+    *info = P->imgs[image].info;
+    return TC_OK;
+}
+
+int tc_plan_execute(tc_plan *P, void *const *d_out)
+{
+    if (!P || !d_out) return TC_E_ARG;
+    int rc = check_ctx(P->ctx);
+    if (rc) return rc;
+    for (size_t i = 0; i < P->imgs.size(); i++)
+        if (!d_out[i]) return fail(P->ctx, TC_E_ARG, "tc_plan_execute: null output");
+    return plan_run(P, d_out);
+}
+
+int tc_decode_j2k(tc_ctx *ctx, const uint8_t *h_cs, size_t len, void *h_out, size_t out_bytes, tc_image_info *info)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!h_cs || !len || !h_out) return fail(ctx, TC_E_ARG, "tc_decode_j2k: bad argument");
+    // The plan borrows the context's grow-only buffers, so repeated decodes
+    // of similar images allocate nothing after the first call.
+    tc_plan P;
+    P.pool = ctx->tmp_pool;
+    P.desc = ctx->tmp_desc;
+    P.order = ctx->tmp_order;
+    P.coef = ctx->tmp_coef;
+    P.scratch = ctx->scratch;
+    auto give_back = [&]() {
+        ctx->tmp_pool = P.pool;
+        ctx->tmp_desc = P.desc;
+        ctx->tmp_order = P.order;
+        ctx->tmp_coef = P.coef;
+        ctx->scratch = P.scratch;
+    };
+    const uint8_t *cs[1] = {h_cs};
+    size_t lens[1] = {len};
+    rc = plan_build(ctx, cs, lens, 1, &P);
+    if (rc) {
+        give_back();
+        return rc;
+    }
+    const size_t need = P.imgs[0].out_bytes;
+    if (info) *info = P.imgs[0].info;
+    if (out_bytes < need) {
+        give_back();
+        return fail(ctx, TC_E_ARG, "tc_decode_j2k: output buffer too small");
+    }
+    cudaError_t e = ctx->tmp_out.ensure(need);
+    if (e != cudaSuccess) {
+        give_back();
+        return cuda_status(ctx, e, "tc_decode_j2k output");
+    }
+    void *outs[1] = {ctx->tmp_out.ptr};
+    rc = plan_run(&P, outs);
+    give_back();
+    if (rc) return rc;
+    e = cudaMemcpyAsync(h_out, ctx->tmp_out.ptr, need, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e != cudaSuccess) return cuda_status(ctx, e, "tc_decode_j2k D2H");
+    return tc_ctx_synchronize(ctx);
+}
+
+int tc_decode_j2k_file(tc_ctx *ctx, const char *path, void *h_out, size_t out_bytes, tc_image_info *info)
+{
+    if (!path) return TC_E_ARG;
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return fail(ctx, TC_E_NOFILE, std::string("cannot open ") + path);
+    std::vector<uint8_t> buf;
+    uint8_t tmp[1 << 16];
+    size_t k;
+    while ((k = std::fread(tmp, 1, sizeof tmp, f)) > 0) buf.insert(buf.end(), tmp, tmp + k);
+    std::fclose(f);
+    return tc_decode_j2k(ctx, buf.data(), buf.size(), h_out, out_bytes, info);
+}
+
+int tc_encode_j2k(const tc_encode_params *p, const void *h_planes, uint8_t *h_out, size_t cap, size_t *out_len)
+{
+    if (!p || !h_planes || !out_len) return TC_E_ARG;
+    std::vector<uint8_t> cs;
+    std::string err;
+    const int rc = encode_codestream(*p, h_planes, cs, err);
+    if (rc) return rc;
+    *out_len = cs.size();
+    if (!h_out || cap < cs.size()) return TC_E_ARG;
+    std::memcpy(h_out, cs.data(), cs.size());
+    return TC_OK;
+}
+
+int tc_t1_encode_block(const int32_t *h_coef, int w, int h, int orient, int mb, int passes, uint8_t *h_out, int cap,
+                       int *len, int *passes_out, int *zero_bitplanes)
+{
+    if (!h_coef || !len || !passes_out || !zero_bitplanes) return TC_E_ARG;
+    std::vector<uint8_t> out;
+    const int rc = t1_encode_block(h_coef, w, h, orient, mb, passes, out, passes_out, zero_bitplanes);
+    if (rc) return rc;
+    *len = (int)out.size();
+    if ((int)out.size() > cap || (!h_out && !out.empty())) return TC_E_ARG;
+    if (!out.empty()) std::memcpy(h_out, out.data(), out.size());
+    return TC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,1375 @@
+// j2k_host.cpp -- host-side JPEG 2000 codestream handling for the B200 decode
+// pipeline:
+//   * geometry of resolutions / subbands / code-blocks (ISO B.5-B.7),
+//   * the Tier-2 parser that turns a codestream into tc_cblk_desc records
+//     (the hand-off the reference makes through codeBlockCallback,
+//     codestream.c:336-470),
+//   * the harness encoder used to generate test and benchmark codestreams:
+//     forward colour transform + DWT on the CPU, deadzone quantisation, an
+//     MQ/EBCOT Tier-1 encoder and a single-tile packet writer.
+// The encoder exists because the reference ships no encoder and no sample
+// files; it writes the subset the parser reads (one tile, one precinct per
+// resolution, code-block style 0).
+#include "j2k_host.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <thread>
+
+namespace tc {
+
+// ============================ small utilities ================================
+
+static int hw_threads(int req)
+{
+    if (req > 0) return req;
+    unsigned n = std::thread::hardware_concurrency();
+    return n ? (int)n : 1;
+}
+
+static void parallel_for(int n, int threads, const std::function<void(int)> &fn)
+{
+    threads = std::min(hw_threads(threads), std::max(n, 1));
+    if (threads <= 1) {
+        for (int i = 0; i < n; i++) fn(i);
+        return;
+    }
+    std::atomic<int> next{0};
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; t++)
+        pool.emplace_back([&] {
+            for (int i; (i = next.fetch_add(1)) < n;) fn(i);
+        });
+    for (auto &th : pool) th.join();
+}
+
+static inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
+
+// ============================ geometry ======================================
+
+void level_sizes(int w, int h, int levels, std::vector<int> &ws, std::vector<int> &hs)
+{
+    ws.assign(levels + 1, 0);
+    hs.assign(levels + 1, 0);
+    ws[0] = w;
+    hs[0] = h;
+    for (int d = 1; d <= levels; d++) {
+        ws[d] = (ws[d - 1] + 1) / 2;
+        hs[d] = (hs[d - 1] + 1) / 2;
+    }
+}
+
+std::vector<Resolution> make_geometry(int w, int h, int levels, int xcb, int ycb)
+{
+    std::vector<int> ws, hs;
+    level_sizes(w, h, levels, ws, hs);
+    std::vector<Resolution> res(levels + 1);
+    auto finish = [&](Band &b) {
+        b.cbw_log2 = xcb;
+        b.cbh_log2 = ycb;
+        b.ncbx = b.w > 0 ? ceil_div(b.w, 1 << xcb) : 0;
+        b.ncby = b.h > 0 ? ceil_div(b.h, 1 << ycb) : 0;
+    };
+    Band ll;
+    ll.orient = 0;
+    ll.level = levels;
+    ll.w = ws[levels];
+    ll.h = hs[levels];
+    finish(ll);
+    res[0].w = ws[levels];
+    res[0].h = hs[levels];
+    res[0].bands.push_back(ll);
+    for (int r = 1; r <= levels; r++) {
+        const int d = levels - r + 1;
+        res[r].w = ws[d - 1];
+        res[r].h = hs[d - 1];
+        for (int o = 1; o <= 3; o++) {
+            Band b;
+            b.orient = o;
+            b.level = d;
+            b.x0 = (o & 1) ? ws[d] : 0;
+            b.y0 = (o & 2) ? hs[d] : 0;
+            b.w = (o & 1) ? ws[d - 1] - ws[d] : ws[d];
+            b.h = (o & 2) ? hs[d - 1] - hs[d] : hs[d];
+            finish(b);
+            res[r].bands.push_back(b);
+        }
+    }
+    return res;
+}
+
+// ============================ DWT (CPU, encoder side) =======================
+
+static inline int pse(int i, int n)
+{
+    if (n == 1) return 0;
+    const int per = 2 * (n - 1);
+    i %= per;
+    if (i < 0) i += per;
+    return i >= n ? per - i : i;
+}
+
+static inline int32_t floordiv(int32_t a, int b)
+{
+    int32_t q = a / b;
+    if ((a % b) != 0 && ((a < 0) != (b < 0))) q--;
+    return q;
+}
+
+static const double kA = -1.586134342059924, kB = -0.052980118572961,
+                    kG = 0.882911075530934, kD = 0.443506852043971,
+                    kK = 1.230174104914001;
+
+static void fwd53_line(int32_t *x, int n)
+{
+    if (n < 2) return;
+    for (int k = 1; k < n; k += 2) x[k] -= floordiv(x[pse(k - 1, n)] + x[pse(k + 1, n)], 2);
+    for (int k = 0; k < n; k += 2) x[k] += floordiv(x[pse(k - 1, n)] + x[pse(k + 1, n)] + 2, 4);
+}
+
+static void fwd97_line(double *x, int n)
+{
+    if (n < 2) return;
+    for (int k = 1; k < n; k += 2) x[k] += kA * (x[pse(k - 1, n)] + x[pse(k + 1, n)]);
+    for (int k = 0; k < n; k += 2) x[k] += kB * (x[pse(k - 1, n)] + x[pse(k + 1, n)]);
+    for (int k = 1; k < n; k += 2) x[k] += kG * (x[pse(k - 1, n)] + x[pse(k + 1, n)]);
+    for (int k = 0; k < n; k += 2) x[k] += kD * (x[pse(k - 1, n)] + x[pse(k + 1, n)]);
+    for (int k = 1; k < n; k += 2) x[k] *= kK;
+    for (int k = 0; k < n; k += 2) x[k] *= 1.0 / kK;
+}
+
+static void inv97_line(double *x, int n)
+{
+    if (n < 2) return;
+    for (int k = 0; k < n; k += 2) x[k] *= kK;
+    for (int k = 1; k < n; k += 2) x[k] *= 1.0 / kK;
+    for (int k = 0; k < n; k += 2) x[k] -= kD * (x[pse(k - 1, n)] + x[pse(k + 1, n)]);
+    for (int k = 1; k < n; k += 2) x[k] -= kG * (x[pse(k - 1, n)] + x[pse(k + 1, n)]);
+    for (int k = 0; k < n; k += 2) x[k] -= kB * (x[pse(k - 1, n)] + x[pse(k + 1, n)]);
+    for (int k = 1; k < n; k += 2) x[k] -= kA * (x[pse(k - 1, n)] + x[pse(k + 1, n)]);
+}
+
+static void inv53r_line(double *x, int n)
+{
+    if (n < 2) return;
+    for (int k = 0; k < n; k += 2) x[k] -= 0.25 * (x[pse(k - 1, n)] + x[pse(k + 1, n)]);
+    for (int k = 1; k < n; k += 2) x[k] += 0.5 * (x[pse(k - 1, n)] + x[pse(k + 1, n)]);
+}
+
+// Forward multi-level transform on a plane (vertical then horizontal per
+// level, ISO F.4.2), output in Mallat layout.
+template <typename T, typename F>
+static void fwd_plane_pitch(T *x, int w, int h, size_t pitch, int levels, F line_fn, int threads)
+{
+    for (int l = 0; l < levels; l++) {
+        const int nl_h = (h + 1) / 2, nl_w = (w + 1) / 2;
+        // vertical
+        const int cgroups = ceil_div(w, 16);
+        parallel_for(cgroups, threads, [&](int g) {
+            std::vector<T> a(h), b(h);
+            for (int c = g * 16; c < std::min(w, g * 16 + 16); c++) {
+                for (int i = 0; i < h; i++) a[i] = x[(size_t)i * pitch + c];
+                line_fn(a.data(), h);
+                for (int i = 0; i < h; i++) b[(i & 1) ? nl_h + i / 2 : i / 2] = a[i];
+                for (int i = 0; i < h; i++) x[(size_t)i * pitch + c] = b[i];
+            }
+        });
+        // horizontal
+        parallel_for(h, threads, [&](int r) {
+            std::vector<T> a(w);
+            T *row = x + (size_t)r * pitch;
+            for (int i = 0; i < w; i++) a[i] = row[i];
+            line_fn(a.data(), w);
+            for (int i = 0; i < w; i++) row[(i & 1) ? nl_w + i / 2 : i / 2] = a[i];
+        });
+        w = nl_w;
+        h = nl_h;
+    }
+}
+
+double subband_norm(bool wavelet97, int level, int orient)
+{
+    auto norm1d = [&](int lvl, int high) {
+        const int n = 1 << (lvl + 7);
+        std::vector<double> x(n, 0.0), t(n);
+        int len = n;
+        for (int l = 0; l < lvl; l++) len = (len + 1) / 2;
+        x[high ? len + len / 2 : len / 2] = 1.0;
+        for (int l = lvl - 1; l >= 0; l--) {
+            int m = n;
+            for (int k = 0; k < l; k++) m = (m + 1) / 2;
+            for (int i = 0; i < m; i++) t[i] = x[(i & 1) ? (m + 1) / 2 + i / 2 : i / 2];
+            if (wavelet97) inv97_line(t.data(), m);
+            else inv53r_line(t.data(), m);
+            std::copy(t.begin(), t.begin() + m, x.begin());
+        }
+        double s = 0.0;
+        for (double v : x) s += v * v;
+        return std::sqrt(s);
+    };
+    const double lo = norm1d(level, 0), hi = norm1d(level, 1);
+    switch (orient) {
+    case 0: return lo * lo;
+    case 1: return hi * lo;
+    case 2: return lo * hi;
+    default: return hi * hi;
+    }
+}
+
+// ============================ MQ encoder (ISO C.2) ==========================
+
+static const uint16_t kQe[47] = {
+    0x5601, 0x3401, 0x1801, 0x0AC1, 0x0521, 0x0221, 0x5601, 0x5401, 0x4801, 0x3801,
+    0x3001, 0x2401, 0x1C01, 0x1601, 0x5601, 0x5401, 0x5101, 0x4801, 0x3801, 0x3401,
+    0x3001, 0x2801, 0x2401, 0x2201, 0x1C01, 0x1801, 0x1601, 0x1401, 0x1201, 0x1101,
+    0x0AC1, 0x09C1, 0x08A1, 0x0521, 0x0441, 0x02A1, 0x0221, 0x0141, 0x0111, 0x0085,
+    0x0049, 0x0025, 0x0015, 0x0009, 0x0005, 0x0001, 0x5601};
+static const uint8_t kNMPS[47] = {
+    1, 2, 3, 4, 5, 38, 7, 8, 9, 10, 11, 12, 13, 29, 15, 16, 17, 18, 19, 20,
+    21, 22, 23, 24, 25, 26, 27, 28, 29, 30, 31, 32, 33, 34, 35, 36, 37, 38, 39, 40,
+    41, 42, 43, 44, 45, 45, 46};
+static const uint8_t kNLPS[47] = {
+    1, 6, 9, 12, 29, 33, 6, 14, 14, 14, 17, 18, 20, 21, 14, 14, 15, 16, 17, 18,
+    19, 19, 20, 21, 22, 23, 24, 25, 26, 27, 28, 29, 30, 31, 32, 33, 34, 35, 36, 37,
+    38, 39, 40, 41, 42, 43, 46};
+static const uint8_t kSW[47] = {1, 0, 0, 0, 0, 0, 1, 0, 0, 0, 0, 0, 0, 0, 1, 0};
+
+struct MQEnc {
+    std::vector<uint8_t> buf;  // buf[0] is the byte before the codeword
+    size_t bp = 0;
+    uint32_t a = 0x8000, c = 0;
+    int ct = 12;
+    uint8_t idx[19]{}, mps[19]{};
+
+    MQEnc()
+    {
+        buf.reserve(4096);
+        buf.push_back(0);
+        idx[0] = 4;
+        idx[18] = 3;
+        idx[17] = 46;
+    }
+    void put(uint32_t v)
+    {
+        bp++;
+        if (bp >= buf.size()) buf.push_back((uint8_t)v);
+        else buf[bp] = (uint8_t)v;
+    }
+    void byteout()
+    {
+        if (buf[bp] == 0xFF) {
+            put(c >> 20);
+            c &= 0xFFFFF;
+            ct = 7;
+        } else if (c < 0x8000000) {
+            put(c >> 19);
+            c &= 0x7FFFF;
+            ct = 8;
+        } else {
+            buf[bp]++;
+            if (buf[bp] == 0xFF) {
+                c &= 0x7FFFFFF;
+                put(c >> 20);
+                c &= 0xFFFFF;
+                ct = 7;
+            } else {
+                put(c >> 19);
+                c &= 0x7FFFF;
+                ct = 8;
+            }
+        }
+    }
+    void renorm()
+    {
+        do {
+            a <<= 1;
+            c <<= 1;
+            if (--ct == 0) byteout();
+        } while ((a & 0x8000) == 0);
+    }
+    void encode(int d, int cx)
+    {
+        const int s = idx[cx];
+        const uint32_t qe = kQe[s];
+        a -= qe;
+        if (d == mps[cx]) {
+            if ((a & 0x8000) == 0) {
+                if (a < qe) a = qe;
+                else c += qe;
+                idx[cx] = kNMPS[s];
+                renorm();
+            } else {
+                c += qe;
+            }
+        } else {
+            if (a < qe) c += qe;
+            else a = qe;
+            if (kSW[s]) mps[cx] ^= 1;
+            idx[cx] = kNLPS[s];
+            renorm();
+        }
+    }
+    // FLUSH (ISO C.2.9) and return the codeword length.
+    size_t flush()
+    {
+        const uint32_t tempc = c + a;
+        c |= 0xFFFF;
+        if (c >= tempc) c -= 0x8000;
+        c <<= ct;
+        byteout();
+        c <<= ct;
+        byteout();
+        return buf[bp] == 0xFF ? bp - 1 : bp;
+    }
+};
+
+// ============================ Tier-1 encoder (ISO D) ========================
+
+namespace {
+struct T1Enc {
+    int w, h, W;
+    std::vector<uint8_t> sig, sgn, ref, vis;
+    std::vector<uint32_t> mag;
+    const int32_t *coef;
+    int orient;
+    MQEnc mq;
+
+    T1Enc(const int32_t *c, int w_, int h_, int o)
+        : w(w_), h(h_), W(w_ + 2), sig((w_ + 2) * (h_ + 2)), sgn(sig.size()), ref(sig.size()),
+          vis(sig.size()), mag((size_t)w_ * h_), coef(c), orient(o)
+    {
+        for (int i = 0; i < w * h; i++) mag[i] = (uint32_t)std::abs((int64_t)coef[i]);
+    }
+    uint8_t &S(std::vector<uint8_t> &v, int x, int y) { return v[(y + 1) * W + x + 1]; }
+    int bit(int x, int y, int p) const { return (mag[y * w + x] >> p) & 1; }
+    int neg(int x, int y) const { return coef[y * w + x] < 0; }
+
+    void counts(int x, int y, int &hh, int &vv, int &dd)
+    {
+        hh = S(sig, x - 1, y) + S(sig, x + 1, y);
+        vv = S(sig, x, y - 1) + S(sig, x, y + 1);
+        dd = S(sig, x - 1, y - 1) + S(sig, x + 1, y - 1) + S(sig, x - 1, y + 1) + S(sig, x + 1, y + 1);
+    }
+    int zc(int hh, int vv, int dd) const
+    {
+        if (orient == 1) std::swap(hh, vv);
+        if (orient == 3) {
+            const int hv = hh + vv;
+            if (dd >= 3) return 8;
+            if (dd == 2) return hv >= 1 ? 7 : 6;
+            if (dd == 1) return hv >= 2 ? 5 : (hv == 1 ? 4 : 3);
+            return hv >= 2 ? 2 : hv;
+        }
+        if (hh == 2) return 8;
+        if (hh == 1) return vv >= 1 ? 7 : (dd >= 1 ? 6 : 5);
+        if (vv == 2) return 4;
+        if (vv == 1) return 3;
+        return dd >= 2 ? 2 : dd;
+    }
+    void code_sign(int x, int y)
+    {
+        auto contrib = [&](int xx, int yy) { return S(sig, xx, yy) ? (S(sgn, xx, yy) ? -1 : 1) : 0; };
+        int hc = contrib(x - 1, y) + contrib(x + 1, y);
+        int vc = contrib(x, y - 1) + contrib(x, y + 1);
+        hc = std::max(-1, std::min(1, hc));
+        vc = std::max(-1, std::min(1, vc));
+        int cx, xr;
+        if (hc == 0) {
+            cx = vc == 0 ? 9 : 10;
+            xr = vc < 0;
+        } else {
+            cx = 12 + hc * vc;
+            xr = hc < 0;
+        }
+        const int s = neg(x, y);
+        mq.encode(s ^ xr, cx);
+        S(sgn, x, y) = (uint8_t)s;
+        S(sig, x, y) = 1;
+    }
+    void spp(int p)
+    {
+        for (int y0 = 0; y0 < h; y0 += 4)
+            for (int x = 0; x < w; x++)
+                for (int y = y0; y < std::min(h, y0 + 4); y++) {
+                    int hh, vv, dd;
+                    if (S(sig, x, y)) continue;
+                    counts(x, y, hh, vv, dd);
+                    if (hh + vv + dd == 0) continue;
+                    S(vis, x, y) = 1;
+                    const int b = bit(x, y, p);
+                    mq.encode(b, zc(hh, vv, dd));
+                    if (b) code_sign(x, y);
+                }
+    }
+    void mrp(int p)
+    {
+        for (int y0 = 0; y0 < h; y0 += 4)
+            for (int x = 0; x < w; x++)
+                for (int y = y0; y < std::min(h, y0 + 4); y++) {
+                    int hh, vv, dd;
+                    if (!S(sig, x, y) || S(vis, x, y)) continue;
+                    counts(x, y, hh, vv, dd);
+                    mq.encode(bit(x, y, p), S(ref, x, y) ? 16 : (hh + vv + dd ? 15 : 14));
+                    S(ref, x, y) = 1;
+                }
+    }
+    void cup(int p)
+    {
+        for (int y0 = 0; y0 < h; y0 += 4)
+            for (int x = 0; x < w; x++) {
+                int y = y0;
+                if (y0 + 4 <= h) {
+                    bool ok = true;
+                    for (int k = 0; k < 4 && ok; k++) {
+                        int hh, vv, dd;
+                        if (S(sig, x, y0 + k) || S(vis, x, y0 + k)) { ok = false; break; }
+                        counts(x, y0 + k, hh, vv, dd);
+                        if (hh + vv + dd) ok = false;
+                    }
+                    if (ok) {
+                        int r = -1;
+                        for (int k = 0; k < 4; k++)
+                            if (bit(x, y0 + k, p)) { r = k; break; }
+                        if (r < 0) {
+                            mq.encode(0, 18);
+                            continue;
+                        }
+                        mq.encode(1, 18);
+                        mq.encode(r >> 1, 17);
+                        mq.encode(r & 1, 17);
+                        code_sign(x, y0 + r);
+                        y = y0 + r + 1;
+                    }
+                }
+                for (; y < std::min(h, y0 + 4); y++) {
+                    int hh, vv, dd;
+                    if (S(sig, x, y) || S(vis, x, y)) continue;
+                    counts(x, y, hh, vv, dd);
+                    const int b = bit(x, y, p);
+                    mq.encode(b, zc(hh, vv, dd));
+                    if (b) code_sign(x, y);
+                }
+            }
+    }
+};
+}  // namespace
+
+int t1_encode_block(const int32_t *coef, int w, int h, int orient, int mb, int passes,
+                    std::vector<uint8_t> &out, int *passes_out, int *zero_bitplanes)
+{
+    if (w < 1 || h < 1 || w > 64 || h > 64 || orient < 0 || orient > 3 || mb < 1 || mb > 31)
+        return TC_E_ARG;
+    uint32_t mx = 0;
+    for (int i = 0; i < w * h; i++) mx = std::max(mx, (uint32_t)std::abs((int64_t)coef[i]));
+    int numbps = 0;
+    while (numbps < 32 && (mx >> numbps)) numbps++;
+    if (numbps > mb) return TC_E_ARG;
+    *zero_bitplanes = mb - numbps;
+    out.clear();
+    if (numbps == 0) {
+        *passes_out = 0;
+        return TC_OK;
+    }
+    const int total = 3 * numbps - 2;
+    if (passes <= 0 || passes > total) passes = total;
+    T1Enc e(coef, w, h, orient);
+    int done = 0;
+    for (int p = numbps - 1; p >= 0 && done < passes; p--) {
+        if (p != numbps - 1) {
+            e.spp(p);
+            if (++done >= passes) break;
+            e.mrp(p);
+            if (++done >= passes) break;
+        }
+        e.cup(p);
+        ++done;
+        std::fill(e.vis.begin(), e.vis.end(), 0);
+    }
+    const size_t len = e.mq.flush();
+    out.assign(e.mq.buf.begin() + 1, e.mq.buf.begin() + 1 + len);
+    *passes_out = passes;
+    return TC_OK;
+}
+
+// ============================ bit I/O and tag trees =========================
+
+namespace {
+struct BitWriter {
+    std::vector<uint8_t> &out;
+    uint32_t cur = 0;
+    int ct = 8;
+    explicit BitWriter(std::vector<uint8_t> &o) : out(o) {}
+    void put(int b)
+    {
+        if (ct == 0) {
+            out.push_back((uint8_t)cur);
+            ct = (cur == 0xFF) ? 7 : 8;
+            cur = 0;
+        }
+        ct--;
+        cur |= (uint32_t)(b & 1) << ct;
+    }
+    void put_bits(uint32_t v, int n)
+    {
+        for (int i = n - 1; i >= 0; i--) put((v >> i) & 1);
+    }
+    // Packet header end (ISO B.10.1): emit the partial byte; a final 0xFF is
+    // followed by a zero byte so the header never ends on 0xFF.
+    void flush()
+    {
+        out.push_back((uint8_t)cur);
+        if (cur == 0xFF) out.push_back(0);
+        cur = 0;
+        ct = 8;
+    }
+};
+
+struct BitReader {
+    const uint8_t *p;
+    size_t pos, end;
+    uint32_t cur = 0;
+    int ct = 0;
+    bool overrun = false;
+    BitReader(const uint8_t *d, size_t start, size_t e) : p(d), pos(start), end(e) {}
+    int get()
+    {
+        if (ct == 0) {
+            const bool ff = (cur == 0xFF);
+            if (pos >= end) {
+                overrun = true;
+                cur = 0;
+            } else {
+                cur = p[pos++];
+            }
+            ct = ff ? 7 : 8;
+        }
+        ct--;
+        return (cur >> ct) & 1;
+    }
+    uint32_t get_bits(int n)
+    {
+        uint32_t v = 0;
+        for (int i = 0; i < n; i++) v = (v << 1) | (uint32_t)get();
+        return v;
+    }
+    void align()
+    {
+        if (cur == 0xFF) {
+            if (pos >= end) overrun = true;
+            else pos++;
+        }
+        cur = 0;
+        ct = 0;
+    }
+};
+
+// Tag tree (ISO B.10.2) over a gw x gh grid of leaves.
+struct TagTree {
+    struct Node {
+        int parent;
+        int value;
+        int low;
+        bool known;
+    };
+    std::vector<Node> nodes;
+    int gw = 0, gh = 0;
+    TagTree(int w, int h) : gw(w), gh(h)
+    {
+        std::vector<std::pair<int, int>> dims;
+        int cw = w, ch = h;
+        do {
+            dims.emplace_back(cw, ch);
+            cw = (cw + 1) / 2;
+            ch = (ch + 1) / 2;
+        } while (dims.back().first * dims.back().second > 1);
+        int total = 0;
+        for (auto &d : dims) total += d.first * d.second;
+        nodes.assign(total, Node{-1, 0x7FFFFFFF, 0, false});
+        int off = 0;
+        for (size_t l = 0; l + 1 < dims.size(); l++) {
+            const int lw = dims[l].first, lh = dims[l].second;
+            const int poff = off + lw * lh;
+            const int pw = dims[l + 1].first;
+            for (int y = 0; y < lh; y++)
+                for (int x = 0; x < lw; x++) nodes[off + y * lw + x].parent = poff + (y / 2) * pw + x / 2;
+            off = poff;
+        }
+    }
+    void set_leaves(const std::vector<int> &vals)
+    {
+        for (auto &n : nodes) n.value = 0x7FFFFFFF;
+        for (size_t i = 0; i < vals.size(); i++) {
+            int k = (int)i;
+            while (k >= 0) {
+                nodes[k].value = std::min(nodes[k].value, vals[i]);
+                k = nodes[k].parent;
+            }
+        }
+    }
+    void path(int leaf, int *stk, int &n) const
+    {
+        n = 0;
+        for (int k = leaf; k >= 0; k = nodes[k].parent) stk[n++] = k;
+    }
+    void encode(BitWriter &bw, int leaf, int threshold)
+    {
+        int stk[40], n;
+        path(leaf, stk, n);
+        int low = 0;
+        for (int i = n - 1; i >= 0; i--) {
+            Node &nd = nodes[stk[i]];
+            if (low > nd.low) nd.low = low;
+            else low = nd.low;
+            while (low < threshold) {
+                if (low >= nd.value) {
+                    if (!nd.known) {
+                        bw.put(1);
+                        nd.known = true;
+                    }
+                    break;
+                }
+                bw.put(0);
+                low++;
+            }
+            nd.low = low;
+        }
+    }
+    // Returns 1 when the leaf's value is below threshold.
+    int decode(BitReader &br, int leaf, int threshold)
+    {
+        int stk[40], n;
+        path(leaf, stk, n);
+        int low = 0;
+        for (int i = n - 1; i >= 0; i--) {
+            Node &nd = nodes[stk[i]];
+            if (low > nd.low) nd.low = low;
+            else low = nd.low;
+            while (low < threshold && low < nd.value) {
+                if (br.get()) nd.value = low;
+                else low++;
+                if (br.overrun) return 0;
+            }
+            nd.low = low;
+        }
+        return nodes[leaf].value < threshold;
+    }
+    void reset_decoder()
+    {
+        for (auto &n : nodes) {
+            n.value = 0x7FFFFFFF;
+            n.low = 0;
+            n.known = false;
+        }
+    }
+};
+
+static void put_num_passes(BitWriter &bw, int n)
+{
+    if (n == 1) bw.put(0);
+    else if (n == 2) bw.put_bits(2, 2);
+    else if (n <= 5) { bw.put_bits(3, 2); bw.put_bits(n - 3, 2); }
+    else if (n <= 36) { bw.put_bits(0xF, 4); bw.put_bits(n - 6, 5); }
+    else { bw.put_bits(0x1FF, 9); bw.put_bits(n - 37, 7); }
+}
+
+// ISO Table B.4 (decode_num_coding_passes, codestream.c:300-313).
+static int get_num_passes(BitReader &br)
+{
+    if (!br.get()) return 1;
+    if (!br.get()) return 2;
+    int n = (int)br.get_bits(2);
+    if (n != 3) return 3 + n;
+    n = (int)br.get_bits(5);
+    if (n != 31) return 6 + n;
+    return 37 + (int)br.get_bits(7);
+}
+
+static int floorlog2(int a)
+{
+    int l = 0;
+    while (a > 1) { a >>= 1; l++; }
+    return l;
+}
+}  // namespace
+
+// ============================ codestream markers ============================
+
+enum : uint16_t {
+    M_SOC = 0xFF4F, M_SIZ = 0xFF51, M_COD = 0xFF52, M_COC = 0xFF53, M_TLM = 0xFF55,
+    M_PLM = 0xFF57, M_PLT = 0xFF58, M_QCD = 0xFF5C, M_QCC = 0xFF5D, M_RGN = 0xFF5E,
+    M_POC = 0xFF5F, M_PPM = 0xFF60, M_PPT = 0xFF61, M_CRG = 0xFF63, M_COM = 0xFF64,
+    M_SOT = 0xFF90, M_SOP = 0xFF91, M_EPH = 0xFF92, M_SOD = 0xFF93, M_EOC = 0xFFD9
+};
+
+namespace {
+struct Writer {
+    std::vector<uint8_t> &o;
+    void u8(uint32_t v) { o.push_back((uint8_t)v); }
+    void u16(uint32_t v) { u8(v >> 8); u8(v); }
+    void u32(uint32_t v) { u16(v >> 16); u16(v & 0xFFFF); }
+};
+
+struct Reader {
+    const uint8_t *d;
+    size_t len, pos = 0;
+    bool bad = false;
+    uint32_t u8()
+    {
+        if (pos + 1 > len) { bad = true; return 0; }
+        return d[pos++];
+    }
+    uint32_t u16() { uint32_t a = u8(); return (a << 8) | u8(); }
+    uint32_t u32() { uint32_t a = u16(); return (a << 16) | u16(); }
+};
+
+// Main-header coding parameters (COD/QCD), shared by all components.
+struct Params {
+    int width = 0, height = 0, ncomp = 0, bits = 0, is_signed = 0;
+    int tw = 0, th = 0;
+    int scod = 0, prog = 0, layers = 1, mct = 0;
+    int levels = 0, xcb = 6, ycb = 6, cblk_style = 0, reversible = 1;
+    std::vector<int> ppx, ppy;
+    int qstyle = 0, guard = 2;
+    std::vector<int> q_eps, q_mu;  // as signalled (1 or 3N+1 entries)
+    bool have_siz = false, have_cod = false, have_qcd = false;
+};
+}  // namespace
+
+static int parse_main(Reader &rd, Params &P, std::string &err)
+{
+    if (rd.u16() != M_SOC) { err = "missing SOC marker"; return TC_E_CODESTREAM; }
+    for (;;) {
+        const uint32_t m = rd.u16();
+        if (rd.bad) { err = "truncated main header"; return TC_E_CODESTREAM; }
+        if (m == M_SOT) { rd.pos -= 2; break; }
+        if ((m >> 8) != 0xFF) { err = "expected a marker in the main header"; return TC_E_CODESTREAM; }
+        const uint32_t L = rd.u16();
+        const size_t seg_end = rd.pos - 2 + L;
+        if (L < 2 || seg_end > rd.len) { err = "bad marker segment length"; return TC_E_CODESTREAM; }
+        switch (m) {
+        case M_SIZ: {
+            rd.u16();  // Rsiz
+            const uint32_t xs = rd.u32(), ys = rd.u32(), xo = rd.u32(), yo = rd.u32();
+            const uint32_t xt = rd.u32(), yt = rd.u32(), xto = rd.u32(), yto = rd.u32();
+            const uint32_t c = rd.u16();
+            if (xo || yo || xto || yto) { err = "image or tile offsets are not supported"; return TC_E_UNSUPPORTED; }
+            if (c < 1 || c > 4) { err = "1 to 4 components supported"; return TC_E_UNSUPPORTED; }
+            if (xs == 0 || ys == 0 || xs > 65535 || ys > 65535) { err = "image size out of range"; return TC_E_UNSUPPORTED; }
+            P.width = (int)xs; P.height = (int)ys; P.tw = (int)xt; P.th = (int)yt; P.ncomp = (int)c;
+            for (uint32_t i = 0; i < c; i++) {
+                const uint32_t ss = rd.u8(), dx = rd.u8(), dy = rd.u8();
+                const int b = (int)(ss & 0x7F) + 1, sg = (int)(ss >> 7);
+                if (dx != 1 || dy != 1) { err = "component subsampling is not supported"; return TC_E_UNSUPPORTED; }
+                if (i == 0) { P.bits = b; P.is_signed = sg; }
+                else if (b != P.bits || sg != P.is_signed) { err = "components must share bit depth"; return TC_E_UNSUPPORTED; }
+            }
+            if (P.bits > 16) { err = "bit depth above 16"; return TC_E_UNSUPPORTED; }
+            if (P.is_signed) { err = "signed samples are not supported"; return TC_E_UNSUPPORTED; }
+            P.have_siz = true;
+            break;
+        }
+        case M_COD: {
+            P.scod = (int)rd.u8();
+            P.prog = (int)rd.u8();
+            P.layers = (int)rd.u16();
+            P.mct = (int)rd.u8();
+            P.levels = (int)rd.u8();
+            P.xcb = (int)rd.u8() + 2;
+            P.ycb = (int)rd.u8() + 2;
+            P.cblk_style = (int)rd.u8();
+            P.reversible = (int)rd.u8();
+            if (P.levels > 32 || P.xcb > 10 || P.ycb > 10 || P.xcb + P.ycb > 12) { err = "bad COD"; return TC_E_CODESTREAM; }
+            if (P.xcb > 6 || P.ycb > 6) { err = "code-blocks larger than 64x64"; return TC_E_UNSUPPORTED; }
+            if (P.cblk_style != 0) { err = "code-block style flags are not supported"; return TC_E_UNSUPPORTED; }
+            if (P.prog > 4 || P.layers < 1) { err = "bad progression or layer count"; return TC_E_CODESTREAM; }
+            if (P.reversible > 1) { err = "unknown wavelet"; return TC_E_CODESTREAM; }
+            P.ppx.assign(P.levels + 1, 15);
+            P.ppy.assign(P.levels + 1, 15);
+            if (P.scod & 1)
+                for (int r = 0; r <= P.levels; r++) {
+                    const uint32_t v = rd.u8();
+                    P.ppx[r] = (int)(v & 0xF);
+                    P.ppy[r] = (int)(v >> 4);
+                }
+            P.have_cod = true;
+            break;
+        }
+        case M_QCD: {
+            const uint32_t s = rd.u8();
+            P.qstyle = (int)(s & 0x1F);
+            P.guard = (int)(s >> 5);
+            P.q_eps.clear();
+            P.q_mu.clear();
+            if (P.qstyle == 0) {
+                while (rd.pos < seg_end) P.q_eps.push_back((int)(rd.u8() >> 3)), P.q_mu.push_back(0);
+            } else if (P.qstyle == 1 || P.qstyle == 2) {
+                while (rd.pos + 1 < seg_end) {
+                    const uint32_t v = rd.u16();
+                    P.q_eps.push_back((int)(v >> 11));
+                    P.q_mu.push_back((int)(v & 0x7FF));
+                }
+            } else {
+                err = "bad quantisation style";
+                return TC_E_CODESTREAM;
+            }
+            P.have_qcd = true;
+            break;
+        }
+        case M_COC: case M_QCC: case M_RGN: case M_POC: case M_PPM: case M_CRG:
+            err = "COC/QCC/RGN/POC/PPM/CRG markers are not supported";
+            return TC_E_UNSUPPORTED;
+        default:
+            break;  // COM, TLM, PLM and others carry nothing we need
+        }
+        rd.pos = seg_end;
+    }
+    if (!P.have_siz || !P.have_cod || !P.have_qcd) { err = "main header lacks SIZ, COD or QCD"; return TC_E_CODESTREAM; }
+    if (P.tw < P.width || P.th < P.height) { err = "multiple tiles are not supported"; return TC_E_UNSUPPORTED; }
+    return TC_OK;
+}
+
+static void fill_info(const Params &P, tc_image_info &info)
+{
+    std::memset(&info, 0, sizeof info);
+    info.width = P.width;
+    info.height = P.height;
+    info.ncomp = P.ncomp;
+    info.bits = P.bits;
+    info.is_signed = P.is_signed;
+    info.levels = P.levels;
+    info.reversible = P.reversible;
+    info.mct = P.mct;
+    info.cblk_w = 1 << P.xcb;
+    info.cblk_h = 1 << P.ycb;
+    info.layers = P.layers;
+    info.progression = P.prog;
+    info.guard_bits = P.guard;
+    info.quant_style = P.qstyle;
+}
+
+int read_header(const uint8_t *cs, size_t len, tc_image_info &info, std::string &err)
+{
+    Reader rd{cs, len};
+    Params P;
+    const int rc = parse_main(rd, P, err);
+    if (rc) return rc;
+    fill_info(P, info);
+    return TC_OK;
+}
+
+// Quantisation parameters per band (ISO A.6.4-A.6.5, E.1).  Derived style
+// restates read_qcd_marker (codestream.c:142-230) with ISO's exponent rule.
+static int assign_quant(const Params &P, std::vector<Resolution> &res, std::string &err)
+{
+    int bi = 0;
+    for (int r = 0; r <= P.levels; r++)
+        for (Band &b : res[r].bands) {
+            int eps, mu;
+            if (P.qstyle == 1) {
+                if (P.q_eps.empty()) { err = "empty QCD"; return TC_E_CODESTREAM; }
+                eps = P.q_eps[0] - P.levels + b.level;
+                mu = P.q_mu[0];
+                if (eps < 0) eps = 0;
+            } else {
+                if (bi >= (int)P.q_eps.size()) { err = "QCD has too few subbands"; return TC_E_CODESTREAM; }
+                eps = P.q_eps[bi];
+                mu = P.q_mu[bi];
+            }
+            bi++;
+            b.eps = eps;
+            b.mu = mu;
+            b.mb = P.guard + eps - 1;
+            if (b.mb > 31) { err = "more than 31 magnitude bit-planes"; return TC_E_UNSUPPORTED; }
+            const int rb = P.bits + band_gain_log2(b.orient);
+            b.step = (float)std::ldexp(1.0 + mu / 2048.0, rb - eps);
+        }
+    return TC_OK;
+}
+
+namespace {
+struct CblkState {
+    int included = 0;
+    int lblock = 3;
+    int zbp = 0;
+    int passes = 0;
+    std::vector<std::pair<size_t, uint32_t>> segs;  // (offset in cs, length)
+};
+}  // namespace
+
+int parse_codestream(const uint8_t *cs, size_t len, Parsed &out, std::string &err)
+{
+    Reader rd{cs, len};
+    Params P;
+    int rc = parse_main(rd, P, err);
+    if (rc) return rc;
+    fill_info(P, out.info);
+
+    // Geometry per resolution (identical for every component).
+    std::vector<Resolution> geo = make_geometry(P.width, P.height, P.levels, P.xcb, P.ycb);
+    for (int r = 0; r <= P.levels; r++) {
+        // Code-block size is capped by the precinct size (ISO B.7); one
+        // precinct per resolution is required.
+        const int px = P.ppx[r], py = P.ppy[r];
+        const int xcb = std::min(P.xcb, r ? px - 1 : px), ycb = std::min(P.ycb, r ? py - 1 : py);
+        if (geo[r].w > (1 << px) || geo[r].h > (1 << py)) { err = "more than one precinct per resolution"; return TC_E_UNSUPPORTED; }
+        if (xcb < 0 || ycb < 0) { err = "bad precinct size"; return TC_E_CODESTREAM; }
+        for (Band &b : geo[r].bands) {
+            b.cbw_log2 = xcb;
+            b.cbh_log2 = ycb;
+            b.ncbx = b.w > 0 ? ceil_div(b.w, 1 << xcb) : 0;
+            b.ncby = b.h > 0 ? ceil_div(b.h, 1 << ycb) : 0;
+        }
+    }
+    if ((rc = assign_quant(P, geo, err))) return rc;
+
+    // Per component, per resolution, per band: code-block states and trees.
+    struct BandState {
+        std::vector<CblkState> cb;
+        TagTree incl, zbp;
+        BandState(int w, int h) : cb((size_t)w * h), incl(std::max(w, 1), std::max(h, 1)),
+                                  zbp(std::max(w, 1), std::max(h, 1)) {}
+    };
+    std::vector<std::vector<std::vector<BandState>>> st(P.ncomp);
+    for (int c = 0; c < P.ncomp; c++) {
+        st[c].resize(P.levels + 1);
+        for (int r = 0; r <= P.levels; r++)
+            for (const Band &b : geo[r].bands) {
+                st[c][r].emplace_back(b.ncbx, b.ncby);
+                st[c][r].back().incl.reset_decoder();
+                st[c][r].back().zbp.reset_decoder();
+            }
+    }
+
+    // Tile-parts of the single tile: collect the packet data ranges.
+    std::vector<std::pair<size_t, size_t>> parts;
+    for (;;) {
+        const uint32_t m = rd.u16();
+        if (rd.bad) { err = "truncated codestream"; return TC_E_CODESTREAM; }
+        if (m == M_EOC) break;
+        if (m != M_SOT) { err = "expected SOT"; return TC_E_CODESTREAM; }
+        const size_t sot_pos = rd.pos - 2;
+        const uint32_t lsot = rd.u16(), isot = rd.u16(), psot = rd.u32();
+        rd.u8();  // TPsot
+        rd.u8();  // TNsot
+        if (lsot != 10 || isot != 0) { err = "bad SOT or tile index"; return TC_E_CODESTREAM; }
+        const size_t end = psot ? sot_pos + psot : len;
+        if (end > len) { err = "tile-part runs past the codestream"; return TC_E_CODESTREAM; }
+        for (;;) {
+            const uint32_t mm = rd.u16();
+            if (rd.bad) { err = "truncated tile-part header"; return TC_E_CODESTREAM; }
+            if (mm == M_SOD) break;
+            const uint32_t L = rd.u16();
+            if (mm == M_COD || mm == M_COC || mm == M_QCD || mm == M_QCC || mm == M_RGN ||
+                mm == M_POC || mm == M_PPT) {
+                err = "tile-part header coding parameters are not supported";
+                return TC_E_UNSUPPORTED;
+            }
+            if (L < 2 || rd.pos - 2 + L > end) { err = "bad tile-part marker"; return TC_E_CODESTREAM; }
+            rd.pos += L - 2;
+        }
+        parts.emplace_back(rd.pos, end);
+        rd.pos = end;
+        if (rd.pos >= len) break;
+    }
+    // Concatenate tile-part bodies logically: packets may not straddle
+    // tile-parts in practice, and we read them part by part.
+    size_t part_i = 0;
+    size_t pos = parts.empty() ? len : parts[0].first;
+    auto part_end = [&]() { return part_i < parts.size() ? parts[part_i].second : len; };
+
+    auto read_packet = [&](int layer, int r, int c) -> int {
+        while (part_i < parts.size() && pos >= parts[part_i].second) {
+            part_i++;
+            if (part_i < parts.size()) pos = parts[part_i].first;
+        }
+        if (part_i >= parts.size()) { err = "packet data missing"; return TC_E_CODESTREAM; }
+        const size_t pend = part_end();
+        if (P.scod & 2) {  // SOP
+            if (pos + 6 <= pend && cs[pos] == 0xFF && cs[pos + 1] == 0x91) pos += 6;
+        }
+        BitReader br(cs, pos, pend);
+        const int present = br.get();
+        std::vector<std::pair<CblkState *, uint32_t>> contrib;
+        if (present) {
+            for (size_t bi = 0; bi < geo[r].bands.size(); bi++) {
+                const Band &b = geo[r].bands[bi];
+                BandState &bs = st[c][r][bi];
+                for (int i = 0; i < b.ncbx * b.ncby; i++) {
+                    CblkState &cb = bs.cb[i];
+                    int inc;
+                    if (!cb.included) inc = bs.incl.decode(br, i, layer + 1);
+                    else inc = br.get();
+                    if (br.overrun) { err = "packet header overrun"; return TC_E_CODESTREAM; }
+                    if (!inc) continue;
+                    if (!cb.included) {
+                        int k = 0;
+                        while (!bs.zbp.decode(br, i, k + 1)) {
+                            if (br.overrun || ++k > 64) { err = "bad zero bit-plane tag tree"; return TC_E_CODESTREAM; }
+                        }
+                        cb.zbp = k;
+                        cb.included = 1;
+                    }
+                    const int np = get_num_passes(br);
+                    int inc_l = 0;
+                    while (br.get()) {
+                        if (br.overrun || ++inc_l > 32) { err = "bad Lblock increment"; return TC_E_CODESTREAM; }
+                    }
+                    cb.lblock += inc_l;
+                    const int nbits = cb.lblock + floorlog2(np);
+                    if (nbits > 31) { err = "code-block length field too wide"; return TC_E_CODESTREAM; }
+                    const uint32_t L = br.get_bits(nbits);
+                    if (br.overrun) { err = "packet header overrun"; return TC_E_CODESTREAM; }
+                    cb.passes += np;
+                    contrib.emplace_back(&cb, L);
+                }
+            }
+        }
+        br.align();
+        if (br.overrun) { err = "packet header overrun"; return TC_E_CODESTREAM; }
+        pos = br.pos;
+        if (P.scod & 4) {  // EPH
+            if (pos + 2 > pend || cs[pos] != 0xFF || cs[pos + 1] != 0x92) { err = "missing EPH"; return TC_E_CODESTREAM; }
+            pos += 2;
+        }
+        for (auto &cl : contrib) {
+            if (pos + cl.second > pend) { err = "code-block data runs past the tile-part"; return TC_E_CODESTREAM; }
+            if (cl.second) cl.first->segs.emplace_back(pos, cl.second);
+            pos += cl.second;
+        }
+        return TC_OK;
+    };
+
+    const int L = P.layers, R = P.levels + 1, C = P.ncomp;
+    auto run = [&](int a, int b2, int c2) { return read_packet(a, b2, c2); };
+    switch (P.prog) {
+    case 0:  // LRCP
+        for (int l = 0; l < L; l++) for (int r = 0; r < R; r++) for (int c = 0; c < C; c++)
+            if ((rc = run(l, r, c))) return rc;
+        break;
+    case 1:  // RLCP
+        for (int r = 0; r < R; r++) for (int l = 0; l < L; l++) for (int c = 0; c < C; c++)
+            if ((rc = run(l, r, c))) return rc;
+        break;
+    case 2:  // RPCL (one precinct per resolution)
+        for (int r = 0; r < R; r++) for (int c = 0; c < C; c++) for (int l = 0; l < L; l++)
+            if ((rc = run(l, r, c))) return rc;
+        break;
+    default:  // PCRL, CPRL (one precinct per resolution, all at the origin)
+        for (int c = 0; c < C; c++) for (int r = 0; r < R; r++) for (int l = 0; l < L; l++)
+            if ((rc = run(l, r, c))) return rc;
+        break;
+    }
+
+    // Emit descriptors.
+    out.desc.clear();
+    out.own_pool.clear();
+    bool multi = false;
+    for (int c = 0; c < C; c++)
+        for (int r = 0; r < R; r++)
+            for (auto &bs : st[c][r])
+                for (auto &cb : bs.cb)
+                    if (cb.segs.size() > 1) multi = true;
+    out.pool_is_cs = !multi;
+    const uint64_t plane = (uint64_t)P.width * P.height;
+    for (int c = 0; c < C; c++)
+        for (int r = 0; r < R; r++)
+            for (size_t bi = 0; bi < geo[r].bands.size(); bi++) {
+                const Band &b = geo[r].bands[bi];
+                BandState &bs = st[c][r][bi];
+                for (int j = 0; j < b.ncby; j++)
+                    for (int i = 0; i < b.ncbx; i++) {
+                        CblkState &cb = bs.cb[j * b.ncbx + i];
+                        tc_cblk_desc d;
+                        std::memset(&d, 0, sizeof d);
+                        const int cx = i << b.cbw_log2, cy = j << b.cbh_log2;
+                        d.w = (uint16_t)std::min(1 << b.cbw_log2, b.w - cx);
+                        d.h = (uint16_t)std::min(1 << b.cbh_log2, b.h - cy);
+                        d.mb = (uint8_t)b.mb;
+                        d.orient = (uint8_t)b.orient;
+                        d.out_pitch = (uint32_t)P.width;
+                        d.out_off = (uint64_t)c * plane + (uint64_t)(b.y0 + cy) * P.width + (uint64_t)(b.x0 + cx);
+                        d.step = P.reversible ? 1.0f : b.step;
+                        d.flags = P.reversible ? 0 : TC_CBLK_IRREVERSIBLE;
+                        if (cb.included && cb.passes > 0) {
+                            if (cb.zbp > b.mb) { err = "zero bit-planes exceed Mb"; return TC_E_CODESTREAM; }
+                            const int numbps = b.mb - cb.zbp;
+                            if (numbps == 0 || cb.passes > 3 * numbps - 2 || cb.passes > 255) {
+                                err = "coding pass count exceeds the bit-planes";
+                                return TC_E_CODESTREAM;
+                            }
+                            d.zero_bitplanes = (uint8_t)cb.zbp;
+                            d.passes = (uint8_t)cb.passes;
+                            uint64_t total = 0;
+                            for (auto &s : cb.segs) total += s.second;
+                            if (multi) {
+                                d.seg_off = out.own_pool.size();
+                                for (auto &s : cb.segs)
+                                    out.own_pool.insert(out.own_pool.end(), cs + s.first, cs + s.first + s.second);
+                            } else {
+                                d.seg_off = cb.segs.empty() ? 0 : cb.segs[0].first;
+                            }
+                            d.seg_len = (uint32_t)total;
+                        } else {
+                            d.zero_bitplanes = (uint8_t)b.mb;
+                            d.passes = 0;
+                        }
+                        out.desc.push_back(d);
+                    }
+            }
+    out.info.ncblk = (uint32_t)out.desc.size();
+    return TC_OK;
+}
+
+// ============================ encoder =======================================
+
+int encode_codestream(const tc_encode_params &p, const void *planes, std::vector<uint8_t> &out,
+                      std::string &err)
+{
+    const int W = p.width, H = p.height, C = p.ncomp, B = p.bits, NL = p.levels;
+    if (W < 1 || H < 1 || W > 65535 || H > 65535 || C < 1 || C > 4 || B < 1 || B > 16 || NL < 0 ||
+        NL > 15 || p.cblk_log2 < 2 || p.cblk_log2 > 6) {
+        err = "encode parameters out of range";
+        return TC_E_ARG;
+    }
+    if (!p.reversible && !(p.base_step > 0.0)) { err = "base_step must be positive"; return TC_E_ARG; }
+    const bool mct = p.mct && C >= 3;
+    const int threads = p.threads;
+    const size_t np = (size_t)W * H;
+    const bool wide = B > 8;
+
+    std::vector<int32_t> ip;
+    std::vector<double> dp;
+    auto sample = [&](int c, size_t i) -> int32_t {
+        return wide ? ((const uint16_t *)planes)[c * np + i] : ((const uint8_t *)planes)[c * np + i];
+    };
+    const int32_t dc = 1 << (B - 1);
+    if (p.reversible) {
+        ip.resize(np * C);
+        for (int c = 0; c < C; c++)
+            for (size_t i = 0; i < np; i++) ip[c * np + i] = sample(c, i) - dc;
+        if (mct)
+            for (size_t i = 0; i < np; i++) {
+                const int32_t r = ip[i], g = ip[np + i], b = ip[2 * np + i];
+                ip[i] = (r + 2 * g + b) >> 2;
+                ip[np + i] = b - g;
+                ip[2 * np + i] = r - g;
+            }
+        for (int c = 0; c < C; c++)
+            fwd_plane_pitch(ip.data() + c * np, W, H, (size_t)W, NL, fwd53_line, threads);
+    } else {
+        dp.resize(np * C);
+        for (int c = 0; c < C; c++)
+            for (size_t i = 0; i < np; i++) dp[c * np + i] = (double)(sample(c, i) - dc);
+        if (mct)
+            for (size_t i = 0; i < np; i++) {
+                const double R = dp[i], G = dp[np + i], Bl = dp[2 * np + i];
+                dp[i] = 0.299 * R + 0.587 * G + 0.114 * Bl;
+                dp[np + i] = -0.16875 * R - 0.33126 * G + 0.5 * Bl;
+                dp[2 * np + i] = 0.5 * R - 0.41869 * G - 0.08131 * Bl;
+            }
+        for (int c = 0; c < C; c++)
+            fwd_plane_pitch(dp.data() + c * np, W, H, (size_t)W, NL, fwd97_line, threads);
+    }
+
+    std::vector<Resolution> geo = make_geometry(W, H, NL, p.cblk_log2, p.cblk_log2);
+    // Quantisation: exponent/mantissa per band, quantised coefficients.
+    std::vector<int32_t> q(np * C);
+    int need_guard = 1;
+    for (int r = 0; r <= NL; r++)
+        for (Band &b : geo[r].bands) {
+            const int rb = B + band_gain_log2(b.orient);
+            if (p.reversible) {
+                b.eps = rb;
+                b.mu = 0;
+                b.step = 1.0f;
+            } else {
+                const double delta = p.base_step * std::ldexp(1.0, B) / subband_norm(true, b.level, b.orient);
+                int e = rb - (int)std::floor(std::log2(delta));
+                int m = (int)std::lround((delta / std::ldexp(1.0, rb - e) - 1.0) * 2048.0);
+                if (m >= 2048) { m = 0; e--; }
+                if (m < 0) m = 0;
+                if (e < 0 || e > 31) { err = "quantisation step out of range"; return TC_E_ARG; }
+                b.eps = e;
+                b.mu = m;
+                b.step = (float)std::ldexp(1.0 + m / 2048.0, rb - e);
+            }
+            uint32_t mx = 0;
+            for (int c = 0; c < C; c++)
+                for (int y = b.y0; y < b.y0 + b.h; y++)
+                    for (int x = b.x0; x < b.x0 + b.w; x++) {
+                        const size_t i = c * np + (size_t)y * W + x;
+                        int32_t v;
+                        if (p.reversible) {
+                            v = ip[i];
+                        } else {
+                            const double a = std::fabs(dp[i]) / (double)b.step;
+                            v = (int32_t)std::floor(a);
+                            if (dp[i] < 0) v = -v;
+                        }
+                        q[i] = v;
+                        mx = std::max(mx, (uint32_t)std::abs((int64_t)v));
+                    }
+            int nb = 0;
+            while (nb < 32 && (mx >> nb)) nb++;
+            need_guard = std::max(need_guard, nb - b.eps + 1);
+        }
+    int G = p.guard_bits > 0 ? p.guard_bits : std::max(2, need_guard);
+    if (G < need_guard || G > 7) { err = "guard bits cannot hold the coefficient range"; return TC_E_ARG; }
+    for (int r = 0; r <= NL; r++)
+        for (Band &b : geo[r].bands) {
+            b.mb = G + b.eps - 1;
+            if (b.mb > 31) { err = "more than 31 magnitude bit-planes"; return TC_E_ARG; }
+        }
+
+    // Tier-1: encode every code-block.
+    struct Job {
+        int c, r, bi, i, j;
+    };
+    std::vector<Job> jobs;
+    for (int c = 0; c < C; c++)
+        for (int r = 0; r <= NL; r++)
+            for (int bi = 0; bi < (int)geo[r].bands.size(); bi++) {
+                const Band &b = geo[r].bands[bi];
+                for (int j = 0; j < b.ncby; j++)
+                    for (int i = 0; i < b.ncbx; i++) jobs.push_back({c, r, bi, i, j});
+            }
+    struct Coded {
+        std::vector<uint8_t> data;
+        int passes = 0, zbp = 0;
+    };
+    std::vector<Coded> coded(jobs.size());
+    std::atomic<int> fail{0};
+    parallel_for((int)jobs.size(), threads, [&](int k) {
+        const Job &jb = jobs[k];
+        const Band &b = geo[jb.r].bands[jb.bi];
+        const int cx = jb.i << b.cbw_log2, cy = jb.j << b.cbh_log2;
+        const int bw = std::min(1 << b.cbw_log2, b.w - cx), bh = std::min(1 << b.cbh_log2, b.h - cy);
+        int32_t blk[64 * 64];
+        for (int y = 0; y < bh; y++)
+            for (int x = 0; x < bw; x++)
+                blk[y * bw + x] = q[jb.c * np + (size_t)(b.y0 + cy + y) * W + b.x0 + cx + x];
+        if (t1_encode_block(blk, bw, bh, b.orient, b.mb, 0, coded[k].data, &coded[k].passes, &coded[k].zbp))
+            fail = 1;
+    });
+    if (fail) { err = "Tier-1 encoding failed"; return TC_E_ARG; }
+
+    // Index jobs by (c, r, bi) for the packet writer.
+    std::vector<std::vector<std::vector<int>>> first(C, std::vector<std::vector<int>>(NL + 1));
+    for (size_t k = 0; k < jobs.size(); k++) {
+        auto &v = first[jobs[k].c][jobs[k].r];
+        if ((int)v.size() <= jobs[k].bi) v.resize(jobs[k].bi + 1, -1);
+        if (v[jobs[k].bi] < 0) v[jobs[k].bi] = (int)k;
+    }
+
+    std::vector<uint8_t> body;
+    body.reserve(np * C / 2);
+    auto write_packet = [&](int r, int c) {
+        std::vector<uint8_t> hdr;
+        BitWriter bw(hdr);
+        bool any = false;
+        for (int bi = 0; bi < (int)geo[r].bands.size(); bi++) {
+            const Band &b = geo[r].bands[bi];
+            if (b.ncbx * b.ncby == 0) continue;
+            const int k0 = first[c][r][bi];
+            for (int i = 0; i < b.ncbx * b.ncby; i++) any |= coded[k0 + i].passes > 0;
+        }
+        if (!any) {
+            bw.put(0);
+            bw.flush();
+            body.insert(body.end(), hdr.begin(), hdr.end());
+            return;
+        }
+        bw.put(1);
+        std::vector<int> order;
+        for (int bi = 0; bi < (int)geo[r].bands.size(); bi++) {
+            const Band &b = geo[r].bands[bi];
+            const int n = b.ncbx * b.ncby;
+            if (n == 0) continue;
+            const int k0 = first[c][r][bi];
+            TagTree incl(b.ncbx, b.ncby), zt(b.ncbx, b.ncby);
+            std::vector<int> iv(n), zv(n);
+            for (int i = 0; i < n; i++) {
+                iv[i] = coded[k0 + i].passes > 0 ? 0 : 1;
+                zv[i] = coded[k0 + i].zbp;
+            }
+            incl.set_leaves(iv);
+            zt.set_leaves(zv);
+            for (int i = 0; i < n; i++) {
+                const Coded &cd = coded[k0 + i];
+                incl.encode(bw, i, 1);
+                if (cd.passes == 0) continue;
+                zt.encode(bw, i, cd.zbp + 1);
+                put_num_passes(bw, cd.passes);
+                const int len = (int)cd.data.size();
+                int lblock = 3, incr = 0;
+                while (len >= (1 << (lblock + incr + floorlog2(cd.passes)))) incr++;
+                for (int t = 0; t < incr; t++) bw.put(1);
+                bw.put(0);
+                lblock += incr;
+                bw.put_bits((uint32_t)len, lblock + floorlog2(cd.passes));
+                order.push_back(k0 + i);
+            }
+        }
+        bw.flush();
+        body.insert(body.end(), hdr.begin(), hdr.end());
+        for (int k : order) body.insert(body.end(), coded[k].data.begin(), coded[k].data.end());
+    };
+    if (p.progression == 1) {
+        for (int r = 0; r <= NL; r++)
+            for (int c = 0; c < C; c++) write_packet(r, c);
+    } else {
+        for (int r = 0; r <= NL; r++)
+            for (int c = 0; c < C; c++) write_packet(r, c);
+    }
+
+    out.clear();
+    Writer wr{out};
+    wr.u16(M_SOC);
+    wr.u16(M_SIZ);
+    wr.u16(38 + 3 * C);
+    wr.u16(0);
+    wr.u32(W); wr.u32(H); wr.u32(0); wr.u32(0);
+    wr.u32(W); wr.u32(H); wr.u32(0); wr.u32(0);
+    wr.u16(C);
+    for (int c = 0; c < C; c++) { wr.u8(B - 1); wr.u8(1); wr.u8(1); }
+    wr.u16(M_COD);
+    wr.u16(12);
+    wr.u8(0);                              // Scod: default precincts, no SOP/EPH
+    wr.u8(p.progression == 1 ? 1 : 0);     // progression (one layer: LRCP == RLCP order)
+    wr.u16(1);                             // layers
+    wr.u8(mct ? 1 : 0);
+    wr.u8(NL);
+    wr.u8(p.cblk_log2 - 2);
+    wr.u8(p.cblk_log2 - 2);
+    wr.u8(0);                              // code-block style
+    wr.u8(p.reversible ? 1 : 0);
+    const int nbands = 3 * NL + 1;
+    wr.u16(M_QCD);
+    if (p.reversible) {
+        wr.u16(3 + nbands);
+        wr.u8((G << 5) | 0);
+    } else {
+        wr.u16(3 + 2 * nbands);
+        wr.u8((G << 5) | 2);
+    }
+    for (int r = 0; r <= NL; r++)
+        for (const Band &b : geo[r].bands) {
+            if (p.reversible) wr.u8(b.eps << 3);
+            else wr.u16((b.eps << 11) | b.mu);
+        }
+    wr.u16(M_SOT);
+    wr.u16(10);
+    wr.u16(0);
+    wr.u32((uint32_t)(12 + 2 + body.size()));
+    wr.u8(0);
+    wr.u8(1);
+    wr.u16(M_SOD);
+    out.insert(out.end(), body.begin(), body.end());
+    wr.u16(M_EOC);
+    return TC_OK;
+}
+
+}  // namespace tc

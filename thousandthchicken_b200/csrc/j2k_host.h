@@ -1,0 +1,63 @@
+// j2k_host.h -- host-side codestream geometry, parser and harness encoder
+// shared by the C ABI implementation.  Host code only (no CUDA types).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "tc_j2k.h"
+
+namespace tc {
+
+// One subband of a tile-component, positioned in the component's Mallat
+// plane.  Geometry follows ISO B.5 for a tile anchored at the origin; the
+// reference builds the same tree in init_resolution_lvls / init_subbands /
+// init_codeblocks (codestream_image.c:96-230).
+struct Band {
+    int orient = 0;       // 0 LL, 1 HL, 2 LH, 3 HH
+    int level = 0;        // decomposition level n_b (LL_N: N)
+    int x0 = 0, y0 = 0;   // position in the Mallat plane
+    int w = 0, h = 0;
+    int cbw_log2 = 6, cbh_log2 = 6;
+    int ncbx = 0, ncby = 0;
+    int eps = 0, mu = 0;  // quantisation exponent / mantissa
+    int mb = 0;           // magnitude bit-planes
+    float step = 1.0f;    // irreversible step
+};
+
+struct Resolution {
+    int w = 0, h = 0;
+    std::vector<Band> bands;  // r = 0: LL; r > 0: HL, LH, HH
+};
+
+// Level sizes ws[d], hs[d] of the LL band after d decompositions.
+void level_sizes(int w, int h, int levels, std::vector<int> &ws, std::vector<int> &hs);
+std::vector<Resolution> make_geometry(int w, int h, int levels, int xcb, int ycb);
+
+// log2 of the subband gain (ISO E.1: LL 0, HL/LH 1, HH 2).
+inline int band_gain_log2(int orient) { return orient == 0 ? 0 : (orient == 3 ? 2 : 1); }
+
+// Synthesis basis L2 norm of a subband (9/7 when wavelet97, else 5/3).
+double subband_norm(bool wavelet97, int level, int orient);
+
+// ---- MQ encoder / Tier-1 encoder (harness) ---------------------------------
+int t1_encode_block(const int32_t *coef, int w, int h, int orient, int mb, int passes,
+                    std::vector<uint8_t> &out, int *passes_out, int *zero_bitplanes);
+
+// ---- parser -----------------------------------------------------------------
+struct Parsed {
+    tc_image_info info{};
+    std::vector<tc_cblk_desc> desc;
+    std::vector<uint8_t> own_pool;  // used when blocks have several segments
+    bool pool_is_cs = true;
+};
+int parse_codestream(const uint8_t *cs, size_t len, Parsed &out, std::string &err);
+int read_header(const uint8_t *cs, size_t len, tc_image_info &info, std::string &err);
+
+// ---- encoder ------------------------------------------------------------------
+int encode_codestream(const tc_encode_params &p, const void *planes, std::vector<uint8_t> &out,
+                      std::string &err);
+
+}  // namespace tc

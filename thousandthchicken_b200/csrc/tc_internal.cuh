@@ -1,0 +1,89 @@
+// tc_internal.cuh -- shared declarations of the CUDA side of libtc_j2k.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "tc_j2k.h"
+
+// Device error word bits (set by kernels, read by tc_ctx_synchronize).
+#define TC_DERR_DESC 0x1u     // a code-block descriptor was out of range
+#define TC_DERR_POOL 0x2u     // a codeword ran past the segment pool
+
+namespace tc {
+
+// Grow-only device buffer owned by a context.
+struct DevBuf {
+    void *ptr = nullptr;
+    size_t size = 0;
+    cudaError_t ensure(size_t bytes);
+    void release();
+};
+
+}  // namespace tc
+
+struct tc_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    uint32_t *d_words = nullptr;  // [0] error word, [1] T1 work counter
+    tc::DevBuf scratch;           // DWT intermediate levels
+    tc::DevBuf tmp_pool, tmp_desc, tmp_order, tmp_coef, tmp_out;
+    uint64_t launches = 0;
+};
+
+namespace tc {
+
+// Records a message on the context and returns the status.
+int fail(tc_ctx *ctx, int status, const std::string &msg);
+// Maps a CUDA error to TC_E_DEVICE with its message (TC_OK on cudaSuccess).
+int cuda_status(tc_ctx *ctx, cudaError_t e, const char *what);
+
+// ---- kernels' host launchers (each returns a cudaError_t of the launch) ----
+
+cudaError_t launch_t1_decode(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint32_t *d_order,
+                             int n, const uint8_t *d_pool, uint64_t pool_len, void *d_out,
+                             int out_mode, float recon_r);
+cudaError_t launch_dequant_raw(tc_ctx *ctx, const tc_cblk_desc *d_desc, int n,
+                               const uint32_t *d_raw, void *d_out, float recon_r);
+
+// One 2-D DWT level over up to 4 components of equal size.
+struct LevelIO {
+    const void *ll[4];     // reverse: LL input; forward: spatial input
+    const void *coef[4];   // reverse: Mallat plane holding HL/LH/HH of the level
+    void *out[4];          // reverse: samples of the level; forward: LL output
+    void *bands[4];        // forward: Mallat plane receiving HL/LH/HH
+    int ll_pitch, coef_pitch, out_pitch, bands_pitch;
+    int w, h;              // size of the level's full-resolution region
+    int ncomp;
+};
+
+// wavelet: 0 = 5/3 int32, 1 = 9/7 float.  rounding: TC_ROUND_*.
+cudaError_t launch_idwt_level(tc_ctx *ctx, const LevelIO &io, int wavelet, int rounding);
+cudaError_t launch_fdwt_level(tc_ctx *ctx, const LevelIO &io, int wavelet, int rounding);
+
+// Last reverse level fused with the inverse colour transform, DC shift,
+// rounding and clamping; writes out_type samples (TC_U8/TC_U16/TC_INT32).
+// color: TC_COLOR_DC / TC_COLOR_RCT / TC_COLOR_ICT.  levels == 0 means the
+// input is already spatial (no lifting).
+cudaError_t launch_idwt_last_color(tc_ctx *ctx, const LevelIO &io, int wavelet, int color,
+                                   int out_type, int bits, bool lift);
+
+// Standalone colour kernels.
+cudaError_t launch_color_inverse(tc_ctx *ctx, int kind, int ncomp, void *const *in, int in_type,
+                                 int in_pitch, void *const *out, int out_type, int out_pitch,
+                                 int w, int h, int bits);
+cudaError_t launch_color_forward(tc_ctx *ctx, int kind, int ncomp, const void *const *in,
+                                 int in_type, int in_pitch, void *const *out, int out_type,
+                                 int out_pitch, int w, int h, int bits);
+
+inline int num_sms(int device)
+{
+    int n = 148;
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, device);
+    return n;
+}
+
+}  // namespace tc
