@@ -1,0 +1,353 @@
+#!/usr/bin/env python
+"""Benchmark: Mpixel/s of JPEG 2000 decode on B200.
+
+Workload (one step): decode of one 4096x4096 3-component 8-bit image coded
+with the forward ICT, a 6-level 9/7 DWT, deadzone quantisation with base step
+1/128 scaled by the 9/7 synthesis L2 norms, and 64x64 code-blocks with all
+passes (12,288 code-blocks).  Synthetic seeded input (bilinear gradients plus
+N(0, 8^2) noise), coded by the project's harness encoder at start-up.
+
+  value   device-resident: Tier-1 + fused dequantisation, reverse DWT and fused
+          inverse ICT/DC shift from a codestream already in HBM, timed with CUDA
+          events per step; L2 is flushed (a 256 MiB write) between steps,
+          outside the timed events.
+  e2e     the public C-ABI call tc_decode_j2k (Decoder.decode): host codestream
+          in, host samples out, parse + H2D + kernels + D2H inside the timer.
+
+Multi-GPU: the path does not shard (one image per decode); --gpus N runs N
+independent replicas (no collective), value = total pixels / max-over-ranks time.
+
+--impl reference: the reference's CPU path on the host cores (the oracle port
+of its algorithm), on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Mpixel/s decode, batched vs per-image, 1 B200; p50/p99 latency; DWT % HBM peak"
+WORKLOAD = dict(workload="lossy_decode_4096x4096x3_8bit_ict_97_6lvl_step1/128_cblk64", width=4096, height=4096,
+                ncomp=3, bits=8, levels=6, base_step=1.0 / 128, cblk=64, seed=2)
+SAMPLE = dict(width=1024, height=1024)   # CPU baseline sample (1/16 of the pixels)
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def make_workload(w, h, seed):
+    from thousandthchicken_b200 import codec
+    from thousandthchicken_b200.synth import gradient_noise_image
+    img = gradient_noise_image(w, h, WORKLOAD["ncomp"], WORKLOAD["bits"], seed)
+    cs = codec.encode(img, WORKLOAD["bits"], levels=WORKLOAD["levels"], reversible=False, mct=True,
+                      base_step=WORKLOAD["base_step"])
+    return img, cs
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.file = None
+
+    def start(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.file, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.file.flush()
+        rows = []
+        for line in Path(self.file.name).read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                rows.append(f)
+        os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [num(r[1]) for r in rows if num(r[1])]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": num(rows[0][2]),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dwt_bytes(w, h, c, levels):
+    """Algorithmic HBM bytes of the reverse DWT stage: every level reads its
+    four subbands (4 B each) and writes its output once (4 B; the last level
+    writes 1 B 8-bit samples after the fused colour transform)."""
+    ws, hs = [w], [h]
+    for _ in range(levels):
+        ws.append((ws[-1] + 1) // 2)
+        hs.append((hs[-1] + 1) // 2)
+    b = 0
+    for lvl in range(levels, 0, -1):
+        n = ws[lvl - 1] * hs[lvl - 1] * c
+        b += 4 * n + (1 * n if lvl == 1 else 4 * n)
+    return b
+
+
+def run_reference(args, rank):
+    """The reference's CPU implementation of the path (oracle port) on all
+    host cores, on a bounded sample of the workload."""
+    if rank != 0:
+        return
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    from thousandthchicken_b200 import codec
+    O.build()
+    w, h = SAMPLE["width"], SAMPLE["height"]
+    img, cs = make_workload(w, h, WORKLOAD["seed"])
+    info, desc, pool = codec.parse(cs)
+    cores = os.cpu_count() or 1
+
+    def step():
+        return O.decode_tile(desc, pool, w, h, 3, 8, WORKLOAD["levels"], False, True, r=0.5, threads=cores)
+
+    for _ in range(args.warmup):
+        step()
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        out = step()
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    mpx = w * h * args.steps / total / 1e6
+    psnr = _psnr(out, img)
+    sample = f"{w}x{h}x3 image of the same generator and coding parameters ({w * h / 4096 / 4096:.4f} of the workload)"
+    line = {"impl": "reference", "metric": METRIC, "value": round(mpx, 3), "unit": "Mpixel/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * total / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {**WORKLOAD, "sample": sample},
+            "cpu_baseline": {"value": round(mpx, 3), "unit": "Mpixel/s", "cores": cores, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": round(mpx, 3), "unit": "Mpixel/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "psnr_db": round(psnr, 2)}
+    print(json.dumps(line), flush=True)
+
+
+def _psnr(a, b):
+    d = a.astype(np.float64) - b.astype(np.float64)
+    mse = float(np.mean(d * d))
+    return 99.0 if mse == 0 else 10 * np.log10(255.0 ** 2 / mse)
+
+
+def cpu_baseline(cores):
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    from thousandthchicken_b200 import codec
+    O.build()
+    w, h = SAMPLE["width"], SAMPLE["height"]
+    img, cs = make_workload(w, h, WORKLOAD["seed"])
+    info, desc, pool = codec.parse(cs)
+    O.decode_tile(desc, pool, w, h, 3, 8, WORKLOAD["levels"], False, True, r=0.5, threads=cores)
+    t0 = time.perf_counter()
+    reps = 2
+    for _ in range(reps):
+        O.decode_tile(desc, pool, w, h, 3, 8, WORKLOAD["levels"], False, True, r=0.5, threads=cores)
+    dt = (time.perf_counter() - t0) / reps
+    return {"value": round(w * h / dt / 1e6, 3), "unit": "Mpixel/s", "cores": cores, "kind": "port",
+            "sample": f"{w}x{h}x3 image of the same generator and coding parameters, oracle full decode"}
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from thousandthchicken_b200.stages import Context, Decoder, Plan
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    W, H, Cn = WORKLOAD["width"], WORKLOAD["height"], WORKLOAD["ncomp"]
+    t0 = time.perf_counter()
+    img, cs = make_workload(W, H, WORKLOAD["seed"])
+    log(f"[rank {rank}] encoded workload: {len(cs)} bytes in {time.perf_counter() - t0:.1f}s")
+
+    stream = torch.cuda.Stream(local_rank)
+    ctx = Context(local_rank, stream)
+    plan = Plan(ctx, [cs])
+    outs = plan.alloc_outputs()
+    ncblk = plan.infos[0]["ncblk"]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local_rank}")
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            plan.execute(outs)
+    ctx.synchronize()
+    decoded = outs[0].cpu().numpy()
+    psnr = _psnr(decoded, img)
+
+    # device-resident timed region
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    launches0 = ctx.launches
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    wall0 = time.perf_counter()
+    with torch.cuda.stream(stream):
+        for k in range(args.steps):
+            flush.fill_(k & 0xFF)            # evict L2 between steps (not inside the events)
+            evs[k][0].record(stream)
+            plan.execute(outs)
+            evs[k][1].record(stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - wall0
+    clocks = sampler.stop()
+    launches = ctx.launches - launches0
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    total_ms = sum(step_ms)
+    if dist:
+        t = torch.tensor([total_ms], device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ctx.synchronize()
+
+    # per-stage device times (CUDA events on the plan's stream)
+    plan.set_profiling(True)
+    t1_ms, dwt_ms = [], []
+    with torch.cuda.stream(stream):
+        for k in range(max(3, min(args.steps, 10))):
+            flush.fill_(k & 0xFF)
+            plan.execute(outs)
+            a, b = plan.stage_ms()
+            t1_ms.append(a)
+            dwt_ms.append(b)
+    plan.set_profiling(False)
+
+    # end to end through the public C-ABI call (host in, host out)
+    dec = Decoder(ctx)
+    host_out = np.empty((Cn, H, W), np.uint8)
+    dec.decode(cs, host_out)
+    e2e_times = []
+    e2e_steps = max(1, min(args.steps, 5))
+    if dist:
+        dist.barrier()
+    for _ in range(e2e_steps):
+        t0 = time.perf_counter()
+        dec.decode(cs, host_out)
+        e2e_times.append(time.perf_counter() - t0)
+    e2e_s = sum(e2e_times) / e2e_steps
+    if dist:
+        t = torch.tensor([e2e_s], device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+
+    if rank == 0:
+        px = W * H
+        value = px * args.steps * world / (total_ms / 1000.0) / 1e6
+        hbm, peak_kind = measured_peaks()
+        t1_avg = statistics.mean(t1_ms)
+        dwt_avg = statistics.mean(dwt_ms)
+        pool_bytes = len(cs)
+        t1_bytes = pool_bytes + 4 * px * Cn
+        dw_bytes = dwt_bytes(W, H, Cn, WORKLOAD["levels"])
+        t1_gbs = t1_bytes / (t1_avg / 1000.0) / 1e9
+        dwt_gbs = dw_bytes / (dwt_avg / 1000.0) / 1e9
+        traffic = None
+        tf = ROOT / "profiles" / "ncu_traffic.json"
+        if tf.exists():
+            traffic = json.loads(tf.read_text()).get("t1_decode_kernel_bytes_per_launch")
+        srt = sorted(step_ms)
+        line = {
+            "metric": METRIC, "value": round(value, 2), "unit": "Mpixel/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+            "config": {**WORKLOAD, "code_blocks": ncblk, "codestream_bytes": pool_bytes,
+                       "l2": "256 MiB flush between steps, outside the timed events",
+                       "parallelism": f"replicas x{world} (no collective)"},
+            "latency_ms": {"p50": round(srt[len(srt) // 2], 3), "p99": round(srt[min(len(srt) - 1,
+                                                                                    int(0.99 * len(srt)))], 3)},
+            "stages_ms": {"tier1_dequant": round(t1_avg, 3), "dwt_colour": round(dwt_avg, 3)},
+            "code_blocks_per_s": round(ncblk / (t1_avg / 1000.0), 1),
+            "roofline": {"bound": "hbm", "kernel": "t1_decode_kernel", "achieved": round(t1_gbs, 2),
+                         "peak": hbm, "unit": "GB/s", "frac": round(t1_gbs / hbm, 4), "traffic": traffic,
+                         "peak_kind": peak_kind,
+                         "note": "Tier-1 is issue/latency bound (serial MQ decoding); bytes = codestream + 4 B per "
+                                 "coefficient written"},
+            "dwt_roofline": {"bound": "hbm", "kernels": "idwt_level_kernel + idwt_last_color_kernel",
+                             "achieved": round(dwt_gbs, 2), "peak": hbm, "unit": "GB/s",
+                             "frac": round(dwt_gbs / hbm, 4), "bytes_per_step": dw_bytes, "peak_kind": peak_kind},
+            "e2e": {"value": round(W * H * world / e2e_s / 1e6, 2), "unit": "Mpixel/s",
+                    "h2d_bytes_per_step": pool_bytes + 40 * ncblk + 4 * ncblk,
+                    "d2h_bytes_per_step": int(host_out.nbytes), "api": "tc_decode_j2k"},
+            "gpu_launches": int(launches), "clocks": clocks, "psnr_db": round(psnr, 2),
+            "wall_s_timed_region": round(wall, 3),
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(os.cpu_count() or 1)
+        print(json.dumps(line), flush=True)
+    plan.close()
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

@@ -241,6 +241,13 @@ int tc_plan_image_info(const tc_plan *plan, int image, tc_image_info *info);
 /* Run the decode of every image in the plan; image i goes to d_out[i]
  * (device memory of tc_plan_output_bytes bytes).  Stream-ordered. */
 int tc_plan_execute(tc_plan *plan, void *const *d_out);
+/* Record CUDA events around the stages of every execute (on = 1): the
+ * Tier-1 launch and the DWT/colour launches.  tc_plan_stage_ms waits for the
+ * last execute and returns the device time of each stage in milliseconds.
+ * (The reference times only the enqueue, CoefficientCoder.cpp:239-250,
+ * defect D19.) */
+int tc_plan_set_profiling(tc_plan *plan, int on);
+int tc_plan_stage_ms(tc_plan *plan, float *t1_ms, float *dwt_ms);
 
 /* ---- harness encoder (test and benchmark input generation) --------------- */
 

@@ -384,10 +384,12 @@ int or_t1_decode(const uint8_t *seg, int len, int w, int h, int orient,
             q[y * w + x] = AT(&st, sgn, x, y) ? -mg : mg;
             if (type >= 0) {
                 u = last_plane;
-                /* Truncated after a significance-propagation pass: the
-                 * coefficients significant before that plane have not been
-                 * refined on it yet (ISO E.1.1.2, Nb(u,v)). */
+                /* Truncated inside a bit-plane (ISO E.1.1.2, Nb(u,v)): after
+                 * a significance-propagation pass only the coefficients it
+                 * visited carry that plane; after a refinement pass the
+                 * significant ones do too; the rest wait for the cleanup. */
                 if (type == 1 && !AT(&st, vis, x, y)) u = last_plane + 1;
+                if (type == 2 && !AT(&st, vis, x, y) && !AT(&st, sig, x, y)) u = last_plane + 1;
             }
             if (undecoded) undecoded[y * w + x] = (uint8_t)u;
         }

@@ -1,0 +1,98 @@
+"""Shared builders for the GPU parity tests (no GPU needed to import)."""
+import numpy as np
+
+import oracle as O
+from thousandthchicken_b200 import codec
+from thousandthchicken_b200.synth import laplacian_block
+
+SLOT = 64 * 64
+
+
+def make_blocks(seed, n, mix="uneven", truncate=True, irreversible=False, mb=16):
+    """n encoded code-blocks, each decoded into its own 64x64 slot of the
+    output; returns (desc, pool, list of (coef, seg, passes, numbps))."""
+    rng = np.random.default_rng(seed)
+    desc = np.zeros(n, codec.DESC_DTYPE)
+    segs = []
+    blocks = []
+    off = 0
+    for i in range(n):
+        r = rng.random()
+        if mix == "uneven":
+            if r < 0.6:
+                w = h = 64
+            elif r < 0.9:
+                w = h = 32
+            else:
+                w, h = int(rng.integers(1, 65)), int(rng.integers(1, 65))
+        else:
+            w = h = 64
+        orient = int(rng.integers(0, 4))
+        coef = laplacian_block(rng, w, h, bitplanes=int(rng.integers(4, 15)))
+        seg, total, zbp = codec.t1_encode_block(coef, orient, mb)
+        passes = total
+        if truncate and total > 1:
+            passes = int(rng.integers(1, total + 1))
+            seg, passes, zbp = codec.t1_encode_block(coef, orient, mb, passes)
+        d = desc[i]
+        d["seg_off"] = off
+        d["seg_len"] = len(seg)
+        d["w"], d["h"] = w, h
+        d["passes"] = passes
+        d["mb"] = mb
+        d["zero_bitplanes"] = zbp
+        d["orient"] = orient
+        d["out_off"] = i * SLOT
+        d["out_pitch"] = 64
+        d["step"] = float(rng.uniform(0.01, 4.0)) if irreversible else 1.0
+        d["flags"] = 1 if irreversible else 0
+        segs.append(seg)
+        off += len(seg)
+        blocks.append((coef, seg, passes, mb - zbp))
+    pool = np.frombuffer(b"".join(segs) + b"\0" * 16, np.uint8).copy()
+    return desc, pool, blocks
+
+
+def oracle_slots(desc, pool, mode, r=0.5):
+    """Decode every block with the oracle into the same slot layout."""
+    n = len(desc)
+    if mode == "raw":
+        out = np.zeros((n, 64, 64), np.uint32)
+    elif mode == "int":
+        out = np.zeros((n, 64, 64), np.int32)
+    else:
+        out = np.zeros((n, 64, 64), np.float32)
+    for i, d in enumerate(desc):
+        w, h = int(d["w"]), int(d["h"])
+        seg = pool[int(d["seg_off"]): int(d["seg_off"]) + int(d["seg_len"])].tobytes()
+        numbps = int(d["mb"]) - int(d["zero_bitplanes"])
+        if mode == "raw":
+            out[i, :h, :w] = O.t1_decode_raw(seg, w, h, int(d["orient"]), int(d["mb"]), int(d["zero_bitplanes"]),
+                                             int(d["passes"]))
+            continue
+        q, u = O.t1_decode(seg, w, h, int(d["orient"]), max(numbps, 0), int(d["passes"]) if numbps > 0 else 0)
+        if mode == "int":
+            out[i, :h, :w] = O.dequant_int(q, u, r)
+        else:
+            out[i, :h, :w] = O.dequant_float(q, u, r, float(d["step"]))
+    return out
+
+
+def oracle_mallat(cs, r=0.5):
+    """Oracle Tier-1 + dequantisation of a whole codestream into Mallat
+    planes [ncomp, h, w] (int32 or float32)."""
+    info, desc, pool = codec.parse(cs)
+    W, H, C = info["width"], info["height"], info["ncomp"]
+    rev = info["reversible"]
+    out = np.zeros((C, H, W), np.int32 if rev else np.float32)
+    flat = out.reshape(-1)
+    for d in desc:
+        w, h = int(d["w"]), int(d["h"])
+        seg = pool[int(d["seg_off"]): int(d["seg_off"]) + int(d["seg_len"])].tobytes()
+        numbps = int(d["mb"]) - int(d["zero_bitplanes"])
+        q, u = O.t1_decode(seg, w, h, int(d["orient"]), max(numbps, 0), int(d["passes"]) if numbps > 0 else 0)
+        v = O.dequant_int(q, u, r) if rev else O.dequant_float(q, u, r, float(d["step"]))
+        for y in range(h):
+            o = int(d["out_off"]) + y * int(d["out_pitch"])
+            flat[o: o + w] = v[y]
+    return out, info

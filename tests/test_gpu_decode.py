@@ -1,0 +1,89 @@
+"""Whole-image decode on the GPU (Tier-1 + fused dequantiser, reverse DWT,
+fused inverse colour / DC shift) against OpenJPEG's decode, the oracle and
+the original samples."""
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import golden_cases, load_golden, synth_image
+from thousandthchicken_b200 import codec
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def _decoder(ctx):
+    from thousandthchicken_b200.stages import Decoder
+    return Decoder(ctx)
+
+
+def _oracle(cs, r=0.5):
+    info, desc, pool = codec.parse(cs)
+    return O.decode_tile(desc, pool, info["width"], info["height"], info["ncomp"], info["bits"], info["levels"],
+                         info["reversible"], info["mct"], r=r), info
+
+
+@pytest.mark.parametrize("name,meta", golden_cases(), ids=[n for n, _ in golden_cases()])
+def test_decode_openjpeg_streams(gpu_ctx, name, meta):
+    cs, original, opj = load_golden(name)
+    got = _decoder(gpu_ctx).decode(cs).astype(np.int64)
+    if not meta["irreversible"]:
+        np.testing.assert_array_equal(got, opj.astype(np.int64))
+    else:
+        d = np.abs(got - opj.astype(np.int64))
+        assert d.max() <= 1
+        want, _ = _oracle(cs)
+        d2 = np.abs(got - want.astype(np.int64))
+        assert d2.max() <= 1
+        assert (d2 > 0).mean() < 0.005
+
+
+@pytest.mark.parametrize("w,h,c,bits,levels", [(512, 512, 3, 8, 5), (333, 217, 3, 12, 4), (64, 64, 1, 16, 3),
+                                               (1, 1, 1, 8, 0), (17, 3, 3, 8, 2), (1000, 40, 1, 8, 5)])
+def test_lossless_round_trip(gpu_ctx, w, h, c, bits, levels):
+    img = synth_image(w, h, c, bits, seed=w + h)
+    cs = codec.encode(img, bits, levels=levels, reversible=True, mct=c >= 3)
+    got = _decoder(gpu_ctx).decode(cs)
+    np.testing.assert_array_equal(got, img)
+
+
+@pytest.mark.parametrize("w,h,levels", [(1024, 1024, 6), (515, 300, 5)])
+def test_lossy_decode_vs_oracle(gpu_ctx, w, h, levels):
+    img = synth_image(w, h, 3, 8, seed=7)
+    cs = codec.encode(img, 8, levels=levels, reversible=False, mct=True, base_step=1 / 128)
+    got = _decoder(gpu_ctx).decode(cs).astype(np.int64)
+    want, _ = _oracle(cs)
+    d = np.abs(got - want.astype(np.int64))
+    assert d.max() <= 1, d.max()
+    assert (d > 0).mean() < 0.002
+    mse = np.mean((got - img.astype(np.int64)) ** 2)
+    assert 10 * np.log10(255 ** 2 / mse) > 40
+
+
+def test_batched_plan_equals_single_decodes(gpu_ctx):
+    from thousandthchicken_b200.stages import Plan
+    streams = [codec.encode(synth_image(300, 200, 3, 8, 1), 8, levels=5, reversible=True),
+               codec.encode(synth_image(128, 256, 1, 12, 2), 12, levels=4, reversible=True, mct=False),
+               codec.encode(synth_image(400, 120, 3, 8, 3), 8, levels=5, reversible=False, base_step=1 / 64)]
+    plan = Plan(gpu_ctx, streams)
+    outs = plan.execute(plan.alloc_outputs())
+    gpu_ctx.synchronize()
+    dec = _decoder(gpu_ctx)
+    for s, o in zip(streams, outs):
+        single = dec.decode(s)
+        got = o.cpu().numpy()
+        if single.dtype == np.uint16:
+            got = got.view(np.uint16)
+        np.testing.assert_array_equal(got, single)
+
+
+def test_decode_file_and_errors(gpu_ctx, tmp_path):
+    from thousandthchicken_b200._lib import TCError
+    img = synth_image(80, 60, 3, 8, seed=4)
+    cs = codec.encode(img, 8, levels=3)
+    p = tmp_path / "x.j2k"
+    p.write_bytes(cs)
+    np.testing.assert_array_equal(_decoder(gpu_ctx).decode(p), img)
+    with pytest.raises(TCError):
+        _decoder(gpu_ctx).decode(cs[: len(cs) // 3])
+    np.testing.assert_array_equal(_decoder(gpu_ctx).decode(cs), img)

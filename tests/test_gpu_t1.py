@@ -1,0 +1,99 @@
+"""Tier-1 CUDA kernel (one warp per code-block, persistent queue, fused
+inverse quantiser) against the CPU oracle: bit-exact for every output mode."""
+import numpy as np
+import pytest
+
+from conftest import golden_cases, load_golden
+from gpu_helpers import make_blocks, oracle_mallat, oracle_slots
+from thousandthchicken_b200 import codec
+from thousandthchicken_b200._lib import TC_E_CODESTREAM, TCError
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def _coder(ctx):
+    from thousandthchicken_b200.stages import CoefficientCoder
+    return CoefficientCoder(ctx)
+
+
+@pytest.mark.parametrize("truncate", [False, True])
+def test_t1_raw_output_matches_oracle(gpu_ctx, truncate):
+    desc, pool, _ = make_blocks(seed=11 + truncate, n=300, truncate=truncate)
+    got = _coder(gpu_ctx).decode_blocks(desc, pool, len(desc) * 4096, raw=True).cpu().numpy()
+    want = oracle_slots(desc, pool, "raw").reshape(-1).view(np.int32)
+    np.testing.assert_array_equal(got, want)
+
+
+@pytest.mark.parametrize("r", [0.0, 0.5])
+def test_t1_dequant_int_matches_oracle(gpu_ctx, r):
+    desc, pool, blocks = make_blocks(seed=21, n=300, truncate=True)
+    got = _coder(gpu_ctx).decode_blocks(desc, pool, len(desc) * 4096, recon_r=r).cpu().numpy()
+    want = oracle_slots(desc, pool, "int", r).reshape(-1)
+    np.testing.assert_array_equal(got, want)
+
+
+def test_t1_full_passes_recover_coefficients(gpu_ctx):
+    desc, pool, blocks = make_blocks(seed=31, n=200, truncate=False)
+    got = _coder(gpu_ctx).decode_blocks(desc, pool, len(desc) * 4096, recon_r=0.0).cpu().numpy()
+    got = got.reshape(len(desc), 64, 64)
+    for i, (coef, _, _, _) in enumerate(blocks):
+        h, w = coef.shape
+        np.testing.assert_array_equal(got[i, :h, :w], coef)
+
+
+def test_t1_dequant_float_matches_oracle(gpu_ctx):
+    desc, pool, _ = make_blocks(seed=41, n=300, truncate=True, irreversible=True)
+    got = _coder(gpu_ctx).decode_blocks(desc, pool, len(desc) * 4096, recon_r=0.5,
+                                        dtype=torch.float32).cpu().numpy()
+    want = oracle_slots(desc, pool, "float", 0.5).reshape(-1)
+    np.testing.assert_array_equal(got.view(np.int32), want.view(np.int32))
+
+
+def test_t1_queue_order_does_not_change_results(gpu_ctx):
+    desc, pool, _ = make_blocks(seed=51, n=500, truncate=True)
+    c = _coder(gpu_ctx)
+    a = c.decode_blocks(desc, pool, len(desc) * 4096, sort=True).cpu().numpy()
+    b = c.decode_blocks(desc, pool, len(desc) * 4096, sort=False).cpu().numpy()
+    np.testing.assert_array_equal(a, b)
+
+
+def test_t1_batched_uneven_blocks_large(gpu_ctx):
+    """Uneven batch (60% 64x64, 30% 32x32, 10% ragged edges), truncated at
+    seeded pass counts, in one persistent launch."""
+    desc, pool, blocks = make_blocks(seed=61, n=4000, truncate=True)
+    got = _coder(gpu_ctx).decode_blocks(desc, pool, len(desc) * 4096, recon_r=0.0).cpu().numpy()
+    want = oracle_slots(desc, pool, "int", 0.0).reshape(-1)
+    np.testing.assert_array_equal(got, want)
+
+
+@pytest.mark.parametrize("name,meta", golden_cases(), ids=[n for n, _ in golden_cases()])
+def test_t1_openjpeg_streams(gpu_ctx, name, meta):
+    cs, _, _ = load_golden(name)
+    got, info = _coder(gpu_ctx).decode_tile(cs, recon_r=0.5)
+    want, _ = oracle_mallat(cs, 0.5)
+    np.testing.assert_array_equal(got.cpu().numpy().view(np.int32), want.view(np.int32))
+
+
+def test_t1_bad_descriptor_sets_error_word(gpu_ctx):
+    desc, pool, _ = make_blocks(seed=71, n=8, truncate=False)
+    bad = desc.copy()
+    bad["seg_len"][3] = 1 << 30          # codeword past the pool
+    with pytest.raises(TCError) as e:
+        _coder(gpu_ctx).decode_blocks(bad, pool, len(bad) * 4096, raw=True)
+    assert e.value.status == TC_E_CODESTREAM
+    bad = desc.copy()
+    bad["w"][2] = 0                      # geometry out of range
+    with pytest.raises(TCError):
+        _coder(gpu_ctx).decode_blocks(bad, pool, len(bad) * 4096, raw=True)
+    # the context stays usable
+    got = _coder(gpu_ctx).decode_blocks(desc, pool, len(desc) * 4096, raw=True).cpu().numpy()
+    np.testing.assert_array_equal(got, oracle_slots(desc, pool, "raw").reshape(-1).view(np.int32))
+
+
+def test_t1_empty_and_zero_pass_blocks(gpu_ctx):
+    desc, pool, _ = make_blocks(seed=81, n=16, truncate=False)
+    desc["passes"][::2] = 0
+    got = _coder(gpu_ctx).decode_blocks(desc, pool, len(desc) * 4096, recon_r=0.0).cpu().numpy()
+    want = oracle_slots(desc, pool, "int", 0.0).reshape(-1)
+    np.testing.assert_array_equal(got, want)

@@ -1,0 +1,111 @@
+"""Host-side code (no GPU): the harness encoder, the Tier-2 parser and the
+Tier-1 oracle round trips, and the error behaviour of the parser."""
+import io
+
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import synth_image
+from thousandthchicken_b200 import codec
+from thousandthchicken_b200._lib import TCError, TC_E_CODESTREAM, TC_E_UNSUPPORTED
+from thousandthchicken_b200.synth import laplacian_block
+
+
+@pytest.mark.parametrize("w,h,c,bits,levels", [(64, 64, 1, 8, 2), (97, 53, 3, 8, 3), (512, 512, 3, 8, 5),
+                                               (130, 70, 3, 12, 4), (1, 1, 1, 8, 0), (1, 37, 1, 8, 3),
+                                               (45, 1, 3, 8, 2), (3, 2, 3, 16, 1), (200, 9, 1, 16, 3)])
+def test_lossless_round_trip_through_oracle(w, h, c, bits, levels):
+    img = synth_image(w, h, c, bits, seed=w * 7 + h)
+    cs = codec.encode(img, bits, levels=levels, reversible=True, mct=c >= 3)
+    info, desc, pool = codec.parse(cs)
+    assert info["ncblk"] == len(desc)
+    out = O.decode_tile(desc, pool, w, h, c, bits, levels, True, info["mct"])
+    np.testing.assert_array_equal(out, img)
+
+
+def test_config0_round_trip_512x512_rgb():
+    """The CPU-runnable round trip: 512x512x3 8-bit, DC shift, RCT, 5-level
+    5/3, lossless quantiser, inverse RCT, inverse DC shift -> identical."""
+    img = synth_image(512, 512, 3, 8, seed=0)
+    cs = codec.encode(img, 8, levels=5, reversible=True, mct=True)
+    info, desc, pool = codec.parse(cs)
+    out = O.decode_tile(desc, pool, 512, 512, 3, 8, 5, True, True)
+    np.testing.assert_array_equal(out, img)
+
+
+@pytest.mark.parametrize("orient", [0, 1, 2, 3])
+@pytest.mark.parametrize("w,h", [(64, 64), (32, 32), (1, 1), (64, 1), (1, 64), (17, 45), (63, 5)])
+def test_t1_block_truncation(orient, w, h):
+    """Encode one block, keep a random number of passes, decode with the
+    oracle: the result equals the coefficients truncated to the decoded
+    bit-planes of each pass."""
+    rng = np.random.default_rng(orient * 1000 + w * 64 + h)
+    coef = laplacian_block(rng, w, h, bitplanes=int(rng.integers(1, 14)))
+    mb = 14
+    seg, total, zbp = codec.t1_encode_block(coef, orient, mb)
+    numbps = mb - zbp
+    if total == 0:
+        assert not coef.any()
+        return
+    assert total == 3 * numbps - 2
+    q, u = O.t1_decode(seg, w, h, orient, numbps, total)
+    np.testing.assert_array_equal(q, coef)
+    for passes in sorted(set(rng.integers(1, total + 1, 4).tolist()) | {1, total}):
+        seg_k, got, _ = codec.t1_encode_block(coef, orient, mb, passes)
+        assert got == passes
+        q, u = O.t1_decode(seg_k, w, h, orient, numbps, passes)
+        # every decoded magnitude is a prefix of the true magnitude
+        mag = np.abs(coef)
+        assert np.all((np.abs(q) >> u) << u == np.abs(q))
+        assert np.all((mag >> u) == np.abs(q) >> u)
+        assert np.all(np.sign(q)[q != 0] == np.sign(coef)[q != 0])
+
+
+def test_parser_rejects_corrupt_streams():
+    img = synth_image(64, 48, 3, 8, seed=3)
+    cs = codec.encode(img, 8, levels=3)
+    with pytest.raises(TCError) as e:
+        codec.parse(cs[:40])
+    assert e.value.status in (TC_E_CODESTREAM,)
+    with pytest.raises(TCError):
+        codec.parse(b"\x00\x01" + cs[2:])
+    # truncated packet data: the code-block lengths run past the tile-part
+    with pytest.raises(TCError) as e:
+        codec.parse(cs[: len(cs) // 2])
+    assert e.value.status == TC_E_CODESTREAM
+    # random corruption never crashes the parser
+    rng = np.random.default_rng(0)
+    for _ in range(200):
+        b = bytearray(cs)
+        for _k in range(4):
+            b[int(rng.integers(0, len(b)))] = int(rng.integers(0, 256))
+        try:
+            codec.parse(bytes(b))
+        except TCError as ex:
+            assert ex.status in (TC_E_CODESTREAM, TC_E_UNSUPPORTED, -1)
+
+
+def test_header_fields():
+    img = synth_image(300, 200, 3, 12, seed=9)
+    cs = codec.encode(img, 12, levels=4, reversible=False, mct=True, base_step=1 / 64)
+    h = codec.read_header(cs)
+    assert (h["width"], h["height"], h["ncomp"], h["bits"], h["levels"], h["reversible"], h["mct"]) == \
+        (300, 200, 3, 12, 4, 0, 1)
+    assert h["quant_style"] == 2
+
+
+def test_our_encoder_decodes_in_openjpeg():
+    PIL = pytest.importorskip("PIL.Image")
+    img = synth_image(96, 80, 3, 8, seed=11)
+    cs = codec.encode(img, 8, levels=4, reversible=True, mct=True)
+    dec = np.moveaxis(np.asarray(PIL.open(io.BytesIO(cs))), -1, 0)
+    np.testing.assert_array_equal(dec, img)
+
+
+def test_sort_order_longest_first():
+    d = np.zeros(5, codec.DESC_DTYPE)
+    d["w"] = d["h"] = 64
+    d["passes"] = [1, 7, 3, 7, 0]
+    d["seg_len"] = [10, 5, 3, 50, 0]
+    assert codec.sort_order(d).tolist() == [3, 1, 2, 0, 4]

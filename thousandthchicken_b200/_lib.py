@@ -103,6 +103,8 @@ _PROTOS = {
     "tc_plan_output_bytes": (_I, [_VP, _I, C.POINTER(C.c_size_t)]),
     "tc_plan_image_info": (_I, [_VP, _I, C.POINTER(ImageInfo)]),
     "tc_plan_execute": (_I, [_VP, _VP]),
+    "tc_plan_set_profiling": (_I, [_VP, _I]),
+    "tc_plan_stage_ms": (_I, [_VP, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "tc_encode_j2k": (_I, [C.POINTER(EncodeParams), _VP, _VP, C.c_size_t, C.POINTER(C.c_size_t)]),
     "tc_t1_encode_block": (_I, [_VP, _I, _I, _I, _I, _I, _VP, _I, C.POINTER(_I), C.POINTER(_I),
                                 C.POINTER(_I)]),

@@ -154,6 +154,8 @@ struct tc_plan {
     uint64_t pool_len = 0;
     size_t scratch_per_img = 0;
     float recon_r = 0.5f;
+    bool profiling = false;
+    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
 };
 
 static int plan_build(tc_ctx *ctx, const uint8_t *const *cs, const size_t *lens, int n, tc_plan *P)
@@ -221,11 +223,13 @@ static int plan_build(tc_ctx *ctx, const uint8_t *const *cs, const size_t *lens,
 static int plan_run(tc_plan *P, void *const *d_out)
 {
     tc_ctx *ctx = P->ctx;
+    if (P->profiling) cudaEventRecord(P->ev[0], ctx->stream);
     cudaError_t e = launch_t1_decode(ctx, static_cast<tc_cblk_desc *>(P->desc.ptr),
                                      static_cast<uint32_t *>(P->order.ptr), P->ncblk,
                                      static_cast<uint8_t *>(P->pool.ptr), P->pool_len, P->coef.ptr,
                                      TC_T1_OUT_DEQUANT, P->recon_r);
     if (e != cudaSuccess) return cuda_status(ctx, e, "Tier-1 launch");
+    if (P->profiling) cudaEventRecord(P->ev[1], ctx->stream);
     for (size_t i = 0; i < P->imgs.size(); i++) {
         const tc_image_info &inf = P->imgs[i].info;
         char *coef = static_cast<char *>(P->coef.ptr) + P->imgs[i].coef_off;
@@ -251,6 +255,7 @@ static int plan_run(tc_plan *P, void *const *d_out)
         }
         if (rc) return rc;
     }
+    if (P->profiling) cudaEventRecord(P->ev[2], ctx->stream);
     return TC_OK;
 }
 
@@ -589,8 +594,35 @@ int tc_plan_destroy(tc_plan *P)
     P->order.release();
     P->coef.release();
     P->scratch.release();
+    for (auto &e : P->ev)
+        if (e) cudaEventDestroy(e);
     delete P;
     return TC_OK;
+}
+
+int tc_plan_set_profiling(tc_plan *P, int on)
+{
+    if (!P) return TC_E_ARG;
+    int rc = check_ctx(P->ctx);
+    if (rc) return rc;
+    if (on && !P->ev[0])
+        for (auto &e : P->ev) {
+            cudaError_t r = cudaEventCreate(&e);
+            if (r != cudaSuccess) return cuda_status(P->ctx, r, "cudaEventCreate");
+        }
+    P->profiling = on != 0;
+    return TC_OK;
+}
+
+int tc_plan_stage_ms(tc_plan *P, float *t1_ms, float *dwt_ms)
+{
+    if (!P || !P->profiling || !t1_ms || !dwt_ms) return TC_E_ARG;
+    int rc = check_ctx(P->ctx);
+    if (rc) return rc;
+    cudaError_t e = cudaEventSynchronize(P->ev[2]);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(t1_ms, P->ev[0], P->ev[1]);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(dwt_ms, P->ev[1], P->ev[2]);
+    return cuda_status(P->ctx, e, "tc_plan_stage_ms");
 }
 
 int tc_plan_output_bytes(const tc_plan *P, int image, size_t *bytes)

@@ -383,7 +383,11 @@ t1_decode_kernel(const tc_cblk_desc *__restrict__ desc, const uint32_t *__restri
         if (lane == 0) idx = (int)atomicAdd(&words[1], 1u);
         idx = __shfl_sync(0xffffffffu, idx, 0);
         if (idx >= n) break;
-        const int bi = order ? (int)order[idx] : idx;
+        const uint32_t bi = order ? order[idx] : (uint32_t)idx;
+        if (bi >= (uint32_t)n) {
+            if (lane == 0) atomicOr(&words[0], TC_DERR_DESC);
+            continue;
+        }
         const tc_cblk_desc d = desc[bi];
         const int w = d.w, h = d.h;
         const bool geom_ok = w >= 1 && w <= 64 && h >= 1 && h <= 64;
