@@ -339,7 +339,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--size", type=int, default=0,
+                    help="square image side for a smaller case of the same workload (profiling)")
     args = ap.parse_args()
+    if args.size:
+        WORKLOAD["width"] = WORKLOAD["height"] = args.size
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
