@@ -100,13 +100,17 @@ typedef struct tc_cblk_desc {
  * blocks taken from a device work queue in the order d_order gives; NULL =
  * descriptor order; the host-side tc_t1_sort_order() produces a
  * longest-first order).  With TC_T1_OUT_DEQUANT the inverse quantiser is
- * fused in: reconstruction point recon_r in [0,1) for truncated blocks
- * (ISO E.1.1.2; 0 = truncated value).  Replaces
- * CoefficientCoder::decode_tile/decodeInit/decode (CoefficientCoder.cpp:62-252)
- * plus Quantizer::dequantize_tile (Quantizer.cpp:181-216). */
+ * fused in: reconstruction point recon_r in [0,1) (ISO E.1.1.2; the
+ * irreversible path adds it on the last decoded plane, the reversible path
+ * only for truncated blocks; 0 = truncated value).  max_bitplanes bounds
+ * Mb - zero_bitplanes over the blocks (0 = up to 31); it sizes the
+ * magnitude storage, and a block above it is flagged as out of range.
+ * Replaces CoefficientCoder::decode_tile/decodeInit/decode
+ * (CoefficientCoder.cpp:62-252) plus Quantizer::dequantize_tile
+ * (Quantizer.cpp:181-216). */
 int tc_t1_decode(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint32_t *d_order,
                  int n, const uint8_t *d_pool, uint64_t pool_len, void *d_out,
-                 int out_mode, float recon_r);
+                 int out_mode, float recon_r, int max_bitplanes);
 
 /* Host helper: write into h_order a permutation of 0..n-1 sorted by
  * decreasing estimated work (passes x area, then codeword length). */

@@ -84,7 +84,7 @@ _PROTOS = {
     "tc_ctx_synchronize": (_I, [_VP]),
     "tc_ctx_last_error": (C.c_char_p, [_VP]),
     "tc_ctx_launch_count": (C.c_uint64, [_VP]),
-    "tc_t1_decode": (_I, [_VP, _VP, _VP, _I, _VP, C.c_uint64, _VP, _I, C.c_float]),
+    "tc_t1_decode": (_I, [_VP, _VP, _VP, _I, _VP, C.c_uint64, _VP, _I, C.c_float, _I]),
     "tc_t1_sort_order": (_I, [_VP, _I, _VP]),
     "tc_dequantize_raw": (_I, [_VP, _VP, _I, _VP, _VP, C.c_float]),
     "tc_dwt_forward53": (_I, [_VP, _VP, _I, _VP, _I, _I, _I, _I, _I]),

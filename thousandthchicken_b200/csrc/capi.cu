@@ -129,6 +129,25 @@ static int run_reverse(tc_ctx *ctx, int wavelet, int rounding, const void *const
     return TC_OK;
 }
 
+void t1_class_order(const tc_cblk_desc *h_desc, int n, uint32_t *h_order, int counts[3])
+{
+    std::vector<uint32_t> all(n);
+    tc_t1_sort_order(h_desc, n, all.data());
+    counts[0] = counts[1] = counts[2] = 0;
+    std::vector<uint32_t> cls[3];
+    for (uint32_t i : all) {
+        const tc_cblk_desc &d = h_desc[i];
+        const int nb = d.passes ? (int)d.mb - (int)d.zero_bitplanes : 0;
+        const int k = nb <= 8 ? 0 : (nb <= 16 ? 1 : 2);
+        cls[k].push_back(i);
+    }
+    int o = 0;
+    for (int k = 0; k < 3; k++) {
+        counts[k] = (int)cls[k].size();
+        for (uint32_t i : cls[k]) h_order[o++] = i;
+    }
+}
+
 static size_t reverse_scratch_bytes(int w, int h, int levels, int ncomp)
 {
     if (levels < 2) return 0;
@@ -154,6 +173,7 @@ struct tc_plan {
     uint64_t pool_len = 0;
     size_t scratch_per_img = 0;
     float recon_r = 0.5f;
+    int class_counts[3] = {0, 0, 0};  // Tier-1 blocks of <= 8, <= 16, <= 31 coded bit-planes
     bool profiling = false;
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
 };
@@ -200,7 +220,7 @@ static int plan_build(tc_ctx *ctx, const uint8_t *const *cs, const size_t *lens,
         po += (pl + 15) & ~uint64_t(15);
     }
     std::vector<uint32_t> horder(P->ncblk);
-    tc_t1_sort_order(hdesc.data(), P->ncblk, horder.data());
+    t1_class_order(hdesc.data(), P->ncblk, horder.data(), P->class_counts);
     P->pool_len = pool_total;
     P->scratch_per_img = scratch_max;
     cudaError_t e;
@@ -224,10 +244,11 @@ static int plan_run(tc_plan *P, void *const *d_out)
 {
     tc_ctx *ctx = P->ctx;
     if (P->profiling) cudaEventRecord(P->ev[0], ctx->stream);
-    cudaError_t e = launch_t1_decode(ctx, static_cast<tc_cblk_desc *>(P->desc.ptr),
-                                     static_cast<uint32_t *>(P->order.ptr), P->ncblk,
-                                     static_cast<uint8_t *>(P->pool.ptr), P->pool_len, P->coef.ptr,
-                                     TC_T1_OUT_DEQUANT, P->recon_r);
+    cudaError_t e = launch_t1_classes(ctx, static_cast<tc_cblk_desc *>(P->desc.ptr),
+                                      static_cast<uint32_t *>(P->order.ptr), P->ncblk, P->class_counts[0],
+                                      P->class_counts[1], P->class_counts[2],
+                                      static_cast<uint8_t *>(P->pool.ptr), P->pool_len, P->coef.ptr,
+                                      TC_T1_OUT_DEQUANT, P->recon_r);
     if (e != cudaSuccess) return cuda_status(ctx, e, "Tier-1 launch");
     if (P->profiling) cudaEventRecord(P->ev[1], ctx->stream);
     for (size_t i = 0; i < P->imgs.size(); i++) {
@@ -340,14 +361,17 @@ const char *tc_ctx_last_error(const tc_ctx *ctx) { return ctx ? ctx->err.c_str()
 uint64_t tc_ctx_launch_count(const tc_ctx *ctx) { return ctx ? ctx->launches : 0; }
 
 int tc_t1_decode(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint32_t *d_order, int n, const uint8_t *d_pool,
-                 uint64_t pool_len, void *d_out, int out_mode, float recon_r)
+                 uint64_t pool_len, void *d_out, int out_mode, float recon_r, int max_bitplanes)
 {
     int rc = check_ctx(ctx);
     if (rc) return rc;
     if (n < 0 || (n > 0 && (!d_desc || !d_out || (!d_pool && pool_len))) ||
         (out_mode != TC_T1_OUT_DEQUANT && out_mode != TC_T1_OUT_RAW) || !(recon_r >= 0.0f && recon_r < 1.0f))
         return fail(ctx, TC_E_ARG, "tc_t1_decode: bad argument");
-    return cuda_status(ctx, launch_t1_decode(ctx, d_desc, d_order, n, d_pool, pool_len, d_out, out_mode, recon_r),
+    if (max_bitplanes <= 0 || max_bitplanes > 31) max_bitplanes = 31;
+    return cuda_status(ctx,
+                       launch_t1_decode(ctx, d_desc, d_order, n, d_pool, pool_len, d_out, out_mode, recon_r,
+                                        max_bitplanes),
                        "tc_t1_decode");
 }
 

@@ -33,6 +33,12 @@ __device__ __forceinline__ int pse(int i, int n)
     return i >= n ? per - i : i;
 }
 
+// Index inside [0, n) after extension; the modulo path only runs at borders.
+__device__ __forceinline__ int mirror(int i, int n)
+{
+    return (unsigned)i < (unsigned)n ? i : pse(i, n);
+}
+
 // 9/7 lifting constants (ISO F.4.8.2).
 constexpr float kA = -1.586134342059924f, kB = -0.052980118572961f, kG = 0.882911075530934f,
                 kD = 0.443506852043971f, kK = 1.230174104914001f, kInvK = 1.0f / 1.230174104914001f;
@@ -268,7 +274,7 @@ __device__ void load_rev(Tile<T, NR, NC> &t, const T *ll, int llp, const T *coef
     for (int q = threadIdx.x; q < NR * NC; q += blockDim.x) {
         const int r = q / NC, rem = q % NC, par = rem / NE, i = rem % NE;
         const int e = 2 * i + par;
-        const int my = pse(y0 - H + r, h), mx = pse(x0 - H + e, w);
+        const int my = mirror(y0 - H + r, h), mx = mirror(x0 - H + e, w);
         const int yb = my >> 1, xb = mx >> 1;
         T v;
         if (!(my & 1)) v = (mx & 1) ? coef[(size_t)yb * cp + wl + xb] : ll[(size_t)yb * llp + xb];
@@ -285,7 +291,7 @@ __device__ void load_fwd(Tile<T, NR, NC> &t, const T *in, int ip, int x0, int y0
     for (int q = threadIdx.x; q < NR * NC; q += blockDim.x) {
         const int r = q / NC, rem = q % NC, par = rem / NE, i = rem % NE;
         const int e = 2 * i + par;
-        const int my = pse(y0 - H + r, h), mx = pse(x0 - H + e, w);
+        const int my = mirror(y0 - H + r, h), mx = mirror(x0 - H + e, w);
         t.d[r * NC + (par ? NE : 0) + i] = in[(size_t)my * ip + mx];
     }
     __syncthreads();
@@ -371,7 +377,7 @@ __device__ __forceinline__ OT clamp_out(int v, int mx)
     return (OT)(v < 0 ? 0 : (v > mx ? mx : v));
 }
 
-template <typename T, int WAVELET, int RND, int COLOR, typename OT>
+template <typename T, int WAVELET, int RND, int COLOR, typename OT, int NCOMP>
 __global__ void __launch_bounds__(256) idwt_last_color_kernel(LevelIO io, int bits)
 {
     constexpr int TX = 64, TY = 32;
@@ -380,8 +386,9 @@ __global__ void __launch_bounds__(256) idwt_last_color_kernel(LevelIO io, int bi
     __shared__ Tile<T, NR, NC> t;
     const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
     const int w = io.w, h = io.h;
-    T res[4][PER];
-    for (int c = 0; c < io.ncomp; c++) {
+    T res[NCOMP][PER];
+#pragma unroll
+    for (int c = 0; c < NCOMP; c++) {
         if (c) __syncthreads();
         load_rev<T, NR, NC, H>(t, static_cast<const T *>(io.ll[c]), io.ll_pitch,
                                static_cast<const T *>(io.coef[c]), io.coef_pitch, x0, y0, w, h);
@@ -418,7 +425,8 @@ __global__ void __launch_bounds__(256) idwt_last_color_kernel(LevelIO io, int bi
             v[1] = __float2int_rn(Y - 0.34413f * Cb - 0.71414f * Cr);
             v[2] = __float2int_rn(fmaf(1.772f, Cb, Y));
         }
-        for (int c = 0; c < io.ncomp; c++) {
+#pragma unroll
+        for (int c = 0; c < NCOMP; c++) {
             int s;
             if (COLOR != TC_COLOR_DC && c < 3) s = v[c];
             else if constexpr (WAVELET == 0) s = (int)res[c][j];
@@ -446,18 +454,33 @@ cudaError_t run_fdwt(tc_ctx *ctx, const LevelIO &io)
     return cudaGetLastError();
 }
 
-template <typename T, int WAVELET, int RND, int COLOR>
-cudaError_t run_last(tc_ctx *ctx, const LevelIO &io, int out_type, int bits)
+template <typename T, int WAVELET, int RND, int COLOR, int NCOMP>
+cudaError_t run_last_n(tc_ctx *ctx, const LevelIO &io, int out_type, int bits)
 {
     dim3 grid((io.w + 63) / 64, (io.h + 31) / 32, 1);
     if (out_type == TC_U8)
-        idwt_last_color_kernel<T, WAVELET, RND, COLOR, uint8_t><<<grid, 256, 0, ctx->stream>>>(io, bits);
+        idwt_last_color_kernel<T, WAVELET, RND, COLOR, uint8_t, NCOMP><<<grid, 256, 0, ctx->stream>>>(io, bits);
     else if (out_type == TC_U16)
-        idwt_last_color_kernel<T, WAVELET, RND, COLOR, uint16_t><<<grid, 256, 0, ctx->stream>>>(io, bits);
+        idwt_last_color_kernel<T, WAVELET, RND, COLOR, uint16_t, NCOMP><<<grid, 256, 0, ctx->stream>>>(io, bits);
     else
-        idwt_last_color_kernel<T, WAVELET, RND, COLOR, int32_t><<<grid, 256, 0, ctx->stream>>>(io, bits);
+        idwt_last_color_kernel<T, WAVELET, RND, COLOR, int32_t, NCOMP><<<grid, 256, 0, ctx->stream>>>(io, bits);
     ctx->launches++;
     return cudaGetLastError();
+}
+
+template <typename T, int WAVELET, int RND, int COLOR>
+cudaError_t run_last(tc_ctx *ctx, const LevelIO &io, int out_type, int bits)
+{
+    if (COLOR != TC_COLOR_DC) {
+        if (io.ncomp == 4) return run_last_n<T, WAVELET, RND, COLOR, 4>(ctx, io, out_type, bits);
+        return run_last_n<T, WAVELET, RND, COLOR, 3>(ctx, io, out_type, bits);
+    }
+    switch (io.ncomp) {
+    case 1: return run_last_n<T, WAVELET, RND, COLOR, 1>(ctx, io, out_type, bits);
+    case 2: return run_last_n<T, WAVELET, RND, COLOR, 2>(ctx, io, out_type, bits);
+    case 3: return run_last_n<T, WAVELET, RND, COLOR, 3>(ctx, io, out_type, bits);
+    default: return run_last_n<T, WAVELET, RND, COLOR, 4>(ctx, io, out_type, bits);
+    }
 }
 
 }  // namespace

@@ -20,6 +20,8 @@
 //     with the inverse quantiser fused in (ISO E.1, reconstruction point r).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "tc_internal.cuh"
 
 namespace tc {
@@ -45,13 +47,16 @@ __constant__ uint8_t c_nlps[47] = {
     19, 19, 20, 21, 22, 23, 24, 25, 26, 27, 28, 29, 30, 31, 32, 33, 34, 35, 36, 37,
     38, 39, 40, 41, 42, 43, 46};
 
+template <typename MagT>
 struct WarpState {
-    unsigned long long sig[kCols];
-    unsigned long long sgn[kCols];
-    unsigned long long ref[kCols];
-    unsigned long long vis[kCols];
-    uint32_t ctx[20];
-    uint32_t mag[64 * 64];
+    unsigned long long sig[kCols];   // significance, bit r = row r
+    unsigned long long sgn[kCols];   // sign (1 = negative)
+    unsigned long long ref[kCols];   // refined at least once (sigma')
+    unsigned long long vis[kCols];   // coded in this plane's significance pass (pi)
+    uint32_t ctx[20];                // packed probability state per context
+    uint8_t mrow[64];                // refinement pass: rows of the stripe to refine
+    uint8_t mctx[64];                // refinement pass: 2-bit context code per row
+    MagT mag[64 * 64];               // magnitude bits decoded so far
 };
 
 struct Tables {
@@ -139,6 +144,8 @@ struct MQ {
             c += byte_at(bp) << 8;
             ct = 8;
         }
+        // keep the codeword stream ahead of the decoder in L1
+        if ((bp & 63) == 0 && bp + 256 < len) asm volatile("prefetch.global.L1 [%0];" ::"l"(p + bp + 256));
     }
     __device__ __forceinline__ void init(const uint8_t *d, int n)
     {
@@ -224,10 +231,25 @@ __device__ __forceinline__ uint32_t nb_rows(uint32_t wl, uint32_t wc, uint32_t w
     return ((n | (n >> 1) | (n >> 2)) | (wc | (wc >> 2))) & 0xFu;
 }
 
-// Serial decode of one code-block by one lane.  Returns the last pass type
-// (0 cleanup, 1 significance propagation, 2 refinement) and its plane.
-__device__ int decode_block(WarpState &S, const Tables &T, const uint8_t *seg, int len, int w,
-                            int h, int orient, int numbps, int passes, int *last_plane)
+// Lane-parallel candidate test for the significance pass: does column c
+// (window rows of stripe s) hold an insignificant coefficient with a
+// significant neighbour?
+template <typename MagT>
+__device__ __forceinline__ bool spp_candidate(const WarpState<MagT> &S, int c, int s, uint32_t rmask)
+{
+    const uint32_t wl = win6(S.sig[c], s), wc = win6(S.sig[c + 1], s), wr = win6(S.sig[c + 2], s);
+    return (~(wc >> 1) & rmask & nb_rows(wl, wc, wr)) != 0u;
+}
+
+// Decode one code-block.  Every lane of the warp runs this function in
+// lock-step (the MQ state is replicated, shared-memory accesses are
+// broadcasts); lanes split the per-stripe candidate searches between them
+// (lane l owns columns l and l+32) and the serial loop visits only the
+// candidate columns, in scan order.  Returns the last pass type (0 cleanup,
+// 1 significance propagation, 2 refinement) and its plane.
+template <typename MagT>
+__device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *seg, int len, int w,
+                            int h, int orient, int numbps, int passes, int *last_plane, int lane)
 {
     MQ mq;
     mq.init(seg, len);
@@ -235,74 +257,97 @@ __device__ int decode_block(WarpState &S, const Tables &T, const uint8_t *seg, i
     const uint32_t *tbl = T.mq;
     const uint8_t *zc = T.zc[orient];
     const int nstripes = (h + 3) >> 2;
+    const int c0 = lane, c1 = lane + 32;
     int type = 0, pass = 0;
     *last_plane = numbps - 1;
 
     for (int p = numbps - 1; p >= 0; --p) {
-        const uint32_t pbit = 1u << p;
+        const MagT pbit = (MagT)(1u << p);
         if (p != numbps - 1) {
             // ---- significance propagation pass (ISO D.3.1; SigPropPassFunctor) ----
             for (int s = 0; s < nstripes; s++) {
                 const int rows = min(4, h - 4 * s);
                 const uint32_t rmask = (1u << rows) - 1u;
-                uint32_t wl = 0, sl = 0;
-                uint32_t wc = win6(S.sig[1], s), sc = win6(S.sgn[1], s);
-                for (int c = 0; c < w; c++) {
-                    const uint32_t wr = win6(S.sig[c + 2], s), sr = win6(S.sgn[c + 2], s);
-                    const uint32_t insig = ~(wc >> 1) & rmask;
-                    if (insig & nb_rows(wl, wc, wr)) {
-                        uint32_t vmask = 0;
-                        const uint32_t wc0 = wc;
-                        for (int k = 0; k < rows; k++) {
-                            if ((wc >> (k + 1)) & 1u) continue;
-                            const uint32_t pat = zc_pattern(wl, wc, wr, k);
-                            if (!pat) continue;
-                            vmask |= 1u << k;
-                            if (mq.decode(ctx, tbl, zc[pat])) {
-                                const uint32_t si = T.sc[sc_index(wl, sl, wc, sc, wr, sr, k)];
-                                const uint32_t neg = (uint32_t)mq.decode(ctx, tbl, si & 15) ^ (si >> 4);
-                                wc |= 2u << k;
-                                sc |= neg << (k + 1);
-                                S.mag[(4 * s + k) * 64 + c] = pbit;
-                            }
+                __syncwarp();
+                const bool a0 = c0 < w && spp_candidate(S, c0, s, rmask);
+                const bool a1 = c1 < w && spp_candidate(S, c1, s, rmask);
+                unsigned long long cand = (unsigned long long)__ballot_sync(0xffffffffu, a0) |
+                                          ((unsigned long long)__ballot_sync(0xffffffffu, a1) << 32);
+                while (cand) {
+                    const int c = __ffsll((long long)cand) - 1;
+                    cand &= cand - 1;
+                    const uint32_t wl = win6(S.sig[c], s), wr = win6(S.sig[c + 2], s);
+                    uint32_t wc = win6(S.sig[c + 1], s);
+                    const uint32_t wc0 = wc;
+                    uint32_t sc = win6(S.sgn[c + 1], s);
+                    uint32_t vmask = 0;
+                    for (int k = 0; k < rows; k++) {
+                        if ((wc >> (k + 1)) & 1u) continue;
+                        const uint32_t pat = zc_pattern(wl, wc, wr, k);
+                        if (!pat) continue;
+                        vmask |= 1u << k;
+                        if (mq.decode(ctx, tbl, zc[pat])) {
+                            const uint32_t sl = win6(S.sgn[c], s), sr = win6(S.sgn[c + 2], s);
+                            const uint32_t si = T.sc[sc_index(wl, sl, wc, sc, wr, sr, k)];
+                            const uint32_t neg = (uint32_t)mq.decode(ctx, tbl, si & 15) ^ (si >> 4);
+                            wc |= 2u << k;
+                            sc |= neg << (k + 1);
+                            S.mag[(4 * s + k) * 64 + c] = pbit;
                         }
-                        if (wc != wc0) {
-                            S.sig[c + 1] |= (unsigned long long)((wc >> 1) & 0xFu) << (4 * s);
-                            S.sgn[c + 1] |= (unsigned long long)((sc >> 1) & 0xFu) << (4 * s);
-                        }
-                        S.vis[c + 1] |= (unsigned long long)vmask << (4 * s);
                     }
-                    wl = wc;
-                    sl = sc;
-                    wc = wr;
-                    sc = sr;
+                    if (wc != wc0) {
+                        S.sig[c + 1] |= (unsigned long long)((wc >> 1) & 0xFu) << (4 * s);
+                        S.sgn[c + 1] |= (unsigned long long)((sc >> 1) & 0xFu) << (4 * s);
+                        if (c + 1 < w) cand |= 1ull << (c + 1);  // the next column gained a neighbour
+                    }
+                    if (vmask) S.vis[c + 1] |= (unsigned long long)vmask << (4 * s);
                 }
             }
             type = 1;
             *last_plane = p;
             if (++pass >= passes) break;
+            __syncwarp();
 
             // ---- magnitude refinement pass (ISO D.3.3; MagRefPassFunctor) ----
+            // The rows to refine and their contexts do not change during the
+            // pass, so the lanes precompute them for their columns.
             for (int s = 0; s < nstripes; s++) {
                 const int rows = min(4, h - 4 * s);
                 const uint32_t rmask = (1u << rows) - 1u;
-                uint32_t wl = 0, wc = win6(S.sig[1], s);
-                for (int c = 0; c < w; c++) {
-                    const uint32_t wr = win6(S.sig[c + 2], s);
-                    const uint32_t vis = (uint32_t)(S.vis[c + 1] >> (4 * s)) & 0xFu;
-                    const uint32_t cand = (wc >> 1) & rmask & ~vis;
-                    if (cand) {
+                bool any[2];
+#pragma unroll
+                for (int j = 0; j < 2; j++) {
+                    const int c = lane + 32 * j;
+                    uint32_t rr = 0, codes = 0;
+                    if (c < w) {
+                        const uint32_t wl = win6(S.sig[c], s), wc = win6(S.sig[c + 1], s),
+                                       wr = win6(S.sig[c + 2], s);
+                        const uint32_t vis = (uint32_t)(S.vis[c + 1] >> (4 * s)) & 0xFu;
                         const uint32_t ref = (uint32_t)(S.ref[c + 1] >> (4 * s)) & 0xFu;
-                        for (int k = 0; k < rows; k++) {
-                            if (!((cand >> k) & 1u)) continue;
-                            const int cx = ((ref >> k) & 1u) ? 16 : (zc_pattern(wl, wc, wr, k) ? 15 : 14);
-                            if (mq.decode(ctx, tbl, cx)) S.mag[(4 * s + k) * 64 + c] |= pbit;
-                        }
-                        S.ref[c + 1] |= (unsigned long long)cand << (4 * s);
+                        rr = (wc >> 1) & rmask & ~vis;
+                        for (int k = 0; k < 4; k++)
+                            codes |= (((ref >> k) & 1u) ? 2u : (zc_pattern(wl, wc, wr, k) ? 1u : 0u)) << (2 * k);
+                        S.mrow[c] = (uint8_t)rr;
+                        S.mctx[c] = (uint8_t)codes;
+                        S.ref[c + 1] |= (unsigned long long)rr << (4 * s);
                     }
-                    wl = wc;
-                    wc = wr;
+                    any[j] = rr != 0;
                 }
+                unsigned long long cand = (unsigned long long)__ballot_sync(0xffffffffu, any[0]) |
+                                          ((unsigned long long)__ballot_sync(0xffffffffu, any[1]) << 32);
+                __syncwarp();
+                while (cand) {
+                    const int c = __ffsll((long long)cand) - 1;
+                    cand &= cand - 1;
+                    uint32_t rr = S.mrow[c];
+                    const uint32_t codes = S.mctx[c];
+                    while (rr) {
+                        const int k = __ffs(rr) - 1;
+                        rr &= rr - 1;
+                        if (mq.decode(ctx, tbl, 14 + ((codes >> (2 * k)) & 3u))) S.mag[(4 * s + k) * 64 + c] |= pbit;
+                    }
+                }
+                __syncwarp();
             }
             type = 2;
             if (++pass >= passes) break;
@@ -311,81 +356,89 @@ __device__ int decode_block(WarpState &S, const Tables &T, const uint8_t *seg, i
         // ---- cleanup pass (ISO D.3.4; CleanUpPassFunctor) ----
         for (int s = 0; s < nstripes; s++) {
             const int rows = min(4, h - 4 * s);
-            uint32_t wl = 0, sl = 0;
-            uint32_t wc = win6(S.sig[1], s), sc = win6(S.sgn[1], s);
-            for (int c = 0; c < w; c++) {
-                const uint32_t wr = win6(S.sig[c + 2], s), sr = win6(S.sgn[c + 2], s);
-                const uint32_t vis = (uint32_t)(S.vis[c + 1] >> (4 * s)) & 0xFu;
+            const uint32_t rmask = (1u << rows) - 1u;
+            __syncwarp();
+            bool any[2];
+#pragma unroll
+            for (int j = 0; j < 2; j++) {
+                const int c = lane + 32 * j;
+                any[j] = c < w && ((~(uint32_t)((S.sig[c + 1] | S.vis[c + 1]) >> (4 * s))) & rmask) != 0u;
+            }
+            unsigned long long cand = (unsigned long long)__ballot_sync(0xffffffffu, any[0]) |
+                                      ((unsigned long long)__ballot_sync(0xffffffffu, any[1]) << 32);
+            while (cand) {
+                const int c = __ffsll((long long)cand) - 1;
+                cand &= cand - 1;
+                const uint32_t wl = win6(S.sig[c], s), wr = win6(S.sig[c + 2], s);
+                uint32_t wc = win6(S.sig[c + 1], s);
                 const uint32_t wc0 = wc;
+                const uint32_t vis = (uint32_t)(S.vis[c + 1] >> (4 * s)) & 0xFu;
+                uint32_t sc = win6(S.sgn[c + 1], s);
                 int k = 0;
-                bool run_done = false;
                 if (rows == 4 && (wl | wc | wr) == 0u) {
                     // run-length mode: four rows with an all-zero neighbourhood
-                    if (!mq.decode(ctx, tbl, 18)) {
-                        run_done = true;
-                    } else {
-                        int r = mq.decode(ctx, tbl, 17) << 1;
-                        r |= mq.decode(ctx, tbl, 17);
-                        const uint32_t si = T.sc[sc_index(wl, sl, wc, sc, wr, sr, r)];
-                        const uint32_t neg = (uint32_t)mq.decode(ctx, tbl, si & 15) ^ (si >> 4);
-                        wc |= 2u << r;
-                        sc |= neg << (r + 1);
-                        S.mag[(4 * s + r) * 64 + c] = pbit;
-                        k = r + 1;
-                    }
+                    if (!mq.decode(ctx, tbl, 18)) continue;
+                    int r = mq.decode(ctx, tbl, 17) << 1;
+                    r |= mq.decode(ctx, tbl, 17);
+                    const uint32_t sl = win6(S.sgn[c], s), sr = win6(S.sgn[c + 2], s);
+                    const uint32_t si = T.sc[sc_index(wl, sl, wc, sc, wr, sr, r)];
+                    const uint32_t neg = (uint32_t)mq.decode(ctx, tbl, si & 15) ^ (si >> 4);
+                    wc |= 2u << r;
+                    sc |= neg << (r + 1);
+                    S.mag[(4 * s + r) * 64 + c] = pbit;
+                    k = r + 1;
                 }
-                if (!run_done) {
-                    for (; k < rows; k++) {
-                        if (((wc >> (k + 1)) | (vis >> k)) & 1u) continue;
-                        if (mq.decode(ctx, tbl, zc[zc_pattern(wl, wc, wr, k)])) {
-                            const uint32_t si = T.sc[sc_index(wl, sl, wc, sc, wr, sr, k)];
-                            const uint32_t neg = (uint32_t)mq.decode(ctx, tbl, si & 15) ^ (si >> 4);
-                            wc |= 2u << k;
-                            sc |= neg << (k + 1);
-                            S.mag[(4 * s + k) * 64 + c] = pbit;
-                        }
+                for (; k < rows; k++) {
+                    if (((wc >> (k + 1)) | (vis >> k)) & 1u) continue;
+                    if (mq.decode(ctx, tbl, zc[zc_pattern(wl, wc, wr, k)])) {
+                        const uint32_t sl = win6(S.sgn[c], s), sr = win6(S.sgn[c + 2], s);
+                        const uint32_t si = T.sc[sc_index(wl, sl, wc, sc, wr, sr, k)];
+                        const uint32_t neg = (uint32_t)mq.decode(ctx, tbl, si & 15) ^ (si >> 4);
+                        wc |= 2u << k;
+                        sc |= neg << (k + 1);
+                        S.mag[(4 * s + k) * 64 + c] = pbit;
                     }
                 }
                 if (wc != wc0) {
                     S.sig[c + 1] |= (unsigned long long)((wc >> 1) & 0xFu) << (4 * s);
                     S.sgn[c + 1] |= (unsigned long long)((sc >> 1) & 0xFu) << (4 * s);
                 }
-                wl = wc;
-                sl = sc;
-                wc = wr;
-                sc = sr;
             }
         }
         type = 0;
         *last_plane = p;
         if (++pass >= passes) break;
-        for (int c = 0; c < kCols; c++) S.vis[c] = 0ull;
+        __syncwarp();
+        for (int c = lane; c < kCols; c += 32) S.vis[c] = 0ull;
+        __syncwarp();
     }
     return type;
 }
 
+template <typename MagT>
 __global__ void __launch_bounds__(32 * kWarps)
-t1_decode_kernel(const tc_cblk_desc *__restrict__ desc, const uint32_t *__restrict__ order, int n,
-                 const uint8_t *__restrict__ pool, uint64_t pool_len, char *__restrict__ out,
-                 int out_mode, float recon_r, uint32_t *words)
+t1_decode_kernel(const tc_cblk_desc *__restrict__ desc, const uint32_t *__restrict__ order, int n, int ndesc,
+                 const uint8_t *__restrict__ pool, uint64_t pool_len, char *__restrict__ out, int out_mode,
+                 float recon_r, uint32_t *__restrict__ counter, uint32_t *__restrict__ err)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     Tables &T = *reinterpret_cast<Tables *>(smem);
-    WarpState *states = reinterpret_cast<WarpState *>(smem + ((sizeof(Tables) + 15) & ~size_t(15)));
+    WarpState<MagT> *states =
+        reinterpret_cast<WarpState<MagT> *>(smem + ((sizeof(Tables) + 15) & ~size_t(15)));
     build_tables(T);
     __syncthreads();
 
     const int lane = threadIdx.x & 31;
-    WarpState &S = states[threadIdx.x >> 5];
+    WarpState<MagT> &S = states[threadIdx.x >> 5];
 
     for (;;) {
         int idx = 0;
-        if (lane == 0) idx = (int)atomicAdd(&words[1], 1u);
+        if (lane == 0) idx = (int)atomicAdd(counter, 1u);
         idx = __shfl_sync(0xffffffffu, idx, 0);
         if (idx >= n) break;
         const uint32_t bi = order ? order[idx] : (uint32_t)idx;
-        if (bi >= (uint32_t)n) {
-            if (lane == 0) atomicOr(&words[0], TC_DERR_DESC);
+        if (bi >= (uint32_t)ndesc) {
+            if (lane == 0) atomicOr(err, TC_DERR_DESC);
             continue;
         }
         const tc_cblk_desc d = desc[bi];
@@ -393,14 +446,14 @@ t1_decode_kernel(const tc_cblk_desc *__restrict__ desc, const uint32_t *__restri
         const bool geom_ok = w >= 1 && w <= 64 && h >= 1 && h <= 64;
         const int numbps = (int)d.mb - (int)d.zero_bitplanes;
         bool ok = geom_ok && d.mb >= 1 && d.mb <= 31 && d.orient <= 3 && numbps >= 0 &&
-                  (numbps == 0 || d.passes <= 3 * numbps - 2);
+                  (numbps == 0 || d.passes <= 3 * numbps - 2) && numbps <= (int)(8 * sizeof(MagT));
         const bool pool_ok = d.seg_off <= pool_len && (uint64_t)d.seg_len <= pool_len - d.seg_off;
         if (!geom_ok) {
-            if (lane == 0) atomicOr(&words[0], TC_DERR_DESC);
+            if (lane == 0) atomicOr(err, TC_DERR_DESC);
             continue;
         }
         if (!ok || !pool_ok) {
-            if (lane == 0) atomicOr(&words[0], ok ? TC_DERR_POOL : TC_DERR_DESC);
+            if (lane == 0) atomicOr(err, ok ? TC_DERR_POOL : TC_DERR_DESC);
             ok = false;
         }
         const bool coded = ok && numbps > 0 && d.passes > 0;
@@ -419,22 +472,21 @@ t1_decode_kernel(const tc_cblk_desc *__restrict__ desc, const uint32_t *__restri
         __syncwarp();
 
         int type = 0, last_plane = 0;
-        if (coded && lane == 0)
-            type = decode_block(S, T, pool + d.seg_off, (int)d.seg_len, w, h, d.orient, numbps,
-                                d.passes, &last_plane);
-        type = __shfl_sync(0xffffffffu, type, 0);
-        last_plane = __shfl_sync(0xffffffffu, last_plane, 0);
+        if (coded)
+            type = decode_block(S, T, pool + d.seg_off, (int)d.seg_len, w, h, d.orient, numbps, d.passes,
+                                &last_plane, lane);
         __syncwarp();
 
         // epilogue: reconstruction + inverse quantisation, coalesced rows
         const bool irrev = (d.flags & TC_CBLK_IRREVERSIBLE) != 0;
+        const float half_step = recon_r;
         for (int y = 0; y < h; y++) {
             char *row = out + 4 * (d.out_off + (uint64_t)y * d.out_pitch);
             for (int x = lane; x < w; x += 32) {
                 const bool sg = coded && ((S.sig[x + 1] >> y) & 1ull);
                 uint32_t mg = 0, neg = 0, u = 0;
                 if (sg) {
-                    mg = S.mag[y * 64 + x];
+                    mg = (uint32_t)S.mag[y * 64 + x];
                     neg = (uint32_t)(S.sgn[x + 1] >> y) & 1u;
                     u = (uint32_t)last_plane;
                     if (type == 1 && !((S.vis[x + 1] >> y) & 1ull)) u++;
@@ -443,11 +495,11 @@ t1_decode_kernel(const tc_cblk_desc *__restrict__ desc, const uint32_t *__restri
                     reinterpret_cast<uint32_t *>(row)[x] = sg ? ((mg << (31 - d.mb)) | (neg << 31)) : 0u;
                 } else if (irrev) {
                     float v = 0.0f;
-                    if (sg) v = ((float)mg + recon_r * (float)(1u << u)) * d.step;
+                    if (sg) v = ((float)mg + half_step * (float)(1u << u)) * d.step;
                     reinterpret_cast<float *>(row)[x] = neg ? -v : v;
                 } else {
                     int32_t v = 0;
-                    if (sg) v = (int32_t)mg + (u ? (int32_t)floorf(recon_r * (float)(1u << u)) : 0);
+                    if (sg) v = (int32_t)mg + (u ? (int32_t)floorf(half_step * (float)(1u << u)) : 0);
                     reinterpret_cast<int32_t *>(row)[x] = neg ? -v : v;
                 }
             }
@@ -494,31 +546,55 @@ __global__ void dequant_raw_kernel(const tc_cblk_desc *__restrict__ desc, int n,
 
 }  // namespace
 
-cudaError_t launch_t1_decode(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint32_t *d_order, int n,
-                             const uint8_t *d_pool, uint64_t pool_len, void *d_out, int out_mode,
-                             float recon_r)
+namespace {
+template <typename MagT>
+cudaError_t launch_class(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint32_t *d_order, int n, int ndesc,
+                         const uint8_t *d_pool, uint64_t pool_len, void *d_out, int out_mode, float recon_r,
+                         int slot)
 {
-    if (n <= 0) return cudaSuccess;
-    const size_t smem = ((sizeof(Tables) + 15) & ~size_t(15)) + kWarps * sizeof(WarpState);
-    static bool attr_done[64] = {};
-    if (ctx->device >= 0 && ctx->device < 64 && !attr_done[ctx->device]) {
-        cudaError_t e = cudaFuncSetAttribute(t1_decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        attr_done[ctx->device] = true;
-    }
+    const size_t smem = ((sizeof(Tables) + 15) & ~size_t(15)) + kWarps * sizeof(WarpState<MagT>);
+    cudaError_t e = cudaFuncSetAttribute(t1_decode_kernel<MagT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
     int per_sm = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, t1_decode_kernel, 32 * kWarps, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, t1_decode_kernel<MagT>, 32 * kWarps, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
     const int want = (n + kWarps - 1) / kWarps;
     const int grid = std::min(want, per_sm * num_sms(ctx->device));
-    e = cudaMemsetAsync(ctx->d_words + 1, 0, sizeof(uint32_t), ctx->stream);
+    e = cudaMemsetAsync(ctx->d_words + slot, 0, sizeof(uint32_t), ctx->stream);
     if (e != cudaSuccess) return e;
-    t1_decode_kernel<<<grid, 32 * kWarps, smem, ctx->stream>>>(d_desc, d_order, n, d_pool, pool_len,
-                                                               static_cast<char *>(d_out), out_mode,
-                                                               recon_r, ctx->d_words);
+    t1_decode_kernel<MagT><<<grid, 32 * kWarps, smem, ctx->stream>>>(
+        d_desc, d_order, n, ndesc, d_pool, pool_len, static_cast<char *>(d_out), out_mode, recon_r,
+        ctx->d_words + slot, ctx->d_words);
     ctx->launches++;
     return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t launch_t1_decode(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint32_t *d_order, int n,
+                             const uint8_t *d_pool, uint64_t pool_len, void *d_out, int out_mode, float recon_r,
+                             int max_bitplanes)
+{
+    return launch_t1_classes(ctx, d_desc, d_order, n, max_bitplanes <= 8 ? n : 0,
+                             max_bitplanes > 8 && max_bitplanes <= 16 ? n : 0, max_bitplanes > 16 ? n : 0, d_pool,
+                             pool_len, d_out, out_mode, recon_r);
+}
+
+cudaError_t launch_t1_classes(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint32_t *d_order, int ndesc,
+                              int n8, int n16, int n32, const uint8_t *d_pool, uint64_t pool_len, void *d_out,
+                              int out_mode, float recon_r)
+{
+    cudaError_t e = cudaSuccess;
+    if (n8 > 0)
+        e = launch_class<uint8_t>(ctx, d_desc, d_order, n8, ndesc, d_pool, pool_len, d_out, out_mode, recon_r, 1);
+    if (e == cudaSuccess && n16 > 0)
+        e = launch_class<uint16_t>(ctx, d_desc, d_order ? d_order + n8 : nullptr, n16, ndesc, d_pool, pool_len,
+                                   d_out, out_mode, recon_r, 2);
+    if (e == cudaSuccess && n32 > 0)
+        e = launch_class<uint32_t>(ctx, d_desc, d_order ? d_order + n8 + n16 : nullptr, n32, ndesc, d_pool,
+                                   pool_len, d_out, out_mode, recon_r, 3);
+    return e;
 }
 
 cudaError_t launch_dequant_raw(tc_ctx *ctx, const tc_cblk_desc *d_desc, int n, const uint32_t *d_raw,

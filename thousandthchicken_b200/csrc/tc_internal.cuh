@@ -28,7 +28,7 @@ struct tc_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     std::string err;
-    uint32_t *d_words = nullptr;  // [0] error word, [1] T1 work counter
+    uint32_t *d_words = nullptr;  // [0] error word, [1..3] Tier-1 work counters
     tc::DevBuf scratch;           // DWT intermediate levels
     tc::DevBuf tmp_pool, tmp_desc, tmp_order, tmp_coef, tmp_out;
     uint64_t launches = 0;
@@ -43,9 +43,18 @@ int cuda_status(tc_ctx *ctx, cudaError_t e, const char *what);
 
 // ---- kernels' host launchers (each returns a cudaError_t of the launch) ----
 
+// One persistent launch over n blocks whose coded bit-planes are at most
+// max_bitplanes (selects the magnitude storage width: 8, 16 or 32 bits).
 cudaError_t launch_t1_decode(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint32_t *d_order,
                              int n, const uint8_t *d_pool, uint64_t pool_len, void *d_out,
-                             int out_mode, float recon_r);
+                             int out_mode, float recon_r, int max_bitplanes);
+// Up to three persistent launches over an order array partitioned into
+// blocks of at most 8, 16 and 31 coded bit-planes (n8 + n16 + n32 entries).
+cudaError_t launch_t1_classes(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint32_t *d_order,
+                              int ndesc, int n8, int n16, int n32, const uint8_t *d_pool,
+                              uint64_t pool_len, void *d_out, int out_mode, float recon_r);
+// Host: order longest-first within each bit-plane class; class sizes out.
+void t1_class_order(const tc_cblk_desc *h_desc, int n, uint32_t *h_order, int counts[3]);
 cudaError_t launch_dequant_raw(tc_ctx *ctx, const tc_cblk_desc *d_desc, int n,
                                const uint32_t *d_raw, void *d_out, float recon_r);
 

@@ -81,12 +81,13 @@ class CoefficientCoder:
         self.ctx = ctx
 
     def decode(self, desc_dev, pool_dev, out, n: int, order_dev=None, raw: bool = False,
-               recon_r: float = 0.5):
+               recon_r: float = 0.5, max_bitplanes: int = 0):
         """Low-level: descriptors, pool, order and out are device tensors."""
         self.ctx.check(L.lib().tc_t1_decode(self.ctx.handle, _ptr(desc_dev),
                                             _ptr(order_dev) if order_dev is not None else None, n,
                                             _ptr(pool_dev), pool_dev.numel(), _ptr(out),
-                                            L.TC_T1_OUT_RAW if raw else L.TC_T1_OUT_DEQUANT, recon_r),
+                                            L.TC_T1_OUT_RAW if raw else L.TC_T1_OUT_DEQUANT, recon_r,
+                                            max_bitplanes),
                        "tc_t1_decode")
 
     def decode_blocks(self, desc: np.ndarray, pool: np.ndarray, out_elems: int, raw: bool = False,
@@ -105,7 +106,9 @@ class CoefficientCoder:
         if dtype is None:
             dtype = torch.int32 if raw or not (len(desc) and desc["flags"][0] & 1) else torch.float32
         out = torch.zeros(max(out_elems, 1), dtype=dtype, device=dev)
-        self.decode(d_desc, d_pool, out, len(desc), d_order, raw, recon_r)
+        nb = desc["mb"].astype(np.int32) - desc["zero_bitplanes"].astype(np.int32)
+        maxb = int(np.clip(nb[desc["passes"] > 0], 0, 31).max()) if (desc["passes"] > 0).any() else 1
+        self.decode(d_desc, d_pool, out, len(desc), d_order, raw, recon_r, max(maxb, 1))
         self.ctx.synchronize()
         return out
 
