@@ -40,6 +40,16 @@ void DevBuf::release()
     size = 0;
 }
 
+cudaError_t ensure_side_streams(tc_ctx *ctx)
+{
+    if (ctx->side[0]) return cudaSuccess;
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < 2 && e == cudaSuccess; i++) e = cudaStreamCreateWithFlags(&ctx->side[i], cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming);
+    for (int i = 0; i < 2 && e == cudaSuccess; i++) e = cudaEventCreateWithFlags(&ctx->ev_join[i], cudaEventDisableTiming);
+    return e;
+}
+
 int fail(tc_ctx *ctx, int status, const std::string &msg)
 {
     if (ctx) ctx->err = msg;
@@ -334,6 +344,11 @@ int tc_ctx_destroy(tc_ctx *ctx)
     ctx->tmp_coef.release();
     ctx->tmp_out.release();
     if (ctx->d_words) cudaFree(ctx->d_words);
+    for (int i = 0; i < 2; i++) {
+        if (ctx->side[i]) cudaStreamDestroy(ctx->side[i]);
+        if (ctx->ev_join[i]) cudaEventDestroy(ctx->ev_join[i]);
+    }
+    if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
     delete ctx;
     return TC_OK;
 }

@@ -1,23 +1,30 @@
 // t1_decode.cu -- Tier-1 EBCOT/MQ code-block decoder for sm_100a.
 //
 // Replaces the reference g_decode kernel (coefficient_coder.cl:778-819) and
-// the dequantiser kernels (quantizer_*_inverse.cl) with one persistent
-// launch:
+// the dequantiser kernels (quantizer_*_inverse.cl) with persistent launches:
 //   * one warp per code-block; warps pull block indices from a device work
 //     queue (an atomic counter over a longest-first order), so blocks of
 //     uneven size and pass count from many tiles and images share a launch;
-//   * the code-block state lives in shared memory as one 64-bit word per
-//     column and per state bit (significance, sign, refined, visited), so
-//     the 3x6 neighbourhood of a stripe column is three 6-bit windows and a
-//     context label is one table lookup (the reference rebuilds a 3x3 window
-//     of packed words from global memory at every step, :271-298);
-//   * the MQ interval state (A, C, CT, byte position) stays in registers and
-//     each context's probability state is one packed word, so the common MPS
-//     path of a decision is a shared load, two compares and a subtract;
+//   * blocks are split by coded bit-planes (<= 8, <= 16, <= 31) into classes
+//     whose magnitudes are stored as 8-, 16- or 32-bit values; the classes run
+//     as concurrent launches, heaviest first;
+//   * the code-block state is one 32-bit flag word per stripe column: the
+//     significance of its 3x6 neighbourhood interleaved so that row k's 3x3
+//     neighbourhood is (F >> 3k) & 0x1FF, plus the visited (pi) and refined
+//     (sigma') bits of its four rows.  A context label is one shift, one mask
+//     and one table lookup; a coefficient that becomes significant updates the
+//     words of its neighbours.  (The reference rebuilds a 3x3 window of packed
+//     words from global memory at every step, coefficient_coder.cl:271-298.)
+//   * all 32 lanes run the decoder in lock-step (replicated MQ state,
+//     broadcast shared-memory accesses); at every stripe the lanes find the
+//     candidate columns of the pass with __ballot_sync and the serial loop
+//     visits only those; refinement contexts are precomputed by the lanes;
+//   * the MQ byte stream is software-pipelined one byte ahead;
 //   * the pass loop honours the coding-pass count (defect D3 fixed) and
-//     updates the state it reads (defects D1/D2 fixed);
-//   * the warp's lanes clear the state, and write the block out coalesced
-//     with the inverse quantiser fused in (ISO E.1, reconstruction point r).
+//     updates the state it reads (defects D1/D2 fixed); every codeword byte is
+//     consumed (defect D22 fixed) and one-column blocks stay in bounds (D23);
+//   * the epilogue writes the block out coalesced with the inverse quantiser
+//     fused in (ISO E.1, reconstruction point r).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -27,11 +34,21 @@
 namespace tc {
 namespace {
 
-constexpr int kWarps = 4;         // warps (code-blocks in flight) per CTA
-constexpr int kCols = 66;         // 64 columns + a zero column on each side
+constexpr int kWarps = 4;          // warps (code-blocks in flight) per CTA
+constexpr int kMaxStripes = 16;    // 64 rows
+constexpr int kSgnCols = 66;       // 64 columns + a zero column on each side
 
-// ISO Table C.2 (coefficient_coder.cl:36-60), packed per state index as
-// Qe | NMPS << 16 | NLPS << 22 | SWITCH << 28.
+// Flag word layout (one per stripe column):
+//   bits 0-17  significance, bit 3*j + col for row j-1 of the stripe
+//              (j = 0..5, rows -1..4) and col 0 = left, 1 = this, 2 = right
+//   bits 18-21 pi: coded in this plane's significance propagation pass
+//   bits 22-25 sigma': refined at least once
+constexpr uint32_t kSigMask = 0x3FFFFu;
+__device__ __forceinline__ uint32_t self_bit(int k) { return 1u << (3 * k + 4); }
+__device__ __forceinline__ uint32_t pi_bit(int k) { return 1u << (18 + k); }
+__device__ __forceinline__ uint32_t ref_bit(int k) { return 1u << (22 + k); }
+
+// ISO Table C.2 (coefficient_coder.cl:36-60).
 __constant__ uint16_t c_qe[47] = {
     0x5601, 0x3401, 0x1801, 0x0AC1, 0x0521, 0x0221, 0x5601, 0x5401, 0x4801, 0x3801,
     0x3001, 0x2401, 0x1C01, 0x1601, 0x5601, 0x5401, 0x5101, 0x4801, 0x3801, 0x3401,
@@ -49,25 +66,22 @@ __constant__ uint8_t c_nlps[47] = {
 
 template <typename MagT>
 struct WarpState {
-    unsigned long long sig[kCols];   // significance, bit r = row r
-    unsigned long long sgn[kCols];   // sign (1 = negative)
-    unsigned long long ref[kCols];   // refined at least once (sigma')
-    unsigned long long vis[kCols];   // coded in this plane's significance pass (pi)
-    uint32_t ctx[20];                // packed probability state per context
-    uint8_t mrow[64];                // refinement pass: rows of the stripe to refine
-    uint8_t mctx[64];                // refinement pass: 2-bit context code per row
-    MagT mag[64 * 64];               // magnitude bits decoded so far
+    uint32_t F[kMaxStripes * 64];          // flag word per stripe column
+    unsigned long long sgn[kSgnCols];      // sign per column (bit y = row y), zero guard columns
+    uint32_t ctx[20];                      // packed probability state per context
+    uint8_t mrow[64];                      // refinement pass: rows of the stripe to refine
+    uint8_t mctx[64];                      // refinement pass: 2-bit context code per row
+    MagT mag[64 * 64];                     // magnitude bits decoded so far
 };
 
 struct Tables {
-    uint32_t mq[48];          // packed probability states
-    uint8_t zc[4][256];       // zero-coding label per orientation and 8-neighbour pattern
+    uint32_t mq[48];          // packed states: Qe | NMPS << 16 | NLPS << 22 | SWITCH << 28
+    uint8_t zc[4][512];       // zero-coding label per orientation and 3x3 neighbourhood
     uint8_t sc[256];          // sign label | XOR bit << 4
 };
 
 // Zero-coding label from neighbour counts, ISO Table D.1 (the reference's
-// SPCXLUT, coefficient_coder.cl:330-393, indexes the same table by a 9-bit
-// window; here the index is an 8-bit neighbour pattern).
+// SPCXLUT, coefficient_coder.cl:330-393).
 __device__ int zc_label(int orient, int h, int v, int d)
 {
     if (orient == 1) { const int t = h; h = v; v = t; }
@@ -90,21 +104,22 @@ __device__ void build_tables(Tables &t)
     for (int i = threadIdx.x; i < 47; i += blockDim.x)
         t.mq[i] = (uint32_t)c_qe[i] | ((uint32_t)c_nmps[i] << 16) | ((uint32_t)c_nlps[i] << 22) |
                   ((uint32_t)(i == 0 || i == 6 || i == 14) << 28);
-    // Pattern bits: 0-2 left column rows k-1..k+1, 3 centre row k-1,
-    // 4 centre row k+1, 5-7 right column rows k-1..k+1.
-    for (int i = threadIdx.x; i < 4 * 256; i += blockDim.x) {
-        const int o = i >> 8, p = i & 255;
-        const int h = ((p >> 1) & 1) + ((p >> 6) & 1);
-        const int v = ((p >> 3) & 1) + ((p >> 4) & 1);
-        const int d = (p & 1) + ((p >> 2) & 1) + ((p >> 5) & 1) + ((p >> 7) & 1);
+    // 3x3 neighbourhood bits: 0 up-left 1 up 2 up-right 3 left 4 self
+    // 5 right 6 down-left 7 down 8 down-right.
+    for (int i = threadIdx.x; i < 4 * 512; i += blockDim.x) {
+        const int o = i >> 9, p = i & 511;
+        const int h = ((p >> 3) & 1) + ((p >> 5) & 1);
+        const int v = ((p >> 1) & 1) + ((p >> 7) & 1);
+        const int d = (p & 1) + ((p >> 2) & 1) + ((p >> 6) & 1) + ((p >> 8) & 1);
         t.zc[o][p] = (uint8_t)zc_label(o, h, v, d);
     }
-    // Sign index bits: 0 sigL 1 sgnL 2 sigR 3 sgnR 4 sigU 5 sgnU 6 sigD 7 sgnD.
+    // Sign index: neighbourhood bits 1,3,5,7 (significance of up, left,
+    // right, down) with the neighbours' signs one bit below them.
     // ISO Tables D.2/D.3 (signcxlut, coefficient_coder.cl:406-435).
     for (int i = threadIdx.x; i < 256; i += blockDim.x) {
-        auto ctb = [&](int s, int n) { return s ? (n ? -1 : 1) : 0; };
-        int hc = ctb(i & 1, (i >> 1) & 1) + ctb((i >> 2) & 1, (i >> 3) & 1);
-        int vc = ctb((i >> 4) & 1, (i >> 5) & 1) + ctb((i >> 6) & 1, (i >> 7) & 1);
+        auto ctb = [&](int sig, int neg) { return sig ? (neg ? -1 : 1) : 0; };
+        int vc = ctb((i >> 1) & 1, i & 1) + ctb((i >> 7) & 1, (i >> 6) & 1);
+        int hc = ctb((i >> 3) & 1, (i >> 2) & 1) + ctb((i >> 5) & 1, (i >> 4) & 1);
         hc = hc > 1 ? 1 : (hc < -1 ? -1 : hc);
         vc = vc > 1 ? 1 : (vc < -1 ? -1 : vc);
         int cx, xr;
@@ -119,32 +134,26 @@ __device__ void build_tables(Tables &t)
     }
 }
 
-// MQ decoder (ISO C.3; bytein/renormd/mqDecode, coefficient_coder.cl:121-252).
+// MQ decoder (ISO C.3; bytein/renormd/mqDecode, coefficient_coder.cl:121-252),
+// with the byte after the current one loaded ahead of use.
 struct MQ {
     const uint8_t *p;
     int len, bp, ct;
-    uint32_t a, c;
+    uint32_t a, c, cur, nxt;
 
     __device__ __forceinline__ uint32_t byte_at(int i) const { return i < len ? (uint32_t)__ldg(p + i) : 0xFFu; }
     __device__ __forceinline__ void bytein()
     {
-        const uint32_t b = byte_at(bp);
-        if (b == 0xFF) {
-            const uint32_t b1 = byte_at(bp + 1);
-            if (b1 > 0x8F) {
-                c += 0xFF00;
-                ct = 8;
-            } else {
-                bp++;
-                c += b1 << 9;
-                ct = 7;
-            }
-        } else {
-            bp++;
-            c += byte_at(bp) << 8;
+        if (cur == 0xFF && nxt > 0x8F) {
+            c += 0xFF00;  // marker (or past the end): feed 1-bits, do not advance
             ct = 8;
+            return;
         }
-        // keep the codeword stream ahead of the decoder in L1
+        c += nxt << (cur == 0xFF ? 9 : 8);
+        ct = cur == 0xFF ? 7 : 8;
+        bp++;
+        cur = nxt;
+        nxt = byte_at(bp + 1);
         if ((bp & 63) == 0 && bp + 256 < len) asm volatile("prefetch.global.L1 [%0];" ::"l"(p + bp + 256));
     }
     __device__ __forceinline__ void init(const uint8_t *d, int n)
@@ -152,7 +161,9 @@ struct MQ {
         p = d;
         len = n;
         bp = 0;
-        c = byte_at(0) << 16;
+        cur = byte_at(0);
+        nxt = byte_at(1);
+        c = cur << 16;
         bytein();
         c <<= 7;
         ct -= 7;
@@ -161,14 +172,15 @@ struct MQ {
     __device__ __forceinline__ void renorm()
     {
         int sh = __clz(a) - 16;
-        while (sh > 0) {
-            if (ct == 0) bytein();
-            const int s = sh < ct ? sh : ct;
-            a <<= s;
-            c <<= s;
-            ct -= s;
-            sh -= s;
+        while (sh > ct) {
+            a <<= ct;
+            c <<= ct;
+            sh -= ct;
+            bytein();
         }
+        a <<= sh;
+        c <<= sh;
+        ct -= sh;
     }
     __device__ __forceinline__ int decode(uint32_t *ctx, const uint32_t *tbl, int cx)
     {
@@ -203,49 +215,48 @@ struct MQ {
     }
 };
 
-// Rows 4s-1 .. 4s+4 of a column word as a 6-bit window.
-__device__ __forceinline__ uint32_t win6(unsigned long long w, int s)
-{
-    return s == 0 ? (uint32_t)((w << 1) & 0x3Full) : (uint32_t)((w >> (4 * s - 1)) & 0x3Full);
-}
-
-__device__ __forceinline__ uint32_t zc_pattern(uint32_t wl, uint32_t wc, uint32_t wr, int k)
-{
-    const uint32_t cc = (wc >> k) & 5u;
-    return ((wl >> k) & 7u) | (((cc & 1u) | ((cc >> 1) & 2u)) << 3) | (((wr >> k) & 7u) << 5);
-}
-
-__device__ __forceinline__ uint32_t sc_index(uint32_t wl, uint32_t sl, uint32_t wc, uint32_t sc,
-                                             uint32_t wr, uint32_t sr, int k)
-{
-    return ((wl >> (k + 1)) & 1u) | (((sl >> (k + 1)) & 1u) << 1) | (((wr >> (k + 1)) & 1u) << 2) |
-           (((sr >> (k + 1)) & 1u) << 3) | (((wc >> k) & 1u) << 4) | (((sc >> k) & 1u) << 5) |
-           (((wc >> (k + 2)) & 1u) << 6) | (((sc >> (k + 2)) & 1u) << 7);
-}
-
-// Rows of a stripe in which a coefficient has at least one significant
-// neighbour (bit k = row 4s+k).
-__device__ __forceinline__ uint32_t nb_rows(uint32_t wl, uint32_t wc, uint32_t wr)
-{
-    const uint32_t n = wl | wr;
-    return ((n | (n >> 1) | (n >> 2)) | (wc | (wc >> 2))) & 0xFu;
-}
-
-// Lane-parallel candidate test for the significance pass: does column c
-// (window rows of stripe s) hold an insignificant coefficient with a
-// significant neighbour?
+// Sign-coding index of row y (= 4s+k) of column c from the flag word's
+// 3x3 neighbourhood n9 and the sign words of columns c-1, c, c+1.
 template <typename MagT>
-__device__ __forceinline__ bool spp_candidate(const WarpState<MagT> &S, int c, int s, uint32_t rmask)
+__device__ __forceinline__ uint32_t sign_index(const WarpState<MagT> &S, uint32_t n9, int c, int y)
 {
-    const uint32_t wl = win6(S.sig[c], s), wc = win6(S.sig[c + 1], s), wr = win6(S.sig[c + 2], s);
-    return (~(wc >> 1) & rmask & nb_rows(wl, wc, wr)) != 0u;
+    const unsigned long long sl = S.sgn[c], sc = S.sgn[c + 1], sr = S.sgn[c + 2];
+    const uint32_t up = y > 0 ? (uint32_t)(sc >> (y - 1)) & 1u : 0u;
+    const uint32_t dn = y < 63 ? (uint32_t)(sc >> (y + 1)) & 1u : 0u;
+    const uint32_t lf = (uint32_t)(sl >> y) & 1u, rt = (uint32_t)(sr >> y) & 1u;
+    return (n9 & 0xAAu) | up | (lf << 2) | (rt << 4) | (dn << 6);
+}
+
+// Record that row k of stripe s in column c became significant: the flag
+// words of the neighbouring columns and of the stripes above and below see
+// it through their neighbourhood bits.
+template <typename MagT>
+__device__ __forceinline__ void mark_significant(WarpState<MagT> &S, int s, int k, int c, int w, int nstripes,
+                                                 uint32_t neg)
+{
+    uint32_t *F = S.F;
+    const int i = s * 64 + c;
+    if (c > 0) F[i - 1] |= 1u << (3 * k + 5);
+    if (c + 1 < w) F[i + 1] |= 1u << (3 * k + 3);
+    if (k == 0 && s > 0) {
+        const int u = i - 64;
+        F[u] |= 1u << 16;
+        if (c > 0) F[u - 1] |= 1u << 17;
+        if (c + 1 < w) F[u + 1] |= 1u << 15;
+    }
+    if (k == 3 && s + 1 < nstripes) {
+        const int d = i + 64;
+        F[d] |= 1u << 1;
+        if (c > 0) F[d - 1] |= 1u << 2;
+        if (c + 1 < w) F[d + 1] |= 1u << 0;
+    }
+    if (neg) S.sgn[c + 1] |= 1ull << (4 * s + k);
 }
 
 // Decode one code-block.  Every lane of the warp runs this function in
-// lock-step (the MQ state is replicated, shared-memory accesses are
-// broadcasts); lanes split the per-stripe candidate searches between them
-// (lane l owns columns l and l+32) and the serial loop visits only the
-// candidate columns, in scan order.  Returns the last pass type (0 cleanup,
+// lock-step; lanes split the per-stripe candidate searches between them
+// (lane l owns columns l and l+32) and the serial loop visits only candidate
+// columns, in scan order.  Returns the last pass type (0 cleanup,
 // 1 significance propagation, 2 refinement) and its plane.
 template <typename MagT>
 __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *seg, int len, int w,
@@ -256,8 +267,8 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
     uint32_t *ctx = S.ctx;
     const uint32_t *tbl = T.mq;
     const uint8_t *zc = T.zc[orient];
+    uint32_t *F = S.F;
     const int nstripes = (h + 3) >> 2;
-    const int c0 = lane, c1 = lane + 32;
     int type = 0, pass = 0;
     *last_plane = numbps - 1;
 
@@ -267,69 +278,71 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
             // ---- significance propagation pass (ISO D.3.1; SigPropPassFunctor) ----
             for (int s = 0; s < nstripes; s++) {
                 const int rows = min(4, h - 4 * s);
-                const uint32_t rmask = (1u << rows) - 1u;
                 __syncwarp();
-                const bool a0 = c0 < w && spp_candidate(S, c0, s, rmask);
-                const bool a1 = c1 < w && spp_candidate(S, c1, s, rmask);
-                unsigned long long cand = (unsigned long long)__ballot_sync(0xffffffffu, a0) |
-                                          ((unsigned long long)__ballot_sync(0xffffffffu, a1) << 32);
+                bool any[2];
+#pragma unroll
+                for (int j = 0; j < 2; j++) {
+                    const int c = lane + 32 * j;
+                    bool a = false;
+                    if (c < w) {
+                        const uint32_t f = F[s * 64 + c];
+                        for (int k = 0; k < rows; k++)
+                            a |= !(f & self_bit(k)) && ((f >> (3 * k)) & 0x1EFu);
+                    }
+                    any[j] = a;
+                }
+                unsigned long long cand = (unsigned long long)__ballot_sync(0xffffffffu, any[0]) |
+                                          ((unsigned long long)__ballot_sync(0xffffffffu, any[1]) << 32);
                 while (cand) {
                     const int c = __ffsll((long long)cand) - 1;
                     cand &= cand - 1;
-                    const uint32_t wl = win6(S.sig[c], s), wr = win6(S.sig[c + 2], s);
-                    uint32_t wc = win6(S.sig[c + 1], s);
-                    const uint32_t wc0 = wc;
-                    uint32_t sc = win6(S.sgn[c + 1], s);
-                    uint32_t vmask = 0;
+                    uint32_t f = F[s * 64 + c];
+                    const uint32_t f0 = f;
                     for (int k = 0; k < rows; k++) {
-                        if ((wc >> (k + 1)) & 1u) continue;
-                        const uint32_t pat = zc_pattern(wl, wc, wr, k);
-                        if (!pat) continue;
-                        vmask |= 1u << k;
-                        if (mq.decode(ctx, tbl, zc[pat])) {
-                            const uint32_t sl = win6(S.sgn[c], s), sr = win6(S.sgn[c + 2], s);
-                            const uint32_t si = T.sc[sc_index(wl, sl, wc, sc, wr, sr, k)];
+                        if (f & self_bit(k)) continue;
+                        const uint32_t n9 = (f >> (3 * k)) & 0x1FFu;
+                        if (!(n9 & 0x1EFu)) continue;
+                        f |= pi_bit(k);
+                        if (mq.decode(ctx, tbl, zc[n9])) {
+                            const int y = 4 * s + k;
+                            const uint32_t si = T.sc[sign_index(S, n9, c, y)];
                             const uint32_t neg = (uint32_t)mq.decode(ctx, tbl, si & 15) ^ (si >> 4);
-                            wc |= 2u << k;
-                            sc |= neg << (k + 1);
-                            S.mag[(4 * s + k) * 64 + c] = pbit;
+                            f |= self_bit(k);
+                            mark_significant(S, s, k, c, w, nstripes, neg);
+                            S.mag[y * 64 + c] = pbit;
+                            if (c + 1 < w) cand |= 1ull << (c + 1);  // the next column gained a neighbour
                         }
                     }
-                    if (wc != wc0) {
-                        S.sig[c + 1] |= (unsigned long long)((wc >> 1) & 0xFu) << (4 * s);
-                        S.sgn[c + 1] |= (unsigned long long)((sc >> 1) & 0xFu) << (4 * s);
-                        if (c + 1 < w) cand |= 1ull << (c + 1);  // the next column gained a neighbour
-                    }
-                    if (vmask) S.vis[c + 1] |= (unsigned long long)vmask << (4 * s);
+                    if (f != f0) F[s * 64 + c] = f;
                 }
             }
             type = 1;
             *last_plane = p;
             if (++pass >= passes) break;
-            __syncwarp();
 
             // ---- magnitude refinement pass (ISO D.3.3; MagRefPassFunctor) ----
-            // The rows to refine and their contexts do not change during the
-            // pass, so the lanes precompute them for their columns.
+            // Rows to refine and their contexts do not change during the pass:
+            // the lanes precompute them for their columns.
             for (int s = 0; s < nstripes; s++) {
                 const int rows = min(4, h - 4 * s);
-                const uint32_t rmask = (1u << rows) - 1u;
+                __syncwarp();
                 bool any[2];
 #pragma unroll
                 for (int j = 0; j < 2; j++) {
                     const int c = lane + 32 * j;
                     uint32_t rr = 0, codes = 0;
                     if (c < w) {
-                        const uint32_t wl = win6(S.sig[c], s), wc = win6(S.sig[c + 1], s),
-                                       wr = win6(S.sig[c + 2], s);
-                        const uint32_t vis = (uint32_t)(S.vis[c + 1] >> (4 * s)) & 0xFu;
-                        const uint32_t ref = (uint32_t)(S.ref[c + 1] >> (4 * s)) & 0xFu;
-                        rr = (wc >> 1) & rmask & ~vis;
-                        for (int k = 0; k < 4; k++)
-                            codes |= (((ref >> k) & 1u) ? 2u : (zc_pattern(wl, wc, wr, k) ? 1u : 0u)) << (2 * k);
+                        const uint32_t f = F[s * 64 + c];
+                        for (int k = 0; k < rows; k++) {
+                            if ((f & self_bit(k)) && !(f & pi_bit(k))) {
+                                rr |= 1u << k;
+                                const uint32_t code = (f & ref_bit(k)) ? 2u : (((f >> (3 * k)) & 0x1EFu) ? 1u : 0u);
+                                codes |= code << (2 * k);
+                            }
+                        }
                         S.mrow[c] = (uint8_t)rr;
                         S.mctx[c] = (uint8_t)codes;
-                        S.ref[c + 1] |= (unsigned long long)rr << (4 * s);
+                        if (rr) F[s * 64 + c] = f | (rr << 22);
                     }
                     any[j] = rr != 0;
                 }
@@ -347,7 +360,6 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
                         if (mq.decode(ctx, tbl, 14 + ((codes >> (2 * k)) & 3u))) S.mag[(4 * s + k) * 64 + c] |= pbit;
                     }
                 }
-                __syncwarp();
             }
             type = 2;
             if (++pass >= passes) break;
@@ -362,55 +374,57 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
 #pragma unroll
             for (int j = 0; j < 2; j++) {
                 const int c = lane + 32 * j;
-                any[j] = c < w && ((~(uint32_t)((S.sig[c + 1] | S.vis[c + 1]) >> (4 * s))) & rmask) != 0u;
+                bool a = false;
+                if (c < w) {
+                    const uint32_t f = F[s * 64 + c];
+                    uint32_t done = (f >> 18) & 0xFu;  // pi
+#pragma unroll
+                    for (int k = 0; k < 4; k++) done |= ((f >> (3 * k + 4)) & 1u) << k;
+                    a = (~done & rmask) != 0u;
+                }
+                any[j] = a;
             }
             unsigned long long cand = (unsigned long long)__ballot_sync(0xffffffffu, any[0]) |
                                       ((unsigned long long)__ballot_sync(0xffffffffu, any[1]) << 32);
             while (cand) {
                 const int c = __ffsll((long long)cand) - 1;
                 cand &= cand - 1;
-                const uint32_t wl = win6(S.sig[c], s), wr = win6(S.sig[c + 2], s);
-                uint32_t wc = win6(S.sig[c + 1], s);
-                const uint32_t wc0 = wc;
-                const uint32_t vis = (uint32_t)(S.vis[c + 1] >> (4 * s)) & 0xFu;
-                uint32_t sc = win6(S.sgn[c + 1], s);
+                uint32_t f = F[s * 64 + c];
+                const uint32_t f0 = f;
                 int k = 0;
-                if (rows == 4 && (wl | wc | wr) == 0u) {
+                if (rows == 4 && (f & kSigMask) == 0u) {
                     // run-length mode: four rows with an all-zero neighbourhood
                     if (!mq.decode(ctx, tbl, 18)) continue;
                     int r = mq.decode(ctx, tbl, 17) << 1;
                     r |= mq.decode(ctx, tbl, 17);
-                    const uint32_t sl = win6(S.sgn[c], s), sr = win6(S.sgn[c + 2], s);
-                    const uint32_t si = T.sc[sc_index(wl, sl, wc, sc, wr, sr, r)];
+                    const int y = 4 * s + r;
+                    const uint32_t si = T.sc[sign_index(S, (f >> (3 * r)) & 0x1FFu, c, y)];
                     const uint32_t neg = (uint32_t)mq.decode(ctx, tbl, si & 15) ^ (si >> 4);
-                    wc |= 2u << r;
-                    sc |= neg << (r + 1);
-                    S.mag[(4 * s + r) * 64 + c] = pbit;
+                    f |= self_bit(r);
+                    mark_significant(S, s, r, c, w, nstripes, neg);
+                    S.mag[y * 64 + c] = pbit;
                     k = r + 1;
                 }
                 for (; k < rows; k++) {
-                    if (((wc >> (k + 1)) | (vis >> k)) & 1u) continue;
-                    if (mq.decode(ctx, tbl, zc[zc_pattern(wl, wc, wr, k)])) {
-                        const uint32_t sl = win6(S.sgn[c], s), sr = win6(S.sgn[c + 2], s);
-                        const uint32_t si = T.sc[sc_index(wl, sl, wc, sc, wr, sr, k)];
+                    if (f & (self_bit(k) | pi_bit(k))) continue;
+                    const uint32_t n9 = (f >> (3 * k)) & 0x1FFu;
+                    if (mq.decode(ctx, tbl, zc[n9])) {
+                        const int y = 4 * s + k;
+                        const uint32_t si = T.sc[sign_index(S, n9, c, y)];
                         const uint32_t neg = (uint32_t)mq.decode(ctx, tbl, si & 15) ^ (si >> 4);
-                        wc |= 2u << k;
-                        sc |= neg << (k + 1);
-                        S.mag[(4 * s + k) * 64 + c] = pbit;
+                        f |= self_bit(k);
+                        mark_significant(S, s, k, c, w, nstripes, neg);
+                        S.mag[y * 64 + c] = pbit;
                     }
                 }
-                if (wc != wc0) {
-                    S.sig[c + 1] |= (unsigned long long)((wc >> 1) & 0xFu) << (4 * s);
-                    S.sgn[c + 1] |= (unsigned long long)((sc >> 1) & 0xFu) << (4 * s);
-                }
+                if (f != f0) F[s * 64 + c] = f;
             }
         }
         type = 0;
         *last_plane = p;
         if (++pass >= passes) break;
         __syncwarp();
-        for (int c = lane; c < kCols; c += 32) S.vis[c] = 0ull;
-        __syncwarp();
+        for (int i = lane; i < nstripes * 64; i += 32) F[i] &= ~0x3C0000u;  // clear pi
     }
     return type;
 }
@@ -457,14 +471,11 @@ t1_decode_kernel(const tc_cblk_desc *__restrict__ desc, const uint32_t *__restri
             ok = false;
         }
         const bool coded = ok && numbps > 0 && d.passes > 0;
+        const int nstripes = (h + 3) >> 2;
 
-        // clear the column state words (all lanes)
-        for (int i = lane; i < kCols; i += 32) {
-            S.sig[i] = 0ull;
-            S.sgn[i] = 0ull;
-            S.ref[i] = 0ull;
-            S.vis[i] = 0ull;
-        }
+        // clear the state (all lanes)
+        for (int i = lane; i < nstripes * 64; i += 32) S.F[i] = 0u;
+        for (int i = lane; i < kSgnCols; i += 32) S.sgn[i] = 0ull;
         if (lane < 19) {
             const int st = lane == 0 ? 4 : (lane == 17 ? 46 : (lane == 18 ? 3 : 0));
             S.ctx[lane] = T.mq[st];
@@ -479,27 +490,28 @@ t1_decode_kernel(const tc_cblk_desc *__restrict__ desc, const uint32_t *__restri
 
         // epilogue: reconstruction + inverse quantisation, coalesced rows
         const bool irrev = (d.flags & TC_CBLK_IRREVERSIBLE) != 0;
-        const float half_step = recon_r;
         for (int y = 0; y < h; y++) {
             char *row = out + 4 * (d.out_off + (uint64_t)y * d.out_pitch);
+            const int s = y >> 2, k = y & 3;
             for (int x = lane; x < w; x += 32) {
-                const bool sg = coded && ((S.sig[x + 1] >> y) & 1ull);
+                const uint32_t f = coded ? S.F[s * 64 + x] : 0u;
+                const bool sg = (f & self_bit(k)) != 0u;
                 uint32_t mg = 0, neg = 0, u = 0;
                 if (sg) {
                     mg = (uint32_t)S.mag[y * 64 + x];
                     neg = (uint32_t)(S.sgn[x + 1] >> y) & 1u;
                     u = (uint32_t)last_plane;
-                    if (type == 1 && !((S.vis[x + 1] >> y) & 1ull)) u++;
+                    if (type == 1 && !(f & pi_bit(k))) u++;
                 }
                 if (out_mode == TC_T1_OUT_RAW) {
                     reinterpret_cast<uint32_t *>(row)[x] = sg ? ((mg << (31 - d.mb)) | (neg << 31)) : 0u;
                 } else if (irrev) {
                     float v = 0.0f;
-                    if (sg) v = ((float)mg + half_step * (float)(1u << u)) * d.step;
+                    if (sg) v = ((float)mg + recon_r * (float)(1u << u)) * d.step;
                     reinterpret_cast<float *>(row)[x] = neg ? -v : v;
                 } else {
                     int32_t v = 0;
-                    if (sg) v = (int32_t)mg + (u ? (int32_t)floorf(half_step * (float)(1u << u)) : 0);
+                    if (sg) v = (int32_t)mg + (u ? (int32_t)floorf(recon_r * (float)(1u << u)) : 0);
                     reinterpret_cast<int32_t *>(row)[x] = neg ? -v : v;
                 }
             }
@@ -544,32 +556,40 @@ __global__ void dequant_raw_kernel(const tc_cblk_desc *__restrict__ desc, int n,
     }
 }
 
-}  // namespace
+struct LaunchCfg {
+    bool ready = false;
+    int per_sm = 1;
+    size_t smem = 0;
+};
 
-namespace {
 template <typename MagT>
-cudaError_t launch_class(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint32_t *d_order, int n, int ndesc,
-                         const uint8_t *d_pool, uint64_t pool_len, void *d_out, int out_mode, float recon_r,
-                         int slot)
+cudaError_t launch_class(tc_ctx *ctx, cudaStream_t stream, const tc_cblk_desc *d_desc, const uint32_t *d_order,
+                         int n, int ndesc, const uint8_t *d_pool, uint64_t pool_len, void *d_out, int out_mode,
+                         float recon_r, int slot)
 {
-    const size_t smem = ((sizeof(Tables) + 15) & ~size_t(15)) + kWarps * sizeof(WarpState<MagT>);
-    cudaError_t e = cudaFuncSetAttribute(t1_decode_kernel<MagT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
-    if (e != cudaSuccess) return e;
-    int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, t1_decode_kernel<MagT>, 32 * kWarps, smem);
-    if (e != cudaSuccess) return e;
-    if (per_sm < 1) per_sm = 1;
+    static LaunchCfg cfg[64];
+    LaunchCfg &C = cfg[ctx->device & 63];
+    if (!C.ready) {
+        C.smem = ((sizeof(Tables) + 15) & ~size_t(15)) + kWarps * sizeof(WarpState<MagT>);
+        cudaError_t e = cudaFuncSetAttribute(t1_decode_kernel<MagT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)C.smem);
+        if (e != cudaSuccess) return e;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&C.per_sm, t1_decode_kernel<MagT>, 32 * kWarps, C.smem);
+        if (e != cudaSuccess) return e;
+        if (C.per_sm < 1) C.per_sm = 1;
+        C.ready = true;
+    }
     const int want = (n + kWarps - 1) / kWarps;
-    const int grid = std::min(want, per_sm * num_sms(ctx->device));
-    e = cudaMemsetAsync(ctx->d_words + slot, 0, sizeof(uint32_t), ctx->stream);
+    const int grid = std::min(want, C.per_sm * num_sms(ctx->device));
+    cudaError_t e = cudaMemsetAsync(ctx->d_words + slot, 0, sizeof(uint32_t), stream);
     if (e != cudaSuccess) return e;
-    t1_decode_kernel<MagT><<<grid, 32 * kWarps, smem, ctx->stream>>>(
-        d_desc, d_order, n, ndesc, d_pool, pool_len, static_cast<char *>(d_out), out_mode, recon_r,
-        ctx->d_words + slot, ctx->d_words);
+    t1_decode_kernel<MagT><<<grid, 32 * kWarps, C.smem, stream>>>(d_desc, d_order, n, ndesc, d_pool, pool_len,
+                                                                   static_cast<char *>(d_out), out_mode, recon_r,
+                                                                   ctx->d_words + slot, ctx->d_words);
     ctx->launches++;
     return cudaGetLastError();
 }
+
 }  // namespace
 
 cudaError_t launch_t1_decode(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint32_t *d_order, int n,
@@ -585,15 +605,37 @@ cudaError_t launch_t1_classes(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uin
                               int n8, int n16, int n32, const uint8_t *d_pool, uint64_t pool_len, void *d_out,
                               int out_mode, float recon_r)
 {
-    cudaError_t e = cudaSuccess;
-    if (n8 > 0)
-        e = launch_class<uint8_t>(ctx, d_desc, d_order, n8, ndesc, d_pool, pool_len, d_out, out_mode, recon_r, 1);
-    if (e == cudaSuccess && n16 > 0)
-        e = launch_class<uint16_t>(ctx, d_desc, d_order ? d_order + n8 : nullptr, n16, ndesc, d_pool, pool_len,
-                                   d_out, out_mode, recon_r, 2);
-    if (e == cudaSuccess && n32 > 0)
-        e = launch_class<uint32_t>(ctx, d_desc, d_order ? d_order + n8 + n16 : nullptr, n32, ndesc, d_pool,
+    const int nclass = (n8 > 0) + (n16 > 0) + (n32 > 0);
+    if (nclass == 0) return cudaSuccess;
+    cudaStream_t s8 = ctx->stream, s16 = ctx->stream, s32 = ctx->stream;
+    cudaError_t e;
+    if (nclass > 1) {
+        // Fork: the heavier classes run on side streams, concurrently with
+        // the 8-bit class on the context's stream, and are joined after it.
+        if ((e = ensure_side_streams(ctx)) != cudaSuccess) return e;
+        if ((e = cudaEventRecord(ctx->ev_fork, ctx->stream)) != cudaSuccess) return e;
+        for (int i = 0; i < 2; i++)
+            if ((e = cudaStreamWaitEvent(ctx->side[i], ctx->ev_fork, 0)) != cudaSuccess) return e;
+        s32 = ctx->side[0];
+        s16 = ctx->side[1];
+    }
+    e = cudaSuccess;
+    if (n32 > 0)
+        e = launch_class<uint32_t>(ctx, s32, d_desc, d_order ? d_order + n8 + n16 : nullptr, n32, ndesc, d_pool,
                                    pool_len, d_out, out_mode, recon_r, 3);
+    if (e == cudaSuccess && n16 > 0)
+        e = launch_class<uint16_t>(ctx, s16, d_desc, d_order ? d_order + n8 : nullptr, n16, ndesc, d_pool,
+                                   pool_len, d_out, out_mode, recon_r, 2);
+    if (e == cudaSuccess && n8 > 0)
+        e = launch_class<uint8_t>(ctx, s8, d_desc, d_order, n8, ndesc, d_pool, pool_len, d_out, out_mode, recon_r,
+                                  1);
+    if (nclass > 1) {
+        for (int i = 0; i < 2; i++) {
+            cudaError_t e2 = cudaEventRecord(ctx->ev_join[i], ctx->side[i]);
+            if (e2 == cudaSuccess) e2 = cudaStreamWaitEvent(ctx->stream, ctx->ev_join[i], 0);
+            if (e == cudaSuccess) e = e2;
+        }
+    }
     return e;
 }
 

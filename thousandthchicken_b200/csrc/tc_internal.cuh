@@ -32,10 +32,15 @@ struct tc_ctx {
     tc::DevBuf scratch;           // DWT intermediate levels
     tc::DevBuf tmp_pool, tmp_desc, tmp_order, tmp_coef, tmp_out;
     uint64_t launches = 0;
+    // side streams for concurrent Tier-1 class launches (created on first use)
+    cudaStream_t side[2] = {nullptr, nullptr};
+    cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
 };
 
 namespace tc {
 
+// Creates the context's side streams and fork/join events if needed.
+cudaError_t ensure_side_streams(tc_ctx *ctx);
 // Records a message on the context and returns the status.
 int fail(tc_ctx *ctx, int status, const std::string &msg);
 // Maps a CUDA error to TC_E_DEVICE with its message (TC_OK on cudaSuccess).
