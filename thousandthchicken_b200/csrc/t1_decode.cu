@@ -75,7 +75,7 @@ struct WarpState {
 };
 
 struct Tables {
-    uint32_t mq[48];          // packed states: Qe | NMPS << 16 | NLPS << 22 | SWITCH << 28
+    uint32_t mq[48];          // packed states: Qe << 16 | NMPS << 1 | NLPS << 7 | SWITCH << 13 (bit 0: MPS)
     uint8_t zc[4][512];       // zero-coding label per orientation and 3x3 neighbourhood
     uint8_t sc[256];          // sign label | XOR bit << 4
 };
@@ -102,8 +102,8 @@ __device__ int zc_label(int orient, int h, int v, int d)
 __device__ void build_tables(Tables &t)
 {
     for (int i = threadIdx.x; i < 47; i += blockDim.x)
-        t.mq[i] = (uint32_t)c_qe[i] | ((uint32_t)c_nmps[i] << 16) | ((uint32_t)c_nlps[i] << 22) |
-                  ((uint32_t)(i == 0 || i == 6 || i == 14) << 28);
+        t.mq[i] = ((uint32_t)c_qe[i] << 16) | ((uint32_t)c_nmps[i] << 1) | ((uint32_t)c_nlps[i] << 7) |
+                  ((uint32_t)(i == 0 || i == 6 || i == 14) << 13);
     // 3x3 neighbourhood bits: 0 up-left 1 up 2 up-right 3 left 4 self
     // 5 right 6 down-left 7 down 8 down-right.
     for (int i = threadIdx.x; i < 4 * 512; i += blockDim.x) {
@@ -134,8 +134,13 @@ __device__ void build_tables(Tables &t)
     }
 }
 
-// MQ decoder (ISO C.3; bytein/renormd/mqDecode, coefficient_coder.cl:121-252),
-// with the byte after the current one loaded ahead of use.
+// MQ decoder (ISO C.3; bytein/renormd/mqDecode, coefficient_coder.cl:121-252).
+// The interval register A is kept scaled by 2^16 so that it lives in the same
+// bit positions as C's upper half: the Qe comparison against C, the
+// "A < 0x8000" test (sign bit of the scaled A) and the renormalisation shift
+// (count of leading zeros) need no extra shifts.  Each context word holds
+// Qe << 16 plus its transition indices and MPS.  The byte after the current
+// one is loaded ahead of use.
 struct MQ {
     const uint8_t *p;
     int len, bp, ct;
@@ -144,13 +149,18 @@ struct MQ {
     __device__ __forceinline__ uint32_t byte_at(int i) const { return i < len ? (uint32_t)__ldg(p + i) : 0xFFu; }
     __device__ __forceinline__ void bytein()
     {
-        if (cur == 0xFF && nxt > 0x8F) {
-            c += 0xFF00;  // marker (or past the end): feed 1-bits, do not advance
+        if (cur == 0xFF) {
+            if (nxt > 0x8F) {
+                c += 0xFF00;  // marker (or past the end): feed 1-bits, do not advance
+                ct = 8;
+                return;
+            }
+            c += nxt << 9;
+            ct = 7;
+        } else {
+            c += nxt << 8;
             ct = 8;
-            return;
         }
-        c += nxt << (cur == 0xFF ? 9 : 8);
-        ct = cur == 0xFF ? 7 : 8;
         bp++;
         cur = nxt;
         nxt = byte_at(bp + 1);
@@ -167,11 +177,11 @@ struct MQ {
         bytein();
         c <<= 7;
         ct -= 7;
-        a = 0x8000;
+        a = 0x80000000u;
     }
     __device__ __forceinline__ void renorm()
     {
-        int sh = __clz(a) - 16;
+        int sh = __clz(a);
         while (sh > ct) {
             a <<= ct;
             c <<= ct;
@@ -182,36 +192,38 @@ struct MQ {
         c <<= sh;
         ct -= sh;
     }
-    __device__ __forceinline__ int decode(uint32_t *ctx, const uint32_t *tbl, int cx)
+    __device__ __forceinline__ uint32_t decode(uint32_t *ctx, const uint32_t *tbl, int cx)
     {
         const uint32_t w = ctx[cx];
-        const uint32_t qe = w & 0xFFFF, mps = w >> 31;
-        a -= qe;
-        if ((c >> 16) < qe) {
+        const uint32_t qs = w & 0xFFFF0000u, mps = w & 1u;
+        a -= qs;
+        if (c < qs) {
+            // LPS_EXCHANGE
             uint32_t d;
-            if (a < qe) {
+            if (a < qs) {
                 d = mps;
-                ctx[cx] = tbl[(w >> 16) & 63] | (mps << 31);
+                ctx[cx] = tbl[(w >> 1) & 63] | mps;
             } else {
-                d = mps ^ 1;
-                ctx[cx] = tbl[(w >> 22) & 63] | ((mps ^ ((w >> 28) & 1)) << 31);
+                d = mps ^ 1u;
+                ctx[cx] = tbl[(w >> 7) & 63] | (mps ^ ((w >> 13) & 1u));
             }
-            a = qe;
+            a = qs;
             renorm();
-            return (int)d;
+            return d;
         }
-        c -= qe << 16;
-        if (a & 0x8000) return (int)mps;
+        c -= qs;
+        if ((int)a < 0) return mps;
+        // MPS_EXCHANGE
         uint32_t d;
-        if (a < qe) {
-            d = mps ^ 1;
-            ctx[cx] = tbl[(w >> 22) & 63] | ((mps ^ ((w >> 28) & 1)) << 31);
+        if (a < qs) {
+            d = mps ^ 1u;
+            ctx[cx] = tbl[(w >> 7) & 63] | (mps ^ ((w >> 13) & 1u));
         } else {
             d = mps;
-            ctx[cx] = tbl[(w >> 16) & 63] | (mps << 31);
+            ctx[cx] = tbl[(w >> 1) & 63] | mps;
         }
         renorm();
-        return (int)d;
+        return d;
     }
 };
 
