@@ -152,6 +152,26 @@ int tc_dwt_reverse53(tc_ctx *ctx, const int32_t *d_in, int in_pitch,
 int tc_dwt_reverse97(tc_ctx *ctx, const float *d_in, int in_pitch,
                      float *d_out, int out_pitch, int w, int h, int levels);
 
+/* Allocation-free reverse 9/7 for callers that cannot allocate device
+ * memory (code under stream capture that must not allocate, hosts whose
+ * memory manager owns every device allocation, real-time paths that cannot
+ * afford cudaMalloc/cudaFree).  No counterpart in the reference: its DWT
+ * allocates and zero-fills a fresh output on every call (DWT.cpp:79-84).
+ * Same transform and result as tc_dwt_reverse97, but it takes a CUDA stream
+ * instead of a context, and the intermediate plane lives in a file-scope
+ * device array of TC_DWT97_STATIC_SCRATCH_ELEMS floats (16 MiB) that every
+ * GPU loading this library holds until exit.  Returns TC_E_ARG when
+ * ceil(w/2) * ceil(h/2) exceeds that size (levels >= 2).  It calls no
+ * cudaMalloc, cudaFree or allocating library routine.  Its first call on a
+ * device looks up the array's address there (cudaGetSymbolAddress with that
+ * device current); make that first call before any stream capture.  Calls
+ * share the array: calls whose work overlaps on the GPU race on it.  The
+ * array keeps the last call's contents and nothing in it needs to start at
+ * zero. */
+#define TC_DWT97_STATIC_SCRATCH_ELEMS (4u * 1024u * 1024u)
+int tc_dwt_reverse97_static(const float *d_in, int in_pitch, float *d_out, int out_pitch,
+                            int w, int h, int levels, void *cuda_stream);
+
 /* ---- colour transform + DC level shift (Preprocessor) -------------------- */
 
 #define TC_COLOR_DC  0  /* DC level shift only, per component */

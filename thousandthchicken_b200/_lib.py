@@ -91,6 +91,7 @@ _PROTOS = {
     "tc_dwt_forward97": (_I, [_VP, _VP, _I, _VP, _I, _I, _I, _I]),
     "tc_dwt_reverse53": (_I, [_VP, _VP, _I, _VP, _I, _I, _I, _I, _I]),
     "tc_dwt_reverse97": (_I, [_VP, _VP, _I, _VP, _I, _I, _I, _I]),
+    "tc_dwt_reverse97_static": (_I, [_VP, _I, _VP, _I, _I, _I, _I, _VP]),
     "tc_color_inverse": (_I, [_VP, _I, _I, _VP, _I, _I, _VP, _I, _I, _I, _I, _I]),
     "tc_color_forward": (_I, [_VP, _I, _I, _VP, _I, _I, _VP, _I, _I, _I, _I, _I]),
     "tc_j2k_read_header": (_I, [_VP, C.c_size_t, C.POINTER(ImageInfo)]),
