@@ -83,6 +83,39 @@ def make_mixed(n=None, seed=None):
     return out
 
 
+def serve_section(args, mixed, device):
+    """Served decode: requests drawn from the mixed batch plus 20% 16-bit
+    2048x2048 lossless images (radial field + N(0, 40^2) noise) arrive as a
+    Poisson process; the continuous-batching server (budget 40 GB) is
+    compared with the per-image path (one request per batch, one in flight)
+    on the same arrivals."""
+    from thousandthchicken_b200 import codec
+    from thousandthchicken_b200.serve import Request, Server, latency_stats, poisson_arrivals
+    from thousandthchicken_b200.synth import radial_noise_image
+    rng = np.random.default_rng(5)
+    radial = [codec.encode(radial_noise_image(2048, 2048, 16, seed=50 + i), 16, levels=5, reversible=True,
+                           mct=False) for i in range(2)]
+    pool = [(cs_, im.shape[1] * im.shape[2]) for im, cs_ in mixed]
+    pool_r = [(cs_, 2048 * 2048) for cs_ in radial]
+    arr = poisson_arrivals(args.serve_requests, args.serve_rate, seed=9)
+    picks = [pool_r[rng.integers(len(pool_r))] if rng.random() < 0.2 else pool[rng.integers(len(pool))]
+             for _ in arr]
+    mpx = sum(px for _, px in picks) / 1e6
+    out = {"requests": len(picks), "rate_per_s": args.serve_rate, "mpixels": round(mpx, 3),
+           "budget_bytes": 40 << 30}
+    for name, kw in (("continuous_batching", dict(max_batch=16, inflight=2)),
+                     ("per_image", dict(max_batch=1, inflight=1))):
+        srv = Server(device, budget_bytes=40 << 30, **kw)
+        srv.run([Request(i, cs_, 0.0) for i, (cs_, _) in enumerate(picks[:4])], realtime=False)  # warm-up
+        reqs = [Request(i, cs_, float(a)) for i, ((cs_, _), a) in enumerate(zip(picks, arr))]
+        done, wall = srv.run(reqs, realtime=True)
+        srv.close()
+        st = latency_stats(done)
+        out[name] = {"mpix_s": round(mpx / wall, 2), "wall_s": round(wall, 3),
+                     "p50_ms": round(st["p50_ms"], 3), "p99_ms": round(st["p99_ms"], 3)}
+    return out
+
+
 def measured_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -313,6 +346,7 @@ def run_ours(args, rank, world, local_rank):
     mpx_mixed = sum(im.shape[1] * im.shape[2] for im, _ in mixed) / 1e6
     bplan = Plan(ctx, streams)
     bouts = bplan.alloc_outputs()
+    bplan.set_graph(True)   # the batched path replays one captured graph per shape bucket
     pplans = [Plan(ctx, [s_]) for s_ in streams]
     pouts = [p_.alloc_outputs() for p_ in pplans]
     mixed_steps = max(3, min(args.steps, 10))
@@ -373,6 +407,9 @@ def run_ours(args, rank, world, local_rank):
     for p_ in pplans:
         p_.close()
 
+    # served decode: Poisson arrivals, continuous batching vs the per-image path
+    served = serve_section(args, mixed, local_rank)
+
     if rank == 0:
         px = W * H
         value = px * args.steps * world / (total_ms / 1000.0) / 1e6
@@ -412,6 +449,7 @@ def run_ours(args, rank, world, local_rank):
                     "h2d_bytes_per_step": pool_bytes + 40 * ncblk + 4 * ncblk,
                     "d2h_bytes_per_step": int(host_out.nbytes), "api": "tc_decode_j2k"},
             "batched_vs_per_image": batched,
+            "served": served,
             "gpu_launches": int(launches), "clocks": clocks, "psnr_db": round(psnr, 2),
             "wall_s_timed_region": round(wall, 3),
         }
@@ -432,6 +470,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-rate", type=float, default=200.0, help="served decode: Poisson arrivals per second")
+    ap.add_argument("--serve-requests", type=int, default=64)
     ap.add_argument("--size", type=int, default=0,
                     help="square image side for a smaller case of the same workload (profiling)")
     args = ap.parse_args()

@@ -65,6 +65,12 @@ const char *tc_status_string(int status);
 int tc_version(void);
 /* Number of kernel launches this ctx issued since creation (diagnostics). */
 uint64_t tc_ctx_launch_count(const tc_ctx *ctx);
+/* Lanes per code-block in the Tier-1 kernel: 32 (one warp per block), 16 or
+ * 8 (two or four blocks per warp, decoded in lock-step).  The best width
+ * depends on the block mix; the package's autotuner measures it per workload
+ * and caches the choice.  Default 32. */
+int tc_ctx_set_t1_group(tc_ctx *ctx, int lanes);
+int tc_ctx_t1_group(const tc_ctx *ctx);
 
 /* ---- Tier-1 code-block decode (CoefficientCoder) ------------------------- */
 
@@ -259,12 +265,23 @@ typedef struct tc_plan tc_plan;
 int tc_plan_create(tc_ctx *ctx, const uint8_t *const *h_cs, const size_t *lens,
                    int nimages, tc_plan **out);
 int tc_plan_destroy(tc_plan *plan);
+/* Re-parse a plan for new codestreams, reusing its device buffers (they only
+ * grow): a serving loop keeps its coefficient, scratch and pool buffers
+ * resident across batches.  Waits for the plan's previous execute. */
+int tc_plan_rebuild(tc_plan *plan, const uint8_t *const *h_cs, const size_t *lens,
+                    int nimages);
 /* Bytes of output for image i (planar, sample type as tc_decode_j2k). */
 int tc_plan_output_bytes(const tc_plan *plan, int image, size_t *bytes);
 int tc_plan_image_info(const tc_plan *plan, int image, tc_image_info *info);
 /* Run the decode of every image in the plan; image i goes to d_out[i]
  * (device memory of tc_plan_output_bytes bytes).  Stream-ordered. */
 int tc_plan_execute(tc_plan *plan, void *const *d_out);
+/* Replay execute as a CUDA graph (on = 1): the first execute with a given
+ * set of outputs runs normally and then captures the same work (Tier-1 class
+ * launches with their fork/join, counter resets and every DWT level) into a
+ * graph; later executes with the same outputs launch the graph.  Other
+ * outputs, tc_plan_rebuild or profiling drop or bypass it. */
+int tc_plan_set_graph(tc_plan *plan, int on);
 /* Record CUDA events around the stages of every execute (on = 1): the
  * Tier-1 launch and the DWT/colour launches.  tc_plan_stage_ms waits for the
  * last execute and returns the device time of each stage in milliseconds.

@@ -87,3 +87,40 @@ def test_decode_file_and_errors(gpu_ctx, tmp_path):
     with pytest.raises(TCError):
         _decoder(gpu_ctx).decode(cs[: len(cs) // 3])
     np.testing.assert_array_equal(_decoder(gpu_ctx).decode(cs), img)
+
+
+def test_graph_replay_and_autotune(gpu_ctx):
+    from thousandthchicken_b200 import _lib as L
+    from thousandthchicken_b200.autotune import tune_plan
+    from thousandthchicken_b200.stages import Plan
+    streams = [codec.encode(synth_image(300, 200, 3, 8, 5), 8, levels=5, reversible=True),
+               codec.encode(synth_image(200, 180, 3, 8, 6), 8, levels=4, reversible=False, base_step=1 / 64)]
+    plan = Plan(gpu_ctx, streams)
+    outs = plan.alloc_outputs()
+    plan.execute(outs)
+    gpu_ctx.synchronize()
+    want = [o.cpu().numpy().copy() for o in outs]
+    for lanes in (8, 16, 32):
+        L.lib().tc_ctx_set_t1_group(gpu_ctx.handle, lanes)
+        for o in outs:
+            o.zero_()
+        plan.execute(outs)
+        gpu_ctx.synchronize()
+        for o, w in zip(outs, want):
+            np.testing.assert_array_equal(o.cpu().numpy(), w)
+    L.lib().tc_ctx_set_t1_group(gpu_ctx.handle, 32)
+    plan.set_graph(True)
+    n0 = gpu_ctx.launches
+    for _ in range(3):
+        for o in outs:
+            o.zero_()
+        plan.execute(outs)
+        gpu_ctx.synchronize()
+        for o, w in zip(outs, want):
+            np.testing.assert_array_equal(o.cpu().numpy(), w)
+    assert gpu_ctx.launches > n0
+    plan.set_graph(False)
+    g = tune_plan(plan, outs, trials=1, use_cache=False)
+    assert g in (8, 16, 32)
+    L.lib().tc_ctx_set_t1_group(gpu_ctx.handle, 32)
+    plan.close()

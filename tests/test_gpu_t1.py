@@ -97,3 +97,19 @@ def test_t1_empty_and_zero_pass_blocks(gpu_ctx):
     got = _coder(gpu_ctx).decode_blocks(desc, pool, len(desc) * 4096, recon_r=0.0).cpu().numpy()
     want = oracle_slots(desc, pool, "int", 0.0).reshape(-1)
     np.testing.assert_array_equal(got, want)
+
+
+@pytest.mark.parametrize("lanes", [8, 16, 32])
+def test_t1_lane_group_widths_bit_exact(gpu_ctx, lanes):
+    """Two or four code-blocks per warp (8/16 lanes each) decode exactly like
+    one block per warp."""
+    from thousandthchicken_b200 import _lib as L
+    desc, pool, _ = make_blocks(seed=91, n=600, truncate=True)
+    assert L.lib().tc_ctx_set_t1_group(gpu_ctx.handle, lanes) == 0
+    try:
+        got = _coder(gpu_ctx).decode_blocks(desc, pool, len(desc) * 4096, recon_r=0.5).cpu().numpy()
+        raw = _coder(gpu_ctx).decode_blocks(desc, pool, len(desc) * 4096, raw=True).cpu().numpy()
+    finally:
+        L.lib().tc_ctx_set_t1_group(gpu_ctx.handle, 32)
+    np.testing.assert_array_equal(got, oracle_slots(desc, pool, "int", 0.5).reshape(-1))
+    np.testing.assert_array_equal(raw, oracle_slots(desc, pool, "raw").reshape(-1).view(np.int32))

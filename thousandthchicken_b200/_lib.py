@@ -84,6 +84,8 @@ _PROTOS = {
     "tc_ctx_synchronize": (_I, [_VP]),
     "tc_ctx_last_error": (C.c_char_p, [_VP]),
     "tc_ctx_launch_count": (C.c_uint64, [_VP]),
+    "tc_ctx_set_t1_group": (_I, [_VP, _I]),
+    "tc_ctx_t1_group": (_I, [_VP]),
     "tc_t1_decode": (_I, [_VP, _VP, _VP, _I, _VP, C.c_uint64, _VP, _I, C.c_float, _I]),
     "tc_t1_sort_order": (_I, [_VP, _I, _VP]),
     "tc_dequantize_raw": (_I, [_VP, _VP, _I, _VP, _VP, C.c_float]),
@@ -101,10 +103,12 @@ _PROTOS = {
     "tc_decode_j2k_file": (_I, [_VP, C.c_char_p, _VP, C.c_size_t, C.POINTER(ImageInfo)]),
     "tc_plan_create": (_I, [_VP, _VP, _VP, _I, C.POINTER(_VP)]),
     "tc_plan_destroy": (_I, [_VP]),
+    "tc_plan_rebuild": (_I, [_VP, _VP, _VP, _I]),
     "tc_plan_output_bytes": (_I, [_VP, _I, C.POINTER(C.c_size_t)]),
     "tc_plan_image_info": (_I, [_VP, _I, C.POINTER(ImageInfo)]),
     "tc_plan_execute": (_I, [_VP, _VP]),
     "tc_plan_set_profiling": (_I, [_VP, _I]),
+    "tc_plan_set_graph": (_I, [_VP, _I]),
     "tc_plan_stage_ms": (_I, [_VP, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "tc_encode_j2k": (_I, [C.POINTER(EncodeParams), _VP, _VP, C.c_size_t, C.POINTER(C.c_size_t)]),
     "tc_t1_encode_block": (_I, [_VP, _I, _I, _I, _I, _I, _VP, _I, C.POINTER(_I), C.POINTER(_I),

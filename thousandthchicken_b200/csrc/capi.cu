@@ -23,10 +23,12 @@ namespace tc {
 cudaError_t DevBuf::ensure(size_t bytes)
 {
     if (bytes <= size && ptr) return cudaSuccess;
+    // Grow by at least half again: a serving loop whose batches vary in size
+    // reallocates (and so synchronises the device in cudaFree) only rarely.
+    const size_t want = std::max<size_t>(std::max<size_t>(bytes, 256), size + size / 2);
     if (ptr) cudaFree(ptr);
     ptr = nullptr;
     size = 0;
-    const size_t want = std::max<size_t>(bytes, 256);
     cudaError_t e = cudaMalloc(&ptr, want);
     if (e == cudaSuccess) size = want;
     else ptr = nullptr;
@@ -62,28 +64,6 @@ int cuda_status(tc_ctx *ctx, cudaError_t e, const char *what)
     if (e == cudaErrorMemoryAllocation) return fail(ctx, TC_E_OOM, std::string(what) + ": out of device memory");
     return fail(ctx, TC_E_DEVICE, std::string(what) + ": " + cudaGetErrorString(e));
 }
-
-// Pinned host staging buffer (grow-only).
-struct PinBuf {
-    void *ptr = nullptr;
-    size_t size = 0;
-    cudaError_t ensure(size_t bytes)
-    {
-        if (bytes <= size && ptr) return cudaSuccess;
-        if (ptr) cudaFreeHost(ptr);
-        ptr = nullptr;
-        size = 0;
-        cudaError_t e = cudaHostAlloc(&ptr, std::max<size_t>(bytes, 4096), cudaHostAllocDefault);
-        if (e == cudaSuccess) size = std::max<size_t>(bytes, 4096);
-        return e;
-    }
-    void release()
-    {
-        if (ptr) cudaFreeHost(ptr);
-        ptr = nullptr;
-        size = 0;
-    }
-};
 
 static int check_ctx(tc_ctx *ctx)
 {
@@ -186,11 +166,26 @@ struct tc_plan {
     int class_counts[3] = {0, 0, 0};  // Tier-1 blocks of <= 8, <= 16, <= 31 coded bit-planes
     bool profiling = false;
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    // graph replay of execute (tc_plan_set_graph)
+    PinBuf h_pool, h_desc, h_order;  // pinned host staging, alive until the next build
+    bool use_graph = false;
+    cudaGraphExec_t graph = nullptr;
+    std::vector<void *> graph_outs;  // outputs the graph was captured for
+    uint64_t graph_launches = 0;     // kernels per replay
 };
+
+static void plan_drop_graph(tc_plan *P)
+{
+    if (P->graph) cudaGraphExecDestroy(P->graph);
+    P->graph = nullptr;
+    P->graph_outs.clear();
+}
 
 static int plan_build(tc_ctx *ctx, const uint8_t *const *cs, const size_t *lens, int n, tc_plan *P)
 {
     P->ctx = ctx;
+    P->imgs.clear();
+    P->ncblk = 0;
     std::vector<Parsed> parsed(n);
     std::string err;
     uint64_t pool_total = 0, coef_total = 0;
@@ -212,41 +207,48 @@ static int plan_build(tc_ctx *ctx, const uint8_t *const *cs, const size_t *lens,
         pool_total += (pl + 15) & ~uint64_t(15);
         P->ncblk += (int)parsed[i].desc.size();
     }
-    // Host staging: pool and rebased descriptors.
-    std::vector<uint8_t> hpool(pool_total ? pool_total : 16);
-    std::vector<tc_cblk_desc> hdesc;
-    hdesc.reserve(P->ncblk);
+    // Pinned host staging (the plan keeps it until its next build, so the
+    // uploads below are asynchronous): pool and rebased descriptors.
+    cudaError_t e;
+    // the previous execute may still read the staging through its uploads
+    if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return cuda_status(ctx, e, "plan staging");
+    const size_t pool_bytes = pool_total ? pool_total : 16;
+    if ((e = P->h_pool.ensure(pool_bytes)) != cudaSuccess ||
+        (e = P->h_desc.ensure(sizeof(tc_cblk_desc) * std::max(1, P->ncblk))) != cudaSuccess ||
+        (e = P->h_order.ensure(sizeof(uint32_t) * std::max(1, P->ncblk))) != cudaSuccess)
+        return cuda_status(ctx, e, "plan staging");
+    uint8_t *hpool = static_cast<uint8_t *>(P->h_pool.ptr);
+    tc_cblk_desc *hdesc = static_cast<tc_cblk_desc *>(P->h_desc.ptr);
+    uint32_t *horder = static_cast<uint32_t *>(P->h_order.ptr);
     uint64_t po = 0;
+    size_t nd = 0;
     for (int i = 0; i < n; i++) {
         const uint8_t *src = parsed[i].pool_is_cs ? cs[i] : parsed[i].own_pool.data();
         const uint64_t pl = parsed[i].pool_is_cs ? lens[i] : parsed[i].own_pool.size();
-        if (pl) std::memcpy(hpool.data() + po, src, pl);
+        if (pl) std::memcpy(hpool + po, src, pl);
         const uint64_t elem_base = P->imgs[i].coef_off / 4;
         for (tc_cblk_desc d : parsed[i].desc) {
             d.seg_off += po;
             d.out_off += elem_base;
-            hdesc.push_back(d);
+            hdesc[nd++] = d;
         }
         po += (pl + 15) & ~uint64_t(15);
     }
-    std::vector<uint32_t> horder(P->ncblk);
-    t1_class_order(hdesc.data(), P->ncblk, horder.data(), P->class_counts);
+    t1_class_order(hdesc, P->ncblk, horder, P->class_counts);
     P->pool_len = pool_total;
     P->scratch_per_img = scratch_max;
-    cudaError_t e;
-    if ((e = P->pool.ensure(hpool.size())) != cudaSuccess ||
+    if ((e = P->pool.ensure(pool_bytes)) != cudaSuccess ||
         (e = P->desc.ensure(sizeof(tc_cblk_desc) * std::max(1, P->ncblk))) != cudaSuccess ||
         (e = P->order.ensure(sizeof(uint32_t) * std::max(1, P->ncblk))) != cudaSuccess ||
         (e = P->coef.ensure(std::max<uint64_t>(coef_total, 256))) != cudaSuccess ||
         (e = P->scratch.ensure(std::max<size_t>(scratch_max, 256))) != cudaSuccess)
         return cuda_status(ctx, e, "plan allocation");
-    if ((e = cudaMemcpyAsync(P->pool.ptr, hpool.data(), hpool.size(), cudaMemcpyHostToDevice, ctx->stream)) ||
-        (e = cudaMemcpyAsync(P->desc.ptr, hdesc.data(), sizeof(tc_cblk_desc) * P->ncblk, cudaMemcpyHostToDevice,
+    if ((e = cudaMemcpyAsync(P->pool.ptr, hpool, pool_bytes, cudaMemcpyHostToDevice, ctx->stream)) ||
+        (e = cudaMemcpyAsync(P->desc.ptr, hdesc, sizeof(tc_cblk_desc) * P->ncblk, cudaMemcpyHostToDevice,
                              ctx->stream)) ||
-        (e = cudaMemcpyAsync(P->order.ptr, horder.data(), sizeof(uint32_t) * P->ncblk, cudaMemcpyHostToDevice,
+        (e = cudaMemcpyAsync(P->order.ptr, horder, sizeof(uint32_t) * P->ncblk, cudaMemcpyHostToDevice,
                              ctx->stream)))
         return cuda_status(ctx, e, "plan upload");
-    if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return cuda_status(ctx, e, "plan upload");
     return TC_OK;
 }
 
@@ -343,6 +345,9 @@ int tc_ctx_destroy(tc_ctx *ctx)
     ctx->tmp_order.release();
     ctx->tmp_coef.release();
     ctx->tmp_out.release();
+    ctx->stage_pool.release();
+    ctx->stage_desc.release();
+    ctx->stage_order.release();
     if (ctx->d_words) cudaFree(ctx->d_words);
     for (int i = 0; i < 2; i++) {
         if (ctx->side[i]) cudaStreamDestroy(ctx->side[i]);
@@ -374,6 +379,15 @@ int tc_ctx_synchronize(tc_ctx *ctx)
 const char *tc_ctx_last_error(const tc_ctx *ctx) { return ctx ? ctx->err.c_str() : "no context"; }
 
 uint64_t tc_ctx_launch_count(const tc_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+int tc_ctx_set_t1_group(tc_ctx *ctx, int lanes)
+{
+    if (!ctx || (lanes != 8 && lanes != 16 && lanes != 32)) return TC_E_ARG;
+    ctx->t1_group = lanes;
+    return TC_OK;
+}
+
+int tc_ctx_t1_group(const tc_ctx *ctx) { return ctx ? ctx->t1_group : TC_E_ARG; }
 
 int tc_t1_decode(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint32_t *d_order, int n, const uint8_t *d_pool,
                  uint64_t pool_len, void *d_out, int out_mode, float recon_r, int max_bitplanes)
@@ -621,6 +635,18 @@ int tc_plan_create(tc_ctx *ctx, const uint8_t *const *h_cs, const size_t *lens, 
     return TC_OK;
 }
 
+int tc_plan_rebuild(tc_plan *P, const uint8_t *const *h_cs, const size_t *lens, int nimages)
+{
+    if (!P || !h_cs || !lens || nimages < 1) return TC_E_ARG;
+    int rc = check_ctx(P->ctx);
+    if (rc) return rc;
+    // wait for the previous execute before its buffers are overwritten
+    cudaError_t e = cudaStreamSynchronize(P->ctx->stream);
+    if (e != cudaSuccess) return cuda_status(P->ctx, e, "tc_plan_rebuild");
+    plan_drop_graph(P);
+    return plan_build(P->ctx, h_cs, lens, nimages, P);
+}
+
 int tc_plan_destroy(tc_plan *P)
 {
     if (!P) return TC_E_ARG;
@@ -633,8 +659,12 @@ int tc_plan_destroy(tc_plan *P)
     P->order.release();
     P->coef.release();
     P->scratch.release();
+    P->h_pool.release();
+    P->h_desc.release();
+    P->h_order.release();
     for (auto &e : P->ev)
         if (e) cudaEventDestroy(e);
+    plan_drop_graph(P);
     delete P;
     return TC_OK;
 }
@@ -685,7 +715,46 @@ int tc_plan_execute(tc_plan *P, void *const *d_out)
     if (rc) return rc;
     for (size_t i = 0; i < P->imgs.size(); i++)
         if (!d_out[i]) return fail(P->ctx, TC_E_ARG, "tc_plan_execute: null output");
-    return plan_run(P, d_out);
+    if (!P->use_graph || P->profiling) return plan_run(P, d_out);
+    tc_ctx *ctx = P->ctx;
+    std::vector<void *> outs(d_out, d_out + P->imgs.size());
+    if (P->graph && outs != P->graph_outs) plan_drop_graph(P);
+    if (!P->graph) {
+        // First execute with these outputs: run normally (kernel attributes
+        // and side streams get set up), then capture the same work.
+        if ((rc = plan_run(P, d_out))) return rc;
+        cudaGraph_t g = nullptr;
+        const uint64_t l0 = ctx->launches;
+        cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return cuda_status(ctx, e, "graph capture");
+        rc = plan_run(P, d_out);
+        e = cudaStreamEndCapture(ctx->stream, &g);
+        if (rc) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&P->graph, g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            P->graph = nullptr;
+            return cuda_status(ctx, e, "graph instantiate");
+        }
+        P->graph_outs = outs;
+        P->graph_launches = ctx->launches - l0;
+        return TC_OK;
+    }
+    cudaError_t e = cudaGraphLaunch(P->graph, ctx->stream);
+    if (e != cudaSuccess) return cuda_status(ctx, e, "graph launch");
+    ctx->launches += P->graph_launches;
+    return TC_OK;
+}
+
+int tc_plan_set_graph(tc_plan *P, int on)
+{
+    if (!P) return TC_E_ARG;
+    P->use_graph = on != 0;
+    if (!on) plan_drop_graph(P);
+    return TC_OK;
 }
 
 int tc_decode_j2k(tc_ctx *ctx, const uint8_t *h_cs, size_t len, void *h_out, size_t out_bytes, tc_image_info *info)
@@ -701,12 +770,18 @@ int tc_decode_j2k(tc_ctx *ctx, const uint8_t *h_cs, size_t len, void *h_out, siz
     P.order = ctx->tmp_order;
     P.coef = ctx->tmp_coef;
     P.scratch = ctx->scratch;
+    P.h_pool = ctx->stage_pool;
+    P.h_desc = ctx->stage_desc;
+    P.h_order = ctx->stage_order;
     auto give_back = [&]() {
         ctx->tmp_pool = P.pool;
         ctx->tmp_desc = P.desc;
         ctx->tmp_order = P.order;
         ctx->tmp_coef = P.coef;
         ctx->scratch = P.scratch;
+        ctx->stage_pool = P.h_pool;
+        ctx->stage_desc = P.h_desc;
+        ctx->stage_order = P.h_order;
     };
     const uint8_t *cs[1] = {h_cs};
     size_t lens[1] = {len};

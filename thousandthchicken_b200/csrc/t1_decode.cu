@@ -34,7 +34,6 @@
 namespace tc {
 namespace {
 
-constexpr int kWarps = 4;          // warps (code-blocks in flight) per CTA
 constexpr int kMaxStripes = 16;    // 64 rows
 constexpr int kSgnCols = 66;       // 64 columns + a zero column on each side
 
@@ -270,9 +269,23 @@ __device__ __forceinline__ void mark_significant(WarpState<MagT> &S, int s, int 
 // (lane l owns columns l and l+32) and the serial loop visits only candidate
 // columns, in scan order.  Returns the last pass type (0 cleanup,
 // 1 significance propagation, 2 refinement) and its plane.
-template <typename MagT>
+// Candidate mask of the group's columns: column gl + G*j for predicate any[j].
+template <int G>
+__device__ __forceinline__ unsigned long long group_ballot(const bool (&any)[64 / G], unsigned gmask, int gshift)
+{
+    unsigned long long m = 0;
+#pragma unroll
+    for (int j = 0; j < 64 / G; j++) {
+        const unsigned b = __ballot_sync(gmask, any[j]);
+        m |= (unsigned long long)((G == 32 ? b : (b >> gshift)) & (G == 32 ? 0xffffffffu : ((1u << G) - 1u))) << (G * j);
+    }
+    return m;
+}
+
+template <typename MagT, int G>
 __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *seg, int len, int w,
-                            int h, int orient, int numbps, int passes, int *last_plane, int lane)
+                            int h, int orient, int numbps, int passes, int *last_plane, int lane, unsigned gmask,
+                            int gshift)
 {
     MQ mq;
     mq.init(seg, len);
@@ -281,6 +294,7 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
     const uint8_t *zc = T.zc[orient];
     uint32_t *F = S.F;
     const int nstripes = (h + 3) >> 2;
+    constexpr int CPL = 64 / G;  // columns per lane
     int type = 0, pass = 0;
     *last_plane = numbps - 1;
 
@@ -290,11 +304,11 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
             // ---- significance propagation pass (ISO D.3.1; SigPropPassFunctor) ----
             for (int s = 0; s < nstripes; s++) {
                 const int rows = min(4, h - 4 * s);
-                __syncwarp();
-                bool any[2];
+                __syncwarp(gmask);
+                bool any[CPL];
 #pragma unroll
-                for (int j = 0; j < 2; j++) {
-                    const int c = lane + 32 * j;
+                for (int j = 0; j < CPL; j++) {
+                    const int c = lane + G * j;
                     bool a = false;
                     if (c < w) {
                         const uint32_t f = F[s * 64 + c];
@@ -303,8 +317,7 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
                     }
                     any[j] = a;
                 }
-                unsigned long long cand = (unsigned long long)__ballot_sync(0xffffffffu, any[0]) |
-                                          ((unsigned long long)__ballot_sync(0xffffffffu, any[1]) << 32);
+                unsigned long long cand = group_ballot<G>(any, gmask, gshift);
                 while (cand) {
                     const int c = __ffsll((long long)cand) - 1;
                     cand &= cand - 1;
@@ -337,11 +350,11 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
             // the lanes precompute them for their columns.
             for (int s = 0; s < nstripes; s++) {
                 const int rows = min(4, h - 4 * s);
-                __syncwarp();
-                bool any[2];
+                __syncwarp(gmask);
+                bool any[CPL];
 #pragma unroll
-                for (int j = 0; j < 2; j++) {
-                    const int c = lane + 32 * j;
+                for (int j = 0; j < CPL; j++) {
+                    const int c = lane + G * j;
                     uint32_t rr = 0, codes = 0;
                     if (c < w) {
                         const uint32_t f = F[s * 64 + c];
@@ -358,9 +371,8 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
                     }
                     any[j] = rr != 0;
                 }
-                unsigned long long cand = (unsigned long long)__ballot_sync(0xffffffffu, any[0]) |
-                                          ((unsigned long long)__ballot_sync(0xffffffffu, any[1]) << 32);
-                __syncwarp();
+                unsigned long long cand = group_ballot<G>(any, gmask, gshift);
+                __syncwarp(gmask);
                 while (cand) {
                     const int c = __ffsll((long long)cand) - 1;
                     cand &= cand - 1;
@@ -381,11 +393,11 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
         for (int s = 0; s < nstripes; s++) {
             const int rows = min(4, h - 4 * s);
             const uint32_t rmask = (1u << rows) - 1u;
-            __syncwarp();
-            bool any[2];
+            __syncwarp(gmask);
+            bool any[CPL];
 #pragma unroll
-            for (int j = 0; j < 2; j++) {
-                const int c = lane + 32 * j;
+            for (int j = 0; j < CPL; j++) {
+                const int c = lane + G * j;
                 bool a = false;
                 if (c < w) {
                     const uint32_t f = F[s * 64 + c];
@@ -396,8 +408,7 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
                 }
                 any[j] = a;
             }
-            unsigned long long cand = (unsigned long long)__ballot_sync(0xffffffffu, any[0]) |
-                                      ((unsigned long long)__ballot_sync(0xffffffffu, any[1]) << 32);
+            unsigned long long cand = group_ballot<G>(any, gmask, gshift);
             while (cand) {
                 const int c = __ffsll((long long)cand) - 1;
                 cand &= cand - 1;
@@ -435,14 +446,25 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
         type = 0;
         *last_plane = p;
         if (++pass >= passes) break;
-        __syncwarp();
-        for (int i = lane; i < nstripes * 64; i += 32) F[i] &= ~0x3C0000u;  // clear pi
+        __syncwarp(gmask);
+        for (int i = lane; i < nstripes * 64; i += G) F[i] &= ~0x3C0000u;  // clear pi
+        __syncwarp(gmask);
     }
     return type;
 }
 
-template <typename MagT>
-__global__ void __launch_bounds__(32 * kWarps)
+// Lanes per code-block G (32, 16 or 8): a warp splits into 32 / G groups that
+// decode different code-blocks in lock-step (each group runs the serial
+// decoder redundantly across its lanes and splits the candidate searches
+// between them), so one warp instruction can advance several code-blocks.
+// Warps per CTA keep four code-blocks in flight per CTA whatever G is.
+template <int G>
+struct GroupCfg {
+    static constexpr int warps = G == 32 ? 4 : (G == 16 ? 2 : 1);
+};
+
+template <typename MagT, int G>
+__global__ void __launch_bounds__(32 * GroupCfg<G>::warps)
 t1_decode_kernel(const tc_cblk_desc *__restrict__ desc, const uint32_t *__restrict__ order, int n, int ndesc,
                  const uint8_t *__restrict__ pool, uint64_t pool_len, char *__restrict__ out, int out_mode,
                  float recon_r, uint32_t *__restrict__ counter, uint32_t *__restrict__ err)
@@ -454,17 +476,20 @@ t1_decode_kernel(const tc_cblk_desc *__restrict__ desc, const uint32_t *__restri
     build_tables(T);
     __syncthreads();
 
-    const int lane = threadIdx.x & 31;
-    WarpState<MagT> &S = states[threadIdx.x >> 5];
+    const int wl = threadIdx.x & 31;             // lane in the warp
+    const int gidx = wl / G, gl = wl % G;         // group in the warp, lane in the group
+    const int gshift = gidx * G;
+    const unsigned gmask = G == 32 ? 0xffffffffu : (((1u << G) - 1u) << gshift);
+    WarpState<MagT> &S = states[(threadIdx.x >> 5) * (32 / G) + gidx];
 
     for (;;) {
         int idx = 0;
-        if (lane == 0) idx = (int)atomicAdd(counter, 1u);
-        idx = __shfl_sync(0xffffffffu, idx, 0);
+        if (gl == 0) idx = (int)atomicAdd(counter, 1u);
+        idx = __shfl_sync(gmask, idx, gshift);
         if (idx >= n) break;
         const uint32_t bi = order ? order[idx] : (uint32_t)idx;
         if (bi >= (uint32_t)ndesc) {
-            if (lane == 0) atomicOr(err, TC_DERR_DESC);
+            if (gl == 0) atomicOr(err, TC_DERR_DESC);
             continue;
         }
         const tc_cblk_desc d = desc[bi];
@@ -475,37 +500,37 @@ t1_decode_kernel(const tc_cblk_desc *__restrict__ desc, const uint32_t *__restri
                   (numbps == 0 || d.passes <= 3 * numbps - 2) && numbps <= (int)(8 * sizeof(MagT));
         const bool pool_ok = d.seg_off <= pool_len && (uint64_t)d.seg_len <= pool_len - d.seg_off;
         if (!geom_ok) {
-            if (lane == 0) atomicOr(err, TC_DERR_DESC);
+            if (gl == 0) atomicOr(err, TC_DERR_DESC);
             continue;
         }
         if (!ok || !pool_ok) {
-            if (lane == 0) atomicOr(err, ok ? TC_DERR_POOL : TC_DERR_DESC);
+            if (gl == 0) atomicOr(err, ok ? TC_DERR_POOL : TC_DERR_DESC);
             ok = false;
         }
         const bool coded = ok && numbps > 0 && d.passes > 0;
         const int nstripes = (h + 3) >> 2;
 
-        // clear the state (all lanes)
-        for (int i = lane; i < nstripes * 64; i += 32) S.F[i] = 0u;
-        for (int i = lane; i < kSgnCols; i += 32) S.sgn[i] = 0ull;
-        if (lane < 19) {
-            const int st = lane == 0 ? 4 : (lane == 17 ? 46 : (lane == 18 ? 3 : 0));
-            S.ctx[lane] = T.mq[st];
+        // clear the state (the group's lanes)
+        for (int i = gl; i < nstripes * 64; i += G) S.F[i] = 0u;
+        for (int i = gl; i < kSgnCols; i += G) S.sgn[i] = 0ull;
+        for (int i = gl; i < 19; i += G) {
+            const int st = i == 0 ? 4 : (i == 17 ? 46 : (i == 18 ? 3 : 0));
+            S.ctx[i] = T.mq[st];
         }
-        __syncwarp();
+        __syncwarp(gmask);
 
         int type = 0, last_plane = 0;
         if (coded)
-            type = decode_block(S, T, pool + d.seg_off, (int)d.seg_len, w, h, d.orient, numbps, d.passes,
-                                &last_plane, lane);
-        __syncwarp();
+            type = decode_block<MagT, G>(S, T, pool + d.seg_off, (int)d.seg_len, w, h, d.orient, numbps, d.passes,
+                                         &last_plane, gl, gmask, gshift);
+        __syncwarp(gmask);
 
         // epilogue: reconstruction + inverse quantisation, coalesced rows
         const bool irrev = (d.flags & TC_CBLK_IRREVERSIBLE) != 0;
         for (int y = 0; y < h; y++) {
             char *row = out + 4 * (d.out_off + (uint64_t)y * d.out_pitch);
             const int s = y >> 2, k = y & 3;
-            for (int x = lane; x < w; x += 32) {
+            for (int x = gl; x < w; x += G) {
                 const uint32_t f = coded ? S.F[s * 64 + x] : 0u;
                 const bool sg = (f & self_bit(k)) != 0u;
                 uint32_t mg = 0, neg = 0, u = 0;
@@ -528,7 +553,7 @@ t1_decode_kernel(const tc_cblk_desc *__restrict__ desc, const uint32_t *__restri
                 }
             }
         }
-        __syncwarp();
+        __syncwarp(gmask);
     }
 }
 
@@ -574,28 +599,31 @@ struct LaunchCfg {
     size_t smem = 0;
 };
 
-template <typename MagT>
+template <typename MagT, int G>
 cudaError_t launch_class(tc_ctx *ctx, cudaStream_t stream, const tc_cblk_desc *d_desc, const uint32_t *d_order,
                          int n, int ndesc, const uint8_t *d_pool, uint64_t pool_len, void *d_out, int out_mode,
                          float recon_r, int slot)
 {
+    constexpr int kWarps = GroupCfg<G>::warps, kGroup = G;
     static LaunchCfg cfg[64];
     LaunchCfg &C = cfg[ctx->device & 63];
     if (!C.ready) {
-        C.smem = ((sizeof(Tables) + 15) & ~size_t(15)) + kWarps * sizeof(WarpState<MagT>);
-        cudaError_t e = cudaFuncSetAttribute(t1_decode_kernel<MagT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)C.smem);
+        C.smem = ((sizeof(Tables) + 15) & ~size_t(15)) + kWarps * (32 / kGroup) * sizeof(WarpState<MagT>);
+        cudaError_t e = cudaFuncSetAttribute(t1_decode_kernel<MagT, kGroup>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C.smem);
         if (e != cudaSuccess) return e;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&C.per_sm, t1_decode_kernel<MagT>, 32 * kWarps, C.smem);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&C.per_sm, t1_decode_kernel<MagT, kGroup>, 32 * kWarps,
+                                                          C.smem);
         if (e != cudaSuccess) return e;
         if (C.per_sm < 1) C.per_sm = 1;
         C.ready = true;
     }
-    const int want = (n + kWarps - 1) / kWarps;
+    const int per_cta = kWarps * (32 / kGroup);
+    const int want = (n + per_cta - 1) / per_cta;
     const int grid = std::min(want, C.per_sm * num_sms(ctx->device));
     cudaError_t e = cudaMemsetAsync(ctx->d_words + slot, 0, sizeof(uint32_t), stream);
     if (e != cudaSuccess) return e;
-    t1_decode_kernel<MagT><<<grid, 32 * kWarps, C.smem, stream>>>(d_desc, d_order, n, ndesc, d_pool, pool_len,
+    t1_decode_kernel<MagT, kGroup><<<grid, 32 * kWarps, C.smem, stream>>>(d_desc, d_order, n, ndesc, d_pool, pool_len,
                                                                    static_cast<char *>(d_out), out_mode, recon_r,
                                                                    ctx->d_words + slot, ctx->d_words);
     ctx->launches++;
@@ -612,6 +640,26 @@ cudaError_t launch_t1_decode(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint
                              max_bitplanes > 8 && max_bitplanes <= 16 ? n : 0, max_bitplanes > 16 ? n : 0, d_pool,
                              pool_len, d_out, out_mode, recon_r);
 }
+
+namespace {
+template <typename MagT>
+cudaError_t launch_class_g(tc_ctx *ctx, cudaStream_t stream, const tc_cblk_desc *d_desc, const uint32_t *d_order,
+                           int n, int ndesc, const uint8_t *d_pool, uint64_t pool_len, void *d_out, int out_mode,
+                           float recon_r, int slot)
+{
+    switch (ctx->t1_group) {
+    case 8:
+        return launch_class<MagT, 8>(ctx, stream, d_desc, d_order, n, ndesc, d_pool, pool_len, d_out, out_mode,
+                                     recon_r, slot);
+    case 16:
+        return launch_class<MagT, 16>(ctx, stream, d_desc, d_order, n, ndesc, d_pool, pool_len, d_out, out_mode,
+                                      recon_r, slot);
+    default:
+        return launch_class<MagT, 32>(ctx, stream, d_desc, d_order, n, ndesc, d_pool, pool_len, d_out, out_mode,
+                                      recon_r, slot);
+    }
+}
+}  // namespace
 
 cudaError_t launch_t1_classes(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint32_t *d_order, int ndesc,
                               int n8, int n16, int n32, const uint8_t *d_pool, uint64_t pool_len, void *d_out,
@@ -633,13 +681,13 @@ cudaError_t launch_t1_classes(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uin
     }
     e = cudaSuccess;
     if (n32 > 0)
-        e = launch_class<uint32_t>(ctx, s32, d_desc, d_order ? d_order + n8 + n16 : nullptr, n32, ndesc, d_pool,
+        e = launch_class_g<uint32_t>(ctx, s32, d_desc, d_order ? d_order + n8 + n16 : nullptr, n32, ndesc, d_pool,
                                    pool_len, d_out, out_mode, recon_r, 3);
     if (e == cudaSuccess && n16 > 0)
-        e = launch_class<uint16_t>(ctx, s16, d_desc, d_order ? d_order + n8 : nullptr, n16, ndesc, d_pool,
+        e = launch_class_g<uint16_t>(ctx, s16, d_desc, d_order ? d_order + n8 : nullptr, n16, ndesc, d_pool,
                                    pool_len, d_out, out_mode, recon_r, 2);
     if (e == cudaSuccess && n8 > 0)
-        e = launch_class<uint8_t>(ctx, s8, d_desc, d_order, n8, ndesc, d_pool, pool_len, d_out, out_mode, recon_r,
+        e = launch_class_g<uint8_t>(ctx, s8, d_desc, d_order, n8, ndesc, d_pool, pool_len, d_out, out_mode, recon_r,
                                   1);
     if (nclass > 1) {
         for (int i = 0; i < 2; i++) {

@@ -22,6 +22,30 @@ struct DevBuf {
     void release();
 };
 
+// Pinned host staging buffer (grow-only).
+struct PinBuf {
+    void *ptr = nullptr;
+    size_t size = 0;
+    cudaError_t ensure(size_t bytes)
+    {
+        if (bytes <= size && ptr) return cudaSuccess;
+        const size_t want = bytes < 4096 ? 4096 : (bytes < size + size / 2 ? size + size / 2 : bytes);
+        if (ptr) cudaFreeHost(ptr);
+        ptr = nullptr;
+        size = 0;
+        cudaError_t e = cudaHostAlloc(&ptr, want, cudaHostAllocDefault);
+        if (e == cudaSuccess) size = want;
+        else ptr = nullptr;
+        return e;
+    }
+    void release()
+    {
+        if (ptr) cudaFreeHost(ptr);
+        ptr = nullptr;
+        size = 0;
+    }
+};
+
 }  // namespace tc
 
 struct tc_ctx {
@@ -31,7 +55,9 @@ struct tc_ctx {
     uint32_t *d_words = nullptr;  // [0] error word, [1..3] Tier-1 work counters
     tc::DevBuf scratch;           // DWT intermediate levels
     tc::DevBuf tmp_pool, tmp_desc, tmp_order, tmp_coef, tmp_out;
+    tc::PinBuf stage_pool, stage_desc, stage_order;  // pinned staging of tc_decode_j2k
     uint64_t launches = 0;
+    int t1_group = 32;            // lanes per code-block in the Tier-1 kernel (8, 16 or 32)
     // side streams for concurrent Tier-1 class launches (created on first use)
     cudaStream_t side[2] = {nullptr, nullptr};
     cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};

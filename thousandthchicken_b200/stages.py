@@ -287,6 +287,10 @@ class Plan:
         self.ctx.check(L.lib().tc_plan_execute(self.handle, ptrs), "tc_plan_execute")
         return outs
 
+    def set_graph(self, on: bool = True):
+        """Replay execute as a captured CUDA graph (per set of outputs)."""
+        L.check(L.lib().tc_plan_set_graph(self.handle, int(on)), self.ctx.handle, "tc_plan_set_graph")
+
     def set_profiling(self, on: bool = True):
         L.check(L.lib().tc_plan_set_profiling(self.handle, int(on)), self.ctx.handle, "tc_plan_set_profiling")
 
