@@ -47,6 +47,7 @@ cudaError_t ensure_side_streams(tc_ctx *ctx)
     if (ctx->side[0]) return cudaSuccess;
     cudaError_t e = cudaSuccess;
     for (int i = 0; i < 2 && e == cudaSuccess; i++) e = cudaStreamCreateWithFlags(&ctx->side[i], cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->capture, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming);
     for (int i = 0; i < 2 && e == cudaSuccess; i++) e = cudaEventCreateWithFlags(&ctx->ev_join[i], cudaEventDisableTiming);
     return e;
@@ -354,6 +355,7 @@ int tc_ctx_destroy(tc_ctx *ctx)
         if (ctx->ev_join[i]) cudaEventDestroy(ctx->ev_join[i]);
     }
     if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+    if (ctx->capture) cudaStreamDestroy(ctx->capture);
     delete ctx;
     return TC_OK;
 }
@@ -723,12 +725,23 @@ int tc_plan_execute(tc_plan *P, void *const *d_out)
         // First execute with these outputs: run normally (kernel attributes
         // and side streams get set up), then capture the same work.
         if ((rc = plan_run(P, d_out))) return rc;
+        // Capture on the context's own stream: the caller's stream may be the
+        // legacy default stream, which cannot be captured.  The graph is then
+        // launched on the caller's stream.
         cudaGraph_t g = nullptr;
         const uint64_t l0 = ctx->launches;
-        cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+        cudaError_t e = ensure_side_streams(ctx);
         if (e != cudaSuccess) return cuda_status(ctx, e, "graph capture");
+        cudaStream_t caller = ctx->stream;
+        ctx->stream = ctx->capture;
+        e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) {
+            ctx->stream = caller;
+            return cuda_status(ctx, e, "graph capture");
+        }
         rc = plan_run(P, d_out);
         e = cudaStreamEndCapture(ctx->stream, &g);
+        ctx->stream = caller;
         if (rc) {
             if (g) cudaGraphDestroy(g);
             return rc;

@@ -1,0 +1,261 @@
+// dwt_rev.cu -- reverse DWT levels (5/3 int32, 9/7 fp32) for sm_100a.
+//
+// One CTA reconstructs a 128-column output tile of one level (56 rows for
+// 9/7, 60 for 5/3): it loads the 64-row extended tile (a halo of H = 4 or 2
+// samples on every side) straight from the level's four subbands into shared
+// memory, with whole-sample symmetric extension (ISO F.3.7; the reference's
+// single reflection, dwt_io.cl:7-38, is defect D14), then
+//   * horizontal lifting: each thread lifts one 32-sample segment of one row
+//     (plus its halo) entirely in registers, fully unrolled;
+//   * vertical lifting: each thread lifts one 64-sample column in registers;
+// so every lifting step is register arithmetic with constant indices and the
+// CTA synchronises only between phases.  The row stride in shared memory is
+// odd, so threads walking different rows hit different banks.
+//
+// COLOR >= 0 fuses the inverse RCT/ICT, DC shift, rounding and clamp into the
+// store of the last level (the reference's tcr_kernel / tci_kernel /
+// idc_level_shift_kernel, Preprocessor.cpp:44-180), writing 8/16-bit samples.
+// The ISO 2D_SR order is kept: rows first, then columns (DWTReverse53/97,
+// dwt_r53.cl / dwt_r97.cl).
+#include <cuda_runtime.h>
+
+#include "dwt_common.cuh"
+#include "tc_internal.cuh"
+
+namespace tc {
+namespace {
+
+using namespace dwt;
+
+constexpr int kThreads = 128;
+
+template <int WAVELET>
+struct RevGeo {
+    static constexpr int H = WAVELET ? 4 : 2;     // halo
+    static constexpr int NR = 64;                 // extended rows per tile
+    static constexpr int TY = NR - 2 * H;         // output rows per tile
+    static constexpr int TX = 128;                // output columns per tile
+    static constexpr int NC = TX + 2 * H;         // extended columns
+    static constexpr int S = NC + 1;              // odd row stride (bank spread)
+    static constexpr int SEG = 32;                // outputs per row segment
+    static constexpr int SEGN = SEG + 2 * H;      // inputs per row segment
+};
+
+// In-place 1-D reverse lifting of an interleaved signal held in registers
+// (v[0] at an even position; even = low-pass).  Only samples at least H away
+// from both ends are exact.
+template <typename T, int WAVELET, int RND, int N>
+__device__ __forceinline__ void lift_reverse(T (&v)[N])
+{
+    if constexpr (WAVELET == 0) {
+#pragma unroll
+        for (int k = 2; k <= N - 2; k += 2) v[k] -= div4r<RND>(v[k - 1] + v[k + 1] + 2);
+#pragma unroll
+        for (int k = 1; k <= N - 3; k += 2) v[k] += div2r<RND>(v[k - 1] + v[k + 1]);
+    } else {
+#pragma unroll
+        for (int k = 0; k < N; k += 2) {
+            v[k] *= kK;
+            v[k + 1] *= kInvK;
+        }
+#pragma unroll
+        for (int k = 2; k <= N - 2; k += 2) v[k] = fmaf(-kD, v[k - 1] + v[k + 1], v[k]);
+#pragma unroll
+        for (int k = 1; k <= N - 3; k += 2) v[k] = fmaf(-kG, v[k - 1] + v[k + 1], v[k]);
+#pragma unroll
+        for (int k = 2; k <= N - 2; k += 2) v[k] = fmaf(-kB, v[k - 1] + v[k + 1], v[k]);
+#pragma unroll
+        for (int k = 1; k <= N - 3; k += 2) v[k] = fmaf(-kA, v[k - 1] + v[k + 1], v[k]);
+    }
+}
+
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+template <typename OT>
+__device__ __forceinline__ OT clamp_out(int v, int mx)
+{
+    return (OT)(v < 0 ? 0 : (v > mx ? mx : v));
+}
+
+template <typename T, int WAVELET, int RND, int NCOMP, int COLOR, typename OT>
+__global__ void __launch_bounds__(kThreads) idwt_rev_kernel(LevelIO io, int bits)
+{
+    using G = RevGeo<WAVELET>;
+    constexpr int H = G::H, NR = G::NR, TY = G::TY, TX = G::TX, NC = G::NC, S = G::S;
+    constexpr bool PLANE = COLOR < 0;
+    constexpr int NT = PLANE ? 1 : NCOMP;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *tiles = reinterpret_cast<T *>(smem_raw);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+    const int w = io.w, h = io.h, wl = (w + 1) >> 1, hl = (h + 1) >> 1;
+    const int cbase = PLANE ? blockIdx.z : 0;
+
+    // 1. load the extended tiles from the four subbands (Mallat layout) with
+    //    4-byte asynchronous copies, so a thread has its whole share of the
+    //    tile in flight at once
+#pragma unroll
+    for (int cc = 0; cc < NT; cc++) {
+        T *t = tiles + cc * NR * S;
+        const T *ll = static_cast<const T *>(io.ll[cbase + cc]);
+        const T *coef = static_cast<const T *>(io.coef[cbase + cc]);
+        for (int r = warp; r < NR; r += kThreads / 32) {
+            const int my = mirror(y0 - H + r, h), yb = my >> 1;
+            const T *lrow = (my & 1) ? coef + (size_t)(hl + yb) * io.coef_pitch : ll + (size_t)yb * io.ll_pitch;
+            const T *hrow = coef + (size_t)((my & 1) ? hl + yb : yb) * io.coef_pitch + wl;
+#pragma unroll
+            for (int e = lane; e < NC; e += 32) {
+                const int mx = mirror(x0 - H + e, w);
+                cp_async4(t + r * S + e, ((mx & 1) ? hrow : lrow) + (mx >> 1));
+            }
+        }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+
+    // 2. horizontal lifting, one row segment per thread, two rounds of 32 rows
+    if (w > 1) {
+        const int seg = tid >> 5;  // 4 segments of 32 outputs per row
+#pragma unroll
+        for (int cc = 0; cc < NT; cc++) {
+            T *t = tiles + cc * NR * S;
+#pragma unroll 1
+            for (int round = 0; round < NR / 32; round++) {
+                const int r = round * 32 + lane;
+                T v[G::SEGN];
+#pragma unroll
+                for (int k = 0; k < G::SEGN; k++) v[k] = t[r * S + seg * G::SEG + k];
+                __syncthreads();  // neighbouring segments overlap: all reads before any write
+                lift_reverse<T, WAVELET, RND, G::SEGN>(v);
+#pragma unroll
+                for (int k = H; k < H + G::SEG; k++) t[r * S + seg * G::SEG + k] = v[k];
+            }
+        }
+        __syncthreads();
+    }
+
+    // 3. vertical lifting, one column per thread
+    const int col = tid, x = x0 + col;
+#pragma unroll
+    for (int cc = 0; cc < NT; cc++) {
+        T *t = tiles + cc * NR * S;
+        T v[NR];
+#pragma unroll
+        for (int r = 0; r < NR; r++) v[r] = t[r * S + H + col];
+        if (h > 1) lift_reverse<T, WAVELET, RND, NR>(v);
+        if constexpr (PLANE) {
+            T *out = static_cast<T *>(io.out[cbase]);
+            if (x < w) {
+#pragma unroll
+                for (int r = 0; r < TY; r++)
+                    if (y0 + r < h) out[(size_t)(y0 + r) * io.out_pitch + x] = v[H + r];
+            }
+        } else {
+#pragma unroll
+            for (int r = 0; r < TY; r++) t[(H + r) * S + H + col] = v[H + r];
+        }
+    }
+
+    // 4. fused inverse colour transform, DC shift, rounding and clamp
+    if constexpr (!PLANE) {
+        __syncthreads();
+        const int dc = 1 << (bits - 1), mx = (1 << bits) - 1;
+        for (int q = tid; q < TX * TY; q += kThreads) {
+            const int r = q / TX, cx = q % TX;
+            const int y = y0 + r, xx = x0 + cx;
+            if (y >= h || xx >= w) continue;
+            const int ci = (H + r) * S + H + cx;
+            const size_t o = (size_t)y * io.out_pitch + xx;
+            int vv[NCOMP];
+            if constexpr (COLOR == TC_COLOR_RCT) {
+                const int Y = (int)tiles[ci], U = (int)tiles[NR * S + ci], V = (int)tiles[2 * NR * S + ci];
+                const int Gc = Y - ((U + V) >> 2);
+                vv[0] = V + Gc;
+                vv[1] = Gc;
+                vv[2] = U + Gc;
+            } else if constexpr (COLOR == TC_COLOR_ICT) {
+                const float Y = (float)tiles[ci], Cb = (float)tiles[NR * S + ci], Cr = (float)tiles[2 * NR * S + ci];
+                vv[0] = __float2int_rn(fmaf(1.402f, Cr, Y));
+                vv[1] = __float2int_rn(Y - 0.34413f * Cb - 0.71414f * Cr);
+                vv[2] = __float2int_rn(fmaf(1.772f, Cb, Y));
+            }
+#pragma unroll
+            for (int c = 0; c < NCOMP; c++) {
+                int sv;
+                if (COLOR != TC_COLOR_DC && c < 3) sv = vv[c];
+                else if constexpr (WAVELET == 0) sv = (int)tiles[c * NR * S + ci];
+                else sv = __float2int_rn((float)tiles[c * NR * S + ci]);
+                static_cast<OT *>(io.out[c])[o] = clamp_out<OT>(sv + dc, mx);
+            }
+        }
+    }
+}
+
+template <typename T, int WAVELET, int RND, int NCOMP, int COLOR, typename OT>
+cudaError_t run_rev(tc_ctx *ctx, const LevelIO &io, int bits)
+{
+    using G = RevGeo<WAVELET>;
+    constexpr int NT = COLOR < 0 ? 1 : NCOMP;
+    constexpr size_t smem = (size_t)NT * G::NR * G::S * sizeof(T);
+    static bool attr[64] = {};
+    if (!attr[ctx->device & 63]) {
+        cudaError_t e = cudaFuncSetAttribute(idwt_rev_kernel<T, WAVELET, RND, NCOMP, COLOR, OT>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr[ctx->device & 63] = true;
+    }
+    dim3 grid((io.w + G::TX - 1) / G::TX, (io.h + G::TY - 1) / G::TY, COLOR < 0 ? io.ncomp : 1);
+    idwt_rev_kernel<T, WAVELET, RND, NCOMP, COLOR, OT><<<grid, kThreads, smem, ctx->stream>>>(io, bits);
+    ctx->launches++;
+    return cudaGetLastError();
+}
+
+template <typename T, int WAVELET, int RND, int COLOR>
+cudaError_t run_last(tc_ctx *ctx, const LevelIO &io, int out_type, int bits)
+{
+#define TC_LAST(NC_)                                                                         \
+    (out_type == TC_U8    ? run_rev<T, WAVELET, RND, NC_, COLOR, uint8_t>(ctx, io, bits)  \
+     : out_type == TC_U16 ? run_rev<T, WAVELET, RND, NC_, COLOR, uint16_t>(ctx, io, bits) \
+                          : run_rev<T, WAVELET, RND, NC_, COLOR, int32_t>(ctx, io, bits))
+    if (COLOR != TC_COLOR_DC) return io.ncomp == 4 ? TC_LAST(4) : TC_LAST(3);
+    switch (io.ncomp) {
+    case 1: return TC_LAST(1);
+    case 2: return TC_LAST(2);
+    case 3: return TC_LAST(3);
+    default: return TC_LAST(4);
+    }
+#undef TC_LAST
+}
+
+}  // namespace
+
+cudaError_t launch_idwt_level(tc_ctx *ctx, const LevelIO &io, int wavelet, int rounding)
+{
+    if (io.w <= 0 || io.h <= 0) return cudaSuccess;
+    if (wavelet) return run_rev<float, 1, 0, 1, -1, float>(ctx, io, 0);
+    if (rounding == TC_ROUND_TRUNC) return run_rev<int32_t, 0, TC_ROUND_TRUNC, 1, -1, int32_t>(ctx, io, 0);
+    return run_rev<int32_t, 0, TC_ROUND_FLOOR, 1, -1, int32_t>(ctx, io, 0);
+}
+
+cudaError_t launch_idwt_last_color(tc_ctx *ctx, const LevelIO &io, int wavelet, int color, int out_type, int bits,
+                                   bool)
+{
+    if (io.w <= 0 || io.h <= 0) return cudaSuccess;
+    if (color != TC_COLOR_DC && io.ncomp < 3) color = TC_COLOR_DC;
+    if (wavelet) {
+        if (color == TC_COLOR_ICT || color == TC_COLOR_RCT)
+            return run_last<float, 1, 0, TC_COLOR_ICT>(ctx, io, out_type, bits);
+        return run_last<float, 1, 0, TC_COLOR_DC>(ctx, io, out_type, bits);
+    }
+    if (color == TC_COLOR_RCT || color == TC_COLOR_ICT)
+        return run_last<int32_t, 0, TC_ROUND_FLOOR, TC_COLOR_RCT>(ctx, io, out_type, bits);
+    return run_last<int32_t, 0, TC_ROUND_FLOOR, TC_COLOR_DC>(ctx, io, out_type, bits);
+}
+
+}  // namespace tc

@@ -61,11 +61,15 @@ struct tc_ctx {
     // side streams for concurrent Tier-1 class launches (created on first use)
     cudaStream_t side[2] = {nullptr, nullptr};
     cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
+    // stream that plan graphs are captured on (the caller's stream may be the
+    // legacy default stream, which cannot be captured)
+    cudaStream_t capture = nullptr;
 };
 
 namespace tc {
 
-// Creates the context's side streams and fork/join events if needed.
+// Creates the context's side streams, capture stream and fork/join events
+// if needed.
 cudaError_t ensure_side_streams(tc_ctx *ctx);
 // Records a message on the context and returns the status.
 int fail(tc_ctx *ctx, int status, const std::string &msg);
