@@ -340,75 +340,77 @@ def run_ours(args, rank, world, local_rank):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
 
-    # batched (one plan: one Tier-1 queue over every image) vs per-image plans
-    mixed = make_mixed()
-    streams = [cs_ for _, cs_ in mixed]
-    mpx_mixed = sum(im.shape[1] * im.shape[2] for im, _ in mixed) / 1e6
-    bplan = Plan(ctx, streams)
-    bouts = bplan.alloc_outputs()
-    bplan.set_graph(True)   # the batched path replays one captured graph per shape bucket
-    pplans = [Plan(ctx, [s_]) for s_ in streams]
-    pouts = [p_.alloc_outputs() for p_ in pplans]
-    mixed_steps = max(3, min(args.steps, 10))
+    batched, served = None, None
+    if not args.core_only:
+        # batched (one plan: one Tier-1 queue over every image) vs per-image plans
+        mixed = make_mixed()
+        streams = [cs_ for _, cs_ in mixed]
+        mpx_mixed = sum(im.shape[1] * im.shape[2] for im, _ in mixed) / 1e6
+        bplan = Plan(ctx, streams)
+        bouts = bplan.alloc_outputs()
+        bplan.set_graph(True)   # the batched path replays one captured graph per shape bucket
+        pplans = [Plan(ctx, [s_]) for s_ in streams]
+        pouts = [p_.alloc_outputs() for p_ in pplans]
+        mixed_steps = max(3, min(args.steps, 10))
 
-    def timed(fn, steps):
-        ms, lat = [], []
-        with torch.cuda.stream(stream):
-            for _ in range(2):
-                fn(None)
-            for k in range(steps):
-                flush.fill_(k & 0xFF)
-                a_, b_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                a_.record(stream)
-                fn(lat)
-                b_.record(stream)
-                ms.append((a_, b_))
-        torch.cuda.synchronize()
-        return sum(x.elapsed_time(y) for x, y in ms) / steps, lat
+        def timed(fn, steps):
+            ms, lat = [], []
+            with torch.cuda.stream(stream):
+                for _ in range(2):
+                    fn(None)
+                for k in range(steps):
+                    flush.fill_(k & 0xFF)
+                    a_, b_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    a_.record(stream)
+                    fn(lat)
+                    b_.record(stream)
+                    ms.append((a_, b_))
+            torch.cuda.synchronize()
+            return sum(x.elapsed_time(y) for x, y in ms) / steps, lat
 
-    def run_batched(lat):
-        bplan.execute(bouts)
+        def run_batched(lat):
+            bplan.execute(bouts)
 
-    def run_per_image(lat):
-        for p_, o_ in zip(pplans, pouts):
-            if lat is not None:
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-                p_.execute(o_)
-                e1.record(stream)
-                lat.append((e0, e1))
+        def run_per_image(lat):
+            for p_, o_ in zip(pplans, pouts):
+                if lat is not None:
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    p_.execute(o_)
+                    e1.record(stream)
+                    lat.append((e0, e1))
+                else:
+                    p_.execute(o_)
+
+        b_ms, _ = timed(run_batched, mixed_steps)
+        p_ms, p_lat = timed(run_per_image, mixed_steps)
+        lat_ms = sorted(x.elapsed_time(y) for x, y in p_lat)
+        ctx.synchronize()
+        lossless_exact, lossy_psnr = True, []
+        for i, ((im, _), o_) in enumerate(zip(mixed, bouts)):
+            got = o_.cpu().numpy()
+            if im.dtype == np.uint16:
+                got = got.view(np.uint16)
+            if i % 2 == 0:
+                lossless_exact &= bool(np.array_equal(got, im))
             else:
-                p_.execute(o_)
+                mx_ = float((1 << (12 if im.dtype == np.uint16 else 8)) - 1)
+                d_ = got.astype(np.float64) - im.astype(np.float64)
+                lossy_psnr.append(10 * np.log10(mx_ * mx_ / max(float(np.mean(d_ * d_)), 1e-12)))
+        batched = {"images": len(mixed), "mpixels": round(mpx_mixed, 3),
+                   "batched_mpix_s": round(mpx_mixed / (b_ms / 1000.0), 2),
+                   "per_image_mpix_s": round(mpx_mixed / (p_ms / 1000.0), 2),
+                   "speedup": round(p_ms / b_ms, 3),
+                   "per_image_latency_ms": {"p50": round(lat_ms[len(lat_ms) // 2], 3),
+                                            "p99": round(lat_ms[min(len(lat_ms) - 1, int(0.99 * len(lat_ms)))], 3)},
+                   "lossless_bit_exact": lossless_exact, "lossy_min_psnr_db": round(min(lossy_psnr), 2),
+                   "workload": "mixed sizes 256-2048 step 16, 1/3 comps, 8/12-bit, half 5/3 lossless, half 9/7 lossy"}
+        bplan.close()
+        for p_ in pplans:
+            p_.close()
 
-    b_ms, _ = timed(run_batched, mixed_steps)
-    p_ms, p_lat = timed(run_per_image, mixed_steps)
-    lat_ms = sorted(x.elapsed_time(y) for x, y in p_lat)
-    ctx.synchronize()
-    lossless_exact, lossy_psnr = True, []
-    for i, ((im, _), o_) in enumerate(zip(mixed, bouts)):
-        got = o_.cpu().numpy()
-        if im.dtype == np.uint16:
-            got = got.view(np.uint16)
-        if i % 2 == 0:
-            lossless_exact &= bool(np.array_equal(got, im))
-        else:
-            mx_ = float((1 << (12 if im.dtype == np.uint16 else 8)) - 1)
-            d_ = got.astype(np.float64) - im.astype(np.float64)
-            lossy_psnr.append(10 * np.log10(mx_ * mx_ / max(float(np.mean(d_ * d_)), 1e-12)))
-    batched = {"images": len(mixed), "mpixels": round(mpx_mixed, 3),
-               "batched_mpix_s": round(mpx_mixed / (b_ms / 1000.0), 2),
-               "per_image_mpix_s": round(mpx_mixed / (p_ms / 1000.0), 2),
-               "speedup": round(p_ms / b_ms, 3),
-               "per_image_latency_ms": {"p50": round(lat_ms[len(lat_ms) // 2], 3),
-                                        "p99": round(lat_ms[min(len(lat_ms) - 1, int(0.99 * len(lat_ms)))], 3)},
-               "lossless_bit_exact": lossless_exact, "lossy_min_psnr_db": round(min(lossy_psnr), 2),
-               "workload": "mixed sizes 256-2048 step 16, 1/3 comps, 8/12-bit, half 5/3 lossless, half 9/7 lossy"}
-    bplan.close()
-    for p_ in pplans:
-        p_.close()
-
-    # served decode: Poisson arrivals, continuous batching vs the per-image path
-    served = serve_section(args, mixed, local_rank)
+        # served decode: Poisson arrivals, continuous batching vs the per-image path
+        served = serve_section(args, mixed, local_rank)
 
     if rank == 0:
         px = W * H
@@ -442,17 +444,18 @@ def run_ours(args, rank, world, local_rank):
                          "peak_kind": peak_kind,
                          "note": "Tier-1 is issue/latency bound (serial MQ decoding); bytes = codestream + 4 B per "
                                  "coefficient written"},
-            "dwt_roofline": {"bound": "hbm", "kernels": "idwt_level_kernel + idwt_last_color_kernel",
+            "dwt_roofline": {"bound": "hbm", "kernel": "idwt_rev_kernel (all levels)",
                              "achieved": round(dwt_gbs, 2), "peak": hbm, "unit": "GB/s",
                              "frac": round(dwt_gbs / hbm, 4), "bytes_per_step": dw_bytes, "peak_kind": peak_kind},
             "e2e": {"value": round(W * H * world / e2e_s / 1e6, 2), "unit": "Mpixel/s",
                     "h2d_bytes_per_step": pool_bytes + 40 * ncblk + 4 * ncblk,
                     "d2h_bytes_per_step": int(host_out.nbytes), "api": "tc_decode_j2k"},
-            "batched_vs_per_image": batched,
-            "served": served,
             "gpu_launches": int(launches), "clocks": clocks, "psnr_db": round(psnr, 2),
             "wall_s_timed_region": round(wall, 3),
         }
+        if batched is not None:
+            line["batched_vs_per_image"] = batched
+            line["served"] = served
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(os.cpu_count() or 1)
         print(json.dumps(line), flush=True)
@@ -470,6 +473,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--core-only", action="store_true",
+                    help="report the headline workload only (no batched or served sections)")
     ap.add_argument("--serve-rate", type=float, default=200.0, help="served decode: Poisson arrivals per second")
     ap.add_argument("--serve-requests", type=int, default=64)
     ap.add_argument("--size", type=int, default=0,

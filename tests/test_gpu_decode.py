@@ -60,6 +60,35 @@ def test_lossy_decode_vs_oracle(gpu_ctx, w, h, levels):
     assert 10 * np.log10(255 ** 2 / mse) > 40
 
 
+def _smooth_image(w, h, seed):
+    """12-bit gradients plus +-2 noise: the detail bands code in a few
+    bit-planes, the low band in about twelve."""
+    rng = np.random.default_rng(seed)
+    y, x = np.mgrid[0:h, 0:w]
+    base = np.stack([x * 3800 // w, y * 3800 // h, (x + y) * 1900 // (w + h)])
+    return (base + 100 + rng.integers(-2, 3, (3, h, w))).astype(np.uint16)
+
+
+def test_few_deep_blocks_ride_with_bulk(gpu_ctx):
+    """A handful of blocks with more than 8 coded bit-planes among hundreds
+    with fewer: the deep ones are decoded inside the 8-bit launch by the
+    heavy decoders.  Lossless, so the output must equal the input."""
+    from thousandthchicken_b200.stages import Plan
+    img = _smooth_image(1024, 768, 11)
+    cs = codec.encode(img, 12, levels=5, reversible=True, mct=True)
+    _, desc, _ = codec.parse(cs)
+    nb = desc["mb"].astype(int) - desc["zero_bitplanes"].astype(int)
+    n16 = int(((nb > 8) & (nb <= 16)).sum())
+    assert int((nb <= 8).sum()) > 100 and 0 < n16 <= 64, (n16, np.bincount(nb))
+    np.testing.assert_array_equal(_decoder(gpu_ctx).decode(cs), img)
+    plan = Plan(gpu_ctx, [cs, cs])
+    outs = plan.execute(plan.alloc_outputs())
+    gpu_ctx.synchronize()
+    for o in outs:
+        np.testing.assert_array_equal(o.cpu().numpy().view(np.uint16), img)
+    plan.close()
+
+
 def test_batched_plan_equals_single_decodes(gpu_ctx):
     from thousandthchicken_b200.stages import Plan
     streams = [codec.encode(synth_image(300, 200, 3, 8, 1), 8, levels=5, reversible=True),

@@ -6,18 +6,24 @@
 // memory, with whole-sample symmetric extension (ISO F.3.7; the reference's
 // single reflection, dwt_io.cl:7-38, is defect D14), then
 //   * horizontal lifting: each thread lifts one 32-sample segment of one row
-//     (plus its halo) entirely in registers, fully unrolled;
-//   * vertical lifting: each thread lifts one 64-sample column in registers;
+//     (plus its halo) entirely in registers, fully unrolled, reading and
+//     writing it with 16-byte shared-memory accesses;
+//   * vertical lifting: each thread lifts one 64-sample column in registers
+//     and stores it (coalesced across the warp);
 // so every lifting step is register arithmetic with constant indices and the
 // CTA synchronises only between phases.  The row stride in shared memory is
-// odd, so threads walking different rows hit different banks.
+// a multiple of four words with an odd quotient, so threads walking
+// different rows hit different banks.
 //
 // COLOR >= 0 fuses the inverse RCT/ICT, DC shift, rounding and clamp into the
 // store of the last level (the reference's tcr_kernel / tci_kernel /
-// idc_level_shift_kernel, Preprocessor.cpp:44-180), writing 8/16-bit samples.
-// The ISO 2D_SR order is kept: rows first, then columns (DWTReverse53/97,
-// dwt_r53.cl / dwt_r97.cl).
+// idc_level_shift_kernel, Preprocessor.cpp:44-180), writing 8/16-bit samples:
+// the last component's column is combined in registers with the other two,
+// parked in shared memory.  The ISO 2D_SR order is kept: rows first, then
+// columns (DWTReverse53/97, dwt_r53.cl / dwt_r97.cl).
 #include <cuda_runtime.h>
+
+#include <type_traits>
 
 #include "dwt_common.cuh"
 #include "tc_internal.cuh"
@@ -36,7 +42,10 @@ struct RevGeo {
     static constexpr int TY = NR - 2 * H;         // output rows per tile
     static constexpr int TX = 128;                // output columns per tile
     static constexpr int NC = TX + 2 * H;         // extended columns
-    static constexpr int S = NC + 1;              // odd row stride (bank spread)
+    // row stride: a multiple of 4 words (16-byte rows for 128-bit access)
+    // with S/4 odd, so 8 threads reading 16 bytes each from 8 consecutive
+    // rows cover all 32 banks once
+    static constexpr int S = (NC % 8 == 4) ? NC : NC + 4;
     static constexpr int SEG = 32;                // outputs per row segment
     static constexpr int SEGN = SEG + 2 * H;      // inputs per row segment
 };
@@ -83,6 +92,17 @@ __device__ __forceinline__ OT clamp_out(int v, int mx)
     return (OT)(v < 0 ? 0 : (v > mx ? mx : v));
 }
 
+template <typename T>
+__device__ __forceinline__ int to_int(T v)
+{
+    if constexpr (std::is_same<T, float>::value) return __float2int_rn(v);
+    else return (int)v;
+}
+
+// 16-byte vector of four T (T is int32_t or float).
+template <typename T>
+using Vec4 = typename std::conditional<std::is_same<T, float>::value, float4, int4>::type;
+
 template <typename T, int WAVELET, int RND, int NCOMP, int COLOR, typename OT>
 __global__ void __launch_bounds__(kThreads) idwt_rev_kernel(LevelIO io, int bits)
 {
@@ -99,27 +119,47 @@ __global__ void __launch_bounds__(kThreads) idwt_rev_kernel(LevelIO io, int bits
 
     // 1. load the extended tiles from the four subbands (Mallat layout) with
     //    4-byte asynchronous copies, so a thread has its whole share of the
-    //    tile in flight at once
+    //    tile in flight at once.  x0 - H is even, so the parity of a column
+    //    is the parity of the lane: inside the plane a lane's sources in a
+    //    row are one strided run of the low or the high band.
+    const bool interior = x0 >= H && x0 + TX + H <= w && y0 >= H && y0 + NR - H <= h;
 #pragma unroll
     for (int cc = 0; cc < NT; cc++) {
         T *t = tiles + cc * NR * S;
         const T *ll = static_cast<const T *>(io.ll[cbase + cc]);
         const T *coef = static_cast<const T *>(io.coef[cbase + cc]);
-        for (int r = warp; r < NR; r += kThreads / 32) {
-            const int my = mirror(y0 - H + r, h), yb = my >> 1;
-            const T *lrow = (my & 1) ? coef + (size_t)(hl + yb) * io.coef_pitch : ll + (size_t)yb * io.ll_pitch;
-            const T *hrow = coef + (size_t)((my & 1) ? hl + yb : yb) * io.coef_pitch + wl;
+        if (interior) {
+            const int xs = ((x0 - H) >> 1) + (lane >> 1);
+            for (int r = warp; r < NR; r += kThreads / 32) {
+                const int y = y0 - H + r, yb = y >> 1;
+                const T *src = (y & 1) ? coef + (size_t)(hl + yb) * io.coef_pitch + ((lane & 1) ? wl : 0)
+                                       : ((lane & 1) ? coef + (size_t)yb * io.coef_pitch + wl
+                                                     : ll + (size_t)yb * io.ll_pitch);
+                src += xs;
+                T *dst = t + r * S + lane;
 #pragma unroll
-            for (int e = lane; e < NC; e += 32) {
-                const int mx = mirror(x0 - H + e, w);
-                cp_async4(t + r * S + e, ((mx & 1) ? hrow : lrow) + (mx >> 1));
+                for (int j = 0; j < NC / 32; j++) cp_async4(dst + 32 * j, src + 16 * j);
+                if (lane < NC % 32) cp_async4(dst + 32 * (NC / 32), src + 16 * (NC / 32));
+            }
+        } else {
+            for (int r = warp; r < NR; r += kThreads / 32) {
+                const int my = mirror(y0 - H + r, h), yb = my >> 1;
+                const T *lrow = (my & 1) ? coef + (size_t)(hl + yb) * io.coef_pitch : ll + (size_t)yb * io.ll_pitch;
+                const T *hrow = coef + (size_t)((my & 1) ? hl + yb : yb) * io.coef_pitch + wl;
+#pragma unroll
+                for (int e = lane; e < NC; e += 32) {
+                    const int mx = mirror(x0 - H + e, w);
+                    cp_async4(t + r * S + e, ((mx & 1) ? hrow : lrow) + (mx >> 1));
+                }
             }
         }
     }
     cp_async_wait_all();
     __syncthreads();
 
-    // 2. horizontal lifting, one row segment per thread, two rounds of 32 rows
+    // 2. horizontal lifting, one row segment per thread, two rounds of 32
+    //    rows; segments are read and written with 16-byte (8-byte for the
+    //    2-sample halo of 5/3) shared-memory accesses
     if (w > 1) {
         const int seg = tid >> 5;  // 4 segments of 32 outputs per row
 #pragma unroll
@@ -128,20 +168,50 @@ __global__ void __launch_bounds__(kThreads) idwt_rev_kernel(LevelIO io, int bits
 #pragma unroll 1
             for (int round = 0; round < NR / 32; round++) {
                 const int r = round * 32 + lane;
+                T *row = t + r * S + seg * G::SEG;
                 T v[G::SEGN];
 #pragma unroll
-                for (int k = 0; k < G::SEGN; k++) v[k] = t[r * S + seg * G::SEG + k];
+                for (int k = 0; k < G::SEGN; k += 4) {
+                    const Vec4<T> q = *reinterpret_cast<const Vec4<T> *>(row + k);
+                    v[k] = q.x;
+                    v[k + 1] = q.y;
+                    v[k + 2] = q.z;
+                    v[k + 3] = q.w;
+                }
                 __syncthreads();  // neighbouring segments overlap: all reads before any write
                 lift_reverse<T, WAVELET, RND, G::SEGN>(v);
+                if constexpr (H % 4 == 0) {
 #pragma unroll
-                for (int k = H; k < H + G::SEG; k++) t[r * S + seg * G::SEG + k] = v[k];
+                    for (int k = H; k < H + G::SEG; k += 4) {
+                        Vec4<T> q;
+                        q.x = v[k];
+                        q.y = v[k + 1];
+                        q.z = v[k + 2];
+                        q.w = v[k + 3];
+                        *reinterpret_cast<Vec4<T> *>(row + k) = q;
+                    }
+                } else {
+                    using V2 = typename std::conditional<std::is_same<T, float>::value, float2, int2>::type;
+#pragma unroll
+                    for (int k = H; k < H + G::SEG; k += 2) {
+                        V2 q;
+                        q.x = v[k];
+                        q.y = v[k + 1];
+                        *reinterpret_cast<V2 *>(row + k) = q;
+                    }
+                }
             }
         }
         __syncthreads();
     }
 
-    // 3. vertical lifting, one column per thread
+    // 3. vertical lifting, one column per thread, and the store.  With a
+    //    colour transform the first two components are parked back in their
+    //    tiles (each thread only touches its own column, so no barrier) and
+    //    the third one's column is combined with them straight from registers.
     const int col = tid, x = x0 + col;
+    const bool full_rows = y0 + TY <= h;
+    const int dc = PLANE ? 0 : 1 << (bits - 1), mx = PLANE ? 0 : (1 << bits) - 1;
 #pragma unroll
     for (int cc = 0; cc < NT; cc++) {
         T *t = tiles + cc * NR * S;
@@ -149,49 +219,45 @@ __global__ void __launch_bounds__(kThreads) idwt_rev_kernel(LevelIO io, int bits
 #pragma unroll
         for (int r = 0; r < NR; r++) v[r] = t[r * S + H + col];
         if (h > 1) lift_reverse<T, WAVELET, RND, NR>(v);
+        if (x >= w) continue;
         if constexpr (PLANE) {
-            T *out = static_cast<T *>(io.out[cbase]);
-            if (x < w) {
+            T *out = static_cast<T *>(io.out[cbase]) + (size_t)y0 * io.out_pitch + x;
 #pragma unroll
-                for (int r = 0; r < TY; r++)
-                    if (y0 + r < h) out[(size_t)(y0 + r) * io.out_pitch + x] = v[H + r];
-            }
-        } else {
+            for (int r = 0; r < TY; r++)
+                if (full_rows || y0 + r < h) out[(size_t)r * io.out_pitch] = v[H + r];
+        } else if (COLOR == TC_COLOR_DC || cc >= 3) {
+            OT *out = static_cast<OT *>(io.out[cc]) + (size_t)y0 * io.out_pitch + x;
+#pragma unroll
+            for (int r = 0; r < TY; r++)
+                if (full_rows || y0 + r < h) out[(size_t)r * io.out_pitch] = clamp_out<OT>(to_int(v[H + r]) + dc, mx);
+        } else if (cc < 2) {
 #pragma unroll
             for (int r = 0; r < TY; r++) t[(H + r) * S + H + col] = v[H + r];
-        }
-    }
-
-    // 4. fused inverse colour transform, DC shift, rounding and clamp
-    if constexpr (!PLANE) {
-        __syncthreads();
-        const int dc = 1 << (bits - 1), mx = (1 << bits) - 1;
-        for (int q = tid; q < TX * TY; q += kThreads) {
-            const int r = q / TX, cx = q % TX;
-            const int y = y0 + r, xx = x0 + cx;
-            if (y >= h || xx >= w) continue;
-            const int ci = (H + r) * S + H + cx;
-            const size_t o = (size_t)y * io.out_pitch + xx;
-            int vv[NCOMP];
-            if constexpr (COLOR == TC_COLOR_RCT) {
-                const int Y = (int)tiles[ci], U = (int)tiles[NR * S + ci], V = (int)tiles[2 * NR * S + ci];
-                const int Gc = Y - ((U + V) >> 2);
-                vv[0] = V + Gc;
-                vv[1] = Gc;
-                vv[2] = U + Gc;
-            } else if constexpr (COLOR == TC_COLOR_ICT) {
-                const float Y = (float)tiles[ci], Cb = (float)tiles[NR * S + ci], Cr = (float)tiles[2 * NR * S + ci];
-                vv[0] = __float2int_rn(fmaf(1.402f, Cr, Y));
-                vv[1] = __float2int_rn(Y - 0.34413f * Cb - 0.71414f * Cr);
-                vv[2] = __float2int_rn(fmaf(1.772f, Cb, Y));
-            }
+        } else {
+            const T *t0 = tiles + (H * S + H + col), *t1 = tiles + (NR * S + H * S + H + col);
+            const size_t o = (size_t)y0 * io.out_pitch + x;
+            OT *o0 = static_cast<OT *>(io.out[0]) + o, *o1 = static_cast<OT *>(io.out[1]) + o,
+               *o2 = static_cast<OT *>(io.out[2]) + o;
 #pragma unroll
-            for (int c = 0; c < NCOMP; c++) {
-                int sv;
-                if (COLOR != TC_COLOR_DC && c < 3) sv = vv[c];
-                else if constexpr (WAVELET == 0) sv = (int)tiles[c * NR * S + ci];
-                else sv = __float2int_rn((float)tiles[c * NR * S + ci]);
-                static_cast<OT *>(io.out[c])[o] = clamp_out<OT>(sv + dc, mx);
+            for (int r = 0; r < TY; r++) {
+                if (!(full_rows || y0 + r < h)) continue;
+                int c0, c1, c2;
+                if constexpr (COLOR == TC_COLOR_RCT) {
+                    const int Y = (int)t0[r * S], U = (int)t1[r * S], V = (int)v[H + r];
+                    const int Gc = Y - ((U + V) >> 2);
+                    c0 = V + Gc;
+                    c1 = Gc;
+                    c2 = U + Gc;
+                } else {
+                    const float Y = (float)t0[r * S], Cb = (float)t1[r * S], Cr = (float)v[H + r];
+                    c0 = __float2int_rn(fmaf(1.402f, Cr, Y));
+                    c1 = __float2int_rn(Y - 0.34413f * Cb - 0.71414f * Cr);
+                    c2 = __float2int_rn(fmaf(1.772f, Cb, Y));
+                }
+                const size_t ro = (size_t)r * io.out_pitch;
+                o0[ro] = clamp_out<OT>(c0 + dc, mx);
+                o1[ro] = clamp_out<OT>(c1 + dc, mx);
+                o2[ro] = clamp_out<OT>(c2 + dc, mx);
             }
         }
     }

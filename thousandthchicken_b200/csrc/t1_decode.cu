@@ -28,6 +28,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
+#include <type_traits>
 
 #include "tc_internal.cuh"
 
@@ -463,11 +465,102 @@ struct GroupCfg {
     static constexpr int warps = G == 32 ? 4 : (G == 16 ? 2 : 1);
 };
 
+// Decode code-block `bi` with the state S and write it out (the group's
+// lanes, in lock-step).  MagT bounds the coded bit-planes it accepts.
+template <typename MagT, int G>
+__device__ __forceinline__ void process_block(WarpState<MagT> &S, const Tables &T, const tc_cblk_desc *__restrict__ desc,
+                                              uint32_t bi, int ndesc, const uint8_t *__restrict__ pool,
+                                              uint64_t pool_len, char *__restrict__ out, int out_mode, float recon_r,
+                                              uint32_t *__restrict__ err, int gl, unsigned gmask, int gshift)
+{
+    if (bi >= (uint32_t)ndesc) {
+        if (gl == 0) atomicOr(err, TC_DERR_DESC);
+        return;
+    }
+    const tc_cblk_desc d = desc[bi];
+    const int w = d.w, h = d.h;
+    const bool geom_ok = w >= 1 && w <= 64 && h >= 1 && h <= 64;
+    const int numbps = (int)d.mb - (int)d.zero_bitplanes;
+    bool ok = geom_ok && d.mb >= 1 && d.mb <= 31 && d.orient <= 3 && numbps >= 0 &&
+              (numbps == 0 || d.passes <= 3 * numbps - 2) && numbps <= (int)(8 * sizeof(MagT));
+    const bool pool_ok = d.seg_off <= pool_len && (uint64_t)d.seg_len <= pool_len - d.seg_off;
+    if (!geom_ok) {
+        if (gl == 0) atomicOr(err, TC_DERR_DESC);
+        return;
+    }
+    if (!ok || !pool_ok) {
+        if (gl == 0) atomicOr(err, ok ? TC_DERR_POOL : TC_DERR_DESC);
+        ok = false;
+    }
+    const bool coded = ok && numbps > 0 && d.passes > 0;
+    const int nstripes = (h + 3) >> 2;
+
+    // clear the state (the group's lanes)
+    for (int i = gl; i < nstripes * 64; i += G) S.F[i] = 0u;
+    for (int i = gl; i < kSgnCols; i += G) S.sgn[i] = 0ull;
+    for (int i = gl; i < 19; i += G) {
+        const int st = i == 0 ? 4 : (i == 17 ? 46 : (i == 18 ? 3 : 0));
+        S.ctx[i] = T.mq[st];
+    }
+    __syncwarp(gmask);
+
+    int type = 0, last_plane = 0;
+    if (coded)
+        type = decode_block<MagT, G>(S, T, pool + d.seg_off, (int)d.seg_len, w, h, d.orient, numbps, d.passes,
+                                     &last_plane, gl, gmask, gshift);
+    __syncwarp(gmask);
+
+    // epilogue: reconstruction + inverse quantisation, coalesced rows
+    const bool irrev = (d.flags & TC_CBLK_IRREVERSIBLE) != 0;
+    for (int y = 0; y < h; y++) {
+        char *row = out + 4 * (d.out_off + (uint64_t)y * d.out_pitch);
+        const int s = y >> 2, k = y & 3;
+        for (int x = gl; x < w; x += G) {
+            const uint32_t f = coded ? S.F[s * 64 + x] : 0u;
+            const bool sg = (f & self_bit(k)) != 0u;
+            uint32_t mg = 0, neg = 0, u = 0;
+            if (sg) {
+                mg = (uint32_t)S.mag[y * 64 + x];
+                neg = (uint32_t)(S.sgn[x + 1] >> y) & 1u;
+                u = (uint32_t)last_plane;
+                if (type == 1 && !(f & pi_bit(k))) u++;
+            }
+            if (out_mode == TC_T1_OUT_RAW) {
+                reinterpret_cast<uint32_t *>(row)[x] = sg ? ((mg << (31 - d.mb)) | (neg << 31)) : 0u;
+            } else if (irrev) {
+                float v = 0.0f;
+                if (sg) v = ((float)mg + recon_r * (float)(1u << u)) * d.step;
+                reinterpret_cast<float *>(row)[x] = neg ? -v : v;
+            } else {
+                int32_t v = 0;
+                if (sg) v = (int32_t)mg + (u ? (int32_t)floorf(recon_r * (float)(1u << u)) : 0);
+                reinterpret_cast<int32_t *>(row)[x] = neg ? -v : v;
+            }
+        }
+    }
+    __syncwarp(gmask);
+}
+
+// Persistent Tier-1 launch over one magnitude class.  The 8-bit class with
+// 32-lane groups can also take a short queue of 16-bit blocks (`heavy`): the
+// first `heavy_ctas` CTAs turn warps 0 and 2 into 16-bit decoders that use
+// their own and their partner warp's state memory (warps 1 and 3 stand
+// down), drain the heavy queue first and then join the 8-bit queue.  A few
+// blocks with many bit-planes thus start at once, in the same longest-first
+// launch as the bulk, instead of running as a separate class whose warps
+// share SMs with the bulk and become the launch's longest chain.
+struct HeavyQueue {
+    const uint32_t *order = nullptr;
+    int n = 0;
+    int ctas = 0;
+    uint32_t *counter = nullptr;
+};
+
 template <typename MagT, int G>
 __global__ void __launch_bounds__(32 * GroupCfg<G>::warps)
 t1_decode_kernel(const tc_cblk_desc *__restrict__ desc, const uint32_t *__restrict__ order, int n, int ndesc,
                  const uint8_t *__restrict__ pool, uint64_t pool_len, char *__restrict__ out, int out_mode,
-                 float recon_r, uint32_t *__restrict__ counter, uint32_t *__restrict__ err)
+                 float recon_r, uint32_t *__restrict__ counter, uint32_t *__restrict__ err, HeavyQueue heavy)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     Tables &T = *reinterpret_cast<Tables *>(smem);
@@ -480,7 +573,24 @@ t1_decode_kernel(const tc_cblk_desc *__restrict__ desc, const uint32_t *__restri
     const int gidx = wl / G, gl = wl % G;         // group in the warp, lane in the group
     const int gshift = gidx * G;
     const unsigned gmask = G == 32 ? 0xffffffffu : (((1u << G) - 1u) << gshift);
-    WarpState<MagT> &S = states[(threadIdx.x >> 5) * (32 / G) + gidx];
+    const int slot = (threadIdx.x >> 5) * (32 / G) + gidx;
+    WarpState<MagT> &S = states[slot];
+
+    if constexpr (std::is_same<MagT, uint8_t>::value && G == 32) {
+        static_assert(sizeof(WarpState<uint16_t>) <= 2 * sizeof(WarpState<uint8_t>), "heavy state spans two slots");
+        if ((int)blockIdx.x < heavy.ctas) {
+            if (slot & 1) return;  // lends its state to warp slot - 1
+            WarpState<uint16_t> &HS = *reinterpret_cast<WarpState<uint16_t> *>(&states[slot]);
+            for (;;) {
+                int idx = 0;
+                if (wl == 0) idx = (int)atomicAdd(heavy.counter, 1u);
+                idx = __shfl_sync(0xffffffffu, idx, 0);
+                if (idx >= heavy.n) break;
+                process_block<uint16_t, 32>(HS, T, desc, heavy.order[idx], ndesc, pool, pool_len, out, out_mode,
+                                            recon_r, err, gl, gmask, gshift);
+            }
+        }
+    }
 
     for (;;) {
         int idx = 0;
@@ -488,72 +598,8 @@ t1_decode_kernel(const tc_cblk_desc *__restrict__ desc, const uint32_t *__restri
         idx = __shfl_sync(gmask, idx, gshift);
         if (idx >= n) break;
         const uint32_t bi = order ? order[idx] : (uint32_t)idx;
-        if (bi >= (uint32_t)ndesc) {
-            if (gl == 0) atomicOr(err, TC_DERR_DESC);
-            continue;
-        }
-        const tc_cblk_desc d = desc[bi];
-        const int w = d.w, h = d.h;
-        const bool geom_ok = w >= 1 && w <= 64 && h >= 1 && h <= 64;
-        const int numbps = (int)d.mb - (int)d.zero_bitplanes;
-        bool ok = geom_ok && d.mb >= 1 && d.mb <= 31 && d.orient <= 3 && numbps >= 0 &&
-                  (numbps == 0 || d.passes <= 3 * numbps - 2) && numbps <= (int)(8 * sizeof(MagT));
-        const bool pool_ok = d.seg_off <= pool_len && (uint64_t)d.seg_len <= pool_len - d.seg_off;
-        if (!geom_ok) {
-            if (gl == 0) atomicOr(err, TC_DERR_DESC);
-            continue;
-        }
-        if (!ok || !pool_ok) {
-            if (gl == 0) atomicOr(err, ok ? TC_DERR_POOL : TC_DERR_DESC);
-            ok = false;
-        }
-        const bool coded = ok && numbps > 0 && d.passes > 0;
-        const int nstripes = (h + 3) >> 2;
-
-        // clear the state (the group's lanes)
-        for (int i = gl; i < nstripes * 64; i += G) S.F[i] = 0u;
-        for (int i = gl; i < kSgnCols; i += G) S.sgn[i] = 0ull;
-        for (int i = gl; i < 19; i += G) {
-            const int st = i == 0 ? 4 : (i == 17 ? 46 : (i == 18 ? 3 : 0));
-            S.ctx[i] = T.mq[st];
-        }
-        __syncwarp(gmask);
-
-        int type = 0, last_plane = 0;
-        if (coded)
-            type = decode_block<MagT, G>(S, T, pool + d.seg_off, (int)d.seg_len, w, h, d.orient, numbps, d.passes,
-                                         &last_plane, gl, gmask, gshift);
-        __syncwarp(gmask);
-
-        // epilogue: reconstruction + inverse quantisation, coalesced rows
-        const bool irrev = (d.flags & TC_CBLK_IRREVERSIBLE) != 0;
-        for (int y = 0; y < h; y++) {
-            char *row = out + 4 * (d.out_off + (uint64_t)y * d.out_pitch);
-            const int s = y >> 2, k = y & 3;
-            for (int x = gl; x < w; x += G) {
-                const uint32_t f = coded ? S.F[s * 64 + x] : 0u;
-                const bool sg = (f & self_bit(k)) != 0u;
-                uint32_t mg = 0, neg = 0, u = 0;
-                if (sg) {
-                    mg = (uint32_t)S.mag[y * 64 + x];
-                    neg = (uint32_t)(S.sgn[x + 1] >> y) & 1u;
-                    u = (uint32_t)last_plane;
-                    if (type == 1 && !(f & pi_bit(k))) u++;
-                }
-                if (out_mode == TC_T1_OUT_RAW) {
-                    reinterpret_cast<uint32_t *>(row)[x] = sg ? ((mg << (31 - d.mb)) | (neg << 31)) : 0u;
-                } else if (irrev) {
-                    float v = 0.0f;
-                    if (sg) v = ((float)mg + recon_r * (float)(1u << u)) * d.step;
-                    reinterpret_cast<float *>(row)[x] = neg ? -v : v;
-                } else {
-                    int32_t v = 0;
-                    if (sg) v = (int32_t)mg + (u ? (int32_t)floorf(recon_r * (float)(1u << u)) : 0);
-                    reinterpret_cast<int32_t *>(row)[x] = neg ? -v : v;
-                }
-            }
-        }
-        __syncwarp(gmask);
+        process_block<MagT, G>(S, T, desc, bi, ndesc, pool, pool_len, out, out_mode, recon_r, err, gl, gmask,
+                               gshift);
     }
 }
 
@@ -595,53 +641,52 @@ __global__ void dequant_raw_kernel(const tc_cblk_desc *__restrict__ desc, int n,
 
 struct LaunchCfg {
     bool ready = false;
-    int per_sm = 1;
-    size_t smem = 0;
+    int per_sm = 1;    // resident CTAs per SM
+    int per_cta = 4;   // code-blocks in flight per CTA
+    size_t smem = 0;   // dynamic shared memory per CTA
 };
 
+// Kernel attributes and occupancy of one class variant, set up once per device.
 template <typename MagT, int G>
-cudaError_t launch_class(tc_ctx *ctx, cudaStream_t stream, const tc_cblk_desc *d_desc, const uint32_t *d_order,
-                         int n, int ndesc, const uint8_t *d_pool, uint64_t pool_len, void *d_out, int out_mode,
-                         float recon_r, int slot)
+cudaError_t class_cfg(tc_ctx *ctx, LaunchCfg **out)
 {
-    constexpr int kWarps = GroupCfg<G>::warps, kGroup = G;
+    constexpr int kWarps = GroupCfg<G>::warps;
     static LaunchCfg cfg[64];
     LaunchCfg &C = cfg[ctx->device & 63];
     if (!C.ready) {
-        C.smem = ((sizeof(Tables) + 15) & ~size_t(15)) + kWarps * (32 / kGroup) * sizeof(WarpState<MagT>);
-        cudaError_t e = cudaFuncSetAttribute(t1_decode_kernel<MagT, kGroup>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C.smem);
+        C.smem = ((sizeof(Tables) + 15) & ~size_t(15)) + kWarps * (32 / G) * sizeof(WarpState<MagT>);
+        C.per_cta = kWarps * (32 / G);
+        cudaError_t e = cudaFuncSetAttribute(t1_decode_kernel<MagT, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)C.smem);
         if (e != cudaSuccess) return e;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&C.per_sm, t1_decode_kernel<MagT, kGroup>, 32 * kWarps,
-                                                          C.smem);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&C.per_sm, t1_decode_kernel<MagT, G>, 32 * kWarps, C.smem);
         if (e != cudaSuccess) return e;
         if (C.per_sm < 1) C.per_sm = 1;
         C.ready = true;
     }
-    const int per_cta = kWarps * (32 / kGroup);
-    const int want = (n + per_cta - 1) / per_cta;
-    const int grid = std::min(want, C.per_sm * num_sms(ctx->device));
-    cudaError_t e = cudaMemsetAsync(ctx->d_words + slot, 0, sizeof(uint32_t), stream);
+    *out = &C;
+    return cudaSuccess;
+}
+
+// One class launch: a persistent grid pulling the class's blocks from its
+// work counter d_words[slot] (zeroed beforehand).
+template <typename MagT, int G>
+cudaError_t launch_class(tc_ctx *ctx, cudaStream_t stream, const tc_cblk_desc *d_desc, const uint32_t *d_order,
+                         int n, int ndesc, const uint8_t *d_pool, uint64_t pool_len, void *d_out, int out_mode,
+                         float recon_r, int slot, const HeavyQueue &heavy = HeavyQueue())
+{
+    LaunchCfg *C = nullptr;
+    cudaError_t e = class_cfg<MagT, G>(ctx, &C);
     if (e != cudaSuccess) return e;
-    t1_decode_kernel<MagT, kGroup><<<grid, 32 * kWarps, C.smem, stream>>>(d_desc, d_order, n, ndesc, d_pool, pool_len,
-                                                                   static_cast<char *>(d_out), out_mode, recon_r,
-                                                                   ctx->d_words + slot, ctx->d_words);
+    const int want = std::max((n + C->per_cta - 1) / C->per_cta, heavy.ctas);
+    const int grid = std::max(1, std::min(want, C->per_sm * num_sms(ctx->device)));
+    t1_decode_kernel<MagT, G><<<grid, 32 * GroupCfg<G>::warps, C->smem, stream>>>(
+        d_desc, d_order, n, ndesc, d_pool, pool_len, static_cast<char *>(d_out), out_mode, recon_r,
+        ctx->d_words + slot, ctx->d_words, heavy);
     ctx->launches++;
     return cudaGetLastError();
 }
 
-}  // namespace
-
-cudaError_t launch_t1_decode(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint32_t *d_order, int n,
-                             const uint8_t *d_pool, uint64_t pool_len, void *d_out, int out_mode, float recon_r,
-                             int max_bitplanes)
-{
-    return launch_t1_classes(ctx, d_desc, d_order, n, max_bitplanes <= 8 ? n : 0,
-                             max_bitplanes > 8 && max_bitplanes <= 16 ? n : 0, max_bitplanes > 16 ? n : 0, d_pool,
-                             pool_len, d_out, out_mode, recon_r);
-}
-
-namespace {
 template <typename MagT>
 cudaError_t launch_class_g(tc_ctx *ctx, cudaStream_t stream, const tc_cblk_desc *d_desc, const uint32_t *d_order,
                            int n, int ndesc, const uint8_t *d_pool, uint64_t pool_len, void *d_out, int out_mode,
@@ -659,17 +704,45 @@ cudaError_t launch_class_g(tc_ctx *ctx, cudaStream_t stream, const tc_cblk_desc 
                                       recon_r, slot);
     }
 }
+
+// Largest 16-bit class that rides along in the 8-bit launch (two heavy
+// decoders per CTA, so at most 32 CTAs, about 4% of a full grid, give up
+// half their warps).
+constexpr int kMaxHeavy = 64;
+
 }  // namespace
 
+cudaError_t launch_t1_decode(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint32_t *d_order, int n,
+                             const uint8_t *d_pool, uint64_t pool_len, void *d_out, int out_mode, float recon_r,
+                             int max_bitplanes)
+{
+    return launch_t1_classes(ctx, d_desc, d_order, n, max_bitplanes <= 8 ? n : 0,
+                             max_bitplanes > 8 && max_bitplanes <= 16 ? n : 0, max_bitplanes > 16 ? n : 0, d_pool,
+                             pool_len, d_out, out_mode, recon_r);
+}
+
+// Classes: blocks of <= 8, <= 16 and <= 31 coded bit-planes, in that order in
+// d_order (each slice longest first).  A short 16-bit class next to an 8-bit
+// bulk joins the 8-bit launch (see HeavyQueue); otherwise the classes run as
+// concurrent launches, the 32- and 16-bit ones on side streams.
 cudaError_t launch_t1_classes(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint32_t *d_order, int ndesc,
                               int n8, int n16, int n32, const uint8_t *d_pool, uint64_t pool_len, void *d_out,
                               int out_mode, float recon_r)
 {
-    const int nclass = (n8 > 0) + (n16 > 0) + (n32 > 0);
-    if (nclass == 0) return cudaSuccess;
+    if (n8 + n16 + n32 == 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(ctx->d_words + 1, 0, 3 * sizeof(uint32_t), ctx->stream);
+    if (e != cudaSuccess) return e;
+    HeavyQueue heavy;
+    if (n8 > 0 && n16 > 0 && n16 <= kMaxHeavy && d_order && ctx->t1_group == 32) {
+        heavy.order = d_order + n8;
+        heavy.n = n16;
+        heavy.ctas = (n16 + 1) / 2;
+        heavy.counter = ctx->d_words + 2;
+        n16 = 0;
+    }
+    const int nlaunch = (n8 > 0) + (n16 > 0) + (n32 > 0);
     cudaStream_t s8 = ctx->stream, s16 = ctx->stream, s32 = ctx->stream;
-    cudaError_t e;
-    if (nclass > 1) {
+    if (nlaunch > 1) {
         // Fork: the heavier classes run on side streams, concurrently with
         // the 8-bit class on the context's stream, and are joined after it.
         if ((e = ensure_side_streams(ctx)) != cudaSuccess) return e;
@@ -679,17 +752,21 @@ cudaError_t launch_t1_classes(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uin
         s32 = ctx->side[0];
         s16 = ctx->side[1];
     }
-    e = cudaSuccess;
     if (n32 > 0)
-        e = launch_class_g<uint32_t>(ctx, s32, d_desc, d_order ? d_order + n8 + n16 : nullptr, n32, ndesc, d_pool,
-                                   pool_len, d_out, out_mode, recon_r, 3);
+        e = launch_class_g<uint32_t>(ctx, s32, d_desc, d_order ? d_order + n8 + heavy.n + n16 : nullptr, n32, ndesc,
+                                     d_pool, pool_len, d_out, out_mode, recon_r, 3);
     if (e == cudaSuccess && n16 > 0)
         e = launch_class_g<uint16_t>(ctx, s16, d_desc, d_order ? d_order + n8 : nullptr, n16, ndesc, d_pool,
-                                   pool_len, d_out, out_mode, recon_r, 2);
-    if (e == cudaSuccess && n8 > 0)
-        e = launch_class_g<uint8_t>(ctx, s8, d_desc, d_order, n8, ndesc, d_pool, pool_len, d_out, out_mode, recon_r,
-                                  1);
-    if (nclass > 1) {
+                                     pool_len, d_out, out_mode, recon_r, 2);
+    if (e == cudaSuccess && n8 > 0) {
+        if (heavy.n > 0)
+            e = launch_class<uint8_t, 32>(ctx, s8, d_desc, d_order, n8, ndesc, d_pool, pool_len, d_out, out_mode,
+                                          recon_r, 1, heavy);
+        else
+            e = launch_class_g<uint8_t>(ctx, s8, d_desc, d_order, n8, ndesc, d_pool, pool_len, d_out, out_mode,
+                                        recon_r, 1);
+    }
+    if (nlaunch > 1) {
         for (int i = 0; i < 2; i++) {
             cudaError_t e2 = cudaEventRecord(ctx->ev_join[i], ctx->side[i]);
             if (e2 == cudaSuccess) e2 = cudaStreamWaitEvent(ctx->stream, ctx->ev_join[i], 0);
