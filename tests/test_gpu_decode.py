@@ -89,6 +89,18 @@ def test_few_deep_blocks_ride_with_bulk(gpu_ctx):
     plan.close()
 
 
+def test_shallow_minority_joins_deep_launch(gpu_ctx):
+    """A 12-bit noisy image: mostly blocks with 9-16 coded bit-planes and a
+    minority with at most 8, which the 16-bit launch decodes too."""
+    img = synth_image(700, 500, 3, 12, seed=21)
+    cs = codec.encode(img, 12, levels=5, reversible=True, mct=True)
+    _, desc, _ = codec.parse(cs)
+    nb = desc["mb"].astype(int) - desc["zero_bitplanes"].astype(int)
+    n8, n16 = int((nb <= 8).sum()), int(((nb > 8) & (nb <= 16)).sum())
+    assert 0 < n8 and 2 * n8 <= n16, (n8, n16)
+    np.testing.assert_array_equal(_decoder(gpu_ctx).decode(cs), img)
+
+
 def test_batched_plan_equals_single_decodes(gpu_ctx):
     from thousandthchicken_b200.stages import Plan
     streams = [codec.encode(synth_image(300, 200, 3, 8, 1), 8, levels=5, reversible=True),

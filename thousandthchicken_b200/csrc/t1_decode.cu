@@ -37,6 +37,10 @@ namespace tc {
 namespace {
 
 constexpr int kMaxStripes = 16;    // 64 rows
+#ifndef TC_T1_BLOCKS8
+#define TC_T1_BLOCKS8 8
+#endif
+constexpr int kBlocks8 = TC_T1_BLOCKS8;  // code-blocks per CTA of the 8-bit class
 constexpr int kSgnCols = 66;       // 64 columns + a zero column on each side
 
 // Flag word layout (one per stripe column):
@@ -459,10 +463,13 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
 // decode different code-blocks in lock-step (each group runs the serial
 // decoder redundantly across its lanes and splits the candidate searches
 // between them), so one warp instruction can advance several code-blocks.
-// Warps per CTA keep four code-blocks in flight per CTA whatever G is.
-template <int G>
+// Code-blocks per CTA: the per-CTA label tables are shared by more blocks
+// when the block state is small, which lets more warps reside per SM (8-bit
+// state: 3 CTAs of 8 blocks = 24 per SM within 228 KB, against 5 CTAs of 4).
+template <typename MagT, int G>
 struct GroupCfg {
-    static constexpr int warps = G == 32 ? 4 : (G == 16 ? 2 : 1);
+    static constexpr int blocks = sizeof(MagT) == 1 ? kBlocks8 : (sizeof(MagT) == 2 ? 4 : 2);
+    static constexpr int warps = blocks * G / 32 > 0 ? blocks * G / 32 : 1;
 };
 
 // Decode code-block `bi` with the state S and write it out (the group's
@@ -542,11 +549,11 @@ __device__ __forceinline__ void process_block(WarpState<MagT> &S, const Tables &
 }
 
 // Persistent Tier-1 launch over one magnitude class.  The 8-bit class with
-// 32-lane groups can also take a short queue of 16-bit blocks (`heavy`): the
-// first `heavy_ctas` CTAs turn warps 0 and 2 into 16-bit decoders that use
-// their own and their partner warp's state memory (warps 1 and 3 stand
-// down), drain the heavy queue first and then join the 8-bit queue.  A few
-// blocks with many bit-planes thus start at once, in the same longest-first
+// 32-lane groups can also take a short queue of 16-bit blocks (`heavy`): in
+// each of the first `heavy_ctas` CTAs warp 0 becomes a 16-bit decoder that
+// uses its own and warp 1's state memory (warp 1 stands down), drains the
+// heavy queue first and then joins the 8-bit queue.  A few blocks with many
+// bit-planes thus start at once, one per CTA, in the same longest-first
 // launch as the bulk, instead of running as a separate class whose warps
 // share SMs with the bulk and become the launch's longest chain.
 struct HeavyQueue {
@@ -557,7 +564,7 @@ struct HeavyQueue {
 };
 
 template <typename MagT, int G>
-__global__ void __launch_bounds__(32 * GroupCfg<G>::warps)
+__global__ void __launch_bounds__(32 * GroupCfg<MagT, G>::warps)
 t1_decode_kernel(const tc_cblk_desc *__restrict__ desc, const uint32_t *__restrict__ order, int n, int ndesc,
                  const uint8_t *__restrict__ pool, uint64_t pool_len, char *__restrict__ out, int out_mode,
                  float recon_r, uint32_t *__restrict__ counter, uint32_t *__restrict__ err, HeavyQueue heavy)
@@ -578,9 +585,9 @@ t1_decode_kernel(const tc_cblk_desc *__restrict__ desc, const uint32_t *__restri
 
     if constexpr (std::is_same<MagT, uint8_t>::value && G == 32) {
         static_assert(sizeof(WarpState<uint16_t>) <= 2 * sizeof(WarpState<uint8_t>), "heavy state spans two slots");
-        if ((int)blockIdx.x < heavy.ctas) {
-            if (slot & 1) return;  // lends its state to warp slot - 1
-            WarpState<uint16_t> &HS = *reinterpret_cast<WarpState<uint16_t> *>(&states[slot]);
+        if ((int)blockIdx.x < heavy.ctas && slot < 2) {
+            if (slot == 1) return;  // lends its state to warp 0
+            WarpState<uint16_t> &HS = *reinterpret_cast<WarpState<uint16_t> *>(&states[0]);
             for (;;) {
                 int idx = 0;
                 if (wl == 0) idx = (int)atomicAdd(heavy.counter, 1u);
@@ -650,7 +657,7 @@ struct LaunchCfg {
 template <typename MagT, int G>
 cudaError_t class_cfg(tc_ctx *ctx, LaunchCfg **out)
 {
-    constexpr int kWarps = GroupCfg<G>::warps;
+    constexpr int kWarps = GroupCfg<MagT, G>::warps;
     static LaunchCfg cfg[64];
     LaunchCfg &C = cfg[ctx->device & 63];
     if (!C.ready) {
@@ -680,7 +687,7 @@ cudaError_t launch_class(tc_ctx *ctx, cudaStream_t stream, const tc_cblk_desc *d
     if (e != cudaSuccess) return e;
     const int want = std::max((n + C->per_cta - 1) / C->per_cta, heavy.ctas);
     const int grid = std::max(1, std::min(want, C->per_sm * num_sms(ctx->device)));
-    t1_decode_kernel<MagT, G><<<grid, 32 * GroupCfg<G>::warps, C->smem, stream>>>(
+    t1_decode_kernel<MagT, G><<<grid, 32 * GroupCfg<MagT, G>::warps, C->smem, stream>>>(
         d_desc, d_order, n, ndesc, d_pool, pool_len, static_cast<char *>(d_out), out_mode, recon_r,
         ctx->d_words + slot, ctx->d_words, heavy);
     ctx->launches++;
@@ -705,10 +712,10 @@ cudaError_t launch_class_g(tc_ctx *ctx, cudaStream_t stream, const tc_cblk_desc 
     }
 }
 
-// Largest 16-bit class that rides along in the 8-bit launch (two heavy
-// decoders per CTA, so at most 32 CTAs, about 4% of a full grid, give up
-// half their warps).
-constexpr int kMaxHeavy = 64;
+// Largest 16-bit class that rides along in the 8-bit launch: one heavy
+// decoder per CTA, so at most one CTA per SM gives up one warp, and only next
+// to a bulk at least eight times larger.
+constexpr int kMaxHeavy = 148;
 
 }  // namespace
 
@@ -722,9 +729,12 @@ cudaError_t launch_t1_decode(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint
 }
 
 // Classes: blocks of <= 8, <= 16 and <= 31 coded bit-planes, in that order in
-// d_order (each slice longest first).  A short 16-bit class next to an 8-bit
-// bulk joins the 8-bit launch (see HeavyQueue); otherwise the classes run as
-// concurrent launches, the 32- and 16-bit ones on side streams.
+// d_order (each slice longest first).  A wider state decodes any narrower
+// block, so a minority class joins its neighbour's launch: a short 16-bit
+// class rides in the 8-bit launch (see HeavyQueue), and an 8-bit class at
+// most half the size of the 16-bit class is decoded by the 16-bit launch.
+// Otherwise the classes run as concurrent launches, the 32- and 16-bit ones
+// on side streams.
 cudaError_t launch_t1_classes(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint32_t *d_order, int ndesc,
                               int n8, int n16, int n32, const uint8_t *d_pool, uint64_t pool_len, void *d_out,
                               int out_mode, float recon_r)
@@ -732,13 +742,19 @@ cudaError_t launch_t1_classes(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uin
     if (n8 + n16 + n32 == 0) return cudaSuccess;
     cudaError_t e = cudaMemsetAsync(ctx->d_words + 1, 0, 3 * sizeof(uint32_t), ctx->stream);
     if (e != cudaSuccess) return e;
+    const uint32_t *o16 = d_order ? d_order + n8 : nullptr;
+    const uint32_t *o32 = d_order ? d_order + n8 + n16 : nullptr;
     HeavyQueue heavy;
-    if (n8 > 0 && n16 > 0 && n16 <= kMaxHeavy && d_order && ctx->t1_group == 32) {
-        heavy.order = d_order + n8;
+    if (n8 > 0 && n16 > 0 && n16 <= kMaxHeavy && 8 * n16 <= n8 && d_order && ctx->t1_group == 32) {
+        heavy.order = o16;
         heavy.n = n16;
-        heavy.ctas = (n16 + 1) / 2;
+        heavy.ctas = n16;
         heavy.counter = ctx->d_words + 2;
         n16 = 0;
+    } else if (n8 > 0 && n16 > 0 && 2 * n8 <= n16 && d_order) {
+        o16 = d_order;  // the 8-bit slice directly precedes the 16-bit one
+        n16 += n8;
+        n8 = 0;
     }
     const int nlaunch = (n8 > 0) + (n16 > 0) + (n32 > 0);
     cudaStream_t s8 = ctx->stream, s16 = ctx->stream, s32 = ctx->stream;
@@ -753,11 +769,11 @@ cudaError_t launch_t1_classes(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uin
         s16 = ctx->side[1];
     }
     if (n32 > 0)
-        e = launch_class_g<uint32_t>(ctx, s32, d_desc, d_order ? d_order + n8 + heavy.n + n16 : nullptr, n32, ndesc,
-                                     d_pool, pool_len, d_out, out_mode, recon_r, 3);
+        e = launch_class_g<uint32_t>(ctx, s32, d_desc, o32, n32, ndesc, d_pool, pool_len, d_out, out_mode,
+                                     recon_r, 3);
     if (e == cudaSuccess && n16 > 0)
-        e = launch_class_g<uint16_t>(ctx, s16, d_desc, d_order ? d_order + n8 : nullptr, n16, ndesc, d_pool,
-                                     pool_len, d_out, out_mode, recon_r, 2);
+        e = launch_class_g<uint16_t>(ctx, s16, d_desc, o16, n16, ndesc, d_pool, pool_len, d_out, out_mode,
+                                     recon_r, 2);
     if (e == cudaSuccess && n8 > 0) {
         if (heavy.n > 0)
             e = launch_class<uint8_t, 32>(ctx, s8, d_desc, d_order, n8, ndesc, d_pool, pool_len, d_out, out_mode,
