@@ -8,8 +8,9 @@
 //   * horizontal lifting: each thread lifts one 32-sample segment of one row
 //     (plus its halo) entirely in registers, fully unrolled, reading and
 //     writing it with 16-byte shared-memory accesses;
-//   * vertical lifting: each thread lifts one 64-sample column in registers
-//     and stores it (coalesced across the warp);
+//   * vertical lifting: two threads per column each lift an overlapping half
+//     (36 rows for 9/7, 34 for 5/3) in registers and store it (coalesced
+//     across the warp);
 // so every lifting step is register arithmetic with constant indices and the
 // CTA synchronises only between phases.  The row stride in shared memory is
 // a multiple of four words with an odd quotient, so threads walking
@@ -33,7 +34,7 @@ namespace {
 
 using namespace dwt;
 
-constexpr int kThreads = 128;
+constexpr int kThreads = 256;
 
 template <int WAVELET>
 struct RevGeo {
@@ -157,90 +158,94 @@ __global__ void __launch_bounds__(kThreads) idwt_rev_kernel(LevelIO io, int bits
     cp_async_wait_all();
     __syncthreads();
 
-    // 2. horizontal lifting, one row segment per thread, two rounds of 32
-    //    rows; segments are read and written with 16-byte (8-byte for the
-    //    2-sample halo of 5/3) shared-memory accesses
+    // 2. horizontal lifting, one row segment per thread (64 rows x 4
+    //    segments of 32 outputs); segments are read and written with 16-byte
+    //    (8-byte for the 2-sample halo of 5/3) shared-memory accesses
+    static_assert(NR * (TX / G::SEG) == kThreads, "one row segment per thread");
     if (w > 1) {
-        const int seg = tid >> 5;  // 4 segments of 32 outputs per row
+        const int seg = tid / NR, r = tid % NR;  // a warp walks 32 consecutive rows
 #pragma unroll
         for (int cc = 0; cc < NT; cc++) {
-            T *t = tiles + cc * NR * S;
-#pragma unroll 1
-            for (int round = 0; round < NR / 32; round++) {
-                const int r = round * 32 + lane;
-                T *row = t + r * S + seg * G::SEG;
-                T v[G::SEGN];
+            T *row = tiles + cc * NR * S + r * S + seg * G::SEG;
+            T v[G::SEGN];
 #pragma unroll
-                for (int k = 0; k < G::SEGN; k += 4) {
-                    const Vec4<T> q = *reinterpret_cast<const Vec4<T> *>(row + k);
-                    v[k] = q.x;
-                    v[k + 1] = q.y;
-                    v[k + 2] = q.z;
-                    v[k + 3] = q.w;
+            for (int k = 0; k < G::SEGN; k += 4) {
+                const Vec4<T> q = *reinterpret_cast<const Vec4<T> *>(row + k);
+                v[k] = q.x;
+                v[k + 1] = q.y;
+                v[k + 2] = q.z;
+                v[k + 3] = q.w;
+            }
+            __syncthreads();  // neighbouring segments overlap: all reads before any write
+            lift_reverse<T, WAVELET, RND, G::SEGN>(v);
+            if constexpr (H % 4 == 0) {
+#pragma unroll
+                for (int k = H; k < H + G::SEG; k += 4) {
+                    Vec4<T> q;
+                    q.x = v[k];
+                    q.y = v[k + 1];
+                    q.z = v[k + 2];
+                    q.w = v[k + 3];
+                    *reinterpret_cast<Vec4<T> *>(row + k) = q;
                 }
-                __syncthreads();  // neighbouring segments overlap: all reads before any write
-                lift_reverse<T, WAVELET, RND, G::SEGN>(v);
-                if constexpr (H % 4 == 0) {
+            } else {
+                using V2 = typename std::conditional<std::is_same<T, float>::value, float2, int2>::type;
 #pragma unroll
-                    for (int k = H; k < H + G::SEG; k += 4) {
-                        Vec4<T> q;
-                        q.x = v[k];
-                        q.y = v[k + 1];
-                        q.z = v[k + 2];
-                        q.w = v[k + 3];
-                        *reinterpret_cast<Vec4<T> *>(row + k) = q;
-                    }
-                } else {
-                    using V2 = typename std::conditional<std::is_same<T, float>::value, float2, int2>::type;
-#pragma unroll
-                    for (int k = H; k < H + G::SEG; k += 2) {
-                        V2 q;
-                        q.x = v[k];
-                        q.y = v[k + 1];
-                        *reinterpret_cast<V2 *>(row + k) = q;
-                    }
+                for (int k = H; k < H + G::SEG; k += 2) {
+                    V2 q;
+                    q.x = v[k];
+                    q.y = v[k + 1];
+                    *reinterpret_cast<V2 *>(row + k) = q;
                 }
             }
         }
         __syncthreads();
     }
 
-    // 3. vertical lifting, one column per thread, and the store.  With a
-    //    colour transform the first two components are parked back in their
-    //    tiles (each thread only touches its own column, so no barrier) and
-    //    the third one's column is combined with them straight from registers.
-    const int col = tid, x = x0 + col;
-    const bool full_rows = y0 + TY <= h;
+    // 3. vertical lifting, two threads per column, and the store.  The top
+    //    thread lifts rows [0, 32 + H) and keeps output rows [0, 32 - H); the
+    //    bottom one lifts rows [32 - H, 64) and keeps [32 - H, TY).  With a
+    //    colour transform the first two components are parked in their own
+    //    tiles, in rows that only the parking thread reads: the top thread at
+    //    rows [0, 32 - H), the bottom one at [NR - (32 - H), NR).  The third
+    //    component's column is then combined with them from registers.
+    constexpr int VN = 32 + H, OUTR = 32 - H;
+    const int col = tid % TX, half = tid / TX, x = x0 + col;
+    const int vbase = half ? 32 - H : 0;             // first tile row lifted
+    const int obase = half ? OUTR : 0;               // first output row kept
+    const int pbase = half ? NR - OUTR : 0;          // first parking row
+    const bool full_rows = y0 + obase + OUTR <= h;
     const int dc = PLANE ? 0 : 1 << (bits - 1), mx = PLANE ? 0 : (1 << bits) - 1;
 #pragma unroll
     for (int cc = 0; cc < NT; cc++) {
         T *t = tiles + cc * NR * S;
-        T v[NR];
+        T v[VN];
 #pragma unroll
-        for (int r = 0; r < NR; r++) v[r] = t[r * S + H + col];
-        if (h > 1) lift_reverse<T, WAVELET, RND, NR>(v);
+        for (int k = 0; k < VN; k++) v[k] = t[(vbase + k) * S + H + col];
+        if (h > 1) lift_reverse<T, WAVELET, RND, VN>(v);
         if (x >= w) continue;
+        const int y = y0 + obase;
         if constexpr (PLANE) {
-            T *out = static_cast<T *>(io.out[cbase]) + (size_t)y0 * io.out_pitch + x;
+            T *out = static_cast<T *>(io.out[cbase]) + (size_t)y * io.out_pitch + x;
 #pragma unroll
-            for (int r = 0; r < TY; r++)
-                if (full_rows || y0 + r < h) out[(size_t)r * io.out_pitch] = v[H + r];
+            for (int r = 0; r < OUTR; r++)
+                if (full_rows || y + r < h) out[(size_t)r * io.out_pitch] = v[H + r];
         } else if (COLOR == TC_COLOR_DC || cc >= 3) {
-            OT *out = static_cast<OT *>(io.out[cc]) + (size_t)y0 * io.out_pitch + x;
+            OT *out = static_cast<OT *>(io.out[cc]) + (size_t)y * io.out_pitch + x;
 #pragma unroll
-            for (int r = 0; r < TY; r++)
-                if (full_rows || y0 + r < h) out[(size_t)r * io.out_pitch] = clamp_out<OT>(to_int(v[H + r]) + dc, mx);
+            for (int r = 0; r < OUTR; r++)
+                if (full_rows || y + r < h) out[(size_t)r * io.out_pitch] = clamp_out<OT>(to_int(v[H + r]) + dc, mx);
         } else if (cc < 2) {
 #pragma unroll
-            for (int r = 0; r < TY; r++) t[(H + r) * S + H + col] = v[H + r];
+            for (int r = 0; r < OUTR; r++) t[(pbase + r) * S + H + col] = v[H + r];
         } else {
-            const T *t0 = tiles + (H * S + H + col), *t1 = tiles + (NR * S + H * S + H + col);
-            const size_t o = (size_t)y0 * io.out_pitch + x;
+            const T *t0 = tiles + (pbase * S + H + col), *t1 = tiles + (NR * S + pbase * S + H + col);
+            const size_t o = (size_t)y * io.out_pitch + x;
             OT *o0 = static_cast<OT *>(io.out[0]) + o, *o1 = static_cast<OT *>(io.out[1]) + o,
                *o2 = static_cast<OT *>(io.out[2]) + o;
 #pragma unroll
-            for (int r = 0; r < TY; r++) {
-                if (!(full_rows || y0 + r < h)) continue;
+            for (int r = 0; r < OUTR; r++) {
+                if (!(full_rows || y + r < h)) continue;
                 int c0, c1, c2;
                 if constexpr (COLOR == TC_COLOR_RCT) {
                     const int Y = (int)t0[r * S], U = (int)t1[r * S], V = (int)v[H + r];
