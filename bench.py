@@ -88,7 +88,8 @@ def serve_section(args, mixed, device):
     2048x2048 lossless images (radial field + N(0, 40^2) noise) arrive as a
     Poisson process; the continuous-batching server (budget 40 GB) is
     compared with the per-image path (one request per batch, one in flight)
-    on the same arrivals."""
+    on the same arrivals, at each rate of --serve-rates (the first rate's
+    figures are also reported at the top level)."""
     from thousandthchicken_b200 import codec
     from thousandthchicken_b200.serve import Request, Server, latency_stats, poisson_arrivals
     from thousandthchicken_b200.synth import radial_noise_image
@@ -97,22 +98,30 @@ def serve_section(args, mixed, device):
                            mct=False) for i in range(2)]
     pool = [(cs_, im.shape[1] * im.shape[2]) for im, cs_ in mixed]
     pool_r = [(cs_, 2048 * 2048) for cs_ in radial]
-    arr = poisson_arrivals(args.serve_requests, args.serve_rate, seed=9)
     picks = [pool_r[rng.integers(len(pool_r))] if rng.random() < 0.2 else pool[rng.integers(len(pool))]
-             for _ in arr]
+             for _ in range(args.serve_requests)]
     mpx = sum(px for _, px in picks) / 1e6
-    out = {"requests": len(picks), "rate_per_s": args.serve_rate, "mpixels": round(mpx, 3),
-           "budget_bytes": 40 << 30}
-    for name, kw in (("continuous_batching", dict(max_batch=16, inflight=2)),
-                     ("per_image", dict(max_batch=1, inflight=1))):
-        srv = Server(device, budget_bytes=40 << 30, **kw)
-        srv.run([Request(i, cs_, 0.0) for i, (cs_, _) in enumerate(picks[:4])], realtime=False)  # warm-up
-        reqs = [Request(i, cs_, float(a)) for i, ((cs_, _), a) in enumerate(zip(picks, arr))]
-        done, wall = srv.run(reqs, realtime=True)
-        srv.close()
-        st = latency_stats(done)
-        out[name] = {"mpix_s": round(mpx / wall, 2), "wall_s": round(wall, 3),
-                     "p50_ms": round(st["p50_ms"], 3), "p99_ms": round(st["p99_ms"], 3)}
+    rates = [float(r) for r in str(args.serve_rates).split(",") if r]
+    out = {"requests": len(picks), "mpixels": round(mpx, 3), "budget_bytes": 40 << 30, "by_rate": []}
+    for rate in rates:
+        arr = poisson_arrivals(args.serve_requests, rate, seed=9)
+        res = {"rate_per_s": rate, "arrival_span_s": round(float(arr[-1]), 3)}
+        for name, kw in (("continuous_batching", dict(max_batch=16, inflight=2)),
+                         ("per_image", dict(max_batch=1, inflight=1))):
+            srv = Server(device, budget_bytes=40 << 30, **kw)
+            srv.run([Request(i, cs_, 0.0) for i, (cs_, _) in enumerate(picks[:4])], realtime=False)  # warm-up
+            reqs = [Request(i, cs_, float(a)) for i, ((cs_, _), a) in enumerate(zip(picks, arr))]
+            done, wall = srv.run(reqs, realtime=True)
+            srv.close()
+            st = latency_stats(done)
+            res[name] = {"mpix_s": round(mpx / wall, 2), "wall_s": round(wall, 3),
+                         "p50_ms": round(st["p50_ms"], 3), "p99_ms": round(st["p99_ms"], 3)}
+        out["by_rate"].append(res)
+    if out["by_rate"]:
+        first = out["by_rate"][0]
+        out["rate_per_s"] = first["rate_per_s"]
+        out["continuous_batching"] = first["continuous_batching"]
+        out["per_image"] = first["per_image"]
     return out
 
 
@@ -188,6 +197,17 @@ def dwt_bytes(w, h, c, levels):
         n = ws[lvl - 1] * hs[lvl - 1] * c
         b += 4 * n + (1 * n if lvl == 1 else 4 * n)
     return b
+
+
+def max_over_ranks(x: float, dist, device) -> float:
+    """The largest of the ranks' values of x (x itself without a process
+    group).  Every rank must call it at the same point."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def run_reference(args, rank):
@@ -299,15 +319,13 @@ def run_ours(args, rank, world, local_rank):
             plan.execute(outs)
             evs[k][1].record(stream)
     torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
     wall = time.perf_counter() - wall0
     clocks = sampler.stop()
     launches = ctx.launches - launches0
     step_ms = [a.elapsed_time(b) for a, b in evs]
-    total_ms = sum(step_ms)
-    if dist:
-        t = torch.tensor([total_ms], device=f"cuda:{local_rank}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(sum(step_ms), dist, f"cuda:{local_rank}")
     ctx.synchronize()
 
     # per-stage device times (CUDA events on the plan's stream)
@@ -334,11 +352,7 @@ def run_ours(args, rank, world, local_rank):
         t0 = time.perf_counter()
         dec.decode(cs, host_out)
         e2e_times.append(time.perf_counter() - t0)
-    e2e_s = sum(e2e_times) / e2e_steps
-    if dist:
-        t = torch.tensor([e2e_s], device=f"cuda:{local_rank}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(sum(e2e_times) / e2e_steps, dist, f"cuda:{local_rank}")
 
     batched, served = None, None
     if not args.core_only:
@@ -475,7 +489,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--core-only", action="store_true",
                     help="report the headline workload only (no batched or served sections)")
-    ap.add_argument("--serve-rate", type=float, default=200.0, help="served decode: Poisson arrivals per second")
+    ap.add_argument("--serve-rates", default="200,2000",
+                    help="served decode: Poisson arrival rates per second, comma-separated")
     ap.add_argument("--serve-requests", type=int, default=64)
     ap.add_argument("--size", type=int, default=0,
                     help="square image side for a smaller case of the same workload (profiling)")

@@ -270,6 +270,13 @@ int tc_plan_destroy(tc_plan *plan);
  * resident across batches.  Waits for the plan's previous execute. */
 int tc_plan_rebuild(tc_plan *plan, const uint8_t *const *h_cs, const size_t *lens,
                     int nimages);
+/* tc_plan_rebuild from codestreams parsed beforehand with tc_j2k_parse (on
+ * any host thread, e.g. as requests arrive), so that the rebuild itself only
+ * lays out and uploads.  The parsed objects (and, for single-layer streams,
+ * the codestream bytes they point into) must stay alive until the rebuild
+ * returns.  No counterpart in the reference, whose parser runs inline in
+ * Decoder::decode (Decoder.cpp:94-217). */
+int tc_plan_rebuild_parsed(tc_plan *plan, const tc_j2k_parsed *const *parsed, int nimages);
 /* Bytes of output for image i (planar, sample type as tc_decode_j2k). */
 int tc_plan_output_bytes(const tc_plan *plan, int image, size_t *bytes);
 int tc_plan_image_info(const tc_plan *plan, int image, tc_image_info *info);

@@ -104,6 +104,7 @@ _PROTOS = {
     "tc_plan_create": (_I, [_VP, _VP, _VP, _I, C.POINTER(_VP)]),
     "tc_plan_destroy": (_I, [_VP]),
     "tc_plan_rebuild": (_I, [_VP, _VP, _VP, _I]),
+    "tc_plan_rebuild_parsed": (_I, [_VP, _VP, _I]),
     "tc_plan_output_bytes": (_I, [_VP, _I, C.POINTER(C.c_size_t)]),
     "tc_plan_image_info": (_I, [_VP, _I, C.POINTER(ImageInfo)]),
     "tc_plan_execute": (_I, [_VP, _VP]),

@@ -35,11 +35,62 @@ cudaError_t DevBuf::ensure(size_t bytes)
     return e;
 }
 
-void DevBuf::release()
+cudaError_t ctx_mem_pool(tc_ctx *ctx, cudaMemPool_t *out)
 {
-    if (ptr) cudaFree(ptr);
+    if (!ctx->pool) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = ctx->device;
+        cudaMemPool_t p = nullptr;
+        cudaError_t e = cudaMemPoolCreate(&p, &props);
+        if (e != cudaSuccess) return e;
+        uint64_t keep = ~uint64_t(0);
+        e = cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+        if (e != cudaSuccess) {
+            cudaMemPoolDestroy(p);
+            return e;
+        }
+        ctx->pool = p;
+    }
+    *out = ctx->pool;
+    return cudaSuccess;
+}
+
+cudaError_t DevBuf::ensure_on(size_t bytes, cudaStream_t s, cudaMemPool_t pool)
+{
+    if (bytes <= size && ptr) return cudaSuccess;
+    const size_t want = std::max<size_t>(std::max<size_t>(bytes, 256), size + size / 2);
+    if (ptr) {
+        if (ordered) cudaFreeAsync(ptr, stream);
+        else cudaFree(ptr);
+    }
     ptr = nullptr;
     size = 0;
+    cudaError_t e = cudaMallocFromPoolAsync(&ptr, want, pool, s);
+    if (e == cudaSuccess) {
+        size = want;
+        stream = s;
+        ordered = true;
+    } else {
+        ptr = nullptr;
+    }
+    return e;
+}
+
+void DevBuf::release()
+{
+    if (ptr) {
+        if (ordered) {
+            cudaFreeAsync(ptr, stream);
+            cudaStreamSynchronize(stream);
+        } else {
+            cudaFree(ptr);
+        }
+    }
+    ptr = nullptr;
+    size = 0;
+    ordered = false;
 }
 
 cudaError_t ensure_side_streams(tc_ctx *ctx)
@@ -182,20 +233,19 @@ static void plan_drop_graph(tc_plan *P)
     P->graph_outs.clear();
 }
 
-static int plan_build(tc_ctx *ctx, const uint8_t *const *cs, const size_t *lens, int n, tc_plan *P)
+// Lays out and uploads a batch from parsed images: parsed[i] with its
+// segment pool pools[i] of pool_lens[i] bytes (the codestream itself for
+// single-layer streams).
+static int plan_build_parsed(tc_ctx *ctx, const Parsed *const *parsed, const uint8_t *const *pools,
+                             const uint64_t *pool_lens, int n, tc_plan *P)
 {
     P->ctx = ctx;
     P->imgs.clear();
     P->ncblk = 0;
-    std::vector<Parsed> parsed(n);
-    std::string err;
     uint64_t pool_total = 0, coef_total = 0;
     size_t scratch_max = 0;
     for (int i = 0; i < n; i++) {
-        if (!cs[i] || !lens[i]) return fail(ctx, TC_E_ARG, "empty codestream");
-        const int rc = parse_codestream(cs[i], lens[i], parsed[i], err);
-        if (rc) return fail(ctx, rc, "image " + std::to_string(i) + ": " + err);
-        const tc_image_info &inf = parsed[i].info;
+        const tc_image_info &inf = parsed[i]->info;
         tc_plan::Img im;
         im.info = inf;
         im.coef_off = coef_total;
@@ -204,9 +254,8 @@ static int plan_build(tc_ctx *ctx, const uint8_t *const *cs, const size_t *lens,
         im.out_bytes = (size_t)inf.ncomp * inf.width * inf.height * sample_bytes(inf.bits);
         scratch_max = std::max(scratch_max, reverse_scratch_bytes(inf.width, inf.height, inf.levels, inf.ncomp));
         P->imgs.push_back(im);
-        const uint64_t pl = parsed[i].pool_is_cs ? lens[i] : parsed[i].own_pool.size();
-        pool_total += (pl + 15) & ~uint64_t(15);
-        P->ncblk += (int)parsed[i].desc.size();
+        pool_total += (pool_lens[i] + 15) & ~uint64_t(15);
+        P->ncblk += (int)parsed[i]->desc.size();
     }
     // Pinned host staging (the plan keeps it until its next build, so the
     // uploads below are asynchronous): pool and rebased descriptors.
@@ -224,11 +273,10 @@ static int plan_build(tc_ctx *ctx, const uint8_t *const *cs, const size_t *lens,
     uint64_t po = 0;
     size_t nd = 0;
     for (int i = 0; i < n; i++) {
-        const uint8_t *src = parsed[i].pool_is_cs ? cs[i] : parsed[i].own_pool.data();
-        const uint64_t pl = parsed[i].pool_is_cs ? lens[i] : parsed[i].own_pool.size();
-        if (pl) std::memcpy(hpool + po, src, pl);
+        const uint64_t pl = pool_lens[i];
+        if (pl) std::memcpy(hpool + po, pools[i], pl);
         const uint64_t elem_base = P->imgs[i].coef_off / 4;
-        for (tc_cblk_desc d : parsed[i].desc) {
+        for (tc_cblk_desc d : parsed[i]->desc) {
             d.seg_off += po;
             d.out_off += elem_base;
             hdesc[nd++] = d;
@@ -238,11 +286,14 @@ static int plan_build(tc_ctx *ctx, const uint8_t *const *cs, const size_t *lens,
     t1_class_order(hdesc, P->ncblk, horder, P->class_counts);
     P->pool_len = pool_total;
     P->scratch_per_img = scratch_max;
-    if ((e = P->pool.ensure(pool_bytes)) != cudaSuccess ||
-        (e = P->desc.ensure(sizeof(tc_cblk_desc) * std::max(1, P->ncblk))) != cudaSuccess ||
-        (e = P->order.ensure(sizeof(uint32_t) * std::max(1, P->ncblk))) != cudaSuccess ||
-        (e = P->coef.ensure(std::max<uint64_t>(coef_total, 256))) != cudaSuccess ||
-        (e = P->scratch.ensure(std::max<size_t>(scratch_max, 256))) != cudaSuccess)
+    cudaStream_t st = ctx->stream;
+    cudaMemPool_t mp = nullptr;
+    if ((e = ctx_mem_pool(ctx, &mp)) != cudaSuccess ||
+        (e = P->pool.ensure_on(pool_bytes, st, mp)) != cudaSuccess ||
+        (e = P->desc.ensure_on(sizeof(tc_cblk_desc) * std::max(1, P->ncblk), st, mp)) != cudaSuccess ||
+        (e = P->order.ensure_on(sizeof(uint32_t) * std::max(1, P->ncblk), st, mp)) != cudaSuccess ||
+        (e = P->coef.ensure_on(std::max<uint64_t>(coef_total, 256), st, mp)) != cudaSuccess ||
+        (e = P->scratch.ensure_on(std::max<size_t>(scratch_max, 256), st, mp)) != cudaSuccess)
         return cuda_status(ctx, e, "plan allocation");
     if ((e = cudaMemcpyAsync(P->pool.ptr, hpool, pool_bytes, cudaMemcpyHostToDevice, ctx->stream)) ||
         (e = cudaMemcpyAsync(P->desc.ptr, hdesc, sizeof(tc_cblk_desc) * P->ncblk, cudaMemcpyHostToDevice,
@@ -251,6 +302,24 @@ static int plan_build(tc_ctx *ctx, const uint8_t *const *cs, const size_t *lens,
                              ctx->stream)))
         return cuda_status(ctx, e, "plan upload");
     return TC_OK;
+}
+
+static int plan_build(tc_ctx *ctx, const uint8_t *const *cs, const size_t *lens, int n, tc_plan *P)
+{
+    std::vector<Parsed> parsed(n);
+    std::vector<const Parsed *> pp(n);
+    std::vector<const uint8_t *> pools(n);
+    std::vector<uint64_t> plens(n);
+    std::string err;
+    for (int i = 0; i < n; i++) {
+        if (!cs[i] || !lens[i]) return fail(ctx, TC_E_ARG, "empty codestream");
+        const int rc = parse_codestream(cs[i], lens[i], parsed[i], err);
+        if (rc) return fail(ctx, rc, "image " + std::to_string(i) + ": " + err);
+        pp[i] = &parsed[i];
+        pools[i] = parsed[i].pool_is_cs ? cs[i] : parsed[i].own_pool.data();
+        plens[i] = parsed[i].pool_is_cs ? lens[i] : parsed[i].own_pool.size();
+    }
+    return plan_build_parsed(ctx, pp.data(), pools.data(), plens.data(), n, P);
 }
 
 static int plan_run(tc_plan *P, void *const *d_out)
@@ -356,6 +425,9 @@ int tc_ctx_destroy(tc_ctx *ctx)
     }
     if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
     if (ctx->capture) cudaStreamDestroy(ctx->capture);
+    // buffers still drawn from the pool (plans not destroyed yet) keep it
+    // alive until they are freed
+    if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
     delete ctx;
     return TC_OK;
 }
@@ -574,6 +646,17 @@ int tc_j2k_read_header(const uint8_t *h_cs, size_t len, tc_image_info *info)
     return read_header(h_cs, len, *info, err);
 }
 
+}  // extern "C"
+
+// A parsed codestream handed out through the C ABI: the public struct first,
+// then the owning parse result.
+struct ParsedBox {
+    tc_j2k_parsed pub;
+    Parsed *own;
+};
+
+extern "C" {
+
 int tc_j2k_parse(const uint8_t *h_cs, size_t len, tc_j2k_parsed **out)
 {
     if (!h_cs || !out || len < 2) return TC_E_ARG;
@@ -586,13 +669,7 @@ int tc_j2k_parse(const uint8_t *h_cs, size_t len, tc_j2k_parsed **out)
         delete holder;
         return rc;
     }
-    // The public struct is followed in memory by nothing we own; keep the
-    // Parsed object alive through a side allocation.
-    struct Box {
-        tc_j2k_parsed pub;
-        Parsed *own;
-    };
-    Box *b = new (std::nothrow) Box;
+    ParsedBox *b = new (std::nothrow) ParsedBox;
     if (!b) {
         delete holder;
         return TC_E_OOM;
@@ -611,11 +688,7 @@ int tc_j2k_parse(const uint8_t *h_cs, size_t len, tc_j2k_parsed **out)
 void tc_j2k_parsed_free(tc_j2k_parsed *p)
 {
     if (!p) return;
-    struct Box {
-        tc_j2k_parsed pub;
-        Parsed *own;
-    };
-    Box *b = reinterpret_cast<Box *>(p);
+    ParsedBox *b = reinterpret_cast<ParsedBox *>(p);
     delete b->own;
     delete b;
 }
@@ -647,6 +720,27 @@ int tc_plan_rebuild(tc_plan *P, const uint8_t *const *h_cs, const size_t *lens, 
     if (e != cudaSuccess) return cuda_status(P->ctx, e, "tc_plan_rebuild");
     plan_drop_graph(P);
     return plan_build(P->ctx, h_cs, lens, nimages, P);
+}
+
+int tc_plan_rebuild_parsed(tc_plan *P, const tc_j2k_parsed *const *parsed, int nimages)
+{
+    if (!P || !parsed || nimages < 1) return TC_E_ARG;
+    int rc = check_ctx(P->ctx);
+    if (rc) return rc;
+    std::vector<const Parsed *> pp(nimages);
+    std::vector<const uint8_t *> pools(nimages);
+    std::vector<uint64_t> plens(nimages);
+    for (int i = 0; i < nimages; i++) {
+        if (!parsed[i]) return fail(P->ctx, TC_E_ARG, "tc_plan_rebuild_parsed: null image");
+        const ParsedBox *b = reinterpret_cast<const ParsedBox *>(parsed[i]);
+        pp[i] = b->own;
+        pools[i] = b->pub.pool;
+        plens[i] = b->pub.pool_len;
+    }
+    cudaError_t e = cudaStreamSynchronize(P->ctx->stream);
+    if (e != cudaSuccess) return cuda_status(P->ctx, e, "tc_plan_rebuild_parsed");
+    plan_drop_graph(P);
+    return plan_build_parsed(P->ctx, pp.data(), pools.data(), plens.data(), nimages, P);
 }
 
 int tc_plan_destroy(tc_plan *P)

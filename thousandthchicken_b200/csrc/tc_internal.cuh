@@ -5,6 +5,7 @@
 
 #include <cstdint>
 #include <string>
+#include <vector>
 
 #include "tc_j2k.h"
 
@@ -18,7 +19,13 @@ namespace tc {
 struct DevBuf {
     void *ptr = nullptr;
     size_t size = 0;
+    cudaStream_t stream = nullptr;  // set by ensure_on: stream-ordered allocation
+    bool ordered = false;
     cudaError_t ensure(size_t bytes);
+    // Grows through the stream-ordered allocator (memory pool `pool`) on
+    // `s`: the old block is freed after the work already queued on `s`, and
+    // no call waits for the rest of the device (cudaFree would).
+    cudaError_t ensure_on(size_t bytes, cudaStream_t s, cudaMemPool_t pool);
     void release();
 };
 
@@ -26,11 +33,16 @@ struct DevBuf {
 struct PinBuf {
     void *ptr = nullptr;
     size_t size = 0;
+    // Outgrown blocks.  cudaFreeHost waits for the whole device, which in a
+    // serving loop means another batch in flight, so they are only freed
+    // with the buffer itself.
+    std::vector<void *> retired;
     cudaError_t ensure(size_t bytes)
     {
         if (bytes <= size && ptr) return cudaSuccess;
-        const size_t want = bytes < 4096 ? 4096 : (bytes < size + size / 2 ? size + size / 2 : bytes);
-        if (ptr) cudaFreeHost(ptr);
+        // doubling: a serving loop's batches vary, and every regrowth re-pins
+        const size_t want = bytes < 4096 ? 4096 : (bytes < 2 * size ? 2 * size : bytes);
+        if (ptr) retired.push_back(ptr);
         ptr = nullptr;
         size = 0;
         cudaError_t e = cudaHostAlloc(&ptr, want, cudaHostAllocDefault);
@@ -41,6 +53,8 @@ struct PinBuf {
     void release()
     {
         if (ptr) cudaFreeHost(ptr);
+        for (void *p : retired) cudaFreeHost(p);
+        retired.clear();
         ptr = nullptr;
         size = 0;
     }
@@ -64,10 +78,15 @@ struct tc_ctx {
     // stream that plan graphs are captured on (the caller's stream may be the
     // legacy default stream, which cannot be captured)
     cudaStream_t capture = nullptr;
+    // device memory pool of the plans' buffers; it keeps freed memory mapped
+    // (release threshold: unlimited) so that regrowth does not map again
+    cudaMemPool_t pool = nullptr;
 };
 
 namespace tc {
 
+// The context's memory pool (created on first use).
+cudaError_t ctx_mem_pool(tc_ctx *ctx, cudaMemPool_t *out);
 // Creates the context's side streams, capture stream and fork/join events
 // if needed.
 cudaError_t ensure_side_streams(tc_ctx *ctx);

@@ -9,13 +9,20 @@ reuses them).  While batches run, newly arrived requests are admitted into the
 next free slot, so arrivals overlap with decoding.  Each request's latency is
 its completion time minus its arrival time.
 
+Each request's codestream is parsed (Tier-2: packet headers, segment
+gathering, descriptors) on a worker thread as soon as it is admitted, while
+earlier batches decode; a batch is then built from the parsed requests with
+`tc_plan_rebuild_parsed`, which only lays out and uploads.
+
 Results are deterministic per code-block, so a request decoded in a mix is
 bit-identical to the same request decoded alone.
 """
 from __future__ import annotations
 
 import ctypes as C
+import os
 import time
+from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -38,6 +45,27 @@ class Request:
     device_bytes: int = 0
     done: float = -1.0
     output: object = None               # numpy array when keep_outputs
+    parsed: object = None               # future of the tc_j2k_parse result
+
+
+def _parse(cs: bytes):
+    """tc_j2k_parse on a worker thread (the call runs without the GIL); the
+    result points into `cs`, which the request keeps alive."""
+    buf = np.frombuffer(cs, np.uint8)
+    out = C.POINTER(L.Parsed)()
+    L.check(L.lib().tc_j2k_parse(buf.ctypes.data, buf.size, C.byref(out)), what="tc_j2k_parse")
+    return out
+
+
+def _free_parsed(r):
+    if r.parsed is not None:
+        try:
+            p = r.parsed.result()
+        except Exception:  # noqa: BLE001 - a failed parse holds nothing
+            p = None
+        if p:
+            L.lib().tc_j2k_parsed_free(p)
+        r.parsed = None
 
 
 def request_device_bytes(info: dict, cs_len: int) -> int:
@@ -63,16 +91,23 @@ class _Slot:
         self.keep = []
 
     def launch(self, batch, keep_outputs):
-        bufs = [np.frombuffer(r.cs, np.uint8) for r in batch]
-        ptrs = (C.c_void_p * len(bufs))(*[b.ctypes.data for b in bufs])
-        lens = (C.c_size_t * len(bufs))(*[b.size for b in bufs])
         lib = L.lib()
-        if self.plan is None:
-            h = C.c_void_p()
-            self.ctx.check(lib.tc_plan_create(self.ctx.handle, ptrs, lens, len(bufs), C.byref(h)), "tc_plan_create")
-            self.plan = h
-        else:
-            self.ctx.check(lib.tc_plan_rebuild(self.plan, ptrs, lens, len(bufs)), "tc_plan_rebuild")
+        try:
+            if self.plan is None:
+                bufs = [np.frombuffer(r.cs, np.uint8) for r in batch]
+                ptrs = (C.c_void_p * len(bufs))(*[b.ctypes.data for b in bufs])
+                lens = (C.c_size_t * len(bufs))(*[b.size for b in bufs])
+                h = C.c_void_p()
+                self.ctx.check(lib.tc_plan_create(self.ctx.handle, ptrs, lens, len(bufs), C.byref(h)),
+                               "tc_plan_create")
+                self.plan = h
+            else:
+                parsed = [r.parsed.result() for r in batch]
+                arr = (C.POINTER(L.Parsed) * len(parsed))(*parsed)
+                self.ctx.check(lib.tc_plan_rebuild_parsed(self.plan, arr, len(parsed)), "tc_plan_rebuild_parsed")
+        finally:
+            for r in batch:
+                _free_parsed(r)
         dev = torch.device("cuda", self.ctx.device)
         self.outs = []
         for r in batch:
@@ -122,10 +157,12 @@ class Server:
         self.budget = budget_bytes
         self.max_batch = max_batch
         self.slots = [_Slot(self, device) for _ in range(inflight)]
+        self.parser = ThreadPoolExecutor(max_workers=max(1, min(8, os.cpu_count() or 1)))
 
     def close(self):
         for s in self.slots:
             s.close()
+        self.parser.shutdown(wait=True)
 
     def run(self, requests, realtime: bool = True, keep_outputs: bool = False):
         """Serve `requests` (Request objects with arrival times in seconds
@@ -150,7 +187,9 @@ class Server:
         while len(finished) < len(requests):
             t = now()
             while nxt < len(pending) and pending[nxt].arrival <= t:
-                queue.append(pending[nxt])
+                r = pending[nxt]
+                r.parsed = self.parser.submit(_parse, r.cs)  # Tier-2 overlaps the decodes in flight
+                queue.append(r)
                 nxt += 1
             for s in self.slots:
                 for r in s.poll(now):
