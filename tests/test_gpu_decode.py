@@ -101,6 +101,35 @@ def test_shallow_minority_joins_deep_launch(gpu_ctx):
     np.testing.assert_array_equal(_decoder(gpu_ctx).decode(cs), img)
 
 
+def test_batched_levels_of_mixed_depth_equal_single_decodes(gpu_ctx):
+    """One plan over images with 0-6 levels, both wavelets, 1 and 3
+    components, 8- and 12-bit samples: their DWT levels share launches step
+    by step (image i runs its level L_i - t at step t) and must give the
+    single-image results bit for bit."""
+    from thousandthchicken_b200.stages import Plan
+    spec = [(300, 200, 3, 8, 5, True), (64, 48, 1, 12, 0, True), (517, 211, 3, 8, 6, False),
+            (33, 129, 1, 8, 1, False), (256, 256, 3, 12, 4, True), (140, 90, 3, 8, 2, False),
+            (96, 300, 1, 12, 4, False)]
+    streams = [codec.encode(synth_image(w, h, c, b, 30 + i), b, levels=lv, reversible=rev, mct=c == 3,
+                            base_step=1 / 64)
+               for i, (w, h, c, b, lv, rev) in enumerate(spec)]
+    plan = Plan(gpu_ctx, streams)
+    outs = plan.alloc_outputs()
+    for _ in range(2):  # the second run reuses the uploaded job table
+        for o in outs:
+            o.zero_()
+        plan.execute(outs)
+        gpu_ctx.synchronize()
+        dec = _decoder(gpu_ctx)
+        for s_, o in zip(streams, outs):
+            single = dec.decode(s_)
+            got = o.cpu().numpy()
+            if single.dtype == np.uint16:
+                got = got.view(np.uint16)
+            np.testing.assert_array_equal(got, single)
+    plan.close()
+
+
 def test_batched_plan_equals_single_decodes(gpu_ctx):
     from thousandthchicken_b200.stages import Plan
     streams = [codec.encode(synth_image(300, 200, 3, 8, 1), 8, levels=5, reversible=True),

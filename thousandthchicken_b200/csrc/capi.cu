@@ -214,6 +214,18 @@ struct tc_plan {
     int ncblk = 0;
     uint64_t pool_len = 0;
     size_t scratch_per_img = 0;
+    // batched reverse DWT (plans of several images): each image's own
+    // scratch region, and the job table of the level launches for the
+    // output buffers it was built for
+    std::vector<size_t> scratch_off;
+    struct DwtLaunch {
+        int first, njobs, ntiles, wavelet, color, ncomp, otype, bits;
+    };
+    std::vector<DwtLaunch> dwt_launches;
+    std::vector<void *> jobs_outs;
+    PinBuf h_jobs;
+    DevBuf jobs;
+    cudaEvent_t jobs_uploaded = nullptr;
     float recon_r = 0.5f;
     int class_counts[3] = {0, 0, 0};  // Tier-1 blocks of <= 8, <= 16, <= 31 coded bit-planes
     bool profiling = false;
@@ -243,9 +255,12 @@ static int plan_build_parsed(tc_ctx *ctx, const Parsed *const *parsed, const uin
     P->imgs.clear();
     P->ncblk = 0;
     uint64_t pool_total = 0, coef_total = 0;
-    size_t scratch_max = 0;
+    size_t scratch_max = 0, scratch_sum = 0;
+    P->scratch_off.clear();
+    P->jobs_outs.clear();
     for (int i = 0; i < n; i++) {
         const tc_image_info &inf = parsed[i]->info;
+        P->scratch_off.push_back(scratch_sum);
         tc_plan::Img im;
         im.info = inf;
         im.coef_off = coef_total;
@@ -253,6 +268,7 @@ static int plan_build_parsed(tc_ctx *ctx, const Parsed *const *parsed, const uin
         coef_total = (coef_total + 255) & ~uint64_t(255);
         im.out_bytes = (size_t)inf.ncomp * inf.width * inf.height * sample_bytes(inf.bits);
         scratch_max = std::max(scratch_max, reverse_scratch_bytes(inf.width, inf.height, inf.levels, inf.ncomp));
+        scratch_sum += (reverse_scratch_bytes(inf.width, inf.height, inf.levels, inf.ncomp) + 255) & ~size_t(255);
         P->imgs.push_back(im);
         pool_total += (pool_lens[i] + 15) & ~uint64_t(15);
         P->ncblk += (int)parsed[i]->desc.size();
@@ -293,7 +309,7 @@ static int plan_build_parsed(tc_ctx *ctx, const Parsed *const *parsed, const uin
         (e = P->desc.ensure_on(sizeof(tc_cblk_desc) * std::max(1, P->ncblk), st, mp)) != cudaSuccess ||
         (e = P->order.ensure_on(sizeof(uint32_t) * std::max(1, P->ncblk), st, mp)) != cudaSuccess ||
         (e = P->coef.ensure_on(std::max<uint64_t>(coef_total, 256), st, mp)) != cudaSuccess ||
-        (e = P->scratch.ensure_on(std::max<size_t>(scratch_max, 256), st, mp)) != cudaSuccess)
+        (e = P->scratch.ensure_on(std::max<size_t>(n > 1 ? scratch_sum : scratch_max, 256), st, mp)) != cudaSuccess)
         return cuda_status(ctx, e, "plan allocation");
     if ((e = cudaMemcpyAsync(P->pool.ptr, hpool, pool_bytes, cudaMemcpyHostToDevice, ctx->stream)) ||
         (e = cudaMemcpyAsync(P->desc.ptr, hdesc, sizeof(tc_cblk_desc) * P->ncblk, cudaMemcpyHostToDevice,
@@ -322,6 +338,172 @@ static int plan_build(tc_ctx *ctx, const uint8_t *const *cs, const size_t *lens,
     return plan_build_parsed(ctx, pp.data(), pools.data(), plens.data(), n, P);
 }
 
+// Reverse DWT of every image of a batch plan with one launch per level step
+// and kind instead of per image and level: at step t image i runs its level
+// L_i - t, so images of different sizes and level counts share the launches.
+// Intermediate levels are grouped by wavelet (each job one component plane);
+// last levels, fused with colour, by wavelet, colour transform, component
+// count, sample type and bit depth.  The job table is built on the host and
+// uploaded once per set of output buffers (a replayed graph needs no copy).
+static int run_reverse_batched(tc_plan *P, void *const *d_out)
+{
+    tc_ctx *ctx = P->ctx;
+    const size_t nimg = P->imgs.size();
+    std::vector<void *> outs(d_out, d_out + nimg);
+    cudaError_t e;
+    auto image_ptrs = [&](size_t i, void **cptr, void **optr) {
+        const tc_image_info &inf = P->imgs[i].info;
+        char *coef = static_cast<char *>(P->coef.ptr) + P->imgs[i].coef_off;
+        const size_t plane = (size_t)inf.width * inf.height;
+        const int ob = sample_bytes(inf.bits);
+        for (int c = 0; c < inf.ncomp; c++) {
+            cptr[c] = coef + (size_t)c * plane * 4;
+            optr[c] = static_cast<char *>(d_out[i]) + (size_t)c * plane * ob;
+        }
+    };
+    auto color_of = [](const tc_image_info &inf) {
+        return inf.mct && inf.ncomp >= 3 ? (inf.reversible ? TC_COLOR_RCT : TC_COLOR_ICT) : TC_COLOR_DC;
+    };
+    // images without a transform: colour only
+    for (size_t i = 0; i < nimg; i++) {
+        const tc_image_info &inf = P->imgs[i].info;
+        if (inf.levels) continue;
+        void *cptr[4], *optr[4];
+        image_ptrs(i, cptr, optr);
+        const int ob = sample_bytes(inf.bits);
+        e = launch_color_inverse(ctx, color_of(inf), inf.ncomp, cptr, inf.reversible ? TC_INT32 : TC_FLOAT32,
+                                 inf.width, optr, ob == 1 ? TC_U8 : TC_U16, inf.width, inf.width, inf.height,
+                                 inf.bits);
+        if (e != cudaSuccess) return cuda_status(ctx, e, "colour");
+    }
+    if (outs != P->jobs_outs) {
+        std::vector<RevJob> jobs;
+        std::vector<tc_plan::DwtLaunch> launches;
+        struct Walk {
+            std::vector<int> ws, hs;
+            const void *src[4];
+            int src_pitch;
+            size_t slab;
+            char *scratch;
+        };
+        std::vector<Walk> wk(nimg);
+        int maxl = 0;
+        for (size_t i = 0; i < nimg; i++) {
+            const tc_image_info &inf = P->imgs[i].info;
+            Walk &W = wk[i];
+            level_sizes(inf.width, inf.height, inf.levels, W.ws, W.hs);
+            void *cptr[4], *optr[4];
+            image_ptrs(i, cptr, optr);
+            for (int c = 0; c < inf.ncomp; c++) W.src[c] = cptr[c];
+            W.src_pitch = inf.width;
+            W.slab = inf.levels >= 1 ? (size_t)W.ws[1] * W.hs[1] * 4 : 0;
+            W.scratch = static_cast<char *>(P->scratch.ptr) + P->scratch_off[i];
+            maxl = std::max(maxl, inf.levels);
+        }
+        for (int t = 0; t < maxl; t++) {
+            // intermediate levels, by wavelet
+            for (int wv = 0; wv < 2; wv++) {
+                const int first = (int)jobs.size();
+                int tiles = 0, tx, ty;
+                rev_tile_shape(wv, &tx, &ty);
+                for (size_t i = 0; i < nimg; i++) {
+                    const tc_image_info &inf = P->imgs[i].info;
+                    const int l = inf.levels - t;
+                    if (l < 2 || (inf.reversible ? 0 : 1) != wv) continue;
+                    Walk &W = wk[i];
+                    void *cptr[4], *optr[4];
+                    image_ptrs(i, cptr, optr);
+                    const int buf = (inf.levels - l) & 1;
+                    for (int c = 0; c < inf.ncomp; c++) {
+                        RevJob J{};
+                        J.io.w = W.ws[l - 1];
+                        J.io.h = W.hs[l - 1];
+                        J.io.ncomp = 1;
+                        J.io.ll[0] = W.src[c];
+                        J.io.ll_pitch = W.src_pitch;
+                        J.io.coef[0] = cptr[c];
+                        J.io.coef_pitch = inf.width;
+                        J.io.out[0] = W.scratch + ((size_t)c * 2 + buf) * W.slab;
+                        J.io.out_pitch = W.ws[1];
+                        J.tiles_x = (J.io.w + tx - 1) / tx;
+                        J.tile0 = tiles;
+                        tiles += J.tiles_x * ((J.io.h + ty - 1) / ty);
+                        jobs.push_back(J);
+                    }
+                    for (int c = 0; c < inf.ncomp; c++) W.src[c] = W.scratch + ((size_t)c * 2 + buf) * W.slab;
+                    W.src_pitch = W.ws[1];
+                }
+                if ((int)jobs.size() > first)
+                    launches.push_back({first, (int)jobs.size() - first, tiles, wv, -1, 1, 0, 0});
+            }
+            // last levels with colour, by kernel instance
+            std::vector<char> taken(nimg, 0);
+            for (size_t i0 = 0; i0 < nimg; i0++) {
+                const tc_image_info &a = P->imgs[i0].info;
+                if (taken[i0] || a.levels - t != 1) continue;
+                const int first = (int)jobs.size();
+                int tiles = 0, tx, ty;
+                const int wv = a.reversible ? 0 : 1;
+                rev_tile_shape(wv, &tx, &ty);
+                for (size_t i = i0; i < nimg; i++) {
+                    const tc_image_info &inf = P->imgs[i].info;
+                    if (taken[i] || inf.levels - t != 1 || inf.reversible != a.reversible ||
+                        color_of(inf) != color_of(a) || inf.ncomp != a.ncomp ||
+                        sample_bytes(inf.bits) != sample_bytes(a.bits) || inf.bits != a.bits)
+                        continue;
+                    taken[i] = 1;
+                    Walk &W = wk[i];
+                    void *cptr[4], *optr[4];
+                    image_ptrs(i, cptr, optr);
+                    RevJob J{};
+                    J.io.w = W.ws[0];
+                    J.io.h = W.hs[0];
+                    J.io.ncomp = inf.ncomp;
+                    J.io.ll_pitch = W.src_pitch;
+                    J.io.coef_pitch = inf.width;
+                    J.io.out_pitch = inf.width;
+                    for (int c = 0; c < inf.ncomp; c++) {
+                        J.io.ll[c] = W.src[c];
+                        J.io.coef[c] = cptr[c];
+                        J.io.out[c] = optr[c];
+                    }
+                    J.tiles_x = (J.io.w + tx - 1) / tx;
+                    J.tile0 = tiles;
+                    tiles += J.tiles_x * ((J.io.h + ty - 1) / ty);
+                    jobs.push_back(J);
+                }
+                launches.push_back({first, (int)jobs.size() - first, tiles, wv, color_of(a), a.ncomp,
+                                    sample_bytes(a.bits) == 1 ? TC_U8 : TC_U16, a.bits});
+            }
+        }
+        // the previous table's upload must be done before its staging is rewritten
+        if (P->jobs_uploaded && (e = cudaEventSynchronize(P->jobs_uploaded)) != cudaSuccess)
+            return cuda_status(ctx, e, "DWT job table");
+        const size_t bytes = std::max<size_t>(jobs.size(), 1) * sizeof(RevJob);
+        cudaMemPool_t mp = nullptr;
+        if ((e = P->h_jobs.ensure(bytes)) != cudaSuccess || (e = ctx_mem_pool(ctx, &mp)) != cudaSuccess ||
+            (e = P->jobs.ensure_on(bytes, ctx->stream, mp)) != cudaSuccess)
+            return cuda_status(ctx, e, "DWT job table");
+        if (!jobs.empty()) std::memcpy(P->h_jobs.ptr, jobs.data(), jobs.size() * sizeof(RevJob));
+        if (!P->jobs_uploaded && (e = cudaEventCreateWithFlags(&P->jobs_uploaded, cudaEventDisableTiming)) !=
+                                     cudaSuccess)
+            return cuda_status(ctx, e, "DWT job table");
+        if ((e = cudaMemcpyAsync(P->jobs.ptr, P->h_jobs.ptr, jobs.size() * sizeof(RevJob), cudaMemcpyHostToDevice,
+                                 ctx->stream)) != cudaSuccess ||
+            (e = cudaEventRecord(P->jobs_uploaded, ctx->stream)) != cudaSuccess)
+            return cuda_status(ctx, e, "DWT job table");
+        P->dwt_launches = launches;
+        P->jobs_outs = outs;
+    }
+    const RevJob *dj = static_cast<const RevJob *>(P->jobs.ptr);
+    for (const tc_plan::DwtLaunch &L : P->dwt_launches) {
+        e = launch_idwt_batch(ctx, dj + L.first, L.njobs, L.ntiles, L.wavelet, TC_ROUND_FLOOR, L.color, L.ncomp,
+                              L.otype, L.bits);
+        if (e != cudaSuccess) return cuda_status(ctx, e, "reverse DWT (batched)");
+    }
+    return TC_OK;
+}
+
 static int plan_run(tc_plan *P, void *const *d_out)
 {
     tc_ctx *ctx = P->ctx;
@@ -333,6 +515,12 @@ static int plan_run(tc_plan *P, void *const *d_out)
                                       TC_T1_OUT_DEQUANT, P->recon_r);
     if (e != cudaSuccess) return cuda_status(ctx, e, "Tier-1 launch");
     if (P->profiling) cudaEventRecord(P->ev[1], ctx->stream);
+    if (P->imgs.size() > 1) {
+        const int rc = run_reverse_batched(P, d_out);
+        if (rc) return rc;
+        if (P->profiling) cudaEventRecord(P->ev[2], ctx->stream);
+        return TC_OK;
+    }
     for (size_t i = 0; i < P->imgs.size(); i++) {
         const tc_image_info &inf = P->imgs[i].info;
         char *coef = static_cast<char *>(P->coef.ptr) + P->imgs[i].coef_off;
@@ -758,6 +946,9 @@ int tc_plan_destroy(tc_plan *P)
     P->h_pool.release();
     P->h_desc.release();
     P->h_order.release();
+    P->h_jobs.release();
+    P->jobs.release();
+    if (P->jobs_uploaded) cudaEventDestroy(P->jobs_uploaded);
     for (auto &e : P->ev)
         if (e) cudaEventDestroy(e);
     plan_drop_graph(P);

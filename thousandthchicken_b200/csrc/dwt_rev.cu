@@ -104,8 +104,9 @@ __device__ __forceinline__ int to_int(T v)
 template <typename T>
 using Vec4 = typename std::conditional<std::is_same<T, float>::value, float4, int4>::type;
 
+// The CTA's work: tile (bx, by) of level `io`, components from cbase.
 template <typename T, int WAVELET, int RND, int NCOMP, int COLOR, typename OT>
-__global__ void __launch_bounds__(kThreads) idwt_rev_kernel(LevelIO io, int bits)
+__device__ __forceinline__ void rev_tile(const LevelIO &io, int bits, int bx, int by, int cbase)
 {
     using G = RevGeo<WAVELET>;
     constexpr int H = G::H, NR = G::NR, TY = G::TY, TX = G::TX, NC = G::NC, S = G::S;
@@ -114,9 +115,8 @@ __global__ void __launch_bounds__(kThreads) idwt_rev_kernel(LevelIO io, int bits
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *tiles = reinterpret_cast<T *>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+    const int x0 = bx * TX, y0 = by * TY;
     const int w = io.w, h = io.h, wl = (w + 1) >> 1, hl = (h + 1) >> 1;
-    const int cbase = PLANE ? blockIdx.z : 0;
 
     // 1. load the extended tiles from the four subbands (Mallat layout) with
     //    4-byte asynchronous copies, so a thread has its whole share of the
@@ -268,34 +268,92 @@ __global__ void __launch_bounds__(kThreads) idwt_rev_kernel(LevelIO io, int bits
     }
 }
 
+// One level of one image: tiles (blockIdx.x, blockIdx.y), one component per
+// blockIdx.z for plane levels.
 template <typename T, int WAVELET, int RND, int NCOMP, int COLOR, typename OT>
-cudaError_t run_rev(tc_ctx *ctx, const LevelIO &io, int bits)
+__global__ void __launch_bounds__(kThreads) idwt_rev_kernel(LevelIO io, int bits)
+{
+    rev_tile<T, WAVELET, RND, NCOMP, COLOR, OT>(io, bits, blockIdx.x, blockIdx.y, COLOR < 0 ? blockIdx.z : 0);
+}
+
+// One level of many images (or planes) of mixed sizes in one launch: the
+// jobs' tiles are numbered consecutively (job j owns tiles
+// [jobs[j].tile0, jobs[j+1].tile0)), and each CTA finds its job by binary
+// search.
+template <typename T, int WAVELET, int RND, int NCOMP, int COLOR, typename OT>
+__global__ void __launch_bounds__(kThreads) idwt_rev_batch_kernel(const RevJob *__restrict__ jobs, int njobs,
+                                                                  int bits)
+{
+    const int b = blockIdx.x;
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (jobs[mid].tile0 <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    const RevJob &J = jobs[lo];
+    const int t = b - J.tile0;
+    rev_tile<T, WAVELET, RND, NCOMP, COLOR, OT>(J.io, bits, t % J.tiles_x, t / J.tiles_x, 0);
+}
+
+template <typename T, int WAVELET, int NCOMP, int COLOR>
+constexpr size_t rev_smem()
+{
+    return (size_t)(COLOR < 0 ? 1 : NCOMP) * RevGeo<WAVELET>::NR * RevGeo<WAVELET>::S * sizeof(T);
+}
+
+template <typename K>
+cudaError_t set_smem_once(tc_ctx *ctx, K kernel, size_t smem, bool (&done)[64])
+{
+    if (done[ctx->device & 63]) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) done[ctx->device & 63] = true;
+    return e;
+}
+
+// A launch of one level: a single image (batch == nullptr, io given) or the
+// jobs of a batch (njobs jobs, ntiles tiles in all).
+struct RevLaunch {
+    const LevelIO *io = nullptr;
+    const RevJob *jobs = nullptr;
+    int njobs = 0, ntiles = 0;
+};
+
+template <typename T, int WAVELET, int RND, int NCOMP, int COLOR, typename OT>
+cudaError_t run_rev(tc_ctx *ctx, const RevLaunch &L, int bits)
 {
     using G = RevGeo<WAVELET>;
-    constexpr int NT = COLOR < 0 ? 1 : NCOMP;
-    constexpr size_t smem = (size_t)NT * G::NR * G::S * sizeof(T);
-    static bool attr[64] = {};
-    if (!attr[ctx->device & 63]) {
-        cudaError_t e = cudaFuncSetAttribute(idwt_rev_kernel<T, WAVELET, RND, NCOMP, COLOR, OT>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        attr[ctx->device & 63] = true;
+    constexpr size_t smem = rev_smem<T, WAVELET, NCOMP, COLOR>();
+    cudaError_t e;
+    if (L.io) {
+        static bool attr[64] = {};
+        if ((e = set_smem_once(ctx, idwt_rev_kernel<T, WAVELET, RND, NCOMP, COLOR, OT>, smem, attr)) != cudaSuccess)
+            return e;
+        const LevelIO &io = *L.io;
+        dim3 grid((io.w + G::TX - 1) / G::TX, (io.h + G::TY - 1) / G::TY, COLOR < 0 ? io.ncomp : 1);
+        idwt_rev_kernel<T, WAVELET, RND, NCOMP, COLOR, OT><<<grid, kThreads, smem, ctx->stream>>>(io, bits);
+    } else {
+        if (L.njobs <= 0 || L.ntiles <= 0) return cudaSuccess;
+        static bool attr[64] = {};
+        if ((e = set_smem_once(ctx, idwt_rev_batch_kernel<T, WAVELET, RND, NCOMP, COLOR, OT>, smem, attr)) !=
+            cudaSuccess)
+            return e;
+        idwt_rev_batch_kernel<T, WAVELET, RND, NCOMP, COLOR, OT>
+            <<<L.ntiles, kThreads, smem, ctx->stream>>>(L.jobs, L.njobs, bits);
     }
-    dim3 grid((io.w + G::TX - 1) / G::TX, (io.h + G::TY - 1) / G::TY, COLOR < 0 ? io.ncomp : 1);
-    idwt_rev_kernel<T, WAVELET, RND, NCOMP, COLOR, OT><<<grid, kThreads, smem, ctx->stream>>>(io, bits);
     ctx->launches++;
     return cudaGetLastError();
 }
 
 template <typename T, int WAVELET, int RND, int COLOR>
-cudaError_t run_last(tc_ctx *ctx, const LevelIO &io, int out_type, int bits)
+cudaError_t run_last(tc_ctx *ctx, const RevLaunch &L, int ncomp, int out_type, int bits)
 {
-#define TC_LAST(NC_)                                                                         \
-    (out_type == TC_U8    ? run_rev<T, WAVELET, RND, NC_, COLOR, uint8_t>(ctx, io, bits)  \
-     : out_type == TC_U16 ? run_rev<T, WAVELET, RND, NC_, COLOR, uint16_t>(ctx, io, bits) \
-                          : run_rev<T, WAVELET, RND, NC_, COLOR, int32_t>(ctx, io, bits))
-    if (COLOR != TC_COLOR_DC) return io.ncomp == 4 ? TC_LAST(4) : TC_LAST(3);
-    switch (io.ncomp) {
+#define TC_LAST(NC_)                                                                        \
+    (out_type == TC_U8    ? run_rev<T, WAVELET, RND, NC_, COLOR, uint8_t>(ctx, L, bits)  \
+     : out_type == TC_U16 ? run_rev<T, WAVELET, RND, NC_, COLOR, uint16_t>(ctx, L, bits) \
+                          : run_rev<T, WAVELET, RND, NC_, COLOR, int32_t>(ctx, L, bits))
+    if (COLOR != TC_COLOR_DC) return ncomp == 4 ? TC_LAST(4) : TC_LAST(3);
+    switch (ncomp) {
     case 1: return TC_LAST(1);
     case 2: return TC_LAST(2);
     case 3: return TC_LAST(3);
@@ -304,29 +362,60 @@ cudaError_t run_last(tc_ctx *ctx, const LevelIO &io, int out_type, int bits)
 #undef TC_LAST
 }
 
+cudaError_t plane_level(tc_ctx *ctx, const RevLaunch &L, int wavelet, int rounding)
+{
+    if (wavelet) return run_rev<float, 1, 0, 1, -1, float>(ctx, L, 0);
+    if (rounding == TC_ROUND_TRUNC) return run_rev<int32_t, 0, TC_ROUND_TRUNC, 1, -1, int32_t>(ctx, L, 0);
+    return run_rev<int32_t, 0, TC_ROUND_FLOOR, 1, -1, int32_t>(ctx, L, 0);
+}
+
+cudaError_t last_level(tc_ctx *ctx, const RevLaunch &L, int ncomp, int wavelet, int color, int out_type, int bits)
+{
+    if (color != TC_COLOR_DC && ncomp < 3) color = TC_COLOR_DC;
+    if (wavelet) {
+        if (color == TC_COLOR_ICT || color == TC_COLOR_RCT)
+            return run_last<float, 1, 0, TC_COLOR_ICT>(ctx, L, ncomp, out_type, bits);
+        return run_last<float, 1, 0, TC_COLOR_DC>(ctx, L, ncomp, out_type, bits);
+    }
+    if (color == TC_COLOR_RCT || color == TC_COLOR_ICT)
+        return run_last<int32_t, 0, TC_ROUND_FLOOR, TC_COLOR_RCT>(ctx, L, ncomp, out_type, bits);
+    return run_last<int32_t, 0, TC_ROUND_FLOOR, TC_COLOR_DC>(ctx, L, ncomp, out_type, bits);
+}
+
 }  // namespace
 
 cudaError_t launch_idwt_level(tc_ctx *ctx, const LevelIO &io, int wavelet, int rounding)
 {
     if (io.w <= 0 || io.h <= 0) return cudaSuccess;
-    if (wavelet) return run_rev<float, 1, 0, 1, -1, float>(ctx, io, 0);
-    if (rounding == TC_ROUND_TRUNC) return run_rev<int32_t, 0, TC_ROUND_TRUNC, 1, -1, int32_t>(ctx, io, 0);
-    return run_rev<int32_t, 0, TC_ROUND_FLOOR, 1, -1, int32_t>(ctx, io, 0);
+    RevLaunch L;
+    L.io = &io;
+    return plane_level(ctx, L, wavelet, rounding);
 }
 
 cudaError_t launch_idwt_last_color(tc_ctx *ctx, const LevelIO &io, int wavelet, int color, int out_type, int bits,
                                    bool)
 {
     if (io.w <= 0 || io.h <= 0) return cudaSuccess;
-    if (color != TC_COLOR_DC && io.ncomp < 3) color = TC_COLOR_DC;
-    if (wavelet) {
-        if (color == TC_COLOR_ICT || color == TC_COLOR_RCT)
-            return run_last<float, 1, 0, TC_COLOR_ICT>(ctx, io, out_type, bits);
-        return run_last<float, 1, 0, TC_COLOR_DC>(ctx, io, out_type, bits);
-    }
-    if (color == TC_COLOR_RCT || color == TC_COLOR_ICT)
-        return run_last<int32_t, 0, TC_ROUND_FLOOR, TC_COLOR_RCT>(ctx, io, out_type, bits);
-    return run_last<int32_t, 0, TC_ROUND_FLOOR, TC_COLOR_DC>(ctx, io, out_type, bits);
+    RevLaunch L;
+    L.io = &io;
+    return last_level(ctx, L, io.ncomp, wavelet, color, out_type, bits);
+}
+
+void rev_tile_shape(int wavelet, int *tx, int *ty)
+{
+    *tx = wavelet ? RevGeo<1>::TX : RevGeo<0>::TX;
+    *ty = wavelet ? RevGeo<1>::TY : RevGeo<0>::TY;
+}
+
+cudaError_t launch_idwt_batch(tc_ctx *ctx, const RevJob *d_jobs, int njobs, int ntiles, int wavelet, int rounding,
+                              int color, int ncomp, int out_type, int bits)
+{
+    RevLaunch L;
+    L.jobs = d_jobs;
+    L.njobs = njobs;
+    L.ntiles = ntiles;
+    if (color < 0) return plane_level(ctx, L, wavelet, rounding);
+    return last_level(ctx, L, ncomp, wavelet, color, out_type, bits);
 }
 
 }  // namespace tc

@@ -125,6 +125,22 @@ struct LevelIO {
 
 // wavelet: 0 = 5/3 int32, 1 = 9/7 float.  rounding: TC_ROUND_*.
 cudaError_t launch_idwt_level(tc_ctx *ctx, const LevelIO &io, int wavelet, int rounding);
+
+// A reverse level of one plane (plane levels) or one image (last level with
+// colour) inside a batched launch; tile0 is the index of its first tile among
+// the launch's tiles, tiles_x its tiles per row (see rev_tile_shape).
+struct RevJob {
+    LevelIO io;
+    int tiles_x;
+    int tile0;
+};
+void rev_tile_shape(int wavelet, int *tx, int *ty);
+// One launch over the jobs d_jobs[0..njobs) (device memory, tile0 ascending,
+// ntiles tiles in all), all of one kind: plane levels when color < 0 (each
+// job one component), else last levels with colour of ncomp components
+// writing out_type samples of `bits` bits.
+cudaError_t launch_idwt_batch(tc_ctx *ctx, const RevJob *d_jobs, int njobs, int ntiles, int wavelet, int rounding,
+                              int color, int ncomp, int out_type, int bits);
 cudaError_t launch_fdwt_level(tc_ctx *ctx, const LevelIO &io, int wavelet, int rounding);
 
 // Last reverse level fused with the inverse colour transform, DC shift,
