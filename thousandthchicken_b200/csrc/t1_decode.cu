@@ -197,37 +197,24 @@ struct MQ {
         c <<= sh;
         ct -= sh;
     }
+    // One decision.  The interval arithmetic of ISO C.3.2 (both the MPS and
+    // the LPS sub-interval, with the conditional exchange) is done with
+    // selects; the one branch left is the renormalisation, which is also
+    // where the context's state moves on.
     __device__ __forceinline__ uint32_t decode(uint32_t *ctx, const uint32_t *tbl, int cx)
     {
         const uint32_t w = ctx[cx];
         const uint32_t qs = w & 0xFFFF0000u, mps = w & 1u;
-        a -= qs;
-        if (c < qs) {
-            // LPS_EXCHANGE
-            uint32_t d;
-            if (a < qs) {
-                d = mps;
-                ctx[cx] = tbl[(w >> 1) & 63] | mps;
-            } else {
-                d = mps ^ 1u;
-                ctx[cx] = tbl[(w >> 7) & 63] | (mps ^ ((w >> 13) & 1u));
-            }
-            a = qs;
+        const uint32_t a1 = a - qs;
+        const bool lower = c < qs;   // the code value lies in the Qe sub-interval
+        const bool exch = a1 < qs;   // the conditional exchange swaps the symbols
+        const uint32_t d = mps ^ (uint32_t)(lower != exch);
+        c = lower ? c : c - qs;
+        a = lower ? qs : a1;
+        if (lower || (int)a1 >= 0) {
+            ctx[cx] = d != mps ? (tbl[(w >> 7) & 63] | (mps ^ ((w >> 13) & 1u))) : (tbl[(w >> 1) & 63] | mps);
             renorm();
-            return d;
         }
-        c -= qs;
-        if ((int)a < 0) return mps;
-        // MPS_EXCHANGE
-        uint32_t d;
-        if (a < qs) {
-            d = mps ^ 1u;
-            ctx[cx] = tbl[(w >> 7) & 63] | (mps ^ ((w >> 13) & 1u));
-        } else {
-            d = mps;
-            ctx[cx] = tbl[(w >> 1) & 63] | mps;
-        }
-        renorm();
         return d;
     }
 };
