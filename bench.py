@@ -273,6 +273,83 @@ def cpu_baseline(cores):
             "sample": f"{w}x{h}x3 image of the same generator and coding parameters, oracle full decode"}
 
 
+def kernels_section(ctx, stream, flush, cs, hbm):
+    """The stand-alone stage kernels on device-resident 4096x4096 data, each
+    timed with CUDA events on the context's stream (median of 5 runs, L2
+    flushed before each): achieved GB/s of algorithmic bytes against the
+    measured copy bandwidth."""
+    import torch
+    from thousandthchicken_b200 import codec
+    from thousandthchicken_b200.stages import (CoefficientCoder, DWTForward53, DWTForward97, DWTReverse97,
+                                               Preprocessor, Quantizer, _dev_bytes)
+    dev = torch.device("cuda", ctx.device)
+    W = H = 4096
+    g = torch.Generator(device=dev).manual_seed(3)
+
+    def timed(fn):
+        ms = []
+        with torch.cuda.stream(stream):
+            fn()
+            for k in range(5):
+                flush.fill_(k & 0xFF)
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                fn()
+                b.record(stream)
+                b.synchronize()
+                ms.append(a.elapsed_time(b))
+        return sorted(ms)[2]
+
+    def entry(ms, nbytes, what):
+        gbs = nbytes / (ms / 1000.0) / 1e9
+        return {"ms": round(ms, 4), "bytes": int(nbytes), "gbs": round(gbs, 1), "frac": round(gbs / hbm, 4),
+                "what": what}
+
+    out = {}
+    lv = 6
+    xf = torch.randn((H, W), generator=g, device=dev) * 64
+    yf = torch.empty_like(xf)
+    zf = torch.empty_like(xf)
+    db = sum(8 * w_ * h_ for w_, h_ in _level_dims(W, H, lv))  # 4 B read + 4 B written per sample and level
+    out["forward_97"] = entry(timed(lambda: DWTForward97(ctx).run(xf, yf, W, H, lv)), db,
+                              "tc_dwt_forward97, one 4096^2 fp32 plane, 6 levels")
+    out["reverse_97"] = entry(timed(lambda: DWTReverse97(ctx).run(yf, zf, W, H, lv)), db,
+                              "tc_dwt_reverse97, one 4096^2 fp32 plane, 6 levels")
+    xi = torch.randint(-128, 128, (H, W), generator=g, device=dev, dtype=torch.int32)
+    yi = torch.empty_like(xi)
+    out["forward_53"] = entry(timed(lambda: DWTForward53(ctx).run(xi, yi, W, H, 5)),
+                              sum(8 * w_ * h_ for w_, h_ in _level_dims(W, H, 5)),
+                              "tc_dwt_forward53, one 4096^2 int32 plane, 5 levels")
+    planes = [torch.randn((H, W), generator=g, device=dev) * 40 for _ in range(3)]
+    px8 = [torch.empty((H, W), dtype=torch.uint8, device=dev) for _ in range(3)]
+    pre = Preprocessor(ctx)
+    out["colour_inverse_ict"] = entry(timed(lambda: pre.color_decoder_lossy(planes, px8, 8)), 3 * W * H * 5,
+                                      "tc_color_inverse ICT, 3 x 4096^2 fp32 in, 8-bit out")
+    fl = [torch.empty((H, W), device=dev) for _ in range(3)]
+    out["colour_forward_ict"] = entry(timed(lambda: pre.color_coder_lossy(px8, fl, 8)), 3 * W * H * 5,
+                                      "tc_color_forward ICT, 3 x 4096^2 8-bit in, fp32 out")
+    info, desc, pool = codec.parse(cs)
+    n = info["ncomp"] * W * H
+    cc = CoefficientCoder(ctx)
+    raw = cc.decode_blocks(desc, pool, n, raw=True)
+    deq = torch.empty(n, dtype=torch.float32, device=dev)
+    d_desc = _dev_bytes(np.ascontiguousarray(desc, codec.DESC_DTYPE), dev)
+    q = Quantizer(ctx)
+    out["dequantize_raw"] = entry(timed(lambda: q.dequantize(d_desc, len(desc), raw, deq, 0.5)), 8 * n,
+                                  "tc_dequantize_raw over the 4096^2 x 3 workload's 12288 blocks")
+    ctx.synchronize()
+    return out
+
+
+def _level_dims(w, h, levels):
+    """(width, height) of each level's region, the full size first."""
+    dims = []
+    for _ in range(levels):
+        dims.append((w, h))
+        w, h = (w + 1) // 2, (h + 1) // 2
+    return dims
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     from thousandthchicken_b200.stages import Context, Decoder, Plan
@@ -354,8 +431,9 @@ def run_ours(args, rank, world, local_rank):
         e2e_times.append(time.perf_counter() - t0)
     e2e_s = max_over_ranks(sum(e2e_times) / e2e_steps, dist, f"cuda:{local_rank}")
 
-    batched, served = None, None
+    batched, served, kernels = None, None, None
     if not args.core_only:
+        kernels = kernels_section(ctx, stream, flush, cs, measured_peaks()[0])
         # batched (one plan: one Tier-1 queue over every image) vs per-image plans
         mixed = make_mixed()
         streams = [cs_ for _, cs_ in mixed]
@@ -470,6 +548,7 @@ def run_ours(args, rank, world, local_rank):
         if batched is not None:
             line["batched_vs_per_image"] = batched
             line["served"] = served
+            line["kernels"] = kernels
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(os.cpu_count() or 1)
         print(json.dumps(line), flush=True)

@@ -3,6 +3,7 @@ inverse quantiser) against the CPU oracle: bit-exact for every output mode."""
 import numpy as np
 import pytest
 
+import oracle as O
 from conftest import golden_cases, load_golden
 from gpu_helpers import make_blocks, oracle_mallat, oracle_slots
 from thousandthchicken_b200 import codec
@@ -113,3 +114,36 @@ def test_t1_lane_group_widths_bit_exact(gpu_ctx, lanes):
         L.lib().tc_ctx_set_t1_group(gpu_ctx.handle, 32)
     np.testing.assert_array_equal(got, oracle_slots(desc, pool, "int", 0.5).reshape(-1))
     np.testing.assert_array_equal(raw, oracle_slots(desc, pool, "raw").reshape(-1).view(np.int32))
+
+
+@pytest.mark.parametrize("irreversible", [False, True])
+def test_standalone_dequantiser_matches_oracle(gpu_ctx, irreversible):
+    """tc_dequantize_raw over raw Tier-1 words (Quantizer::dequantize_tile):
+    every block's coefficients with the reconstruction offset of the last
+    decoded plane, against the oracle's dequantiser on the same words."""
+    from thousandthchicken_b200.stages import Quantizer, _dev_bytes
+    desc, pool, _ = make_blocks(seed=171, n=300, truncate=True)
+    raw = _coder(gpu_ctx).decode_blocks(desc, pool, len(desc) * 4096, raw=True)
+    rng = np.random.default_rng(5)
+    if irreversible:
+        desc["flags"] = 1
+        desc["step"] = rng.uniform(0.01, 4.0, len(desc)).astype(np.float32)
+    dt = torch.float32 if irreversible else torch.int32
+    out = torch.zeros(len(desc) * 4096, dtype=dt, device="cuda")
+    d_desc = _dev_bytes(np.ascontiguousarray(desc, codec.DESC_DTYPE), torch.device("cuda"))
+    Quantizer(gpu_ctx).dequantize(d_desc, len(desc), raw, out, 0.5)
+    gpu_ctx.synchronize()
+    got = out.cpu().numpy().reshape(len(desc), 64, 64)
+    words = raw.cpu().numpy().view(np.uint32).reshape(len(desc), 64, 64)
+    for i, d in enumerate(desc):
+        w, h, mb = int(d["w"]), int(d["h"]), int(d["mb"])
+        q = ((words[i, :h, :w] & 0x7FFFFFFF) >> (31 - mb)).astype(np.int32)
+        q = np.where(words[i, :h, :w] >> 31, -q, q)
+        numbps = mb - int(d["zero_bitplanes"])
+        u = max(numbps - 1 - (int(d["passes"]) + 1) // 3, 0) if numbps > 0 and d["passes"] > 0 else 0
+        uu = np.full(q.shape, u, np.uint8)
+        if irreversible:
+            want = O.dequant_float(q, uu, 0.5, float(d["step"]))
+            np.testing.assert_array_equal(got[i, :h, :w].view(np.int32), want.view(np.int32))
+        else:
+            np.testing.assert_array_equal(got[i, :h, :w], O.dequant_int(q, uu, 0.5))

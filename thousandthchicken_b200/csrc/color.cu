@@ -19,117 +19,222 @@ struct Planes {
     void *out[4];
 };
 
-template <typename T>
-__device__ __forceinline__ float ldf(const void *p, size_t i)
-{
-    return (float)static_cast<const T *>(p)[i];
-}
-
-template <typename IT>
-__device__ __forceinline__ IT ld(const void *p, size_t i)
-{
-    return static_cast<const IT *>(p)[i];
-}
-
 template <typename OT>
-__device__ __forceinline__ void st_clamped(void *p, size_t i, int v, int mx)
+__device__ __forceinline__ OT clamped(int v, int mx)
 {
-    static_cast<OT *>(p)[i] = (OT)(v < 0 ? 0 : (v > mx ? mx : v));
+    return (OT)(v < 0 ? 0 : (v > mx ? mx : v));
+}
+
+// Four consecutive samples of a row: one 16-byte (or 8/4-byte) access when
+// the row is aligned for it, else four scalar accesses; `n` of them valid.
+template <typename T>
+__device__ __forceinline__ void load4(const T *p, bool vec, int n, T (&v)[4])
+{
+    if (vec && n == 4) {
+        if constexpr (sizeof(T) == 4) {
+            const int4 q = *reinterpret_cast<const int4 *>(p);
+            if constexpr (std::is_integral<T>::value) {
+                v[0] = (T)q.x, v[1] = (T)q.y, v[2] = (T)q.z, v[3] = (T)q.w;
+            } else {
+                v[0] = __int_as_float(q.x), v[1] = __int_as_float(q.y), v[2] = __int_as_float(q.z),
+                v[3] = __int_as_float(q.w);
+            }
+        } else if constexpr (sizeof(T) == 2) {
+            const uint2 q = *reinterpret_cast<const uint2 *>(p);
+            v[0] = (T)(q.x & 0xFFFFu), v[1] = (T)(q.x >> 16), v[2] = (T)(q.y & 0xFFFFu), v[3] = (T)(q.y >> 16);
+        } else {
+            const uint32_t q = *reinterpret_cast<const uint32_t *>(p);
+            v[0] = (T)(q & 0xFF), v[1] = (T)((q >> 8) & 0xFF), v[2] = (T)((q >> 16) & 0xFF), v[3] = (T)(q >> 24);
+        }
+        return;
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++) v[j] = j < n ? p[j] : T(0);
+}
+
+template <typename T>
+__device__ __forceinline__ void store4(T *p, bool vec, int n, const T (&v)[4])
+{
+    if (vec && n == 4) {
+        if constexpr (sizeof(T) == 4) {
+            int4 q;
+            if constexpr (std::is_integral<T>::value) q = make_int4(v[0], v[1], v[2], v[3]);
+            else q = make_int4(__float_as_int(v[0]), __float_as_int(v[1]), __float_as_int(v[2]), __float_as_int(v[3]));
+            *reinterpret_cast<int4 *>(p) = q;
+        } else if constexpr (sizeof(T) == 2) {
+            *reinterpret_cast<uint2 *>(p) = make_uint2((uint32_t)(uint16_t)v[0] | ((uint32_t)(uint16_t)v[1] << 16),
+                                                       (uint32_t)(uint16_t)v[2] | ((uint32_t)(uint16_t)v[3] << 16));
+        } else {
+            *reinterpret_cast<uint32_t *>(p) = (uint32_t)(uint8_t)v[0] | ((uint32_t)(uint8_t)v[1] << 8) |
+                                               ((uint32_t)(uint8_t)v[2] << 16) | ((uint32_t)(uint8_t)v[3] << 24);
+        }
+        return;
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+        if (j < n) p[j] = v[j];
+}
+
+// Launch shape shared by the colour kernels: a thread covers four
+// consecutive samples of a row; blockIdx.y strides over rows.
+constexpr int kColThreads = 256;
+
+inline dim3 color_grid(int w, int h)
+{
+    const int gx = (w + 4 * kColThreads - 1) / (4 * kColThreads);
+    int gy = (148 * 16 + gx - 1) / gx;
+    if (gy > h) gy = h;
+    return dim3(gx, gy < 1 ? 1 : gy);
 }
 
 // Inverse: IT = int32_t or float input planes; OT = output sample type.
-template <typename IT, typename OT, int KIND>
-__global__ void color_inverse_kernel(Planes P, int ncomp, int in_pitch, int out_pitch, int w, int h,
-                                     int bits)
+// vin / vout: every input / output row is aligned for 4-sample accesses.
+template <typename IT, typename OT, int KIND, int NC>
+__global__ void __launch_bounds__(kColThreads) color_inverse_kernel(Planes P, int in_pitch, int out_pitch, int w,
+                                                                    int h, int bits, bool vin, bool vout)
 {
-    const size_t n = (size_t)w * h;
+    const int x0 = 4 * (blockIdx.x * kColThreads + threadIdx.x);
+    if (x0 >= w) return;
+    const int n = min(4, w - x0);
     const int dc = 1 << (bits - 1), mx = (1 << bits) - 1;
-    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
-        const int y = (int)(q / w), x = (int)(q % w);
-        const size_t ii = (size_t)y * in_pitch + x, oi = (size_t)y * out_pitch + x;
-        int v[4];
-        for (int c = 0; c < ncomp; c++) {
-            if constexpr (std::is_integral<IT>::value) v[c] = (int)ld<IT>(P.in[c], ii);
-            else v[c] = __float2int_rn((float)ld<IT>(P.in[c], ii));
+    for (int y = blockIdx.y; y < h; y += gridDim.y) {
+        const size_t ii = (size_t)y * in_pitch + x0, oi = (size_t)y * out_pitch + x0;
+        IT a[NC][4];
+#pragma unroll
+        for (int c = 0; c < NC; c++) load4<IT>(static_cast<const IT *>(P.in[c]) + ii, vin, n, a[c]);
+        OT o[NC][4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            int v[NC];
+            if constexpr (KIND == TC_COLOR_RCT && NC >= 3) {
+                // tcr_kernel, preprocess_rct_inverse.cl:18-36
+                const int Y = (int)a[0][j], U = (int)a[1][j], V = (int)a[2][j];
+                const int G = Y - ((U + V) >> 2);
+                v[0] = V + G;
+                v[1] = G;
+                v[2] = U + G;
+            } else if constexpr (KIND == TC_COLOR_ICT && NC >= 3) {
+                // ISO G.2 inverse ICT (tci_kernel's constants are defect D9)
+                const float Y = (float)a[0][j], Cb = (float)a[1][j], Cr = (float)a[2][j];
+                v[0] = __float2int_rn(fmaf(1.402f, Cr, Y));
+                v[1] = __float2int_rn(Y - 0.34413f * Cb - 0.71414f * Cr);
+                v[2] = __float2int_rn(fmaf(1.772f, Cb, Y));
+            }
+            constexpr int c0 = (KIND != TC_COLOR_DC && NC >= 3) ? 3 : 0;
+#pragma unroll
+            for (int c = c0; c < NC; c++) {
+                if constexpr (std::is_integral<IT>::value) v[c] = (int)a[c][j];
+                else v[c] = __float2int_rn((float)a[c][j]);
+            }
+#pragma unroll
+            for (int c = 0; c < NC; c++) o[c][j] = clamped<OT>(v[c] + dc, mx);
         }
-        if constexpr (KIND == TC_COLOR_RCT) {
-            // tcr_kernel, preprocess_rct_inverse.cl:18-36
-            const int Y = (int)ld<IT>(P.in[0], ii), U = (int)ld<IT>(P.in[1], ii), V = (int)ld<IT>(P.in[2], ii);
-            const int G = Y - ((U + V) >> 2);
-            v[0] = V + G;
-            v[1] = G;
-            v[2] = U + G;
-        } else if constexpr (KIND == TC_COLOR_ICT) {
-            // ISO G.2 inverse ICT (tci_kernel's constants are defect D9)
-            const float Y = (float)ld<IT>(P.in[0], ii), Cb = (float)ld<IT>(P.in[1], ii),
-                        Cr = (float)ld<IT>(P.in[2], ii);
-            v[0] = __float2int_rn(fmaf(1.402f, Cr, Y));
-            v[1] = __float2int_rn(Y - 0.34413f * Cb - 0.71414f * Cr);
-            v[2] = __float2int_rn(fmaf(1.772f, Cb, Y));
-        }
-        for (int c = 0; c < ncomp; c++) st_clamped<OT>(P.out[c], oi, v[c] + dc, mx);
+#pragma unroll
+        for (int c = 0; c < NC; c++) store4<OT>(static_cast<OT *>(P.out[c]) + oi, vout, n, o[c]);
     }
 }
 
 // Forward: unsigned samples -> DC shift + RCT (int32 out) / ICT (float out)
 // / DC only (int32 or float out).
-template <typename IT, typename OT, int KIND>
-__global__ void color_forward_kernel(Planes P, int ncomp, int in_pitch, int out_pitch, int w, int h,
-                                     int bits)
+template <typename IT, typename OT, int KIND, int NC>
+__global__ void __launch_bounds__(kColThreads) color_forward_kernel(Planes P, int in_pitch, int out_pitch, int w,
+                                                                    int h, int bits, bool vin, bool vout)
 {
-    const size_t n = (size_t)w * h;
+    const int x0 = 4 * (blockIdx.x * kColThreads + threadIdx.x);
+    if (x0 >= w) return;
+    const int n = min(4, w - x0);
     const int dc = 1 << (bits - 1);
-    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
-        const int y = (int)(q / w), x = (int)(q % w);
-        const size_t ii = (size_t)y * in_pitch + x, oi = (size_t)y * out_pitch + x;
-        int s[4];
-        for (int c = 0; c < ncomp; c++) s[c] = (int)ld<IT>(P.in[c], ii) - dc;
-        int c0 = 0;
-        if constexpr (KIND == TC_COLOR_RCT) {
-            // rct_kernel, preprocess_rct.cl:18-31
-            static_cast<OT *>(P.out[0])[oi] = (OT)((s[0] + 2 * s[1] + s[2]) >> 2);
-            static_cast<OT *>(P.out[1])[oi] = (OT)(s[2] - s[1]);
-            static_cast<OT *>(P.out[2])[oi] = (OT)(s[0] - s[1]);
-            c0 = 3;
-        } else if constexpr (KIND == TC_COLOR_ICT) {
-            // ict_kernel, preprocess_ict.cl:20-37 (kept in float, no rounding)
-            const float R = (float)s[0], G = (float)s[1], B = (float)s[2];
-            const float Y = 0.299f * R + 0.587f * G + 0.114f * B;
-            const float Cb = -0.16875f * R - 0.33126f * G + 0.5f * B;
-            const float Cr = 0.5f * R - 0.41869f * G - 0.08131f * B;
-            if constexpr (std::is_integral<OT>::value) {
-                // integer output rounds to nearest even like ict_kernel's convert_int_sat_rte
-                static_cast<OT *>(P.out[0])[oi] = (OT)__float2int_rn(Y);
-                static_cast<OT *>(P.out[1])[oi] = (OT)__float2int_rn(Cb);
-                static_cast<OT *>(P.out[2])[oi] = (OT)__float2int_rn(Cr);
-            } else {
-                static_cast<OT *>(P.out[0])[oi] = Y;
-                static_cast<OT *>(P.out[1])[oi] = Cb;
-                static_cast<OT *>(P.out[2])[oi] = Cr;
+    for (int y = blockIdx.y; y < h; y += gridDim.y) {
+        const size_t ii = (size_t)y * in_pitch + x0, oi = (size_t)y * out_pitch + x0;
+        IT a[NC][4];
+#pragma unroll
+        for (int c = 0; c < NC; c++) load4<IT>(static_cast<const IT *>(P.in[c]) + ii, vin, n, a[c]);
+        OT o[NC][4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            int s_[NC];
+#pragma unroll
+            for (int c = 0; c < NC; c++) s_[c] = (int)a[c][j] - dc;
+            int c0 = 0;
+            if constexpr (KIND == TC_COLOR_RCT && NC >= 3) {
+                // rct_kernel, preprocess_rct.cl:18-31
+                o[0][j] = (OT)((s_[0] + 2 * s_[1] + s_[2]) >> 2);
+                o[1][j] = (OT)(s_[2] - s_[1]);
+                o[2][j] = (OT)(s_[0] - s_[1]);
+                c0 = 3;
+            } else if constexpr (KIND == TC_COLOR_ICT && NC >= 3) {
+                // ict_kernel, preprocess_ict.cl:20-37 (kept in float, no rounding)
+                const float R = (float)s_[0], G = (float)s_[1], B = (float)s_[2];
+                const float Y = 0.299f * R + 0.587f * G + 0.114f * B;
+                const float Cb = -0.16875f * R - 0.33126f * G + 0.5f * B;
+                const float Cr = 0.5f * R - 0.41869f * G - 0.08131f * B;
+                if constexpr (std::is_integral<OT>::value) {
+                    // integer output rounds to nearest even like ict_kernel's convert_int_sat_rte
+                    o[0][j] = (OT)__float2int_rn(Y);
+                    o[1][j] = (OT)__float2int_rn(Cb);
+                    o[2][j] = (OT)__float2int_rn(Cr);
+                } else {
+                    o[0][j] = Y;
+                    o[1][j] = Cb;
+                    o[2][j] = Cr;
+                }
+                c0 = 3;
             }
-            c0 = 3;
+#pragma unroll
+            for (int c = 0; c < NC; c++)
+                if (c >= c0) o[c][j] = (OT)s_[c];
         }
-        for (int c = c0; c < ncomp; c++) static_cast<OT *>(P.out[c])[oi] = (OT)s[c];
+#pragma unroll
+        for (int c = 0; c < NC; c++) store4<OT>(static_cast<OT *>(P.out[c]) + oi, vout, n, o[c]);
     }
 }
 
-int grid_for(size_t n)
+// Whether every row of every plane starts aligned for 4-sample accesses.
+bool rows_aligned(const void *const *planes, int ncomp, int pitch, size_t elem)
 {
-    const size_t b = (n + 255) / 256;
-    return (int)(b < 148 * 16 ? (b ? b : 1) : 148 * 16);
+    const size_t a = 4 * elem;
+    if (((size_t)pitch * elem) % a) return false;
+    for (int c = 0; c < ncomp; c++)
+        if (reinterpret_cast<uintptr_t>(planes[c]) % a) return false;
+    return true;
+}
+
+template <typename IT, typename OT, int KIND>
+cudaError_t inv_launch(tc_ctx *ctx, int ncomp, const Planes &P, int ip, int op, int w, int h, int bits, bool vi,
+                       bool vo)
+{
+    const dim3 g = color_grid(w, h);
+    switch (ncomp) {
+    case 1: color_inverse_kernel<IT, OT, KIND, 1><<<g, kColThreads, 0, ctx->stream>>>(P, ip, op, w, h, bits, vi, vo); break;
+    case 2: color_inverse_kernel<IT, OT, KIND, 2><<<g, kColThreads, 0, ctx->stream>>>(P, ip, op, w, h, bits, vi, vo); break;
+    case 3: color_inverse_kernel<IT, OT, KIND, 3><<<g, kColThreads, 0, ctx->stream>>>(P, ip, op, w, h, bits, vi, vo); break;
+    default: color_inverse_kernel<IT, OT, KIND, 4><<<g, kColThreads, 0, ctx->stream>>>(P, ip, op, w, h, bits, vi, vo); break;
+    }
+    ctx->launches++;
+    return cudaGetLastError();
 }
 
 template <typename IT, typename OT>
 cudaError_t inv_dispatch(tc_ctx *ctx, int kind, const Planes &P, int ncomp, int ip, int op, int w, int h,
                          int bits)
 {
-    const int g = grid_for((size_t)w * h);
-    if (kind == TC_COLOR_RCT)
-        color_inverse_kernel<IT, OT, TC_COLOR_RCT><<<g, 256, 0, ctx->stream>>>(P, ncomp, ip, op, w, h, bits);
-    else if (kind == TC_COLOR_ICT)
-        color_inverse_kernel<IT, OT, TC_COLOR_ICT><<<g, 256, 0, ctx->stream>>>(P, ncomp, ip, op, w, h, bits);
-    else
-        color_inverse_kernel<IT, OT, TC_COLOR_DC><<<g, 256, 0, ctx->stream>>>(P, ncomp, ip, op, w, h, bits);
+    const bool vi = rows_aligned(P.in, ncomp, ip, sizeof(IT)), vo = rows_aligned(P.out, ncomp, op, sizeof(OT));
+    if (kind == TC_COLOR_RCT) return inv_launch<IT, OT, TC_COLOR_RCT>(ctx, ncomp, P, ip, op, w, h, bits, vi, vo);
+    if (kind == TC_COLOR_ICT) return inv_launch<IT, OT, TC_COLOR_ICT>(ctx, ncomp, P, ip, op, w, h, bits, vi, vo);
+    return inv_launch<IT, OT, TC_COLOR_DC>(ctx, ncomp, P, ip, op, w, h, bits, vi, vo);
+}
+
+template <typename IT, typename OT, int KIND>
+cudaError_t fwd_launch(tc_ctx *ctx, int ncomp, const Planes &P, int ip, int op, int w, int h, int bits, bool vi,
+                       bool vo)
+{
+    const dim3 g = color_grid(w, h);
+    switch (ncomp) {
+    case 1: color_forward_kernel<IT, OT, KIND, 1><<<g, kColThreads, 0, ctx->stream>>>(P, ip, op, w, h, bits, vi, vo); break;
+    case 2: color_forward_kernel<IT, OT, KIND, 2><<<g, kColThreads, 0, ctx->stream>>>(P, ip, op, w, h, bits, vi, vo); break;
+    case 3: color_forward_kernel<IT, OT, KIND, 3><<<g, kColThreads, 0, ctx->stream>>>(P, ip, op, w, h, bits, vi, vo); break;
+    default: color_forward_kernel<IT, OT, KIND, 4><<<g, kColThreads, 0, ctx->stream>>>(P, ip, op, w, h, bits, vi, vo); break;
+    }
     ctx->launches++;
     return cudaGetLastError();
 }
@@ -138,15 +243,10 @@ template <typename IT, typename OT>
 cudaError_t fwd_dispatch(tc_ctx *ctx, int kind, const Planes &P, int ncomp, int ip, int op, int w, int h,
                          int bits)
 {
-    const int g = grid_for((size_t)w * h);
-    if (kind == TC_COLOR_RCT)
-        color_forward_kernel<IT, OT, TC_COLOR_RCT><<<g, 256, 0, ctx->stream>>>(P, ncomp, ip, op, w, h, bits);
-    else if (kind == TC_COLOR_ICT)
-        color_forward_kernel<IT, OT, TC_COLOR_ICT><<<g, 256, 0, ctx->stream>>>(P, ncomp, ip, op, w, h, bits);
-    else
-        color_forward_kernel<IT, OT, TC_COLOR_DC><<<g, 256, 0, ctx->stream>>>(P, ncomp, ip, op, w, h, bits);
-    ctx->launches++;
-    return cudaGetLastError();
+    const bool vi = rows_aligned(P.in, ncomp, ip, sizeof(IT)), vo = rows_aligned(P.out, ncomp, op, sizeof(OT));
+    if (kind == TC_COLOR_RCT) return fwd_launch<IT, OT, TC_COLOR_RCT>(ctx, ncomp, P, ip, op, w, h, bits, vi, vo);
+    if (kind == TC_COLOR_ICT) return fwd_launch<IT, OT, TC_COLOR_ICT>(ctx, ncomp, P, ip, op, w, h, bits, vi, vo);
+    return fwd_launch<IT, OT, TC_COLOR_DC>(ctx, ncomp, P, ip, op, w, h, bits, vi, vo);
 }
 
 }  // namespace

@@ -617,17 +617,21 @@ __global__ void dequant_raw_kernel(const tc_cblk_desc *__restrict__ desc, int n,
         u = p_last < 0 ? 0 : p_last;
     }
     const bool irrev = (d.flags & TC_CBLK_IRREVERSIBLE) != 0;
-    for (int i = threadIdx.x; i < d.w * d.h; i += blockDim.x) {
-        const int y = i / d.w, x = i - y * d.w;
+    const float fr = recon_r * (float)(1u << u);
+    const int32_t ir = u ? (int32_t)floorf(fr) : 0;
+    // 64 columns x 4 rows per pass of the CTA: whole rows, no index division
+    const int x = threadIdx.x & 63;
+    if (x >= d.w) return;
+    for (int y = threadIdx.x >> 6; y < d.h; y += blockDim.x >> 6) {
         const uint64_t o = d.out_off + (uint64_t)y * d.out_pitch + x;
         const uint32_t r = raw[o];
         const uint32_t mg = (r & 0x7FFFFFFFu) >> (31 - d.mb);
         const bool neg = (r >> 31) != 0;
         if (irrev) {
-            float v = mg ? ((float)mg + recon_r * (float)(1u << u)) * d.step : 0.0f;
+            float v = mg ? ((float)mg + fr) * d.step : 0.0f;
             reinterpret_cast<float *>(out)[o] = neg ? -v : v;
         } else {
-            int32_t v = mg ? (int32_t)mg + (u ? (int32_t)floorf(recon_r * (float)(1u << u)) : 0) : 0;
+            int32_t v = mg ? (int32_t)mg + ir : 0;
             reinterpret_cast<int32_t *>(out)[o] = neg ? -v : v;
         }
     }
