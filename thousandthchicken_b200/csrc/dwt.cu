@@ -3,19 +3,25 @@
 // levels are in dwt_rev.cu).
 //
 // Replaces the reference's forward kernels (dwt_f53.cl, dwt_f97.cl over
-// dwt_transform_buffer.cl / dwt_io.cl):
-//   * one launch per level; each CTA owns a TX x TY output tile and stages
-//     the tile plus a halo of H samples (2 for 5/3, 4 for 9/7) in shared
-//     memory with whole-sample symmetric extension (full periodic
-//     reflection, ISO F.3.7, instead of the single reflection of
-//     dwt_io.cl:7-38, defect D14);
-//   * rows are stored split into even/odd halves so every lifting step is a
-//     unit-stride, bank-conflict-free sweep; the store deinterleaves the
-//     tile straight into the Mallat subbands;
-//   * 5/3 uses floor (ISO) or truncating (reference, defect D13) rounding;
-//     9/7 uses fp32 with the scaling factors applied as floats (defects
-//     D10-D12 fixed).
+// dwt_transform_buffer.cl / dwt_io.cl).  One 256-thread CTA transforms a tile
+// of 120 output columns by 56 (9/7) or 60 (5/3) output rows of one level:
+//   * it stages the extended tile (halo of H = 4 or 2 samples on every side)
+//     in shared memory with 4-byte asynchronous copies, whole-sample
+//     symmetric extension at the image edges (ISO F.3.7; the reference's
+//     single reflection, dwt_io.cl:7-38, is defect D14);
+//   * vertical lifting first (ISO 2D_SD: columns, then rows): two threads
+//     per column each lift an overlapping half of it in registers;
+//   * horizontal lifting: one thread per 30-output row segment, in
+//     registers, whose low- and high-pass results go back to shared memory
+//     de-interleaved;
+//   * the store writes each row's low and high halves to the level's LL and
+//     HL (even rows) or LH and HH (odd rows) bands, coalesced.
+// 5/3 uses floor (ISO) or truncating (reference, defect D13) rounding; 9/7
+// uses fp32 with the scaling factors applied as floats (defects D10-D12
+// fixed).  The lifting steps and their order follow ISO F.4.8.
 #include <cuda_runtime.h>
+
+#include <type_traits>
 
 #include "dwt_common.cuh"
 #include "tc_internal.cuh"
@@ -25,183 +31,168 @@ namespace {
 
 using namespace dwt;
 
-// A tile buffer of NR rows x NC columns, each row split into an even half
-// [0, NC/2) and an odd half [NC/2, NC).
-template <typename T, int NR, int NC>
-struct Tile {
-    static constexpr int NE = NC / 2;
-    T d[NR * NC];
-    __device__ __forceinline__ T &at(int r, int e) { return d[r * NC + ((e & 1) ? NE + (e >> 1) : (e >> 1))]; }
-    __device__ __forceinline__ T &ev(int r, int i) { return d[r * NC + i]; }
-    __device__ __forceinline__ T &od(int r, int i) { return d[r * NC + NE + i]; }
-};
-
-// ---- horizontal lifting over all rows; vertical over central columns -----
-
-// Forward lifting: vertical over all columns first, then horizontal over
-// central rows (ISO F.4.2 order).
-template <typename T, int NR, int NC, int RND>
-__device__ void lift_v_fwd53(Tile<T, NR, NC> &t)
-{
-    for (int q = threadIdx.x; q < (NR / 2 - 1) * NC; q += blockDim.x) {
-        const int i = q / NC, e = q % NC;
-        t.at(2 * i + 1, e) -= div2r<RND>(t.at(2 * i, e) + t.at(2 * i + 2, e));
-    }
-    __syncthreads();
-    for (int q = threadIdx.x; q < (NR / 2 - 2) * NC; q += blockDim.x) {
-        const int i = 1 + q / NC, e = q % NC;
-        t.at(2 * i, e) += div4r<RND>(t.at(2 * i - 1, e) + t.at(2 * i + 1, e) + 2);
-    }
-    __syncthreads();
-}
-
-template <typename T, int NR, int NC, int RND>
-__device__ void lift_h_fwd53(Tile<T, NR, NC> &t, int r0, int r1)
-{
-    constexpr int NE = NC / 2;
-    const int nr = r1 - r0;
-    for (int q = threadIdx.x; q < nr * (NE - 1); q += blockDim.x) {
-        const int r = r0 + q / (NE - 1), i = q % (NE - 1);
-        t.od(r, i) -= div2r<RND>(t.ev(r, i) + t.ev(r, i + 1));
-    }
-    __syncthreads();
-    for (int q = threadIdx.x; q < nr * (NE - 2); q += blockDim.x) {
-        const int r = r0 + q / (NE - 2), i = 1 + q % (NE - 2);
-        t.ev(r, i) += div4r<RND>(t.od(r, i - 1) + t.od(r, i) + 2);
-    }
-    __syncthreads();
-}
-
-template <int NR, int NC>
-__device__ void lift_v_fwd97(Tile<float, NR, NC> &t)
-{
-    for (int q = threadIdx.x; q < (NR / 2 - 1) * NC; q += blockDim.x) {
-        const int i = q / NC, e = q % NC;
-        t.at(2 * i + 1, e) = fmaf(kA, t.at(2 * i, e) + t.at(2 * i + 2, e), t.at(2 * i + 1, e));
-    }
-    __syncthreads();
-    for (int q = threadIdx.x; q < (NR / 2 - 2) * NC; q += blockDim.x) {
-        const int i = 1 + q / NC, e = q % NC;
-        t.at(2 * i, e) = fmaf(kB, t.at(2 * i - 1, e) + t.at(2 * i + 1, e), t.at(2 * i, e));
-    }
-    __syncthreads();
-    for (int q = threadIdx.x; q < (NR / 2 - 2) * NC; q += blockDim.x) {
-        const int i = 1 + q / NC, e = q % NC;
-        t.at(2 * i + 1, e) = fmaf(kG, t.at(2 * i, e) + t.at(2 * i + 2, e), t.at(2 * i + 1, e));
-    }
-    __syncthreads();
-    for (int q = threadIdx.x; q < (NR / 2 - 3) * NC; q += blockDim.x) {
-        const int i = 2 + q / NC, e = q % NC;
-        t.at(2 * i, e) = fmaf(kD, t.at(2 * i - 1, e) + t.at(2 * i + 1, e), t.at(2 * i, e));
-    }
-    __syncthreads();
-    for (int q = threadIdx.x; q < (NR / 2) * NC; q += blockDim.x) {
-        const int i = q / NC, e = q % NC;
-        t.at(2 * i + 1, e) *= kK;
-        t.at(2 * i, e) *= kInvK;
-    }
-    __syncthreads();
-}
-
-template <int NR, int NC>
-__device__ void lift_h_fwd97(Tile<float, NR, NC> &t, int r0, int r1)
-{
-    constexpr int NE = NC / 2;
-    const int nr = r1 - r0;
-    for (int q = threadIdx.x; q < nr * (NE - 1); q += blockDim.x) {
-        const int r = r0 + q / (NE - 1), i = q % (NE - 1);
-        t.od(r, i) = fmaf(kA, t.ev(r, i) + t.ev(r, i + 1), t.od(r, i));
-    }
-    __syncthreads();
-    for (int q = threadIdx.x; q < nr * (NE - 2); q += blockDim.x) {
-        const int r = r0 + q / (NE - 2), i = 1 + q % (NE - 2);
-        t.ev(r, i) = fmaf(kB, t.od(r, i - 1) + t.od(r, i), t.ev(r, i));
-    }
-    __syncthreads();
-    for (int q = threadIdx.x; q < nr * (NE - 2); q += blockDim.x) {
-        const int r = r0 + q / (NE - 2), i = 1 + q % (NE - 2);
-        t.od(r, i) = fmaf(kG, t.ev(r, i) + t.ev(r, i + 1), t.od(r, i));
-    }
-    __syncthreads();
-    for (int q = threadIdx.x; q < nr * (NE - 3); q += blockDim.x) {
-        const int r = r0 + q / (NE - 3), i = 2 + q % (NE - 3);
-        t.ev(r, i) = fmaf(kD, t.od(r, i - 1) + t.od(r, i), t.ev(r, i));
-    }
-    __syncthreads();
-    for (int q = threadIdx.x; q < nr * NE; q += blockDim.x) {
-        const int r = r0 + q / NE, i = q % NE;
-        t.od(r, i) *= kK;
-        t.ev(r, i) *= kInvK;
-    }
-    __syncthreads();
-}
-
-// ---- loads ---------------------------------------------------------------
-
-template <typename T, int NR, int NC, int H>
-__device__ void load_fwd(Tile<T, NR, NC> &t, const T *in, int ip, int x0, int y0, int w, int h)
-{
-    constexpr int NE = NC / 2;
-    for (int q = threadIdx.x; q < NR * NC; q += blockDim.x) {
-        const int r = q / NC, rem = q % NC, par = rem / NE, i = rem % NE;
-        const int e = 2 * i + par;
-        const int my = mirror(y0 - H + r, h), mx = mirror(x0 - H + e, w);
-        t.d[r * NC + (par ? NE : 0) + i] = in[(size_t)my * ip + mx];
-    }
-    __syncthreads();
-}
-
-// ---- kernels --------------------------------------------------------------
+constexpr int kThreads = 256;
 
 template <int WAVELET>
-struct Geo {
-    static constexpr int H = WAVELET ? 4 : 2;
+struct FwdGeo {
+    static constexpr int H = WAVELET ? 4 : 2;     // halo
+    static constexpr int NR = 64;                 // extended rows per tile
+    static constexpr int TY = NR - 2 * H;         // output rows per tile
+    static constexpr int TX = 120;                // output columns per tile (even)
+    static constexpr int NC = TX + 2 * H;         // extended columns
+    static constexpr int S = (NC % 8 == 4) ? NC : NC + 4;  // row stride, S/4 odd
+    static constexpr int SEG = 30;                // outputs per row segment (even)
+    static constexpr int SEGN = SEG + 2 * H;      // inputs per row segment
+    static constexpr int VN = 32 + H;             // rows lifted by one thread of a column pair
+    static constexpr int OUTV = 32 - H;           // rows it keeps
 };
 
-// Forward level, one component per blockIdx.z.
-template <typename T, int WAVELET, int RND, int TX, int TY>
-__global__ void __launch_bounds__(256) fdwt_level_kernel(LevelIO io)
+// In-place 1-D forward lifting of a signal held in registers (v[0] at an
+// even position).  Only samples at least H away from both ends are exact.
+template <typename T, int WAVELET, int RND, int N>
+__device__ __forceinline__ void lift_forward(T (&v)[N])
 {
-    constexpr int H = Geo<WAVELET>::H, NR = TY + 2 * H, NC = TX + 2 * H;
-    __shared__ Tile<T, NR, NC> t;
-    const int c = blockIdx.z;
-    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
-    const int w = io.w, h = io.h;
-    load_fwd<T, NR, NC, H>(t, static_cast<const T *>(io.ll[c]), io.ll_pitch, x0, y0, w, h);
     if constexpr (WAVELET == 0) {
-        if (h > 1) lift_v_fwd53<T, NR, NC, RND>(t);
-        if (w > 1) lift_h_fwd53<T, NR, NC, RND>(t, H, H + TY);
+#pragma unroll
+        for (int k = 1; k <= N - 2; k += 2) v[k] -= div2r<RND>(v[k - 1] + v[k + 1]);
+#pragma unroll
+        for (int k = 2; k <= N - 2; k += 2) v[k] += div4r<RND>(v[k - 1] + v[k + 1] + 2);
     } else {
-        if (h > 1) lift_v_fwd97<NR, NC>(t);
-        if (w > 1) lift_h_fwd97<NR, NC>(t, H, H + TY);
-    }
-    const int wl = (w + 1) >> 1, hl = (h + 1) >> 1;
-    T *ll = static_cast<T *>(io.out[c]);
-    T *bands = static_cast<T *>(io.bands[c]);
-    constexpr int NE = TX / 2;
-    // group stores so a warp writes consecutive elements of one band row
-    for (int q = threadIdx.x; q < TX * TY; q += blockDim.x) {
-        const int r = q / TX, rem = q % TX, par = rem / NE, i = rem % NE;
-        const int e = 2 * i + par;
-        const int y = y0 + r, x = x0 + e;
-        if (y >= h || x >= w) continue;
-        const T v = t.at(r + H, e + H);
-        const int yb = y >> 1, xb = x >> 1;
-        if (!(y & 1)) {
-            if (!(x & 1)) ll[(size_t)yb * io.out_pitch + xb] = v;
-            else bands[(size_t)yb * io.bands_pitch + wl + xb] = v;
-        } else {
-            if (!(x & 1)) bands[(size_t)(hl + yb) * io.bands_pitch + xb] = v;
-            else bands[(size_t)(hl + yb) * io.bands_pitch + wl + xb] = v;
+#pragma unroll
+        for (int k = 1; k <= N - 2; k += 2) v[k] = fmaf(kA, v[k - 1] + v[k + 1], v[k]);
+#pragma unroll
+        for (int k = 2; k <= N - 2; k += 2) v[k] = fmaf(kB, v[k - 1] + v[k + 1], v[k]);
+#pragma unroll
+        for (int k = 1; k <= N - 2; k += 2) v[k] = fmaf(kG, v[k - 1] + v[k + 1], v[k]);
+#pragma unroll
+        for (int k = 2; k <= N - 2; k += 2) v[k] = fmaf(kD, v[k - 1] + v[k + 1], v[k]);
+#pragma unroll
+        for (int k = 0; k + 1 < N; k += 2) {
+            v[k] *= kInvK;
+            v[k + 1] *= kK;
         }
     }
 }
 
-template <typename T, int WAVELET, int RND, int TX, int TY>
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Forward level, one component per blockIdx.z: io.ll[c] is the spatial input
+// (pitch ll_pitch), io.out[c] receives LL (out_pitch), io.bands[c] the Mallat
+// plane holding HL/LH/HH (bands_pitch).
+template <typename T, int WAVELET, int RND>
+__global__ void __launch_bounds__(kThreads) fdwt_level_kernel(LevelIO io)
+{
+    using G = FwdGeo<WAVELET>;
+    constexpr int H = G::H, NR = G::NR, TY = G::TY, TX = G::TX, NC = G::NC, S = G::S;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *t = reinterpret_cast<T *>(smem_raw);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int c = blockIdx.z;
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+    const int w = io.w, h = io.h;
+    const T *in = static_cast<const T *>(io.ll[c]);
+
+    // 1. stage the extended tile
+    const bool interior = x0 >= H && x0 - H + NC <= w && y0 >= H && y0 - H + NR <= h;
+    for (int r = warp; r < NR; r += kThreads / 32) {
+        const int y = interior ? y0 - H + r : mirror(y0 - H + r, h);
+        const T *row = in + (size_t)y * io.ll_pitch;
+        for (int e = lane; e < NC; e += 32) {
+            const int x = interior ? x0 - H + e : mirror(x0 - H + e, w);
+            cp_async4(t + r * S + e, row + x);
+        }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+
+    // 2. vertical lifting: column pairs of threads, rows [0, VN) and
+    //    [NR - VN, NR); the results go back in place once all have read
+    {
+        const int col = tid % 128, half = tid / 128;
+        const int vbase = half ? NR - G::VN : 0;
+        T v[G::VN];
+        if (col < NC) {
+#pragma unroll
+            for (int k = 0; k < G::VN; k++) v[k] = t[(vbase + k) * S + col];
+        }
+        __syncthreads();
+        if (col < NC) {
+            if (h > 1) lift_forward<T, WAVELET, RND, G::VN>(v);
+#pragma unroll
+            for (int k = 0; k < G::OUTV; k++) t[(vbase + H + k) * S + col] = v[H + k];
+        }
+        __syncthreads();
+    }
+
+    // 3. horizontal lifting of the TY output rows, one 30-output segment per
+    //    thread; low outputs go to row words [0, TX/2), high to [64, 64 + TX/2)
+    {
+        constexpr int NSEG = TX / G::SEG;
+        const bool active = tid < TY * NSEG;
+        const int seg = tid / TY, r = H + tid % TY;  // a warp walks consecutive rows
+        T v[G::SEGN];
+        if (active) {
+#pragma unroll
+            for (int k = 0; k < G::SEGN; k++) v[k] = t[r * S + seg * G::SEG + k];
+        }
+        __syncthreads();  // segments overlap, and the outputs overwrite the inputs
+        if (active) {
+            if (w > 1) lift_forward<T, WAVELET, RND, G::SEGN>(v);
+#pragma unroll
+            for (int i = 0; i < G::SEG / 2; i++) {
+                t[r * S + seg * (G::SEG / 2) + i] = v[H + 2 * i];
+                t[r * S + 64 + seg * (G::SEG / 2) + i] = v[H + 2 * i + 1];
+            }
+        }
+        __syncthreads();
+    }
+
+    // 4. store: row by row, the low half to LL / LH, the high half to HL / HH;
+    //    a thread keeps one of the 120 output slots of a row (60 low, 60 high)
+    //    and walks every other row
+    const int wl = (w + 1) >> 1, hl = (h + 1) >> 1;
+    constexpr int HALF = TX / 2;
+    const int j = tid % 128, r0 = tid / 128;
+    if (j < TX) {
+        const bool hi = j >= HALF;
+        const int i = hi ? j - HALF : j;
+        const int x = x0 + 2 * i + (hi ? 1 : 0);
+        if (x < w) {
+            const int xb = (x0 >> 1) + i;
+            T *ll = static_cast<T *>(io.out[c]) + xb;
+            T *bands = static_cast<T *>(io.bands[c]) + xb + (hi ? wl : 0);
+            const T *src = t + (hi ? 64 : 0) + i;
+            for (int r = r0; r < TY && y0 + r < h; r += 2) {
+                const int y = y0 + r, yb = y >> 1;
+                const T val = src[(H + r) * S];
+                if (y & 1) bands[(size_t)(hl + yb) * io.bands_pitch] = val;
+                else if (hi) bands[(size_t)yb * io.bands_pitch] = val;
+                else ll[(size_t)yb * io.out_pitch] = val;
+            }
+        }
+    }
+}
+
+template <typename T, int WAVELET, int RND>
 cudaError_t run_fdwt(tc_ctx *ctx, const LevelIO &io)
 {
-    dim3 grid((io.w + TX - 1) / TX, (io.h + TY - 1) / TY, io.ncomp);
-    fdwt_level_kernel<T, WAVELET, RND, TX, TY><<<grid, 256, 0, ctx->stream>>>(io);
+    using G = FwdGeo<WAVELET>;
+    constexpr size_t smem = (size_t)G::NR * G::S * sizeof(T);
+    static bool attr[64] = {};
+    if (!attr[ctx->device & 63]) {
+        cudaError_t e = cudaFuncSetAttribute(fdwt_level_kernel<T, WAVELET, RND>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr[ctx->device & 63] = true;
+    }
+    dim3 grid((io.w + G::TX - 1) / G::TX, (io.h + G::TY - 1) / G::TY, io.ncomp);
+    fdwt_level_kernel<T, WAVELET, RND><<<grid, kThreads, smem, ctx->stream>>>(io);
     ctx->launches++;
     return cudaGetLastError();
 }
@@ -211,9 +202,9 @@ cudaError_t run_fdwt(tc_ctx *ctx, const LevelIO &io)
 cudaError_t launch_fdwt_level(tc_ctx *ctx, const LevelIO &io, int wavelet, int rounding)
 {
     if (io.w <= 0 || io.h <= 0) return cudaSuccess;
-    if (wavelet) return run_fdwt<float, 1, 0, 128, 64>(ctx, io);
-    if (rounding == TC_ROUND_TRUNC) return run_fdwt<int32_t, 0, TC_ROUND_TRUNC, 128, 64>(ctx, io);
-    return run_fdwt<int32_t, 0, TC_ROUND_FLOOR, 128, 64>(ctx, io);
+    if (wavelet) return run_fdwt<float, 1, 0>(ctx, io);
+    if (rounding == TC_ROUND_TRUNC) return run_fdwt<int32_t, 0, TC_ROUND_TRUNC>(ctx, io);
+    return run_fdwt<int32_t, 0, TC_ROUND_FLOOR>(ctx, io);
 }
 
 }  // namespace tc

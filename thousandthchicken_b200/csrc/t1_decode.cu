@@ -600,7 +600,7 @@ t1_decode_kernel(const tc_cblk_desc *__restrict__ desc, const uint32_t *__restri
 // Standalone inverse quantiser over raw sign-magnitude words.
 __global__ void dequant_raw_kernel(const tc_cblk_desc *__restrict__ desc, int n,
                                    const uint32_t *__restrict__ raw, char *__restrict__ out,
-                                   float recon_r, uint32_t *words)
+                                   float recon_r, uint32_t *words, bool base16)
 {
     const int b = blockIdx.x;
     if (b >= n) return;
@@ -619,20 +619,30 @@ __global__ void dequant_raw_kernel(const tc_cblk_desc *__restrict__ desc, int n,
     const bool irrev = (d.flags & TC_CBLK_IRREVERSIBLE) != 0;
     const float fr = recon_r * (float)(1u << u);
     const int32_t ir = u ? (int32_t)floorf(fr) : 0;
-    // 64 columns x 4 rows per pass of the CTA: whole rows, no index division
-    const int x = threadIdx.x & 63;
-    if (x >= d.w) return;
-    for (int y = threadIdx.x >> 6; y < d.h; y += blockDim.x >> 6) {
-        const uint64_t o = d.out_off + (uint64_t)y * d.out_pitch + x;
-        const uint32_t r = raw[o];
+    // 16 threads per row, four consecutive coefficients each (one 16-byte
+    // load and store when the block's rows are aligned): whole rows, no
+    // index division
+    auto one = [&](uint32_t r) -> uint32_t {
         const uint32_t mg = (r & 0x7FFFFFFFu) >> (31 - d.mb);
         const bool neg = (r >> 31) != 0;
         if (irrev) {
-            float v = mg ? ((float)mg + fr) * d.step : 0.0f;
-            reinterpret_cast<float *>(out)[o] = neg ? -v : v;
+            const float v = mg ? ((float)mg + fr) * d.step : 0.0f;
+            return __float_as_uint(neg ? -v : v);
+        }
+        const int32_t v = mg ? (int32_t)mg + ir : 0;
+        return (uint32_t)(neg ? -v : v);
+    };
+    const int x = 4 * (threadIdx.x & 15);
+    if (x >= d.w) return;
+    const bool vec = base16 && ((d.out_off | (uint64_t)d.out_pitch) & 3u) == 0 && x + 4 <= d.w;
+    uint32_t *dst = reinterpret_cast<uint32_t *>(out);
+    for (int y = threadIdx.x >> 4; y < d.h; y += blockDim.x >> 4) {
+        const uint64_t o = d.out_off + (uint64_t)y * d.out_pitch + x;
+        if (vec) {
+            const uint4 r = *reinterpret_cast<const uint4 *>(raw + o);
+            *reinterpret_cast<uint4 *>(dst + o) = make_uint4(one(r.x), one(r.y), one(r.z), one(r.w));
         } else {
-            int32_t v = mg ? (int32_t)mg + ir : 0;
-            reinterpret_cast<int32_t *>(out)[o] = neg ? -v : v;
+            for (int j = 0; j < 4 && x + j < d.w; j++) dst[o + j] = one(raw[o + j]);
         }
     }
 }
@@ -787,8 +797,9 @@ cudaError_t launch_dequant_raw(tc_ctx *ctx, const tc_cblk_desc *d_desc, int n, c
                                void *d_out, float recon_r)
 {
     if (n <= 0) return cudaSuccess;
+    const bool base16 = ((reinterpret_cast<uintptr_t>(d_raw) | reinterpret_cast<uintptr_t>(d_out)) & 15) == 0;
     dequant_raw_kernel<<<n, 256, 0, ctx->stream>>>(d_desc, n, d_raw, static_cast<char *>(d_out), recon_r,
-                                                   ctx->d_words);
+                                                   ctx->d_words, base16);
     ctx->launches++;
     return cudaGetLastError();
 }
