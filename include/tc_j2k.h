@@ -250,7 +250,11 @@ void tc_j2k_parsed_free(tc_j2k_parsed *p);
  * components, TC_U8 samples when bits <= 8 else TC_U16, component c at
  * h_out + c*width*height*bytes.  Runs Tier-1 with fused dequantisation, the
  * reverse DWT and the fused inverse colour transform / DC shift on the GPU.
- * Replaces Decoder::decode (Decoder.cpp:94-217). */
+ * Replaces Decoder::decode (Decoder.cpp:94-217).  Every entry point that
+ * takes a codestream (here, tc_decode_j2k_file, tc_j2k_parse,
+ * tc_j2k_read_header, tc_plan_create/rebuild) also takes a JP2 file and
+ * decodes its first codestream box, as Decoder::decode does for .jp2 files
+ * through jp2_parse_boxes (boxes.c:265-307). */
 int tc_decode_j2k(tc_ctx *ctx, const uint8_t *h_cs, size_t len,
                   void *h_out, size_t out_bytes, tc_image_info *info);
 

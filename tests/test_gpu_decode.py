@@ -194,3 +194,23 @@ def test_graph_replay_and_autotune(gpu_ctx):
     assert g in (8, 16, 32)
     L.lib().tc_ctx_set_t1_group(gpu_ctx.handle, 32)
     plan.close()
+
+
+def test_jp2_files_decode(gpu_ctx, tmp_path):
+    """JP2 files (the reference's Decoder::decode parses their boxes): one
+    written by OpenJPEG through Pillow, losslessly, and the harness's own
+    codestream in a JP2 container, from memory and from a .jp2 file."""
+    import io
+    from PIL import Image
+    from test_host_codec import _jp2
+    img = synth_image(301, 199, 3, 8, seed=9)
+    buf = io.BytesIO()
+    Image.fromarray(np.moveaxis(img, 0, -1)).save(buf, format="JPEG2000")
+    np.testing.assert_array_equal(_decoder(gpu_ctx).decode(buf.getvalue()), img)
+    cs = codec.encode(img, 8, levels=4, reversible=False, base_step=1 / 128)
+    jp2 = _jp2(cs, 301, 199, 3, 8)
+    p = tmp_path / "x.jp2"
+    p.write_bytes(jp2)
+    want = _decoder(gpu_ctx).decode(cs)
+    np.testing.assert_array_equal(_decoder(gpu_ctx).decode(jp2), want)
+    np.testing.assert_array_equal(_decoder(gpu_ctx).decode(p), want)

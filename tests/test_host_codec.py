@@ -109,3 +109,70 @@ def test_sort_order_longest_first():
     d["passes"] = [1, 7, 3, 7, 0]
     d["seg_len"] = [10, 5, 3, 50, 0]
     assert codec.sort_order(d).tolist() == [3, 1, 2, 0, 4]
+
+
+# ---- JP2 file format (Decoder::decode reads .jp2 through jp2_parse_boxes) ----
+
+def _box(t: bytes, body: bytes, form: str = "short") -> bytes:
+    import struct
+    if form == "xl":  # LBox = 1, 8-byte length follows
+        return struct.pack(">I4sQ", 1, t, 16 + len(body)) + body
+    if form == "eof":  # LBox = 0, the box runs to the end of the file
+        return struct.pack(">I4s", 0, t) + body
+    return struct.pack(">I4s", 8 + len(body), t) + body
+
+
+def _jp2(cs: bytes, w: int, h: int, nc: int, bits: int, form: str = "short", ihdr_w: int | None = None) -> bytes:
+    import struct
+    sig = _box(b"jP  ", bytes.fromhex("0d0a870a"))
+    ftyp = _box(b"ftyp", b"jp2 " + struct.pack(">I", 0) + b"jp2 ")
+    ihdr = _box(b"ihdr", struct.pack(">IIHBBBB", h, ihdr_w if ihdr_w is not None else w, nc, bits - 1, 7, 0, 0))
+    colr = _box(b"colr", struct.pack(">BBBI", 1, 0, 0, 16 if nc >= 3 else 17))
+    return sig + ftyp + _box(b"jp2h", ihdr + colr) + _box(b"xml ", b"<x/>") + _box(b"jp2c", cs, form)
+
+
+@pytest.mark.parametrize("form", ["short", "xl", "eof"])
+def test_jp2_file_parses_like_its_codestream(form):
+    img = synth_image(90, 70, 3, 8, seed=3)
+    cs = codec.encode(img, 8, levels=3)
+    jp2 = _jp2(cs, 90, 70, 3, 8, form)
+    off = len(jp2) - len(cs)
+    info_a, desc_a, pool_a = codec.parse(cs)
+    info_b, desc_b, pool_b = codec.parse(jp2)
+    assert info_a == info_b
+    assert codec.read_header(jp2) == codec.read_header(cs)
+    np.testing.assert_array_equal(desc_b["seg_off"], desc_a["seg_off"] + off)
+    for name in desc_a.dtype.names:
+        if name != "seg_off":
+            np.testing.assert_array_equal(desc_a[name], desc_b[name])
+    for da, db in zip(desc_a, desc_b):
+        a, b = int(da["seg_off"]), int(db["seg_off"])
+        assert bytes(pool_a[a:a + da["seg_len"]]) == bytes(pool_b[b:b + db["seg_len"]])
+
+
+def test_jp2_written_by_openjpeg_parses():
+    import io
+    from PIL import Image
+    img = synth_image(52, 40, 3, 8, seed=4)
+    buf = io.BytesIO()
+    Image.fromarray(np.moveaxis(img, 0, -1)).save(buf, format="JPEG2000")
+    data = buf.getvalue()
+    assert data[4:8] == b"jP  "
+    info = codec.read_header(data)
+    assert (info["width"], info["height"], info["ncomp"]) == (52, 40, 3)
+    _, desc, _ = codec.parse(data)
+    assert len(desc) > 0
+
+
+@pytest.mark.parametrize("case", ["no_jp2c", "truncated", "ihdr_mismatch", "no_ftyp", "garbage"])
+def test_bad_jp2_files_are_rejected(case):
+    img = synth_image(40, 30, 1, 8, seed=5)
+    cs = codec.encode(img, 8, levels=2, mct=False)
+    good = _jp2(cs, 40, 30, 1, 8)
+    data = {"no_jp2c": good[: len(good) - len(cs) - 8],
+            "truncated": good[: len(good) - len(cs) // 2 - 4] + b"\x00" * 3,
+            "ihdr_mismatch": _jp2(cs, 40, 30, 1, 8, ihdr_w=41),
+            "no_ftyp": good.replace(b"ftyp", b"ftyq", 1),
+            "garbage": b"\x00\x01\x02\x03" * 8}[case]
+    with pytest.raises(TCError):
+        codec.parse(data)

@@ -850,7 +850,7 @@ static void fill_info(const Params &P, tc_image_info &info)
     info.quant_style = P.qstyle;
 }
 
-int read_header(const uint8_t *cs, size_t len, tc_image_info &info, std::string &err)
+static int read_raw_header(const uint8_t *cs, size_t len, tc_image_info &info, std::string &err)
 {
     Reader rd{cs, len};
     Params P;
@@ -899,7 +899,7 @@ struct CblkState {
 };
 }  // namespace
 
-int parse_codestream(const uint8_t *cs, size_t len, Parsed &out, std::string &err)
+static int parse_raw_codestream(const uint8_t *cs, size_t len, Parsed &out, std::string &err)
 {
     Reader rd{cs, len};
     Params P;
@@ -1369,6 +1369,146 @@ int encode_codestream(const tc_encode_params &p, const void *planes, std::vector
     wr.u16(M_SOD);
     out.insert(out.end(), body.begin(), body.end());
     wr.u16(M_EOC);
+    return TC_OK;
+}
+
+}  // namespace tc
+
+namespace tc {
+
+// ---- JP2 file format (ISO 15444-1 Annex I; the reference's
+//      jp2_parse_boxes, boxes.c:265-307, reached from Decoder::decode for
+//      .jp2 files, Decoder.cpp:121-125) ------------------------------------
+//
+// A JP2 file is a sequence of boxes: a 4-byte big-endian length LBox (1: an
+// 8-byte length XLBox follows; 0: the box runs to the end of the file), a
+// 4-byte type, then the content.  The decoder needs the signature box, the
+// file type box (brand or compatibility list "jp2 "), the header superbox
+// with its image header box, and the first contiguous codestream box, whose
+// content is the codestream.
+
+namespace {
+
+constexpr uint32_t kBoxSig = 0x6A502020u, kBoxFtyp = 0x66747970u, kBoxJp2h = 0x6A703268u,
+                   kBoxIhdr = 0x69686472u, kBoxJp2c = 0x6A703263u, kSigContent = 0x0D0A870Au,
+                   kBrandJp2 = 0x6A703220u;
+
+uint32_t be32(const uint8_t *p) { return (uint32_t)p[0] << 24 | (uint32_t)p[1] << 16 | (uint32_t)p[2] << 8 | p[3]; }
+
+struct Box {
+    uint32_t type = 0;
+    size_t body = 0, end = 0;  // content [body, end) of the buffer
+};
+
+// The box starting at `pos` of d[0..len); false when it does not fit.
+bool next_box(const uint8_t *d, size_t len, size_t pos, Box &b)
+{
+    if (len < 8 || pos > len - 8) return false;
+    uint64_t lbox = be32(d + pos);
+    b.type = be32(d + pos + 4);
+    size_t hdr = 8;
+    if (lbox == 1) {
+        if (pos > len - 16) return false;
+        lbox = (uint64_t)be32(d + pos + 8) << 32 | be32(d + pos + 12);
+        hdr = 16;
+    } else if (lbox == 0) {
+        lbox = len - pos;
+    }
+    if (lbox < hdr || lbox > len - pos) return false;
+    b.body = pos + hdr;
+    b.end = pos + (size_t)lbox;
+    return true;
+}
+
+struct Jp2Header {
+    bool have = false;
+    uint32_t width = 0, height = 0, ncomp = 0;
+};
+
+// Locates the codestream of a JP2 file; a buffer that starts with the SOC
+// marker is a codestream already (offset 0).
+int locate_codestream(const uint8_t *d, size_t len, size_t &off, size_t &n, Jp2Header &ih, std::string &err)
+{
+    off = 0;
+    n = len;
+    if (len >= 2 && d[0] == 0xFF && d[1] == 0x4F) return TC_OK;
+    Box b;
+    if (!next_box(d, len, 0, b) || b.type != kBoxSig || b.end - b.body != 4 || be32(d + b.body) != kSigContent) {
+        err = "neither a JPEG 2000 codestream (SOC) nor a JP2 file (signature box)";
+        return TC_E_CODESTREAM;
+    }
+    bool ftyp_ok = false;
+    for (size_t pos = b.end; pos < len;) {
+        if (!next_box(d, len, pos, b)) {
+            err = "truncated JP2 box";
+            return TC_E_CODESTREAM;
+        }
+        if (b.type == kBoxFtyp) {
+            for (size_t q = b.body; q + 4 <= b.end; q += 4)
+                if ((q == b.body || q >= b.body + 8) && be32(d + q) == kBrandJp2) ftyp_ok = true;
+        } else if (b.type == kBoxJp2h) {
+            Box c;
+            for (size_t q = b.body; q < b.end; q = c.end) {
+                if (!next_box(d, b.end, q, c)) {
+                    err = "truncated box in the JP2 header";
+                    return TC_E_CODESTREAM;
+                }
+                if (c.type == kBoxIhdr && c.end - c.body >= 14) {
+                    ih.have = true;
+                    ih.height = be32(d + c.body);
+                    ih.width = be32(d + c.body + 4);
+                    ih.ncomp = (uint32_t)d[c.body + 8] << 8 | d[c.body + 9];
+                }
+            }
+        } else if (b.type == kBoxJp2c) {
+            if (!ftyp_ok) {
+                err = "JP2 file without a jp2 file type box before its codestream";
+                return TC_E_CODESTREAM;
+            }
+            off = b.body;
+            n = b.end - b.body;
+            return TC_OK;
+        }
+        pos = b.end;
+    }
+    err = "JP2 file without a codestream box";
+    return TC_E_CODESTREAM;
+}
+
+int check_header(const Jp2Header &ih, const tc_image_info &info, std::string &err)
+{
+    if (ih.have && (ih.width != (uint32_t)info.width || ih.height != (uint32_t)info.height ||
+                    ih.ncomp != (uint32_t)info.ncomp)) {
+        err = "the JP2 image header disagrees with the codestream's SIZ marker";
+        return TC_E_CODESTREAM;
+    }
+    return TC_OK;
+}
+
+}  // namespace
+
+int read_header(const uint8_t *cs, size_t len, tc_image_info &info, std::string &err)
+{
+    size_t off, n;
+    Jp2Header ih;
+    int rc = locate_codestream(cs, len, off, n, ih, err);
+    if (rc) return rc;
+    if ((rc = read_raw_header(cs + off, n, info, err))) return rc;
+    return check_header(ih, info, err);
+}
+
+int parse_codestream(const uint8_t *cs, size_t len, Parsed &out, std::string &err)
+{
+    size_t off, n;
+    Jp2Header ih;
+    int rc = locate_codestream(cs, len, off, n, ih, err);
+    if (rc) return rc;
+    if ((rc = parse_raw_codestream(cs + off, n, out, err))) return rc;
+    if ((rc = check_header(ih, out.info, err))) return rc;
+    // Segments of a single-layer stream are read in place: make their offsets
+    // count from the start of the file.
+    if (off && out.pool_is_cs)
+        for (tc_cblk_desc &d : out.desc) d.seg_off += off;
     return TC_OK;
 }
 

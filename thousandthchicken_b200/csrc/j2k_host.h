@@ -53,6 +53,8 @@ struct Parsed {
     std::vector<uint8_t> own_pool;  // used when blocks have several segments
     bool pool_is_cs = true;
 };
+// cs: a raw codestream (starts with SOC) or a JP2 file, whose first
+// codestream box is decoded; segment offsets count from the start of `cs`.
 int parse_codestream(const uint8_t *cs, size_t len, Parsed &out, std::string &err);
 int read_header(const uint8_t *cs, size_t len, tc_image_info &info, std::string &err);
 
