@@ -210,7 +210,8 @@ int tc_color_forward(tc_ctx *ctx, int kind, int ncomp,
 /* ---- codestream parsing (the Tier-2 hand-off) ---------------------------- */
 
 typedef struct tc_image_info {
-    int32_t width, height, ncomp, bits;    /* all components share size/depth */
+    int32_t width, height, ncomp, bits;    /* all components share size/depth;
+                                              width/height: Xsiz-XOsiz, Ysiz-YOsiz */
     int32_t is_signed;
     int32_t levels;                        /* decomposition levels NL */
     int32_t reversible;                    /* 1 = 5/3, 0 = 9/7 */
@@ -219,18 +220,34 @@ typedef struct tc_image_info {
     int32_t layers, progression;
     int32_t guard_bits, quant_style;
     uint32_t ncblk;                        /* code-blocks over all components */
-    uint32_t reserved;
+    uint32_t ntiles;                       /* tiles (ISO B.3); 1 for an untiled image */
 } tc_image_info;
 
-/* Read the main header only.  Replaces read_main_header (codestream.c:233-258). */
+/* One tile of a parsed image: its region in samples from the image's
+ * top-left corner, and the element offset of its coefficients in the
+ * image's coefficient arena.  The arena is tile-major: tile t's component c
+ * is a w*h plane (pitch w) at coef_off + c*w*h.  Tiles follow the reference's
+ * type_tile geometry (codestream_image.c:256-270, tlx/tly/width/height) with
+ * the SIZ offsets of ISO B.3.  Tiled images are decoded when every tile's
+ * origin on the reference grid is a multiple of 2^levels in both axes (all
+ * power-of-two tile sizes of at least 2^levels); others are
+ * TC_E_UNSUPPORTED. */
+typedef struct tc_tile_info {
+    int32_t x0, y0, w, h;
+    uint64_t coef_off;
+} tc_tile_info;
+
+/* Read the main header only (tile grid included).  Replaces read_main_header
+ * (codestream.c:233-258). */
 int tc_j2k_read_header(const uint8_t *h_cs, size_t len, tc_image_info *info);
 
 /* Parse a whole codestream into code-block descriptors.  Segment offsets
  * refer to h_pool: for single-layer streams h_pool is the codestream itself
  * (zero copy) and *pool_is_cs is set; otherwise the parser gathers each
- * block's layers into a contiguous pool it owns.  Output offsets address a
- * plane set of ncomp planes of width*height elements (plane c at element
- * c*width*height).  Replaces decode_codestream / decode_tiles /
+ * block's layers into a contiguous pool it owns.  Output offsets address the
+ * image's tile-major coefficient arena (see tc_tile_info; an untiled image is
+ * one tile, so plane c starts at element c*width*height).  Descriptors come
+ * tile by tile.  Replaces decode_codestream / decode_tiles /
  * decode_packet_header / decode_packet_body (codestream.c:336-536) and the
  * codeBlockCallback hand-off.  Free with tc_j2k_parsed_free. */
 typedef struct tc_j2k_parsed {
@@ -240,6 +257,7 @@ typedef struct tc_j2k_parsed {
     uint64_t pool_len;
     int32_t pool_is_cs;
     int32_t reserved;
+    const tc_tile_info *tiles;  /* info.ntiles entries, raster order */
 } tc_j2k_parsed;
 int tc_j2k_parse(const uint8_t *h_cs, size_t len, tc_j2k_parsed **out);
 void tc_j2k_parsed_free(tc_j2k_parsed *p);

@@ -96,3 +96,39 @@ def oracle_mallat(cs, r=0.5):
             o = int(d["out_off"]) + y * int(d["out_pitch"])
             flat[o: o + w] = v[y]
     return out, info
+
+
+def pil_j2k(img, **kw):
+    """OpenJPEG (through Pillow) codestream of a planar uint8/uint16 image."""
+    import io
+    from PIL import Image
+    a = np.moveaxis(img, 0, -1) if img.shape[0] == 3 else img[0]
+    buf = io.BytesIO()
+    Image.fromarray(a).save(buf, "JPEG2000", no_jp2=True, **kw)
+    return buf.getvalue()
+
+
+def openjpeg_decode(cs):
+    """OpenJPEG's own decode of a codestream, planar."""
+    import io
+    from PIL import Image
+    a = np.asarray(Image.open(io.BytesIO(cs)))
+    return np.moveaxis(a, -1, 0) if a.ndim == 3 else a[None]
+
+
+def oracle_decode_tiled(cs, r=0.5):
+    """Oracle decode of a (possibly tiled) codestream: each tile's
+    descriptors, rebased to the tile's own planes, through the oracle's
+    whole-tile decode, placed at the tile's position.  Returns (info, uint16
+    [ncomp, height, width])."""
+    info, desc, pool = codec.parse(cs)
+    W, H, C = info["width"], info["height"], info["ncomp"]
+    out = np.zeros((C, H, W), np.uint16)
+    bounds = [t[4] for t in info["tiles"]] + [C * W * H]
+    for k, (x0, y0, w, h, co) in enumerate(info["tiles"]):
+        sel = (desc["out_off"] >= bounds[k]) & (desc["out_off"] < bounds[k + 1])
+        d = desc[sel].copy()
+        d["out_off"] -= np.uint64(co)
+        out[:, y0:y0 + h, x0:x0 + w] = O.decode_tile(d, pool, w, h, C, info["bits"], info["levels"],
+                                                     bool(info["reversible"]), bool(info["mct"]), r=r)
+    return info, out

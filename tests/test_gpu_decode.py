@@ -6,6 +6,7 @@ import pytest
 
 import oracle as O
 from conftest import golden_cases, load_golden, synth_image
+from test_host_codec import TILED
 from thousandthchicken_b200 import codec
 
 pytestmark = pytest.mark.gpu
@@ -214,3 +215,61 @@ def test_jp2_files_decode(gpu_ctx, tmp_path):
     want = _decoder(gpu_ctx).decode(cs)
     np.testing.assert_array_equal(_decoder(gpu_ctx).decode(jp2), want)
     np.testing.assert_array_equal(_decoder(gpu_ctx).decode(p), want)
+
+
+def _tiled_ids(kw):
+    return "-".join(f"{k}={v}" for k, v in kw.items())
+
+
+@pytest.mark.parametrize("kw", TILED, ids=_tiled_ids)
+def test_tiled_streams_decode(gpu_ctx, kw):
+    """Tiled OpenJPEG streams (the reference's Decoder::decode loops over
+    tiles, Decoder.cpp:127-197): each tile's levels run in the batched
+    reverse-DWT launches and its last level writes the tile's region of the
+    image.  Lossless: the original; lossy: within 1 LSB of the oracle's
+    tile-by-tile decode."""
+    from gpu_helpers import oracle_decode_tiled, pil_j2k
+    img = synth_image(600, 400, 3, 8, seed=3)
+    cs = pil_j2k(img, **kw)
+    got = _decoder(gpu_ctx).decode(cs).astype(np.int64)
+    _, want = oracle_decode_tiled(cs)
+    if kw.get("irreversible"):
+        d = np.abs(got - want.astype(np.int64))
+        assert d.max() <= 1
+        assert (d > 0).mean() < 0.005
+    else:
+        np.testing.assert_array_equal(got, img)
+
+
+def test_tiled_and_untiled_images_in_one_plan(gpu_ctx):
+    """Tiled and untiled images of both wavelets, 8- and 16-bit, in one plan,
+    run twice (the second reuses the job table) and replayed as a graph:
+    each output equals the image's own single decode."""
+    from gpu_helpers import openjpeg_decode, pil_j2k
+    from thousandthchicken_b200.stages import Plan
+    g16 = synth_image(300, 260, 1, 16, seed=21)
+    streams = [pil_j2k(synth_image(520, 300, 3, 8, seed=20), tile_size=(128, 128)),
+               codec.encode(synth_image(400, 120, 3, 8, 22), 8, levels=5, reversible=False, base_step=1 / 64),
+               pil_j2k(g16, tile_size=(256, 64), num_resolutions=5),
+               pil_j2k(synth_image(333, 257, 3, 8, seed=23), tile_size=(64, 128), irreversible=True),
+               codec.encode(synth_image(96, 80, 1, 8, 24), 8, levels=3, reversible=True, mct=False)]
+    dec = _decoder(gpu_ctx)
+    singles = [dec.decode(s) for s in streams]
+    # Pillow's 16-bit tile writer does not hand OpenJPEG the input samples of
+    # every tile, so the stream's own content is OpenJPEG's decode of it
+    np.testing.assert_array_equal(singles[2], openjpeg_decode(streams[2]))
+    np.testing.assert_array_equal(singles[0], synth_image(520, 300, 3, 8, seed=20))
+    plan = Plan(gpu_ctx, streams)
+    outs = plan.alloc_outputs()
+    for graph in (False, False, True, True):
+        plan.set_graph(graph)
+        for o in outs:
+            o.zero_()
+        plan.execute(outs)
+        gpu_ctx.synchronize()
+        for single, o in zip(singles, outs):
+            got = o.cpu().numpy()
+            if single.dtype == np.uint16:
+                got = got.view(np.uint16)
+            np.testing.assert_array_equal(got.reshape(single.shape), single)
+    plan.close()

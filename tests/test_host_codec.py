@@ -176,3 +176,64 @@ def test_bad_jp2_files_are_rejected(case):
             "garbage": b"\x00\x01\x02\x03" * 8}[case]
     with pytest.raises(TCError):
         codec.parse(data)
+
+
+TILED = [  # OpenJPEG encoder options: tile grids, image and tile offsets, progressions
+    dict(tile_size=(256, 256)),
+    dict(tile_size=(128, 256), num_resolutions=4),
+    dict(tile_size=(256, 128), progression="RPCL"),
+    dict(tile_size=(96, 160)),  # tiles whose subbands start inside a code-block
+    dict(tile_size=(256, 256), offset=(32, 64)),
+    dict(tile_size=(192, 96), offset=(64, 32), irreversible=True),
+    dict(tile_size=(512, 512), irreversible=True, quality_mode="rates", quality_layers=[20, 5]),
+]
+
+
+@pytest.mark.parametrize("kw", TILED, ids=lambda kw: "-".join(f"{k}={v}" for k, v in kw.items()))
+def test_tiled_streams_through_oracle(kw):
+    """Tiled codestreams written by OpenJPEG: the parser's tile grid (ISO B.3,
+    the reference's init_tiles, codestream_image.c:256-270) partitions the
+    image, each tile's coefficients are a tile-major arena, and the oracle
+    decodes each tile to the original (lossless) or within 1 LSB of
+    OpenJPEG's own decode (lossy)."""
+    pytest.importorskip("PIL.Image")
+    from gpu_helpers import oracle_decode_tiled, openjpeg_decode, pil_j2k
+    img = synth_image(600, 400, 3, 8, seed=3)
+    cs = pil_j2k(img, **kw)
+    info, out = oracle_decode_tiled(cs)
+    tiles = info["tiles"]
+    assert info["ntiles"] == len(tiles) > 1
+    cover = np.zeros((400, 600), np.int32)
+    off = 0
+    for x0, y0, w, h, co in tiles:
+        cover[y0:y0 + h, x0:x0 + w] += 1
+        assert co == off
+        off += 3 * w * h
+    assert (cover == 1).all()
+    if kw.get("irreversible"):
+        assert np.abs(out.astype(np.int64) - openjpeg_decode(cs)).max() <= 1
+    else:
+        np.testing.assert_array_equal(out, img)
+
+
+def test_tile_origins_off_the_dwt_grid_are_unsupported():
+    """Tiles whose origin is not a multiple of 2^levels would need odd-origin
+    lifting: refused as unsupported, by the header reader too."""
+    pytest.importorskip("PIL.Image")
+    from gpu_helpers import pil_j2k
+    cs = pil_j2k(synth_image(300, 200, 1, 8, seed=4), tile_size=(100, 100))
+    for fn in (codec.parse, codec.read_header):
+        with pytest.raises(TCError) as ei:
+            fn(cs)
+        assert ei.value.status == TC_E_UNSUPPORTED
+
+
+def test_tiled_16bit_stream_matches_openjpeg():
+    """A 16-bit single-component tiled stream with ragged edge tiles decodes
+    through the oracle exactly as OpenJPEG decodes it."""
+    pytest.importorskip("PIL.Image")
+    from gpu_helpers import oracle_decode_tiled, openjpeg_decode, pil_j2k
+    cs = pil_j2k(synth_image(300, 260, 1, 16, seed=21), tile_size=(256, 64), num_resolutions=5)
+    info, out = oracle_decode_tiled(cs)
+    assert info["ntiles"] == 10 and info["bits"] == 16
+    np.testing.assert_array_equal(out, openjpeg_decode(cs))

@@ -56,12 +56,18 @@ class ImageInfo(C.Structure):
     _fields_ = [(n, C.c_int32) for n in ("width", "height", "ncomp", "bits", "is_signed", "levels",
                                         "reversible", "mct", "cblk_w", "cblk_h", "layers", "progression",
                                         "guard_bits", "quant_style")] + \
-               [("ncblk", C.c_uint32), ("reserved", C.c_uint32)]
+               [("ncblk", C.c_uint32), ("ntiles", C.c_uint32)]
+
+
+class TileInfo(C.Structure):
+    _fields_ = [("x0", C.c_int32), ("y0", C.c_int32), ("w", C.c_int32), ("h", C.c_int32),
+                ("coef_off", C.c_uint64)]
 
 
 class Parsed(C.Structure):
     _fields_ = [("info", ImageInfo), ("desc", C.POINTER(CblkDesc)), ("pool", C.POINTER(C.c_uint8)),
-                ("pool_len", C.c_uint64), ("pool_is_cs", C.c_int32), ("reserved", C.c_int32)]
+                ("pool_len", C.c_uint64), ("pool_is_cs", C.c_int32), ("reserved", C.c_int32),
+                ("tiles", C.POINTER(TileInfo))]
 
 
 class EncodeParams(C.Structure):

@@ -16,7 +16,7 @@ DESC_DTYPE = np.dtype([("seg_off", "<u8"), ("out_off", "<u8"), ("seg_len", "<u4"
 assert DESC_DTYPE.itemsize == 40
 
 INFO_FIELDS = ("width", "height", "ncomp", "bits", "is_signed", "levels", "reversible", "mct", "cblk_w",
-               "cblk_h", "layers", "progression", "guard_bits", "quant_style", "ncblk")
+               "cblk_h", "layers", "progression", "guard_bits", "quant_style", "ncblk", "ntiles")
 
 
 def _info_dict(info: L.ImageInfo) -> dict:
@@ -36,13 +36,17 @@ def read_header(cs) -> dict:
 
 
 def parse(cs):
-    """Parse a codestream: returns (info dict, descriptor array, segment pool)."""
+    """Parse a codestream: returns (info dict, descriptor array, segment pool).
+    info["tiles"] lists each tile as (x0, y0, w, h, coef_off): its region of
+    the image and the element offset of its planes in the tile-major
+    coefficient arena the descriptors' out_off address."""
     a = _buf(cs)
     out = C.POINTER(L.Parsed)()
     L.check(L.lib().tc_j2k_parse(a.ctypes.data, a.size, C.byref(out)), what="tc_j2k_parse")
     try:
         p = out.contents
         info = _info_dict(p.info)
+        info["tiles"] = [(t.x0, t.y0, t.w, t.h, t.coef_off) for t in p.tiles[:info["ntiles"]]]
         n = info["ncblk"]
         desc = np.empty(n, DESC_DTYPE)
         if n:

@@ -208,6 +208,8 @@ struct tc_plan {
         tc_image_info info{};
         uint64_t coef_off = 0;     // byte offset in the coefficient arena
         size_t out_bytes = 0;
+        std::vector<tc_tile_info> tiles;  // tile-major coefficients from coef_off
+        std::vector<size_t> tile_scratch; // each tile's scratch, from the image's
     };
     std::vector<Img> imgs;
     DevBuf pool, desc, order, coef, scratch;
@@ -238,6 +240,12 @@ struct tc_plan {
     uint64_t graph_launches = 0;     // kernels per replay
 };
 
+// Plans of several images or of tiled images run the batched reverse DWT.
+static bool plan_batched(const tc_plan *P)
+{
+    return P->imgs.size() > 1 || (P->imgs.size() == 1 && P->imgs[0].tiles.size() > 1);
+}
+
 static void plan_drop_graph(tc_plan *P)
 {
     if (P->graph) cudaGraphExecDestroy(P->graph);
@@ -267,8 +275,14 @@ static int plan_build_parsed(tc_ctx *ctx, const Parsed *const *parsed, const uin
         coef_total += (uint64_t)inf.ncomp * inf.width * inf.height * 4;
         coef_total = (coef_total + 255) & ~uint64_t(255);
         im.out_bytes = (size_t)inf.ncomp * inf.width * inf.height * sample_bytes(inf.bits);
-        scratch_max = std::max(scratch_max, reverse_scratch_bytes(inf.width, inf.height, inf.levels, inf.ncomp));
-        scratch_sum += (reverse_scratch_bytes(inf.width, inf.height, inf.levels, inf.ncomp) + 255) & ~size_t(255);
+        im.tiles = parsed[i]->tiles;
+        size_t img_scratch = 0;
+        for (const tc_tile_info &t : im.tiles) {
+            im.tile_scratch.push_back(img_scratch);
+            img_scratch += (reverse_scratch_bytes(t.w, t.h, inf.levels, inf.ncomp) + 255) & ~size_t(255);
+        }
+        scratch_max = std::max(scratch_max, img_scratch);
+        scratch_sum += img_scratch;
         P->imgs.push_back(im);
         pool_total += (pool_lens[i] + 15) & ~uint64_t(15);
         P->ncblk += (int)parsed[i]->desc.size();
@@ -309,7 +323,8 @@ static int plan_build_parsed(tc_ctx *ctx, const Parsed *const *parsed, const uin
         (e = P->desc.ensure_on(sizeof(tc_cblk_desc) * std::max(1, P->ncblk), st, mp)) != cudaSuccess ||
         (e = P->order.ensure_on(sizeof(uint32_t) * std::max(1, P->ncblk), st, mp)) != cudaSuccess ||
         (e = P->coef.ensure_on(std::max<uint64_t>(coef_total, 256), st, mp)) != cudaSuccess ||
-        (e = P->scratch.ensure_on(std::max<size_t>(n > 1 ? scratch_sum : scratch_max, 256), st, mp)) != cudaSuccess)
+        (e = P->scratch.ensure_on(std::max<size_t>(plan_batched(P) ? scratch_sum : scratch_max, 256), st, mp)) !=
+            cudaSuccess)
         return cuda_status(ctx, e, "plan allocation");
     if ((e = cudaMemcpyAsync(P->pool.ptr, hpool, pool_bytes, cudaMemcpyHostToDevice, ctx->stream)) ||
         (e = cudaMemcpyAsync(P->desc.ptr, hdesc, sizeof(tc_cblk_desc) * P->ncblk, cudaMemcpyHostToDevice,
@@ -338,42 +353,61 @@ static int plan_build(tc_ctx *ctx, const uint8_t *const *cs, const size_t *lens,
     return plan_build_parsed(ctx, pp.data(), pools.data(), plens.data(), n, P);
 }
 
-// Reverse DWT of every image of a batch plan with one launch per level step
-// and kind instead of per image and level: at step t image i runs its level
-// L_i - t, so images of different sizes and level counts share the launches.
-// Intermediate levels are grouped by wavelet (each job one component plane);
-// last levels, fused with colour, by wavelet, colour transform, component
-// count, sample type and bit depth.  The job table is built on the host and
-// uploaded once per set of output buffers (a replayed graph needs no copy).
+// Reverse DWT of every tile of every image of a plan with one launch per
+// level step and kind instead of per tile and level: at step t a tile of an
+// image of L levels runs its level L - t, so tiles and images of different
+// sizes and level counts share the launches.  Intermediate levels are
+// grouped by wavelet (each job one component plane of one tile); last
+// levels, fused with colour and written into the image at the tile's
+// position, by wavelet, colour transform, component count, sample type and
+// bit depth.  The job table is built on the host and uploaded once per set
+// of output buffers (a replayed graph needs no copy).
 static int run_reverse_batched(tc_plan *P, void *const *d_out)
 {
     tc_ctx *ctx = P->ctx;
     const size_t nimg = P->imgs.size();
     std::vector<void *> outs(d_out, d_out + nimg);
     cudaError_t e;
-    auto image_ptrs = [&](size_t i, void **cptr, void **optr) {
-        const tc_image_info &inf = P->imgs[i].info;
-        char *coef = static_cast<char *>(P->coef.ptr) + P->imgs[i].coef_off;
+    // one reverse transform: a tile of an image (an untiled image is one tile)
+    struct Unit {
+        const tc_image_info *inf;
+        int w, h;
+        void *coef[4];   // the tile's component planes, pitch w
+        void *out[4];    // the tile's first sample in each output plane
+        char *scratch;
+    };
+    std::vector<Unit> units;
+    for (size_t i = 0; i < nimg; i++) {
+        const tc_plan::Img &im = P->imgs[i];
+        const tc_image_info &inf = im.info;
+        char *coef = static_cast<char *>(P->coef.ptr) + im.coef_off;
         const size_t plane = (size_t)inf.width * inf.height;
         const int ob = sample_bytes(inf.bits);
-        for (int c = 0; c < inf.ncomp; c++) {
-            cptr[c] = coef + (size_t)c * plane * 4;
-            optr[c] = static_cast<char *>(d_out[i]) + (size_t)c * plane * ob;
+        for (size_t k = 0; k < im.tiles.size(); k++) {
+            const tc_tile_info &t = im.tiles[k];
+            Unit u;
+            u.inf = &inf;
+            u.w = t.w;
+            u.h = t.h;
+            for (int c = 0; c < inf.ncomp; c++) {
+                u.coef[c] = coef + (t.coef_off + (size_t)c * t.w * t.h) * 4;
+                u.out[c] = static_cast<char *>(d_out[i]) + ((size_t)c * plane + (size_t)t.y0 * inf.width + t.x0) * ob;
+            }
+            u.scratch = static_cast<char *>(P->scratch.ptr) + P->scratch_off[i] + im.tile_scratch[k];
+            units.push_back(u);
         }
-    };
+    }
+    const size_t nu = units.size();
     auto color_of = [](const tc_image_info &inf) {
         return inf.mct && inf.ncomp >= 3 ? (inf.reversible ? TC_COLOR_RCT : TC_COLOR_ICT) : TC_COLOR_DC;
     };
     // images without a transform: colour only
-    for (size_t i = 0; i < nimg; i++) {
-        const tc_image_info &inf = P->imgs[i].info;
+    for (const Unit &u : units) {
+        const tc_image_info &inf = *u.inf;
         if (inf.levels) continue;
-        void *cptr[4], *optr[4];
-        image_ptrs(i, cptr, optr);
         const int ob = sample_bytes(inf.bits);
-        e = launch_color_inverse(ctx, color_of(inf), inf.ncomp, cptr, inf.reversible ? TC_INT32 : TC_FLOAT32,
-                                 inf.width, optr, ob == 1 ? TC_U8 : TC_U16, inf.width, inf.width, inf.height,
-                                 inf.bits);
+        e = launch_color_inverse(ctx, color_of(inf), inf.ncomp, u.coef, inf.reversible ? TC_INT32 : TC_FLOAT32, u.w,
+                                 u.out, ob == 1 ? TC_U8 : TC_U16, inf.width, u.w, u.h, inf.bits);
         if (e != cudaSuccess) return cuda_status(ctx, e, "colour");
     }
     if (outs != P->jobs_outs) {
@@ -384,21 +418,17 @@ static int run_reverse_batched(tc_plan *P, void *const *d_out)
             const void *src[4];
             int src_pitch;
             size_t slab;
-            char *scratch;
         };
-        std::vector<Walk> wk(nimg);
+        std::vector<Walk> wk(nu);
         int maxl = 0;
-        for (size_t i = 0; i < nimg; i++) {
-            const tc_image_info &inf = P->imgs[i].info;
+        for (size_t i = 0; i < nu; i++) {
+            const Unit &u = units[i];
             Walk &W = wk[i];
-            level_sizes(inf.width, inf.height, inf.levels, W.ws, W.hs);
-            void *cptr[4], *optr[4];
-            image_ptrs(i, cptr, optr);
-            for (int c = 0; c < inf.ncomp; c++) W.src[c] = cptr[c];
-            W.src_pitch = inf.width;
-            W.slab = inf.levels >= 1 ? (size_t)W.ws[1] * W.hs[1] * 4 : 0;
-            W.scratch = static_cast<char *>(P->scratch.ptr) + P->scratch_off[i];
-            maxl = std::max(maxl, inf.levels);
+            level_sizes(u.w, u.h, u.inf->levels, W.ws, W.hs);
+            for (int c = 0; c < u.inf->ncomp; c++) W.src[c] = u.coef[c];
+            W.src_pitch = u.w;
+            W.slab = u.inf->levels >= 1 ? (size_t)W.ws[1] * W.hs[1] * 4 : 0;
+            maxl = std::max(maxl, u.inf->levels);
         }
         for (int t = 0; t < maxl; t++) {
             // intermediate levels, by wavelet
@@ -406,13 +436,12 @@ static int run_reverse_batched(tc_plan *P, void *const *d_out)
                 const int first = (int)jobs.size();
                 int tiles = 0, tx, ty;
                 rev_tile_shape(wv, &tx, &ty);
-                for (size_t i = 0; i < nimg; i++) {
-                    const tc_image_info &inf = P->imgs[i].info;
+                for (size_t i = 0; i < nu; i++) {
+                    const Unit &u = units[i];
+                    const tc_image_info &inf = *u.inf;
                     const int l = inf.levels - t;
                     if (l < 2 || (inf.reversible ? 0 : 1) != wv) continue;
                     Walk &W = wk[i];
-                    void *cptr[4], *optr[4];
-                    image_ptrs(i, cptr, optr);
                     const int buf = (inf.levels - l) & 1;
                     for (int c = 0; c < inf.ncomp; c++) {
                         RevJob J{};
@@ -421,51 +450,50 @@ static int run_reverse_batched(tc_plan *P, void *const *d_out)
                         J.io.ncomp = 1;
                         J.io.ll[0] = W.src[c];
                         J.io.ll_pitch = W.src_pitch;
-                        J.io.coef[0] = cptr[c];
-                        J.io.coef_pitch = inf.width;
-                        J.io.out[0] = W.scratch + ((size_t)c * 2 + buf) * W.slab;
+                        J.io.coef[0] = u.coef[c];
+                        J.io.coef_pitch = u.w;
+                        J.io.out[0] = u.scratch + ((size_t)c * 2 + buf) * W.slab;
                         J.io.out_pitch = W.ws[1];
                         J.tiles_x = (J.io.w + tx - 1) / tx;
                         J.tile0 = tiles;
                         tiles += J.tiles_x * ((J.io.h + ty - 1) / ty);
                         jobs.push_back(J);
                     }
-                    for (int c = 0; c < inf.ncomp; c++) W.src[c] = W.scratch + ((size_t)c * 2 + buf) * W.slab;
+                    for (int c = 0; c < inf.ncomp; c++) W.src[c] = u.scratch + ((size_t)c * 2 + buf) * W.slab;
                     W.src_pitch = W.ws[1];
                 }
                 if ((int)jobs.size() > first)
                     launches.push_back({first, (int)jobs.size() - first, tiles, wv, -1, 1, 0, 0});
             }
             // last levels with colour, by kernel instance
-            std::vector<char> taken(nimg, 0);
-            for (size_t i0 = 0; i0 < nimg; i0++) {
-                const tc_image_info &a = P->imgs[i0].info;
+            std::vector<char> taken(nu, 0);
+            for (size_t i0 = 0; i0 < nu; i0++) {
+                const tc_image_info &a = *units[i0].inf;
                 if (taken[i0] || a.levels - t != 1) continue;
                 const int first = (int)jobs.size();
                 int tiles = 0, tx, ty;
                 const int wv = a.reversible ? 0 : 1;
                 rev_tile_shape(wv, &tx, &ty);
-                for (size_t i = i0; i < nimg; i++) {
-                    const tc_image_info &inf = P->imgs[i].info;
+                for (size_t i = i0; i < nu; i++) {
+                    const Unit &u = units[i];
+                    const tc_image_info &inf = *u.inf;
                     if (taken[i] || inf.levels - t != 1 || inf.reversible != a.reversible ||
                         color_of(inf) != color_of(a) || inf.ncomp != a.ncomp ||
                         sample_bytes(inf.bits) != sample_bytes(a.bits) || inf.bits != a.bits)
                         continue;
                     taken[i] = 1;
                     Walk &W = wk[i];
-                    void *cptr[4], *optr[4];
-                    image_ptrs(i, cptr, optr);
                     RevJob J{};
                     J.io.w = W.ws[0];
                     J.io.h = W.hs[0];
                     J.io.ncomp = inf.ncomp;
                     J.io.ll_pitch = W.src_pitch;
-                    J.io.coef_pitch = inf.width;
+                    J.io.coef_pitch = u.w;
                     J.io.out_pitch = inf.width;
                     for (int c = 0; c < inf.ncomp; c++) {
                         J.io.ll[c] = W.src[c];
-                        J.io.coef[c] = cptr[c];
-                        J.io.out[c] = optr[c];
+                        J.io.coef[c] = u.coef[c];
+                        J.io.out[c] = u.out[c];
                     }
                     J.tiles_x = (J.io.w + tx - 1) / tx;
                     J.tile0 = tiles;
@@ -515,7 +543,7 @@ static int plan_run(tc_plan *P, void *const *d_out)
                                       TC_T1_OUT_DEQUANT, P->recon_r);
     if (e != cudaSuccess) return cuda_status(ctx, e, "Tier-1 launch");
     if (P->profiling) cudaEventRecord(P->ev[1], ctx->stream);
-    if (P->imgs.size() > 1) {
+    if (plan_batched(P)) {
         const int rc = run_reverse_batched(P, d_out);
         if (rc) return rc;
         if (P->profiling) cudaEventRecord(P->ev[2], ctx->stream);
@@ -606,6 +634,9 @@ int tc_ctx_destroy(tc_ctx *ctx)
     ctx->stage_pool.release();
     ctx->stage_desc.release();
     ctx->stage_order.release();
+    ctx->tmp_jobs.release();
+    ctx->stage_jobs.release();
+    if (ctx->jobs_uploaded) cudaEventDestroy(ctx->jobs_uploaded);
     if (ctx->d_words) cudaFree(ctx->d_words);
     for (int i = 0; i < 2; i++) {
         if (ctx->side[i]) cudaStreamDestroy(ctx->side[i]);
@@ -866,6 +897,7 @@ int tc_j2k_parse(const uint8_t *h_cs, size_t len, tc_j2k_parsed **out)
     b->own = holder;
     b->pub.info = holder->info;
     b->pub.desc = holder->desc.data();
+    b->pub.tiles = holder->tiles.data();
     b->pub.pool_is_cs = holder->pool_is_cs ? 1 : 0;
     b->pub.pool = holder->pool_is_cs ? h_cs : holder->own_pool.data();
     b->pub.pool_len = holder->pool_is_cs ? len : holder->own_pool.size();
@@ -1071,6 +1103,9 @@ int tc_decode_j2k(tc_ctx *ctx, const uint8_t *h_cs, size_t len, void *h_out, siz
     P.h_pool = ctx->stage_pool;
     P.h_desc = ctx->stage_desc;
     P.h_order = ctx->stage_order;
+    P.jobs = ctx->tmp_jobs;
+    P.h_jobs = ctx->stage_jobs;
+    P.jobs_uploaded = ctx->jobs_uploaded;
     auto give_back = [&]() {
         ctx->tmp_pool = P.pool;
         ctx->tmp_desc = P.desc;
@@ -1080,6 +1115,9 @@ int tc_decode_j2k(tc_ctx *ctx, const uint8_t *h_cs, size_t len, void *h_out, siz
         ctx->stage_pool = P.h_pool;
         ctx->stage_desc = P.h_desc;
         ctx->stage_order = P.h_order;
+        ctx->tmp_jobs = P.jobs;
+        ctx->stage_jobs = P.h_jobs;
+        ctx->jobs_uploaded = P.jobs_uploaded;
     };
     const uint8_t *cs[1] = {h_cs};
     size_t lens[1] = {len};

@@ -728,6 +728,9 @@ struct Reader {
 // Main-header coding parameters (COD/QCD), shared by all components.
 struct Params {
     int width = 0, height = 0, ncomp = 0, bits = 0, is_signed = 0;
+    // reference grid (ISO B.2): image [xo, xs) x [yo, ys); tiles of tw x th
+    // anchored at (xto, yto)
+    int64_t xs = 0, ys = 0, xo = 0, yo = 0, xto = 0, yto = 0;
     int tw = 0, th = 0;
     int scod = 0, prog = 0, layers = 1, mct = 0;
     int levels = 0, xcb = 6, ycb = 6, cblk_style = 0, reversible = 1;
@@ -735,8 +738,42 @@ struct Params {
     int qstyle = 0, guard = 2;
     std::vector<int> q_eps, q_mu;  // as signalled (1 or 3N+1 entries)
     bool have_siz = false, have_cod = false, have_qcd = false;
+    // tiles in raster order, on the reference grid: [x0, x1) x [y0, y1)
+    struct Tile {
+        int64_t x0, y0, x1, y1;
+    };
+    std::vector<Tile> tiles;
 };
 }  // namespace
+
+// Tile grid (ISO B.3): tile (p, q) covers [max(XTOsiz + p*XTsiz, XOsiz),
+// min(XTOsiz + (p+1)*XTsiz, Xsiz)) horizontally, likewise vertically, as
+// the reference's init_tiles places tile p, q at p*tile_w, q*tile_h
+// (codestream_image.c:256-270) for a grid without offsets.  Each tile's
+// origin must be a multiple of 2^levels: the tile's subbands, and so its
+// reverse DWT, then have the geometry of an image of the tile's size at the
+// origin.
+static int tile_grid(Params &P, std::string &err)
+{
+    const int64_t nx = (P.xs - P.xto + P.tw - 1) / P.tw, ny = (P.ys - P.yto + P.th - 1) / P.th;
+    if (nx * ny > 65535) { err = "more than 65535 tiles"; return TC_E_CODESTREAM; }
+    const int64_t mask = (P.levels >= 62 ? INT64_MAX : ((int64_t)1 << P.levels) - 1);
+    P.tiles.clear();
+    for (int64_t q = 0; q < ny; q++)
+        for (int64_t p = 0; p < nx; p++) {
+            Params::Tile t;
+            t.x0 = std::max(P.xto + p * P.tw, P.xo);
+            t.y0 = std::max(P.yto + q * P.th, P.yo);
+            t.x1 = std::min(P.xto + (p + 1) * P.tw, P.xs);
+            t.y1 = std::min(P.yto + (q + 1) * P.th, P.ys);
+            if ((t.x0 & mask) || (t.y0 & mask)) {
+                err = "tile or image origins that are not multiples of 2^levels are not supported";
+                return TC_E_UNSUPPORTED;
+            }
+            P.tiles.push_back(t);
+        }
+    return TC_OK;
+}
 
 static int parse_main(Reader &rd, Params &P, std::string &err)
 {
@@ -755,10 +792,18 @@ static int parse_main(Reader &rd, Params &P, std::string &err)
             const uint32_t xs = rd.u32(), ys = rd.u32(), xo = rd.u32(), yo = rd.u32();
             const uint32_t xt = rd.u32(), yt = rd.u32(), xto = rd.u32(), yto = rd.u32();
             const uint32_t c = rd.u16();
-            if (xo || yo || xto || yto) { err = "image or tile offsets are not supported"; return TC_E_UNSUPPORTED; }
+            if (xo >= xs || yo >= ys || xt == 0 || yt == 0 || xto > xo || yto > yo ||
+                (uint64_t)xto + xt <= xo || (uint64_t)yto + yt <= yo) {
+                err = "bad image or tile geometry in SIZ";
+                return TC_E_CODESTREAM;
+            }
             if (c < 1 || c > 4) { err = "1 to 4 components supported"; return TC_E_UNSUPPORTED; }
-            if (xs == 0 || ys == 0 || xs > 65535 || ys > 65535) { err = "image size out of range"; return TC_E_UNSUPPORTED; }
-            P.width = (int)xs; P.height = (int)ys; P.tw = (int)xt; P.th = (int)yt; P.ncomp = (int)c;
+            if (xs - xo > 65535 || ys - yo > 65535) { err = "image size out of range"; return TC_E_UNSUPPORTED; }
+            P.xs = xs; P.ys = ys; P.xo = xo; P.yo = yo; P.xto = xto; P.yto = yto;
+            P.width = (int)(xs - xo); P.height = (int)(ys - yo);
+            P.tw = (int)std::min<uint32_t>(xt, 0x7FFFFFFF);
+            P.th = (int)std::min<uint32_t>(yt, 0x7FFFFFFF);
+            P.ncomp = (int)c;
             for (uint32_t i = 0; i < c; i++) {
                 const uint32_t ss = rd.u8(), dx = rd.u8(), dy = rd.u8();
                 const int b = (int)(ss & 0x7F) + 1, sg = (int)(ss >> 7);
@@ -827,8 +872,7 @@ static int parse_main(Reader &rd, Params &P, std::string &err)
         rd.pos = seg_end;
     }
     if (!P.have_siz || !P.have_cod || !P.have_qcd) { err = "main header lacks SIZ, COD or QCD"; return TC_E_CODESTREAM; }
-    if (P.tw < P.width || P.th < P.height) { err = "multiple tiles are not supported"; return TC_E_UNSUPPORTED; }
-    return TC_OK;
+    return tile_grid(P, err);
 }
 
 static void fill_info(const Params &P, tc_image_info &info)
@@ -848,6 +892,7 @@ static void fill_info(const Params &P, tc_image_info &info)
     info.progression = P.prog;
     info.guard_bits = P.guard;
     info.quant_style = P.qstyle;
+    info.ntiles = (uint32_t)P.tiles.size();
 }
 
 static int read_raw_header(const uint8_t *cs, size_t len, tc_image_info &info, std::string &err)
@@ -897,30 +942,52 @@ struct CblkState {
     int passes = 0;
     std::vector<std::pair<size_t, uint32_t>> segs;  // (offset in cs, length)
 };
+
+// Descriptors of all tiles before their segments are placed: each entry's
+// segments are segs[first[k] .. first[k+1]).
+struct Emit {
+    std::vector<std::pair<size_t, uint32_t>> segs;
+    std::vector<uint32_t> first;
+    bool multi = false;  // some block has more than one segment
+};
 }  // namespace
 
-static int parse_raw_codestream(const uint8_t *cs, size_t len, Parsed &out, std::string &err)
+// Packets of one tile (ISO B.9-B.10) read from its tile-parts `parts` (packet
+// data ranges in codestream order), and its code-block descriptors appended
+// to out.desc with coefficients at element coef_off of the image's arena.
+// Follows decode_tiles / decode_packet_header / decode_packet_body
+// (codestream.c:336-510), one call per tile as decode_codestream loops over
+// the tiles (codestream.c:524-527).
+static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Params::Tile &T,
+                      const std::vector<std::pair<size_t, size_t>> &parts, uint64_t coef_off, Parsed &out,
+                      Emit &em, std::string &err)
 {
-    Reader rd{cs, len};
-    Params P;
-    int rc = parse_main(rd, P, err);
-    if (rc) return rc;
-    fill_info(P, out.info);
-
-    // Geometry per resolution (identical for every component).
-    std::vector<Resolution> geo = make_geometry(P.width, P.height, P.levels, P.xcb, P.ycb);
+    int rc;
+    const int tw = (int)(T.x1 - T.x0), th = (int)(T.y1 - T.y0);
+    // With the tile origin a multiple of 2^levels, the subband sizes are
+    // those of a tw x th image at the origin; only the code-block grid,
+    // anchored at the reference grid's origin, depends on where the tile is.
+    std::vector<Resolution> geo = make_geometry(tw, th, P.levels, P.xcb, P.ycb);
     for (int r = 0; r <= P.levels; r++) {
         // Code-block size is capped by the precinct size (ISO B.7); one
         // precinct per resolution is required.
         const int px = P.ppx[r], py = P.ppy[r];
         const int xcb = std::min(P.xcb, r ? px - 1 : px), ycb = std::min(P.ycb, r ? py - 1 : py);
-        if (geo[r].w > (1 << px) || geo[r].h > (1 << py)) { err = "more than one precinct per resolution"; return TC_E_UNSUPPORTED; }
+        const int sh = P.levels - r;
+        const int64_t rx0 = T.x0 >> sh, ry0 = T.y0 >> sh;
+        const int64_t rx1 = (T.x1 + ((int64_t)1 << sh) - 1) >> sh, ry1 = (T.y1 + ((int64_t)1 << sh) - 1) >> sh;
+        if ((rx0 >> px) != ((rx1 - 1) >> px) || (ry0 >> py) != ((ry1 - 1) >> py)) {
+            err = "more than one precinct per resolution";
+            return TC_E_UNSUPPORTED;
+        }
         if (xcb < 0 || ycb < 0) { err = "bad precinct size"; return TC_E_CODESTREAM; }
         for (Band &b : geo[r].bands) {
             b.cbw_log2 = xcb;
             b.cbh_log2 = ycb;
-            b.ncbx = b.w > 0 ? ceil_div(b.w, 1 << xcb) : 0;
-            b.ncby = b.h > 0 ? ceil_div(b.h, 1 << ycb) : 0;
+            b.ox = (int)((T.x0 >> b.level) & ((1 << xcb) - 1));
+            b.oy = (int)((T.y0 >> b.level) & ((1 << ycb) - 1));
+            b.ncbx = b.w > 0 ? ceil_div(b.ox + b.w, 1 << xcb) : 0;
+            b.ncby = b.h > 0 ? ceil_div(b.oy + b.h, 1 << ycb) : 0;
         }
     }
     if ((rc = assign_quant(P, geo, err))) return rc;
@@ -943,39 +1010,8 @@ static int parse_raw_codestream(const uint8_t *cs, size_t len, Parsed &out, std:
             }
     }
 
-    // Tile-parts of the single tile: collect the packet data ranges.
-    std::vector<std::pair<size_t, size_t>> parts;
-    for (;;) {
-        const uint32_t m = rd.u16();
-        if (rd.bad) { err = "truncated codestream"; return TC_E_CODESTREAM; }
-        if (m == M_EOC) break;
-        if (m != M_SOT) { err = "expected SOT"; return TC_E_CODESTREAM; }
-        const size_t sot_pos = rd.pos - 2;
-        const uint32_t lsot = rd.u16(), isot = rd.u16(), psot = rd.u32();
-        rd.u8();  // TPsot
-        rd.u8();  // TNsot
-        if (lsot != 10 || isot != 0) { err = "bad SOT or tile index"; return TC_E_CODESTREAM; }
-        const size_t end = psot ? sot_pos + psot : len;
-        if (end > len) { err = "tile-part runs past the codestream"; return TC_E_CODESTREAM; }
-        for (;;) {
-            const uint32_t mm = rd.u16();
-            if (rd.bad) { err = "truncated tile-part header"; return TC_E_CODESTREAM; }
-            if (mm == M_SOD) break;
-            const uint32_t L = rd.u16();
-            if (mm == M_COD || mm == M_COC || mm == M_QCD || mm == M_QCC || mm == M_RGN ||
-                mm == M_POC || mm == M_PPT) {
-                err = "tile-part header coding parameters are not supported";
-                return TC_E_UNSUPPORTED;
-            }
-            if (L < 2 || rd.pos - 2 + L > end) { err = "bad tile-part marker"; return TC_E_CODESTREAM; }
-            rd.pos += L - 2;
-        }
-        parts.emplace_back(rd.pos, end);
-        rd.pos = end;
-        if (rd.pos >= len) break;
-    }
-    // Concatenate tile-part bodies logically: packets may not straddle
-    // tile-parts in practice, and we read them part by part.
+    // The tile-part bodies are read one after the other as one packet
+    // sequence; a packet does not straddle two tile-parts.
     size_t part_i = 0;
     size_t pos = parts.empty() ? len : parts[0].first;
     auto part_end = [&]() { return part_i < parts.size() ? parts[part_i].second : len; };
@@ -1057,42 +1093,36 @@ static int parse_raw_codestream(const uint8_t *cs, size_t len, Parsed &out, std:
         for (int r = 0; r < R; r++) for (int c = 0; c < C; c++) for (int l = 0; l < L; l++)
             if ((rc = run(l, r, c))) return rc;
         break;
-    default:  // PCRL, CPRL (one precinct per resolution, all at the origin)
+    default:  // PCRL, CPRL (one precinct per resolution)
         for (int c = 0; c < C; c++) for (int r = 0; r < R; r++) for (int l = 0; l < L; l++)
             if ((rc = run(l, r, c))) return rc;
         break;
     }
 
-    // Emit descriptors.
-    out.desc.clear();
-    out.own_pool.clear();
-    bool multi = false;
-    for (int c = 0; c < C; c++)
-        for (int r = 0; r < R; r++)
-            for (auto &bs : st[c][r])
-                for (auto &cb : bs.cb)
-                    if (cb.segs.size() > 1) multi = true;
-    out.pool_is_cs = !multi;
-    const uint64_t plane = (uint64_t)P.width * P.height;
+    // Descriptors, component by component; segments are placed once every
+    // tile is read (parse_raw_codestream).
+    const uint64_t plane = (uint64_t)tw * th;
     for (int c = 0; c < C; c++)
         for (int r = 0; r < R; r++)
             for (size_t bi = 0; bi < geo[r].bands.size(); bi++) {
                 const Band &b = geo[r].bands[bi];
                 BandState &bs = st[c][r][bi];
+                const int cbw = 1 << b.cbw_log2, cbh = 1 << b.cbh_log2;
                 for (int j = 0; j < b.ncby; j++)
                     for (int i = 0; i < b.ncbx; i++) {
                         CblkState &cb = bs.cb[j * b.ncbx + i];
                         tc_cblk_desc d;
                         std::memset(&d, 0, sizeof d);
-                        const int cx = i << b.cbw_log2, cy = j << b.cbh_log2;
-                        d.w = (uint16_t)std::min(1 << b.cbw_log2, b.w - cx);
-                        d.h = (uint16_t)std::min(1 << b.cbh_log2, b.h - cy);
+                        const int cx = std::max(i * cbw - b.ox, 0), cy = std::max(j * cbh - b.oy, 0);
+                        d.w = (uint16_t)(std::min((i + 1) * cbw - b.ox, b.w) - cx);
+                        d.h = (uint16_t)(std::min((j + 1) * cbh - b.oy, b.h) - cy);
                         d.mb = (uint8_t)b.mb;
                         d.orient = (uint8_t)b.orient;
-                        d.out_pitch = (uint32_t)P.width;
-                        d.out_off = (uint64_t)c * plane + (uint64_t)(b.y0 + cy) * P.width + (uint64_t)(b.x0 + cx);
+                        d.out_pitch = (uint32_t)tw;
+                        d.out_off = coef_off + (uint64_t)c * plane + (uint64_t)(b.y0 + cy) * tw + (uint64_t)(b.x0 + cx);
                         d.step = P.reversible ? 1.0f : b.step;
                         d.flags = P.reversible ? 0 : TC_CBLK_IRREVERSIBLE;
+                        em.first.push_back((uint32_t)em.segs.size());
                         if (cb.included && cb.passes > 0) {
                             if (cb.zbp > b.mb) { err = "zero bit-planes exceed Mb"; return TC_E_CODESTREAM; }
                             const int numbps = b.mb - cb.zbp;
@@ -1104,14 +1134,10 @@ static int parse_raw_codestream(const uint8_t *cs, size_t len, Parsed &out, std:
                             d.passes = (uint8_t)cb.passes;
                             uint64_t total = 0;
                             for (auto &s : cb.segs) total += s.second;
-                            if (multi) {
-                                d.seg_off = out.own_pool.size();
-                                for (auto &s : cb.segs)
-                                    out.own_pool.insert(out.own_pool.end(), cs + s.first, cs + s.first + s.second);
-                            } else {
-                                d.seg_off = cb.segs.empty() ? 0 : cb.segs[0].first;
-                            }
+                            if (total > 0xFFFFFFFFull) { err = "code-block data too long"; return TC_E_CODESTREAM; }
                             d.seg_len = (uint32_t)total;
+                            if (cb.segs.size() > 1) em.multi = true;
+                            em.segs.insert(em.segs.end(), cb.segs.begin(), cb.segs.end());
                         } else {
                             d.zero_bitplanes = (uint8_t)b.mb;
                             d.passes = 0;
@@ -1119,6 +1145,91 @@ static int parse_raw_codestream(const uint8_t *cs, size_t len, Parsed &out, std:
                         out.desc.push_back(d);
                     }
             }
+    return TC_OK;
+}
+
+static int parse_raw_codestream(const uint8_t *cs, size_t len, Parsed &out, std::string &err)
+{
+    Reader rd{cs, len};
+    Params P;
+    int rc = parse_main(rd, P, err);
+    if (rc) return rc;
+    fill_info(P, out.info);
+    const size_t ntiles = P.tiles.size();
+
+    // Tile-parts (ISO A.4.2) in codestream order, grouped by tile index Isot:
+    // the packet data range of each.
+    std::vector<std::vector<std::pair<size_t, size_t>>> parts(ntiles);
+    for (;;) {
+        const uint32_t m = rd.u16();
+        if (rd.bad) { err = "truncated codestream"; return TC_E_CODESTREAM; }
+        if (m == M_EOC) break;
+        if (m != M_SOT) { err = "expected SOT"; return TC_E_CODESTREAM; }
+        const size_t sot_pos = rd.pos - 2;
+        const uint32_t lsot = rd.u16(), isot = rd.u16(), psot = rd.u32();
+        rd.u8();  // TPsot
+        rd.u8();  // TNsot
+        if (lsot != 10 || isot >= ntiles || (psot && psot < 14)) { err = "bad SOT or tile index"; return TC_E_CODESTREAM; }
+        const size_t end = psot ? sot_pos + psot : len;
+        if (end > len) { err = "tile-part runs past the codestream"; return TC_E_CODESTREAM; }
+        for (;;) {
+            const uint32_t mm = rd.u16();
+            if (rd.bad || rd.pos > end) { err = "truncated tile-part header"; return TC_E_CODESTREAM; }
+            if (mm == M_SOD) break;
+            const uint32_t L = rd.u16();
+            if (mm == M_COD || mm == M_COC || mm == M_QCD || mm == M_QCC || mm == M_RGN ||
+                mm == M_POC || mm == M_PPT) {
+                err = "tile-part header coding parameters are not supported";
+                return TC_E_UNSUPPORTED;
+            }
+            if (L < 2 || rd.pos - 2 + L > end) { err = "bad tile-part marker"; return TC_E_CODESTREAM; }
+            rd.pos += L - 2;
+        }
+        parts[isot].emplace_back(rd.pos, end);
+        rd.pos = end;
+        if (rd.pos >= len) break;
+    }
+
+    // Tiles one after the other, each with its own coefficient planes.
+    out.desc.clear();
+    out.own_pool.clear();
+    out.tiles.clear();
+    Emit em;
+    uint64_t coef_off = 0;
+    for (size_t t = 0; t < ntiles; t++) {
+        const Params::Tile &T = P.tiles[t];
+        if (parts[t].empty()) { err = "tile " + std::to_string(t) + " has no tile-part"; return TC_E_CODESTREAM; }
+        if ((rc = parse_tile(cs, len, P, T, parts[t], coef_off, out, em, err))) return rc;
+        tc_tile_info ti;
+        ti.x0 = (int32_t)(T.x0 - P.xo);
+        ti.y0 = (int32_t)(T.y0 - P.yo);
+        ti.w = (int32_t)(T.x1 - T.x0);
+        ti.h = (int32_t)(T.y1 - T.y0);
+        ti.coef_off = coef_off;
+        out.tiles.push_back(ti);
+        coef_off += (uint64_t)P.ncomp * ti.w * ti.h;
+    }
+    em.first.push_back((uint32_t)em.segs.size());
+
+    // Segments: in place in the codestream when every block has at most one,
+    // else gathered block by block into a pool of the parse's own.
+    out.pool_is_cs = !em.multi;
+    if (em.multi) {
+        uint64_t total = 0;
+        for (auto &s : em.segs) total += s.second;
+        out.own_pool.reserve(total);
+    }
+    for (size_t k = 0; k < out.desc.size(); k++) {
+        tc_cblk_desc &d = out.desc[k];
+        const uint32_t a = em.first[k], b = em.first[k + 1];
+        if (em.multi) {
+            d.seg_off = a < b ? out.own_pool.size() : 0;
+            for (uint32_t s = a; s < b; s++)
+                out.own_pool.insert(out.own_pool.end(), cs + em.segs[s].first, cs + em.segs[s].first + em.segs[s].second);
+        } else {
+            d.seg_off = a < b ? em.segs[a].first : 0;
+        }
+    }
     out.info.ncblk = (uint32_t)out.desc.size();
     return TC_OK;
 }

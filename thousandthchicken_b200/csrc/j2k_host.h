@@ -22,6 +22,11 @@ struct Band {
     int w = 0, h = 0;
     int cbw_log2 = 6, cbh_log2 = 6;
     int ncbx = 0, ncby = 0;
+    // offset of the band's first sample inside its first code-block: the
+    // code-block grid is anchored at the reference grid's origin (ISO B.7),
+    // so a tile that does not start on a block boundary has a narrower
+    // first block.  Block i spans [max(i*cbw - ox, 0), min((i+1)*cbw - ox, w)).
+    int ox = 0, oy = 0;
     int eps = 0, mu = 0;  // quantisation exponent / mantissa
     int mb = 0;           // magnitude bit-planes
     float step = 1.0f;    // irreversible step
@@ -52,6 +57,7 @@ struct Parsed {
     std::vector<tc_cblk_desc> desc;
     std::vector<uint8_t> own_pool;  // used when blocks have several segments
     bool pool_is_cs = true;
+    std::vector<tc_tile_info> tiles;  // info.ntiles entries
 };
 // cs: a raw codestream (starts with SOC) or a JP2 file, whose first
 // codestream box is decoded; segment offsets count from the start of `cs`.

@@ -70,6 +70,10 @@ struct tc_ctx {
     tc::DevBuf scratch;           // DWT intermediate levels
     tc::DevBuf tmp_pool, tmp_desc, tmp_order, tmp_coef, tmp_out;
     tc::PinBuf stage_pool, stage_desc, stage_order;  // pinned staging of tc_decode_j2k
+    // reverse-DWT job table of tc_decode_j2k's tiled images
+    tc::DevBuf tmp_jobs;
+    tc::PinBuf stage_jobs;
+    cudaEvent_t jobs_uploaded = nullptr;
     uint64_t launches = 0;
     int t1_group = 32;            // lanes per code-block in the Tier-1 kernel (8, 16 or 32)
     // side streams for concurrent Tier-1 class launches (created on first use)
