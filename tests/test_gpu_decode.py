@@ -6,7 +6,7 @@ import pytest
 
 import oracle as O
 from conftest import golden_cases, load_golden, synth_image
-from test_host_codec import TILED
+from test_host_codec import PRECINCTS, TILED
 from thousandthchicken_b200 import codec
 
 pytestmark = pytest.mark.gpu
@@ -273,3 +273,21 @@ def test_tiled_and_untiled_images_in_one_plan(gpu_ctx):
                 got = got.view(np.uint16)
             np.testing.assert_array_equal(got.reshape(single.shape), single)
     plan.close()
+
+
+@pytest.mark.parametrize("kw", [PRECINCTS[3], PRECINCTS[5], PRECINCTS[7]], ids=_tiled_ids)
+def test_precinct_streams_decode(gpu_ctx, kw):
+    """Precinct-partitioned streams (code-blocks as small as 2x2 at the
+    lowest resolutions) through the GPU: lossless equals the original, lossy
+    within 1 LSB of the oracle."""
+    from gpu_helpers import oracle_decode_tiled, pil_j2k
+    img = synth_image(600, 400, 3, 8, seed=3)
+    cs = pil_j2k(img, **kw)
+    got = _decoder(gpu_ctx).decode(cs).astype(np.int64)
+    if kw.get("irreversible"):
+        _, want = oracle_decode_tiled(cs)
+        d = np.abs(got - want.astype(np.int64))
+        assert d.max() <= 1
+        assert (d > 0).mean() < 0.005
+    else:
+        np.testing.assert_array_equal(got, img)

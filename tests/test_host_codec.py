@@ -237,3 +237,37 @@ def test_tiled_16bit_stream_matches_openjpeg():
     info, out = oracle_decode_tiled(cs)
     assert info["ntiles"] == 10 and info["bits"] == 16
     np.testing.assert_array_equal(out, openjpeg_decode(cs))
+
+
+PRECINCTS = [  # OpenJPEG encoder options with precinct partitions (several precincts per resolution)
+    dict(codeblock_size=(32, 32), precinct_size=(64, 64), progression="LRCP"),
+    dict(codeblock_size=(32, 32), precinct_size=(64, 64), progression="RLCP"),
+    dict(codeblock_size=(32, 32), precinct_size=(64, 64), progression="RPCL"),
+    dict(codeblock_size=(32, 32), precinct_size=(64, 64), progression="PCRL"),
+    dict(codeblock_size=(32, 32), precinct_size=(64, 64), progression="CPRL"),
+    dict(codeblock_size=(16, 16), precinct_size=(128, 32), progression="PCRL", irreversible=True),
+    dict(codeblock_size=(32, 32), precinct_size=(64, 64), tile_size=(256, 256), progression="CPRL"),
+    dict(codeblock_size=(32, 32), precinct_size=(128, 128), tile_size=(192, 96), offset=(64, 32),
+         progression="RPCL", quality_mode="rates", quality_layers=[20, 5], irreversible=True),
+    dict(codeblock_size=(64, 64), precinct_size=(256, 256), num_resolutions=7, progression="PCRL"),
+]
+
+
+@pytest.mark.parametrize("kw", PRECINCTS, ids=lambda kw: "-".join(f"{k}={v}" for k, v in kw.items()))
+def test_precinct_streams_through_oracle(kw):
+    """Precinct partitions (ISO B.6): packets per precinct in all five
+    progression orders, the position-driven ones (RPCL, PCRL, CPRL) visiting
+    each precinct at its first reference-grid position (B.12.1.3-B.12.1.5),
+    code-blocks capped to the precinct size (B.7), one tag-tree pair per
+    precinct and band.  The reference reads one precinct per resolution
+    (codestream.c:373-376); lossless decodes equal the original, lossy ones
+    OpenJPEG's decode within 1 LSB."""
+    pytest.importorskip("PIL.Image")
+    from gpu_helpers import oracle_decode_tiled, openjpeg_decode, pil_j2k
+    img = synth_image(600, 400, 3, 8, seed=3)
+    cs = pil_j2k(img, **kw)
+    info, out = oracle_decode_tiled(cs)
+    if kw.get("irreversible"):
+        assert np.abs(out.astype(np.int64) - openjpeg_decode(cs)).max() <= 1
+    else:
+        np.testing.assert_array_equal(out, img)

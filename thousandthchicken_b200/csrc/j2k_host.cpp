@@ -964,23 +964,42 @@ static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Para
 {
     int rc;
     const int tw = (int)(T.x1 - T.x0), th = (int)(T.y1 - T.y0);
+    const int NL = P.levels, R = NL + 1, C = P.ncomp, L = P.layers;
     // With the tile origin a multiple of 2^levels, the subband sizes are
-    // those of a tw x th image at the origin; only the code-block grid,
-    // anchored at the reference grid's origin, depends on where the tile is.
-    std::vector<Resolution> geo = make_geometry(tw, th, P.levels, P.xcb, P.ycb);
-    for (int r = 0; r <= P.levels; r++) {
-        // Code-block size is capped by the precinct size (ISO B.7); one
-        // precinct per resolution is required.
+    // those of a tw x th image at the origin; the code-block and precinct
+    // grids, anchored at the reference grid's origin, depend on where the
+    // tile is.
+    std::vector<Resolution> geo = make_geometry(tw, th, NL, P.xcb, P.ycb);
+
+    // Precinct partition of each resolution (ISO B.6): 2^PPx x 2^PPy cells
+    // of the resolution's grid; in a subband of resolution r > 0 the cells
+    // are 2^(PPx-1) x 2^(PPy-1), and code-blocks are capped to fit them (B.7).
+    struct PrecBand {
+        int i0 = 0, i1 = 0, j0 = 0, j1 = 0;  // the band's code-blocks inside the precinct
+        TagTree incl{1, 1}, zbp{1, 1};
+    };
+    struct ResState {
+        int64_t rx0 = 0, ry0 = 0;  // the resolution's origin on its own grid
+        int pw = 0, ph = 0;        // precincts across and down
+        std::vector<std::vector<CblkState>> cb;   // per band: its code-blocks
+        std::vector<std::vector<PrecBand>> prec;  // per precinct: per band
+    };
+    std::vector<ResState> rgeo(R);
+    int64_t nprec_bands = 0;
+    for (int r = 0; r <= NL; r++) {
         const int px = P.ppx[r], py = P.ppy[r];
         const int xcb = std::min(P.xcb, r ? px - 1 : px), ycb = std::min(P.ycb, r ? py - 1 : py);
-        const int sh = P.levels - r;
-        const int64_t rx0 = T.x0 >> sh, ry0 = T.y0 >> sh;
-        const int64_t rx1 = (T.x1 + ((int64_t)1 << sh) - 1) >> sh, ry1 = (T.y1 + ((int64_t)1 << sh) - 1) >> sh;
-        if ((rx0 >> px) != ((rx1 - 1) >> px) || (ry0 >> py) != ((ry1 - 1) >> py)) {
-            err = "more than one precinct per resolution";
-            return TC_E_UNSUPPORTED;
-        }
         if (xcb < 0 || ycb < 0) { err = "bad precinct size"; return TC_E_CODESTREAM; }
+        const int sh = NL - r;
+        const int64_t rx0 = (T.x0 + ((int64_t)1 << sh) - 1) >> sh, ry0 = (T.y0 + ((int64_t)1 << sh) - 1) >> sh;
+        const int64_t rx1 = (T.x1 + ((int64_t)1 << sh) - 1) >> sh, ry1 = (T.y1 + ((int64_t)1 << sh) - 1) >> sh;
+        ResState &rs = rgeo[r];
+        rs.rx0 = rx0;
+        rs.ry0 = ry0;
+        rs.pw = (int)(((rx1 + ((int64_t)1 << px) - 1) >> px) - (rx0 >> px));
+        rs.ph = (int)(((ry1 + ((int64_t)1 << py) - 1) >> py) - (ry0 >> py));
+        nprec_bands += (int64_t)rs.pw * rs.ph * (int64_t)geo[r].bands.size();
+        if (nprec_bands > (1 << 22)) { err = "too many precincts"; return TC_E_UNSUPPORTED; }
         for (Band &b : geo[r].bands) {
             b.cbw_log2 = xcb;
             b.cbh_log2 = ycb;
@@ -992,23 +1011,42 @@ static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Para
     }
     if ((rc = assign_quant(P, geo, err))) return rc;
 
-    // Per component, per resolution, per band: code-block states and trees.
-    struct BandState {
-        std::vector<CblkState> cb;
-        TagTree incl, zbp;
-        BandState(int w, int h) : cb((size_t)w * h), incl(std::max(w, 1), std::max(h, 1)),
-                                  zbp(std::max(w, 1), std::max(h, 1)) {}
-    };
-    std::vector<std::vector<std::vector<BandState>>> st(P.ncomp);
-    for (int c = 0; c < P.ncomp; c++) {
-        st[c].resize(P.levels + 1);
-        for (int r = 0; r <= P.levels; r++)
-            for (const Band &b : geo[r].bands) {
-                st[c][r].emplace_back(b.ncbx, b.ncby);
-                st[c][r].back().incl.reset_decoder();
-                st[c][r].back().zbp.reset_decoder();
-            }
-    }
+    // Per component and resolution: code-block states of each band, and per
+    // precinct the block range and tag trees of each band.
+    std::vector<std::vector<ResState>> st(C, rgeo);
+    for (int c = 0; c < C; c++)
+        for (int r = 0; r <= NL; r++) {
+            ResState &rs = st[c][r];
+            const int ppx = r ? P.ppx[r] - 1 : P.ppx[r], ppy = r ? P.ppy[r] - 1 : P.ppy[r];
+            const int64_t kx0 = rs.rx0 >> P.ppx[r], ky0 = rs.ry0 >> P.ppy[r];
+            for (const Band &b : geo[r].bands) rs.cb.emplace_back((size_t)b.ncbx * b.ncby);
+            rs.prec.resize((size_t)rs.pw * rs.ph);
+            for (int q = 0; q < rs.ph; q++)
+                for (int p = 0; p < rs.pw; p++) {
+                    auto &pbs = rs.prec[(size_t)q * rs.pw + p];
+                    for (const Band &b : geo[r].bands) {
+                        PrecBand pb;
+                        // the band and the precinct cell on the band's grid
+                        const int64_t bx0 = T.x0 >> b.level, by0 = T.y0 >> b.level;
+                        const int64_t cx0 = std::max(bx0, (kx0 + p) << ppx);
+                        const int64_t cx1 = std::min(bx0 + b.w, (kx0 + p + 1) << ppx);
+                        const int64_t cy0 = std::max(by0, (ky0 + q) << ppy);
+                        const int64_t cy1 = std::min(by0 + b.h, (ky0 + q + 1) << ppy);
+                        if (cx0 < cx1 && cy0 < cy1) {
+                            const int64_t fx = bx0 >> b.cbw_log2, fy = by0 >> b.cbh_log2;
+                            pb.i0 = (int)((cx0 >> b.cbw_log2) - fx);
+                            pb.i1 = (int)(((cx1 - 1) >> b.cbw_log2) + 1 - fx);
+                            pb.j0 = (int)((cy0 >> b.cbh_log2) - fy);
+                            pb.j1 = (int)(((cy1 - 1) >> b.cbh_log2) + 1 - fy);
+                            pb.incl = TagTree(pb.i1 - pb.i0, pb.j1 - pb.j0);
+                            pb.zbp = TagTree(pb.i1 - pb.i0, pb.j1 - pb.j0);
+                        }
+                        pb.incl.reset_decoder();
+                        pb.zbp.reset_decoder();
+                        pbs.push_back(std::move(pb));
+                    }
+                }
+        }
 
     // The tile-part bodies are read one after the other as one packet
     // sequence; a packet does not straddle two tile-parts.
@@ -1016,7 +1054,8 @@ static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Para
     size_t pos = parts.empty() ? len : parts[0].first;
     auto part_end = [&]() { return part_i < parts.size() ? parts[part_i].second : len; };
 
-    auto read_packet = [&](int layer, int r, int c) -> int {
+    // One packet (ISO B.9, B.10): layer, resolution, component, precinct.
+    auto read_packet = [&](int layer, int r, int c, int prec) -> int {
         while (part_i < parts.size() && pos >= parts[part_i].second) {
             part_i++;
             if (part_i < parts.size()) pos = parts[part_i].first;
@@ -1029,38 +1068,42 @@ static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Para
         BitReader br(cs, pos, pend);
         const int present = br.get();
         std::vector<std::pair<CblkState *, uint32_t>> contrib;
+        ResState &rs = st[c][r];
         if (present) {
             for (size_t bi = 0; bi < geo[r].bands.size(); bi++) {
                 const Band &b = geo[r].bands[bi];
-                BandState &bs = st[c][r][bi];
-                for (int i = 0; i < b.ncbx * b.ncby; i++) {
-                    CblkState &cb = bs.cb[i];
-                    int inc;
-                    if (!cb.included) inc = bs.incl.decode(br, i, layer + 1);
-                    else inc = br.get();
-                    if (br.overrun) { err = "packet header overrun"; return TC_E_CODESTREAM; }
-                    if (!inc) continue;
-                    if (!cb.included) {
-                        int k = 0;
-                        while (!bs.zbp.decode(br, i, k + 1)) {
-                            if (br.overrun || ++k > 64) { err = "bad zero bit-plane tag tree"; return TC_E_CODESTREAM; }
+                PrecBand &pb = rs.prec[prec][bi];
+                const int gw = pb.i1 - pb.i0;
+                for (int j = pb.j0; j < pb.j1; j++)
+                    for (int i = pb.i0; i < pb.i1; i++) {
+                        CblkState &cb = rs.cb[bi][(size_t)j * b.ncbx + i];
+                        const int leaf = (j - pb.j0) * gw + (i - pb.i0);
+                        int inc;
+                        if (!cb.included) inc = pb.incl.decode(br, leaf, layer + 1);
+                        else inc = br.get();
+                        if (br.overrun) { err = "packet header overrun"; return TC_E_CODESTREAM; }
+                        if (!inc) continue;
+                        if (!cb.included) {
+                            int k = 0;
+                            while (!pb.zbp.decode(br, leaf, k + 1)) {
+                                if (br.overrun || ++k > 64) { err = "bad zero bit-plane tag tree"; return TC_E_CODESTREAM; }
+                            }
+                            cb.zbp = k;
+                            cb.included = 1;
                         }
-                        cb.zbp = k;
-                        cb.included = 1;
+                        const int np = get_num_passes(br);
+                        int inc_l = 0;
+                        while (br.get()) {
+                            if (br.overrun || ++inc_l > 32) { err = "bad Lblock increment"; return TC_E_CODESTREAM; }
+                        }
+                        cb.lblock += inc_l;
+                        const int nbits = cb.lblock + floorlog2(np);
+                        if (nbits > 31) { err = "code-block length field too wide"; return TC_E_CODESTREAM; }
+                        const uint32_t Lc = br.get_bits(nbits);
+                        if (br.overrun) { err = "packet header overrun"; return TC_E_CODESTREAM; }
+                        cb.passes += np;
+                        contrib.emplace_back(&cb, Lc);
                     }
-                    const int np = get_num_passes(br);
-                    int inc_l = 0;
-                    while (br.get()) {
-                        if (br.overrun || ++inc_l > 32) { err = "bad Lblock increment"; return TC_E_CODESTREAM; }
-                    }
-                    cb.lblock += inc_l;
-                    const int nbits = cb.lblock + floorlog2(np);
-                    if (nbits > 31) { err = "code-block length field too wide"; return TC_E_CODESTREAM; }
-                    const uint32_t L = br.get_bits(nbits);
-                    if (br.overrun) { err = "packet header overrun"; return TC_E_CODESTREAM; }
-                    cb.passes += np;
-                    contrib.emplace_back(&cb, L);
-                }
             }
         }
         br.align();
@@ -1078,24 +1121,72 @@ static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Para
         return TC_OK;
     };
 
-    const int L = P.layers, R = P.levels + 1, C = P.ncomp;
-    auto run = [&](int a, int b2, int c2) { return read_packet(a, b2, c2); };
+    // Position-driven orders (ISO B.12.1.3-B.12.1.5) visit a precinct at the
+    // first reference-grid position it covers, stepping over the tile by the
+    // smallest precinct of any resolution.  All components share one
+    // precinct grid (no subsampling, one COD), so the test is per resolution.
+    int64_t dx = INT64_MAX, dy = INT64_MAX;
+    for (int r = 0; r <= NL; r++) {
+        dx = std::min<int64_t>(dx, (int64_t)1 << (P.ppx[r] + NL - r));
+        dy = std::min<int64_t>(dy, (int64_t)1 << (P.ppy[r] + NL - r));
+    }
+    // precinct of resolution r that starts at (x, y), or -1
+    auto prec_at = [&](int r, int64_t x, int64_t y) -> int {
+        const int sh = NL - r, px = P.ppx[r], py = P.ppy[r];
+        const ResState &rs = rgeo[r];
+        const int64_t mx = ((int64_t)1 << (px + sh)) - 1, my = ((int64_t)1 << (py + sh)) - 1;
+        const bool sx = !(x & mx) || (x == T.x0 && ((rs.rx0 << sh) & mx));
+        const bool sy = !(y & my) || (y == T.y0 && ((rs.ry0 << sh) & my));
+        if (!sx || !sy) return -1;
+        const int64_t kx = (((x + ((int64_t)1 << sh) - 1) >> sh) >> px) - (rs.rx0 >> px);
+        const int64_t ky = (((y + ((int64_t)1 << sh) - 1) >> sh) >> py) - (rs.ry0 >> py);
+        if (kx < 0 || ky < 0 || kx >= rs.pw || ky >= rs.ph) return -1;
+        return (int)(ky * rs.pw + kx);
+    };
+    auto next = [](int64_t v, int64_t step) { return (v / step + 1) * step; };
+    auto layers = [&](int r, int c, int prec) -> int {
+        for (int l = 0; l < L; l++)
+            if (int e = read_packet(l, r, c, prec)) return e;
+        return TC_OK;
+    };
     switch (P.prog) {
     case 0:  // LRCP
         for (int l = 0; l < L; l++) for (int r = 0; r < R; r++) for (int c = 0; c < C; c++)
-            if ((rc = run(l, r, c))) return rc;
+            for (int k = 0; k < rgeo[r].pw * rgeo[r].ph; k++)
+                if ((rc = read_packet(l, r, c, k))) return rc;
         break;
     case 1:  // RLCP
         for (int r = 0; r < R; r++) for (int l = 0; l < L; l++) for (int c = 0; c < C; c++)
-            if ((rc = run(l, r, c))) return rc;
+            for (int k = 0; k < rgeo[r].pw * rgeo[r].ph; k++)
+                if ((rc = read_packet(l, r, c, k))) return rc;
         break;
-    case 2:  // RPCL (one precinct per resolution)
-        for (int r = 0; r < R; r++) for (int c = 0; c < C; c++) for (int l = 0; l < L; l++)
-            if ((rc = run(l, r, c))) return rc;
+    case 2:  // RPCL
+        for (int r = 0; r < R; r++)
+            for (int64_t y = T.y0; y < T.y1; y = next(y, dy))
+                for (int64_t x = T.x0; x < T.x1; x = next(x, dx)) {
+                    const int k = prec_at(r, x, y);
+                    if (k >= 0)
+                        for (int c = 0; c < C; c++)
+                            if ((rc = layers(r, c, k))) return rc;
+                }
         break;
-    default:  // PCRL, CPRL (one precinct per resolution)
-        for (int c = 0; c < C; c++) for (int r = 0; r < R; r++) for (int l = 0; l < L; l++)
-            if ((rc = run(l, r, c))) return rc;
+    case 3:  // PCRL
+        for (int64_t y = T.y0; y < T.y1; y = next(y, dy))
+            for (int64_t x = T.x0; x < T.x1; x = next(x, dx))
+                for (int c = 0; c < C; c++)
+                    for (int r = 0; r < R; r++) {
+                        const int k = prec_at(r, x, y);
+                        if (k >= 0 && (rc = layers(r, c, k))) return rc;
+                    }
+        break;
+    default:  // CPRL
+        for (int c = 0; c < C; c++)
+            for (int64_t y = T.y0; y < T.y1; y = next(y, dy))
+                for (int64_t x = T.x0; x < T.x1; x = next(x, dx))
+                    for (int r = 0; r < R; r++) {
+                        const int k = prec_at(r, x, y);
+                        if (k >= 0 && (rc = layers(r, c, k))) return rc;
+                    }
         break;
     }
 
@@ -1106,11 +1197,11 @@ static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Para
         for (int r = 0; r < R; r++)
             for (size_t bi = 0; bi < geo[r].bands.size(); bi++) {
                 const Band &b = geo[r].bands[bi];
-                BandState &bs = st[c][r][bi];
+                std::vector<CblkState> &cbs = st[c][r].cb[bi];
                 const int cbw = 1 << b.cbw_log2, cbh = 1 << b.cbh_log2;
                 for (int j = 0; j < b.ncby; j++)
                     for (int i = 0; i < b.ncbx; i++) {
-                        CblkState &cb = bs.cb[j * b.ncbx + i];
+                        CblkState &cb = cbs[(size_t)j * b.ncbx + i];
                         tc_cblk_desc d;
                         std::memset(&d, 0, sizeof d);
                         const int cx = std::max(i * cbw - b.ox, 0), cy = std::max(j * cbh - b.oy, 0);
