@@ -25,6 +25,26 @@ __device__ __forceinline__ int mirror(int i, int n)
 // 9/7 lifting constants (ISO F.4.8.2).
 constexpr float kA = -1.586134342059924f, kB = -0.052980118572961f, kG = 0.882911075530934f,
                 kD = 0.443506852043971f, kK = 1.230174104914001f, kInvK = 1.0f / 1.230174104914001f;
+// Scaling-free reverse lifting: with E = X(2n)/K and O = X(2n+1)*K lifted in
+// place of the K-scaled samples of ISO F.3.8.2, the four steps become
+// E -= (delta/K^2)(O + O'), O -= (gamma K^2)(E + E'), E -= (beta/K^2)(..),
+// O -= (alpha K^2)(..), and a row-then-column level leaves each output off
+// by a factor of K^2 (even row and column), 1/K^2 (odd, odd) or 1.
+constexpr double kK2d = 1.230174104914001 * 1.230174104914001;
+constexpr float kSfD = (float)(0.443506852043971 / kK2d), kSfG = (float)(0.882911075530934 * kK2d),
+                kSfB = (float)(-0.052980118572961 / kK2d), kSfA = (float)(-1.586134342059924 * kK2d),
+                kSfEven = (float)kK2d, kSfOdd = (float)(1.0 / kK2d);
+
+// Combined output factor of the scaling-free row and column passes of a
+// 9/7 level, by the parity of the output row and column: K^2, 1, 1, 1/K^2
+// (a pass that did not run, over a single row or column, contributes 1).
+__device__ __forceinline__ float sf_factor(int row_odd, int col_odd, bool rows_lifted, bool cols_lifted)
+{
+    const float fc = rows_lifted ? (col_odd ? kInvK : kK) : 1.0f;
+    const float fr = cols_lifted ? (row_odd ? kInvK : kK) : 1.0f;
+    if (rows_lifted && cols_lifted) return row_odd == col_odd ? (row_odd ? kSfOdd : kSfEven) : 1.0f;
+    return fc * fr;
+}
 
 template <int RND>
 __device__ __forceinline__ int div4r(int v)

@@ -63,19 +63,17 @@ __device__ __forceinline__ void lift_reverse(T (&v)[N])
 #pragma unroll
         for (int k = 1; k <= N - 3; k += 2) v[k] += div2r<RND>(v[k - 1] + v[k + 1]);
     } else {
+        // scaling-free form: the K / 1/K factors of ISO F.3.8.2 steps 1-2
+        // are folded into the constants (E/K and O*K are lifted), and the
+        // caller applies the remaining per-parity factor once per output
 #pragma unroll
-        for (int k = 0; k < N; k += 2) {
-            v[k] *= kK;
-            v[k + 1] *= kInvK;
-        }
+        for (int k = 2; k <= N - 2; k += 2) v[k] = fmaf(-kSfD, v[k - 1] + v[k + 1], v[k]);
 #pragma unroll
-        for (int k = 2; k <= N - 2; k += 2) v[k] = fmaf(-kD, v[k - 1] + v[k + 1], v[k]);
+        for (int k = 1; k <= N - 3; k += 2) v[k] = fmaf(-kSfG, v[k - 1] + v[k + 1], v[k]);
 #pragma unroll
-        for (int k = 1; k <= N - 3; k += 2) v[k] = fmaf(-kG, v[k - 1] + v[k + 1], v[k]);
+        for (int k = 2; k <= N - 2; k += 2) v[k] = fmaf(-kSfB, v[k - 1] + v[k + 1], v[k]);
 #pragma unroll
-        for (int k = 2; k <= N - 2; k += 2) v[k] = fmaf(-kB, v[k - 1] + v[k + 1], v[k]);
-#pragma unroll
-        for (int k = 1; k <= N - 3; k += 2) v[k] = fmaf(-kA, v[k - 1] + v[k + 1], v[k]);
+        for (int k = 1; k <= N - 3; k += 2) v[k] = fmaf(-kSfA, v[k - 1] + v[k + 1], v[k]);
     }
 }
 
@@ -223,6 +221,12 @@ __device__ __forceinline__ void rev_tile(const LevelIO &io, int bits, int bx, in
 #pragma unroll
         for (int k = 0; k < VN; k++) v[k] = t[(vbase + k) * S + H + col];
         if (h > 1) lift_reverse<T, WAVELET, RND, VN>(v);
+        if constexpr (WAVELET == 1) {
+            // x0 and the first kept row are even: parities are col & 1, r & 1
+            const float fe = sf_factor(0, col & 1, w > 1, h > 1), fo = sf_factor(1, col & 1, w > 1, h > 1);
+#pragma unroll
+            for (int r = 0; r < OUTR; r++) v[H + r] *= (r & 1) ? fo : fe;
+        }
         if (x >= w) continue;
         const int y = y0 + obase;
         if constexpr (PLANE) {
@@ -396,6 +400,8 @@ cudaError_t launch_idwt_last_color(tc_ctx *ctx, const LevelIO &io, int wavelet, 
                                    bool)
 {
     if (io.w <= 0 || io.h <= 0) return cudaSuccess;
+    if (color != TC_COLOR_DC && io.ncomp < 3) color = TC_COLOR_DC;
+    if (wavelet && rev97_handles(color, io.ncomp, out_type)) return launch_rev97_level(ctx, io, out_type, bits);
     RevLaunch L;
     L.io = &io;
     return last_level(ctx, L, io.ncomp, wavelet, color, out_type, bits);
@@ -410,6 +416,9 @@ void rev_tile_shape(int wavelet, int *tx, int *ty)
 cudaError_t launch_idwt_batch(tc_ctx *ctx, const RevJob *d_jobs, int njobs, int ntiles, int wavelet, int rounding,
                               int color, int ncomp, int out_type, int bits)
 {
+    if (color >= 0 && color != TC_COLOR_DC && ncomp < 3) color = TC_COLOR_DC;
+    if (wavelet && rev97_handles(color, ncomp, out_type))
+        return launch_rev97_batch(ctx, d_jobs, njobs, ntiles, out_type, bits);
     RevLaunch L;
     L.jobs = d_jobs;
     L.njobs = njobs;

@@ -147,6 +147,13 @@ cudaError_t launch_idwt_batch(tc_ctx *ctx, const RevJob *d_jobs, int njobs, int 
                               int color, int ncomp, int out_type, int bits);
 cudaError_t launch_fdwt_level(tc_ctx *ctx, const LevelIO &io, int wavelet, int rounding);
 
+// Last reverse 9/7 level of a three-component image with the inverse ICT
+// fused in, packed fp32x2 lifting (dwt_rev97.cu).  rev97_handles says
+// whether a last level runs there (ICT, 3 components, 8- or 16-bit out).
+bool rev97_handles(int color, int ncomp, int out_type);
+cudaError_t launch_rev97_level(tc_ctx *ctx, const LevelIO &io, int out_type, int bits);
+cudaError_t launch_rev97_batch(tc_ctx *ctx, const RevJob *d_jobs, int njobs, int ntiles, int out_type, int bits);
+
 // Last reverse level fused with the inverse colour transform, DC shift,
 // rounding and clamping; writes out_type samples (TC_U8/TC_U16/TC_INT32).
 // color: TC_COLOR_DC / TC_COLOR_RCT / TC_COLOR_ICT.  levels == 0 means the
