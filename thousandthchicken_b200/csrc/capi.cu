@@ -229,6 +229,10 @@ struct tc_plan {
     DevBuf jobs;
     cudaEvent_t jobs_uploaded = nullptr;
     float recon_r = 0.5f;
+    // a single image's segment pool already uploaded from pinned memory
+    // (tc_decode_j2k): its host address and length
+    const void *preloaded = nullptr;
+    uint64_t preloaded_len = 0;
     int class_counts[3] = {0, 0, 0};  // Tier-1 blocks of <= 8, <= 16, <= 31 coded bit-planes
     bool profiling = false;
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
@@ -300,11 +304,13 @@ static int plan_build_parsed(tc_ctx *ctx, const Parsed *const *parsed, const uin
     uint8_t *hpool = static_cast<uint8_t *>(P->h_pool.ptr);
     tc_cblk_desc *hdesc = static_cast<tc_cblk_desc *>(P->h_desc.ptr);
     uint32_t *horder = static_cast<uint32_t *>(P->h_order.ptr);
+    const bool preloaded = n == 1 && P->preloaded && pools[0] == P->preloaded && pool_lens[0] == P->preloaded_len;
+    P->preloaded = nullptr;
     uint64_t po = 0;
     size_t nd = 0;
     for (int i = 0; i < n; i++) {
         const uint64_t pl = pool_lens[i];
-        if (pl) std::memcpy(hpool + po, pools[i], pl);
+        if (pl && !preloaded) std::memcpy(hpool + po, pools[i], pl);
         const uint64_t elem_base = P->imgs[i].coef_off / 4;
         for (tc_cblk_desc d : parsed[i]->desc) {
             d.seg_off += po;
@@ -326,7 +332,8 @@ static int plan_build_parsed(tc_ctx *ctx, const Parsed *const *parsed, const uin
         (e = P->scratch.ensure_on(std::max<size_t>(plan_batched(P) ? scratch_sum : scratch_max, 256), st, mp)) !=
             cudaSuccess)
         return cuda_status(ctx, e, "plan allocation");
-    if ((e = cudaMemcpyAsync(P->pool.ptr, hpool, pool_bytes, cudaMemcpyHostToDevice, ctx->stream)) ||
+    if ((!preloaded &&
+         (e = cudaMemcpyAsync(P->pool.ptr, hpool, pool_bytes, cudaMemcpyHostToDevice, ctx->stream))) ||
         (e = cudaMemcpyAsync(P->desc.ptr, hdesc, sizeof(tc_cblk_desc) * P->ncblk, cudaMemcpyHostToDevice,
                              ctx->stream)) ||
         (e = cudaMemcpyAsync(P->order.ptr, horder, sizeof(uint32_t) * P->ncblk, cudaMemcpyHostToDevice,
@@ -1119,6 +1126,25 @@ int tc_decode_j2k(tc_ctx *ctx, const uint8_t *h_cs, size_t len, void *h_out, siz
         ctx->stage_jobs = P.h_jobs;
         ctx->jobs_uploaded = P.jobs_uploaded;
     };
+    // A codestream in pinned memory is uploaded while it is parsed: the
+    // segment pool of a single-layer stream is the codestream itself (the
+    // plan re-uploads a gathered pool over it otherwise, in stream order).
+    cudaPointerAttributes pa;
+    if (cudaPointerGetAttributes(&pa, h_cs) == cudaSuccess && pa.type == cudaMemoryTypeHost) {
+        cudaMemPool_t mp = nullptr;
+        const size_t bytes = (len + 15) & ~size_t(15);  // the plan's pool size for this stream
+        cudaError_t e = ctx_mem_pool(ctx, &mp);
+        if (e == cudaSuccess) e = P.pool.ensure_on(bytes, ctx->stream, mp);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(P.pool.ptr, h_cs, len, cudaMemcpyHostToDevice, ctx->stream);
+        if (e != cudaSuccess) {
+            give_back();
+            return cuda_status(ctx, e, "tc_decode_j2k upload");
+        }
+        P.preloaded = h_cs;
+        P.preloaded_len = len;
+    } else {
+        cudaGetLastError();  // pageable memory: not an error
+    }
     const uint8_t *cs[1] = {h_cs};
     size_t lens[1] = {len};
     rc = plan_build(ctx, cs, lens, 1, &P);

@@ -656,6 +656,27 @@ struct TagTree {
         }
         return nodes[leaf].value < threshold;
     }
+    // Decodes the leaf's value outright (one walk from the root instead of
+    // one per threshold); -1 when the bits run out or the value passes limit.
+    int decode_value(BitReader &br, int leaf, int limit)
+    {
+        int stk[40], n;
+        path(leaf, stk, n);
+        int low = 0;
+        for (int i = n - 1; i >= 0; i--) {
+            Node &nd = nodes[stk[i]];
+            if (low > nd.low) nd.low = low;
+            else low = nd.low;
+            while (low < nd.value) {
+                if (low > limit) return -1;
+                if (br.get()) nd.value = low;
+                else low++;
+                if (br.overrun) return -1;
+            }
+            nd.low = low;
+        }
+        return nodes[leaf].value;
+    }
     void reset_decoder()
     {
         for (auto &n : nodes) {
@@ -935,12 +956,21 @@ static int assign_quant(const Params &P, std::vector<Resolution> &res, std::stri
 }
 
 namespace {
+// A code-block's codeword segments (one per layer that adds bytes) are a
+// list threaded through the tile's segment arena.
+struct SegNode {
+    size_t off;    // in the codestream
+    uint32_t len;
+    int next;
+};
+
 struct CblkState {
     int included = 0;
     int lblock = 3;
     int zbp = 0;
     int passes = 0;
-    std::vector<std::pair<size_t, uint32_t>> segs;  // (offset in cs, length)
+    int head = -1, tail = -1, nseg = 0;  // segment list in the tile's arena
+    uint64_t bytes = 0;
 };
 
 // Descriptors of all tiles before their segments are placed: each entry's
@@ -1054,6 +1084,8 @@ static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Para
     size_t pos = parts.empty() ? len : parts[0].first;
     auto part_end = [&]() { return part_i < parts.size() ? parts[part_i].second : len; };
 
+    std::vector<SegNode> arena;
+    std::vector<std::pair<CblkState *, uint32_t>> contrib;  // one packet's blocks and lengths
     // One packet (ISO B.9, B.10): layer, resolution, component, precinct.
     auto read_packet = [&](int layer, int r, int c, int prec) -> int {
         while (part_i < parts.size() && pos >= parts[part_i].second) {
@@ -1067,7 +1099,7 @@ static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Para
         }
         BitReader br(cs, pos, pend);
         const int present = br.get();
-        std::vector<std::pair<CblkState *, uint32_t>> contrib;
+        contrib.clear();
         ResState &rs = st[c][r];
         if (present) {
             for (size_t bi = 0; bi < geo[r].bands.size(); bi++) {
@@ -1084,10 +1116,8 @@ static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Para
                         if (br.overrun) { err = "packet header overrun"; return TC_E_CODESTREAM; }
                         if (!inc) continue;
                         if (!cb.included) {
-                            int k = 0;
-                            while (!pb.zbp.decode(br, leaf, k + 1)) {
-                                if (br.overrun || ++k > 64) { err = "bad zero bit-plane tag tree"; return TC_E_CODESTREAM; }
-                            }
+                            const int k = pb.zbp.decode_value(br, leaf, 64);
+                            if (k < 0) { err = "bad zero bit-plane tag tree"; return TC_E_CODESTREAM; }
                             cb.zbp = k;
                             cb.included = 1;
                         }
@@ -1115,7 +1145,16 @@ static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Para
         }
         for (auto &cl : contrib) {
             if (pos + cl.second > pend) { err = "code-block data runs past the tile-part"; return TC_E_CODESTREAM; }
-            if (cl.second) cl.first->segs.emplace_back(pos, cl.second);
+            if (cl.second) {
+                CblkState &cb = *cl.first;
+                const int k = (int)arena.size();
+                arena.push_back(SegNode{pos, cl.second, -1});
+                if (cb.tail >= 0) arena[cb.tail].next = k;
+                else cb.head = k;
+                cb.tail = k;
+                cb.nseg++;
+                cb.bytes += cl.second;
+            }
             pos += cl.second;
         }
         return TC_OK;
@@ -1193,6 +1232,14 @@ static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Para
     // Descriptors, component by component; segments are placed once every
     // tile is read (parse_raw_codestream).
     const uint64_t plane = (uint64_t)tw * th;
+    {
+        size_t nb = 0;
+        for (int r = 0; r < R; r++)
+            for (const Band &b : geo[r].bands) nb += (size_t)b.ncbx * b.ncby;
+        out.desc.reserve(out.desc.size() + nb * C);
+        em.first.reserve(em.first.size() + nb * C + 1);
+        em.segs.reserve(em.segs.size() + arena.size());
+    }
     for (int c = 0; c < C; c++)
         for (int r = 0; r < R; r++)
             for (size_t bi = 0; bi < geo[r].bands.size(); bi++) {
@@ -1223,12 +1270,11 @@ static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Para
                             }
                             d.zero_bitplanes = (uint8_t)cb.zbp;
                             d.passes = (uint8_t)cb.passes;
-                            uint64_t total = 0;
-                            for (auto &s : cb.segs) total += s.second;
-                            if (total > 0xFFFFFFFFull) { err = "code-block data too long"; return TC_E_CODESTREAM; }
-                            d.seg_len = (uint32_t)total;
-                            if (cb.segs.size() > 1) em.multi = true;
-                            em.segs.insert(em.segs.end(), cb.segs.begin(), cb.segs.end());
+                            if (cb.bytes > 0xFFFFFFFFull) { err = "code-block data too long"; return TC_E_CODESTREAM; }
+                            d.seg_len = (uint32_t)cb.bytes;
+                            if (cb.nseg > 1) em.multi = true;
+                            for (int k = cb.head; k >= 0; k = arena[k].next)
+                                em.segs.emplace_back(arena[k].off, arena[k].len);
                         } else {
                             d.zero_bitplanes = (uint8_t)b.mb;
                             d.passes = 0;

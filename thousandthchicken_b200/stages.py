@@ -320,9 +320,16 @@ class Decoder:
         self.ctx = ctx or Context()
 
     def decode(self, cs, out: np.ndarray | None = None):
+        """cs: bytes, a path, or a uint8 array (read in place: a codestream in
+        pinned memory is uploaded while it is parsed).  out: optional
+        [ncomp, height, width] array to fill (pinned memory gives the fastest
+        read-back)."""
         if isinstance(cs, (str, Path)):
             cs = Path(cs).read_bytes()
-        buf = np.frombuffer(bytes(cs), np.uint8)
+        if isinstance(cs, np.ndarray):
+            buf = np.ascontiguousarray(cs.reshape(-1).view(np.uint8))
+        else:
+            buf = np.frombuffer(cs, np.uint8)
         hdr = L.ImageInfo()
         self.ctx.check(L.lib().tc_j2k_read_header(buf.ctypes.data, buf.size, C.byref(hdr)), "tc_j2k_read_header")
         dt = np.uint8 if hdr.bits <= 8 else np.uint16
