@@ -209,9 +209,12 @@ int tc_color_forward(tc_ctx *ctx, int kind, int ncomp,
 
 /* ---- codestream parsing (the Tier-2 hand-off) ---------------------------- */
 
+/* Image information from the main header.  Components share size, depth,
+ * decomposition levels and wavelet; their code-block sizes and steps may
+ * differ (COC / QCC, main or tile-part header), and cblk_w/cblk_h,
+ * guard_bits and quant_style report the COD / QCD values. */
 typedef struct tc_image_info {
-    int32_t width, height, ncomp, bits;    /* all components share size/depth;
-                                              width/height: Xsiz-XOsiz, Ysiz-YOsiz */
+    int32_t width, height, ncomp, bits;    /* width/height: Xsiz-XOsiz, Ysiz-YOsiz */
     int32_t is_signed;
     int32_t levels;                        /* decomposition levels NL */
     int32_t reversible;                    /* 1 = 5/3, 0 = 9/7 */
@@ -333,10 +336,16 @@ typedef struct tc_encode_params {
     int32_t progression;   /* 0 = LRCP, 1 = RLCP */
     int32_t threads;       /* <= 0: all cores */
     int32_t reserved;
+    /* Per-component overrides (0: the values above), written as COC and QCC
+     * marker segments: the code-block size exponent and a multiplier of the
+     * irreversible step. */
+    int32_t comp_cblk_log2[4];
+    double  comp_step_scale[4];
 } tc_encode_params;
 
 /* Encode planar unsigned samples (TC_U8 when bits <= 8, else TC_U16) into a
- * single-tile, single-layer codestream with all coding passes. */
+ * single-tile, single-layer codestream with all coding passes (a harness
+ * encoder: the reference has none). */
 int tc_encode_j2k(const tc_encode_params *p, const void *h_planes,
                   uint8_t *h_out, size_t cap, size_t *out_len);
 

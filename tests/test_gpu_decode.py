@@ -6,7 +6,7 @@ import pytest
 
 import oracle as O
 from conftest import golden_cases, load_golden, synth_image
-from test_host_codec import PRECINCTS, TILED
+from test_host_codec import COC_QCC, PRECINCTS, TILED
 from thousandthchicken_b200 import codec
 
 pytestmark = pytest.mark.gpu
@@ -291,3 +291,23 @@ def test_precinct_streams_decode(gpu_ctx, kw):
         assert (d > 0).mean() < 0.005
     else:
         np.testing.assert_array_equal(got, img)
+
+
+@pytest.mark.parametrize("kw", COC_QCC, ids=["coc-rev", "qcc-irr", "coc-qcc-irr"])
+def test_coc_qcc_streams_decode(gpu_ctx, kw):
+    """Per-component code-block sizes and steps (COC / QCC, in the main or
+    the tile-part header) through the GPU: lossless equals the original,
+    lossy within 1 LSB of the oracle."""
+    from gpu_helpers import oracle_decode_tiled
+    from test_host_codec import _move_to_tile_header
+    img = synth_image(300, 200, 3, 8, seed=5)
+    cs = codec.encode(img, 8, levels=4, **kw)
+    for s in (cs, _move_to_tile_header(cs)):
+        got = _decoder(gpu_ctx).decode(s).astype(np.int64)
+        if kw["reversible"]:
+            np.testing.assert_array_equal(got, img)
+        else:
+            _, want = oracle_decode_tiled(s)
+            d = np.abs(got - want.astype(np.int64))
+            assert d.max() <= 1
+            assert (d > 0).mean() < 0.005

@@ -271,3 +271,78 @@ def test_precinct_streams_through_oracle(kw):
         assert np.abs(out.astype(np.int64) - openjpeg_decode(cs)).max() <= 1
     else:
         np.testing.assert_array_equal(out, img)
+
+
+def _main_header_markers(cs):
+    """(marker, offset, length) of the main header's marker segments."""
+    out, pos = [], 2
+    while True:
+        m = int.from_bytes(cs[pos:pos + 2], "big")
+        if m == 0xFF90:
+            return out, pos
+        n = int.from_bytes(cs[pos + 2:pos + 4], "big")
+        out.append((m, pos, n + 2))
+        pos += n + 2
+
+
+def _move_to_tile_header(cs, markers=(0xFF53, 0xFF5D)):
+    """The same codestream with the main header's COC/QCC segments moved
+    into the single tile-part's header (Psot grown to match)."""
+    segs, sot = _main_header_markers(cs)
+    moved = b"".join(cs[o:o + n] for m, o, n in segs if m in markers)
+    main = cs[:2] + b"".join(cs[o:o + n] for m, o, n in segs if m not in markers)
+    psot = int.from_bytes(cs[sot + 6:sot + 10], "big")
+    sot_seg = bytearray(cs[sot:sot + 12])
+    sot_seg[6:10] = (psot + len(moved)).to_bytes(4, "big")
+    return main + bytes(sot_seg) + moved + cs[sot + 12:]
+
+
+COC_QCC = [  # harness-encoder options written as COC / QCC marker segments
+    dict(reversible=True, comp_cblk_log2=[0, 4, 5]),
+    dict(reversible=False, comp_step_scale=[1, 4, 0.5]),
+    dict(reversible=False, comp_cblk_log2=[5, 0, 3], comp_step_scale=[0, 2, 2]),
+]
+
+
+@pytest.mark.parametrize("kw", COC_QCC, ids=["coc-rev", "qcc-irr", "coc-qcc-irr"])
+def test_coc_qcc_streams_through_oracle(kw):
+    """Per-component code-block sizes (COC) and step sizes (QCC), in the main
+    header and moved into the tile-part header (ISO A.6 precedence: tile
+    COC/QCC > tile COD/QCD > main COC/QCC > main COD/QCD).  The reference
+    reads COD/QCD only and stubs COC/QCC (codestream.c:137-140).  OpenJPEG
+    decodes the same streams; lossless equals the original, lossy agrees
+    with OpenJPEG within 1 LSB."""
+    pytest.importorskip("PIL.Image")
+    from gpu_helpers import oracle_decode_tiled, openjpeg_decode
+    img = synth_image(300, 200, 3, 8, seed=5)
+    cs = codec.encode(img, 8, levels=4, **kw)
+    segs, _ = _main_header_markers(cs)
+    kinds = {m for m, _, _ in segs}
+    assert (0xFF53 in kinds) == bool(kw.get("comp_cblk_log2"))
+    assert (0xFF5D in kinds) == bool(kw.get("comp_step_scale"))
+    info, out = oracle_decode_tiled(cs)
+    if kw["reversible"]:
+        np.testing.assert_array_equal(out, img)
+    else:
+        assert np.abs(out.astype(np.int64) - openjpeg_decode(cs)).max() <= 1
+    moved = _move_to_tile_header(cs)
+    assert moved != cs and len(moved) == len(cs)
+    info2, out2 = oracle_decode_tiled(moved)
+    np.testing.assert_array_equal(out2, out)
+    _, d1, _ = codec.parse(cs)
+    _, d2, _ = codec.parse(moved)
+    for f in ("w", "h", "mb", "zero_bitplanes", "passes", "step", "out_off", "seg_len"):
+        np.testing.assert_array_equal(d1[f], d2[f])
+
+
+def test_component_levels_must_agree():
+    """A COC that changes a component's decomposition levels is refused as
+    unsupported (the fused colour level needs one geometry per image)."""
+    img = synth_image(64, 48, 3, 8, seed=6)
+    cs = bytearray(codec.encode(img, 8, levels=3, reversible=True, comp_cblk_log2=[0, 5, 0]))
+    segs, _ = _main_header_markers(bytes(cs))
+    (_, off, _), = [s for s in segs if s[0] == 0xFF53]
+    cs[off + 6] = 2  # SPcoc levels: 3 -> 2
+    with pytest.raises(TCError) as ei:
+        codec.parse(bytes(cs))
+    assert ei.value.status == TC_E_UNSUPPORTED

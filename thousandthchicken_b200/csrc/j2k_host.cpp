@@ -746,26 +746,174 @@ struct Reader {
     uint32_t u32() { uint32_t a = u16(); return (a << 16) | u16(); }
 };
 
-// Main-header coding parameters (COD/QCD), shared by all components.
+// Coding style of a component: SPcod of COD, SPcoc of COC (ISO A.6.1-A.6.2).
+struct Coding {
+    int levels = 0, xcb = 6, ycb = 6, cblk_style = 0, reversible = 1;
+    std::vector<int> ppx, ppy;  // precinct size exponents per resolution
+};
+
+// Quantisation of a component: QCD or QCC (ISO A.6.4-A.6.5).
+struct Quant {
+    int qstyle = 0, guard = 2;
+    std::vector<int> eps, mu;  // as signalled (1 or 3N+1 entries)
+};
+
+// The coding parameters one header sets: the main header, or a tile's first
+// tile-part header.  Per component, a COC / QCC replaces the header's COD /
+// QCD.
+struct Scope {
+    bool has_cod = false, has_qcd = false;
+    int scod = 0, prog = 0, layers = 1, mct = 0;
+    Coding cod;
+    Quant qcd;
+    std::vector<char> has_coc, has_qcc;
+    std::vector<Coding> coc;
+    std::vector<Quant> qcc;
+    void init(int ncomp)
+    {
+        has_coc.assign(ncomp, 0);
+        has_qcc.assign(ncomp, 0);
+        coc.resize(ncomp);
+        qcc.resize(ncomp);
+    }
+};
+
 struct Params {
     int width = 0, height = 0, ncomp = 0, bits = 0, is_signed = 0;
     // reference grid (ISO B.2): image [xo, xs) x [yo, ys); tiles of tw x th
     // anchored at (xto, yto)
     int64_t xs = 0, ys = 0, xo = 0, yo = 0, xto = 0, yto = 0;
     int tw = 0, th = 0;
-    int scod = 0, prog = 0, layers = 1, mct = 0;
-    int levels = 0, xcb = 6, ycb = 6, cblk_style = 0, reversible = 1;
-    std::vector<int> ppx, ppy;
-    int qstyle = 0, guard = 2;
-    std::vector<int> q_eps, q_mu;  // as signalled (1 or 3N+1 entries)
-    bool have_siz = false, have_cod = false, have_qcd = false;
+    Scope main;
+    int levels = 0;  // decomposition levels, shared by every component and tile
+    bool have_siz = false;
     // tiles in raster order, on the reference grid: [x0, x1) x [y0, y1)
     struct Tile {
         int64_t x0, y0, x1, y1;
     };
     std::vector<Tile> tiles;
 };
+
+// Precedence of ISO A.6: tile COC > tile COD > main COC > main COD, and
+// likewise for QCC / QCD.  t: the tile's header scope, or null.
+const Coding &coding_of(const Params &P, const Scope *t, int c)
+{
+    if (t && t->has_coc[c]) return t->coc[c];
+    if (t && t->has_cod) return t->cod;
+    if (P.main.has_coc[c]) return P.main.coc[c];
+    return P.main.cod;
+}
+
+const Quant &quant_of(const Params &P, const Scope *t, int c)
+{
+    if (t && t->has_qcc[c]) return t->qcc[c];
+    if (t && t->has_qcd) return t->qcd;
+    if (P.main.has_qcc[c]) return P.main.qcc[c];
+    return P.main.qcd;
+}
+
+// Progression, layers, SOP/EPH and the colour transform come from COD only.
+const Scope &cod_scope(const Params &P, const Scope *t) { return t && t->has_cod ? *t : P.main; }
 }  // namespace
+
+// SPcod / SPcoc: levels, code-block size and style, wavelet, precincts.
+static int read_spcod(Reader &rd, bool precincts, Coding &c, std::string &err)
+{
+    c.levels = (int)rd.u8();
+    c.xcb = (int)rd.u8() + 2;
+    c.ycb = (int)rd.u8() + 2;
+    c.cblk_style = (int)rd.u8();
+    c.reversible = (int)rd.u8();
+    if (c.levels > 32 || c.xcb > 10 || c.ycb > 10 || c.xcb + c.ycb > 12) { err = "bad COD/COC"; return TC_E_CODESTREAM; }
+    if (c.xcb > 6 || c.ycb > 6) { err = "code-blocks larger than 64x64"; return TC_E_UNSUPPORTED; }
+    if (c.cblk_style != 0) { err = "code-block style flags are not supported"; return TC_E_UNSUPPORTED; }
+    if (c.reversible > 1) { err = "unknown wavelet"; return TC_E_CODESTREAM; }
+    c.ppx.assign(c.levels + 1, 15);
+    c.ppy.assign(c.levels + 1, 15);
+    if (precincts)
+        for (int r = 0; r <= c.levels; r++) {
+            const uint32_t v = rd.u8();
+            c.ppx[r] = (int)(v & 0xF);
+            c.ppy[r] = (int)(v >> 4);
+        }
+    return TC_OK;
+}
+
+// Sqcd / Sqcc and the step sizes up to the end of the marker segment.
+static int read_quant(Reader &rd, size_t seg_end, Quant &q, std::string &err)
+{
+    const uint32_t s = rd.u8();
+    q.qstyle = (int)(s & 0x1F);
+    q.guard = (int)(s >> 5);
+    q.eps.clear();
+    q.mu.clear();
+    if (q.qstyle == 0) {
+        while (rd.pos < seg_end) q.eps.push_back((int)(rd.u8() >> 3)), q.mu.push_back(0);
+    } else if (q.qstyle == 1 || q.qstyle == 2) {
+        while (rd.pos + 1 < seg_end) {
+            const uint32_t v = rd.u16();
+            q.eps.push_back((int)(v >> 11));
+            q.mu.push_back((int)(v & 0x7FF));
+        }
+    } else {
+        err = "bad quantisation style";
+        return TC_E_CODESTREAM;
+    }
+    return TC_OK;
+}
+
+// COD, COC, QCD and QCC of a main or tile-part header into scope S.  The
+// reference's parser reads COD and QCD (read_cod_marker, read_qcd_marker,
+// codestream.c:95-230) and leaves COC/QCC as a stub (codestream.c:137-140).
+static int read_coding_marker(Reader &rd, uint32_t m, size_t seg_end, int ncomp, Scope &S, std::string &err)
+{
+    int rc;
+    if (m == M_COD) {
+        S.scod = (int)rd.u8();
+        S.prog = (int)rd.u8();
+        S.layers = (int)rd.u16();
+        S.mct = (int)rd.u8();
+        if (S.prog > 4 || S.layers < 1) { err = "bad progression or layer count"; return TC_E_CODESTREAM; }
+        if ((rc = read_spcod(rd, S.scod & 1, S.cod, err))) return rc;
+        S.has_cod = true;
+    } else if (m == M_QCD) {
+        if ((rc = read_quant(rd, seg_end, S.qcd, err))) return rc;
+        S.has_qcd = true;
+    } else {
+        const int c = (int)(ncomp < 257 ? rd.u8() : rd.u16());
+        if (c >= ncomp) { err = "COC/QCC for a component that does not exist"; return TC_E_CODESTREAM; }
+        if (m == M_COC) {
+            const int scoc = (int)rd.u8();
+            if ((rc = read_spcod(rd, scoc & 1, S.coc[c], err))) return rc;
+            S.has_coc[c] = 1;
+        } else {
+            if ((rc = read_quant(rd, seg_end, S.qcc[c], err))) return rc;
+            S.has_qcc[c] = 1;
+        }
+    }
+    if (rd.bad || rd.pos > seg_end) { err = "truncated coding marker"; return TC_E_CODESTREAM; }
+    return TC_OK;
+}
+
+// Every component of the image (t null) or of a tile must share the
+// decomposition levels and the wavelet, and every tile the colour transform:
+// the DWT launches and the fused colour stage need one geometry per image.
+static int check_coding(const Params &P, const Scope *t, std::string &err)
+{
+    const Coding &c0 = P.main.cod;
+    for (int c = 0; c < P.ncomp; c++) {
+        const Coding &k = coding_of(P, t, c);
+        if (k.levels != c0.levels || k.reversible != c0.reversible) {
+            err = "components or tiles with different decomposition levels or wavelets are not supported";
+            return TC_E_UNSUPPORTED;
+        }
+    }
+    if (cod_scope(P, t).mct != P.main.mct) {
+        err = "tiles with different colour transforms are not supported";
+        return TC_E_UNSUPPORTED;
+    }
+    return TC_OK;
+}
 
 // Tile grid (ISO B.3): tile (p, q) covers [max(XTOsiz + p*XTsiz, XOsiz),
 // min(XTOsiz + (p+1)*XTsiz, Xsiz)) horizontally, likewise vertically, as
@@ -834,68 +982,37 @@ static int parse_main(Reader &rd, Params &P, std::string &err)
             }
             if (P.bits > 16) { err = "bit depth above 16"; return TC_E_UNSUPPORTED; }
             if (P.is_signed) { err = "signed samples are not supported"; return TC_E_UNSUPPORTED; }
+            P.main.init(P.ncomp);
             P.have_siz = true;
             break;
         }
-        case M_COD: {
-            P.scod = (int)rd.u8();
-            P.prog = (int)rd.u8();
-            P.layers = (int)rd.u16();
-            P.mct = (int)rd.u8();
-            P.levels = (int)rd.u8();
-            P.xcb = (int)rd.u8() + 2;
-            P.ycb = (int)rd.u8() + 2;
-            P.cblk_style = (int)rd.u8();
-            P.reversible = (int)rd.u8();
-            if (P.levels > 32 || P.xcb > 10 || P.ycb > 10 || P.xcb + P.ycb > 12) { err = "bad COD"; return TC_E_CODESTREAM; }
-            if (P.xcb > 6 || P.ycb > 6) { err = "code-blocks larger than 64x64"; return TC_E_UNSUPPORTED; }
-            if (P.cblk_style != 0) { err = "code-block style flags are not supported"; return TC_E_UNSUPPORTED; }
-            if (P.prog > 4 || P.layers < 1) { err = "bad progression or layer count"; return TC_E_CODESTREAM; }
-            if (P.reversible > 1) { err = "unknown wavelet"; return TC_E_CODESTREAM; }
-            P.ppx.assign(P.levels + 1, 15);
-            P.ppy.assign(P.levels + 1, 15);
-            if (P.scod & 1)
-                for (int r = 0; r <= P.levels; r++) {
-                    const uint32_t v = rd.u8();
-                    P.ppx[r] = (int)(v & 0xF);
-                    P.ppy[r] = (int)(v >> 4);
-                }
-            P.have_cod = true;
+        case M_COD: case M_COC: case M_QCD: case M_QCC: {
+            if (!P.have_siz) { err = "coding marker before SIZ"; return TC_E_CODESTREAM; }
+            const int rc = read_coding_marker(rd, m, seg_end, P.ncomp, P.main, err);
+            if (rc) return rc;
             break;
         }
-        case M_QCD: {
-            const uint32_t s = rd.u8();
-            P.qstyle = (int)(s & 0x1F);
-            P.guard = (int)(s >> 5);
-            P.q_eps.clear();
-            P.q_mu.clear();
-            if (P.qstyle == 0) {
-                while (rd.pos < seg_end) P.q_eps.push_back((int)(rd.u8() >> 3)), P.q_mu.push_back(0);
-            } else if (P.qstyle == 1 || P.qstyle == 2) {
-                while (rd.pos + 1 < seg_end) {
-                    const uint32_t v = rd.u16();
-                    P.q_eps.push_back((int)(v >> 11));
-                    P.q_mu.push_back((int)(v & 0x7FF));
-                }
-            } else {
-                err = "bad quantisation style";
-                return TC_E_CODESTREAM;
-            }
-            P.have_qcd = true;
-            break;
-        }
-        case M_COC: case M_QCC: case M_RGN: case M_POC: case M_PPM: case M_CRG:
-            err = "COC/QCC/RGN/POC/PPM/CRG markers are not supported";
+        case M_RGN: case M_POC: case M_PPM: case M_CRG:
+            err = "RGN/POC/PPM/CRG markers are not supported";
             return TC_E_UNSUPPORTED;
         default:
             break;  // COM, TLM, PLM and others carry nothing we need
         }
         rd.pos = seg_end;
     }
-    if (!P.have_siz || !P.have_cod || !P.have_qcd) { err = "main header lacks SIZ, COD or QCD"; return TC_E_CODESTREAM; }
+    if (!P.have_siz || !P.main.has_cod || !P.main.has_qcd) {
+        err = "main header lacks SIZ, COD or QCD";
+        return TC_E_CODESTREAM;
+    }
+    P.levels = P.main.cod.levels;
+    const int rc = check_coding(P, nullptr, err);
+    if (rc) return rc;
     return tile_grid(P, err);
 }
 
+// Image information from the main header (COD and QCD; per-component COC /
+// QCC values and tile-part headers may differ in code-block size and
+// quantisation).
 static void fill_info(const Params &P, tc_image_info &info)
 {
     std::memset(&info, 0, sizeof info);
@@ -905,14 +1022,14 @@ static void fill_info(const Params &P, tc_image_info &info)
     info.bits = P.bits;
     info.is_signed = P.is_signed;
     info.levels = P.levels;
-    info.reversible = P.reversible;
-    info.mct = P.mct;
-    info.cblk_w = 1 << P.xcb;
-    info.cblk_h = 1 << P.ycb;
-    info.layers = P.layers;
-    info.progression = P.prog;
-    info.guard_bits = P.guard;
-    info.quant_style = P.qstyle;
+    info.reversible = P.main.cod.reversible;
+    info.mct = P.main.mct;
+    info.cblk_w = 1 << P.main.cod.xcb;
+    info.cblk_h = 1 << P.main.cod.ycb;
+    info.layers = P.main.layers;
+    info.progression = P.main.prog;
+    info.guard_bits = P.main.qcd.guard;
+    info.quant_style = P.main.qcd.qstyle;
     info.ntiles = (uint32_t)P.tiles.size();
 }
 
@@ -928,28 +1045,28 @@ static int read_raw_header(const uint8_t *cs, size_t len, tc_image_info &info, s
 
 // Quantisation parameters per band (ISO A.6.4-A.6.5, E.1).  Derived style
 // restates read_qcd_marker (codestream.c:142-230) with ISO's exponent rule.
-static int assign_quant(const Params &P, std::vector<Resolution> &res, std::string &err)
+static int assign_quant(const Quant &Q, int bits, int levels, std::vector<Resolution> &res, std::string &err)
 {
     int bi = 0;
-    for (int r = 0; r <= P.levels; r++)
+    for (int r = 0; r <= levels; r++)
         for (Band &b : res[r].bands) {
             int eps, mu;
-            if (P.qstyle == 1) {
-                if (P.q_eps.empty()) { err = "empty QCD"; return TC_E_CODESTREAM; }
-                eps = P.q_eps[0] - P.levels + b.level;
-                mu = P.q_mu[0];
+            if (Q.qstyle == 1) {
+                if (Q.eps.empty()) { err = "empty QCD/QCC"; return TC_E_CODESTREAM; }
+                eps = Q.eps[0] - levels + b.level;
+                mu = Q.mu[0];
                 if (eps < 0) eps = 0;
             } else {
-                if (bi >= (int)P.q_eps.size()) { err = "QCD has too few subbands"; return TC_E_CODESTREAM; }
-                eps = P.q_eps[bi];
-                mu = P.q_mu[bi];
+                if (bi >= (int)Q.eps.size()) { err = "QCD/QCC has too few subbands"; return TC_E_CODESTREAM; }
+                eps = Q.eps[bi];
+                mu = Q.mu[bi];
             }
             bi++;
             b.eps = eps;
             b.mu = mu;
-            b.mb = P.guard + eps - 1;
+            b.mb = Q.guard + eps - 1;
             if (b.mb > 31) { err = "more than 31 magnitude bit-planes"; return TC_E_UNSUPPORTED; }
-            const int rb = P.bits + band_gain_log2(b.orient);
+            const int rb = bits + band_gain_log2(b.orient);
             b.step = (float)std::ldexp(1.0 + mu / 2048.0, rb - eps);
         }
     return TC_OK;
@@ -988,18 +1105,16 @@ struct Emit {
 // Follows decode_tiles / decode_packet_header / decode_packet_body
 // (codestream.c:336-510), one call per tile as decode_codestream loops over
 // the tiles (codestream.c:524-527).
-static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Params::Tile &T,
+static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Params::Tile &T, const Scope &ts,
                       const std::vector<std::pair<size_t, size_t>> &parts, uint64_t coef_off, Parsed &out,
                       Emit &em, std::string &err)
 {
     int rc;
+    if ((rc = check_coding(P, &ts, err))) return rc;
     const int tw = (int)(T.x1 - T.x0), th = (int)(T.y1 - T.y0);
-    const int NL = P.levels, R = NL + 1, C = P.ncomp, L = P.layers;
-    // With the tile origin a multiple of 2^levels, the subband sizes are
-    // those of a tw x th image at the origin; the code-block and precinct
-    // grids, anchored at the reference grid's origin, depend on where the
-    // tile is.
-    std::vector<Resolution> geo = make_geometry(tw, th, NL, P.xcb, P.ycb);
+    const Scope &cs_ = cod_scope(P, &ts);
+    const int NL = P.levels, R = NL + 1, C = P.ncomp, L = cs_.layers, scod = cs_.scod, prog = cs_.prog;
+    const bool reversible = P.main.cod.reversible != 0;
 
     // Precinct partition of each resolution (ISO B.6): 2^PPx x 2^PPy cells
     // of the resolution's grid; in a subband of resolution r > 0 the cells
@@ -1010,51 +1125,55 @@ static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Para
     };
     struct ResState {
         int64_t rx0 = 0, ry0 = 0;  // the resolution's origin on its own grid
+        int px = 15, py = 15;      // precinct size exponents
         int pw = 0, ph = 0;        // precincts across and down
         std::vector<std::vector<CblkState>> cb;   // per band: its code-blocks
         std::vector<std::vector<PrecBand>> prec;  // per precinct: per band
     };
-    std::vector<ResState> rgeo(R);
+    // Per component (its own code-block and precinct sizes and quantisation,
+    // COC / QCC): subband geometry, then per resolution the code-block
+    // states of each band and per precinct each band's block range and tag
+    // trees.  With the tile origin a multiple of 2^levels the subband sizes
+    // are those of a tw x th image at the origin; the code-block and
+    // precinct grids, anchored at the reference grid's origin, depend on
+    // where the tile is.
+    std::vector<std::vector<Resolution>> geo(C);
+    std::vector<std::vector<ResState>> st(C, std::vector<ResState>(R));
     int64_t nprec_bands = 0;
-    for (int r = 0; r <= NL; r++) {
-        const int px = P.ppx[r], py = P.ppy[r];
-        const int xcb = std::min(P.xcb, r ? px - 1 : px), ycb = std::min(P.ycb, r ? py - 1 : py);
-        if (xcb < 0 || ycb < 0) { err = "bad precinct size"; return TC_E_CODESTREAM; }
-        const int sh = NL - r;
-        const int64_t rx0 = (T.x0 + ((int64_t)1 << sh) - 1) >> sh, ry0 = (T.y0 + ((int64_t)1 << sh) - 1) >> sh;
-        const int64_t rx1 = (T.x1 + ((int64_t)1 << sh) - 1) >> sh, ry1 = (T.y1 + ((int64_t)1 << sh) - 1) >> sh;
-        ResState &rs = rgeo[r];
-        rs.rx0 = rx0;
-        rs.ry0 = ry0;
-        rs.pw = (int)(((rx1 + ((int64_t)1 << px) - 1) >> px) - (rx0 >> px));
-        rs.ph = (int)(((ry1 + ((int64_t)1 << py) - 1) >> py) - (ry0 >> py));
-        nprec_bands += (int64_t)rs.pw * rs.ph * (int64_t)geo[r].bands.size();
-        if (nprec_bands > (1 << 22)) { err = "too many precincts"; return TC_E_UNSUPPORTED; }
-        for (Band &b : geo[r].bands) {
-            b.cbw_log2 = xcb;
-            b.cbh_log2 = ycb;
-            b.ox = (int)((T.x0 >> b.level) & ((1 << xcb) - 1));
-            b.oy = (int)((T.y0 >> b.level) & ((1 << ycb) - 1));
-            b.ncbx = b.w > 0 ? ceil_div(b.ox + b.w, 1 << xcb) : 0;
-            b.ncby = b.h > 0 ? ceil_div(b.oy + b.h, 1 << ycb) : 0;
-        }
-    }
-    if ((rc = assign_quant(P, geo, err))) return rc;
-
-    // Per component and resolution: code-block states of each band, and per
-    // precinct the block range and tag trees of each band.
-    std::vector<std::vector<ResState>> st(C, rgeo);
-    for (int c = 0; c < C; c++)
+    for (int c = 0; c < C; c++) {
+        const Coding &cd = coding_of(P, &ts, c);
+        geo[c] = make_geometry(tw, th, NL, cd.xcb, cd.ycb);
         for (int r = 0; r <= NL; r++) {
+            const int px = cd.ppx[r], py = cd.ppy[r];
+            const int xcb = std::min(cd.xcb, r ? px - 1 : px), ycb = std::min(cd.ycb, r ? py - 1 : py);
+            if (xcb < 0 || ycb < 0) { err = "bad precinct size"; return TC_E_CODESTREAM; }
+            const int sh = NL - r;
             ResState &rs = st[c][r];
-            const int ppx = r ? P.ppx[r] - 1 : P.ppx[r], ppy = r ? P.ppy[r] - 1 : P.ppy[r];
-            const int64_t kx0 = rs.rx0 >> P.ppx[r], ky0 = rs.ry0 >> P.ppy[r];
-            for (const Band &b : geo[r].bands) rs.cb.emplace_back((size_t)b.ncbx * b.ncby);
+            const int64_t rx1 = (T.x1 + ((int64_t)1 << sh) - 1) >> sh, ry1 = (T.y1 + ((int64_t)1 << sh) - 1) >> sh;
+            rs.rx0 = (T.x0 + ((int64_t)1 << sh) - 1) >> sh;
+            rs.ry0 = (T.y0 + ((int64_t)1 << sh) - 1) >> sh;
+            rs.px = px;
+            rs.py = py;
+            rs.pw = (int)(((rx1 + ((int64_t)1 << px) - 1) >> px) - (rs.rx0 >> px));
+            rs.ph = (int)(((ry1 + ((int64_t)1 << py) - 1) >> py) - (rs.ry0 >> py));
+            nprec_bands += (int64_t)rs.pw * rs.ph * (int64_t)geo[c][r].bands.size();
+            if (nprec_bands > (1 << 22)) { err = "too many precincts"; return TC_E_UNSUPPORTED; }
+            for (Band &b : geo[c][r].bands) {
+                b.cbw_log2 = xcb;
+                b.cbh_log2 = ycb;
+                b.ox = (int)((T.x0 >> b.level) & ((1 << xcb) - 1));
+                b.oy = (int)((T.y0 >> b.level) & ((1 << ycb) - 1));
+                b.ncbx = b.w > 0 ? ceil_div(b.ox + b.w, 1 << xcb) : 0;
+                b.ncby = b.h > 0 ? ceil_div(b.oy + b.h, 1 << ycb) : 0;
+            }
+            const int ppx = r ? px - 1 : px, ppy = r ? py - 1 : py;
+            const int64_t kx0 = rs.rx0 >> px, ky0 = rs.ry0 >> py;
+            for (const Band &b : geo[c][r].bands) rs.cb.emplace_back((size_t)b.ncbx * b.ncby);
             rs.prec.resize((size_t)rs.pw * rs.ph);
             for (int q = 0; q < rs.ph; q++)
                 for (int p = 0; p < rs.pw; p++) {
                     auto &pbs = rs.prec[(size_t)q * rs.pw + p];
-                    for (const Band &b : geo[r].bands) {
+                    for (const Band &b : geo[c][r].bands) {
                         PrecBand pb;
                         // the band and the precinct cell on the band's grid
                         const int64_t bx0 = T.x0 >> b.level, by0 = T.y0 >> b.level;
@@ -1077,6 +1196,8 @@ static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Para
                     }
                 }
         }
+        if ((rc = assign_quant(quant_of(P, &ts, c), P.bits, NL, geo[c], err))) return rc;
+    }
 
     // The tile-part bodies are read one after the other as one packet
     // sequence; a packet does not straddle two tile-parts.
@@ -1094,7 +1215,7 @@ static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Para
         }
         if (part_i >= parts.size()) { err = "packet data missing"; return TC_E_CODESTREAM; }
         const size_t pend = part_end();
-        if (P.scod & 2) {  // SOP
+        if (scod & 2) {  // SOP
             if (pos + 6 <= pend && cs[pos] == 0xFF && cs[pos + 1] == 0x91) pos += 6;
         }
         BitReader br(cs, pos, pend);
@@ -1102,8 +1223,8 @@ static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Para
         contrib.clear();
         ResState &rs = st[c][r];
         if (present) {
-            for (size_t bi = 0; bi < geo[r].bands.size(); bi++) {
-                const Band &b = geo[r].bands[bi];
+            for (size_t bi = 0; bi < geo[c][r].bands.size(); bi++) {
+                const Band &b = geo[c][r].bands[bi];
                 PrecBand &pb = rs.prec[prec][bi];
                 const int gw = pb.i1 - pb.i0;
                 for (int j = pb.j0; j < pb.j1; j++)
@@ -1139,7 +1260,7 @@ static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Para
         br.align();
         if (br.overrun) { err = "packet header overrun"; return TC_E_CODESTREAM; }
         pos = br.pos;
-        if (P.scod & 4) {  // EPH
+        if (scod & 4) {  // EPH
             if (pos + 2 > pend || cs[pos] != 0xFF || cs[pos + 1] != 0x92) { err = "missing EPH"; return TC_E_CODESTREAM; }
             pos += 2;
         }
@@ -1162,17 +1283,17 @@ static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Para
 
     // Position-driven orders (ISO B.12.1.3-B.12.1.5) visit a precinct at the
     // first reference-grid position it covers, stepping over the tile by the
-    // smallest precinct of any resolution.  All components share one
-    // precinct grid (no subsampling, one COD), so the test is per resolution.
+    // smallest precinct of any component and resolution.
     int64_t dx = INT64_MAX, dy = INT64_MAX;
-    for (int r = 0; r <= NL; r++) {
-        dx = std::min<int64_t>(dx, (int64_t)1 << (P.ppx[r] + NL - r));
-        dy = std::min<int64_t>(dy, (int64_t)1 << (P.ppy[r] + NL - r));
-    }
-    // precinct of resolution r that starts at (x, y), or -1
-    auto prec_at = [&](int r, int64_t x, int64_t y) -> int {
-        const int sh = NL - r, px = P.ppx[r], py = P.ppy[r];
-        const ResState &rs = rgeo[r];
+    for (int c = 0; c < C; c++)
+        for (int r = 0; r <= NL; r++) {
+            dx = std::min<int64_t>(dx, (int64_t)1 << (st[c][r].px + NL - r));
+            dy = std::min<int64_t>(dy, (int64_t)1 << (st[c][r].py + NL - r));
+        }
+    // precinct of component c, resolution r that starts at (x, y), or -1
+    auto prec_at = [&](int c, int r, int64_t x, int64_t y) -> int {
+        const ResState &rs = st[c][r];
+        const int sh = NL - r, px = rs.px, py = rs.py;
         const int64_t mx = ((int64_t)1 << (px + sh)) - 1, my = ((int64_t)1 << (py + sh)) - 1;
         const bool sx = !(x & mx) || (x == T.x0 && ((rs.rx0 << sh) & mx));
         const bool sy = !(y & my) || (y == T.y0 && ((rs.ry0 << sh) & my));
@@ -1188,33 +1309,32 @@ static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Para
             if (int e = read_packet(l, r, c, prec)) return e;
         return TC_OK;
     };
-    switch (P.prog) {
+    switch (prog) {
     case 0:  // LRCP
         for (int l = 0; l < L; l++) for (int r = 0; r < R; r++) for (int c = 0; c < C; c++)
-            for (int k = 0; k < rgeo[r].pw * rgeo[r].ph; k++)
+            for (int k = 0; k < st[c][r].pw * st[c][r].ph; k++)
                 if ((rc = read_packet(l, r, c, k))) return rc;
         break;
     case 1:  // RLCP
         for (int r = 0; r < R; r++) for (int l = 0; l < L; l++) for (int c = 0; c < C; c++)
-            for (int k = 0; k < rgeo[r].pw * rgeo[r].ph; k++)
+            for (int k = 0; k < st[c][r].pw * st[c][r].ph; k++)
                 if ((rc = read_packet(l, r, c, k))) return rc;
         break;
     case 2:  // RPCL
         for (int r = 0; r < R; r++)
             for (int64_t y = T.y0; y < T.y1; y = next(y, dy))
-                for (int64_t x = T.x0; x < T.x1; x = next(x, dx)) {
-                    const int k = prec_at(r, x, y);
-                    if (k >= 0)
-                        for (int c = 0; c < C; c++)
-                            if ((rc = layers(r, c, k))) return rc;
-                }
+                for (int64_t x = T.x0; x < T.x1; x = next(x, dx))
+                    for (int c = 0; c < C; c++) {
+                        const int k = prec_at(c, r, x, y);
+                        if (k >= 0 && (rc = layers(r, c, k))) return rc;
+                    }
         break;
     case 3:  // PCRL
         for (int64_t y = T.y0; y < T.y1; y = next(y, dy))
             for (int64_t x = T.x0; x < T.x1; x = next(x, dx))
                 for (int c = 0; c < C; c++)
                     for (int r = 0; r < R; r++) {
-                        const int k = prec_at(r, x, y);
+                        const int k = prec_at(c, r, x, y);
                         if (k >= 0 && (rc = layers(r, c, k))) return rc;
                     }
         break;
@@ -1223,7 +1343,7 @@ static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Para
             for (int64_t y = T.y0; y < T.y1; y = next(y, dy))
                 for (int64_t x = T.x0; x < T.x1; x = next(x, dx))
                     for (int r = 0; r < R; r++) {
-                        const int k = prec_at(r, x, y);
+                        const int k = prec_at(c, r, x, y);
                         if (k >= 0 && (rc = layers(r, c, k))) return rc;
                     }
         break;
@@ -1234,16 +1354,17 @@ static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Para
     const uint64_t plane = (uint64_t)tw * th;
     {
         size_t nb = 0;
-        for (int r = 0; r < R; r++)
-            for (const Band &b : geo[r].bands) nb += (size_t)b.ncbx * b.ncby;
-        out.desc.reserve(out.desc.size() + nb * C);
-        em.first.reserve(em.first.size() + nb * C + 1);
+        for (int c = 0; c < C; c++)
+            for (int r = 0; r < R; r++)
+                for (const Band &b : geo[c][r].bands) nb += (size_t)b.ncbx * b.ncby;
+        out.desc.reserve(out.desc.size() + nb);
+        em.first.reserve(em.first.size() + nb + 1);
         em.segs.reserve(em.segs.size() + arena.size());
     }
     for (int c = 0; c < C; c++)
         for (int r = 0; r < R; r++)
-            for (size_t bi = 0; bi < geo[r].bands.size(); bi++) {
-                const Band &b = geo[r].bands[bi];
+            for (size_t bi = 0; bi < geo[c][r].bands.size(); bi++) {
+                const Band &b = geo[c][r].bands[bi];
                 std::vector<CblkState> &cbs = st[c][r].cb[bi];
                 const int cbw = 1 << b.cbw_log2, cbh = 1 << b.cbh_log2;
                 for (int j = 0; j < b.ncby; j++)
@@ -1258,8 +1379,8 @@ static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Para
                         d.orient = (uint8_t)b.orient;
                         d.out_pitch = (uint32_t)tw;
                         d.out_off = coef_off + (uint64_t)c * plane + (uint64_t)(b.y0 + cy) * tw + (uint64_t)(b.x0 + cx);
-                        d.step = P.reversible ? 1.0f : b.step;
-                        d.flags = P.reversible ? 0 : TC_CBLK_IRREVERSIBLE;
+                        d.step = reversible ? 1.0f : b.step;
+                        d.flags = reversible ? 0 : TC_CBLK_IRREVERSIBLE;
                         em.first.push_back((uint32_t)em.segs.size());
                         if (cb.included && cb.passes > 0) {
                             if (cb.zbp > b.mb) { err = "zero bit-planes exceed Mb"; return TC_E_CODESTREAM; }
@@ -1295,8 +1416,11 @@ static int parse_raw_codestream(const uint8_t *cs, size_t len, Parsed &out, std:
     const size_t ntiles = P.tiles.size();
 
     // Tile-parts (ISO A.4.2) in codestream order, grouped by tile index Isot:
-    // the packet data range of each.
+    // the packet data range of each.  The first tile-part of a tile may carry
+    // COD / COC / QCD / QCC for that tile.
     std::vector<std::vector<std::pair<size_t, size_t>>> parts(ntiles);
+    std::vector<Scope> tscope(ntiles);
+    for (Scope &t : tscope) t.init(P.ncomp);
     for (;;) {
         const uint32_t m = rd.u16();
         if (rd.bad) { err = "truncated codestream"; return TC_E_CODESTREAM; }
@@ -1309,18 +1433,22 @@ static int parse_raw_codestream(const uint8_t *cs, size_t len, Parsed &out, std:
         if (lsot != 10 || isot >= ntiles || (psot && psot < 14)) { err = "bad SOT or tile index"; return TC_E_CODESTREAM; }
         const size_t end = psot ? sot_pos + psot : len;
         if (end > len) { err = "tile-part runs past the codestream"; return TC_E_CODESTREAM; }
+        const bool first_part = parts[isot].empty();
         for (;;) {
             const uint32_t mm = rd.u16();
             if (rd.bad || rd.pos > end) { err = "truncated tile-part header"; return TC_E_CODESTREAM; }
             if (mm == M_SOD) break;
             const uint32_t L = rd.u16();
-            if (mm == M_COD || mm == M_COC || mm == M_QCD || mm == M_QCC || mm == M_RGN ||
-                mm == M_POC || mm == M_PPT) {
-                err = "tile-part header coding parameters are not supported";
+            if (L < 2 || rd.pos - 2 + L > end) { err = "bad tile-part marker"; return TC_E_CODESTREAM; }
+            const size_t seg_end = rd.pos - 2 + L;
+            if (mm == M_COD || mm == M_COC || mm == M_QCD || mm == M_QCC) {
+                if (!first_part) { err = "coding parameters after a tile's first tile-part"; return TC_E_CODESTREAM; }
+                if ((rc = read_coding_marker(rd, mm, seg_end, P.ncomp, tscope[isot], err))) return rc;
+            } else if (mm == M_RGN || mm == M_POC || mm == M_PPT) {
+                err = "RGN/POC/PPT in a tile-part header are not supported";
                 return TC_E_UNSUPPORTED;
             }
-            if (L < 2 || rd.pos - 2 + L > end) { err = "bad tile-part marker"; return TC_E_CODESTREAM; }
-            rd.pos += L - 2;
+            rd.pos = seg_end;
         }
         parts[isot].emplace_back(rd.pos, end);
         rd.pos = end;
@@ -1336,7 +1464,7 @@ static int parse_raw_codestream(const uint8_t *cs, size_t len, Parsed &out, std:
     for (size_t t = 0; t < ntiles; t++) {
         const Params::Tile &T = P.tiles[t];
         if (parts[t].empty()) { err = "tile " + std::to_string(t) + " has no tile-part"; return TC_E_CODESTREAM; }
-        if ((rc = parse_tile(cs, len, P, T, parts[t], coef_off, out, em, err))) return rc;
+        if ((rc = parse_tile(cs, len, P, T, tscope[t], parts[t], coef_off, out, em, err))) return rc;
         tc_tile_info ti;
         ti.x0 = (int32_t)(T.x0 - P.xo);
         ti.y0 = (int32_t)(T.y0 - P.yo);
@@ -1422,30 +1550,41 @@ int encode_codestream(const tc_encode_params &p, const void *planes, std::vector
             fwd_plane_pitch(dp.data() + c * np, W, H, (size_t)W, NL, fwd97_line, threads);
     }
 
-    std::vector<Resolution> geo = make_geometry(W, H, NL, p.cblk_log2, p.cblk_log2);
+    // Per component: code-block size (COC when it differs from COD) and
+    // step multiplier (QCC when it differs from QCD).
+    int cblk[4];
+    double scale[4];
+    for (int c = 0; c < C; c++) {
+        cblk[c] = p.comp_cblk_log2[c] > 0 ? p.comp_cblk_log2[c] : p.cblk_log2;
+        scale[c] = p.comp_step_scale[c] > 0.0 ? p.comp_step_scale[c] : 1.0;
+        if (cblk[c] < 2 || cblk[c] > 6) { err = "code-block size out of range"; return TC_E_ARG; }
+    }
+    std::vector<std::vector<Resolution>> geo(C);
+    for (int c = 0; c < C; c++) geo[c] = make_geometry(W, H, NL, cblk[c], cblk[c]);
     // Quantisation: exponent/mantissa per band, quantised coefficients.
     std::vector<int32_t> q(np * C);
     int need_guard = 1;
-    for (int r = 0; r <= NL; r++)
-        for (Band &b : geo[r].bands) {
-            const int rb = B + band_gain_log2(b.orient);
-            if (p.reversible) {
-                b.eps = rb;
-                b.mu = 0;
-                b.step = 1.0f;
-            } else {
-                const double delta = p.base_step * std::ldexp(1.0, B) / subband_norm(true, b.level, b.orient);
-                int e = rb - (int)std::floor(std::log2(delta));
-                int m = (int)std::lround((delta / std::ldexp(1.0, rb - e) - 1.0) * 2048.0);
-                if (m >= 2048) { m = 0; e--; }
-                if (m < 0) m = 0;
-                if (e < 0 || e > 31) { err = "quantisation step out of range"; return TC_E_ARG; }
-                b.eps = e;
-                b.mu = m;
-                b.step = (float)std::ldexp(1.0 + m / 2048.0, rb - e);
-            }
-            uint32_t mx = 0;
-            for (int c = 0; c < C; c++)
+    for (int c = 0; c < C; c++)
+        for (int r = 0; r <= NL; r++)
+            for (Band &b : geo[c][r].bands) {
+                const int rb = B + band_gain_log2(b.orient);
+                if (p.reversible) {
+                    b.eps = rb;
+                    b.mu = 0;
+                    b.step = 1.0f;
+                } else {
+                    const double delta =
+                        scale[c] * p.base_step * std::ldexp(1.0, B) / subband_norm(true, b.level, b.orient);
+                    int e = rb - (int)std::floor(std::log2(delta));
+                    int m = (int)std::lround((delta / std::ldexp(1.0, rb - e) - 1.0) * 2048.0);
+                    if (m >= 2048) { m = 0; e--; }
+                    if (m < 0) m = 0;
+                    if (e < 0 || e > 31) { err = "quantisation step out of range"; return TC_E_ARG; }
+                    b.eps = e;
+                    b.mu = m;
+                    b.step = (float)std::ldexp(1.0 + m / 2048.0, rb - e);
+                }
+                uint32_t mx = 0;
                 for (int y = b.y0; y < b.y0 + b.h; y++)
                     for (int x = b.x0; x < b.x0 + b.w; x++) {
                         const size_t i = c * np + (size_t)y * W + x;
@@ -1460,17 +1599,18 @@ int encode_codestream(const tc_encode_params &p, const void *planes, std::vector
                         q[i] = v;
                         mx = std::max(mx, (uint32_t)std::abs((int64_t)v));
                     }
-            int nb = 0;
-            while (nb < 32 && (mx >> nb)) nb++;
-            need_guard = std::max(need_guard, nb - b.eps + 1);
-        }
+                int nb = 0;
+                while (nb < 32 && (mx >> nb)) nb++;
+                need_guard = std::max(need_guard, nb - b.eps + 1);
+            }
     int G = p.guard_bits > 0 ? p.guard_bits : std::max(2, need_guard);
     if (G < need_guard || G > 7) { err = "guard bits cannot hold the coefficient range"; return TC_E_ARG; }
-    for (int r = 0; r <= NL; r++)
-        for (Band &b : geo[r].bands) {
-            b.mb = G + b.eps - 1;
-            if (b.mb > 31) { err = "more than 31 magnitude bit-planes"; return TC_E_ARG; }
-        }
+    for (int c = 0; c < C; c++)
+        for (int r = 0; r <= NL; r++)
+            for (Band &b : geo[c][r].bands) {
+                b.mb = G + b.eps - 1;
+                if (b.mb > 31) { err = "more than 31 magnitude bit-planes"; return TC_E_ARG; }
+            }
 
     // Tier-1: encode every code-block.
     struct Job {
@@ -1479,8 +1619,8 @@ int encode_codestream(const tc_encode_params &p, const void *planes, std::vector
     std::vector<Job> jobs;
     for (int c = 0; c < C; c++)
         for (int r = 0; r <= NL; r++)
-            for (int bi = 0; bi < (int)geo[r].bands.size(); bi++) {
-                const Band &b = geo[r].bands[bi];
+            for (int bi = 0; bi < (int)geo[c][r].bands.size(); bi++) {
+                const Band &b = geo[c][r].bands[bi];
                 for (int j = 0; j < b.ncby; j++)
                     for (int i = 0; i < b.ncbx; i++) jobs.push_back({c, r, bi, i, j});
             }
@@ -1492,7 +1632,7 @@ int encode_codestream(const tc_encode_params &p, const void *planes, std::vector
     std::atomic<int> fail{0};
     parallel_for((int)jobs.size(), threads, [&](int k) {
         const Job &jb = jobs[k];
-        const Band &b = geo[jb.r].bands[jb.bi];
+        const Band &b = geo[jb.c][jb.r].bands[jb.bi];
         const int cx = jb.i << b.cbw_log2, cy = jb.j << b.cbh_log2;
         const int bw = std::min(1 << b.cbw_log2, b.w - cx), bh = std::min(1 << b.cbh_log2, b.h - cy);
         int32_t blk[64 * 64];
@@ -1518,8 +1658,8 @@ int encode_codestream(const tc_encode_params &p, const void *planes, std::vector
         std::vector<uint8_t> hdr;
         BitWriter bw(hdr);
         bool any = false;
-        for (int bi = 0; bi < (int)geo[r].bands.size(); bi++) {
-            const Band &b = geo[r].bands[bi];
+        for (int bi = 0; bi < (int)geo[c][r].bands.size(); bi++) {
+            const Band &b = geo[c][r].bands[bi];
             if (b.ncbx * b.ncby == 0) continue;
             const int k0 = first[c][r][bi];
             for (int i = 0; i < b.ncbx * b.ncby; i++) any |= coded[k0 + i].passes > 0;
@@ -1532,8 +1672,8 @@ int encode_codestream(const tc_encode_params &p, const void *planes, std::vector
         }
         bw.put(1);
         std::vector<int> order;
-        for (int bi = 0; bi < (int)geo[r].bands.size(); bi++) {
-            const Band &b = geo[r].bands[bi];
+        for (int bi = 0; bi < (int)geo[c][r].bands.size(); bi++) {
+            const Band &b = geo[c][r].bands[bi];
             const int n = b.ncbx * b.ncby;
             if (n == 0) continue;
             const int k0 = first[c][r][bi];
@@ -1594,20 +1734,41 @@ int encode_codestream(const tc_encode_params &p, const void *planes, std::vector
     wr.u8(p.cblk_log2 - 2);
     wr.u8(0);                              // code-block style
     wr.u8(p.reversible ? 1 : 0);
-    const int nbands = 3 * NL + 1;
-    wr.u16(M_QCD);
-    if (p.reversible) {
-        wr.u16(3 + nbands);
-        wr.u8((G << 5) | 0);
-    } else {
-        wr.u16(3 + 2 * nbands);
-        wr.u8((G << 5) | 2);
+    // COC for components whose code-block size differs from COD's
+    for (int c = 0; c < C; c++) {
+        if (cblk[c] == p.cblk_log2) continue;
+        wr.u16(M_COC);
+        wr.u16(9);
+        wr.u8(c);                          // Ccoc
+        wr.u8(0);                          // Scoc: default precincts
+        wr.u8(NL);
+        wr.u8(cblk[c] - 2);
+        wr.u8(cblk[c] - 2);
+        wr.u8(0);
+        wr.u8(p.reversible ? 1 : 0);
     }
-    for (int r = 0; r <= NL; r++)
-        for (const Band &b : geo[r].bands) {
-            if (p.reversible) wr.u8(b.eps << 3);
-            else wr.u16((b.eps << 11) | b.mu);
-        }
+    const int nbands = 3 * NL + 1;
+    // QCD with component 0's steps, QCC for components whose steps differ
+    auto write_steps = [&](int c) {
+        if (p.reversible) wr.u8((G << 5) | 0);
+        else wr.u8((G << 5) | 2);
+        for (int r = 0; r <= NL; r++)
+            for (const Band &b : geo[c][r].bands) {
+                if (p.reversible) wr.u8(b.eps << 3);
+                else wr.u16((b.eps << 11) | b.mu);
+            }
+    };
+    const int qbytes = p.reversible ? nbands : 2 * nbands;
+    wr.u16(M_QCD);
+    wr.u16(3 + qbytes);
+    write_steps(0);
+    for (int c = 1; c < C; c++) {
+        if (scale[c] == scale[0]) continue;
+        wr.u16(M_QCC);
+        wr.u16(4 + qbytes);
+        wr.u8(c);                          // Cqcc
+        write_steps(c);
+    }
     wr.u16(M_SOT);
     wr.u16(10);
     wr.u16(0);
