@@ -311,3 +311,21 @@ def test_coc_qcc_streams_decode(gpu_ctx, kw):
             d = np.abs(got - want.astype(np.int64))
             assert d.max() <= 1
             assert (d > 0).mean() < 0.005
+
+
+def test_digital_cinema_4k_decode(gpu_ctx):
+    """OpenJPEG's 4K digital-cinema profile (CPRL with a POC, six
+    tile-parts, precincts, 32x32 code-blocks) through the GPU: within 1 LSB
+    of the oracle."""
+    import io
+    from PIL import Image
+    from gpu_helpers import oracle_decode_tiled
+    img = synth_image(4096, 2160, 3, 8, seed=10)
+    buf = io.BytesIO()
+    Image.fromarray(np.moveaxis(img, 0, -1)).save(buf, "JPEG2000", cinema_mode="cinema4k-24", no_jp2=True)
+    cs = buf.getvalue()
+    got = _decoder(gpu_ctx).decode(cs).astype(np.int64)
+    _, want = oracle_decode_tiled(cs)
+    d = np.abs(got - want.astype(np.int64))
+    assert d.max() <= 1
+    assert (d > 0).mean() < 0.005

@@ -346,3 +346,71 @@ def test_component_levels_must_agree():
     with pytest.raises(TCError) as ei:
         codec.parse(bytes(cs))
     assert ei.value.status == TC_E_UNSUPPORTED
+
+
+def _with_main_marker(cs, marker, body):
+    """The codestream with one more main-header marker segment before the
+    first SOT."""
+    _, sot = _main_header_markers(cs)
+    return cs[:sot] + marker.to_bytes(2, "big") + (len(body) + 2).to_bytes(2, "big") + body + cs[sot:]
+
+
+def _poc(*entries):
+    """POC body (ISO A.6.6) for fewer than 257 components: (RSpoc, CSpoc,
+    LYEpoc, REpoc, CEpoc, Ppoc) per progression volume."""
+    return b"".join(bytes([rs, cs]) + lye.to_bytes(2, "big") + bytes([re, ce, p]) for rs, cs, lye, re, ce, p in entries)
+
+
+@pytest.mark.parametrize("prog,vols", [
+    ("LRCP", [(0, 0, 1, 6, 3, 0), (0, 0, 3, 6, 3, 0)]),            # layer 0 first, then the rest
+    ("RPCL", [(0, 0, 3, 2, 3, 2), (2, 0, 3, 6, 3, 2)]),            # resolutions 0-1, then 2-5
+    # resolution 3 in two volumes by layer, the second skipping what the first read
+    ("RLCP", [(0, 0, 3, 3, 3, 1), (3, 0, 2, 4, 3, 1), (3, 0, 3, 4, 3, 1), (4, 0, 3, 6, 3, 1)]),
+], ids=["lrcp-by-layer", "rpcl-by-resolution", "rlcp-four-volumes"])
+def test_poc_volumes(prog, vols):
+    """Progression order changes (POC, ISO A.6.6): volumes that restate the
+    stream's own order in pieces give the same descriptors as the plain
+    stream, each packet read once at the first volume that reaches it (the
+    reference reads one order from COD)."""
+    pytest.importorskip("PIL.Image")
+    from gpu_helpers import pil_j2k
+    img = synth_image(300, 200, 3, 8, seed=7)
+    cs = pil_j2k(img, num_resolutions=6, progression=prog, irreversible=True, quality_mode="rates",
+                 quality_layers=[40, 20, 10], codeblock_size=(32, 32), precinct_size=(64, 64))
+    with_poc = _with_main_marker(cs, 0xFF5F, _poc(*vols))
+    _, d1, p1 = codec.parse(cs)
+    _, d2, p2 = codec.parse(with_poc)
+    for f in ("w", "h", "mb", "zero_bitplanes", "passes", "step", "out_off", "seg_len"):
+        np.testing.assert_array_equal(d1[f], d2[f])
+    np.testing.assert_array_equal(p1, p2)  # multi-layer: gathered pools, byte for byte
+
+
+def test_bad_poc_entries_are_rejected():
+    """A volume whose resolution or component range is empty, or whose
+    progression is out of range, is a malformed codestream."""
+    pytest.importorskip("PIL.Image")
+    from gpu_helpers import pil_j2k
+    cs = pil_j2k(synth_image(64, 64, 1, 8, seed=8), num_resolutions=3)
+    for entry in [(2, 0, 1, 1, 1, 0), (0, 1, 1, 3, 1, 0), (0, 0, 1, 3, 1, 5)]:
+        with pytest.raises(TCError) as ei:
+            codec.parse(_with_main_marker(cs, 0xFF5F, _poc(entry)))
+        assert ei.value.status == TC_E_CODESTREAM
+
+
+@pytest.mark.parametrize("mode", ["cinema2k-24", "cinema4k-24"])
+def test_digital_cinema_profiles(mode):
+    """OpenJPEG's digital-cinema profiles: 2K (CPRL, one tile-part per
+    component, precincts) and 4K (CPRL with a POC in the first of six
+    tile-parts) decode within 1 LSB of OpenJPEG."""
+    pytest.importorskip("PIL.Image")
+    from gpu_helpers import oracle_decode_tiled, openjpeg_decode
+    import io
+    from PIL import Image
+    w, h = (4096, 2160) if mode.startswith("cinema4k") else (2048, 1080)
+    img = synth_image(w, h, 3, 8, seed=10)
+    buf = io.BytesIO()
+    Image.fromarray(np.moveaxis(img, 0, -1)).save(buf, "JPEG2000", cinema_mode=mode, no_jp2=True)
+    cs = buf.getvalue()
+    info, out = oracle_decode_tiled(cs)
+    assert info["progression"] == 4
+    assert np.abs(out.astype(np.int64) - openjpeg_decode(cs)).max() <= 1

@@ -758,10 +758,17 @@ struct Quant {
     std::vector<int> eps, mu;  // as signalled (1 or 3N+1 entries)
 };
 
-// The coding parameters one header sets: the main header, or a tile's first
-// tile-part header.  Per component, a COC / QCC replaces the header's COD /
-// QCD.
+// One progression volume of a POC marker (ISO A.6.6): layers [0, lye),
+// resolutions [rs, re), components [cs, ce) in order prog.
+struct PocEntry {
+    int rs, cs, lye, re, ce, prog;
+};
+
+// The coding parameters one header sets: the main header, or a tile's
+// tile-part headers (COD / COC / QCD / QCC in the first one, POC in any).
+// Per component, a COC / QCC replaces the header's COD / QCD.
 struct Scope {
+    std::vector<PocEntry> poc;
     bool has_cod = false, has_qcd = false;
     int scod = 0, prog = 0, layers = 1, mct = 0;
     Coding cod;
@@ -895,6 +902,28 @@ static int read_coding_marker(Reader &rd, uint32_t m, size_t seg_end, int ncomp,
     return TC_OK;
 }
 
+// POC (ISO A.6.6): progression volumes appended to `poc`.  The reference
+// reads one progression order from COD (codestream.c:95-136).
+static int read_poc(Reader &rd, size_t seg_end, int ncomp, std::vector<PocEntry> &poc, std::string &err)
+{
+    const bool wide = ncomp >= 257;
+    const size_t entry = wide ? 9 : 7;
+    while (rd.pos + entry <= seg_end) {
+        PocEntry e;
+        e.rs = (int)rd.u8();
+        e.cs = (int)(wide ? rd.u16() : rd.u8());
+        e.lye = (int)rd.u16();
+        e.re = (int)rd.u8();
+        e.ce = (int)(wide ? rd.u16() : rd.u8());
+        if (!wide && e.ce == 0) e.ce = 256;
+        e.prog = (int)rd.u8();
+        if (e.prog > 4 || e.re <= e.rs || e.ce <= e.cs) { err = "bad POC entry"; return TC_E_CODESTREAM; }
+        poc.push_back(e);
+    }
+    if (rd.bad || rd.pos != seg_end) { err = "bad POC length"; return TC_E_CODESTREAM; }
+    return TC_OK;
+}
+
 // Every component of the image (t null) or of a tile must share the
 // decomposition levels and the wavelet, and every tile the colour transform:
 // the DWT launches and the fused colour stage need one geometry per image.
@@ -992,8 +1021,14 @@ static int parse_main(Reader &rd, Params &P, std::string &err)
             if (rc) return rc;
             break;
         }
-        case M_RGN: case M_POC: case M_PPM: case M_CRG:
-            err = "RGN/POC/PPM/CRG markers are not supported";
+        case M_POC: {
+            if (!P.have_siz) { err = "POC before SIZ"; return TC_E_CODESTREAM; }
+            const int rc = read_poc(rd, seg_end, P.ncomp, P.main.poc, err);
+            if (rc) return rc;
+            break;
+        }
+        case M_RGN: case M_PPM: case M_CRG:
+            err = "RGN/PPM/CRG markers are not supported";
             return TC_E_UNSUPPORTED;
         default:
             break;  // COM, TLM, PLM and others carry nothing we need
@@ -1304,49 +1339,69 @@ static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Para
         return (int)(ky * rs.pw + kx);
     };
     auto next = [](int64_t v, int64_t step) { return (v / step + 1) * step; };
-    auto layers = [&](int r, int c, int prec) -> int {
-        for (int l = 0; l < L; l++)
-            if (int e = read_packet(l, r, c, prec)) return e;
-        return TC_OK;
+    // Progression volumes: the tile's POC, else the main header's, else one
+    // volume of everything in COD's order.  A packet (c, r, precinct, layer)
+    // is read once, at the first volume that reaches it: done[c][r][k]
+    // counts the layers already read (ISO A.6.6, B.12).
+    std::vector<PocEntry> vols = !ts.poc.empty() ? ts.poc : P.main.poc;
+    if (vols.empty()) vols.push_back(PocEntry{0, 0, L, R, C, prog});
+    std::vector<std::vector<std::vector<int>>> done(C, std::vector<std::vector<int>>(R));
+    for (int c = 0; c < C; c++)
+        for (int r = 0; r < R; r++) done[c][r].assign((size_t)st[c][r].pw * st[c][r].ph, 0);
+    auto packet = [&](int l, int r, int c, int k) -> int {
+        int &d = done[c][r][k];
+        if (l < d) return TC_OK;  // read by an earlier volume
+        if (l > d) { err = "progression volumes skip a layer"; return TC_E_CODESTREAM; }
+        d++;
+        return read_packet(l, r, c, k);
     };
-    switch (prog) {
-    case 0:  // LRCP
-        for (int l = 0; l < L; l++) for (int r = 0; r < R; r++) for (int c = 0; c < C; c++)
-            for (int k = 0; k < st[c][r].pw * st[c][r].ph; k++)
-                if ((rc = read_packet(l, r, c, k))) return rc;
-        break;
-    case 1:  // RLCP
-        for (int r = 0; r < R; r++) for (int l = 0; l < L; l++) for (int c = 0; c < C; c++)
-            for (int k = 0; k < st[c][r].pw * st[c][r].ph; k++)
-                if ((rc = read_packet(l, r, c, k))) return rc;
-        break;
-    case 2:  // RPCL
-        for (int r = 0; r < R; r++)
+    for (const PocEntry &v : vols) {
+        const int lye = std::min(v.lye, L), re = std::min(v.re, R), ce = std::min(v.ce, C);
+        const int rs = v.rs, cs0 = v.cs;
+        auto layers = [&](int r, int c, int k) -> int {
+            for (int l = 0; l < lye; l++)
+                if (int e = packet(l, r, c, k)) return e;
+            return TC_OK;
+        };
+        switch (v.prog) {
+        case 0:  // LRCP
+            for (int l = 0; l < lye; l++) for (int r = rs; r < re; r++) for (int c = cs0; c < ce; c++)
+                for (int k = 0; k < st[c][r].pw * st[c][r].ph; k++)
+                    if ((rc = packet(l, r, c, k))) return rc;
+            break;
+        case 1:  // RLCP
+            for (int r = rs; r < re; r++) for (int l = 0; l < lye; l++) for (int c = cs0; c < ce; c++)
+                for (int k = 0; k < st[c][r].pw * st[c][r].ph; k++)
+                    if ((rc = packet(l, r, c, k))) return rc;
+            break;
+        case 2:  // RPCL
+            for (int r = rs; r < re; r++)
+                for (int64_t y = T.y0; y < T.y1; y = next(y, dy))
+                    for (int64_t x = T.x0; x < T.x1; x = next(x, dx))
+                        for (int c = cs0; c < ce; c++) {
+                            const int k = prec_at(c, r, x, y);
+                            if (k >= 0 && (rc = layers(r, c, k))) return rc;
+                        }
+            break;
+        case 3:  // PCRL
             for (int64_t y = T.y0; y < T.y1; y = next(y, dy))
                 for (int64_t x = T.x0; x < T.x1; x = next(x, dx))
-                    for (int c = 0; c < C; c++) {
-                        const int k = prec_at(c, r, x, y);
-                        if (k >= 0 && (rc = layers(r, c, k))) return rc;
-                    }
-        break;
-    case 3:  // PCRL
-        for (int64_t y = T.y0; y < T.y1; y = next(y, dy))
-            for (int64_t x = T.x0; x < T.x1; x = next(x, dx))
-                for (int c = 0; c < C; c++)
-                    for (int r = 0; r < R; r++) {
-                        const int k = prec_at(c, r, x, y);
-                        if (k >= 0 && (rc = layers(r, c, k))) return rc;
-                    }
-        break;
-    default:  // CPRL
-        for (int c = 0; c < C; c++)
-            for (int64_t y = T.y0; y < T.y1; y = next(y, dy))
-                for (int64_t x = T.x0; x < T.x1; x = next(x, dx))
-                    for (int r = 0; r < R; r++) {
-                        const int k = prec_at(c, r, x, y);
-                        if (k >= 0 && (rc = layers(r, c, k))) return rc;
-                    }
-        break;
+                    for (int c = cs0; c < ce; c++)
+                        for (int r = rs; r < re; r++) {
+                            const int k = prec_at(c, r, x, y);
+                            if (k >= 0 && (rc = layers(r, c, k))) return rc;
+                        }
+            break;
+        default:  // CPRL
+            for (int c = cs0; c < ce; c++)
+                for (int64_t y = T.y0; y < T.y1; y = next(y, dy))
+                    for (int64_t x = T.x0; x < T.x1; x = next(x, dx))
+                        for (int r = rs; r < re; r++) {
+                            const int k = prec_at(c, r, x, y);
+                            if (k >= 0 && (rc = layers(r, c, k))) return rc;
+                        }
+            break;
+        }
     }
 
     // Descriptors, component by component; segments are placed once every
@@ -1444,8 +1499,10 @@ static int parse_raw_codestream(const uint8_t *cs, size_t len, Parsed &out, std:
             if (mm == M_COD || mm == M_COC || mm == M_QCD || mm == M_QCC) {
                 if (!first_part) { err = "coding parameters after a tile's first tile-part"; return TC_E_CODESTREAM; }
                 if ((rc = read_coding_marker(rd, mm, seg_end, P.ncomp, tscope[isot], err))) return rc;
-            } else if (mm == M_RGN || mm == M_POC || mm == M_PPT) {
-                err = "RGN/POC/PPT in a tile-part header are not supported";
+            } else if (mm == M_POC) {
+                if ((rc = read_poc(rd, seg_end, P.ncomp, tscope[isot].poc, err))) return rc;
+            } else if (mm == M_RGN || mm == M_PPT) {
+                err = "RGN/PPT in a tile-part header are not supported";
                 return TC_E_UNSUPPORTED;
             }
             rd.pos = seg_end;
