@@ -24,6 +24,7 @@
 // columns (DWTReverse53/97, dwt_r53.cl / dwt_r97.cl).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <type_traits>
 
 #include "dwt_common.cuh"
@@ -102,16 +103,13 @@ __device__ __forceinline__ int to_int(T v)
 template <typename T>
 using Vec4 = typename std::conditional<std::is_same<T, float>::value, float4, int4>::type;
 
-// The CTA's work: tile (bx, by) of level `io`, components from cbase.
-template <typename T, int WAVELET, int RND, int NCOMP, int COLOR, typename OT>
-__device__ __forceinline__ void rev_tile(const LevelIO &io, int bits, int bx, int by, int cbase)
+// Phase 1 of a tile: issues the asynchronous copies of tile (bx, by) of
+// level `io`, NT components from cbase, into `tiles` (the caller waits).
+template <typename T, int WAVELET, int NT>
+__device__ __forceinline__ void rev_stage(const LevelIO &io, int bx, int by, int cbase, T *tiles)
 {
     using G = RevGeo<WAVELET>;
     constexpr int H = G::H, NR = G::NR, TY = G::TY, TX = G::TX, NC = G::NC, S = G::S;
-    constexpr bool PLANE = COLOR < 0;
-    constexpr int NT = PLANE ? 1 : NCOMP;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *tiles = reinterpret_cast<T *>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int x0 = bx * TX, y0 = by * TY;
     const int w = io.w, h = io.h, wl = (w + 1) >> 1, hl = (h + 1) >> 1;
@@ -128,14 +126,23 @@ __device__ __forceinline__ void rev_tile(const LevelIO &io, int bits, int bx, in
         const T *ll = static_cast<const T *>(io.ll[cbase + cc]);
         const T *coef = static_cast<const T *>(io.coef[cbase + cc]);
         if (interior) {
+            // y0 - H is even and a warp's rows step by 8: a warp copies rows
+            // of one parity only, so each lane's source is one band row
+            // advancing by 4 rows of its plane per step
+            constexpr int RSTEP = kThreads / 32;
+            static_assert(RSTEP % 2 == 0, "a warp's rows share a parity");
             const int xs = ((x0 - H) >> 1) + (lane >> 1);
-            for (int r = warp; r < NR; r += kThreads / 32) {
-                const int y = y0 - H + r, yb = y >> 1;
-                const T *src = (y & 1) ? coef + (size_t)(hl + yb) * io.coef_pitch + ((lane & 1) ? wl : 0)
-                                       : ((lane & 1) ? coef + (size_t)yb * io.coef_pitch + wl
-                                                     : ll + (size_t)yb * io.ll_pitch);
-                src += xs;
-                T *dst = t + r * S + lane;
+            const int y = y0 - H + warp, yb = y >> 1;
+            const bool from_ll = !(y & 1) && !(lane & 1);
+            const size_t pitch = from_ll ? (size_t)io.ll_pitch : (size_t)io.coef_pitch;
+            const T *src = (y & 1) ? coef + (size_t)(hl + yb) * io.coef_pitch + ((lane & 1) ? wl : 0)
+                                   : ((lane & 1) ? coef + (size_t)yb * io.coef_pitch + wl
+                                                 : ll + (size_t)yb * io.ll_pitch);
+            src += xs;
+            const size_t step = pitch * (RSTEP / 2);
+            T *dst = t + warp * S + lane;
+#pragma unroll 2
+            for (int r = warp; r < NR; r += RSTEP, src += step, dst += RSTEP * S) {
 #pragma unroll
                 for (int j = 0; j < NC / 32; j++) cp_async4(dst + 32 * j, src + 16 * j);
                 if (lane < NC % 32) cp_async4(dst + 32 * (NC / 32), src + 16 * (NC / 32));
@@ -153,8 +160,19 @@ __device__ __forceinline__ void rev_tile(const LevelIO &io, int bits, int bx, in
             }
         }
     }
-    cp_async_wait_all();
-    __syncthreads();
+}
+
+// Phases 2-3 of a staged tile: lifting and the store.
+template <typename T, int WAVELET, int RND, int NCOMP, int COLOR, typename OT>
+__device__ __forceinline__ void rev_compute(const LevelIO &io, int bits, int bx, int by, int cbase, T *tiles)
+{
+    using G = RevGeo<WAVELET>;
+    constexpr int H = G::H, NR = G::NR, TY = G::TY, TX = G::TX, S = G::S;
+    constexpr bool PLANE = COLOR < 0;
+    constexpr int NT = PLANE ? 1 : NCOMP;
+    const int tid = threadIdx.x;
+    const int x0 = bx * TX, y0 = by * TY;
+    const int w = io.w, h = io.h;
 
     // 2. horizontal lifting, one row segment per thread (64 rows x 4
     //    segments of 32 outputs); segments are read and written with 16-byte
@@ -231,9 +249,15 @@ __device__ __forceinline__ void rev_tile(const LevelIO &io, int bits, int bx, in
         const int y = y0 + obase;
         if constexpr (PLANE) {
             T *out = static_cast<T *>(io.out[cbase]) + (size_t)y * io.out_pitch + x;
+            const size_t pitch = (size_t)io.out_pitch;
+            if (full_rows) {
 #pragma unroll
-            for (int r = 0; r < OUTR; r++)
-                if (full_rows || y + r < h) out[(size_t)r * io.out_pitch] = v[H + r];
+                for (int r = 0; r < OUTR; r++, out += pitch) *out = v[H + r];
+            } else {
+#pragma unroll
+                for (int r = 0; r < OUTR; r++, out += pitch)
+                    if (y + r < h) *out = v[H + r];
+            }
         } else if (COLOR == TC_COLOR_DC || cc >= 3) {
             OT *out = static_cast<OT *>(io.out[cc]) + (size_t)y * io.out_pitch + x;
 #pragma unroll
@@ -270,6 +294,18 @@ __device__ __forceinline__ void rev_tile(const LevelIO &io, int bits, int bx, in
             }
         }
     }
+}
+
+// The CTA's work: tile (bx, by) of level `io`, components from cbase.
+template <typename T, int WAVELET, int RND, int NCOMP, int COLOR, typename OT>
+__device__ __forceinline__ void rev_tile(const LevelIO &io, int bits, int bx, int by, int cbase)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *tiles = reinterpret_cast<T *>(smem_raw);
+    rev_stage<T, WAVELET, COLOR < 0 ? 1 : NCOMP>(io, bx, by, cbase, tiles);
+    cp_async_wait_all();
+    __syncthreads();
+    rev_compute<T, WAVELET, RND, NCOMP, COLOR, OT>(io, bits, bx, by, cbase, tiles);
 }
 
 // One level of one image: tiles (blockIdx.x, blockIdx.y), one component per
