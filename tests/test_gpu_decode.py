@@ -329,3 +329,19 @@ def test_digital_cinema_4k_decode(gpu_ctx):
     d = np.abs(got - want.astype(np.int64))
     assert d.max() <= 1
     assert (d > 0).mean() < 0.005
+
+
+def test_decode_to_pnm_and_pgx(gpu_ctx, tmp_path):
+    """Decoder.decode_to_file writes what decode returns: a PPM that Pillow
+    reads as the original (lossless) and one PGX per component."""
+    from PIL import Image
+    from thousandthchicken_b200.imageio import read_pgx
+    img = synth_image(120, 90, 3, 8, seed=12)
+    cs = codec.encode(img, 8, levels=3)
+    dec = _decoder(gpu_ctx)
+    (ppm,) = dec.decode_to_file(cs, tmp_path / "o.ppm")
+    np.testing.assert_array_equal(np.moveaxis(np.asarray(Image.open(ppm)), -1, 0), img)
+    paths = dec.decode_to_file(cs, tmp_path / "o.pgx")
+    for c, p in enumerate(paths):
+        plane, bits, signed = read_pgx(p)
+        np.testing.assert_array_equal(plane, img[c])

@@ -414,3 +414,28 @@ def test_digital_cinema_profiles(mode):
     info, out = oracle_decode_tiled(cs)
     assert info["progression"] == 4
     assert np.abs(out.astype(np.int64) - openjpeg_decode(cs)).max() <= 1
+
+
+def test_pnm_and_pgx_writers_round_trip(tmp_path):
+    """The output writers: PGM/PPM (8 and 12 bit) and PGX (unsigned and
+    signed) read back identically, and Pillow reads the 8-bit PNM files."""
+    from PIL import Image
+    from thousandthchicken_b200.imageio import read_pgx, read_pnm, write_image
+    rgb = synth_image(37, 21, 3, 8, seed=1)
+    g12 = synth_image(40, 30, 1, 12, seed=2)
+    for planes, bits, name in [(rgb, 8, "a.ppm"), (g12, 12, "b.pgm"), (rgb[:1], 8, "c.pgm")]:
+        (p,) = write_image(tmp_path / name, planes, bits)
+        back, b2 = read_pnm(p)
+        np.testing.assert_array_equal(back, planes)
+        assert b2 == bits
+        if bits == 8:  # (Pillow rescales deeper PGMs to 16 bits)
+            pil = np.asarray(Image.open(p))
+            np.testing.assert_array_equal(pil[None] if pil.ndim == 2 else np.moveaxis(pil, -1, 0), planes)
+    s16 = (synth_image(20, 10, 2, 16, seed=3).astype(np.int32) - 32768).astype(np.int16)
+    for planes, bits, signed in [(rgb, 8, False), (s16, 16, True)]:
+        paths = write_image(tmp_path / "x.pgx", planes, bits, signed)
+        assert len(paths) == planes.shape[0]
+        for c, p in enumerate(paths):
+            plane, b2, sg = read_pgx(p)
+            np.testing.assert_array_equal(plane, planes[c])
+            assert (b2, sg) == (bits, signed)

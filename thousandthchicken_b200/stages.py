@@ -341,5 +341,16 @@ class Decoder:
                                              out.nbytes, C.byref(info)), "tc_decode_j2k")
         return out
 
+    def decode_to_file(self, cs, path):
+        """Decode and write the samples as PNM (.pgm/.ppm) or PGX (.pgx, one
+        file per component); returns the written paths."""
+        from .imageio import write_image
+        out = self.decode(cs)
+        hdr = L.ImageInfo()
+        buf = np.frombuffer(cs, np.uint8) if not isinstance(cs, (str, Path)) else \
+            np.frombuffer(Path(cs).read_bytes(), np.uint8)
+        self.ctx.check(L.lib().tc_j2k_read_header(buf.ctypes.data, buf.size, C.byref(hdr)), "tc_j2k_read_header")
+        return write_image(path, out, hdr.bits, bool(hdr.is_signed))
+
     def plan(self, codestreams) -> Plan:
         return Plan(self.ctx, codestreams)
