@@ -183,10 +183,15 @@ int tc_dwt_reverse97_static(const float *d_in, int in_pitch, float *d_out, int o
 #define TC_COLOR_DC  0  /* DC level shift only, per component */
 #define TC_COLOR_RCT 1  /* reversible component transform (components 0-2) */
 #define TC_COLOR_ICT 2  /* irreversible component transform (components 0-2) */
+/* Flag or-ed into a `bits` argument: the samples are signed (two's
+ * complement, no DC level shift, clamped to [-2^(bits-1), 2^(bits-1)-1]). */
+#define TC_SIGNED 0x100
 
 /* Inverse: planes of in_type (TC_INT32 or TC_FLOAT32) -> inverse colour
  * transform, DC shift, rounding (float input: to nearest even) and clamp to
- * [0, 2^bits-1] -> planes of out_type (TC_U8, TC_U16 or TC_INT32).
+ * [0, 2^bits-1] -> planes of out_type (TC_U8, TC_U16 or TC_INT32).  With
+ * bits | TC_SIGNED: no DC shift, clamp to the signed range, two's
+ * complement in the same sample types.
  * Replaces Preprocessor::color_decoder_lossless/color_decoder_lossy/
  * idc_level_shifting (Preprocessor.cpp:44-180) and the tcr_kernel,
  * tci_kernel and idc_level_shift_kernel kernels; the ICT uses the ISO G.2
@@ -197,7 +202,8 @@ int tc_color_inverse(tc_ctx *ctx, int kind, int ncomp,
                      void *const *d_out, int out_type, int out_pitch,
                      int w, int h, int bits);
 
-/* Forward: unsigned samples of in_type (TC_U8, TC_U16 or TC_INT32) -> DC
+/* Forward: unsigned samples of in_type (TC_U8, TC_U16 or TC_INT32; signed,
+ * two's complement and not DC-shifted, with bits | TC_SIGNED) -> DC
  * shift and forward colour transform -> TC_INT32 (RCT/DC) or TC_FLOAT32
  * (ICT, or DC to float) planes.  Replaces the rct_kernel, ict_kernel and
  * fdc_level_shift_kernel kernels (preprocess_rct.cl, preprocess_ict.cl,
@@ -335,7 +341,8 @@ typedef struct tc_encode_params {
     int32_t guard_bits;    /* 0 = choose automatically */
     int32_t progression;   /* 0 = LRCP, 1 = RLCP */
     int32_t threads;       /* <= 0: all cores */
-    int32_t reserved;
+    int32_t is_signed;     /* signed samples (TC_S8 / TC_S16 style two's
+                              complement input, no DC level shift) */
     /* Per-component overrides (0: the values above), written as COC and QCC
      * marker segments: the code-block size exponent and a multiplier of the
      * irreversible step. */
@@ -343,7 +350,8 @@ typedef struct tc_encode_params {
     double  comp_step_scale[4];
 } tc_encode_params;
 
-/* Encode planar unsigned samples (TC_U8 when bits <= 8, else TC_U16) into a
+/* Encode planar samples (8-bit when bits <= 8, else 16-bit; unsigned, or
+ * two's complement when is_signed) into a
  * single-tile, single-layer codestream with all coding passes (a harness
  * encoder: the reference has none). */
 int tc_encode_j2k(const tc_encode_params *p, const void *h_planes,

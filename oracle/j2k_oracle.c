@@ -652,15 +652,32 @@ void or_rct_forward(int32_t *c0, int32_t *c1, int32_t *c2, size_t n, int bits)
     }
 }
 
+/* Output range of `bits` (OR_SIGNED set: signed samples, no DC level shift;
+ * ISO G.1.2 shifts unsigned components only). */
+static void out_range(int bits, int32_t *dc, int32_t *lo, int32_t *hi)
+{
+    const int b = bits & 0xFF;
+    if (bits & OR_SIGNED) {
+        *dc = 0;
+        *lo = -(1 << (b - 1));
+        *hi = (1 << (b - 1)) - 1;
+    } else {
+        *dc = 1 << (b - 1);
+        *lo = 0;
+        *hi = (1 << b) - 1;
+    }
+}
+
 void or_rct_inverse(int32_t *c0, int32_t *c1, int32_t *c2, size_t n, int bits)
 {
-    const int32_t dc = 1 << (bits - 1), mx = (1 << bits) - 1;
+    int32_t dc, lo, mx;
+    out_range(bits, &dc, &lo, &mx);
     for (size_t i = 0; i < n; i++) {
         const int32_t y = c0[i], u = c1[i], v = c2[i];
         const int32_t g = y - ((u + v) >> 2), r = v + g, b = u + g;
-        c0[i] = clampi(r + dc, 0, mx);
-        c1[i] = clampi(g + dc, 0, mx);
-        c2[i] = clampi(b + dc, 0, mx);
+        c0[i] = clampi(r + dc, lo, mx);
+        c1[i] = clampi(g + dc, lo, mx);
+        c2[i] = clampi(b + dc, lo, mx);
     }
 }
 
@@ -679,14 +696,15 @@ void or_ict_forward(const int32_t *r, const int32_t *g, const int32_t *b,
 void or_ict_inverse(const double *y, const double *cb, const double *cr,
                     int32_t *r, int32_t *g, int32_t *b, size_t n, int bits)
 {
-    const int32_t dc = 1 << (bits - 1), mx = (1 << bits) - 1;
+    int32_t dc, lo, mx;
+    out_range(bits, &dc, &lo, &mx);
     for (size_t i = 0; i < n; i++) {
         const double R = y[i] + 1.402 * cr[i];
         const double G = y[i] - 0.34413 * cb[i] - 0.71414 * cr[i];
         const double B = y[i] + 1.772 * cb[i];
-        r[i] = clampi((int32_t)rint(R) + dc, 0, mx);
-        g[i] = clampi((int32_t)rint(G) + dc, 0, mx);
-        b[i] = clampi((int32_t)rint(B) + dc, 0, mx);
+        r[i] = clampi((int32_t)rint(R) + dc, lo, mx);
+        g[i] = clampi((int32_t)rint(G) + dc, lo, mx);
+        b[i] = clampi((int32_t)rint(B) + dc, lo, mx);
     }
 }
 
@@ -697,14 +715,16 @@ void or_dc_forward(int32_t *x, size_t n, int bits)
 
 void or_dc_inverse_clamp(int32_t *x, size_t n, int bits)
 {
-    const int32_t dc = 1 << (bits - 1), mx = (1 << bits) - 1;
-    for (size_t i = 0; i < n; i++) x[i] = clampi(x[i] + dc, 0, mx);
+    int32_t dc, lo, mx;
+    out_range(bits, &dc, &lo, &mx);
+    for (size_t i = 0; i < n; i++) x[i] = clampi(x[i] + dc, lo, mx);
 }
 
 void or_dc_inverse_float(const double *x, int32_t *out, size_t n, int bits)
 {
-    const int32_t dc = 1 << (bits - 1), mx = (1 << bits) - 1;
-    for (size_t i = 0; i < n; i++) out[i] = clampi((int32_t)rint(x[i]) + dc, 0, mx);
+    int32_t dc, lo, mx;
+    out_range(bits, &dc, &lo, &mx);
+    for (size_t i = 0; i < n; i++) out[i] = clampi((int32_t)rint(x[i]) + dc, lo, mx);
 }
 
 /* ===================== Whole-tile decode ================================= */
@@ -767,7 +787,9 @@ int or_decode_tile(const or_cblk *cb, int n, const uint8_t *pool,
     const size_t np = (size_t)w * h;
     int32_t *ip = NULL;
     double *fp = NULL;
-    if (ncomp < 1 || ncomp > 4 || bits < 1 || bits > 16 || levels < 0 || levels > 32) return -1;
+    if (ncomp < 1 || ncomp > 4 || (bits & 0xFF) < 1 || (bits & 0xFF) > 16 || (bits & ~(0xFF | OR_SIGNED)) ||
+        levels < 0 || levels > 32)
+        return -1;
     if (reversible) ip = calloc(np * ncomp, sizeof(int32_t));
     else fp = calloc(np * ncomp, sizeof(double));
     if (!ip && !fp) return -2;

@@ -127,6 +127,10 @@ typedef struct or_cblk {
  * colour transform (mct: 0 none, 1 RCT/ICT by wavelet) and DC shift, and write
  * clamped samples as uint16 planes (out + c*w*h).  threads <= 0 uses all
  * cores.  Returns 0 or a negative error. */
+/* Flag or-ed into `bits`: signed samples (no DC level shift, clamped to the
+ * signed range; or_decode_tile's 16-bit output then holds two's complement). */
+#define OR_SIGNED 0x100
+
 int or_decode_tile(const or_cblk *cb, int n, const uint8_t *pool,
                    int w, int h, int ncomp, int bits, int levels,
                    int reversible, int mct, float r, int threads,

@@ -181,10 +181,11 @@ def dc_inverse_float(x, bits):
     return out
 
 
-def decode_tile(cblks, pool: np.ndarray, w, h, ncomp, bits, levels, reversible, mct, r=0.5, threads=0):
+def decode_tile(cblks, pool: np.ndarray, w, h, ncomp, bits, levels, reversible, mct, r=0.5, threads=0,
+                signed=False):
     """Whole-tile decode from parsed code-block descriptors (numpy structured
     rows with the tc_cblk_desc fields of one image).  Returns uint16
-    [ncomp, h, w]."""
+    [ncomp, h, w], or int16 for signed samples (no DC level shift)."""
     n = len(cblks)
     arr = (OrCblk * max(n, 1))()
     plane = w * h
@@ -203,8 +204,8 @@ def decode_tile(cblks, pool: np.ndarray, w, h, ncomp, bits, levels, reversible, 
         c.step = float(d["step"])
     out = np.zeros((ncomp, h, w), np.uint16)
     pool = np.ascontiguousarray(pool, np.uint8)
-    rc = lib().or_decode_tile(arr, n, _p(pool), w, h, ncomp, bits, levels, int(reversible), int(mct), r,
-                              threads, _p(out))
+    rc = lib().or_decode_tile(arr, n, _p(pool), w, h, ncomp, bits | (0x100 if signed else 0), levels,
+                              int(reversible), int(mct), r, threads, _p(out))
     if rc:
         raise ValueError(f"or_decode_tile failed: {rc}")
-    return out
+    return out.view(np.int16) if signed else out

@@ -123,12 +123,13 @@ def oracle_decode_tiled(cs, r=0.5):
     [ncomp, height, width])."""
     info, desc, pool = codec.parse(cs)
     W, H, C = info["width"], info["height"], info["ncomp"]
-    out = np.zeros((C, H, W), np.uint16)
+    out = np.zeros((C, H, W), np.int16 if info["is_signed"] else np.uint16)
     bounds = [t[4] for t in info["tiles"]] + [C * W * H]
     for k, (x0, y0, w, h, co) in enumerate(info["tiles"]):
         sel = (desc["out_off"] >= bounds[k]) & (desc["out_off"] < bounds[k + 1])
         d = desc[sel].copy()
         d["out_off"] -= np.uint64(co)
         out[:, y0:y0 + h, x0:x0 + w] = O.decode_tile(d, pool, w, h, C, info["bits"], info["levels"],
-                                                     bool(info["reversible"]), bool(info["mct"]), r=r)
+                                                     bool(info["reversible"]), bool(info["mct"]), r=r,
+                                                     signed=bool(info["is_signed"]))
     return info, out

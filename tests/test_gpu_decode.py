@@ -6,7 +6,7 @@ import pytest
 
 import oracle as O
 from conftest import golden_cases, load_golden, synth_image
-from test_host_codec import COC_QCC, PRECINCTS, TILED
+from test_host_codec import COC_QCC, PRECINCTS, SIGNED, TILED
 from thousandthchicken_b200 import codec
 
 pytestmark = pytest.mark.gpu
@@ -345,3 +345,31 @@ def test_decode_to_pnm_and_pgx(gpu_ctx, tmp_path):
     for c, p in enumerate(paths):
         plane, bits, signed = read_pgx(p)
         np.testing.assert_array_equal(plane, img[c])
+
+
+@pytest.mark.parametrize("bits,comps,kw", SIGNED, ids=["s12-53", "s16-53", "s8-rct", "s12-97"])
+def test_signed_samples_decode(gpu_ctx, bits, comps, kw):
+    """Signed components through the GPU (no DC shift, signed clamp, int8 /
+    int16 output), alone and in a plan with an unsigned image: lossless
+    equals the original, lossy within 1 of the oracle."""
+    from gpu_helpers import oracle_decode_tiled
+    from test_host_codec import _ct_like
+    from thousandthchicken_b200.stages import Plan
+    img = _ct_like(120, 150, bits, seed=bits) if comps == 1 else \
+        np.random.default_rng(5).integers(-128, 128, (3, 40, 50)).astype(np.int8)
+    cs = codec.encode(img, bits, levels=4, **kw)
+    got = _decoder(gpu_ctx).decode(cs)
+    assert got.dtype == (np.int8 if bits <= 8 else np.int16)
+    _, want = oracle_decode_tiled(cs)
+    if kw["reversible"]:
+        np.testing.assert_array_equal(got, img)
+    else:
+        d = np.abs(got.astype(np.int64) - want.astype(np.int64))
+        assert d.max() <= 1 and (d > 0).mean() < 0.005
+    other = codec.encode(synth_image(64, 48, comps, bits, seed=1), bits, levels=3, **kw)
+    plan = Plan(gpu_ctx, [cs, other])
+    outs = plan.execute(plan.alloc_outputs())
+    gpu_ctx.synchronize()
+    g0 = outs[0].cpu().numpy()
+    np.testing.assert_array_equal(g0.view(np.int16) if bits > 8 else g0, got)
+    plan.close()

@@ -439,3 +439,43 @@ def test_pnm_and_pgx_writers_round_trip(tmp_path):
             plane, b2, sg = read_pgx(p)
             np.testing.assert_array_equal(plane, planes[c])
             assert (b2, sg) == (bits, signed)
+
+
+def _ct_like(h, w, bits, seed):
+    """A signed single-component image like a CT slice: a smooth field
+    around zero plus noise, clipped to the signed range of `bits`."""
+    rng = np.random.default_rng(seed)
+    yy, xx = np.mgrid[0:h, 0:w]
+    lo, hi = -(1 << (bits - 1)), (1 << (bits - 1)) - 1
+    v = np.sin(xx / 15.0) * hi * 0.4 + (yy / h - 0.5) * hi * 0.5 + rng.normal(0, hi / 60, (h, w))
+    return np.clip(np.rint(v), lo, hi).astype(np.int8 if bits <= 8 else np.int16)[None]
+
+
+SIGNED = [  # (bits, components, harness-encoder options)
+    (12, 1, dict(reversible=True, mct=False)),
+    (16, 1, dict(reversible=True, mct=False)),
+    (8, 3, dict(reversible=True, mct=True)),
+    (12, 1, dict(reversible=False, mct=False, base_step=1 / 256)),
+]
+
+
+@pytest.mark.parametrize("bits,comps,kw", SIGNED, ids=["s12-53", "s16-53", "s8-rct", "s12-97"])
+def test_signed_samples_through_oracle(bits, comps, kw):
+    """Signed components (Ssiz bit 7): no DC level shift (ISO G.1.2 shifts
+    unsigned ones only), two's complement samples clamped to the signed
+    range.  Lossless streams give back the original; OpenJPEG decodes the
+    8- and 16-bit ones to the same values (Pillow presents them offset by
+    2^(bits-1))."""
+    img = _ct_like(120, 150, bits, seed=bits) if comps == 1 else \
+        np.random.default_rng(5).integers(-128, 128, (3, 40, 50)).astype(np.int8)
+    cs = codec.encode(img, bits, levels=4, **kw)
+    from gpu_helpers import oracle_decode_tiled, openjpeg_decode
+    info, out = oracle_decode_tiled(cs)
+    assert info["is_signed"] == 1 and out.dtype == np.int16
+    if kw["reversible"]:
+        np.testing.assert_array_equal(out, img.astype(np.int16))
+        if bits in (8, 16):
+            opj = openjpeg_decode(cs).astype(np.int64) - (1 << (bits - 1))
+            np.testing.assert_array_equal(opj, img.astype(np.int64))
+    else:
+        assert np.abs(out.astype(np.int64) - img).max() <= 64

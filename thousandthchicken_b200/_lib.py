@@ -74,7 +74,7 @@ class EncodeParams(C.Structure):
     _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("ncomp", C.c_int32), ("bits", C.c_int32),
                 ("levels", C.c_int32), ("reversible", C.c_int32), ("mct", C.c_int32),
                 ("cblk_log2", C.c_int32), ("base_step", C.c_double), ("guard_bits", C.c_int32),
-                ("progression", C.c_int32), ("threads", C.c_int32), ("reserved", C.c_int32),
+                ("progression", C.c_int32), ("threads", C.c_int32), ("is_signed", C.c_int32),
                 ("comp_cblk_log2", C.c_int32 * 4), ("comp_step_scale", C.c_double * 4)]
 
 

@@ -65,17 +65,22 @@ def parse(cs):
 def encode(planes: np.ndarray, bits: int, levels: int = 5, reversible: bool = True, mct: bool = True,
            cblk_log2: int = 6, base_step: float = 1.0 / 128, guard_bits: int = 0, progression: int = 0,
            threads: int = 0, comp_cblk_log2=None, comp_step_scale=None) -> bytes:
-    """Harness encoder: planar unsigned samples [ncomp, h, w] -> codestream.
+    """Harness encoder: planar samples [ncomp, h, w] -> codestream; signed
+    integer arrays (int8 / int16) give signed components (no DC shift).
     comp_cblk_log2 / comp_step_scale: per-component code-block size exponent
     and irreversible step multiplier (0 = the image-wide value), written as
     COC / QCC marker segments."""
-    planes = np.ascontiguousarray(planes, np.uint8 if bits <= 8 else np.uint16)
+    signed = np.asarray(planes).dtype.kind == "i"
+    if signed:
+        planes = np.ascontiguousarray(planes, np.int8 if bits <= 8 else np.int16)
+    else:
+        planes = np.ascontiguousarray(planes, np.uint8 if bits <= 8 else np.uint16)
     if planes.ndim == 2:
         planes = planes[None]
     ncomp, h, w = planes.shape
     p = L.EncodeParams(width=w, height=h, ncomp=ncomp, bits=bits, levels=levels, reversible=int(reversible),
                        mct=int(mct), cblk_log2=cblk_log2, base_step=base_step, guard_bits=guard_bits,
-                       progression=progression, threads=threads)
+                       progression=progression, threads=threads, is_signed=int(signed))
     for c, v in enumerate(comp_cblk_log2 or []):
         p.comp_cblk_log2[c] = int(v)
     for c, v in enumerate(comp_step_scale or []):

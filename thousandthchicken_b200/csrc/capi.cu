@@ -125,6 +125,8 @@ static int check_ctx(tc_ctx *ctx)
 }
 
 static int sample_bytes(int bits) { return bits <= 8 ? 1 : 2; }
+// The `bits` argument of the output stages: the depth, TC_SIGNED for signed samples.
+static int out_bits(const tc_image_info &inf) { return inf.bits | (inf.is_signed ? TC_SIGNED : 0); }
 
 // Reverse DWT of ncomp components from Mallat planes coef[c] (pitch cp)
 // through levels >= 2 into ping-pong scratch, and the last level either into
@@ -414,7 +416,7 @@ static int run_reverse_batched(tc_plan *P, void *const *d_out)
         if (inf.levels) continue;
         const int ob = sample_bytes(inf.bits);
         e = launch_color_inverse(ctx, color_of(inf), inf.ncomp, u.coef, inf.reversible ? TC_INT32 : TC_FLOAT32, u.w,
-                                 u.out, ob == 1 ? TC_U8 : TC_U16, inf.width, u.w, u.h, inf.bits);
+                                 u.out, ob == 1 ? TC_U8 : TC_U16, inf.width, u.w, u.h, out_bits(inf));
         if (e != cudaSuccess) return cuda_status(ctx, e, "colour");
     }
     if (outs != P->jobs_outs) {
@@ -486,7 +488,7 @@ static int run_reverse_batched(tc_plan *P, void *const *d_out)
                     const tc_image_info &inf = *u.inf;
                     if (taken[i] || inf.levels - t != 1 || inf.reversible != a.reversible ||
                         color_of(inf) != color_of(a) || inf.ncomp != a.ncomp ||
-                        sample_bytes(inf.bits) != sample_bytes(a.bits) || inf.bits != a.bits)
+                        sample_bytes(inf.bits) != sample_bytes(a.bits) || out_bits(inf) != out_bits(a))
                         continue;
                     taken[i] = 1;
                     Walk &W = wk[i];
@@ -508,7 +510,7 @@ static int run_reverse_batched(tc_plan *P, void *const *d_out)
                     jobs.push_back(J);
                 }
                 launches.push_back({first, (int)jobs.size() - first, tiles, wv, color_of(a), a.ncomp,
-                                    sample_bytes(a.bits) == 1 ? TC_U8 : TC_U16, a.bits});
+                                    sample_bytes(a.bits) == 1 ? TC_U8 : TC_U16, out_bits(a)});
             }
         }
         // the previous table's upload must be done before its staging is rewritten
@@ -572,12 +574,12 @@ static int plan_run(tc_plan *P, void *const *d_out)
         int rc;
         if (inf.levels == 0) {
             e = launch_color_inverse(ctx, color, inf.ncomp, cptr, inf.reversible ? TC_INT32 : TC_FLOAT32,
-                                     inf.width, optr, otype, inf.width, inf.width, inf.height, inf.bits);
+                                     inf.width, optr, otype, inf.width, inf.width, inf.height, out_bits(inf));
             rc = cuda_status(ctx, e, "colour");
         } else {
             rc = run_reverse(ctx, wavelet, TC_ROUND_FLOOR, cptr, inf.width, inf.width, inf.height, inf.levels,
                              inf.ncomp, static_cast<char *>(P->scratch.ptr), optr, inf.width, color, otype,
-                             inf.bits);
+                             out_bits(inf));
         }
         if (rc) return rc;
     }
@@ -829,7 +831,8 @@ static int color_args_ok(int kind, int ncomp, const void *const *in, const void 
 {
     if (kind < TC_COLOR_DC || kind > TC_COLOR_ICT || ncomp < 1 || ncomp > 4 || !in || !out) return 0;
     if ((kind != TC_COLOR_DC) && ncomp < 3) return 0;
-    if (w <= 0 || h <= 0 || ip < w || op < w || bits < 1 || bits > 16) return 0;
+    const int b = bits & ~TC_SIGNED;
+    if (w <= 0 || h <= 0 || ip < w || op < w || b < 1 || b > 16) return 0;
     for (int c = 0; c < ncomp; c++)
         if (!in[c] || !out[c]) return 0;
     return 1;

@@ -20,9 +20,9 @@ struct Planes {
 };
 
 template <typename OT>
-__device__ __forceinline__ OT clamped(int v, int mx)
+__device__ __forceinline__ OT clamped(int v, int lo, int hi)
 {
-    return (OT)(v < 0 ? 0 : (v > mx ? mx : v));
+    return (OT)(v < lo ? lo : (v > hi ? hi : v));
 }
 
 // Four consecutive samples of a row: one 16-byte (or 8/4-byte) access when
@@ -96,7 +96,7 @@ __global__ void __launch_bounds__(kColThreads) color_inverse_kernel(Planes P, in
     const int x0 = 4 * (blockIdx.x * kColThreads + threadIdx.x);
     if (x0 >= w) return;
     const int n = min(4, w - x0);
-    const int dc = 1 << (bits - 1), mx = (1 << bits) - 1;
+    const OutRange R = out_range(bits);
     for (int y = blockIdx.y; y < h; y += gridDim.y) {
         const size_t ii = (size_t)y * in_pitch + x0, oi = (size_t)y * out_pitch + x0;
         IT a[NC][4];
@@ -127,7 +127,7 @@ __global__ void __launch_bounds__(kColThreads) color_inverse_kernel(Planes P, in
                 else v[c] = __float2int_rn((float)a[c][j]);
             }
 #pragma unroll
-            for (int c = 0; c < NC; c++) o[c][j] = clamped<OT>(v[c] + dc, mx);
+            for (int c = 0; c < NC; c++) o[c][j] = clamped<OT>(v[c] + R.dc, R.lo, R.hi);
         }
 #pragma unroll
         for (int c = 0; c < NC; c++) store4<OT>(static_cast<OT *>(P.out[c]) + oi, vout, n, o[c]);
@@ -143,7 +143,8 @@ __global__ void __launch_bounds__(kColThreads) color_forward_kernel(Planes P, in
     const int x0 = 4 * (blockIdx.x * kColThreads + threadIdx.x);
     if (x0 >= w) return;
     const int n = min(4, w - x0);
-    const int dc = 1 << (bits - 1);
+    const int dc = out_range(bits).dc;
+    const bool sgn = bits & TC_SIGNED;
     for (int y = blockIdx.y; y < h; y += gridDim.y) {
         const size_t ii = (size_t)y * in_pitch + x0, oi = (size_t)y * out_pitch + x0;
         IT a[NC][4];
@@ -154,7 +155,13 @@ __global__ void __launch_bounds__(kColThreads) color_forward_kernel(Planes P, in
         for (int j = 0; j < 4; j++) {
             int s_[NC];
 #pragma unroll
-            for (int c = 0; c < NC; c++) s_[c] = (int)a[c][j] - dc;
+            for (int c = 0; c < NC; c++) {
+                int v = (int)a[c][j];
+                // signed samples arrive in two's complement
+                if constexpr (sizeof(IT) == 1) v = sgn ? (int)(int8_t)a[c][j] : v;
+                if constexpr (sizeof(IT) == 2) v = sgn ? (int)(int16_t)a[c][j] : v;
+                s_[c] = v - dc;
+            }
             int c0 = 0;
             if constexpr (KIND == TC_COLOR_RCT && NC >= 3) {
                 // rct_kernel, preprocess_rct.cl:18-31

@@ -87,9 +87,9 @@ __device__ __forceinline__ void cp_async4(void *smem, const void *gmem)
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 template <typename OT>
-__device__ __forceinline__ OT clamp_out(int v, int mx)
+__device__ __forceinline__ OT clamp_out(int v, const OutRange &R)
 {
-    return (OT)(v < 0 ? 0 : (v > mx ? mx : v));
+    return (OT)(v < R.lo ? R.lo : (v > R.hi ? R.hi : v));
 }
 
 template <typename T>
@@ -231,7 +231,8 @@ __device__ __forceinline__ void rev_compute(const LevelIO &io, int bits, int bx,
     const int obase = half ? OUTR : 0;               // first output row kept
     const int pbase = half ? NR - OUTR : 0;          // first parking row
     const bool full_rows = y0 + obase + OUTR <= h;
-    const int dc = PLANE ? 0 : 1 << (bits - 1), mx = PLANE ? 0 : (1 << bits) - 1;
+    const OutRange R = out_range(PLANE ? 8 : bits);
+    const int dc = PLANE ? 0 : R.dc;
 #pragma unroll
     for (int cc = 0; cc < NT; cc++) {
         T *t = tiles + cc * NR * S;
@@ -262,7 +263,7 @@ __device__ __forceinline__ void rev_compute(const LevelIO &io, int bits, int bx,
             OT *out = static_cast<OT *>(io.out[cc]) + (size_t)y * io.out_pitch + x;
 #pragma unroll
             for (int r = 0; r < OUTR; r++)
-                if (full_rows || y + r < h) out[(size_t)r * io.out_pitch] = clamp_out<OT>(to_int(v[H + r]) + dc, mx);
+                if (full_rows || y + r < h) out[(size_t)r * io.out_pitch] = clamp_out<OT>(to_int(v[H + r]) + dc, R);
         } else if (cc < 2) {
 #pragma unroll
             for (int r = 0; r < OUTR; r++) t[(pbase + r) * S + H + col] = v[H + r];
@@ -288,9 +289,9 @@ __device__ __forceinline__ void rev_compute(const LevelIO &io, int bits, int bx,
                     c2 = __float2int_rn(fmaf(1.772f, Cb, Y));
                 }
                 const size_t ro = (size_t)r * io.out_pitch;
-                o0[ro] = clamp_out<OT>(c0 + dc, mx);
-                o1[ro] = clamp_out<OT>(c1 + dc, mx);
-                o2[ro] = clamp_out<OT>(c2 + dc, mx);
+                o0[ro] = clamp_out<OT>(c0 + dc, R);
+                o1[ro] = clamp_out<OT>(c1 + dc, R);
+                o2[ro] = clamp_out<OT>(c2 + dc, R);
             }
         }
     }

@@ -80,18 +80,21 @@ __device__ __forceinline__ void cp_async4(void *smem, const void *gmem)
 
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-// Round to nearest even and saturate to the output type's range.
-// (mx: 2^bits - 1; below the type's maximum only for narrower samples)
+// Round to nearest even, saturate to the output type's range and clamp to
+// [R.lo, R.hi] when the samples are narrower than the type; signed samples
+// are stored in two's complement.
 template <typename OT>
-__device__ __forceinline__ OT to_out(float v, int mx)
+__device__ __forceinline__ OT to_out(float v, const OutRange &R, bool sgn)
 {
-    unsigned r;
+    int r;
     if constexpr (std::is_same<OT, uint8_t>::value) {
-        asm("cvt.rni.sat.u8.f32 %0, %1;" : "=r"(r) : "f"(v));
-        if (mx < 255) r = min(r, (unsigned)mx);
+        if (sgn) asm("cvt.rni.sat.s8.f32 %0, %1;" : "=r"(r) : "f"(v));
+        else asm("cvt.rni.sat.u8.f32 %0, %1;" : "=r"(r) : "f"(v));
+        if (R.hi < 127 || (!sgn && R.hi < 255)) r = min(max(r, R.lo), R.hi);
     } else {
-        asm("cvt.rni.sat.u16.f32 %0, %1;" : "=r"(r) : "f"(v));
-        if (mx < 65535) r = min(r, (unsigned)mx);
+        if (sgn) asm("cvt.rni.sat.s16.f32 %0, %1;" : "=r"(r) : "f"(v));
+        else asm("cvt.rni.sat.u16.f32 %0, %1;" : "=r"(r) : "f"(v));
+        if (R.hi < 32767 || (!sgn && R.hi < 65535)) r = min(max(r, R.lo), R.hi);
     }
     return (OT)r;
 }
@@ -257,8 +260,9 @@ __device__ __forceinline__ void ict_tile(const LevelIO &io, int bx, int by, int 
     const bool full = y + OUTR <= io.h;
     const int cx = col & 1;
     const float fa = sf_factor(0, cx, hx, vy), fb = sf_factor(1, cx, hx, vy);  // obase is even
-    const float dc = (float)(1 << (bits - 1));
-    const int mx = (1 << bits) - 1;
+    const OutRange R = out_range(bits);
+    const bool sgn = bits & TC_SIGNED;
+    const float dc = (float)R.dc;
     const size_t o = (size_t)y * io.out_pitch + x;
     OT *o0 = static_cast<OT *>(io.out[0]) + o, *o1 = static_cast<OT *>(io.out[1]) + o,
        *o2 = static_cast<OT *>(io.out[2]) + o;
@@ -270,13 +274,13 @@ __device__ __forceinline__ void ict_tile(const LevelIO &io, int bx, int by, int 
         // inverse ICT (ISO G.3) on the unscaled samples, the output factor
         // and the DC shift folded into the coefficients
         const float yf = fmaf(f, Y, dc);
-        const float R = fmaf(1.402f * f, Cr, yf);
+        const float Rc = fmaf(1.402f * f, Cr, yf);
         const float Gc = fmaf(-0.71414f * f, Cr, fmaf(-0.34413f * f, Cb, yf));
         const float B = fmaf(1.772f * f, Cb, yf);
         const size_t ro = (size_t)r * io.out_pitch;
-        o0[ro] = to_out<OT>(R, mx);
-        o1[ro] = to_out<OT>(Gc, mx);
-        o2[ro] = to_out<OT>(B, mx);
+        o0[ro] = to_out<OT>(Rc, R, sgn);
+        o1[ro] = to_out<OT>(Gc, R, sgn);
+        o2[ro] = to_out<OT>(B, R, sgn);
     }
 }
 

@@ -1010,7 +1010,6 @@ static int parse_main(Reader &rd, Params &P, std::string &err)
                 else if (b != P.bits || sg != P.is_signed) { err = "components must share bit depth"; return TC_E_UNSUPPORTED; }
             }
             if (P.bits > 16) { err = "bit depth above 16"; return TC_E_UNSUPPORTED; }
-            if (P.is_signed) { err = "signed samples are not supported"; return TC_E_UNSUPPORTED; }
             P.main.init(P.ncomp);
             P.have_siz = true;
             break;
@@ -1575,10 +1574,12 @@ int encode_codestream(const tc_encode_params &p, const void *planes, std::vector
 
     std::vector<int32_t> ip;
     std::vector<double> dp;
+    const bool sgn = p.is_signed != 0;
     auto sample = [&](int c, size_t i) -> int32_t {
+        if (sgn) return wide ? ((const int16_t *)planes)[c * np + i] : ((const int8_t *)planes)[c * np + i];
         return wide ? ((const uint16_t *)planes)[c * np + i] : ((const uint8_t *)planes)[c * np + i];
     };
-    const int32_t dc = 1 << (B - 1);
+    const int32_t dc = sgn ? 0 : 1 << (B - 1);  // ISO G.1.2: unsigned samples only
     if (p.reversible) {
         ip.resize(np * C);
         for (int c = 0; c < C; c++)
@@ -1779,7 +1780,7 @@ int encode_codestream(const tc_encode_params &p, const void *planes, std::vector
     wr.u32(W); wr.u32(H); wr.u32(0); wr.u32(0);
     wr.u32(W); wr.u32(H); wr.u32(0); wr.u32(0);
     wr.u16(C);
-    for (int c = 0; c < C; c++) { wr.u8(B - 1); wr.u8(1); wr.u8(1); }
+    for (int c = 0; c < C; c++) { wr.u8((B - 1) | (sgn ? 0x80 : 0)); wr.u8(1); wr.u8(1); }
     wr.u16(M_COD);
     wr.u16(12);
     wr.u8(0);                              // Scod: default precincts, no SOP/EPH

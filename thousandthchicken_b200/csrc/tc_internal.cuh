@@ -15,6 +15,18 @@
 
 namespace tc {
 
+// Sample range of an output of `bits` bits (TC_SIGNED set: signed samples,
+// two's complement, no DC level shift; ISO G.1.2 shifts unsigned ones only).
+struct OutRange {
+    int dc, lo, hi;
+};
+__host__ __device__ inline OutRange out_range(int bits)
+{
+    const int b = bits & 0xFF;
+    if (bits & TC_SIGNED) return OutRange{0, -(1 << (b - 1)), (1 << (b - 1)) - 1};
+    return OutRange{1 << (b - 1), 0, (1 << b) - 1};
+}
+
 // Grow-only device buffer owned by a context.
 struct DevBuf {
     void *ptr = nullptr;

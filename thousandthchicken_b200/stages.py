@@ -278,7 +278,10 @@ class Plan:
         dev = torch.device("cuda", self.ctx.device)
         outs = []
         for info in self.infos:
-            dt = torch.uint8 if info["bits"] <= 8 else torch.int16
+            if info["bits"] <= 8:
+                dt = torch.int8 if info["is_signed"] else torch.uint8
+            else:
+                dt = torch.int16  # 16-bit samples, unsigned ones read back as uint16
             outs.append(torch.empty((info["ncomp"], info["height"], info["width"]), dtype=dt, device=dev))
         return outs
 
@@ -332,7 +335,10 @@ class Decoder:
             buf = np.frombuffer(cs, np.uint8)
         hdr = L.ImageInfo()
         self.ctx.check(L.lib().tc_j2k_read_header(buf.ctypes.data, buf.size, C.byref(hdr)), "tc_j2k_read_header")
-        dt = np.uint8 if hdr.bits <= 8 else np.uint16
+        if hdr.is_signed:
+            dt = np.int8 if hdr.bits <= 8 else np.int16
+        else:
+            dt = np.uint8 if hdr.bits <= 8 else np.uint16
         shape = (hdr.ncomp, hdr.height, hdr.width)
         if out is None:
             out = np.empty(shape, dt)
