@@ -357,6 +357,37 @@ typedef struct tc_encode_params {
 int tc_encode_j2k(const tc_encode_params *p, const void *h_planes,
                   uint8_t *h_out, size_t cap, size_t *out_len);
 
+/* ---- GPU Tier-1 encoder (no counterpart in the reference, which decodes
+ *      only) -------------------------------------------------------------- */
+
+/* One code-block to encode: its samples in the input plane set, its band. */
+typedef struct tc_t1_enc_desc {
+    uint64_t in_off;     /* element offset of sample (0,0) */
+    uint32_t in_pitch;   /* row pitch in elements */
+    float    inv_step;   /* TC_CBLK_IRREVERSIBLE: 1 / step of the band */
+    uint16_t w, h;       /* 1..64 */
+    uint8_t  orient;     /* 0 LL, 1 HL, 2 LH, 3 HH */
+    uint8_t  mb;         /* magnitude bit-planes Mb of the band (1..31) */
+    uint8_t  flags;      /* TC_CBLK_IRREVERSIBLE: float input, quantised
+                            floor(|x| / step); else int32 quantised input */
+    uint8_t  reserved;
+} tc_t1_enc_desc;
+
+typedef struct tc_t1_enc_result {
+    uint32_t len;            /* codeword bytes */
+    uint32_t passes;         /* coding passes (all of them) */
+    uint32_t zero_bitplanes; /* Mb - coded bit-planes */
+    uint32_t status;         /* 0 ok, 1 bad descriptor, 2 magnitude above
+                                2^Mb, 3 codeword longer than cap */
+} tc_t1_enc_result;
+
+/* Encode n code-blocks on the GPU, one warp each: block i's codeword (all
+ * coding passes, MQ FLUSH termination) goes to d_out + i*cap, its result to
+ * d_res[i].  Bit-exact with tc_t1_encode_block on the same quantised
+ * coefficients.  Stream-ordered. */
+int tc_t1_encode(tc_ctx *ctx, const tc_t1_enc_desc *d_desc, int n, const void *d_in,
+                 uint8_t *d_out, uint32_t cap, tc_t1_enc_result *d_res);
+
 /* Encode one code-block of quantised coefficients (row-major int32, w x h)
  * with the MQ coder, keeping the first `passes` coding passes (0 or more
  * than available = all) and terminating the codeword there.  Returns the

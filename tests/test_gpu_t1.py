@@ -147,3 +147,62 @@ def test_standalone_dequantiser_matches_oracle(gpu_ctx, irreversible):
             np.testing.assert_array_equal(got[i, :h, :w].view(np.int32), want.view(np.int32))
         else:
             np.testing.assert_array_equal(got[i, :h, :w], O.dequant_int(q, uu, 0.5))
+
+
+def _enc_blocks(seed, n):
+    """n blocks of quantised Laplacian coefficients in 64x64 slots of one
+    int32 plane (64 wide), with their encoder descriptors and the host
+    encoder's (codeword, passes, zero bit-planes) for each."""
+    from thousandthchicken_b200.synth import laplacian_block
+    rng = np.random.default_rng(seed)
+    plane = np.zeros((n * 64, 64), np.int32)
+    desc = np.zeros(n, codec.ENC_DESC_DTYPE)
+    want = []
+    for i in range(n):
+        r = rng.random()
+        w, h = (64, 64) if r < 0.5 else ((32, 32) if r < 0.8 else (int(rng.integers(1, 65)), int(rng.integers(1, 65))))
+        orient = int(rng.integers(0, 4))
+        coef = laplacian_block(rng, w, h, bitplanes=int(rng.integers(1, 15)))
+        if rng.random() < 0.05:
+            coef[:] = 0  # an empty block
+        mb = 16
+        plane[i * 64:i * 64 + h, :w] = coef
+        d = desc[i]
+        d["in_off"], d["in_pitch"], d["w"], d["h"], d["orient"], d["mb"] = i * 64 * 64, 64, w, h, orient, mb
+        seg, passes, zbp = codec.t1_encode_block(coef, orient, mb)
+        want.append((seg, passes, zbp))
+    return desc, plane, want
+
+
+def test_gpu_encoder_matches_host_encoder(gpu_ctx):
+    """The GPU Tier-1 encoder (one warp per block, flag-word contexts,
+    register MQ encoder) writes, block for block, the host encoder's
+    codeword, pass count and zero bit-planes; and the GPU decoder reads the
+    GPU codewords back to the coefficients."""
+    from thousandthchicken_b200.stages import T1Encoder
+    desc, plane, want = _enc_blocks(seed=41, n=400)
+    got = T1Encoder(gpu_ctx).encode(desc, torch.from_numpy(plane.reshape(-1)).cuda())
+    for i, (g, w_) in enumerate(zip(got, want)):
+        assert g[1:] == w_[1:] or (w_[0] == b"" and g[0] == b""), (i, g[1:], w_[1:])
+        assert g[0] == w_[0], i
+    # decode the GPU codewords with the GPU decoder: the coefficients come back
+    ddesc = np.zeros(len(desc), codec.DESC_DTYPE)
+    pool, off = [], 0
+    for i, (seg, passes, zbp) in enumerate(got):
+        d = ddesc[i]
+        d["seg_off"], d["seg_len"] = off, len(seg)
+        d["w"], d["h"], d["passes"], d["mb"], d["zero_bitplanes"] = desc["w"][i], desc["h"][i], passes, 16, zbp
+        d["orient"], d["out_off"], d["out_pitch"], d["step"] = desc["orient"][i], i * 4096, 64, 1.0
+        pool.append(seg)
+        off += len(seg)
+    pool = np.frombuffer(b"".join(pool) + b"\0" * 16, np.uint8).copy()
+    back = _coder(gpu_ctx).decode_blocks(ddesc, pool, len(desc) * 4096, recon_r=0.0).cpu().numpy()
+    np.testing.assert_array_equal(back.reshape(-1, 64), plane)
+
+
+def test_gpu_encoder_flags_a_short_buffer(gpu_ctx):
+    from thousandthchicken_b200._lib import TCError
+    from thousandthchicken_b200.stages import T1Encoder
+    desc, plane, _ = _enc_blocks(seed=42, n=8)
+    with pytest.raises(TCError):
+        T1Encoder(gpu_ctx).encode(desc, torch.from_numpy(plane.reshape(-1)).cuda(), cap=16)

@@ -35,6 +35,13 @@ def read_header(cs) -> dict:
     return _info_dict(info)
 
 
+# tc_t1_enc_desc / tc_t1_enc_result (tc_j2k.h)
+ENC_DESC_DTYPE = np.dtype([("in_off", "<u8"), ("in_pitch", "<u4"), ("inv_step", "<f4"), ("w", "<u2"), ("h", "<u2"),
+                           ("orient", "u1"), ("mb", "u1"), ("flags", "u1"), ("reserved", "u1")])
+ENC_RESULT_DTYPE = np.dtype([("len", "<u4"), ("passes", "<u4"), ("zero_bitplanes", "<u4"), ("status", "<u4")])
+assert ENC_DESC_DTYPE.itemsize == 24 and ENC_RESULT_DTYPE.itemsize == 16
+
+
 def parse(cs):
     """Parse a codestream: returns (info dict, descriptor array, segment pool).
     info["tiles"] lists each tile as (x0, y0, w, h, coef_off): its region of

@@ -1201,6 +1201,16 @@ int tc_encode_j2k(const tc_encode_params *p, const void *h_planes, uint8_t *h_ou
     return TC_OK;
 }
 
+int tc_t1_encode(tc_ctx *ctx, const tc_t1_enc_desc *d_desc, int n, const void *d_in, uint8_t *d_out, uint32_t cap,
+                 tc_t1_enc_result *d_res)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (n < 0 || (n > 0 && (!d_desc || !d_in || !d_out || !d_res || cap == 0)))
+        return fail(ctx, TC_E_ARG, "tc_t1_encode: bad argument");
+    return cuda_status(ctx, launch_t1_encode(ctx, d_desc, n, d_in, d_out, cap, d_res), "tc_t1_encode");
+}
+
 int tc_t1_encode_block(const int32_t *h_coef, int w, int h, int orient, int mb, int passes, uint8_t *h_out, int cap,
                        int *len, int *passes_out, int *zero_bitplanes)
 {

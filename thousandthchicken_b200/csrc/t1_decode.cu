@@ -31,43 +31,16 @@
 #include <climits>
 #include <type_traits>
 
+#include "t1_common.cuh"
 #include "tc_internal.cuh"
 
 namespace tc {
 namespace {
 
-constexpr int kMaxStripes = 16;    // 64 rows
 #ifndef TC_T1_BLOCKS8
 #define TC_T1_BLOCKS8 8
 #endif
 constexpr int kBlocks8 = TC_T1_BLOCKS8;  // code-blocks per CTA of the 8-bit class
-constexpr int kSgnCols = 66;       // 64 columns + a zero column on each side
-
-// Flag word layout (one per stripe column):
-//   bits 0-17  significance, bit 3*j + col for row j-1 of the stripe
-//              (j = 0..5, rows -1..4) and col 0 = left, 1 = this, 2 = right
-//   bits 18-21 pi: coded in this plane's significance propagation pass
-//   bits 22-25 sigma': refined at least once
-constexpr uint32_t kSigMask = 0x3FFFFu;
-__device__ __forceinline__ uint32_t self_bit(int k) { return 1u << (3 * k + 4); }
-__device__ __forceinline__ uint32_t pi_bit(int k) { return 1u << (18 + k); }
-__device__ __forceinline__ uint32_t ref_bit(int k) { return 1u << (22 + k); }
-
-// ISO Table C.2 (coefficient_coder.cl:36-60).
-__constant__ uint16_t c_qe[47] = {
-    0x5601, 0x3401, 0x1801, 0x0AC1, 0x0521, 0x0221, 0x5601, 0x5401, 0x4801, 0x3801,
-    0x3001, 0x2401, 0x1C01, 0x1601, 0x5601, 0x5401, 0x5101, 0x4801, 0x3801, 0x3401,
-    0x3001, 0x2801, 0x2401, 0x2201, 0x1C01, 0x1801, 0x1601, 0x1401, 0x1201, 0x1101,
-    0x0AC1, 0x09C1, 0x08A1, 0x0521, 0x0441, 0x02A1, 0x0221, 0x0141, 0x0111, 0x0085,
-    0x0049, 0x0025, 0x0015, 0x0009, 0x0005, 0x0001, 0x5601};
-__constant__ uint8_t c_nmps[47] = {
-    1, 2, 3, 4, 5, 38, 7, 8, 9, 10, 11, 12, 13, 29, 15, 16, 17, 18, 19, 20,
-    21, 22, 23, 24, 25, 26, 27, 28, 29, 30, 31, 32, 33, 34, 35, 36, 37, 38, 39, 40,
-    41, 42, 43, 44, 45, 45, 46};
-__constant__ uint8_t c_nlps[47] = {
-    1, 6, 9, 12, 29, 33, 6, 14, 14, 14, 17, 18, 20, 21, 14, 14, 15, 16, 17, 18,
-    19, 19, 20, 21, 22, 23, 24, 25, 26, 27, 28, 29, 30, 31, 32, 33, 34, 35, 36, 37,
-    38, 39, 40, 41, 42, 43, 46};
 
 template <typename MagT>
 struct WarpState {
@@ -78,66 +51,6 @@ struct WarpState {
     uint8_t mctx[64];                      // refinement pass: 2-bit context code per row
     MagT mag[64 * 64];                     // magnitude bits decoded so far
 };
-
-struct Tables {
-    uint32_t mq[48];          // packed states: Qe << 16 | NMPS << 1 | NLPS << 7 | SWITCH << 13 (bit 0: MPS)
-    uint8_t zc[4][512];       // zero-coding label per orientation and 3x3 neighbourhood
-    uint8_t sc[256];          // sign label | XOR bit << 4
-};
-
-// Zero-coding label from neighbour counts, ISO Table D.1 (the reference's
-// SPCXLUT, coefficient_coder.cl:330-393).
-__device__ int zc_label(int orient, int h, int v, int d)
-{
-    if (orient == 1) { const int t = h; h = v; v = t; }
-    if (orient == 3) {
-        const int hv = h + v;
-        if (d >= 3) return 8;
-        if (d == 2) return hv >= 1 ? 7 : 6;
-        if (d == 1) return hv >= 2 ? 5 : (hv == 1 ? 4 : 3);
-        return hv >= 2 ? 2 : hv;
-    }
-    if (h == 2) return 8;
-    if (h == 1) return v >= 1 ? 7 : (d >= 1 ? 6 : 5);
-    if (v == 2) return 4;
-    if (v == 1) return 3;
-    return d >= 2 ? 2 : d;
-}
-
-__device__ void build_tables(Tables &t)
-{
-    for (int i = threadIdx.x; i < 47; i += blockDim.x)
-        t.mq[i] = ((uint32_t)c_qe[i] << 16) | ((uint32_t)c_nmps[i] << 1) | ((uint32_t)c_nlps[i] << 7) |
-                  ((uint32_t)(i == 0 || i == 6 || i == 14) << 13);
-    // 3x3 neighbourhood bits: 0 up-left 1 up 2 up-right 3 left 4 self
-    // 5 right 6 down-left 7 down 8 down-right.
-    for (int i = threadIdx.x; i < 4 * 512; i += blockDim.x) {
-        const int o = i >> 9, p = i & 511;
-        const int h = ((p >> 3) & 1) + ((p >> 5) & 1);
-        const int v = ((p >> 1) & 1) + ((p >> 7) & 1);
-        const int d = (p & 1) + ((p >> 2) & 1) + ((p >> 6) & 1) + ((p >> 8) & 1);
-        t.zc[o][p] = (uint8_t)zc_label(o, h, v, d);
-    }
-    // Sign index: neighbourhood bits 1,3,5,7 (significance of up, left,
-    // right, down) with the neighbours' signs one bit below them.
-    // ISO Tables D.2/D.3 (signcxlut, coefficient_coder.cl:406-435).
-    for (int i = threadIdx.x; i < 256; i += blockDim.x) {
-        auto ctb = [&](int sig, int neg) { return sig ? (neg ? -1 : 1) : 0; };
-        int vc = ctb((i >> 1) & 1, i & 1) + ctb((i >> 7) & 1, (i >> 6) & 1);
-        int hc = ctb((i >> 3) & 1, (i >> 2) & 1) + ctb((i >> 5) & 1, (i >> 4) & 1);
-        hc = hc > 1 ? 1 : (hc < -1 ? -1 : hc);
-        vc = vc > 1 ? 1 : (vc < -1 ? -1 : vc);
-        int cx, xr;
-        if (hc == 0) {
-            cx = vc == 0 ? 9 : 10;
-            xr = vc < 0;
-        } else {
-            cx = 12 + hc * vc;
-            xr = hc < 0;
-        }
-        t.sc[i] = (uint8_t)(cx | (xr << 4));
-    }
-}
 
 // MQ decoder (ISO C.3; bytein/renormd/mqDecode, coefficient_coder.cl:121-252).
 // The interval register A is kept scaled by 2^16 so that it lives in the same
@@ -219,62 +132,11 @@ struct MQ {
     }
 };
 
-// Sign-coding index of row y (= 4s+k) of column c from the flag word's
-// 3x3 neighbourhood n9 and the sign words of columns c-1, c, c+1.
-template <typename MagT>
-__device__ __forceinline__ uint32_t sign_index(const WarpState<MagT> &S, uint32_t n9, int c, int y)
-{
-    const unsigned long long sl = S.sgn[c], sc = S.sgn[c + 1], sr = S.sgn[c + 2];
-    const uint32_t up = y > 0 ? (uint32_t)(sc >> (y - 1)) & 1u : 0u;
-    const uint32_t dn = y < 63 ? (uint32_t)(sc >> (y + 1)) & 1u : 0u;
-    const uint32_t lf = (uint32_t)(sl >> y) & 1u, rt = (uint32_t)(sr >> y) & 1u;
-    return (n9 & 0xAAu) | up | (lf << 2) | (rt << 4) | (dn << 6);
-}
-
-// Record that row k of stripe s in column c became significant: the flag
-// words of the neighbouring columns and of the stripes above and below see
-// it through their neighbourhood bits.
-template <typename MagT>
-__device__ __forceinline__ void mark_significant(WarpState<MagT> &S, int s, int k, int c, int w, int nstripes,
-                                                 uint32_t neg)
-{
-    uint32_t *F = S.F;
-    const int i = s * 64 + c;
-    if (c > 0) F[i - 1] |= 1u << (3 * k + 5);
-    if (c + 1 < w) F[i + 1] |= 1u << (3 * k + 3);
-    if (k == 0 && s > 0) {
-        const int u = i - 64;
-        F[u] |= 1u << 16;
-        if (c > 0) F[u - 1] |= 1u << 17;
-        if (c + 1 < w) F[u + 1] |= 1u << 15;
-    }
-    if (k == 3 && s + 1 < nstripes) {
-        const int d = i + 64;
-        F[d] |= 1u << 1;
-        if (c > 0) F[d - 1] |= 1u << 2;
-        if (c + 1 < w) F[d + 1] |= 1u << 0;
-    }
-    if (neg) S.sgn[c + 1] |= 1ull << (4 * s + k);
-}
-
 // Decode one code-block.  Every lane of the warp runs this function in
 // lock-step; lanes split the per-stripe candidate searches between them
 // (lane l owns columns l and l+32) and the serial loop visits only candidate
 // columns, in scan order.  Returns the last pass type (0 cleanup,
 // 1 significance propagation, 2 refinement) and its plane.
-// Candidate mask of the group's columns: column gl + G*j for predicate any[j].
-template <int G>
-__device__ __forceinline__ unsigned long long group_ballot(const bool (&any)[64 / G], unsigned gmask, int gshift)
-{
-    unsigned long long m = 0;
-#pragma unroll
-    for (int j = 0; j < 64 / G; j++) {
-        const unsigned b = __ballot_sync(gmask, any[j]);
-        m |= (unsigned long long)((G == 32 ? b : (b >> gshift)) & (G == 32 ? 0xffffffffu : ((1u << G) - 1u))) << (G * j);
-    }
-    return m;
-}
-
 template <typename MagT, int G>
 __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *seg, int len, int w,
                             int h, int orient, int numbps, int passes, int *last_plane, int lane, unsigned gmask,
@@ -323,10 +185,10 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
                         f |= pi_bit(k);
                         if (mq.decode(ctx, tbl, zc[n9])) {
                             const int y = 4 * s + k;
-                            const uint32_t si = T.sc[sign_index(S, n9, c, y)];
+                            const uint32_t si = T.sc[sign_index(S.sgn, n9, c, y)];
                             const uint32_t neg = (uint32_t)mq.decode(ctx, tbl, si & 15) ^ (si >> 4);
                             f |= self_bit(k);
-                            mark_significant(S, s, k, c, w, nstripes, neg);
+                            mark_significant(S.F, S.sgn, s, k, c, w, nstripes, neg);
                             S.mag[y * 64 + c] = pbit;
                             if (c + 1 < w) cand |= 1ull << (c + 1);  // the next column gained a neighbour
                         }
@@ -414,10 +276,10 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
                     int r = mq.decode(ctx, tbl, 17) << 1;
                     r |= mq.decode(ctx, tbl, 17);
                     const int y = 4 * s + r;
-                    const uint32_t si = T.sc[sign_index(S, (f >> (3 * r)) & 0x1FFu, c, y)];
+                    const uint32_t si = T.sc[sign_index(S.sgn, (f >> (3 * r)) & 0x1FFu, c, y)];
                     const uint32_t neg = (uint32_t)mq.decode(ctx, tbl, si & 15) ^ (si >> 4);
                     f |= self_bit(r);
-                    mark_significant(S, s, r, c, w, nstripes, neg);
+                    mark_significant(S.F, S.sgn, s, r, c, w, nstripes, neg);
                     S.mag[y * 64 + c] = pbit;
                     k = r + 1;
                 }
@@ -426,10 +288,10 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
                     const uint32_t n9 = (f >> (3 * k)) & 0x1FFu;
                     if (mq.decode(ctx, tbl, zc[n9])) {
                         const int y = 4 * s + k;
-                        const uint32_t si = T.sc[sign_index(S, n9, c, y)];
+                        const uint32_t si = T.sc[sign_index(S.sgn, n9, c, y)];
                         const uint32_t neg = (uint32_t)mq.decode(ctx, tbl, si & 15) ^ (si >> 4);
                         f |= self_bit(k);
-                        mark_significant(S, s, k, c, w, nstripes, neg);
+                        mark_significant(S.F, S.sgn, s, k, c, w, nstripes, neg);
                         S.mag[y * 64 + c] = pbit;
                     }
                 }

@@ -127,6 +127,8 @@ cudaError_t launch_t1_classes(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uin
 void t1_class_order(const tc_cblk_desc *h_desc, int n, uint32_t *h_order, int counts[3]);
 cudaError_t launch_dequant_raw(tc_ctx *ctx, const tc_cblk_desc *d_desc, int n,
                                const uint32_t *d_raw, void *d_out, float recon_r);
+cudaError_t launch_t1_encode(tc_ctx *ctx, const tc_t1_enc_desc *d_desc, int n, const void *d_in, uint8_t *d_out,
+                             uint32_t cap, tc_t1_enc_result *d_res);
 
 // One 2-D DWT level over up to 4 components of equal size.
 struct LevelIO {

@@ -122,6 +122,40 @@ class CoefficientCoder:
         return out.view(info["ncomp"], info["height"], info["width"]), info
 
 
+class T1Encoder:
+    """GPU Tier-1 encoder (tc_t1_encode): code-blocks of a device plane set
+    -> codewords, bit-exact with the host encoder (codec.t1_encode_block)."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+
+    def encode(self, desc: np.ndarray, planes, cap: int = 0):
+        """desc: ENC_DESC_DTYPE rows addressing `planes` (a device tensor of
+        int32 quantised coefficients, or float32 with TC_CBLK_IRREVERSIBLE).
+        Returns a list of (codeword bytes, passes, zero_bitplanes)."""
+        from .codec import ENC_DESC_DTYPE, ENC_RESULT_DTYPE
+        dev = torch.device("cuda", self.ctx.device)
+        desc = np.ascontiguousarray(desc, ENC_DESC_DTYPE)
+        n = len(desc)
+        if n == 0:
+            return []
+        if cap <= 0:
+            cap = int(max(4096, 8 * int(desc["w"].max()) * int(desc["h"].max())))
+        d_desc = _dev_bytes(desc, dev)
+        out = torch.empty(n * cap, dtype=torch.uint8, device=dev)
+        res = torch.empty(n * ENC_RESULT_DTYPE.itemsize, dtype=torch.uint8, device=dev)
+        self.ctx.check(L.lib().tc_t1_encode(self.ctx.handle, _ptr(d_desc), n, _ptr(planes), _ptr(out), cap,
+                                            _ptr(res)), "tc_t1_encode")
+        self.ctx.synchronize()
+        r = res.cpu().numpy().view(ENC_RESULT_DTYPE)
+        if (r["status"] != 0).any():
+            bad = int(np.nonzero(r["status"])[0][0])
+            raise L.TCError(L.TC_E_ARG, f"tc_t1_encode: block {bad} status {int(r['status'][bad])}")
+        data = out.cpu().numpy()
+        return [(data[i * cap:i * cap + int(r["len"][i])].tobytes(), int(r["passes"][i]), int(r["zero_bitplanes"][i]))
+                for i in range(n)]
+
+
 class Quantizer:
     """Standalone inverse quantiser over raw Tier-1 words
     (Quantizer::dequantize_tile, Quantizer.cpp:181-216)."""
