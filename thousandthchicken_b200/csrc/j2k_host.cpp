@@ -1557,8 +1557,7 @@ static int parse_raw_codestream(const uint8_t *cs, size_t len, Parsed &out, std:
 
 // ============================ encoder =======================================
 
-int encode_codestream(const tc_encode_params &p, const void *planes, std::vector<uint8_t> &out,
-                      std::string &err)
+int encode_layout(const tc_encode_params &p, EncodeLayout &L, std::string &err)
 {
     const int W = p.width, H = p.height, C = p.ncomp, B = p.bits, NL = p.levels;
     if (W < 1 || H < 1 || W > 65535 || H > 65535 || C < 1 || C > 4 || B < 1 || B > 16 || NL < 0 ||
@@ -1567,6 +1566,59 @@ int encode_codestream(const tc_encode_params &p, const void *planes, std::vector
         return TC_E_ARG;
     }
     if (!p.reversible && !(p.base_step > 0.0)) { err = "base_step must be positive"; return TC_E_ARG; }
+    // Per component: code-block size (COC when it differs from COD) and
+    // step multiplier (QCC when it differs from QCD).
+    for (int c = 0; c < C; c++) {
+        L.cblk[c] = p.comp_cblk_log2[c] > 0 ? p.comp_cblk_log2[c] : p.cblk_log2;
+        L.scale[c] = p.comp_step_scale[c] > 0.0 ? p.comp_step_scale[c] : 1.0;
+        if (L.cblk[c] < 2 || L.cblk[c] > 6) { err = "code-block size out of range"; return TC_E_ARG; }
+    }
+    L.geo.assign(C, {});
+    for (int c = 0; c < C; c++) L.geo[c] = make_geometry(W, H, NL, L.cblk[c], L.cblk[c]);
+    // Quantisation exponent / mantissa / step per band (ISO E.1).
+    for (int c = 0; c < C; c++)
+        for (int r = 0; r <= NL; r++)
+            for (Band &b : L.geo[c][r].bands) {
+                const int rb = B + band_gain_log2(b.orient);
+                if (p.reversible) {
+                    b.eps = rb;
+                    b.mu = 0;
+                    b.step = 1.0f;
+                } else {
+                    const double delta =
+                        L.scale[c] * p.base_step * std::ldexp(1.0, B) / subband_norm(true, b.level, b.orient);
+                    int e = rb - (int)std::floor(std::log2(delta));
+                    int m = (int)std::lround((delta / std::ldexp(1.0, rb - e) - 1.0) * 2048.0);
+                    if (m >= 2048) { m = 0; e--; }
+                    if (m < 0) m = 0;
+                    if (e < 0 || e > 31) { err = "quantisation step out of range"; return TC_E_ARG; }
+                    b.eps = e;
+                    b.mu = m;
+                    b.step = (float)std::ldexp(1.0 + m / 2048.0, rb - e);
+                }
+            }
+    // Code-blocks in packet order.
+    L.jobs.clear();
+    for (int c = 0; c < C; c++)
+        for (int r = 0; r <= NL; r++)
+            for (int bi = 0; bi < (int)L.geo[c][r].bands.size(); bi++) {
+                const Band &b = L.geo[c][r].bands[bi];
+                for (int j = 0; j < b.ncby; j++)
+                    for (int i = 0; i < b.ncbx; i++) L.jobs.push_back({c, r, bi, i, j});
+            }
+    return TC_OK;
+}
+
+// The host encoder: colour transform and DWT on the CPU (double precision
+// for 9/7), deadzone quantisation, Tier-1 per code-block, then
+// encode_assemble.
+int encode_codestream(const tc_encode_params &p, const void *planes, std::vector<uint8_t> &out,
+                      std::string &err)
+{
+    EncodeLayout L;
+    int rc = encode_layout(p, L, err);
+    if (rc) return rc;
+    const int W = p.width, H = p.height, C = p.ncomp, B = p.bits, NL = p.levels;
     const bool mct = p.mct && C >= 3;
     const int threads = p.threads;
     const size_t np = (size_t)W * H;
@@ -1608,41 +1660,11 @@ int encode_codestream(const tc_encode_params &p, const void *planes, std::vector
             fwd_plane_pitch(dp.data() + c * np, W, H, (size_t)W, NL, fwd97_line, threads);
     }
 
-    // Per component: code-block size (COC when it differs from COD) and
-    // step multiplier (QCC when it differs from QCD).
-    int cblk[4];
-    double scale[4];
-    for (int c = 0; c < C; c++) {
-        cblk[c] = p.comp_cblk_log2[c] > 0 ? p.comp_cblk_log2[c] : p.cblk_log2;
-        scale[c] = p.comp_step_scale[c] > 0.0 ? p.comp_step_scale[c] : 1.0;
-        if (cblk[c] < 2 || cblk[c] > 6) { err = "code-block size out of range"; return TC_E_ARG; }
-    }
-    std::vector<std::vector<Resolution>> geo(C);
-    for (int c = 0; c < C; c++) geo[c] = make_geometry(W, H, NL, cblk[c], cblk[c]);
-    // Quantisation: exponent/mantissa per band, quantised coefficients.
+    // Quantised coefficients.
     std::vector<int32_t> q(np * C);
-    int need_guard = 1;
     for (int c = 0; c < C; c++)
         for (int r = 0; r <= NL; r++)
-            for (Band &b : geo[c][r].bands) {
-                const int rb = B + band_gain_log2(b.orient);
-                if (p.reversible) {
-                    b.eps = rb;
-                    b.mu = 0;
-                    b.step = 1.0f;
-                } else {
-                    const double delta =
-                        scale[c] * p.base_step * std::ldexp(1.0, B) / subband_norm(true, b.level, b.orient);
-                    int e = rb - (int)std::floor(std::log2(delta));
-                    int m = (int)std::lround((delta / std::ldexp(1.0, rb - e) - 1.0) * 2048.0);
-                    if (m >= 2048) { m = 0; e--; }
-                    if (m < 0) m = 0;
-                    if (e < 0 || e > 31) { err = "quantisation step out of range"; return TC_E_ARG; }
-                    b.eps = e;
-                    b.mu = m;
-                    b.step = (float)std::ldexp(1.0 + m / 2048.0, rb - e);
-                }
-                uint32_t mx = 0;
+            for (const Band &b : L.geo[c][r].bands)
                 for (int y = b.y0; y < b.y0 + b.h; y++)
                     for (int x = b.x0; x < b.x0 + b.w; x++) {
                         const size_t i = c * np + (size_t)y * W + x;
@@ -1655,12 +1677,53 @@ int encode_codestream(const tc_encode_params &p, const void *planes, std::vector
                             if (dp[i] < 0) v = -v;
                         }
                         q[i] = v;
-                        mx = std::max(mx, (uint32_t)std::abs((int64_t)v));
                     }
-                int nb = 0;
-                while (nb < 32 && (mx >> nb)) nb++;
-                need_guard = std::max(need_guard, nb - b.eps + 1);
-            }
+
+    // Tier-1: every code-block with all passes; the codeword does not
+    // depend on Mb, so the blocks are coded before the guard bits are known.
+    std::vector<CodedBlock> coded(L.jobs.size());
+    std::atomic<int> fail{0};
+    parallel_for((int)L.jobs.size(), threads, [&](int k) {
+        const EncodeLayout::Job &jb = L.jobs[k];
+        const Band &b = L.geo[jb.c][jb.r].bands[jb.bi];
+        const int cx = jb.i << b.cbw_log2, cy = jb.j << b.cbh_log2;
+        const int bw = std::min(1 << b.cbw_log2, b.w - cx), bh = std::min(1 << b.cbh_log2, b.h - cy);
+        int32_t blk[64 * 64];
+        for (int y = 0; y < bh; y++)
+            for (int x = 0; x < bw; x++)
+                blk[y * bw + x] = q[jb.c * np + (size_t)(b.y0 + cy + y) * W + b.x0 + cx + x];
+        int zbp = 0;
+        if (t1_encode_block(blk, bw, bh, b.orient, 31, 0, coded[k].data, &coded[k].passes, &zbp)) fail = 1;
+        coded[k].numbps = 31 - zbp;
+    });
+    if (fail) { err = "Tier-1 encoding failed"; return TC_E_ARG; }
+    return encode_assemble(p, L, coded, out, err);
+}
+
+int encode_assemble(const tc_encode_params &p, EncodeLayout &L, const std::vector<CodedBlock> &coded,
+                    std::vector<uint8_t> &out, std::string &err)
+{
+    const int W = p.width, H = p.height, C = p.ncomp, B = p.bits, NL = p.levels;
+    const bool mct = p.mct && C >= 3;
+    const bool sgn = p.is_signed != 0;
+    auto &geo = L.geo;
+    const int *cblk = L.cblk;
+    const double *scale = L.scale;
+    const auto &jobs = L.jobs;
+    if (coded.size() != jobs.size()) { err = "coded block count does not match the layout"; return TC_E_ARG; }
+    // Guard bits (ISO E.1): enough for every band's largest magnitude.
+    std::vector<std::vector<std::vector<int>>> band_bps(C, std::vector<std::vector<int>>(NL + 1));
+    for (int c = 0; c < C; c++)
+        for (int r = 0; r <= NL; r++) band_bps[c][r].assign(geo[c][r].bands.size(), 0);
+    for (size_t k = 0; k < jobs.size(); k++) {
+        int &m = band_bps[jobs[k].c][jobs[k].r][jobs[k].bi];
+        m = std::max(m, coded[k].numbps);
+    }
+    int need_guard = 1;
+    for (int c = 0; c < C; c++)
+        for (int r = 0; r <= NL; r++)
+            for (size_t bi = 0; bi < geo[c][r].bands.size(); bi++)
+                need_guard = std::max(need_guard, band_bps[c][r][bi] - geo[c][r].bands[bi].eps + 1);
     int G = p.guard_bits > 0 ? p.guard_bits : std::max(2, need_guard);
     if (G < need_guard || G > 7) { err = "guard bits cannot hold the coefficient range"; return TC_E_ARG; }
     for (int c = 0; c < C; c++)
@@ -1669,38 +1732,10 @@ int encode_codestream(const tc_encode_params &p, const void *planes, std::vector
                 b.mb = G + b.eps - 1;
                 if (b.mb > 31) { err = "more than 31 magnitude bit-planes"; return TC_E_ARG; }
             }
-
-    // Tier-1: encode every code-block.
-    struct Job {
-        int c, r, bi, i, j;
-    };
-    std::vector<Job> jobs;
-    for (int c = 0; c < C; c++)
-        for (int r = 0; r <= NL; r++)
-            for (int bi = 0; bi < (int)geo[c][r].bands.size(); bi++) {
-                const Band &b = geo[c][r].bands[bi];
-                for (int j = 0; j < b.ncby; j++)
-                    for (int i = 0; i < b.ncbx; i++) jobs.push_back({c, r, bi, i, j});
-            }
-    struct Coded {
-        std::vector<uint8_t> data;
-        int passes = 0, zbp = 0;
-    };
-    std::vector<Coded> coded(jobs.size());
-    std::atomic<int> fail{0};
-    parallel_for((int)jobs.size(), threads, [&](int k) {
-        const Job &jb = jobs[k];
-        const Band &b = geo[jb.c][jb.r].bands[jb.bi];
-        const int cx = jb.i << b.cbw_log2, cy = jb.j << b.cbh_log2;
-        const int bw = std::min(1 << b.cbw_log2, b.w - cx), bh = std::min(1 << b.cbh_log2, b.h - cy);
-        int32_t blk[64 * 64];
-        for (int y = 0; y < bh; y++)
-            for (int x = 0; x < bw; x++)
-                blk[y * bw + x] = q[jb.c * np + (size_t)(b.y0 + cy + y) * W + b.x0 + cx + x];
-        if (t1_encode_block(blk, bw, bh, b.orient, b.mb, 0, coded[k].data, &coded[k].passes, &coded[k].zbp))
-            fail = 1;
-    });
-    if (fail) { err = "Tier-1 encoding failed"; return TC_E_ARG; }
+    std::vector<int> zbps(jobs.size());
+    for (size_t k = 0; k < jobs.size(); k++)
+        zbps[k] = geo[jobs[k].c][jobs[k].r].bands[jobs[k].bi].mb - coded[k].numbps;
+    const size_t np = (size_t)W * H;
 
     // Index jobs by (c, r, bi) for the packet writer.
     std::vector<std::vector<std::vector<int>>> first(C, std::vector<std::vector<int>>(NL + 1));
@@ -1739,15 +1774,15 @@ int encode_codestream(const tc_encode_params &p, const void *planes, std::vector
             std::vector<int> iv(n), zv(n);
             for (int i = 0; i < n; i++) {
                 iv[i] = coded[k0 + i].passes > 0 ? 0 : 1;
-                zv[i] = coded[k0 + i].zbp;
+                zv[i] = zbps[k0 + i];
             }
             incl.set_leaves(iv);
             zt.set_leaves(zv);
             for (int i = 0; i < n; i++) {
-                const Coded &cd = coded[k0 + i];
+                const CodedBlock &cd = coded[k0 + i];
                 incl.encode(bw, i, 1);
                 if (cd.passes == 0) continue;
-                zt.encode(bw, i, cd.zbp + 1);
+                zt.encode(bw, i, zbps[k0 + i] + 1);
                 put_num_passes(bw, cd.passes);
                 const int len = (int)cd.data.size();
                 int lblock = 3, incr = 0;

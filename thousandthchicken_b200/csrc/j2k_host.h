@@ -65,6 +65,28 @@ int parse_codestream(const uint8_t *cs, size_t len, Parsed &out, std::string &er
 int read_header(const uint8_t *cs, size_t len, tc_image_info &info, std::string &err);
 
 // ---- encoder ------------------------------------------------------------------
+// Layout of a codestream to encode: per component the code-block size, step
+// multiplier and subband geometry with its quantisation (eps, mu, step),
+// and the code-blocks in packet order.
+struct EncodeLayout {
+    int cblk[4] = {6, 6, 6, 6};
+    double scale[4] = {1, 1, 1, 1};
+    std::vector<std::vector<Resolution>> geo;  // per component
+    struct Job {
+        int c, r, bi, i, j;  // component, resolution, band, block column, block row
+    };
+    std::vector<Job> jobs;
+};
+// One code-block coded with all passes (its codeword does not depend on Mb).
+struct CodedBlock {
+    std::vector<uint8_t> data;
+    int passes = 0, numbps = 0;
+};
+int encode_layout(const tc_encode_params &p, EncodeLayout &L, std::string &err);
+// Guard bits from the blocks' bit-planes (unless p.guard_bits is set), Mb
+// per band, zero bit-planes per block, packets and headers.
+int encode_assemble(const tc_encode_params &p, EncodeLayout &L, const std::vector<CodedBlock> &coded,
+                    std::vector<uint8_t> &out, std::string &err);
 int encode_codestream(const tc_encode_params &p, const void *planes, std::vector<uint8_t> &out,
                       std::string &err);
 
