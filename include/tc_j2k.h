@@ -381,6 +381,16 @@ typedef struct tc_t1_enc_result {
                                 2^Mb, 3 codeword longer than cap */
 } tc_t1_enc_result;
 
+/* The whole encoder on the GPU: the forward colour transform with the DC
+ * shift, the forward DWT levels, deadzone quantisation and Tier-1 per
+ * code-block run as kernels; the host assembles packets and headers from
+ * the codewords (as tc_encode_j2k does).  Lossless output is byte-identical
+ * to tc_encode_j2k's; lossy output differs only where the fp32 DWT of the
+ * GPU and the fp64 one of the host quantise a coefficient differently.
+ * Same parameters and output as tc_encode_j2k. */
+int tc_encode_j2k_gpu(tc_ctx *ctx, const tc_encode_params *p, const void *h_planes,
+                      uint8_t *h_out, size_t cap, size_t *out_len);
+
 /* Encode n code-blocks on the GPU, one warp each: block i's codeword (all
  * coding passes, MQ FLUSH termination) goes to d_out + i*cap, its result to
  * d_res[i].  Bit-exact with tc_t1_encode_block on the same quantised

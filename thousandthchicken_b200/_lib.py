@@ -122,6 +122,7 @@ _PROTOS = {
     "tc_t1_encode_block": (_I, [_VP, _I, _I, _I, _I, _I, _VP, _I, C.POINTER(_I), C.POINTER(_I),
                                 C.POINTER(_I)]),
     "tc_t1_encode": (_I, [_VP, _VP, _I, _VP, _VP, C.c_uint32, _VP]),
+    "tc_encode_j2k_gpu": (_I, [_VP, C.POINTER(EncodeParams), _VP, _VP, C.c_size_t, C.POINTER(C.c_size_t)]),
 }
 
 _lib = None

@@ -69,14 +69,8 @@ def parse(cs):
     return info, desc, pool
 
 
-def encode(planes: np.ndarray, bits: int, levels: int = 5, reversible: bool = True, mct: bool = True,
-           cblk_log2: int = 6, base_step: float = 1.0 / 128, guard_bits: int = 0, progression: int = 0,
-           threads: int = 0, comp_cblk_log2=None, comp_step_scale=None) -> bytes:
-    """Harness encoder: planar samples [ncomp, h, w] -> codestream; signed
-    integer arrays (int8 / int16) give signed components (no DC shift).
-    comp_cblk_log2 / comp_step_scale: per-component code-block size exponent
-    and irreversible step multiplier (0 = the image-wide value), written as
-    COC / QCC marker segments."""
+def _encode_params(planes, bits, levels, reversible, mct, cblk_log2, base_step, guard_bits, progression, threads,
+                   comp_cblk_log2, comp_step_scale):
     signed = np.asarray(planes).dtype.kind == "i"
     if signed:
         planes = np.ascontiguousarray(planes, np.int8 if bits <= 8 else np.int16)
@@ -92,6 +86,35 @@ def encode(planes: np.ndarray, bits: int, levels: int = 5, reversible: bool = Tr
         p.comp_cblk_log2[c] = int(v)
     for c, v in enumerate(comp_step_scale or []):
         p.comp_step_scale[c] = float(v)
+    return planes, p
+
+
+def encode_gpu(ctx, planes: np.ndarray, bits: int, levels: int = 5, reversible: bool = True, mct: bool = True,
+               cblk_log2: int = 6, base_step: float = 1.0 / 128, guard_bits: int = 0, progression: int = 0,
+               comp_cblk_log2=None, comp_step_scale=None) -> bytes:
+    """The encoder on the GPU (tc_encode_j2k_gpu): colour transform, DWT,
+    quantisation and Tier-1 as kernels on ctx's device, packets on the
+    host.  Same parameters as encode; lossless output is byte-identical."""
+    planes, p = _encode_params(planes, bits, levels, reversible, mct, cblk_log2, base_step, guard_bits, progression,
+                               0, comp_cblk_log2, comp_step_scale)
+    cap = planes.nbytes * 3 + 65536
+    out = np.empty(cap, np.uint8)
+    n = C.c_size_t(0)
+    ctx.check(L.lib().tc_encode_j2k_gpu(ctx.handle, C.byref(p), planes.ctypes.data, out.ctypes.data, cap,
+                                        C.byref(n)), "tc_encode_j2k_gpu")
+    return out[: n.value].tobytes()
+
+
+def encode(planes: np.ndarray, bits: int, levels: int = 5, reversible: bool = True, mct: bool = True,
+           cblk_log2: int = 6, base_step: float = 1.0 / 128, guard_bits: int = 0, progression: int = 0,
+           threads: int = 0, comp_cblk_log2=None, comp_step_scale=None) -> bytes:
+    """Harness encoder: planar samples [ncomp, h, w] -> codestream; signed
+    integer arrays (int8 / int16) give signed components (no DC shift).
+    comp_cblk_log2 / comp_step_scale: per-component code-block size exponent
+    and irreversible step multiplier (0 = the image-wide value), written as
+    COC / QCC marker segments."""
+    planes, p = _encode_params(planes, bits, levels, reversible, mct, cblk_log2, base_step, guard_bits, progression,
+                               threads, comp_cblk_log2, comp_step_scale)
     cap = planes.nbytes * 3 + 65536
     out = np.empty(cap, np.uint8)
     n = C.c_size_t(0)

@@ -1201,6 +1201,117 @@ int tc_encode_j2k(const tc_encode_params *p, const void *h_planes, uint8_t *h_ou
     return TC_OK;
 }
 
+int tc_encode_j2k_gpu(tc_ctx *ctx, const tc_encode_params *p, const void *h_planes, uint8_t *h_out, size_t cap,
+                      size_t *out_len)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!p || !h_planes || !out_len) return fail(ctx, TC_E_ARG, "tc_encode_j2k_gpu: bad argument");
+    std::string err;
+    EncodeLayout L;
+    if ((rc = encode_layout(*p, L, err))) return fail(ctx, rc, err);
+    const int W = p->width, H = p->height, C = p->ncomp, B = p->bits, NL = p->levels;
+    const size_t np = (size_t)W * H;
+    const int sb = B <= 8 ? 1 : 2;
+    const bool rev = p->reversible != 0;
+    const int nb = (int)L.jobs.size();
+    // worst case per block: about 1.2 decisions per sample per bit-plane over
+    // 31 bit-planes, at most one bit per decision, plus the termination
+    uint32_t bcap = 0;
+    for (int c = 0; c < C; c++) bcap = std::max<uint32_t>(bcap, 5u << (2 * L.cblk[c]));
+    bcap += 256;
+    DevBuf in, col, coef, desc, words, res, off, packed;
+    auto done = [&](int status) {
+        cudaStreamSynchronize(ctx->stream);
+        for (DevBuf *b : {&in, &col, &coef, &desc, &words, &res, &off, &packed}) b->release();
+        return status;
+    };
+    cudaError_t e;
+    if ((e = in.ensure(np * C * sb)) != cudaSuccess || (e = col.ensure(np * C * 4)) != cudaSuccess ||
+        (e = coef.ensure(np * C * 4)) != cudaSuccess ||
+        (e = desc.ensure(std::max(1, nb) * sizeof(tc_t1_enc_desc))) != cudaSuccess ||
+        (e = words.ensure((size_t)std::max(1, nb) * bcap)) != cudaSuccess ||
+        (e = res.ensure(std::max(1, nb) * sizeof(tc_t1_enc_result))) != cudaSuccess ||
+        (e = off.ensure(std::max(1, nb) * sizeof(uint64_t))) != cudaSuccess)
+        return done(cuda_status(ctx, e, "tc_encode_j2k_gpu allocation"));
+    if ((e = cudaMemcpyAsync(in.ptr, h_planes, np * C * sb, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess)
+        return done(cuda_status(ctx, e, "tc_encode_j2k_gpu upload"));
+    // forward colour transform with the DC shift (ISO G.1-G.2), per plane the DWT (ISO F.4)
+    const void *ip[4];
+    void *cp[4];
+    for (int c = 0; c < C; c++) {
+        ip[c] = static_cast<char *>(in.ptr) + c * np * sb;
+        cp[c] = static_cast<char *>(col.ptr) + c * np * 4;
+    }
+    const int kind = p->mct && C >= 3 ? (rev ? TC_COLOR_RCT : TC_COLOR_ICT) : TC_COLOR_DC;
+    e = launch_color_forward(ctx, kind, C, ip, sb == 1 ? TC_U8 : TC_U16, W, cp, rev ? TC_INT32 : TC_FLOAT32, W, W, H,
+                             B | (p->is_signed ? TC_SIGNED : 0));
+    if (e != cudaSuccess) return done(cuda_status(ctx, e, "tc_encode_j2k_gpu colour"));
+    for (int c = 0; c < C; c++) {
+        rc = dwt_forward(ctx, rev ? 0 : 1, TC_ROUND_FLOOR, cp[c], W, static_cast<char *>(coef.ptr) + c * np * 4, W,
+                         W, H, NL);
+        if (rc) return done(rc);
+    }
+    // Tier-1 of every block with Mb = 31 (the codeword does not depend on Mb)
+    std::vector<tc_t1_enc_desc> hd(nb);
+    for (int k = 0; k < nb; k++) {
+        const EncodeLayout::Job &jb = L.jobs[k];
+        const Band &b = L.geo[jb.c][jb.r].bands[jb.bi];
+        const int cx = jb.i << b.cbw_log2, cy = jb.j << b.cbh_log2;
+        tc_t1_enc_desc &d = hd[k];
+        std::memset(&d, 0, sizeof d);
+        d.in_off = (uint64_t)jb.c * np + (uint64_t)(b.y0 + cy) * W + (uint64_t)(b.x0 + cx);
+        d.in_pitch = (uint32_t)W;
+        d.w = (uint16_t)std::min(1 << b.cbw_log2, b.w - cx);
+        d.h = (uint16_t)std::min(1 << b.cbh_log2, b.h - cy);
+        d.orient = (uint8_t)b.orient;
+        d.mb = 31;
+        d.flags = rev ? 0 : TC_CBLK_IRREVERSIBLE;
+        d.inv_step = rev ? 1.0f : 1.0f / b.step;
+    }
+    std::vector<tc_t1_enc_result> hr(nb);
+    if ((e = cudaMemcpyAsync(desc.ptr, hd.data(), nb * sizeof(tc_t1_enc_desc), cudaMemcpyHostToDevice, ctx->stream)) !=
+            cudaSuccess ||
+        (e = launch_t1_encode(ctx, static_cast<tc_t1_enc_desc *>(desc.ptr), nb, coef.ptr,
+                              static_cast<uint8_t *>(words.ptr), bcap, static_cast<tc_t1_enc_result *>(res.ptr))) !=
+            cudaSuccess ||
+        (e = cudaMemcpyAsync(hr.data(), res.ptr, nb * sizeof(tc_t1_enc_result), cudaMemcpyDeviceToHost,
+                             ctx->stream)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess)
+        return done(cuda_status(ctx, e, "tc_encode_j2k_gpu Tier-1"));
+    // pack the codewords and bring them back
+    std::vector<uint64_t> ho(nb);
+    uint64_t total = 0;
+    for (int k = 0; k < nb; k++) {
+        if (hr[k].status) return done(fail(ctx, TC_E_ARG, "tc_encode_j2k_gpu: code-block " + std::to_string(k) +
+                                                              " status " + std::to_string(hr[k].status)));
+        ho[k] = total;
+        total += hr[k].len;
+    }
+    std::vector<uint8_t> hw(std::max<uint64_t>(total, 1));
+    if ((e = packed.ensure(std::max<uint64_t>(total, 1))) != cudaSuccess ||
+        (e = cudaMemcpyAsync(off.ptr, ho.data(), nb * sizeof(uint64_t), cudaMemcpyHostToDevice, ctx->stream)) !=
+            cudaSuccess ||
+        (e = launch_gather_codewords(ctx, static_cast<uint8_t *>(words.ptr), bcap,
+                                     static_cast<tc_t1_enc_result *>(res.ptr), static_cast<uint64_t *>(off.ptr), nb,
+                                     static_cast<uint8_t *>(packed.ptr))) != cudaSuccess ||
+        (e = cudaMemcpyAsync(hw.data(), packed.ptr, total, cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess)
+        return done(cuda_status(ctx, e, "tc_encode_j2k_gpu read-back"));
+    std::vector<CodedBlock> coded(nb);
+    for (int k = 0; k < nb; k++) {
+        coded[k].data.assign(hw.begin() + ho[k], hw.begin() + ho[k] + hr[k].len);
+        coded[k].passes = (int)hr[k].passes;
+        coded[k].numbps = 31 - (int)hr[k].zero_bitplanes;
+    }
+    std::vector<uint8_t> cs;
+    if ((rc = encode_assemble(*p, L, coded, cs, err))) return done(fail(ctx, rc, err));
+    *out_len = cs.size();
+    if (!h_out || cap < cs.size()) return done(fail(ctx, TC_E_ARG, "tc_encode_j2k_gpu: output buffer too small"));
+    std::memcpy(h_out, cs.data(), cs.size());
+    return done(TC_OK);
+}
+
 int tc_t1_encode(tc_ctx *ctx, const tc_t1_enc_desc *d_desc, int n, const void *d_in, uint8_t *d_out, uint32_t cap,
                  tc_t1_enc_result *d_res)
 {

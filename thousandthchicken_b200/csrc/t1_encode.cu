@@ -412,3 +412,33 @@ cudaError_t launch_t1_encode(tc_ctx *ctx, const tc_t1_enc_desc *d_desc, int n, c
 }
 
 }  // namespace tc
+
+namespace tc {
+namespace {
+
+// Packs the codewords: block k's len[k] bytes from src + k * cap to
+// dst + off[k] (one CTA per block).
+__global__ void gather_codewords_kernel(const uint8_t *__restrict__ src, uint32_t cap,
+                                        const tc_t1_enc_result *__restrict__ res, const uint64_t *__restrict__ off,
+                                        int n, uint8_t *__restrict__ dst)
+{
+    const int k = blockIdx.x;
+    if (k >= n) return;
+    const uint32_t len = res[k].len;
+    const uint8_t *s = src + (size_t)k * cap;
+    uint8_t *d = dst + off[k];
+    for (uint32_t i = threadIdx.x; i < len && i < cap; i += blockDim.x) d[i] = s[i];
+}
+
+}  // namespace
+
+cudaError_t launch_gather_codewords(tc_ctx *ctx, const uint8_t *src, uint32_t cap, const tc_t1_enc_result *res,
+                                    const uint64_t *off, int n, uint8_t *dst)
+{
+    if (n <= 0) return cudaSuccess;
+    gather_codewords_kernel<<<n, 128, 0, ctx->stream>>>(src, cap, res, off, n, dst);
+    ctx->launches++;
+    return cudaGetLastError();
+}
+
+}  // namespace tc

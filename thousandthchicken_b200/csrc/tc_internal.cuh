@@ -129,6 +129,9 @@ cudaError_t launch_dequant_raw(tc_ctx *ctx, const tc_cblk_desc *d_desc, int n,
                                const uint32_t *d_raw, void *d_out, float recon_r);
 cudaError_t launch_t1_encode(tc_ctx *ctx, const tc_t1_enc_desc *d_desc, int n, const void *d_in, uint8_t *d_out,
                              uint32_t cap, tc_t1_enc_result *d_res);
+// Packs n codewords (block k: res[k].len bytes at src + k * cap) to dst + off[k].
+cudaError_t launch_gather_codewords(tc_ctx *ctx, const uint8_t *src, uint32_t cap, const tc_t1_enc_result *res,
+                                    const uint64_t *off, int n, uint8_t *dst);
 
 // One 2-D DWT level over up to 4 components of equal size.
 struct LevelIO {

@@ -135,7 +135,9 @@ class _Slot:
             r.done = t
             if self.keep:
                 a = o.cpu().numpy()
-                r.output = a.view(np.uint16) if r.info["bits"] > 8 else a
+                if r.info["bits"] > 8:
+                    a = a.view(np.int16 if r.info.get("is_signed") else np.uint16)
+                r.output = a
         self.batch = []
         self.outs = None
         return done

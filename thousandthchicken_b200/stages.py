@@ -14,6 +14,7 @@ fallback.
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 from pathlib import Path
 
 import numpy as np
@@ -45,9 +46,12 @@ class Context:
         L.check(L.lib().tc_ctx_create(device, C.c_void_p(self.stream.cuda_stream), C.byref(h)),
                 what="tc_ctx_create")
         self.handle = h
+        self._plans = weakref.WeakSet()
 
     def close(self):
         if getattr(self, "handle", None):
+            for plan in list(getattr(self, "_plans", ())):
+                plan.close()
             L.lib().tc_ctx_destroy(self.handle)
             self.handle = None
 
@@ -297,13 +301,14 @@ class Plan:
         h = C.c_void_p()
         ctx.check(L.lib().tc_plan_create(ctx.handle, ptrs, lens, n, C.byref(h)), "tc_plan_create")
         self.handle = h
+        ctx._plans.add(self)  # destroyed before the context (a plan uses its context's stream and pool)
         self.infos = []
         self.out_bytes = []
         for i in range(n):
             info = L.ImageInfo()
             L.check(L.lib().tc_plan_image_info(h, i, C.byref(info)))
-            self.infos.append({k: int(getattr(info, k)) for k in ("width", "height", "ncomp", "bits", "levels",
-                                                                  "reversible", "mct", "ncblk")})
+            from .codec import _info_dict
+            self.infos.append(_info_dict(info))
             nb = C.c_size_t(0)
             L.check(L.lib().tc_plan_output_bytes(h, i, C.byref(nb)))
             self.out_bytes.append(nb.value)
