@@ -644,6 +644,7 @@ int tc_ctx_destroy(tc_ctx *ctx)
     ctx->stage_desc.release();
     ctx->stage_order.release();
     ctx->tmp_jobs.release();
+    for (auto &b : ctx->enc) b.release();
     ctx->stage_jobs.release();
     if (ctx->jobs_uploaded) cudaEventDestroy(ctx->jobs_uploaded);
     if (ctx->d_words) cudaFree(ctx->d_words);
@@ -1220,10 +1221,10 @@ int tc_encode_j2k_gpu(tc_ctx *ctx, const tc_encode_params *p, const void *h_plan
     uint32_t bcap = 0;
     for (int c = 0; c < C; c++) bcap = std::max<uint32_t>(bcap, 5u << (2 * L.cblk[c]));
     bcap += 256;
-    DevBuf in, col, coef, desc, words, res, off, packed;
+    DevBuf &in = ctx->enc[0], &col = ctx->enc[1], &coef = ctx->enc[2], &desc = ctx->enc[3], &words = ctx->enc[4],
+           &res = ctx->enc[5], &off = ctx->enc[6], &packed = ctx->enc[7];
     auto done = [&](int status) {
         cudaStreamSynchronize(ctx->stream);
-        for (DevBuf *b : {&in, &col, &coef, &desc, &words, &res, &off, &packed}) b->release();
         return status;
     };
     cudaError_t e;

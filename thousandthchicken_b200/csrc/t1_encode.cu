@@ -6,9 +6,10 @@
 // (t1_encode_block in j2k_host.cpp): all coding passes, MQ termination by
 // the FLUSH procedure of ISO C.2.9.
 //
-//   * one warp per code-block, CTAs of kEncWarps blocks; the block's
-//     magnitudes are loaded coalesced into shared memory (quantised from
-//     float with the band's step, or taken as int32);
+//   * one warp per code-block, CTAs of kEncWarps blocks; at every bit-plane
+//     the lanes rebuild the plane's bits per column from the input (float
+//     quantised with the band's step, or int32), read coalesced and cached,
+//     so a block's state is 5.7 KB of shared memory;
 //   * the coding state is the decoder's flag-word layout (t1_common.cuh):
 //     at every stripe the lanes find the candidate columns of the pass with
 //     __ballot_sync and the serial loop visits only those, in scan order;
@@ -25,16 +26,29 @@
 namespace tc {
 namespace {
 
-constexpr int kEncWarps = 4;
+constexpr int kEncWarps = 8;
 
+// A block's coding state: 5.7 KB, so that 32 warps fit an SM.  The
+// magnitudes are not kept: at every bit-plane the lanes rebuild that
+// plane's bits per column from the (cached) input.
 struct EncState {
     uint32_t F[kMaxStripes * 64];       // flag word per stripe column
     unsigned long long sgn[kSgnCols];   // sign of the significant samples per column
     unsigned long long neg[64];         // sign of every sample per column (bit y)
+    unsigned long long bits[64];        // the current bit-plane per column (bit y)
     uint32_t ctx[20];                   // packed probability state per context
     uint8_t mrow[64], mctx[64];         // refinement pass: rows and context codes per column
-    uint32_t mag[64 * 64];              // magnitudes, row-major with pitch 64
 };
+
+// Magnitude of sample (x, y) of block d: the int32 input, or the float input
+// quantised floor(|v| / step) (ISO E.2 deadzone).
+__device__ __forceinline__ uint32_t magnitude(const tc_t1_enc_desc &d, const void *in, int x, int y)
+{
+    const size_t i = d.in_off + (size_t)y * d.in_pitch + x;
+    if (d.flags & TC_CBLK_IRREVERSIBLE) return (uint32_t)floorf(fabsf(__ldg(static_cast<const float *>(in) + i)) * d.inv_step);
+    const int32_t v = __ldg(static_cast<const int32_t *>(in) + i);
+    return (uint32_t)(v < 0 ? -(int64_t)v : v);
+}
 
 // MQ encoder (ISO C.2.1-C.2.9).  A is 16 bits wide as in the standard; each
 // context word is the decoder's packed state (Qe << 16 | NMPS << 1 |
@@ -149,9 +163,10 @@ struct MQEnc {
 
 // All coding passes of a block whose state S holds the magnitudes, signs
 // and a cleared coding state (the lanes in lock-step).
-__device__ void encode_block(EncState &S, const Tables &T, MQEnc &mq, int w, int h, int orient, int numbps,
-                             int lane)
+__device__ void encode_block(EncState &S, const Tables &T, MQEnc &mq, const tc_t1_enc_desc &d, const void *in,
+                             int numbps, int lane)
 {
+    const int w = d.w, h = d.h, orient = d.orient;
     uint32_t *ctx = S.ctx;
     const uint32_t *tbl = T.mq;
     const uint8_t *zc = T.zc[orient];
@@ -159,10 +174,20 @@ __device__ void encode_block(EncState &S, const Tables &T, MQEnc &mq, int w, int
     const int nstripes = (h + 3) >> 2;
     constexpr int G = 32, CPL = 2;
     const unsigned gmask = 0xffffffffu;
-    auto bit = [&](int y, int c, int p) -> uint32_t { return (S.mag[y * 64 + c] >> p) & 1u; };
+    auto bit = [&](int y, int c, int) -> uint32_t { return (uint32_t)(S.bits[c] >> y) & 1u; };
     auto sign_bit = [&](int y, int c) -> uint32_t { return (uint32_t)(S.neg[c] >> y) & 1u; };
 
     for (int p = numbps - 1; p >= 0; --p) {
+        // this bit-plane's bits, the lanes' columns
+#pragma unroll
+        for (int j = 0; j < CPL; j++) {
+            const int c = lane + G * j;
+            unsigned long long m = 0;
+            if (c < w)
+                for (int y = 0; y < h; y++) m |= (unsigned long long)((magnitude(d, in, c, y) >> p) & 1u) << y;
+            S.bits[c] = m;
+        }
+        __syncwarp();
         if (p != numbps - 1) {
             // ---- significance propagation pass (ISO D.3.1) ----
             for (int s = 0; s < nstripes; s++) {
@@ -274,9 +299,8 @@ __device__ void encode_block(EncState &S, const Tables &T, MQEnc &mq, int w, int
                 int k = 0;
                 if (rows == 4 && (f & kSigMask) == 0u) {
                     // run-length mode: four rows with an all-zero neighbourhood
-                    int r = -1;
-                    for (int q = 0; q < 4; q++)
-                        if (r < 0 && bit(4 * s + q, c, p)) r = q;
+                    const uint32_t four = (uint32_t)(S.bits[c] >> (4 * s)) & 0xFu;
+                    const int r = four ? __ffs(four) - 1 : -1;
                     if (r < 0) {
                         mq.encode(ctx, tbl, 18, 0u);
                         continue;
@@ -336,7 +360,7 @@ __global__ void __launch_bounds__(32 * kEncWarps)
         if (lane == 0) res[bi] = r;
         return;
     }
-    // magnitudes and signs, rows coalesced across the lanes
+    // largest magnitude and the signs, rows coalesced across the lanes
     const bool irrev = (d.flags & TC_CBLK_IRREVERSIBLE) != 0;
     uint32_t mx = 0;
     unsigned long long neg0 = 0, neg1 = 0;  // columns lane and lane + 32
@@ -345,19 +369,9 @@ __global__ void __launch_bounds__(32 * kEncWarps)
         for (int j = 0; j < 2; j++) {
             const int x = lane + 32 * j;
             if (x >= w) continue;
-            uint32_t m;
-            bool ng;
-            if (irrev) {
-                // deadzone quantisation (ISO E.2): floor(|x| / step)
-                const float v = static_cast<const float *>(in)[row + x];
-                m = (uint32_t)floorf(fabsf(v) * d.inv_step);
-                ng = v < 0.0f;
-            } else {
-                const int32_t v = static_cast<const int32_t *>(in)[row + x];
-                m = (uint32_t)(v < 0 ? -(int64_t)v : v);
-                ng = v < 0;
-            }
-            S.mag[y * 64 + x] = m;
+            const uint32_t m = magnitude(d, in, x, y);
+            const bool ng = irrev ? static_cast<const float *>(in)[row + x] < 0.0f
+                                  : static_cast<const int32_t *>(in)[row + x] < 0;
             mx = max(mx, m);
             if (ng && m) (j ? neg1 : neg0) |= 1ull << y;
         }
@@ -379,7 +393,7 @@ __global__ void __launch_bounds__(32 * kEncWarps)
     } else if (numbps > 0) {
         MQEnc mq;
         mq.init(out + (size_t)bi * cap, cap, lane == 0);
-        encode_block(S, T, mq, w, h, d.orient, numbps, lane);
+        encode_block(S, T, mq, d, in, numbps, lane);
         r.len = mq.flush();
         r.passes = 3 * numbps - 2;
         if (mq.overflow || r.len > cap) {

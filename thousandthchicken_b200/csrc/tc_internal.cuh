@@ -82,6 +82,10 @@ struct tc_ctx {
     tc::DevBuf scratch;           // DWT intermediate levels
     tc::DevBuf tmp_pool, tmp_desc, tmp_order, tmp_coef, tmp_out;
     tc::PinBuf stage_pool, stage_desc, stage_order;  // pinned staging of tc_decode_j2k
+    // tc_encode_j2k_gpu's buffers (samples, colour planes, coefficients,
+    // Tier-1 descriptors, codewords, results, offsets, packed codewords);
+    // grow-only, so repeated encodes allocate nothing after the first
+    tc::DevBuf enc[8];
     // reverse-DWT job table of tc_decode_j2k's tiled images
     tc::DevBuf tmp_jobs;
     tc::PinBuf stage_jobs;
