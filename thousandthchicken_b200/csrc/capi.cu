@@ -645,6 +645,7 @@ int tc_ctx_destroy(tc_ctx *ctx)
     ctx->stage_order.release();
     ctx->tmp_jobs.release();
     for (auto &b : ctx->enc) b.release();
+    ctx->enc_host.release();
     ctx->stage_jobs.release();
     if (ctx->jobs_uploaded) cudaEventDestroy(ctx->jobs_uploaded);
     if (ctx->d_words) cudaFree(ctx->d_words);
@@ -1289,19 +1290,22 @@ int tc_encode_j2k_gpu(tc_ctx *ctx, const tc_encode_params *p, const void *h_plan
         ho[k] = total;
         total += hr[k].len;
     }
-    std::vector<uint8_t> hw(std::max<uint64_t>(total, 1));
+    if ((e = ctx->enc_host.ensure(std::max<uint64_t>(total, 1))) != cudaSuccess)
+        return done(cuda_status(ctx, e, "tc_encode_j2k_gpu staging"));
+    uint8_t *hw = static_cast<uint8_t *>(ctx->enc_host.ptr);
     if ((e = packed.ensure(std::max<uint64_t>(total, 1))) != cudaSuccess ||
         (e = cudaMemcpyAsync(off.ptr, ho.data(), nb * sizeof(uint64_t), cudaMemcpyHostToDevice, ctx->stream)) !=
             cudaSuccess ||
         (e = launch_gather_codewords(ctx, static_cast<uint8_t *>(words.ptr), bcap,
                                      static_cast<tc_t1_enc_result *>(res.ptr), static_cast<uint64_t *>(off.ptr), nb,
                                      static_cast<uint8_t *>(packed.ptr))) != cudaSuccess ||
-        (e = cudaMemcpyAsync(hw.data(), packed.ptr, total, cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(hw, packed.ptr, total, cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess ||
         (e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess)
         return done(cuda_status(ctx, e, "tc_encode_j2k_gpu read-back"));
     std::vector<CodedBlock> coded(nb);
     for (int k = 0; k < nb; k++) {
-        coded[k].data.assign(hw.begin() + ho[k], hw.begin() + ho[k] + hr[k].len);
+        coded[k].data = hw + ho[k];
+        coded[k].len = hr[k].len;
         coded[k].passes = (int)hr[k].passes;
         coded[k].numbps = 31 - (int)hr[k].zero_bitplanes;
     }

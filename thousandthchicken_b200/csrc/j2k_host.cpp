@@ -1682,6 +1682,7 @@ int encode_codestream(const tc_encode_params &p, const void *planes, std::vector
     // Tier-1: every code-block with all passes; the codeword does not
     // depend on Mb, so the blocks are coded before the guard bits are known.
     std::vector<CodedBlock> coded(L.jobs.size());
+    std::vector<std::vector<uint8_t>> words(L.jobs.size());
     std::atomic<int> fail{0};
     parallel_for((int)L.jobs.size(), threads, [&](int k) {
         const EncodeLayout::Job &jb = L.jobs[k];
@@ -1693,8 +1694,10 @@ int encode_codestream(const tc_encode_params &p, const void *planes, std::vector
             for (int x = 0; x < bw; x++)
                 blk[y * bw + x] = q[jb.c * np + (size_t)(b.y0 + cy + y) * W + b.x0 + cx + x];
         int zbp = 0;
-        if (t1_encode_block(blk, bw, bh, b.orient, 31, 0, coded[k].data, &coded[k].passes, &zbp)) fail = 1;
+        if (t1_encode_block(blk, bw, bh, b.orient, 31, 0, words[k], &coded[k].passes, &zbp)) fail = 1;
         coded[k].numbps = 31 - zbp;
+        coded[k].data = words[k].data();
+        coded[k].len = (uint32_t)words[k].size();
     });
     if (fail) { err = "Tier-1 encoding failed"; return TC_E_ARG; }
     return encode_assemble(p, L, coded, out, err);
@@ -1735,7 +1738,6 @@ int encode_assemble(const tc_encode_params &p, EncodeLayout &L, const std::vecto
     std::vector<int> zbps(jobs.size());
     for (size_t k = 0; k < jobs.size(); k++)
         zbps[k] = geo[jobs[k].c][jobs[k].r].bands[jobs[k].bi].mb - coded[k].numbps;
-    const size_t np = (size_t)W * H;
 
     // Index jobs by (c, r, bi) for the packet writer.
     std::vector<std::vector<std::vector<int>>> first(C, std::vector<std::vector<int>>(NL + 1));
@@ -1745,68 +1747,12 @@ int encode_assemble(const tc_encode_params &p, EncodeLayout &L, const std::vecto
         if (v[jobs[k].bi] < 0) v[jobs[k].bi] = (int)k;
     }
 
-    std::vector<uint8_t> body;
-    body.reserve(np * C / 2);
-    auto write_packet = [&](int r, int c) {
-        std::vector<uint8_t> hdr;
-        BitWriter bw(hdr);
-        bool any = false;
-        for (int bi = 0; bi < (int)geo[c][r].bands.size(); bi++) {
-            const Band &b = geo[c][r].bands[bi];
-            if (b.ncbx * b.ncby == 0) continue;
-            const int k0 = first[c][r][bi];
-            for (int i = 0; i < b.ncbx * b.ncby; i++) any |= coded[k0 + i].passes > 0;
-        }
-        if (!any) {
-            bw.put(0);
-            bw.flush();
-            body.insert(body.end(), hdr.begin(), hdr.end());
-            return;
-        }
-        bw.put(1);
-        std::vector<int> order;
-        for (int bi = 0; bi < (int)geo[c][r].bands.size(); bi++) {
-            const Band &b = geo[c][r].bands[bi];
-            const int n = b.ncbx * b.ncby;
-            if (n == 0) continue;
-            const int k0 = first[c][r][bi];
-            TagTree incl(b.ncbx, b.ncby), zt(b.ncbx, b.ncby);
-            std::vector<int> iv(n), zv(n);
-            for (int i = 0; i < n; i++) {
-                iv[i] = coded[k0 + i].passes > 0 ? 0 : 1;
-                zv[i] = zbps[k0 + i];
-            }
-            incl.set_leaves(iv);
-            zt.set_leaves(zv);
-            for (int i = 0; i < n; i++) {
-                const CodedBlock &cd = coded[k0 + i];
-                incl.encode(bw, i, 1);
-                if (cd.passes == 0) continue;
-                zt.encode(bw, i, zbps[k0 + i] + 1);
-                put_num_passes(bw, cd.passes);
-                const int len = (int)cd.data.size();
-                int lblock = 3, incr = 0;
-                while (len >= (1 << (lblock + incr + floorlog2(cd.passes)))) incr++;
-                for (int t = 0; t < incr; t++) bw.put(1);
-                bw.put(0);
-                lblock += incr;
-                bw.put_bits((uint32_t)len, lblock + floorlog2(cd.passes));
-                order.push_back(k0 + i);
-            }
-        }
-        bw.flush();
-        body.insert(body.end(), hdr.begin(), hdr.end());
-        for (int k : order) body.insert(body.end(), coded[k].data.begin(), coded[k].data.end());
-    };
-    if (p.progression == 1) {
-        for (int r = 0; r <= NL; r++)
-            for (int c = 0; c < C; c++) write_packet(r, c);
-    } else {
-        for (int r = 0; r <= NL; r++)
-            for (int c = 0; c < C; c++) write_packet(r, c);
-    }
-
+    // Main header, then the single tile-part: its length is patched in once
+    // the packets are written straight into `out`.
+    size_t total = 0;
+    for (const CodedBlock &cb : coded) total += cb.len;
     out.clear();
+    out.reserve(1024 + total + 8 * jobs.size());
     Writer wr{out};
     wr.u16(M_SOC);
     wr.u16(M_SIZ);
@@ -1862,14 +1808,79 @@ int encode_assemble(const tc_encode_params &p, EncodeLayout &L, const std::vecto
         wr.u8(c);                          // Cqcc
         write_steps(c);
     }
+    const size_t sot = out.size();
     wr.u16(M_SOT);
     wr.u16(10);
     wr.u16(0);
-    wr.u32((uint32_t)(12 + 2 + body.size()));
+    wr.u32(0);  // Psot, below
     wr.u8(0);
     wr.u8(1);
     wr.u16(M_SOD);
-    out.insert(out.end(), body.begin(), body.end());
+    std::vector<uint8_t> hdr;
+    auto write_packet = [&](int r, int c) {
+        hdr.clear();
+        BitWriter bw(hdr);
+        bool any = false;
+        for (int bi = 0; bi < (int)geo[c][r].bands.size(); bi++) {
+            const Band &b = geo[c][r].bands[bi];
+            if (b.ncbx * b.ncby == 0) continue;
+            const int k0 = first[c][r][bi];
+            for (int i = 0; i < b.ncbx * b.ncby; i++) any |= coded[k0 + i].passes > 0;
+        }
+        if (!any) {
+            bw.put(0);
+            bw.flush();
+            out.insert(out.end(), hdr.begin(), hdr.end());
+            return;
+        }
+        bw.put(1);
+        std::vector<int> order;
+        for (int bi = 0; bi < (int)geo[c][r].bands.size(); bi++) {
+            const Band &b = geo[c][r].bands[bi];
+            const int n = b.ncbx * b.ncby;
+            if (n == 0) continue;
+            const int k0 = first[c][r][bi];
+            TagTree incl(b.ncbx, b.ncby), zt(b.ncbx, b.ncby);
+            std::vector<int> iv(n), zv(n);
+            for (int i = 0; i < n; i++) {
+                iv[i] = coded[k0 + i].passes > 0 ? 0 : 1;
+                zv[i] = zbps[k0 + i];
+            }
+            incl.set_leaves(iv);
+            zt.set_leaves(zv);
+            for (int i = 0; i < n; i++) {
+                const CodedBlock &cd = coded[k0 + i];
+                incl.encode(bw, i, 1);
+                if (cd.passes == 0) continue;
+                zt.encode(bw, i, zbps[k0 + i] + 1);
+                put_num_passes(bw, cd.passes);
+                const int len = (int)cd.len;
+                int lblock = 3, incr = 0;
+                while (len >= (1 << (lblock + incr + floorlog2(cd.passes)))) incr++;
+                for (int t = 0; t < incr; t++) bw.put(1);
+                bw.put(0);
+                lblock += incr;
+                bw.put_bits((uint32_t)len, lblock + floorlog2(cd.passes));
+                order.push_back(k0 + i);
+            }
+        }
+        bw.flush();
+        out.insert(out.end(), hdr.begin(), hdr.end());
+        for (int k : order) out.insert(out.end(), coded[k].data, coded[k].data + coded[k].len);
+    };
+    if (p.progression == 1) {
+        for (int r = 0; r <= NL; r++)
+            for (int c = 0; c < C; c++) write_packet(r, c);
+    } else {
+        for (int r = 0; r <= NL; r++)
+            for (int c = 0; c < C; c++) write_packet(r, c);
+    }
+
+    const uint32_t psot = (uint32_t)(out.size() - sot);
+    out[sot + 6] = (uint8_t)(psot >> 24);
+    out[sot + 7] = (uint8_t)(psot >> 16);
+    out[sot + 8] = (uint8_t)(psot >> 8);
+    out[sot + 9] = (uint8_t)psot;
     wr.u16(M_EOC);
     return TC_OK;
 }

@@ -77,9 +77,11 @@ struct EncodeLayout {
     };
     std::vector<Job> jobs;
 };
-// One code-block coded with all passes (its codeword does not depend on Mb).
+// One code-block coded with all passes (its codeword does not depend on
+// Mb): the codeword's bytes (held by the caller), its passes and bit-planes.
 struct CodedBlock {
-    std::vector<uint8_t> data;
+    const uint8_t *data = nullptr;
+    uint32_t len = 0;
     int passes = 0, numbps = 0;
 };
 int encode_layout(const tc_encode_params &p, EncodeLayout &L, std::string &err);

@@ -86,6 +86,7 @@ struct tc_ctx {
     // Tier-1 descriptors, codewords, results, offsets, packed codewords);
     // grow-only, so repeated encodes allocate nothing after the first
     tc::DevBuf enc[8];
+    tc::PinBuf enc_host;          // the packed codewords read back
     // reverse-DWT job table of tc_decode_j2k's tiled images
     tc::DevBuf tmp_jobs;
     tc::PinBuf stage_jobs;
