@@ -274,6 +274,36 @@ def cpu_baseline(cores):
             "sample": f"{w}x{h}x3 image of the same generator and coding parameters, oracle full decode"}
 
 
+def encode_section(ctx, img):
+    """The forward pipeline: the workload image encoded on the GPU
+    (tc_encode_j2k_gpu: colour, DWT, quantisation and Tier-1 as kernels,
+    packets on the host; host samples in, codestream out, median of 3)
+    against the host encoder on all cores, and a lossless 1024^2 check that
+    both write the same bytes."""
+    from thousandthchicken_b200 import codec
+    kw = dict(levels=WORKLOAD["levels"], reversible=False, mct=True, base_step=WORKLOAD["base_step"])
+    bits = WORKLOAD["bits"]
+    mpx = img.shape[1] * img.shape[2] / 1e6
+    codec.encode_gpu(ctx, img, bits, **kw)
+    ts = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        codec.encode_gpu(ctx, img, bits, **kw)
+        ts.append(time.perf_counter() - t0)
+    gpu_s = sorted(ts)[1]
+    t0 = time.perf_counter()
+    codec.encode(img, bits, **kw)
+    host_s = time.perf_counter() - t0
+    small = np.ascontiguousarray(img[:, :1024, :1024])
+    same = codec.encode_gpu(ctx, small, bits, levels=5, reversible=True) == codec.encode(small, bits, levels=5,
+                                                                                           reversible=True)
+    return {"gpu_mpix_s": round(mpx / gpu_s, 1), "gpu_ms": round(gpu_s * 1e3, 2),
+            "host_mpix_s": round(mpx / host_s, 1), "host_ms": round(host_s * 1e3, 1),
+            "host_threads": os.cpu_count() or 1, "lossless_1024_identical": bool(same),
+            "what": "encode of the workload image (ICT, 6-level 9/7, step 1/128, 64x64 blocks), host samples in, "
+                    "codestream out"}
+
+
 def kernels_section(ctx, stream, flush, cs, hbm):
     """The stand-alone stage kernels on device-resident 4096x4096 data, each
     timed with CUDA events on the context's stream (median of 5 runs, L2
@@ -435,9 +465,10 @@ def run_ours(args, rank, world, local_rank):
         e2e_times.append(time.perf_counter() - t0)
     e2e_s = max_over_ranks(sum(e2e_times) / e2e_steps, dist, f"cuda:{local_rank}")
 
-    batched, served, kernels = None, None, None
+    batched, served, kernels, encode = None, None, None, None
     if not args.core_only:
         kernels = kernels_section(ctx, stream, flush, cs, measured_peaks()[0])
+        encode = encode_section(ctx, img)
         # batched (one plan: one Tier-1 queue over every image) vs per-image plans
         mixed = make_mixed()
         streams = [cs_ for _, cs_ in mixed]
@@ -553,6 +584,7 @@ def run_ours(args, rank, world, local_rank):
             line["batched_vs_per_image"] = batched
             line["served"] = served
             line["kernels"] = kernels
+            line["encode"] = encode
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(os.cpu_count() or 1)
         print(json.dumps(line), flush=True)
