@@ -215,10 +215,12 @@ int tc_color_forward(tc_ctx *ctx, int kind, int ncomp,
 
 /* ---- codestream parsing (the Tier-2 hand-off) ---------------------------- */
 
-/* Image information from the main header.  Components share size, depth,
+/* Image information from the main header.  Components share depth,
  * decomposition levels and wavelet; their code-block sizes and steps may
  * differ (COC / QCC, main or tile-part header), and cblk_w/cblk_h,
- * guard_bits and quant_style report the COD / QCD values. */
+ * guard_bits and quant_style report the COD / QCD values.  Components may
+ * be subsampled (single-tile images at the origin): planar outputs then
+ * hold each component at its own size, one after the other. */
 typedef struct tc_image_info {
     int32_t width, height, ncomp, bits;    /* width/height: Xsiz-XOsiz, Ysiz-YOsiz */
     int32_t is_signed;
@@ -230,6 +232,9 @@ typedef struct tc_image_info {
     int32_t guard_bits, quant_style;
     uint32_t ncblk;                        /* code-blocks over all components */
     uint32_t ntiles;                       /* tiles (ISO B.3); 1 for an untiled image */
+    uint8_t  comp_dx[4], comp_dy[4];       /* component subsampling XRsiz / YRsiz:
+                                              component c is a ceil(width/dx) x
+                                              ceil(height/dy) plane */
 } tc_image_info;
 
 /* One tile of a parsed image: its region in samples from the image's
@@ -339,7 +344,7 @@ typedef struct tc_encode_params {
     double  base_step;     /* irreversible: step relative to 2^bits, divided
                               by the subband's synthesis L2 norm */
     int32_t guard_bits;    /* 0 = choose automatically */
-    int32_t progression;   /* 0 = LRCP, 1 = RLCP */
+    int32_t progression;   /* 0 LRCP, 1 RLCP, 2 RPCL, 3 PCRL, 4 CPRL */
     int32_t threads;       /* <= 0: all cores */
     int32_t is_signed;     /* signed samples (TC_S8 / TC_S16 style two's
                               complement input, no DC level shift) */
@@ -348,6 +353,10 @@ typedef struct tc_encode_params {
      * irreversible step. */
     int32_t comp_cblk_log2[4];
     double  comp_step_scale[4];
+    /* Component subsampling XRsiz / YRsiz (0: 1).  Component c is a
+     * ceil(width/dx) x ceil(height/dy) plane; the planes follow one another.
+     * The colour transform needs components 0-2 at one size. */
+    int32_t comp_dx[4], comp_dy[4];
 } tc_encode_params;
 
 /* Encode planar samples (8-bit when bits <= 8, else 16-bit; unsigned, or

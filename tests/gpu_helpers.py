@@ -133,3 +133,21 @@ def oracle_decode_tiled(cs, r=0.5):
                                                      bool(info["reversible"]), bool(info["mct"]), r=r,
                                                      signed=bool(info["is_signed"]))
     return info, out
+
+
+def oracle_decode_components(cs, r=0.5):
+    """Oracle decode of a single-tile codestream whose components may be
+    subsampled (no colour transform across them): each component's
+    descriptors through the oracle's one-component decode.  Returns (info,
+    list of [h, w] planes)."""
+    info, desc, pool = codec.parse(cs)
+    sizes = info["comp_sizes"]
+    bounds = np.cumsum([0] + [h * w for h, w in sizes])
+    planes = []
+    for c, (h, w) in enumerate(sizes):
+        sel = (desc["out_off"] >= bounds[c]) & (desc["out_off"] < bounds[c + 1])
+        d = desc[sel].copy()
+        d["out_off"] -= np.uint64(bounds[c])
+        planes.append(O.decode_tile(d, pool, w, h, 1, info["bits"], info["levels"], bool(info["reversible"]), False,
+                                    r=r, signed=bool(info["is_signed"]))[0])
+    return info, planes

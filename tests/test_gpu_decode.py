@@ -6,7 +6,7 @@ import pytest
 
 import oracle as O
 from conftest import golden_cases, load_golden, synth_image
-from test_host_codec import COC_QCC, PRECINCTS, SIGNED, TILED
+from test_host_codec import COC_QCC, PRECINCTS, SIGNED, SUBSAMPLED, TILED
 from thousandthchicken_b200 import codec
 
 pytestmark = pytest.mark.gpu
@@ -372,4 +372,36 @@ def test_signed_samples_decode(gpu_ctx, bits, comps, kw):
     gpu_ctx.synchronize()
     g0 = outs[0].cpu().numpy()
     np.testing.assert_array_equal(g0.view(np.int16) if bits > 8 else g0, got)
+    plan.close()
+
+
+@pytest.mark.parametrize("w,h,bits,dxy,kw", SUBSAMPLED, ids=["420", "422-97-odd", "g12-pcrl", "cprl-odd-factors"])
+def test_subsampled_components_decode(gpu_ctx, w, h, bits, dxy, kw):
+    """Subsampled components through the GPU: one reverse DWT unit per
+    component at its own size, each written to its own plane of the planar
+    output; alone (Decoder.decode returns one array per component) and in a
+    plan beside an image without subsampling.  Lossless: the original
+    components; lossy: within 1 of the oracle."""
+    from gpu_helpers import oracle_decode_components
+    from test_host_codec import _subsampled
+    from thousandthchicken_b200.stages import Plan, split_components
+    comps = _subsampled(w, h, bits, dxy, seed=w)
+    cs = codec.encode(comps, bits, levels=3, mct=False, comp_subsampling=dxy, **kw)
+    got = _decoder(gpu_ctx).decode(cs)
+    _, want = oracle_decode_components(cs)
+    for g, c_, o in zip(got, comps, want):
+        if kw["reversible"]:
+            np.testing.assert_array_equal(g, c_)
+        else:
+            d = np.abs(g.astype(np.int64) - o.astype(np.int64))
+            assert d.max() <= 1 and (d > 0).mean() < 0.01
+    other = codec.encode(synth_image(64, 48, 3, bits, seed=1), bits, levels=3, reversible=True)
+    plan = Plan(gpu_ctx, [other, cs])
+    outs = plan.execute(plan.alloc_outputs())
+    gpu_ctx.synchronize()
+    flat = outs[1].cpu().numpy()
+    if bits > 8:
+        flat = flat.view(np.uint16)
+    for g, p_ in zip(got, split_components(flat, plan.infos[1]["comp_sizes"])):
+        np.testing.assert_array_equal(p_, g)
     plan.close()

@@ -479,3 +479,59 @@ def test_signed_samples_through_oracle(bits, comps, kw):
             np.testing.assert_array_equal(opj, img.astype(np.int64))
     else:
         assert np.abs(out.astype(np.int64) - img).max() <= 64
+
+
+def _subsampled(w, h, bits, dxy, seed):
+    """Components of a w x h image subsampled by dxy[c] = (dx, dy)."""
+    full = synth_image(w, h, len(dxy), bits, seed=seed)
+    return [full[c, ::dy, ::dx] for c, (dx, dy) in enumerate(dxy)]
+
+
+SUBSAMPLED = [  # (w, h, bits, per-component (dx, dy), harness options)
+    (200, 120, 8, [(1, 1), (2, 2), (2, 2)], dict(reversible=True)),                  # 4:2:0
+    (201, 121, 8, [(1, 1), (2, 1), (2, 1)], dict(reversible=False, base_step=1 / 256)),  # 4:2:2, odd sizes
+    (150, 98, 12, [(1, 1), (2, 2)], dict(reversible=True, progression=3)),          # PCRL
+    (97, 63, 8, [(1, 1), (4, 2), (3, 3)], dict(reversible=True, progression=4)),    # CPRL, odd factors
+]
+
+
+@pytest.mark.parametrize("w,h,bits,dxy,kw", SUBSAMPLED, ids=["420", "422-97-odd", "g12-pcrl", "cprl-odd-factors"])
+def test_subsampled_components_through_oracle(w, h, bits, dxy, kw):
+    """Subsampled components (SIZ XRsiz / YRsiz, ISO B.2): each component
+    on its own ceil(w/dx) x ceil(h/dy) grid, with its own subband geometry
+    and its precincts visited at reference-grid positions scaled by its
+    subsampling (ISO B.12.1.3).  Lossless streams give back every
+    component; OpenJPEG reads the 4:2:0 one as YCbCr, within 1 of the same
+    conversion of the original components."""
+    comps = _subsampled(w, h, bits, dxy, seed=w)
+    cs = codec.encode(comps, bits, levels=3, mct=False, comp_subsampling=dxy, **kw)
+    from gpu_helpers import oracle_decode_components
+    info, planes = oracle_decode_components(cs)
+    assert info["subsampling"] == dxy
+    assert [p.shape for p in planes] == [c.shape for c in comps]
+    for p_, c_ in zip(planes, comps):
+        if kw["reversible"]:
+            np.testing.assert_array_equal(p_, c_)
+        else:
+            assert np.abs(p_.astype(np.int64) - c_).max() <= 8
+    if dxy == [(1, 1), (2, 2), (2, 2)]:
+        import io
+        from PIL import Image
+        rgb = np.asarray(Image.open(io.BytesIO(cs))).astype(np.float64)
+        up = [np.repeat(np.repeat(c_.astype(np.float64), 2, 0), 2, 1)[:h, :w] - 128 for c_ in comps[1:]]
+        y = comps[0].astype(np.float64)
+        want = np.stack([y + 1.402 * up[1], y - 0.344136 * up[0] - 0.714136 * up[1], y + 1.772 * up[0]], -1)
+        assert np.abs(rgb - np.clip(np.rint(want), 0, 255)).max() <= 1
+
+
+def test_subsampled_tiles_are_unsupported():
+    comps = _subsampled(128, 128, 8, [(1, 1), (2, 2)], seed=2)
+    cs = codec.encode(comps, 8, levels=2, mct=False, comp_subsampling=[(1, 1), (2, 2)])
+    # rewrite SIZ for 64x64 tiles: XTsiz / YTsiz at bytes 22-29 from the marker
+    b = bytearray(cs)
+    i = bytes(b).index(b"\xff\x51")
+    b[i + 22:i + 26] = (64).to_bytes(4, "big")
+    b[i + 26:i + 30] = (64).to_bytes(4, "big")
+    with pytest.raises(TCError) as ei:
+        codec.read_header(bytes(b))
+    assert ei.value.status == TC_E_UNSUPPORTED

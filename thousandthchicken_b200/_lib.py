@@ -56,7 +56,8 @@ class ImageInfo(C.Structure):
     _fields_ = [(n, C.c_int32) for n in ("width", "height", "ncomp", "bits", "is_signed", "levels",
                                         "reversible", "mct", "cblk_w", "cblk_h", "layers", "progression",
                                         "guard_bits", "quant_style")] + \
-               [("ncblk", C.c_uint32), ("ntiles", C.c_uint32)]
+               [("ncblk", C.c_uint32), ("ntiles", C.c_uint32), ("comp_dx", C.c_uint8 * 4),
+                ("comp_dy", C.c_uint8 * 4)]
 
 
 class TileInfo(C.Structure):
@@ -75,7 +76,8 @@ class EncodeParams(C.Structure):
                 ("levels", C.c_int32), ("reversible", C.c_int32), ("mct", C.c_int32),
                 ("cblk_log2", C.c_int32), ("base_step", C.c_double), ("guard_bits", C.c_int32),
                 ("progression", C.c_int32), ("threads", C.c_int32), ("is_signed", C.c_int32),
-                ("comp_cblk_log2", C.c_int32 * 4), ("comp_step_scale", C.c_double * 4)]
+                ("comp_cblk_log2", C.c_int32 * 4), ("comp_step_scale", C.c_double * 4),
+                ("comp_dx", C.c_int32 * 4), ("comp_dy", C.c_int32 * 4)]
 
 
 assert C.sizeof(CblkDesc) == 40

@@ -20,7 +20,11 @@ INFO_FIELDS = ("width", "height", "ncomp", "bits", "is_signed", "levels", "rever
 
 
 def _info_dict(info: L.ImageInfo) -> dict:
-    return {k: int(getattr(info, k)) for k in INFO_FIELDS}
+    d = {k: int(getattr(info, k)) for k in INFO_FIELDS}
+    n = d["ncomp"]
+    d["subsampling"] = [(int(info.comp_dx[c]), int(info.comp_dy[c])) for c in range(n)]
+    d["comp_sizes"] = [(-(-d["height"] // dy), -(-d["width"] // dx)) for dx, dy in d["subsampling"]]
+    return d
 
 
 def _buf(data) -> np.ndarray:
@@ -70,15 +74,34 @@ def parse(cs):
 
 
 def _encode_params(planes, bits, levels, reversible, mct, cblk_log2, base_step, guard_bits, progression, threads,
-                   comp_cblk_log2, comp_step_scale):
-    signed = np.asarray(planes).dtype.kind == "i"
-    if signed:
-        planes = np.ascontiguousarray(planes, np.int8 if bits <= 8 else np.int16)
+                   comp_cblk_log2, comp_step_scale, comp_subsampling=None):
+    if comp_subsampling:
+        # a list of component planes of their own sizes: ceil(w/dx) x ceil(h/dy)
+        comps = [np.asarray(a) for a in planes]
+        signed = comps[0].dtype.kind == "i"
+        dt = (np.int8 if bits <= 8 else np.int16) if signed else (np.uint8 if bits <= 8 else np.uint16)
+        ncomp = len(comps)
+        dxy = list(comp_subsampling) + [(1, 1)] * (ncomp - len(comp_subsampling))
+        # the image size: a component at 1:1, else what the first one implies
+        full = [i for i, (a, b) in enumerate(dxy) if a == 1 and b == 1]
+        if full:
+            h, w = comps[full[0]].shape
+        else:
+            h, w = comps[0].shape[0] * dxy[0][1], comps[0].shape[1] * dxy[0][0]
+        for a, (dx, dy) in zip(comps, dxy):
+            if a.shape != (-(-h // dy), -(-w // dx)):
+                raise ValueError(f"component of shape {a.shape} does not match {w}x{h} at {dx}x{dy}")
+        planes = np.concatenate([np.ascontiguousarray(a, dt).reshape(-1) for a in comps])
     else:
-        planes = np.ascontiguousarray(planes, np.uint8 if bits <= 8 else np.uint16)
-    if planes.ndim == 2:
-        planes = planes[None]
-    ncomp, h, w = planes.shape
+        signed = np.asarray(planes).dtype.kind == "i"
+        if signed:
+            planes = np.ascontiguousarray(planes, np.int8 if bits <= 8 else np.int16)
+        else:
+            planes = np.ascontiguousarray(planes, np.uint8 if bits <= 8 else np.uint16)
+        if planes.ndim == 2:
+            planes = planes[None]
+        ncomp, h, w = planes.shape
+        dxy = [(1, 1)] * ncomp
     p = L.EncodeParams(width=w, height=h, ncomp=ncomp, bits=bits, levels=levels, reversible=int(reversible),
                        mct=int(mct), cblk_log2=cblk_log2, base_step=base_step, guard_bits=guard_bits,
                        progression=progression, threads=threads, is_signed=int(signed))
@@ -86,6 +109,8 @@ def _encode_params(planes, bits, levels, reversible, mct, cblk_log2, base_step, 
         p.comp_cblk_log2[c] = int(v)
     for c, v in enumerate(comp_step_scale or []):
         p.comp_step_scale[c] = float(v)
+    for c, (dx, dy) in enumerate(dxy):
+        p.comp_dx[c], p.comp_dy[c] = int(dx), int(dy)
     return planes, p
 
 
@@ -107,14 +132,15 @@ def encode_gpu(ctx, planes: np.ndarray, bits: int, levels: int = 5, reversible: 
 
 def encode(planes: np.ndarray, bits: int, levels: int = 5, reversible: bool = True, mct: bool = True,
            cblk_log2: int = 6, base_step: float = 1.0 / 128, guard_bits: int = 0, progression: int = 0,
-           threads: int = 0, comp_cblk_log2=None, comp_step_scale=None) -> bytes:
+           threads: int = 0, comp_cblk_log2=None, comp_step_scale=None, comp_subsampling=None) -> bytes:
     """Harness encoder: planar samples [ncomp, h, w] -> codestream; signed
     integer arrays (int8 / int16) give signed components (no DC shift).
     comp_cblk_log2 / comp_step_scale: per-component code-block size exponent
     and irreversible step multiplier (0 = the image-wide value), written as
-    COC / QCC marker segments."""
+    COC / QCC marker segments.  comp_subsampling: per component (dx, dy);
+    planes is then a list of component arrays of ceil(h/dy) x ceil(w/dx)."""
     planes, p = _encode_params(planes, bits, levels, reversible, mct, cblk_log2, base_step, guard_bits, progression,
-                               threads, comp_cblk_log2, comp_step_scale)
+                               threads, comp_cblk_log2, comp_step_scale, comp_subsampling)
     cap = planes.nbytes * 3 + 65536
     out = np.empty(cap, np.uint8)
     n = C.c_size_t(0)

@@ -127,6 +127,30 @@ static int check_ctx(tc_ctx *ctx)
 static int sample_bytes(int bits) { return bits <= 8 ? 1 : 2; }
 // The `bits` argument of the output stages: the depth, TC_SIGNED for signed samples.
 static int out_bits(const tc_image_info &inf) { return inf.bits | (inf.is_signed ? TC_SIGNED : 0); }
+// Whether the image has subsampled components, and component c's plane size.
+static bool subsampled(const tc_image_info &inf)
+{
+    for (int c = 0; c < inf.ncomp && c < 4; c++)
+        if (inf.comp_dx[c] > 1 || inf.comp_dy[c] > 1) return true;
+    return false;
+}
+static void comp_size(const tc_image_info &inf, int c, int *w, int *h)
+{
+    const int dx = inf.comp_dx[c] ? inf.comp_dx[c] : 1, dy = inf.comp_dy[c] ? inf.comp_dy[c] : 1;
+    *w = (inf.width + dx - 1) / dx;
+    *h = (inf.height + dy - 1) / dy;
+}
+// Samples of all components (planar, each at its own size).
+static size_t image_samples(const tc_image_info &inf)
+{
+    size_t n = 0;
+    for (int c = 0; c < inf.ncomp; c++) {
+        int w, h;
+        comp_size(inf, c, &w, &h);
+        n += (size_t)w * h;
+    }
+    return n;
+}
 
 // Reverse DWT of ncomp components from Mallat planes coef[c] (pitch cp)
 // through levels >= 2 into ping-pong scratch, and the last level either into
@@ -212,6 +236,7 @@ struct tc_plan {
         size_t out_bytes = 0;
         std::vector<tc_tile_info> tiles;  // tile-major coefficients from coef_off
         std::vector<size_t> tile_scratch; // each tile's scratch, from the image's
+        size_t comp_scratch[4] = {0, 0, 0, 0};  // subsampled images: each component's scratch
     };
     std::vector<Img> imgs;
     DevBuf pool, desc, order, coef, scratch;
@@ -249,7 +274,8 @@ struct tc_plan {
 // Plans of several images or of tiled images run the batched reverse DWT.
 static bool plan_batched(const tc_plan *P)
 {
-    return P->imgs.size() > 1 || (P->imgs.size() == 1 && P->imgs[0].tiles.size() > 1);
+    return P->imgs.size() > 1 ||
+           (P->imgs.size() == 1 && (P->imgs[0].tiles.size() > 1 || subsampled(P->imgs[0].info)));
 }
 
 static void plan_drop_graph(tc_plan *P)
@@ -278,14 +304,23 @@ static int plan_build_parsed(tc_ctx *ctx, const Parsed *const *parsed, const uin
         tc_plan::Img im;
         im.info = inf;
         im.coef_off = coef_total;
-        coef_total += (uint64_t)inf.ncomp * inf.width * inf.height * 4;
+        coef_total += (uint64_t)image_samples(inf) * 4;
         coef_total = (coef_total + 255) & ~uint64_t(255);
-        im.out_bytes = (size_t)inf.ncomp * inf.width * inf.height * sample_bytes(inf.bits);
+        im.out_bytes = image_samples(inf) * sample_bytes(inf.bits);
         im.tiles = parsed[i]->tiles;
         size_t img_scratch = 0;
-        for (const tc_tile_info &t : im.tiles) {
-            im.tile_scratch.push_back(img_scratch);
-            img_scratch += (reverse_scratch_bytes(t.w, t.h, inf.levels, inf.ncomp) + 255) & ~size_t(255);
+        if (subsampled(inf)) {
+            for (int c = 0; c < inf.ncomp; c++) {
+                int cw, ch;
+                comp_size(inf, c, &cw, &ch);
+                im.comp_scratch[c] = img_scratch;
+                img_scratch += (reverse_scratch_bytes(cw, ch, inf.levels, 1) + 255) & ~size_t(255);
+            }
+        } else {
+            for (const tc_tile_info &t : im.tiles) {
+                im.tile_scratch.push_back(img_scratch);
+                img_scratch += (reverse_scratch_bytes(t.w, t.h, inf.levels, inf.ncomp) + 255) & ~size_t(255);
+            }
         }
         scratch_max = std::max(scratch_max, img_scratch);
         scratch_sum += img_scratch;
@@ -377,12 +412,17 @@ static int run_reverse_batched(tc_plan *P, void *const *d_out)
     const size_t nimg = P->imgs.size();
     std::vector<void *> outs(d_out, d_out + nimg);
     cudaError_t e;
-    // one reverse transform: a tile of an image (an untiled image is one tile)
+    auto color_of = [](const tc_image_info &inf) {
+        return inf.mct && inf.ncomp >= 3 ? (inf.reversible ? TC_COLOR_RCT : TC_COLOR_ICT) : TC_COLOR_DC;
+    };
+    // one reverse transform: a tile of an image (an untiled image is one
+    // tile), or one component of an image whose components are subsampled
     struct Unit {
         const tc_image_info *inf;
-        int w, h;
-        void *coef[4];   // the tile's component planes, pitch w
-        void *out[4];    // the tile's first sample in each output plane
+        int w, h, ncomp, color;
+        void *coef[4];   // the unit's component planes, pitch w
+        void *out[4];    // the unit's first sample in each output plane
+        int out_pitch;
         char *scratch;
     };
     std::vector<Unit> units;
@@ -390,33 +430,52 @@ static int run_reverse_batched(tc_plan *P, void *const *d_out)
         const tc_plan::Img &im = P->imgs[i];
         const tc_image_info &inf = im.info;
         char *coef = static_cast<char *>(P->coef.ptr) + im.coef_off;
+        char *out = static_cast<char *>(d_out[i]);
+        char *scratch = static_cast<char *>(P->scratch.ptr) + P->scratch_off[i];
         const size_t plane = (size_t)inf.width * inf.height;
         const int ob = sample_bytes(inf.bits);
+        if (subsampled(inf)) {
+            size_t off = 0;  // the parser's and the output's planar order
+            for (int c = 0; c < inf.ncomp; c++) {
+                Unit u{};
+                u.inf = &inf;
+                comp_size(inf, c, &u.w, &u.h);
+                u.ncomp = 1;
+                u.color = TC_COLOR_DC;
+                u.coef[0] = coef + off * 4;
+                u.out[0] = out + off * ob;
+                u.out_pitch = u.w;
+                u.scratch = scratch + im.comp_scratch[c];
+                units.push_back(u);
+                off += (size_t)u.w * u.h;
+            }
+            continue;
+        }
         for (size_t k = 0; k < im.tiles.size(); k++) {
             const tc_tile_info &t = im.tiles[k];
-            Unit u;
+            Unit u{};
             u.inf = &inf;
             u.w = t.w;
             u.h = t.h;
+            u.ncomp = inf.ncomp;
+            u.color = color_of(inf);
             for (int c = 0; c < inf.ncomp; c++) {
                 u.coef[c] = coef + (t.coef_off + (size_t)c * t.w * t.h) * 4;
-                u.out[c] = static_cast<char *>(d_out[i]) + ((size_t)c * plane + (size_t)t.y0 * inf.width + t.x0) * ob;
+                u.out[c] = out + ((size_t)c * plane + (size_t)t.y0 * inf.width + t.x0) * ob;
             }
-            u.scratch = static_cast<char *>(P->scratch.ptr) + P->scratch_off[i] + im.tile_scratch[k];
+            u.out_pitch = inf.width;
+            u.scratch = scratch + im.tile_scratch[k];
             units.push_back(u);
         }
     }
     const size_t nu = units.size();
-    auto color_of = [](const tc_image_info &inf) {
-        return inf.mct && inf.ncomp >= 3 ? (inf.reversible ? TC_COLOR_RCT : TC_COLOR_ICT) : TC_COLOR_DC;
-    };
     // images without a transform: colour only
     for (const Unit &u : units) {
         const tc_image_info &inf = *u.inf;
         if (inf.levels) continue;
         const int ob = sample_bytes(inf.bits);
-        e = launch_color_inverse(ctx, color_of(inf), inf.ncomp, u.coef, inf.reversible ? TC_INT32 : TC_FLOAT32, u.w,
-                                 u.out, ob == 1 ? TC_U8 : TC_U16, inf.width, u.w, u.h, out_bits(inf));
+        e = launch_color_inverse(ctx, u.color, u.ncomp, u.coef, inf.reversible ? TC_INT32 : TC_FLOAT32, u.w, u.out,
+                                 ob == 1 ? TC_U8 : TC_U16, u.out_pitch, u.w, u.h, out_bits(inf));
         if (e != cudaSuccess) return cuda_status(ctx, e, "colour");
     }
     if (outs != P->jobs_outs) {
@@ -434,7 +493,7 @@ static int run_reverse_batched(tc_plan *P, void *const *d_out)
             const Unit &u = units[i];
             Walk &W = wk[i];
             level_sizes(u.w, u.h, u.inf->levels, W.ws, W.hs);
-            for (int c = 0; c < u.inf->ncomp; c++) W.src[c] = u.coef[c];
+            for (int c = 0; c < u.ncomp; c++) W.src[c] = u.coef[c];
             W.src_pitch = u.w;
             W.slab = u.inf->levels >= 1 ? (size_t)W.ws[1] * W.hs[1] * 4 : 0;
             maxl = std::max(maxl, u.inf->levels);
@@ -452,7 +511,7 @@ static int run_reverse_batched(tc_plan *P, void *const *d_out)
                     if (l < 2 || (inf.reversible ? 0 : 1) != wv) continue;
                     Walk &W = wk[i];
                     const int buf = (inf.levels - l) & 1;
-                    for (int c = 0; c < inf.ncomp; c++) {
+                    for (int c = 0; c < u.ncomp; c++) {
                         RevJob J{};
                         J.io.w = W.ws[l - 1];
                         J.io.h = W.hs[l - 1];
@@ -468,7 +527,7 @@ static int run_reverse_batched(tc_plan *P, void *const *d_out)
                         tiles += J.tiles_x * ((J.io.h + ty - 1) / ty);
                         jobs.push_back(J);
                     }
-                    for (int c = 0; c < inf.ncomp; c++) W.src[c] = u.scratch + ((size_t)c * 2 + buf) * W.slab;
+                    for (int c = 0; c < u.ncomp; c++) W.src[c] = u.scratch + ((size_t)c * 2 + buf) * W.slab;
                     W.src_pitch = W.ws[1];
                 }
                 if ((int)jobs.size() > first)
@@ -477,7 +536,8 @@ static int run_reverse_batched(tc_plan *P, void *const *d_out)
             // last levels with colour, by kernel instance
             std::vector<char> taken(nu, 0);
             for (size_t i0 = 0; i0 < nu; i0++) {
-                const tc_image_info &a = *units[i0].inf;
+                const Unit &ua = units[i0];
+                const tc_image_info &a = *ua.inf;
                 if (taken[i0] || a.levels - t != 1) continue;
                 const int first = (int)jobs.size();
                 int tiles = 0, tx, ty;
@@ -486,20 +546,20 @@ static int run_reverse_batched(tc_plan *P, void *const *d_out)
                 for (size_t i = i0; i < nu; i++) {
                     const Unit &u = units[i];
                     const tc_image_info &inf = *u.inf;
-                    if (taken[i] || inf.levels - t != 1 || inf.reversible != a.reversible ||
-                        color_of(inf) != color_of(a) || inf.ncomp != a.ncomp ||
-                        sample_bytes(inf.bits) != sample_bytes(a.bits) || out_bits(inf) != out_bits(a))
+                    if (taken[i] || inf.levels - t != 1 || inf.reversible != a.reversible || u.color != ua.color ||
+                        u.ncomp != ua.ncomp || sample_bytes(inf.bits) != sample_bytes(a.bits) ||
+                        out_bits(inf) != out_bits(a))
                         continue;
                     taken[i] = 1;
                     Walk &W = wk[i];
                     RevJob J{};
                     J.io.w = W.ws[0];
                     J.io.h = W.hs[0];
-                    J.io.ncomp = inf.ncomp;
+                    J.io.ncomp = u.ncomp;
                     J.io.ll_pitch = W.src_pitch;
                     J.io.coef_pitch = u.w;
-                    J.io.out_pitch = inf.width;
-                    for (int c = 0; c < inf.ncomp; c++) {
+                    J.io.out_pitch = u.out_pitch;
+                    for (int c = 0; c < u.ncomp; c++) {
                         J.io.ll[c] = W.src[c];
                         J.io.coef[c] = u.coef[c];
                         J.io.out[c] = u.out[c];
@@ -509,7 +569,7 @@ static int run_reverse_batched(tc_plan *P, void *const *d_out)
                     tiles += J.tiles_x * ((J.io.h + ty - 1) / ty);
                     jobs.push_back(J);
                 }
-                launches.push_back({first, (int)jobs.size() - first, tiles, wv, color_of(a), a.ncomp,
+                launches.push_back({first, (int)jobs.size() - first, tiles, wv, ua.color, ua.ncomp,
                                     sample_bytes(a.bits) == 1 ? TC_U8 : TC_U16, out_bits(a)});
             }
         }
@@ -1212,6 +1272,9 @@ int tc_encode_j2k_gpu(tc_ctx *ctx, const tc_encode_params *p, const void *h_plan
     std::string err;
     EncodeLayout L;
     if ((rc = encode_layout(*p, L, err))) return fail(ctx, rc, err);
+    for (int c = 0; c < p->ncomp; c++)
+        if (L.dx[c] != 1 || L.dy[c] != 1)
+            return fail(ctx, TC_E_UNSUPPORTED, "tc_encode_j2k_gpu: subsampled components (use tc_encode_j2k)");
     const int W = p->width, H = p->height, C = p->ncomp, B = p->bits, NL = p->levels;
     const size_t np = (size_t)W * H;
     const int sb = B <= 8 ? 1 : 2;

@@ -791,6 +791,8 @@ struct Params {
     // anchored at (xto, yto)
     int64_t xs = 0, ys = 0, xo = 0, yo = 0, xto = 0, yto = 0;
     int tw = 0, th = 0;
+    int dx[4] = {1, 1, 1, 1}, dy[4] = {1, 1, 1, 1};  // component subsampling XRsiz, YRsiz
+    bool subsampled = false;
     Scope main;
     int levels = 0;  // decomposition levels, shared by every component and tile
     bool have_siz = false;
@@ -1005,7 +1007,12 @@ static int parse_main(Reader &rd, Params &P, std::string &err)
             for (uint32_t i = 0; i < c; i++) {
                 const uint32_t ss = rd.u8(), dx = rd.u8(), dy = rd.u8();
                 const int b = (int)(ss & 0x7F) + 1, sg = (int)(ss >> 7);
-                if (dx != 1 || dy != 1) { err = "component subsampling is not supported"; return TC_E_UNSUPPORTED; }
+                if (dx < 1 || dy < 1) { err = "bad component subsampling"; return TC_E_CODESTREAM; }
+                if (i < 4) {
+                    P.dx[i] = (int)dx;
+                    P.dy[i] = (int)dy;
+                }
+                if (dx != 1 || dy != 1) P.subsampled = true;
                 if (i == 0) { P.bits = b; P.is_signed = sg; }
                 else if (b != P.bits || sg != P.is_signed) { err = "components must share bit depth"; return TC_E_UNSUPPORTED; }
             }
@@ -1039,9 +1046,23 @@ static int parse_main(Reader &rd, Params &P, std::string &err)
         return TC_E_CODESTREAM;
     }
     P.levels = P.main.cod.levels;
-    const int rc = check_coding(P, nullptr, err);
+    int rc = check_coding(P, nullptr, err);
     if (rc) return rc;
-    return tile_grid(P, err);
+    if ((rc = tile_grid(P, err))) return rc;
+    if (P.subsampled) {
+        // subsampled components: one tile at the origin; the colour
+        // transform only over components 0-2 of one size
+        if (P.tiles.size() != 1 || P.xo || P.yo) {
+            err = "subsampled components in tiled or offset images are not supported";
+            return TC_E_UNSUPPORTED;
+        }
+        if (P.main.mct && P.ncomp >= 3 &&
+            (P.dx[1] != P.dx[0] || P.dx[2] != P.dx[0] || P.dy[1] != P.dy[0] || P.dy[2] != P.dy[0])) {
+            err = "a colour transform over components of different sizes";
+            return TC_E_CODESTREAM;
+        }
+    }
+    return TC_OK;
 }
 
 // Image information from the main header (COD and QCD; per-component COC /
@@ -1065,6 +1086,10 @@ static void fill_info(const Params &P, tc_image_info &info)
     info.guard_bits = P.main.qcd.guard;
     info.quant_style = P.main.qcd.qstyle;
     info.ntiles = (uint32_t)P.tiles.size();
+    for (int c = 0; c < 4; c++) {
+        info.comp_dx[c] = (uint8_t)(c < P.ncomp ? P.dx[c] : 1);
+        info.comp_dy[c] = (uint8_t)(c < P.ncomp ? P.dy[c] : 1);
+    }
 }
 
 static int read_raw_header(const uint8_t *cs, size_t len, tc_image_info &info, std::string &err)
@@ -1145,7 +1170,6 @@ static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Para
 {
     int rc;
     if ((rc = check_coding(P, &ts, err))) return rc;
-    const int tw = (int)(T.x1 - T.x0), th = (int)(T.y1 - T.y0);
     const Scope &cs_ = cod_scope(P, &ts);
     const int NL = P.levels, R = NL + 1, C = P.ncomp, L = cs_.layers, scod = cs_.scod, prog = cs_.prog;
     const bool reversible = P.main.cod.reversible != 0;
@@ -1173,19 +1197,29 @@ static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Para
     // where the tile is.
     std::vector<std::vector<Resolution>> geo(C);
     std::vector<std::vector<ResState>> st(C, std::vector<ResState>(R));
+    // the tile on each component's grid (ISO B.3: ceil of the reference-grid
+    // box over the subsampling), its plane size and offset in the arena
+    std::vector<Params::Tile> tc(C);
+    std::vector<uint64_t> coff(C + 1, 0);
+    for (int c = 0; c < C; c++) {
+        const int64_t dx = c < 4 ? P.dx[c] : 1, dy = c < 4 ? P.dy[c] : 1;
+        tc[c] = Params::Tile{(T.x0 + dx - 1) / dx, (T.y0 + dy - 1) / dy, (T.x1 + dx - 1) / dx, (T.y1 + dy - 1) / dy};
+        coff[c + 1] = coff[c] + (uint64_t)(tc[c].x1 - tc[c].x0) * (tc[c].y1 - tc[c].y0);
+    }
     int64_t nprec_bands = 0;
     for (int c = 0; c < C; c++) {
         const Coding &cd = coding_of(P, &ts, c);
-        geo[c] = make_geometry(tw, th, NL, cd.xcb, cd.ycb);
+        const Params::Tile &Tc = tc[c];
+        geo[c] = make_geometry((int)(Tc.x1 - Tc.x0), (int)(Tc.y1 - Tc.y0), NL, cd.xcb, cd.ycb);
         for (int r = 0; r <= NL; r++) {
             const int px = cd.ppx[r], py = cd.ppy[r];
             const int xcb = std::min(cd.xcb, r ? px - 1 : px), ycb = std::min(cd.ycb, r ? py - 1 : py);
             if (xcb < 0 || ycb < 0) { err = "bad precinct size"; return TC_E_CODESTREAM; }
             const int sh = NL - r;
             ResState &rs = st[c][r];
-            const int64_t rx1 = (T.x1 + ((int64_t)1 << sh) - 1) >> sh, ry1 = (T.y1 + ((int64_t)1 << sh) - 1) >> sh;
-            rs.rx0 = (T.x0 + ((int64_t)1 << sh) - 1) >> sh;
-            rs.ry0 = (T.y0 + ((int64_t)1 << sh) - 1) >> sh;
+            const int64_t rx1 = (Tc.x1 + ((int64_t)1 << sh) - 1) >> sh, ry1 = (Tc.y1 + ((int64_t)1 << sh) - 1) >> sh;
+            rs.rx0 = (Tc.x0 + ((int64_t)1 << sh) - 1) >> sh;
+            rs.ry0 = (Tc.y0 + ((int64_t)1 << sh) - 1) >> sh;
             rs.px = px;
             rs.py = py;
             rs.pw = (int)(((rx1 + ((int64_t)1 << px) - 1) >> px) - (rs.rx0 >> px));
@@ -1195,8 +1229,8 @@ static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Para
             for (Band &b : geo[c][r].bands) {
                 b.cbw_log2 = xcb;
                 b.cbh_log2 = ycb;
-                b.ox = (int)((T.x0 >> b.level) & ((1 << xcb) - 1));
-                b.oy = (int)((T.y0 >> b.level) & ((1 << ycb) - 1));
+                b.ox = (int)((Tc.x0 >> b.level) & ((1 << xcb) - 1));
+                b.oy = (int)((Tc.y0 >> b.level) & ((1 << ycb) - 1));
                 b.ncbx = b.w > 0 ? ceil_div(b.ox + b.w, 1 << xcb) : 0;
                 b.ncby = b.h > 0 ? ceil_div(b.oy + b.h, 1 << ycb) : 0;
             }
@@ -1210,7 +1244,7 @@ static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Para
                     for (const Band &b : geo[c][r].bands) {
                         PrecBand pb;
                         // the band and the precinct cell on the band's grid
-                        const int64_t bx0 = T.x0 >> b.level, by0 = T.y0 >> b.level;
+                        const int64_t bx0 = Tc.x0 >> b.level, by0 = Tc.y0 >> b.level;
                         const int64_t cx0 = std::max(bx0, (kx0 + p) << ppx);
                         const int64_t cx1 = std::min(bx0 + b.w, (kx0 + p + 1) << ppx);
                         const int64_t cy0 = std::max(by0, (ky0 + q) << ppy);
@@ -1318,22 +1352,27 @@ static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Para
     // Position-driven orders (ISO B.12.1.3-B.12.1.5) visit a precinct at the
     // first reference-grid position it covers, stepping over the tile by the
     // smallest precinct of any component and resolution.
+    auto cdx = [&](int c) -> int64_t { return c < 4 ? P.dx[c] : 1; };
+    auto cdy = [&](int c) -> int64_t { return c < 4 ? P.dy[c] : 1; };
     int64_t dx = INT64_MAX, dy = INT64_MAX;
     for (int c = 0; c < C; c++)
         for (int r = 0; r <= NL; r++) {
-            dx = std::min<int64_t>(dx, (int64_t)1 << (st[c][r].px + NL - r));
-            dy = std::min<int64_t>(dy, (int64_t)1 << (st[c][r].py + NL - r));
+            dx = std::min<int64_t>(dx, cdx(c) << (st[c][r].px + NL - r));
+            dy = std::min<int64_t>(dy, cdy(c) << (st[c][r].py + NL - r));
         }
-    // precinct of component c, resolution r that starts at (x, y), or -1
+    // precinct of component c, resolution r that starts at reference-grid
+    // position (x, y), or -1 (the component's subsampling scales its grid)
     auto prec_at = [&](int c, int r, int64_t x, int64_t y) -> int {
         const ResState &rs = st[c][r];
         const int sh = NL - r, px = rs.px, py = rs.py;
-        const int64_t mx = ((int64_t)1 << (px + sh)) - 1, my = ((int64_t)1 << (py + sh)) - 1;
-        const bool sx = !(x & mx) || (x == T.x0 && ((rs.rx0 << sh) & mx));
-        const bool sy = !(y & my) || (y == T.y0 && ((rs.ry0 << sh) & my));
+        const int64_t sx_ = cdx(c) << (px + sh), sy_ = cdy(c) << (py + sh);
+        const int64_t pmx = ((int64_t)1 << (px + sh)) - 1, pmy = ((int64_t)1 << (py + sh)) - 1;
+        const bool sx = x % sx_ == 0 || (x == T.x0 && ((rs.rx0 << sh) & pmx));
+        const bool sy = y % sy_ == 0 || (y == T.y0 && ((rs.ry0 << sh) & pmy));
         if (!sx || !sy) return -1;
-        const int64_t kx = (((x + ((int64_t)1 << sh) - 1) >> sh) >> px) - (rs.rx0 >> px);
-        const int64_t ky = (((y + ((int64_t)1 << sh) - 1) >> sh) >> py) - (rs.ry0 >> py);
+        const int64_t ux = cdx(c) << sh, uy = cdy(c) << sh;
+        const int64_t kx = (((x + ux - 1) / ux) >> px) - (rs.rx0 >> px);
+        const int64_t ky = (((y + uy - 1) / uy) >> py) - (rs.ry0 >> py);
         if (kx < 0 || ky < 0 || kx >= rs.pw || ky >= rs.ph) return -1;
         return (int)(ky * rs.pw + kx);
     };
@@ -1405,7 +1444,6 @@ static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Para
 
     // Descriptors, component by component; segments are placed once every
     // tile is read (parse_raw_codestream).
-    const uint64_t plane = (uint64_t)tw * th;
     {
         size_t nb = 0;
         for (int c = 0; c < C; c++)
@@ -1431,8 +1469,9 @@ static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Para
                         d.h = (uint16_t)(std::min((j + 1) * cbh - b.oy, b.h) - cy);
                         d.mb = (uint8_t)b.mb;
                         d.orient = (uint8_t)b.orient;
-                        d.out_pitch = (uint32_t)tw;
-                        d.out_off = coef_off + (uint64_t)c * plane + (uint64_t)(b.y0 + cy) * tw + (uint64_t)(b.x0 + cx);
+                        const int cw = (int)(tc[c].x1 - tc[c].x0);
+                        d.out_pitch = (uint32_t)cw;
+                        d.out_off = coef_off + coff[c] + (uint64_t)(b.y0 + cy) * cw + (uint64_t)(b.x0 + cx);
                         d.step = reversible ? 1.0f : b.step;
                         d.flags = reversible ? 0 : TC_CBLK_IRREVERSIBLE;
                         em.first.push_back((uint32_t)em.segs.size());
@@ -1528,7 +1567,11 @@ static int parse_raw_codestream(const uint8_t *cs, size_t len, Parsed &out, std:
         ti.h = (int32_t)(T.y1 - T.y0);
         ti.coef_off = coef_off;
         out.tiles.push_back(ti);
-        coef_off += (uint64_t)P.ncomp * ti.w * ti.h;
+        for (int c = 0; c < P.ncomp; c++) {
+            const int64_t dx = c < 4 ? P.dx[c] : 1, dy = c < 4 ? P.dy[c] : 1;
+            coef_off += (uint64_t)((T.x1 + dx - 1) / dx - (T.x0 + dx - 1) / dx) *
+                        (uint64_t)((T.y1 + dy - 1) / dy - (T.y0 + dy - 1) / dy);
+        }
     }
     em.first.push_back((uint32_t)em.segs.size());
 
@@ -1561,20 +1604,30 @@ int encode_layout(const tc_encode_params &p, EncodeLayout &L, std::string &err)
 {
     const int W = p.width, H = p.height, C = p.ncomp, B = p.bits, NL = p.levels;
     if (W < 1 || H < 1 || W > 65535 || H > 65535 || C < 1 || C > 4 || B < 1 || B > 16 || NL < 0 ||
-        NL > 15 || p.cblk_log2 < 2 || p.cblk_log2 > 6) {
+        NL > 15 || p.cblk_log2 < 2 || p.cblk_log2 > 6 || p.progression < 0 || p.progression > 4) {
         err = "encode parameters out of range";
         return TC_E_ARG;
     }
     if (!p.reversible && !(p.base_step > 0.0)) { err = "base_step must be positive"; return TC_E_ARG; }
-    // Per component: code-block size (COC when it differs from COD) and
-    // step multiplier (QCC when it differs from QCD).
+    // Per component: code-block size (COC when it differs from COD), step
+    // multiplier (QCC when it differs from QCD) and subsampling (SIZ).
     for (int c = 0; c < C; c++) {
         L.cblk[c] = p.comp_cblk_log2[c] > 0 ? p.comp_cblk_log2[c] : p.cblk_log2;
         L.scale[c] = p.comp_step_scale[c] > 0.0 ? p.comp_step_scale[c] : 1.0;
         if (L.cblk[c] < 2 || L.cblk[c] > 6) { err = "code-block size out of range"; return TC_E_ARG; }
+        L.dx[c] = p.comp_dx[c] > 0 ? p.comp_dx[c] : 1;
+        L.dy[c] = p.comp_dy[c] > 0 ? p.comp_dy[c] : 1;
+        if (L.dx[c] > 255 || L.dy[c] > 255) { err = "subsampling out of range"; return TC_E_ARG; }
+        L.cw[c] = (W + L.dx[c] - 1) / L.dx[c];
+        L.ch[c] = (H + L.dy[c] - 1) / L.dy[c];
+        L.coff[c + 1] = L.coff[c] + (size_t)L.cw[c] * L.ch[c];
+    }
+    if (p.mct && C >= 3 && (L.cw[1] != L.cw[0] || L.cw[2] != L.cw[0] || L.ch[1] != L.ch[0] || L.ch[2] != L.ch[0])) {
+        err = "the colour transform needs components 0-2 at one size";
+        return TC_E_ARG;
     }
     L.geo.assign(C, {});
-    for (int c = 0; c < C; c++) L.geo[c] = make_geometry(W, H, NL, L.cblk[c], L.cblk[c]);
+    for (int c = 0; c < C; c++) L.geo[c] = make_geometry(L.cw[c], L.ch[c], NL, L.cblk[c], L.cblk[c]);
     // Quantisation exponent / mantissa / step per band (ISO E.1).
     for (int c = 0; c < C; c++)
         for (int r = 0; r <= NL; r++)
@@ -1618,24 +1671,24 @@ int encode_codestream(const tc_encode_params &p, const void *planes, std::vector
     EncodeLayout L;
     int rc = encode_layout(p, L, err);
     if (rc) return rc;
-    const int W = p.width, H = p.height, C = p.ncomp, B = p.bits, NL = p.levels;
+    const int C = p.ncomp, B = p.bits, NL = p.levels;
     const bool mct = p.mct && C >= 3;
     const int threads = p.threads;
-    const size_t np = (size_t)W * H;
+    const size_t np = (size_t)L.cw[0] * L.ch[0];  // components 0-2 under a colour transform
+    const size_t ntot = L.coff[C];
     const bool wide = B > 8;
 
     std::vector<int32_t> ip;
     std::vector<double> dp;
     const bool sgn = p.is_signed != 0;
-    auto sample = [&](int c, size_t i) -> int32_t {
-        if (sgn) return wide ? ((const int16_t *)planes)[c * np + i] : ((const int8_t *)planes)[c * np + i];
-        return wide ? ((const uint16_t *)planes)[c * np + i] : ((const uint8_t *)planes)[c * np + i];
+    auto sample = [&](size_t i) -> int32_t {
+        if (sgn) return wide ? ((const int16_t *)planes)[i] : ((const int8_t *)planes)[i];
+        return wide ? ((const uint16_t *)planes)[i] : ((const uint8_t *)planes)[i];
     };
     const int32_t dc = sgn ? 0 : 1 << (B - 1);  // ISO G.1.2: unsigned samples only
     if (p.reversible) {
-        ip.resize(np * C);
-        for (int c = 0; c < C; c++)
-            for (size_t i = 0; i < np; i++) ip[c * np + i] = sample(c, i) - dc;
+        ip.resize(ntot);
+        for (size_t i = 0; i < ntot; i++) ip[i] = sample(i) - dc;
         if (mct)
             for (size_t i = 0; i < np; i++) {
                 const int32_t r = ip[i], g = ip[np + i], b = ip[2 * np + i];
@@ -1644,11 +1697,10 @@ int encode_codestream(const tc_encode_params &p, const void *planes, std::vector
                 ip[2 * np + i] = r - g;
             }
         for (int c = 0; c < C; c++)
-            fwd_plane_pitch(ip.data() + c * np, W, H, (size_t)W, NL, fwd53_line, threads);
+            fwd_plane_pitch(ip.data() + L.coff[c], L.cw[c], L.ch[c], (size_t)L.cw[c], NL, fwd53_line, threads);
     } else {
-        dp.resize(np * C);
-        for (int c = 0; c < C; c++)
-            for (size_t i = 0; i < np; i++) dp[c * np + i] = (double)(sample(c, i) - dc);
+        dp.resize(ntot);
+        for (size_t i = 0; i < ntot; i++) dp[i] = (double)(sample(i) - dc);
         if (mct)
             for (size_t i = 0; i < np; i++) {
                 const double R = dp[i], G = dp[np + i], Bl = dp[2 * np + i];
@@ -1657,17 +1709,17 @@ int encode_codestream(const tc_encode_params &p, const void *planes, std::vector
                 dp[2 * np + i] = 0.5 * R - 0.41869 * G - 0.08131 * Bl;
             }
         for (int c = 0; c < C; c++)
-            fwd_plane_pitch(dp.data() + c * np, W, H, (size_t)W, NL, fwd97_line, threads);
+            fwd_plane_pitch(dp.data() + L.coff[c], L.cw[c], L.ch[c], (size_t)L.cw[c], NL, fwd97_line, threads);
     }
 
     // Quantised coefficients.
-    std::vector<int32_t> q(np * C);
+    std::vector<int32_t> q(ntot);
     for (int c = 0; c < C; c++)
         for (int r = 0; r <= NL; r++)
             for (const Band &b : L.geo[c][r].bands)
                 for (int y = b.y0; y < b.y0 + b.h; y++)
                     for (int x = b.x0; x < b.x0 + b.w; x++) {
-                        const size_t i = c * np + (size_t)y * W + x;
+                        const size_t i = L.coff[c] + (size_t)y * L.cw[c] + x;
                         int32_t v;
                         if (p.reversible) {
                             v = ip[i];
@@ -1692,7 +1744,7 @@ int encode_codestream(const tc_encode_params &p, const void *planes, std::vector
         int32_t blk[64 * 64];
         for (int y = 0; y < bh; y++)
             for (int x = 0; x < bw; x++)
-                blk[y * bw + x] = q[jb.c * np + (size_t)(b.y0 + cy + y) * W + b.x0 + cx + x];
+                blk[y * bw + x] = q[L.coff[jb.c] + (size_t)(b.y0 + cy + y) * L.cw[jb.c] + b.x0 + cx + x];
         int zbp = 0;
         if (t1_encode_block(blk, bw, bh, b.orient, 31, 0, words[k], &coded[k].passes, &zbp)) fail = 1;
         coded[k].numbps = 31 - zbp;
@@ -1761,11 +1813,11 @@ int encode_assemble(const tc_encode_params &p, EncodeLayout &L, const std::vecto
     wr.u32(W); wr.u32(H); wr.u32(0); wr.u32(0);
     wr.u32(W); wr.u32(H); wr.u32(0); wr.u32(0);
     wr.u16(C);
-    for (int c = 0; c < C; c++) { wr.u8((B - 1) | (sgn ? 0x80 : 0)); wr.u8(1); wr.u8(1); }
+    for (int c = 0; c < C; c++) { wr.u8((B - 1) | (sgn ? 0x80 : 0)); wr.u8(L.dx[c]); wr.u8(L.dy[c]); }
     wr.u16(M_COD);
     wr.u16(12);
     wr.u8(0);                              // Scod: default precincts, no SOP/EPH
-    wr.u8(p.progression == 1 ? 1 : 0);     // progression (one layer: LRCP == RLCP order)
+    wr.u8(p.progression);                  // progression order
     wr.u16(1);                             // layers
     wr.u8(mct ? 1 : 0);
     wr.u8(NL);
@@ -1868,9 +1920,12 @@ int encode_assemble(const tc_encode_params &p, EncodeLayout &L, const std::vecto
         out.insert(out.end(), hdr.begin(), hdr.end());
         for (int k : order) out.insert(out.end(), coded[k].data, coded[k].data + coded[k].len);
     };
-    if (p.progression == 1) {
-        for (int r = 0; r <= NL; r++)
-            for (int c = 0; c < C; c++) write_packet(r, c);
+    // One layer and one precinct per resolution: LRCP, RLCP and RPCL visit
+    // resolution-major, PCRL and CPRL (every precinct starts at the origin)
+    // component-major.
+    if (p.progression >= 3) {
+        for (int c = 0; c < C; c++)
+            for (int r = 0; r <= NL; r++) write_packet(r, c);
     } else {
         for (int r = 0; r <= NL; r++)
             for (int c = 0; c < C; c++) write_packet(r, c);

@@ -71,6 +71,9 @@ int read_header(const uint8_t *cs, size_t len, tc_image_info &info, std::string 
 struct EncodeLayout {
     int cblk[4] = {6, 6, 6, 6};
     double scale[4] = {1, 1, 1, 1};
+    int dx[4] = {1, 1, 1, 1}, dy[4] = {1, 1, 1, 1};  // component subsampling (XRsiz, YRsiz)
+    int cw[4] = {0, 0, 0, 0}, ch[4] = {0, 0, 0, 0};  // component sizes ceil(W/dx) x ceil(H/dy)
+    size_t coff[5] = {0, 0, 0, 0, 0};                // element offset of each component's plane
     std::vector<std::vector<Resolution>> geo;  // per component
     struct Job {
         int c, r, bi, i, j;  // component, resolution, band, block column, block row

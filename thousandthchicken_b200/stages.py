@@ -321,7 +321,11 @@ class Plan:
                 dt = torch.int8 if info["is_signed"] else torch.uint8
             else:
                 dt = torch.int16  # 16-bit samples, unsigned ones read back as uint16
-            outs.append(torch.empty((info["ncomp"], info["height"], info["width"]), dtype=dt, device=dev))
+            sizes = info["comp_sizes"]
+            if len(set(sizes)) > 1:  # subsampled components: one flat planar buffer (split_components)
+                outs.append(torch.empty(sum(h * w for h, w in sizes), dtype=dt, device=dev))
+            else:
+                outs.append(torch.empty((info["ncomp"], info["height"], info["width"]), dtype=dt, device=dev))
         return outs
 
     def execute(self, outs):
@@ -354,6 +358,16 @@ class Plan:
             pass
 
 
+def split_components(flat, sizes):
+    """Views of a planar output whose components have their own sizes
+    (subsampled components): one [h, w] array per component."""
+    views, off = [], 0
+    for h, w in sizes:
+        views.append(flat[off:off + h * w].reshape(h, w))
+        off += h * w
+    return views
+
+
 class Decoder:
     """Decoder::decode (Decoder.cpp:94-217): codestream in host memory (or a
     file) -> planar samples in host memory."""
@@ -378,6 +392,14 @@ class Decoder:
             dt = np.int8 if hdr.bits <= 8 else np.int16
         else:
             dt = np.uint8 if hdr.bits <= 8 else np.uint16
+        from .codec import _info_dict
+        sizes = _info_dict(hdr)["comp_sizes"]
+        if len(set(sizes)) > 1:
+            # subsampled components: planar at their own sizes, returned as a list
+            flat = np.empty(sum(h * w for h, w in sizes), dt) if out is None else out.reshape(-1)
+            self.ctx.check(L.lib().tc_decode_j2k(self.ctx.handle, buf.ctypes.data, buf.size, flat.ctypes.data,
+                                                 flat.nbytes, None), "tc_decode_j2k")
+            return split_components(flat, sizes)
         shape = (hdr.ncomp, hdr.height, hdr.width)
         if out is None:
             out = np.empty(shape, dt)
