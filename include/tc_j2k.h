@@ -80,9 +80,13 @@ int tc_ctx_t1_group(const tc_ctx *ctx);
  * codestream_image_types.h:30-120 and CodeBlockAdditionalInfo,
  * coefficientcoder_common.h:5-24). */
 typedef struct tc_cblk_desc {
-    uint64_t seg_off;        /* byte offset of the block's codeword in the pool */
+    uint64_t seg_off;        /* byte offset of the block's codeword in the pool;
+                                with style BYPASS or TERMALL, of a 4-byte aligned
+                                table of its codeword segments' lengths (uint32,
+                                little-endian, one per segment the passes span)
+                                that the codeword follows */
     uint64_t out_off;        /* element offset (4-byte elements) of sample (0,0) */
-    uint32_t seg_len;        /* codeword bytes (cblk->length) */
+    uint32_t seg_len;        /* codeword bytes (cblk->length), table excluded */
     uint32_t out_pitch;      /* output row pitch in elements */
     float    step;           /* dequantisation step, irreversible blocks only */
     uint16_t w, h;           /* block size, 1..64 each */
@@ -91,16 +95,31 @@ typedef struct tc_cblk_desc {
     uint8_t  zero_bitplanes; /* Mb - significant_bits */
     uint8_t  orient;         /* 0 LL, 1 HL, 2 LH, 3 HH (type_orient) */
     uint8_t  flags;          /* TC_CBLK_* */
-    uint8_t  reserved[3];
+    uint8_t  style;          /* code-block style, TC_CBLK_STYLE_* (0: none) */
+    uint8_t  reserved[2];
 } tc_cblk_desc;
 
 #define TC_CBLK_IRREVERSIBLE 0x01  /* float output, multiply by step */
+
+/* Code-block style bits (COD / COC SPcod, ISO Table A.19). */
+#define TC_CBLK_STYLE_BYPASS  0x01  /* selective arithmetic coding bypass */
+#define TC_CBLK_STYLE_RESET   0x02  /* contexts reset after each pass */
+#define TC_CBLK_STYLE_TERMALL 0x04  /* every pass terminated */
+#define TC_CBLK_STYLE_VSC     0x08  /* vertically stripe-causal contexts */
+#define TC_CBLK_STYLE_PTERM   0x10  /* predictable termination */
+#define TC_CBLK_STYLE_SEGSYM  0x20  /* segmentation symbols */
 
 /* Output modes of tc_t1_decode. */
 #define TC_T1_OUT_DEQUANT 0  /* int32 (reversible) or float (irreversible) values */
 #define TC_T1_OUT_RAW     1  /* uint32 sign-magnitude, sign at bit 31, magnitude
                                 bit b at bit b+31-Mb: the reference g_decode
                                 output (coefficient_coder.cl:605-626,805-816) */
+
+/* Or-ed into out_mode: the descriptors may carry code-block styles
+ * (tc_cblk_desc.style); every block is decoded by the style-capable kernel.
+ * Without it a block with a style that changes decoding is reported as an
+ * error by tc_ctx_synchronize and left undecoded. */
+#define TC_T1_STYLED      0x10
 
 /* Decode n code-blocks in one persistent launch (one warp per code-block,
  * blocks taken from a device work queue in the order d_order gives; NULL =
@@ -357,6 +376,10 @@ typedef struct tc_encode_params {
      * ceil(width/dx) x ceil(height/dy) plane; the planes follow one another.
      * The colour transform needs components 0-2 at one size. */
     int32_t comp_dx[4], comp_dy[4];
+    /* Code-block style bits (TC_CBLK_STYLE_*) for COD's SPcod; PTERM is
+     * accepted and written, the terminations are the plain ones (ISO D.4.2
+     * allows either encoder). The GPU encoder takes 0 only. */
+    int32_t cblk_style;
 } tc_encode_params;
 
 /* Encode planar samples (8-bit when bits <= 8, else 16-bit; unsigned, or

@@ -15,6 +15,10 @@
  *   quantizer_*_inverse.cl, Quantizer.cpp:37-65   dequantisation
  *   dwt_transform_buffer.cl:102-489, dwt_io.cl:7-38  lifting and mirroring
  *   preprocess_*.cl               colour transforms and DC level shift
+ * The code-block style modes (ISO D.4-D.6: bypass, context reset,
+ * termination on every pass, vertically causal contexts, segmentation
+ * symbols) have no counterpart in the reference, which decodes style 0 only;
+ * they follow the standard and are pinned against OpenJPEG's decoder.
  */
 #include "j2k_oracle.h"
 
@@ -94,6 +98,9 @@ typedef struct {
     int len, bp, ct;
     uint32_t a, c;
     uint8_t idx[NCX], mps[NCX];
+    /* raw (bypass) segment: the bits of d MSB first (ISO D.6) */
+    int raw, rct;
+    uint32_t rbyte;
 } mqdec;
 
 static inline uint32_t mq_byte(const mqdec *m, int i)
@@ -121,19 +128,55 @@ static void mq_bytein(mqdec *m)
     }
 }
 
-static void mq_init(mqdec *m, const uint8_t *d, int len)
+/* The decoder's registers at the start of a codeword segment (INITDEC, ISO
+ * C.3.5); the contexts are left as they are. */
+static void mq_start(mqdec *m, const uint8_t *d, int len)
 {
     m->d = d;
     m->len = len;
     m->bp = 0;
+    m->raw = 0;
     m->c = mq_byte(m, 0) << 16;
     mq_bytein(m);
     m->c <<= 7;
     m->ct -= 7;
     m->a = 0x8000;
+}
+
+/* A raw segment: bits MSB first; a byte after 0xFF holds 7 bits (its MSB is
+ * a stuffed 0), and after 0xFF a byte above 0x8F is a marker that is not
+ * consumed: 1-bits are read from there on, as past the end. */
+static void raw_start(mqdec *m, const uint8_t *d, int len)
+{
+    m->d = d;
+    m->len = len;
+    m->bp = 0;
+    m->raw = 1;
+    m->rct = 0;
+    m->rbyte = 0;
+}
+
+static int raw_bit(mqdec *m)
+{
+    if (m->rct == 0) {
+        const uint32_t b = mq_byte(m, m->bp);
+        if (m->rbyte == 0xFF && b > 0x8F) {
+            m->rct = 8;  /* rbyte stays 0xFF */
+        } else {
+            m->rct = m->rbyte == 0xFF ? 7 : 8;
+            m->rbyte = b;
+            m->bp++;
+        }
+    }
+    m->rct--;
+    return (int)((m->rbyte >> m->rct) & 1u);
+}
+
+/* Initial context states: ISO Table D.7; mqResetDec, coefficient_coder.cl:158-172. */
+static void mq_reset(mqdec *m)
+{
     memset(m->idx, 0, sizeof m->idx);
     memset(m->mps, 0, sizeof m->mps);
-    /* Initial states: ISO Table D.7; mqResetDec, coefficient_coder.cl:158-172. */
     m->idx[0] = 4;
     m->idx[CX_RUN] = 3;
     m->idx[CX_UNI] = 46;
@@ -187,6 +230,12 @@ static int mq_decode(mqdec *m, int cx)
     return d;
 }
 
+/* One decision of a pass: raw in a bypass segment, else MQ with context cx. */
+static int dec_bit(mqdec *m, int cx)
+{
+    return m->raw ? raw_bit(m) : mq_decode(m, cx);
+}
+
 /* ===================== Tier-1 decoder (ISO D) ============================ */
 
 /* Zero-coding context from neighbour significance counts, ISO Table D.1
@@ -212,16 +261,22 @@ typedef struct {
     int w, h, W;          /* W = padded row stride (w + 2) */
     uint8_t *sig, *sgn, *ref, *vis;
     int32_t *mag;
+    int vsc;              /* vertically causal contexts (ISO D.7) */
 } t1st;
 
 #define AT(st, arr, x, y) ((st)->arr[((y) + 1) * (st)->W + (x) + 1])
 
+/* Whether row y's neighbours in row y + 1 count: not across a stripe
+ * boundary under vertically causal contexts. */
+static inline int below_seen(const t1st *s, int y) { return !(s->vsc && (y & 3) == 3); }
+
 static void nb_counts(const t1st *s, int x, int y, int *h, int *v, int *d)
 {
+    const int b = below_seen(s, y);
     *h = AT(s, sig, x - 1, y) + AT(s, sig, x + 1, y);
-    *v = AT(s, sig, x, y - 1) + AT(s, sig, x, y + 1);
+    *v = AT(s, sig, x, y - 1) + (b ? AT(s, sig, x, y + 1) : 0);
     *d = AT(s, sig, x - 1, y - 1) + AT(s, sig, x + 1, y - 1) +
-         AT(s, sig, x - 1, y + 1) + AT(s, sig, x + 1, y + 1);
+         (b ? AT(s, sig, x - 1, y + 1) + AT(s, sig, x + 1, y + 1) : 0);
 }
 
 /* Sign coding, ISO Tables D.2/D.3 (signcxlut, coefficient_coder.cl:406-435). */
@@ -229,8 +284,9 @@ static int decode_sign(mqdec *m, const t1st *s, int x, int y)
 {
     int hc = 0, vc = 0, cx, xr;
 #define CONTRIB(xx, yy) (AT(s, sig, xx, yy) ? (AT(s, sgn, xx, yy) ? -1 : 1) : 0)
+    if (m->raw) return raw_bit(m); /* bypass: the sign bit itself */
     hc = CONTRIB(x - 1, y) + CONTRIB(x + 1, y);
-    vc = CONTRIB(x, y - 1) + CONTRIB(x, y + 1);
+    vc = CONTRIB(x, y - 1) + (below_seen(s, y) ? CONTRIB(x, y + 1) : 0);
 #undef CONTRIB
     hc = hc > 1 ? 1 : (hc < -1 ? -1 : hc);
     vc = vc > 1 ? 1 : (vc < -1 ? -1 : vc);
@@ -262,7 +318,7 @@ static void pass_spp(mqdec *m, t1st *s, int orient, int p)
                 nb_counts(s, x, y, &hh, &vv, &dd);
                 if (hh + vv + dd == 0) continue;
                 AT(s, vis, x, y) = 1;
-                if (mq_decode(m, zc_context(orient, hh, vv, dd)))
+                if (dec_bit(m, zc_context(orient, hh, vv, dd)))
                     become_significant(m, s, x, y, p);
             }
 }
@@ -277,7 +333,7 @@ static void pass_mrp(mqdec *m, t1st *s, int p)
                 nb_counts(s, x, y, &hh, &vv, &dd);
                 /* ISO Table D.4; getMRCX, coefficient_coder.cl:461-469. */
                 cx = AT(s, ref, x, y) ? 16 : (hh + vv + dd ? 15 : 14);
-                if (mq_decode(m, cx)) AT(s, mag, x, y) |= (int32_t)1 << p;
+                if (dec_bit(m, cx)) AT(s, mag, x, y) |= (int32_t)1 << p;
                 AT(s, ref, x, y) = 1;
             }
 }
@@ -316,26 +372,79 @@ static void pass_cup(mqdec *m, t1st *s, int orient, int p)
         }
 }
 
-/* Shared body of the two decode entry points.  Leaves the magnitude/sign
- * state in st and returns the last pass type (0 CUP, 1 SPP, 2 MRP) and the
- * plane it ran on, or -1 when no pass ran. */
+int or_pass_terminates(int style, int t)
+{
+    if (style & OR_STYLE_TERMALL) return 1;
+    if (style & OR_STYLE_BYPASS) return t == 9 || (t >= 10 && t % 3 != 1);
+    return 0;
+}
+
+int or_pass_segments(int style, int passes)
+{
+    int n = passes > 0;
+    for (int t = 0; t + 1 < passes; t++) n += or_pass_terminates(style, t);
+    return n;
+}
+
+/* Pass t of a bypass stream is raw-coded: SPP and MRP from the 11th pass. */
+static int pass_is_raw(int style, int t) { return (style & OR_STYLE_BYPASS) && t >= 10 && t % 3 != 0; }
+
+/* Codeword segments of one block: lens[0..nseg) when given (BYPASS /
+ * TERMALL), else one segment of len bytes. */
+typedef struct {
+    const uint8_t *seg;
+    int len, style, nseg, si;
+    const uint32_t *lens;
+    size_t off;
+} segwalk;
+
+/* Before pass t: start the next codeword segment where one begins. */
+static int begin_pass(mqdec *m, segwalk *g, int t)
+{
+    if (!g->lens) {
+        if (t == 0) mq_start(m, g->seg, g->len);
+        return 0;
+    }
+    if (t > 0 && !or_pass_terminates(g->style, t - 1)) return 0;
+    if (t > 0) g->off += g->lens[g->si++];
+    if (g->si >= g->nseg || g->off + g->lens[g->si] > (size_t)g->len) return -1;
+    if (pass_is_raw(g->style, t)) raw_start(m, g->seg + g->off, (int)g->lens[g->si]);
+    else mq_start(m, g->seg + g->off, (int)g->lens[g->si]);
+    return 0;
+}
+
+/* Shared body of the decode entry points.  Leaves the magnitude/sign state
+ * in st and returns the last pass type (0 CUP, 1 SPP, 2 MRP) and the plane
+ * it ran on, -1 when no pass ran, or -2 for a bad segment table. */
 static int t1_run(const uint8_t *seg, int len, int w, int h, int orient,
-                  int numbps, int passes, t1st *st, int *last_plane)
+                  int numbps, int passes, t1st *st, int *last_plane,
+                  int style, const uint32_t *lens, int nseg)
 {
     mqdec m;
+    segwalk g = {seg, len, style, nseg, 0, lens, 0};
     int type = -1, pi = 0;
-    mq_init(&m, seg, len);
+    memset(&m, 0, sizeof m);
+    mq_reset(&m);
+    st->vsc = (style & OR_STYLE_VSC) != 0;
     *last_plane = numbps;
     for (int p = numbps - 1; p >= 0 && pi < passes; p--) {
         if (p != numbps - 1) {
+            if (begin_pass(&m, &g, pi)) return -2;
             pass_spp(&m, st, orient, p);
+            if (style & OR_STYLE_RESET) mq_reset(&m);
             type = 1; *last_plane = p;
             if (++pi >= passes) break;
+            if (begin_pass(&m, &g, pi)) return -2;
             pass_mrp(&m, st, p);
+            if (style & OR_STYLE_RESET) mq_reset(&m);
             type = 2;
             if (++pi >= passes) break;
         }
+        if (begin_pass(&m, &g, pi)) return -2;
         pass_cup(&m, st, orient, p);
+        if (style & OR_STYLE_SEGSYM) /* segmentation symbol, ISO D.5 */
+            for (int k = 0; k < 4; k++) mq_decode(&m, CX_UNI);
+        if (style & OR_STYLE_RESET) mq_reset(&m);
         type = 0; *last_plane = p;
         ++pi;
         memset(st->vis, 0, (size_t)(st->W) * (st->h + 2));
@@ -370,13 +479,22 @@ static int t1_args_ok(int len, int w, int h, int orient, int numbps, int passes)
 int or_t1_decode(const uint8_t *seg, int len, int w, int h, int orient,
                  int numbps, int passes, int32_t *q, uint8_t *undecoded)
 {
+    return or_t1_decode_style(seg, len, w, h, orient, numbps, passes, 0, NULL, 0, q, undecoded);
+}
+
+int or_t1_decode_style(const uint8_t *seg, int len, int w, int h, int orient,
+                       int numbps, int passes, int style, const uint32_t *lens,
+                       int nseg, int32_t *q, uint8_t *undecoded)
+{
     t1st st;
     int last_plane, type;
     if (!t1_args_ok(len, w, h, orient, numbps, passes)) return -1;
+    if (lens && nseg != or_pass_segments(style, passes)) return -1;
     if (t1_alloc(&st, w, h)) { t1_free(&st); return -2; }
     type = (numbps > 0 && passes > 0)
-               ? t1_run(seg, len, w, h, orient, numbps, passes, &st, &last_plane)
+               ? t1_run(seg, len, w, h, orient, numbps, passes, &st, &last_plane, style, lens, nseg)
                : -1;
+    if (type == -2) { t1_free(&st); return -3; }
     for (int y = 0; y < h; y++)
         for (int x = 0; x < w; x++) {
             const int32_t mg = AT(&st, mag, x, y);
@@ -408,7 +526,7 @@ int or_t1_decode_raw(const uint8_t *seg, int len, int w, int h, int orient,
     if (!t1_args_ok(len, w, h, orient, numbps < 0 ? 0 : numbps, passes)) return -1;
     if (t1_alloc(&st, w, h)) { t1_free(&st); return -2; }
     if (numbps > 0 && passes > 0)
-        t1_run(seg, len, w, h, orient, numbps, passes, &st, &last_plane);
+        t1_run(seg, len, w, h, orient, numbps, passes, &st, &last_plane, 0, NULL, 0);
     for (int y = 0; y < h; y++)
         for (int x = 0; x < w; x++) {
             const uint32_t mg = (uint32_t)AT(&st, mag, x, y);
@@ -747,9 +865,21 @@ static void or_t1_one(void *arg, int i)
     uint8_t u[64 * 64];
     const size_t np = (size_t)J->w * J->h;
     const int numbps = (int)c->mb - (int)c->zero_bitplanes;
+    const int passes = numbps <= 0 ? 0 : c->passes;
+    /* terminated segments: a table of their lengths precedes the codeword */
+    uint32_t lens[256];
+    int nseg = 0;
+    const uint8_t *seg = J->pool + c->seg_off;
+    if ((c->style & (OR_STYLE_BYPASS | OR_STYLE_TERMALL)) && passes > 0) {
+        nseg = or_pass_segments(c->style, passes);
+        for (int k = 0; k < nseg; k++)
+            lens[k] = (uint32_t)seg[4 * k] | (uint32_t)seg[4 * k + 1] << 8 |
+                      (uint32_t)seg[4 * k + 2] << 16 | (uint32_t)seg[4 * k + 3] << 24;
+        seg += 4 * (size_t)nseg;
+    }
     if (c->comp >= J->ncomp || c->out_x + c->w > (uint32_t)J->w || c->out_y + c->h > (uint32_t)J->h ||
-        or_t1_decode(J->pool + c->seg_off, (int)c->seg_len, c->w, c->h, c->orient,
-                     numbps < 0 ? 0 : numbps, numbps <= 0 ? 0 : c->passes, q, u)) {
+        or_t1_decode_style(seg, (int)c->seg_len, c->w, c->h, c->orient, numbps < 0 ? 0 : numbps, passes,
+                           c->style, nseg ? lens : NULL, nseg, q, u)) {
         __atomic_store_n(&J->err, 1, __ATOMIC_RELAXED);
         return;
     }

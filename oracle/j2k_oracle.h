@@ -46,6 +46,27 @@ extern "C" {
 int or_t1_decode(const uint8_t *seg, int len, int w, int h, int orient,
                  int numbps, int passes, int32_t *q, uint8_t *undecoded);
 
+/* Code-block style bits (SPcod, ISO Table A.19). */
+#define OR_STYLE_BYPASS  0x01
+#define OR_STYLE_RESET   0x02
+#define OR_STYLE_TERMALL 0x04
+#define OR_STYLE_VSC     0x08
+#define OR_STYLE_PTERM   0x10
+#define OR_STYLE_SEGSYM  0x20
+
+/* Whether coding pass t (0: the first cleanup pass) ends a codeword segment
+ * (ISO D.4.2, D.6), and how many segments passes [0, passes) span. */
+int or_pass_terminates(int style, int t);
+int or_pass_segments(int style, int passes);
+
+/* or_t1_decode under code-block style `style`: with BYPASS or TERMALL the
+ * codeword is nseg terminated segments of lens[k] bytes one after the other
+ * (nseg = or_pass_segments(style, passes)), else lens is NULL.  Returns -3
+ * for segment lengths that run past len. */
+int or_t1_decode_style(const uint8_t *seg, int len, int w, int h, int orient,
+                       int numbps, int passes, int style, const uint32_t *lens,
+                       int nseg, int32_t *q, uint8_t *undecoded);
+
 /* Same decode, written in the reference kernel's output format: 32-bit
  * sign-magnitude with the sign at bit 31 and magnitude bit b of the
  * coefficient at bit b + 31 - mb (coefficient_coder.cl:605-626,805-816).
@@ -117,7 +138,7 @@ typedef struct or_cblk {
     uint32_t seg_len;
     uint16_t w, h;
     uint8_t passes, mb, zero_bitplanes, orient;
-    uint8_t comp, flags, pad0, pad1;
+    uint8_t comp, flags, style, pad1;  /* style: OR_STYLE_* */
     uint32_t out_x, out_y;   /* position in the component's Mallat plane */
     float step;              /* dequantisation step (irreversible only) */
 } or_cblk;

@@ -6,7 +6,7 @@ import pytest
 
 import oracle as O
 from conftest import golden_cases, load_golden, synth_image
-from test_host_codec import COC_QCC, PRECINCTS, SIGNED, SUBSAMPLED, TILED
+from test_host_codec import COC_QCC, PRECINCTS, SIGNED, STYLE_IDS, STYLES, SUBSAMPLED, TILED
 from thousandthchicken_b200 import codec
 
 pytestmark = pytest.mark.gpu
@@ -405,3 +405,64 @@ def test_subsampled_components_decode(gpu_ctx, w, h, bits, dxy, kw):
     for g, p_ in zip(got, split_components(flat, plan.infos[1]["comp_sizes"])):
         np.testing.assert_array_equal(p_, g)
     plan.close()
+
+
+@pytest.mark.parametrize("style,bits,kw", STYLES, ids=STYLE_IDS)
+def test_code_block_styles_decode(gpu_ctx, style, bits, kw):
+    """Code-block styles through the GPU: the styled blocks run in the
+    style-capable Tier-1 launch (terminated segments from the pool's length
+    tables, raw bypass passes, context resets, vertically causal contexts,
+    segmentation symbols).  Lossless: the original; lossy: within 1 of the
+    oracle."""
+    from gpu_helpers import oracle_decode_tiled
+    from test_host_codec import styled_stream
+    img, cs = styled_stream(style, bits, kw)
+    got = _decoder(gpu_ctx).decode(cs)
+    if kw["reversible"]:
+        np.testing.assert_array_equal(got, img)
+    else:
+        _, want = oracle_decode_tiled(cs)
+        d = np.abs(got.astype(np.int64) - want.astype(np.int64))
+        assert d.max() <= 1 and (d > 0).mean() < 0.01
+
+
+def test_styled_and_plain_streams_in_one_plan(gpu_ctx):
+    """A plan over a styled stream and a style-0 one: the styled blocks form
+    a class of their own after the three bit-plane classes; both images
+    come out as their single decodes."""
+    from test_host_codec import styled_stream
+    from thousandthchicken_b200.stages import Plan
+    img_a, a = styled_stream(0x3F, 8, dict(reversible=True))
+    img_b = synth_image(96, 80, 3, 8, seed=4)
+    b = codec.encode(img_b, 8, levels=3, reversible=True)
+    plan = Plan(gpu_ctx, [a, b])
+    outs = plan.execute(plan.alloc_outputs())
+    gpu_ctx.synchronize()
+    np.testing.assert_array_equal(outs[0].cpu().numpy(), img_a)
+    np.testing.assert_array_equal(outs[1].cpu().numpy(), img_b)
+    plan.close()
+
+
+def test_styled_blocks_in_a_style0_launch_are_errors(gpu_ctx):
+    """tc_t1_decode without TC_T1_STYLED leaves styled blocks undecoded and
+    reports them at the next synchronize; with it they decode like the
+    oracle's Tier-1."""
+    from test_host_codec import styled_stream
+    from thousandthchicken_b200._lib import TCError
+    from thousandthchicken_b200.stages import CoefficientCoder, _dev_bytes
+    import torch
+    img, cs = styled_stream(codec.CBLK_STYLE_BYPASS | codec.CBLK_STYLE_TERMALL, 8, dict(reversible=True))
+    coder = CoefficientCoder(gpu_ctx)
+    info, desc, pool = codec.parse(cs)
+    dev = torch.device("cuda")
+    n = info["ncomp"] * info["width"] * info["height"]
+    out = torch.zeros(n, dtype=torch.int32, device=dev)
+    d_desc, d_pool = _dev_bytes(desc, dev), _dev_bytes(pool, dev)
+    coder.decode(d_desc, d_pool, out, len(desc), styled=False)
+    with pytest.raises(TCError):
+        gpu_ctx.synchronize()
+    gpu_ctx.synchronize()  # the error word was cleared
+    got, _ = coder.decode_tile(cs)
+    plain_cs = codec.encode(img, 8, levels=3, cblk_log2=5, reversible=True)
+    want, _ = coder.decode_tile(plain_cs)
+    np.testing.assert_array_equal(got.cpu().numpy(), want.cpu().numpy())

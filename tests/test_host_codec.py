@@ -535,3 +535,88 @@ def test_subsampled_tiles_are_unsupported():
     with pytest.raises(TCError) as ei:
         codec.read_header(bytes(b))
     assert ei.value.status == TC_E_UNSUPPORTED
+
+
+STYLES = [  # (code-block style bits, bits, harness options)
+    (codec.CBLK_STYLE_BYPASS, 8, dict(reversible=True)),
+    (codec.CBLK_STYLE_RESET, 8, dict(reversible=True)),
+    (codec.CBLK_STYLE_TERMALL, 8, dict(reversible=True)),
+    (codec.CBLK_STYLE_VSC, 8, dict(reversible=True)),
+    (codec.CBLK_STYLE_PTERM, 8, dict(reversible=True)),
+    (codec.CBLK_STYLE_SEGSYM, 8, dict(reversible=True)),
+    (0x3F, 8, dict(reversible=True)),
+    (codec.CBLK_STYLE_BYPASS | codec.CBLK_STYLE_TERMALL, 12, dict(reversible=True, cblk_log2=4)),
+    (codec.CBLK_STYLE_BYPASS | codec.CBLK_STYLE_VSC, 16, dict(reversible=True)),
+    (codec.CBLK_STYLE_RESET | codec.CBLK_STYLE_SEGSYM, 8, dict(reversible=False, base_step=1 / 512)),
+    (0x3F, 12, dict(reversible=False, base_step=1 / 1024)),
+]
+STYLE_IDS = ["bypass", "reset", "termall", "vsc", "pterm", "segsym", "all", "bypass-termall-12",
+             "bypass-vsc-16", "reset-segsym-97", "all-97-12"]
+
+
+def styled_stream(style, bits, kw, w=133, h=91):
+    c = 3 if bits == 8 else 1  # OpenJPEG through Pillow: 16-bit samples as one component
+    img = synth_image(w, h, c, bits, seed=style + bits)
+    opts = dict(levels=3, cblk_log2=5, mct=c >= 3)
+    opts.update(kw)
+    return img, codec.encode(img, bits, cblk_style=style, **opts)
+
+
+@pytest.mark.parametrize("style,bits,kw", STYLES, ids=STYLE_IDS)
+def test_code_block_styles_through_oracle(style, bits, kw):
+    """Code-block styles (SPcod, ISO Table A.19; D.4-D.7): bypass (raw
+    significance and refinement passes from the 11th pass on), context
+    reset, termination on every pass, vertically causal contexts,
+    predictable termination and segmentation symbols, alone and combined.
+    OpenJPEG decodes the harness encoder's streams to the original
+    (lossless); the parser's terminated segments and the oracle's modes give
+    the original too, and within 1 of OpenJPEG for 9/7."""
+    from gpu_helpers import oracle_decode_tiled, openjpeg_decode
+    img, cs = styled_stream(style, bits, kw)
+    info, desc, pool = codec.parse(cs)
+    assert (desc["style"] == style).all()
+    _, out = oracle_decode_tiled(cs)
+    if kw["reversible"]:
+        np.testing.assert_array_equal(out, img)
+        if bits in (8, 16):
+            np.testing.assert_array_equal(openjpeg_decode(cs), img)
+    elif bits == 8:
+        assert np.abs(out.astype(np.int64) - openjpeg_decode(cs)).max() <= 1
+
+
+def test_terminated_segments_have_a_length_table():
+    """With TERMALL every pass is a codeword segment of its own: the block's
+    pool entry starts (4-byte aligned) with one uint32 length per pass, the
+    codeword after it, and the lengths add up to seg_len."""
+    img, cs = styled_stream(codec.CBLK_STYLE_TERMALL, 8, dict(reversible=True))
+    info, desc, pool = codec.parse(cs)
+    assert info["pool_is_cs"] == 0
+    coded = desc[desc["passes"] > 0]
+    assert len(coded) > 10
+    for d in coded:
+        off, n = int(d["seg_off"]), int(d["passes"])
+        assert off % 4 == 0
+        lens = np.frombuffer(pool[off: off + 4 * n].tobytes(), "<u4")
+        assert lens.sum() == d["seg_len"]
+    # bypass alone: segments of 10, then 2 and 1 passes
+    img, cs = styled_stream(codec.CBLK_STYLE_BYPASS, 16, dict(reversible=True))
+    _, desc, pool = codec.parse(cs)
+    deep = desc[desc["passes"] >= 14][0]
+    p = int(deep["passes"])
+    # passes 0-9 form one segment; from pass 10 on, {SPP, MRP} and {CUP}
+    n = 1 + len({(t - 10) // 3 * 2 + ((t - 10) % 3 == 2) for t in range(10, p)})
+    assert O.lib().or_pass_segments(int(deep["style"]), p) == n
+    off = int(deep["seg_off"])
+    assert np.frombuffer(pool[off: off + 4 * n].tobytes(), "<u4").sum() == deep["seg_len"]
+
+
+def test_unknown_style_bits_are_rejected():
+    img, cs = styled_stream(0, 8, dict(reversible=True))
+    i = cs.find(b"\xff\x52")
+    bad = bytearray(cs)
+    bad[i + 2 + 2 + 1 + 1 + 2 + 1 + 1 + 2] = 0x40  # SPcod code-block style
+    with pytest.raises(TCError) as e:
+        codec.parse(bytes(bad))
+    assert e.value.status == TC_E_UNSUPPORTED
+    with pytest.raises(TCError):
+        codec.encode(img, 8, cblk_style=0x40)

@@ -23,7 +23,7 @@ TC_E_NOFILE = -7
 
 TC_U8, TC_U16, TC_INT32, TC_FLOAT32 = 1, 2, 3, 4
 TC_CBLK_IRREVERSIBLE = 1
-TC_T1_OUT_DEQUANT, TC_T1_OUT_RAW = 0, 1
+TC_T1_OUT_DEQUANT, TC_T1_OUT_RAW, TC_T1_STYLED = 0, 1, 0x10
 TC_ROUND_FLOOR, TC_ROUND_TRUNC = 0, 1
 TC_COLOR_DC, TC_COLOR_RCT, TC_COLOR_ICT = 0, 1, 2
 
@@ -49,7 +49,7 @@ class CblkDesc(C.Structure):
     _fields_ = [("seg_off", C.c_uint64), ("out_off", C.c_uint64), ("seg_len", C.c_uint32),
                 ("out_pitch", C.c_uint32), ("step", C.c_float), ("w", C.c_uint16), ("h", C.c_uint16),
                 ("passes", C.c_uint8), ("mb", C.c_uint8), ("zero_bitplanes", C.c_uint8),
-                ("orient", C.c_uint8), ("flags", C.c_uint8), ("reserved", C.c_uint8 * 3)]
+                ("orient", C.c_uint8), ("flags", C.c_uint8), ("style", C.c_uint8), ("reserved", C.c_uint8 * 2)]
 
 
 class ImageInfo(C.Structure):
@@ -77,7 +77,7 @@ class EncodeParams(C.Structure):
                 ("cblk_log2", C.c_int32), ("base_step", C.c_double), ("guard_bits", C.c_int32),
                 ("progression", C.c_int32), ("threads", C.c_int32), ("is_signed", C.c_int32),
                 ("comp_cblk_log2", C.c_int32 * 4), ("comp_step_scale", C.c_double * 4),
-                ("comp_dx", C.c_int32 * 4), ("comp_dy", C.c_int32 * 4)]
+                ("comp_dx", C.c_int32 * 4), ("comp_dy", C.c_int32 * 4), ("cblk_style", C.c_int32)]
 
 
 assert C.sizeof(CblkDesc) == 40

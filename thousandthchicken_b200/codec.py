@@ -12,7 +12,8 @@ from . import _lib as L
 # numpy view of tc_cblk_desc (include/tc_j2k.h)
 DESC_DTYPE = np.dtype([("seg_off", "<u8"), ("out_off", "<u8"), ("seg_len", "<u4"), ("out_pitch", "<u4"),
                        ("step", "<f4"), ("w", "<u2"), ("h", "<u2"), ("passes", "u1"), ("mb", "u1"),
-                       ("zero_bitplanes", "u1"), ("orient", "u1"), ("flags", "u1"), ("reserved", "u1", (3,))])
+                       ("zero_bitplanes", "u1"), ("orient", "u1"), ("flags", "u1"), ("style", "u1"),
+                       ("reserved", "u1", (2,))])
 assert DESC_DTYPE.itemsize == 40
 
 INFO_FIELDS = ("width", "height", "ncomp", "bits", "is_signed", "levels", "reversible", "mct", "cblk_w",
@@ -58,6 +59,7 @@ def parse(cs):
         p = out.contents
         info = _info_dict(p.info)
         info["tiles"] = [(t.x0, t.y0, t.w, t.h, t.coef_off) for t in p.tiles[:info["ntiles"]]]
+        info["pool_is_cs"] = int(p.pool_is_cs)  # segments read in place from the codestream
         n = info["ncblk"]
         desc = np.empty(n, DESC_DTYPE)
         if n:
@@ -71,6 +73,11 @@ def parse(cs):
     finally:
         L.lib().tc_j2k_parsed_free(out)
     return info, desc, pool
+
+
+# Code-block style bits (COD / COC SPcod, ISO Table A.19).
+CBLK_STYLE_BYPASS, CBLK_STYLE_RESET, CBLK_STYLE_TERMALL = 0x01, 0x02, 0x04
+CBLK_STYLE_VSC, CBLK_STYLE_PTERM, CBLK_STYLE_SEGSYM = 0x08, 0x10, 0x20
 
 
 def _encode_params(planes, bits, levels, reversible, mct, cblk_log2, base_step, guard_bits, progression, threads,
@@ -132,15 +139,18 @@ def encode_gpu(ctx, planes: np.ndarray, bits: int, levels: int = 5, reversible: 
 
 def encode(planes: np.ndarray, bits: int, levels: int = 5, reversible: bool = True, mct: bool = True,
            cblk_log2: int = 6, base_step: float = 1.0 / 128, guard_bits: int = 0, progression: int = 0,
-           threads: int = 0, comp_cblk_log2=None, comp_step_scale=None, comp_subsampling=None) -> bytes:
+           threads: int = 0, comp_cblk_log2=None, comp_step_scale=None, comp_subsampling=None,
+           cblk_style: int = 0) -> bytes:
     """Harness encoder: planar samples [ncomp, h, w] -> codestream; signed
     integer arrays (int8 / int16) give signed components (no DC shift).
     comp_cblk_log2 / comp_step_scale: per-component code-block size exponent
     and irreversible step multiplier (0 = the image-wide value), written as
     COC / QCC marker segments.  comp_subsampling: per component (dx, dy);
-    planes is then a list of component arrays of ceil(h/dy) x ceil(w/dx)."""
+    planes is then a list of component arrays of ceil(h/dy) x ceil(w/dx).
+    cblk_style: code-block style bits (CBLK_STYLE_*) for every component."""
     planes, p = _encode_params(planes, bits, levels, reversible, mct, cblk_log2, base_step, guard_bits, progression,
                                threads, comp_cblk_log2, comp_step_scale, comp_subsampling)
+    p.cblk_style = int(cblk_style)
     cap = planes.nbytes * 3 + 65536
     out = np.empty(cap, np.uint8)
     n = C.c_size_t(0)

@@ -197,20 +197,19 @@ static int run_reverse(tc_ctx *ctx, int wavelet, int rounding, const void *const
     return TC_OK;
 }
 
-void t1_class_order(const tc_cblk_desc *h_desc, int n, uint32_t *h_order, int counts[3])
+void t1_class_order(const tc_cblk_desc *h_desc, int n, uint32_t *h_order, int counts[4])
 {
     std::vector<uint32_t> all(n);
     tc_t1_sort_order(h_desc, n, all.data());
-    counts[0] = counts[1] = counts[2] = 0;
-    std::vector<uint32_t> cls[3];
+    std::vector<uint32_t> cls[4];
     for (uint32_t i : all) {
         const tc_cblk_desc &d = h_desc[i];
         const int nb = d.passes ? (int)d.mb - (int)d.zero_bitplanes : 0;
-        const int k = nb <= 8 ? 0 : (nb <= 16 ? 1 : 2);
+        const int k = (d.style & kStyleDecodeBits) ? 3 : (nb <= 8 ? 0 : (nb <= 16 ? 1 : 2));
         cls[k].push_back(i);
     }
     int o = 0;
-    for (int k = 0; k < 3; k++) {
+    for (int k = 0; k < 4; k++) {
         counts[k] = (int)cls[k].size();
         for (uint32_t i : cls[k]) h_order[o++] = i;
     }
@@ -260,7 +259,7 @@ struct tc_plan {
     // (tc_decode_j2k): its host address and length
     const void *preloaded = nullptr;
     uint64_t preloaded_len = 0;
-    int class_counts[3] = {0, 0, 0};  // Tier-1 blocks of <= 8, <= 16, <= 31 coded bit-planes
+    int class_counts[4] = {0, 0, 0, 0};  // Tier-1 blocks of <= 8, <= 16, <= 31 coded bit-planes, styled
     bool profiling = false;
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
     // graph replay of execute (tc_plan_set_graph)
@@ -609,7 +608,7 @@ static int plan_run(tc_plan *P, void *const *d_out)
                                       static_cast<uint32_t *>(P->order.ptr), P->ncblk, P->class_counts[0],
                                       P->class_counts[1], P->class_counts[2],
                                       static_cast<uint8_t *>(P->pool.ptr), P->pool_len, P->coef.ptr,
-                                      TC_T1_OUT_DEQUANT, P->recon_r);
+                                      TC_T1_OUT_DEQUANT, P->recon_r, P->class_counts[3]);
     if (e != cudaSuccess) return cuda_status(ctx, e, "Tier-1 launch");
     if (P->profiling) cudaEventRecord(P->ev[1], ctx->stream);
     if (plan_batched(P)) {
@@ -679,8 +678,8 @@ int tc_ctx_create(int device, void *cuda_stream, tc_ctx **out)
     ctx->device = device;
     ctx->stream = static_cast<cudaStream_t>(cuda_stream);
     cudaError_t e = cudaSetDevice(device);
-    if (e == cudaSuccess) e = cudaMalloc(&ctx->d_words, 4 * sizeof(uint32_t));
-    if (e == cudaSuccess) e = cudaMemset(ctx->d_words, 0, 4 * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&ctx->d_words, 8 * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMemset(ctx->d_words, 0, 8 * sizeof(uint32_t));
     if (e != cudaSuccess) {
         delete ctx;
         return e == cudaErrorMemoryAllocation ? TC_E_OOM : TC_E_DEVICE;
@@ -734,8 +733,9 @@ int tc_ctx_synchronize(tc_ctx *ctx)
     if (w) {
         cudaMemset(ctx->d_words, 0, sizeof w);
         return fail(ctx, TC_E_CODESTREAM,
-                    (w & TC_DERR_POOL) ? "a code-block codeword runs past the segment pool"
-                                       : "a code-block descriptor is out of range");
+                    (w & TC_DERR_POOL)    ? "a code-block codeword runs past the segment pool"
+                    : (w & TC_DERR_STYLE) ? "a code-block style this launch does not decode, or a bad segment table"
+                                          : "a code-block descriptor is out of range");
     }
     return TC_OK;
 }
@@ -759,7 +759,8 @@ int tc_t1_decode(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint32_t *d_orde
     int rc = check_ctx(ctx);
     if (rc) return rc;
     if (n < 0 || (n > 0 && (!d_desc || !d_out || (!d_pool && pool_len))) ||
-        (out_mode != TC_T1_OUT_DEQUANT && out_mode != TC_T1_OUT_RAW) || !(recon_r >= 0.0f && recon_r < 1.0f))
+        ((out_mode & ~TC_T1_STYLED) != TC_T1_OUT_DEQUANT && (out_mode & ~TC_T1_STYLED) != TC_T1_OUT_RAW) ||
+        !(recon_r >= 0.0f && recon_r < 1.0f))
         return fail(ctx, TC_E_ARG, "tc_t1_decode: bad argument");
     if (max_bitplanes <= 0 || max_bitplanes > 31) max_bitplanes = 31;
     return cuda_status(ctx,
@@ -1275,6 +1276,8 @@ int tc_encode_j2k_gpu(tc_ctx *ctx, const tc_encode_params *p, const void *h_plan
     for (int c = 0; c < p->ncomp; c++)
         if (L.dx[c] != 1 || L.dy[c] != 1)
             return fail(ctx, TC_E_UNSUPPORTED, "tc_encode_j2k_gpu: subsampled components (use tc_encode_j2k)");
+    if (p->cblk_style)
+        return fail(ctx, TC_E_UNSUPPORTED, "tc_encode_j2k_gpu: code-block style modes (use tc_encode_j2k)");
     const int W = p->width, H = p->height, C = p->ncomp, B = p->bits, NL = p->levels;
     const size_t np = (size_t)W * H;
     const int sb = B <= 8 ? 1 : 2;

@@ -248,9 +248,25 @@ struct MQEnc {
     {
         buf.reserve(4096);
         buf.push_back(0);
+        reset_contexts();
+    }
+    // Initial probability states (ISO Table D.7).
+    void reset_contexts()
+    {
+        for (int i = 0; i < 19; i++) idx[i] = mps[i] = 0;
         idx[0] = 4;
         idx[18] = 3;
         idx[17] = 46;
+    }
+    // A new codeword segment (after a termination): the coder registers
+    // start over, the contexts carry on.
+    void restart()
+    {
+        buf.assign(1, 0);
+        bp = 0;
+        a = 0x8000;
+        c = 0;
+        ct = 12;
     }
     void put(uint32_t v)
     {
@@ -326,6 +342,57 @@ struct MQEnc {
     }
 };
 
+// Raw (bypass) coding of ISO D.6: bits stored MSB first; a byte that
+// follows 0xFF carries 7 bits (its MSB is a stuffed 0).  A segment that
+// would end on 0xFF gets a zero byte, so it never ends on a marker prefix.
+struct RawEnc {
+    std::vector<uint8_t> buf;
+    uint32_t cur = 0;
+    int ct = 8;
+    void restart()
+    {
+        buf.clear();
+        cur = 0;
+        ct = 8;
+    }
+    void put(uint32_t b)
+    {
+        cur = (cur << 1) | (b & 1u);
+        if (--ct == 0) {
+            buf.push_back((uint8_t)cur);
+            ct = cur == 0xFF ? 7 : 8;
+            cur = 0;
+        }
+    }
+    size_t flush()
+    {
+        const int full = !buf.empty() && buf.back() == 0xFF ? 7 : 8;
+        if (ct < full) buf.push_back((uint8_t)(cur << ct));
+        if (!buf.empty() && buf.back() == 0xFF) buf.push_back(0);
+        return buf.size();
+    }
+};
+
+// Whether coding pass t (0: the first cleanup pass) ends a codeword
+// segment under code-block style `style` (ISO D.4.2, D.6): every pass with
+// TERMALL; with BYPASS the tenth pass, then each raw SPP+MRP pair and each
+// cleanup pass after it.
+inline bool pass_terminates(int style, int t)
+{
+    if (style & TC_CBLK_STYLE_TERMALL) return true;
+    if (style & TC_CBLK_STYLE_BYPASS) return t == 9 || (t >= 10 && t % 3 != 1);
+    return false;
+}
+// Whether pass t is raw-coded (BYPASS: SPP and MRP passes from the 11th on).
+inline bool pass_raw(int style, int t) { return (style & TC_CBLK_STYLE_BYPASS) && t >= 10 && t % 3 != 0; }
+// Codeword segments that passes [0, passes) span.
+inline int pass_segments(int style, int passes)
+{
+    int n = passes > 0;
+    for (int t = 0; t + 1 < passes; t++) n += pass_terminates(style, t);
+    return n;
+}
+
 // ============================ Tier-1 encoder (ISO D) ========================
 
 namespace {
@@ -335,11 +402,14 @@ struct T1Enc {
     std::vector<uint32_t> mag;
     const int32_t *coef;
     int orient;
+    int style = 0;     // code-block style (VSC read here)
+    bool raw = false;  // the current pass is raw-coded (BYPASS)
     MQEnc mq;
+    RawEnc rw;
 
-    T1Enc(const int32_t *c, int w_, int h_, int o)
+    T1Enc(const int32_t *c, int w_, int h_, int o, int st)
         : w(w_), h(h_), W(w_ + 2), sig((w_ + 2) * (h_ + 2)), sgn(sig.size()), ref(sig.size()),
-          vis(sig.size()), mag((size_t)w_ * h_), coef(c), orient(o)
+          vis(sig.size()), mag((size_t)w_ * h_), coef(c), orient(o), style(st)
     {
         for (int i = 0; i < w * h; i++) mag[i] = (uint32_t)std::abs((int64_t)coef[i]);
     }
@@ -347,11 +417,20 @@ struct T1Enc {
     int bit(int x, int y, int p) const { return (mag[y * w + x] >> p) & 1; }
     int neg(int x, int y) const { return coef[y * w + x] < 0; }
 
+    // Vertically causal contexts (VSC): the row below a stripe counts as
+    // insignificant.
+    bool below_hidden(int y) const { return (style & TC_CBLK_STYLE_VSC) && (y & 3) == 3; }
     void counts(int x, int y, int &hh, int &vv, int &dd)
     {
+        const bool nb = !below_hidden(y);
         hh = S(sig, x - 1, y) + S(sig, x + 1, y);
-        vv = S(sig, x, y - 1) + S(sig, x, y + 1);
-        dd = S(sig, x - 1, y - 1) + S(sig, x + 1, y - 1) + S(sig, x - 1, y + 1) + S(sig, x + 1, y + 1);
+        vv = S(sig, x, y - 1) + (nb ? S(sig, x, y + 1) : 0);
+        dd = S(sig, x - 1, y - 1) + S(sig, x + 1, y - 1) + (nb ? S(sig, x - 1, y + 1) + S(sig, x + 1, y + 1) : 0);
+    }
+    void code(int d, int cx)
+    {
+        if (raw) rw.put((uint32_t)d);
+        else mq.encode(d, cx);
     }
     int zc(int hh, int vv, int dd) const
     {
@@ -373,7 +452,7 @@ struct T1Enc {
     {
         auto contrib = [&](int xx, int yy) { return S(sig, xx, yy) ? (S(sgn, xx, yy) ? -1 : 1) : 0; };
         int hc = contrib(x - 1, y) + contrib(x + 1, y);
-        int vc = contrib(x, y - 1) + contrib(x, y + 1);
+        int vc = contrib(x, y - 1) + (below_hidden(y) ? 0 : contrib(x, y + 1));
         hc = std::max(-1, std::min(1, hc));
         vc = std::max(-1, std::min(1, vc));
         int cx, xr;
@@ -385,7 +464,8 @@ struct T1Enc {
             xr = hc < 0;
         }
         const int s = neg(x, y);
-        mq.encode(s ^ xr, cx);
+        if (raw) rw.put((uint32_t)s);  // raw: the sign itself
+        else mq.encode(s ^ xr, cx);
         S(sgn, x, y) = (uint8_t)s;
         S(sig, x, y) = 1;
     }
@@ -400,7 +480,7 @@ struct T1Enc {
                     if (hh + vv + dd == 0) continue;
                     S(vis, x, y) = 1;
                     const int b = bit(x, y, p);
-                    mq.encode(b, zc(hh, vv, dd));
+                    code(b, zc(hh, vv, dd));
                     if (b) code_sign(x, y);
                 }
     }
@@ -412,7 +492,7 @@ struct T1Enc {
                     int hh, vv, dd;
                     if (!S(sig, x, y) || S(vis, x, y)) continue;
                     counts(x, y, hh, vv, dd);
-                    mq.encode(bit(x, y, p), S(ref, x, y) ? 16 : (hh + vv + dd ? 15 : 14));
+                    code(bit(x, y, p), S(ref, x, y) ? 16 : (hh + vv + dd ? 15 : 14));
                     S(ref, x, y) = 1;
                 }
     }
@@ -458,8 +538,10 @@ struct T1Enc {
 }  // namespace
 
 int t1_encode_block(const int32_t *coef, int w, int h, int orient, int mb, int passes,
-                    std::vector<uint8_t> &out, int *passes_out, int *zero_bitplanes)
+                    std::vector<uint8_t> &out, int *passes_out, int *zero_bitplanes, int style,
+                    std::vector<std::pair<uint32_t, int>> *segments)
 {
+    if (segments) segments->clear();
     if (w < 1 || h < 1 || w > 64 || h > 64 || orient < 0 || orient > 3 || mb < 1 || mb > 31)
         return TC_E_ARG;
     uint32_t mx = 0;
@@ -475,21 +557,49 @@ int t1_encode_block(const int32_t *coef, int w, int h, int orient, int mb, int p
     }
     const int total = 3 * numbps - 2;
     if (passes <= 0 || passes > total) passes = total;
-    T1Enc e(coef, w, h, orient);
-    int done = 0;
+    T1Enc e(coef, w, h, orient, style);
+    out.clear();
+    int done = 0, seg_passes = 0;
+    // ends the current codeword segment (MQ FLUSH or raw padding)
+    auto terminate = [&]() {
+        size_t len;
+        if (e.raw) {
+            len = e.rw.flush();
+            out.insert(out.end(), e.rw.buf.begin(), e.rw.buf.end());
+            e.rw.restart();
+        } else {
+            len = e.mq.flush();
+            out.insert(out.end(), e.mq.buf.begin() + 1, e.mq.buf.begin() + 1 + len);
+            e.mq.restart();
+        }
+        if (segments) segments->emplace_back((uint32_t)len, seg_passes);
+        seg_passes = 0;
+    };
+    // after pass t: context reset, termination
+    auto pass_done = [&](int t) {
+        if (style & TC_CBLK_STYLE_RESET) e.mq.reset_contexts();
+        ++seg_passes;
+        if (t + 1 == passes || pass_terminates(style, t)) terminate();
+    };
     for (int p = numbps - 1; p >= 0 && done < passes; p--) {
         if (p != numbps - 1) {
+            e.raw = pass_raw(style, done);
             e.spp(p);
+            pass_done(done);
             if (++done >= passes) break;
+            e.raw = pass_raw(style, done);
             e.mrp(p);
+            pass_done(done);
             if (++done >= passes) break;
         }
+        e.raw = false;
         e.cup(p);
+        if (style & TC_CBLK_STYLE_SEGSYM)  // segmentation symbol 1010 (ISO D.5)
+            for (int b : {1, 0, 1, 0}) e.mq.encode(b, 17);
+        pass_done(done);
         ++done;
         std::fill(e.vis.begin(), e.vis.end(), 0);
     }
-    const size_t len = e.mq.flush();
-    out.assign(e.mq.buf.begin() + 1, e.mq.buf.begin() + 1 + len);
     *passes_out = passes;
     return TC_OK;
 }
@@ -835,7 +945,7 @@ static int read_spcod(Reader &rd, bool precincts, Coding &c, std::string &err)
     c.reversible = (int)rd.u8();
     if (c.levels > 32 || c.xcb > 10 || c.ycb > 10 || c.xcb + c.ycb > 12) { err = "bad COD/COC"; return TC_E_CODESTREAM; }
     if (c.xcb > 6 || c.ycb > 6) { err = "code-blocks larger than 64x64"; return TC_E_UNSUPPORTED; }
-    if (c.cblk_style != 0) { err = "code-block style flags are not supported"; return TC_E_UNSUPPORTED; }
+    if (c.cblk_style & ~0x3F) { err = "unknown code-block style bits"; return TC_E_UNSUPPORTED; }
     if (c.reversible > 1) { err = "unknown wavelet"; return TC_E_CODESTREAM; }
     c.ppx.assign(c.levels + 1, 15);
     c.ppy.assign(c.levels + 1, 15);
@@ -1147,6 +1257,7 @@ struct CblkState {
     int passes = 0;
     int head = -1, tail = -1, nseg = 0;  // segment list in the tile's arena
     uint64_t bytes = 0;
+    std::vector<uint32_t> seglen;  // BYPASS / TERMALL: codeword segment lengths
 };
 
 // Descriptors of all tiles before their segments are placed: each entry's
@@ -1155,6 +1266,14 @@ struct Emit {
     std::vector<std::pair<size_t, uint32_t>> segs;
     std::vector<uint32_t> first;
     bool multi = false;  // some block has more than one segment
+    // Blocks whose codeword segments are terminated (BYPASS / TERMALL):
+    // descriptor index and its segment lengths at tab[at .. at + n).
+    struct Table {
+        size_t desc;
+        uint32_t at, n;
+    };
+    std::vector<Table> tables;
+    std::vector<uint32_t> tab;
 };
 }  // namespace
 
@@ -1197,6 +1316,8 @@ static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Para
     // where the tile is.
     std::vector<std::vector<Resolution>> geo(C);
     std::vector<std::vector<ResState>> st(C, std::vector<ResState>(R));
+    std::vector<int> style(C);  // code-block style per component (COD / COC)
+    for (int c = 0; c < C; c++) style[c] = coding_of(P, &ts, c).cblk_style;
     // the tile on each component's grid (ISO B.3: ceil of the reference-grid
     // box over the subsampling), its plane size and offset in the arena
     std::vector<Params::Tile> tc(C);
@@ -1316,12 +1437,38 @@ static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Para
                             if (br.overrun || ++inc_l > 32) { err = "bad Lblock increment"; return TC_E_CODESTREAM; }
                         }
                         cb.lblock += inc_l;
-                        const int nbits = cb.lblock + floorlog2(np);
-                        if (nbits > 31) { err = "code-block length field too wide"; return TC_E_CODESTREAM; }
-                        const uint32_t Lc = br.get_bits(nbits);
-                        if (br.overrun) { err = "packet header overrun"; return TC_E_CODESTREAM; }
-                        cb.passes += np;
-                        contrib.emplace_back(&cb, Lc);
+                        const int sty = style[c];
+                        if (cb.passes + np > 255) { err = "more than 255 coding passes"; return TC_E_CODESTREAM; }
+                        if (!(sty & (TC_CBLK_STYLE_BYPASS | TC_CBLK_STYLE_TERMALL))) {
+                            const int nbits = cb.lblock + floorlog2(np);
+                            if (nbits > 31) { err = "code-block length field too wide"; return TC_E_CODESTREAM; }
+                            const uint32_t Lc = br.get_bits(nbits);
+                            if (br.overrun) { err = "packet header overrun"; return TC_E_CODESTREAM; }
+                            cb.passes += np;
+                            contrib.emplace_back(&cb, Lc);
+                            continue;
+                        }
+                        // Terminated segments: one length per segment the new
+                        // passes reach, in Lblock + floorlog2(its new passes)
+                        // bits (ISO B.10.7.2); a segment left open continues
+                        // in the block's next contribution.
+                        uint64_t total = 0;
+                        for (int left = np; left > 0;) {
+                            const int t = cb.passes;
+                            int n = 1;
+                            while (n < left && !pass_terminates(sty, t + n - 1)) n++;
+                            const int nbits = cb.lblock + floorlog2(n);
+                            if (nbits > 31) { err = "code-block length field too wide"; return TC_E_CODESTREAM; }
+                            const uint32_t Lc = br.get_bits(nbits);
+                            if (br.overrun) { err = "packet header overrun"; return TC_E_CODESTREAM; }
+                            if (t == 0 || pass_terminates(sty, t - 1)) cb.seglen.push_back(Lc);
+                            else if ((cb.seglen.back() += Lc) < Lc) { err = "codeword segment too long"; return TC_E_CODESTREAM; }
+                            total += Lc;
+                            cb.passes += n;
+                            left -= n;
+                        }
+                        if (total > 0xFFFFFFFFull) { err = "code-block data too long"; return TC_E_CODESTREAM; }
+                        contrib.emplace_back(&cb, (uint32_t)total);
                     }
             }
         }
@@ -1474,6 +1621,7 @@ static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Para
                         d.out_off = coef_off + coff[c] + (uint64_t)(b.y0 + cy) * cw + (uint64_t)(b.x0 + cx);
                         d.step = reversible ? 1.0f : b.step;
                         d.flags = reversible ? 0 : TC_CBLK_IRREVERSIBLE;
+                        d.style = (uint8_t)style[c];
                         em.first.push_back((uint32_t)em.segs.size());
                         if (cb.included && cb.passes > 0) {
                             if (cb.zbp > b.mb) { err = "zero bit-planes exceed Mb"; return TC_E_CODESTREAM; }
@@ -1489,6 +1637,15 @@ static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Para
                             if (cb.nseg > 1) em.multi = true;
                             for (int k = cb.head; k >= 0; k = arena[k].next)
                                 em.segs.emplace_back(arena[k].off, arena[k].len);
+                            if (style[c] & (TC_CBLK_STYLE_BYPASS | TC_CBLK_STYLE_TERMALL)) {
+                                if ((int)cb.seglen.size() != pass_segments(style[c], cb.passes)) {
+                                    err = "codeword segments do not match the passes";
+                                    return TC_E_CODESTREAM;
+                                }
+                                em.multi = true;
+                                em.tables.push_back({out.desc.size(), (uint32_t)em.tab.size(), (uint32_t)cb.seglen.size()});
+                                em.tab.insert(em.tab.end(), cb.seglen.begin(), cb.seglen.end());
+                            }
                         } else {
                             d.zero_bitplanes = (uint8_t)b.mb;
                             d.passes = 0;
@@ -1583,10 +1740,24 @@ static int parse_raw_codestream(const uint8_t *cs, size_t len, Parsed &out, std:
         for (auto &s : em.segs) total += s.second;
         out.own_pool.reserve(total);
     }
+    size_t ti = 0;  // next entry of em.tables
     for (size_t k = 0; k < out.desc.size(); k++) {
         tc_cblk_desc &d = out.desc[k];
         const uint32_t a = em.first[k], b = em.first[k + 1];
-        if (em.multi) {
+        if (ti < em.tables.size() && em.tables[ti].desc == k) {
+            // 4-byte aligned table of the segment lengths (uint32 each,
+            // little-endian), then the codeword
+            const Emit::Table &tb = em.tables[ti++];
+            out.own_pool.resize((out.own_pool.size() + 3) & ~size_t(3), 0);
+            d.seg_off = out.own_pool.size();
+            for (uint32_t i = 0; i < tb.n; i++) {
+                const uint32_t v = em.tab[tb.at + i];
+                const uint8_t le[4] = {(uint8_t)v, (uint8_t)(v >> 8), (uint8_t)(v >> 16), (uint8_t)(v >> 24)};
+                out.own_pool.insert(out.own_pool.end(), le, le + 4);
+            }
+            for (uint32_t s = a; s < b; s++)
+                out.own_pool.insert(out.own_pool.end(), cs + em.segs[s].first, cs + em.segs[s].first + em.segs[s].second);
+        } else if (em.multi) {
             d.seg_off = a < b ? out.own_pool.size() : 0;
             for (uint32_t s = a; s < b; s++)
                 out.own_pool.insert(out.own_pool.end(), cs + em.segs[s].first, cs + em.segs[s].first + em.segs[s].second);
@@ -1609,6 +1780,7 @@ int encode_layout(const tc_encode_params &p, EncodeLayout &L, std::string &err)
         return TC_E_ARG;
     }
     if (!p.reversible && !(p.base_step > 0.0)) { err = "base_step must be positive"; return TC_E_ARG; }
+    if (p.cblk_style & ~0x3F) { err = "unknown code-block style bits"; return TC_E_ARG; }
     // Per component: code-block size (COC when it differs from COD), step
     // multiplier (QCC when it differs from QCD) and subsampling (SIZ).
     for (int c = 0; c < C; c++) {
@@ -1735,6 +1907,9 @@ int encode_codestream(const tc_encode_params &p, const void *planes, std::vector
     // depend on Mb, so the blocks are coded before the guard bits are known.
     std::vector<CodedBlock> coded(L.jobs.size());
     std::vector<std::vector<uint8_t>> words(L.jobs.size());
+    std::vector<std::vector<std::pair<uint32_t, int>>> segs(L.jobs.size());
+    const int style = p.cblk_style;
+    const bool segmented = style & (TC_CBLK_STYLE_BYPASS | TC_CBLK_STYLE_TERMALL);
     std::atomic<int> fail{0};
     parallel_for((int)L.jobs.size(), threads, [&](int k) {
         const EncodeLayout::Job &jb = L.jobs[k];
@@ -1746,10 +1921,14 @@ int encode_codestream(const tc_encode_params &p, const void *planes, std::vector
             for (int x = 0; x < bw; x++)
                 blk[y * bw + x] = q[L.coff[jb.c] + (size_t)(b.y0 + cy + y) * L.cw[jb.c] + b.x0 + cx + x];
         int zbp = 0;
-        if (t1_encode_block(blk, bw, bh, b.orient, 31, 0, words[k], &coded[k].passes, &zbp)) fail = 1;
+        if (t1_encode_block(blk, bw, bh, b.orient, 31, 0, words[k], &coded[k].passes, &zbp, style,
+                            segmented ? &segs[k] : nullptr))
+            fail = 1;
         coded[k].numbps = 31 - zbp;
         coded[k].data = words[k].data();
         coded[k].len = (uint32_t)words[k].size();
+        coded[k].seg = segs[k].data();
+        coded[k].nseg = (int)segs[k].size();
     });
     if (fail) { err = "Tier-1 encoding failed"; return TC_E_ARG; }
     return encode_assemble(p, L, coded, out, err);
@@ -1823,7 +2002,7 @@ int encode_assemble(const tc_encode_params &p, EncodeLayout &L, const std::vecto
     wr.u8(NL);
     wr.u8(p.cblk_log2 - 2);
     wr.u8(p.cblk_log2 - 2);
-    wr.u8(0);                              // code-block style
+    wr.u8(p.cblk_style);                   // code-block style
     wr.u8(p.reversible ? 1 : 0);
     // COC for components whose code-block size differs from COD's
     for (int c = 0; c < C; c++) {
@@ -1835,7 +2014,7 @@ int encode_assemble(const tc_encode_params &p, EncodeLayout &L, const std::vecto
         wr.u8(NL);
         wr.u8(cblk[c] - 2);
         wr.u8(cblk[c] - 2);
-        wr.u8(0);
+        wr.u8(p.cblk_style);
         wr.u8(p.reversible ? 1 : 0);
     }
     const int nbands = 3 * NL + 1;
@@ -1906,13 +2085,18 @@ int encode_assemble(const tc_encode_params &p, EncodeLayout &L, const std::vecto
                 if (cd.passes == 0) continue;
                 zt.encode(bw, i, zbps[k0 + i] + 1);
                 put_num_passes(bw, cd.passes);
-                const int len = (int)cd.len;
+                // One Lblock increment, then each codeword segment's length
+                // in Lblock + floorlog2(its passes) bits (ISO B.10.7).
+                const std::pair<uint32_t, int> whole((uint32_t)cd.len, cd.passes);
+                const std::pair<uint32_t, int> *sg = cd.nseg ? cd.seg : &whole;
+                const int ns = cd.nseg ? cd.nseg : 1;
                 int lblock = 3, incr = 0;
-                while (len >= (1 << (lblock + incr + floorlog2(cd.passes)))) incr++;
+                for (int s = 0; s < ns; s++)
+                    while (sg[s].first >= (1u << (lblock + incr + floorlog2(sg[s].second)))) incr++;
                 for (int t = 0; t < incr; t++) bw.put(1);
                 bw.put(0);
                 lblock += incr;
-                bw.put_bits((uint32_t)len, lblock + floorlog2(cd.passes));
+                for (int s = 0; s < ns; s++) bw.put_bits(sg[s].first, lblock + floorlog2(sg[s].second));
                 order.push_back(k0 + i);
             }
         }

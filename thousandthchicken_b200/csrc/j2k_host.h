@@ -48,8 +48,11 @@ inline int band_gain_log2(int orient) { return orient == 0 ? 0 : (orient == 3 ? 
 double subband_norm(bool wavelet97, int level, int orient);
 
 // ---- MQ encoder / Tier-1 encoder (harness) ---------------------------------
+// `style`: code-block style bits (TC_CBLK_STYLE_*); `segments`, when given,
+// receives each terminated codeword segment's length and pass count.
 int t1_encode_block(const int32_t *coef, int w, int h, int orient, int mb, int passes,
-                    std::vector<uint8_t> &out, int *passes_out, int *zero_bitplanes);
+                    std::vector<uint8_t> &out, int *passes_out, int *zero_bitplanes, int style = 0,
+                    std::vector<std::pair<uint32_t, int>> *segments = nullptr);
 
 // ---- parser -----------------------------------------------------------------
 struct Parsed {
@@ -86,6 +89,10 @@ struct CodedBlock {
     const uint8_t *data = nullptr;
     uint32_t len = 0;
     int passes = 0, numbps = 0;
+    // Codeword segments (length, passes) when the style terminates passes
+    // (BYPASS / TERMALL); none: one segment of len bytes.
+    const std::pair<uint32_t, int> *seg = nullptr;
+    int nseg = 0;
 };
 int encode_layout(const tc_encode_params &p, EncodeLayout &L, std::string &err);
 // Guard bits from the blocks' bit-planes (unless p.guard_bits is set), Mb

@@ -8,6 +8,8 @@
 
 #include <cstdint>
 
+#include "tc_j2k.h"
+
 namespace tc {
 namespace {
 
@@ -114,14 +116,17 @@ __device__ __forceinline__ uint32_t sign_index(const unsigned long long *sgn, ui
 
 // Record that row k of stripe s in column c became significant: the flag
 // words of the neighbouring columns and of the stripes above and below see
-// it through their neighbourhood bits.
+// it through their neighbourhood bits.  With vertically causal contexts
+// (vsc, ISO D.7) the stripe above does not: its last row's neighbourhood
+// then leaves out the row below for every context (zero coding, sign, run
+// mode, refinement).
 __device__ __forceinline__ void mark_significant(uint32_t *F, unsigned long long *sgn, int s, int k, int c, int w,
-                                                 int nstripes, uint32_t neg)
+                                                 int nstripes, uint32_t neg, bool vsc = false)
 {
     const int i = s * 64 + c;
     if (c > 0) F[i - 1] |= 1u << (3 * k + 5);
     if (c + 1 < w) F[i + 1] |= 1u << (3 * k + 3);
-    if (k == 0 && s > 0) {
+    if (k == 0 && s > 0 && !vsc) {
         const int u = i - 64;
         F[u] |= 1u << 16;
         if (c > 0) F[u - 1] |= 1u << 17;
@@ -136,6 +141,26 @@ __device__ __forceinline__ void mark_significant(uint32_t *F, unsigned long long
     if (neg) sgn[c + 1] |= 1ull << (4 * s + k);
 }
 
+// Code-block style (ISO Table A.19): whether coding pass t (0: the first
+// cleanup pass) ends a codeword segment (D.4.2, D.6), whether it is raw-coded
+// (bypass: SPP and MRP from the 11th pass on), and the segments that passes
+// [0, passes) span.
+__host__ __device__ __forceinline__ bool style_pass_terminates(int style, int t)
+{
+    if (style & TC_CBLK_STYLE_TERMALL) return true;
+    if (style & TC_CBLK_STYLE_BYPASS) return t == 9 || (t >= 10 && t % 3 != 1);
+    return false;
+}
+__host__ __device__ __forceinline__ bool style_pass_raw(int style, int t)
+{
+    return (style & TC_CBLK_STYLE_BYPASS) && t >= 10 && t % 3 != 0;
+}
+__host__ __device__ __forceinline__ int style_segments(int style, int passes)
+{
+    int n = passes > 0;
+    for (int t = 0; t + 1 < passes; t++) n += style_pass_terminates(style, t);
+    return n;
+}
 // Candidate mask of the group's columns: column gl + G*j for predicate any[j].
 template <int G>
 __device__ __forceinline__ unsigned long long group_ballot(const bool (&any)[64 / G], unsigned gmask, int gshift)

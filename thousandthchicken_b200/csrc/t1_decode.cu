@@ -24,7 +24,12 @@
 //     updates the state it reads (defects D1/D2 fixed); every codeword byte is
 //     consumed (defect D22 fixed) and one-column blocks stay in bounds (D23);
 //   * the epilogue writes the block out coalesced with the inverse quantiser
-//     fused in (ISO E.1, reconstruction point r).
+//     fused in (ISO E.1, reconstruction point r);
+//   * code-blocks with a coding style (bypass, context reset, termination on
+//     every pass, vertically causal contexts, segmentation symbols; ISO
+//     D.4-D.7) run in a launch of their own, an instantiation of the same
+//     decoder that switches codeword segments at pass boundaries; the
+//     reference decodes style 0 only.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -132,18 +137,59 @@ struct MQ {
     }
 };
 
+// Raw (bypass) bits of ISO D.6: MSB first; a byte after 0xFF holds 7 bits
+// (its MSB is a stuffed 0); after 0xFF a byte above 0x8F is a marker that is
+// not consumed, and from there on (as past the end) 1-bits are read.
+struct RawBits {
+    const uint8_t *p;
+    int len, bp, ct;
+    uint32_t b;
+
+    __device__ __forceinline__ void init(const uint8_t *d, int n)
+    {
+        p = d;
+        len = n;
+        bp = 0;
+        ct = 0;
+        b = 0;
+    }
+    __device__ __forceinline__ uint32_t bit()
+    {
+        if (ct == 0) {
+            const uint32_t nb = bp < len ? (uint32_t)__ldg(p + bp) : 0xFFu;
+            if (b == 0xFF && nb > 0x8F) {
+                ct = 8;
+            } else {
+                ct = b == 0xFF ? 7 : 8;
+                b = nb;
+                bp++;
+            }
+        }
+        --ct;
+        return (b >> ct) & 1u;
+    }
+};
+
 // Decode one code-block.  Every lane of the warp runs this function in
 // lock-step; lanes split the per-stripe candidate searches between them
 // (lane l owns columns l and l+32) and the serial loop visits only candidate
 // columns, in scan order.  Returns the last pass type (0 cleanup,
 // 1 significance propagation, 2 refinement) and its plane.
-template <typename MagT, int G>
+// Modes: the code-block style `style` applies; lens, when not null, holds
+// the lengths of the codeword's terminated segments (BYPASS / TERMALL),
+// which follow one another from seg.
+template <typename MagT, int G, bool Modes = false>
 __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *seg, int len, int w,
                             int h, int orient, int numbps, int passes, int *last_plane, int lane, unsigned gmask,
-                            int gshift)
+                            int gshift, int style = 0, const uint32_t *lens = nullptr)
 {
     MQ mq;
-    mq.init(seg, len);
+    RawBits rw;
+    bool raw = false;      // the current segment is raw-coded
+    int segi = 0;          // current segment
+    uint32_t segoff = 0;   // its first byte
+    const bool vsc = Modes && (style & TC_CBLK_STYLE_VSC);
+    if (!Modes || !lens) mq.init(seg, len);
     uint32_t *ctx = S.ctx;
     const uint32_t *tbl = T.mq;
     const uint8_t *zc = T.zc[orient];
@@ -153,10 +199,47 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
     int type = 0, pass = 0;
     *last_plane = numbps - 1;
 
+    // before coding pass t: the next codeword segment starts where the
+    // previous pass ended one
+    auto begin_pass = [&](int t) {
+        if constexpr (Modes) {
+            if (!lens || (t > 0 && !style_pass_terminates(style, t - 1))) return;
+            if (t > 0) segoff += lens[segi++];
+            raw = style_pass_raw(style, t);
+            if (raw) rw.init(seg + segoff, (int)lens[segi]);
+            else mq.init(seg + segoff, (int)lens[segi]);
+        }
+    };
+    // after a pass: the contexts start over (RESET)
+    auto end_pass = [&]() {
+        if constexpr (Modes) {
+            if (style & TC_CBLK_STYLE_RESET) {
+                __syncwarp(gmask);
+                for (int i = lane; i < 19; i += G)
+                    ctx[i] = tbl[i == 0 ? 4 : (i == 17 ? 46 : (i == 18 ? 3 : 0))];
+                __syncwarp(gmask);
+            }
+        }
+    };
+    // one decision of a significance or refinement pass, and a sign
+    auto decide = [&](int cx) -> uint32_t {
+        if constexpr (Modes) {
+            if (raw) return rw.bit();
+        }
+        return mq.decode(ctx, tbl, cx);
+    };
+    auto sign = [&](uint32_t si) -> uint32_t {
+        if constexpr (Modes) {
+            if (raw) return rw.bit();
+        }
+        return (uint32_t)mq.decode(ctx, tbl, si & 15) ^ (si >> 4);
+    };
+
     for (int p = numbps - 1; p >= 0; --p) {
         const MagT pbit = (MagT)(1u << p);
         if (p != numbps - 1) {
             // ---- significance propagation pass (ISO D.3.1; SigPropPassFunctor) ----
+            begin_pass(pass);
             for (int s = 0; s < nstripes; s++) {
                 const int rows = min(4, h - 4 * s);
                 __syncwarp(gmask);
@@ -183,12 +266,12 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
                         const uint32_t n9 = (f >> (3 * k)) & 0x1FFu;
                         if (!(n9 & 0x1EFu)) continue;
                         f |= pi_bit(k);
-                        if (mq.decode(ctx, tbl, zc[n9])) {
+                        if (decide(zc[n9])) {
                             const int y = 4 * s + k;
                             const uint32_t si = T.sc[sign_index(S.sgn, n9, c, y)];
-                            const uint32_t neg = (uint32_t)mq.decode(ctx, tbl, si & 15) ^ (si >> 4);
+                            const uint32_t neg = sign(si);
                             f |= self_bit(k);
-                            mark_significant(S.F, S.sgn, s, k, c, w, nstripes, neg);
+                            mark_significant(S.F, S.sgn, s, k, c, w, nstripes, neg, vsc);
                             S.mag[y * 64 + c] = pbit;
                             if (c + 1 < w) cand |= 1ull << (c + 1);  // the next column gained a neighbour
                         }
@@ -196,6 +279,7 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
                     if (f != f0) F[s * 64 + c] = f;
                 }
             }
+            end_pass();
             type = 1;
             *last_plane = p;
             if (++pass >= passes) break;
@@ -203,6 +287,7 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
             // ---- magnitude refinement pass (ISO D.3.3; MagRefPassFunctor) ----
             // Rows to refine and their contexts do not change during the pass:
             // the lanes precompute them for their columns.
+            begin_pass(pass);
             for (int s = 0; s < nstripes; s++) {
                 const int rows = min(4, h - 4 * s);
                 __syncwarp(gmask);
@@ -236,15 +321,17 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
                     while (rr) {
                         const int k = __ffs(rr) - 1;
                         rr &= rr - 1;
-                        if (mq.decode(ctx, tbl, 14 + ((codes >> (2 * k)) & 3u))) S.mag[(4 * s + k) * 64 + c] |= pbit;
+                        if (decide(14 + ((codes >> (2 * k)) & 3u))) S.mag[(4 * s + k) * 64 + c] |= pbit;
                     }
                 }
             }
+            end_pass();
             type = 2;
             if (++pass >= passes) break;
         }
 
         // ---- cleanup pass (ISO D.3.4; CleanUpPassFunctor) ----
+        begin_pass(pass);
         for (int s = 0; s < nstripes; s++) {
             const int rows = min(4, h - 4 * s);
             const uint32_t rmask = (1u << rows) - 1u;
@@ -279,7 +366,7 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
                     const uint32_t si = T.sc[sign_index(S.sgn, (f >> (3 * r)) & 0x1FFu, c, y)];
                     const uint32_t neg = (uint32_t)mq.decode(ctx, tbl, si & 15) ^ (si >> 4);
                     f |= self_bit(r);
-                    mark_significant(S.F, S.sgn, s, r, c, w, nstripes, neg);
+                    mark_significant(S.F, S.sgn, s, r, c, w, nstripes, neg, vsc);
                     S.mag[y * 64 + c] = pbit;
                     k = r + 1;
                 }
@@ -291,13 +378,18 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
                         const uint32_t si = T.sc[sign_index(S.sgn, n9, c, y)];
                         const uint32_t neg = (uint32_t)mq.decode(ctx, tbl, si & 15) ^ (si >> 4);
                         f |= self_bit(k);
-                        mark_significant(S.F, S.sgn, s, k, c, w, nstripes, neg);
+                        mark_significant(S.F, S.sgn, s, k, c, w, nstripes, neg, vsc);
                         S.mag[y * 64 + c] = pbit;
                     }
                 }
                 if (f != f0) F[s * 64 + c] = f;
             }
         }
+        if constexpr (Modes) {
+            if (style & TC_CBLK_STYLE_SEGSYM)  // segmentation symbol 1010 (ISO D.5)
+                for (int i = 0; i < 4; i++) mq.decode(ctx, tbl, 17);
+        }
+        end_pass();
         type = 0;
         *last_plane = p;
         if (++pass >= passes) break;
@@ -323,7 +415,7 @@ struct GroupCfg {
 
 // Decode code-block `bi` with the state S and write it out (the group's
 // lanes, in lock-step).  MagT bounds the coded bit-planes it accepts.
-template <typename MagT, int G>
+template <typename MagT, int G, bool Modes = false>
 __device__ __forceinline__ void process_block(WarpState<MagT> &S, const Tables &T, const tc_cblk_desc *__restrict__ desc,
                                               uint32_t bi, int ndesc, const uint8_t *__restrict__ pool,
                                               uint64_t pool_len, char *__restrict__ out, int out_mode, float recon_r,
@@ -348,6 +440,33 @@ __device__ __forceinline__ void process_block(WarpState<MagT> &S, const Tables &
         if (gl == 0) atomicOr(err, ok ? TC_DERR_POOL : TC_DERR_DESC);
         ok = false;
     }
+    // Styled blocks: only the Modes launch decodes them.  A segment table
+    // (BYPASS / TERMALL) sits 4-byte aligned at seg_off, the codeword after
+    // it, and its lengths add up to seg_len.
+    const int style = d.style & kStyleDecodeBits;
+    const uint32_t *lens = nullptr;
+    uint64_t cw_off = d.seg_off;
+    if (!Modes && style) {
+        if (gl == 0) atomicOr(err, TC_DERR_STYLE);
+        ok = false;
+    }
+    if (Modes && ok && (style & (TC_CBLK_STYLE_BYPASS | TC_CBLK_STYLE_TERMALL)) && numbps > 0 && d.passes > 0) {
+        const int nseg = style_segments(style, d.passes);
+        const uint64_t tab = 4ull * (uint64_t)nseg;
+        bool tab_ok = (d.seg_off & 3u) == 0 && d.seg_off + tab <= pool_len &&
+                      (uint64_t)d.seg_len <= pool_len - d.seg_off - tab;
+        if (tab_ok) {
+            lens = reinterpret_cast<const uint32_t *>(pool + d.seg_off);
+            uint64_t sum = 0;
+            for (int i = 0; i < nseg; i++) sum += __ldg(lens + i);
+            tab_ok = sum == d.seg_len;
+            cw_off += tab;
+        }
+        if (!tab_ok) {
+            if (gl == 0) atomicOr(err, TC_DERR_STYLE);
+            ok = false;
+        }
+    }
     const bool coded = ok && numbps > 0 && d.passes > 0;
     const int nstripes = (h + 3) >> 2;
 
@@ -362,8 +481,8 @@ __device__ __forceinline__ void process_block(WarpState<MagT> &S, const Tables &
 
     int type = 0, last_plane = 0;
     if (coded)
-        type = decode_block<MagT, G>(S, T, pool + d.seg_off, (int)d.seg_len, w, h, d.orient, numbps, d.passes,
-                                     &last_plane, gl, gmask, gshift);
+        type = decode_block<MagT, G, Modes>(S, T, pool + cw_off, (int)d.seg_len, w, h, d.orient, numbps, d.passes,
+                                            &last_plane, gl, gmask, gshift, style, lens);
     __syncwarp(gmask);
 
     // epilogue: reconstruction + inverse quantisation, coalesced rows
@@ -412,7 +531,7 @@ struct HeavyQueue {
     uint32_t *counter = nullptr;
 };
 
-template <typename MagT, int G>
+template <typename MagT, int G, bool Modes = false>
 __global__ void __launch_bounds__(32 * GroupCfg<MagT, G>::warps)
 t1_decode_kernel(const tc_cblk_desc *__restrict__ desc, const uint32_t *__restrict__ order, int n, int ndesc,
                  const uint8_t *__restrict__ pool, uint64_t pool_len, char *__restrict__ out, int out_mode,
@@ -432,7 +551,7 @@ t1_decode_kernel(const tc_cblk_desc *__restrict__ desc, const uint32_t *__restri
     const int slot = (threadIdx.x >> 5) * (32 / G) + gidx;
     WarpState<MagT> &S = states[slot];
 
-    if constexpr (std::is_same<MagT, uint8_t>::value && G == 32) {
+    if constexpr (std::is_same<MagT, uint8_t>::value && G == 32 && !Modes) {
         static_assert(sizeof(WarpState<uint16_t>) <= 2 * sizeof(WarpState<uint8_t>), "heavy state spans two slots");
         if ((int)blockIdx.x < heavy.ctas && slot < 2) {
             if (slot == 1) return;  // lends its state to warp 0
@@ -454,8 +573,8 @@ t1_decode_kernel(const tc_cblk_desc *__restrict__ desc, const uint32_t *__restri
         idx = __shfl_sync(gmask, idx, gshift);
         if (idx >= n) break;
         const uint32_t bi = order ? order[idx] : (uint32_t)idx;
-        process_block<MagT, G>(S, T, desc, bi, ndesc, pool, pool_len, out, out_mode, recon_r, err, gl, gmask,
-                               gshift);
+        process_block<MagT, G, Modes>(S, T, desc, bi, ndesc, pool, pool_len, out, out_mode, recon_r, err, gl,
+                                      gmask, gshift);
     }
 }
 
@@ -517,7 +636,7 @@ struct LaunchCfg {
 };
 
 // Kernel attributes and occupancy of one class variant, set up once per device.
-template <typename MagT, int G>
+template <typename MagT, int G, bool Modes = false>
 cudaError_t class_cfg(tc_ctx *ctx, LaunchCfg **out)
 {
     constexpr int kWarps = GroupCfg<MagT, G>::warps;
@@ -526,10 +645,11 @@ cudaError_t class_cfg(tc_ctx *ctx, LaunchCfg **out)
     if (!C.ready) {
         C.smem = ((sizeof(Tables) + 15) & ~size_t(15)) + kWarps * (32 / G) * sizeof(WarpState<MagT>);
         C.per_cta = kWarps * (32 / G);
-        cudaError_t e = cudaFuncSetAttribute(t1_decode_kernel<MagT, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)C.smem);
+        cudaError_t e = cudaFuncSetAttribute(t1_decode_kernel<MagT, G, Modes>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C.smem);
         if (e != cudaSuccess) return e;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&C.per_sm, t1_decode_kernel<MagT, G>, 32 * kWarps, C.smem);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&C.per_sm, t1_decode_kernel<MagT, G, Modes>, 32 * kWarps,
+                                                          C.smem);
         if (e != cudaSuccess) return e;
         if (C.per_sm < 1) C.per_sm = 1;
         C.ready = true;
@@ -540,17 +660,17 @@ cudaError_t class_cfg(tc_ctx *ctx, LaunchCfg **out)
 
 // One class launch: a persistent grid pulling the class's blocks from its
 // work counter d_words[slot] (zeroed beforehand).
-template <typename MagT, int G>
+template <typename MagT, int G, bool Modes = false>
 cudaError_t launch_class(tc_ctx *ctx, cudaStream_t stream, const tc_cblk_desc *d_desc, const uint32_t *d_order,
                          int n, int ndesc, const uint8_t *d_pool, uint64_t pool_len, void *d_out, int out_mode,
                          float recon_r, int slot, const HeavyQueue &heavy = HeavyQueue())
 {
     LaunchCfg *C = nullptr;
-    cudaError_t e = class_cfg<MagT, G>(ctx, &C);
+    cudaError_t e = class_cfg<MagT, G, Modes>(ctx, &C);
     if (e != cudaSuccess) return e;
     const int want = std::max((n + C->per_cta - 1) / C->per_cta, heavy.ctas);
     const int grid = std::max(1, std::min(want, C->per_sm * num_sms(ctx->device)));
-    t1_decode_kernel<MagT, G><<<grid, 32 * GroupCfg<MagT, G>::warps, C->smem, stream>>>(
+    t1_decode_kernel<MagT, G, Modes><<<grid, 32 * GroupCfg<MagT, G>::warps, C->smem, stream>>>(
         d_desc, d_order, n, ndesc, d_pool, pool_len, static_cast<char *>(d_out), out_mode, recon_r,
         ctx->d_words + slot, ctx->d_words, heavy);
     ctx->launches++;
@@ -586,6 +706,9 @@ cudaError_t launch_t1_decode(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint
                              const uint8_t *d_pool, uint64_t pool_len, void *d_out, int out_mode, float recon_r,
                              int max_bitplanes)
 {
+    if (out_mode & TC_T1_STYLED)
+        return launch_t1_classes(ctx, d_desc, d_order, n, 0, 0, 0, d_pool, pool_len, d_out, out_mode & ~TC_T1_STYLED,
+                                 recon_r, n);
     return launch_t1_classes(ctx, d_desc, d_order, n, max_bitplanes <= 8 ? n : 0,
                              max_bitplanes > 8 && max_bitplanes <= 16 ? n : 0, max_bitplanes > 16 ? n : 0, d_pool,
                              pool_len, d_out, out_mode, recon_r);
@@ -597,14 +720,21 @@ cudaError_t launch_t1_decode(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint
 // class rides in the 8-bit launch (see HeavyQueue), and an 8-bit class at
 // most half the size of the 16-bit class is decoded by the 16-bit launch.
 // Otherwise the classes run as concurrent launches, the 32- and 16-bit ones
-// on side streams.
+// on side streams.  Styled blocks (nstyled, after the three classes) run in
+// a 32-bit Modes launch on the context's stream.
 cudaError_t launch_t1_classes(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint32_t *d_order, int ndesc,
                               int n8, int n16, int n32, const uint8_t *d_pool, uint64_t pool_len, void *d_out,
-                              int out_mode, float recon_r)
+                              int out_mode, float recon_r, int nstyled)
 {
-    if (n8 + n16 + n32 == 0) return cudaSuccess;
-    cudaError_t e = cudaMemsetAsync(ctx->d_words + 1, 0, 3 * sizeof(uint32_t), ctx->stream);
+    if (n8 + n16 + n32 + nstyled == 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(ctx->d_words + 1, 0, 4 * sizeof(uint32_t), ctx->stream);
     if (e != cudaSuccess) return e;
+    if (nstyled > 0) {
+        const uint32_t *os = d_order ? d_order + n8 + n16 + n32 : nullptr;
+        e = launch_class<uint32_t, 32, true>(ctx, ctx->stream, d_desc, os, nstyled, ndesc, d_pool, pool_len, d_out,
+                                             out_mode, recon_r, 4);
+        if (e != cudaSuccess || n8 + n16 + n32 == 0) return e;
+    }
     const uint32_t *o16 = d_order ? d_order + n8 : nullptr;
     const uint32_t *o32 = d_order ? d_order + n8 + n16 : nullptr;
     HeavyQueue heavy;

@@ -12,8 +12,14 @@
 // Device error word bits (set by kernels, read by tc_ctx_synchronize).
 #define TC_DERR_DESC 0x1u     // a code-block descriptor was out of range
 #define TC_DERR_POOL 0x2u     // a codeword ran past the segment pool
+#define TC_DERR_STYLE 0x4u    // a styled code-block reached a style-0 launch, or its segment table is bad
 
 namespace tc {
+
+// Code-block style bits that change decoding (PTERM only constrains the
+// encoder's terminations).
+constexpr int kStyleDecodeBits = TC_CBLK_STYLE_BYPASS | TC_CBLK_STYLE_RESET | TC_CBLK_STYLE_TERMALL |
+                                 TC_CBLK_STYLE_VSC | TC_CBLK_STYLE_SEGSYM;
 
 // Sample range of an output of `bits` bits (TC_SIGNED set: signed samples,
 // two's complement, no DC level shift; ISO G.1.2 shifts unsigned ones only).
@@ -78,7 +84,7 @@ struct tc_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     std::string err;
-    uint32_t *d_words = nullptr;  // [0] error word, [1..3] Tier-1 work counters
+    uint32_t *d_words = nullptr;  // [0] error word, [1..4] Tier-1 work counters
     tc::DevBuf scratch;           // DWT intermediate levels
     tc::DevBuf tmp_pool, tmp_desc, tmp_order, tmp_coef, tmp_out;
     tc::PinBuf stage_pool, stage_desc, stage_order;  // pinned staging of tc_decode_j2k
@@ -124,12 +130,14 @@ cudaError_t launch_t1_decode(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint
                              int n, const uint8_t *d_pool, uint64_t pool_len, void *d_out,
                              int out_mode, float recon_r, int max_bitplanes);
 // Up to three persistent launches over an order array partitioned into
-// blocks of at most 8, 16 and 31 coded bit-planes (n8 + n16 + n32 entries).
+// blocks of at most 8, 16 and 31 coded bit-planes (n8 + n16 + n32 entries),
+// then nstyled blocks with a code-block style.
 cudaError_t launch_t1_classes(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint32_t *d_order,
                               int ndesc, int n8, int n16, int n32, const uint8_t *d_pool,
-                              uint64_t pool_len, void *d_out, int out_mode, float recon_r);
-// Host: order longest-first within each bit-plane class; class sizes out.
-void t1_class_order(const tc_cblk_desc *h_desc, int n, uint32_t *h_order, int counts[3]);
+                              uint64_t pool_len, void *d_out, int out_mode, float recon_r, int nstyled = 0);
+// Host: order longest-first within each class (<= 8, <= 16, <= 31 coded
+// bit-planes, then styled blocks); class sizes out.
+void t1_class_order(const tc_cblk_desc *h_desc, int n, uint32_t *h_order, int counts[4]);
 cudaError_t launch_dequant_raw(tc_ctx *ctx, const tc_cblk_desc *d_desc, int n,
                                const uint32_t *d_raw, void *d_out, float recon_r);
 cudaError_t launch_t1_encode(tc_ctx *ctx, const tc_t1_enc_desc *d_desc, int n, const void *d_in, uint8_t *d_out,

@@ -72,6 +72,10 @@ class Context:
         L.check(status, self.handle, what)
 
 
+# code-block style bits that change decoding (all but PTERM)
+STYLE_DECODE_BITS = 0x2F
+
+
 def _dev_bytes(arr: np.ndarray, device) -> "torch.Tensor":
     return torch.from_numpy(np.ascontiguousarray(arr).view(np.uint8).reshape(-1)).to(device, non_blocking=False)
 
@@ -85,12 +89,14 @@ class CoefficientCoder:
         self.ctx = ctx
 
     def decode(self, desc_dev, pool_dev, out, n: int, order_dev=None, raw: bool = False,
-               recon_r: float = 0.5, max_bitplanes: int = 0):
-        """Low-level: descriptors, pool, order and out are device tensors."""
+               recon_r: float = 0.5, max_bitplanes: int = 0, styled: bool = False):
+        """Low-level: descriptors, pool, order and out are device tensors.
+        styled: the descriptors may carry code-block styles (decoded by the
+        style-capable kernel; without it such blocks are reported as errors)."""
+        mode = (L.TC_T1_OUT_RAW if raw else L.TC_T1_OUT_DEQUANT) | (L.TC_T1_STYLED if styled else 0)
         self.ctx.check(L.lib().tc_t1_decode(self.ctx.handle, _ptr(desc_dev),
                                             _ptr(order_dev) if order_dev is not None else None, n,
-                                            _ptr(pool_dev), pool_dev.numel(), _ptr(out),
-                                            L.TC_T1_OUT_RAW if raw else L.TC_T1_OUT_DEQUANT, recon_r,
+                                            _ptr(pool_dev), pool_dev.numel(), _ptr(out), mode, recon_r,
                                             max_bitplanes),
                        "tc_t1_decode")
 
@@ -112,7 +118,8 @@ class CoefficientCoder:
         out = torch.zeros(max(out_elems, 1), dtype=dtype, device=dev)
         nb = desc["mb"].astype(np.int32) - desc["zero_bitplanes"].astype(np.int32)
         maxb = int(np.clip(nb[desc["passes"] > 0], 0, 31).max()) if (desc["passes"] > 0).any() else 1
-        self.decode(d_desc, d_pool, out, len(desc), d_order, raw, recon_r, max(maxb, 1))
+        styled = bool(len(desc) and (desc["style"] & STYLE_DECODE_BITS).any())
+        self.decode(d_desc, d_pool, out, len(desc), d_order, raw, recon_r, max(maxb, 1), styled)
         self.ctx.synchronize()
         return out
 
