@@ -380,12 +380,17 @@ typedef struct tc_encode_params {
      * accepted and written, the terminations are the plain ones (ISO D.4.2
      * allows either encoder). The GPU encoder takes 0 only. */
     int32_t cblk_style;
+    /* Quality layers (0 or 1: one).  Each block's passes are split evenly
+     * over the layers; a codeword segment that a layer boundary cuts is
+     * split by bytes in proportion, so every layer together gives the whole
+     * codeword (no rate-distortion truncation points). */
+    int32_t layers;
 } tc_encode_params;
 
 /* Encode planar samples (8-bit when bits <= 8, else 16-bit; unsigned, or
- * two's complement when is_signed) into a
- * single-tile, single-layer codestream with all coding passes (a harness
- * encoder: the reference has none). */
+ * two's complement when is_signed) into a single-tile codestream with all
+ * coding passes in p.layers quality layers (a harness encoder: the
+ * reference has none). */
 int tc_encode_j2k(const tc_encode_params *p, const void *h_planes,
                   uint8_t *h_out, size_t cap, size_t *out_len);
 

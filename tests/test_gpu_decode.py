@@ -6,7 +6,7 @@ import pytest
 
 import oracle as O
 from conftest import golden_cases, load_golden, synth_image
-from test_host_codec import COC_QCC, PRECINCTS, SIGNED, STYLE_IDS, STYLES, SUBSAMPLED, TILED
+from test_host_codec import COC_QCC, LAYERED, LAYERED_IDS, PRECINCTS, SIGNED, STYLE_IDS, STYLES, SUBSAMPLED, TILED
 from thousandthchicken_b200 import codec
 
 pytestmark = pytest.mark.gpu
@@ -466,3 +466,15 @@ def test_styled_blocks_in_a_style0_launch_are_errors(gpu_ctx):
     plain_cs = codec.encode(img, 8, levels=3, cblk_log2=5, reversible=True)
     want, _ = coder.decode_tile(plain_cs)
     np.testing.assert_array_equal(got.cpu().numpy(), want.cpu().numpy())
+
+
+@pytest.mark.parametrize("style,prog,layers", LAYERED, ids=LAYERED_IDS)
+def test_layered_streams_decode(gpu_ctx, style, prog, layers):
+    """Harness-encoded quality layers in every progression order, with and
+    without code-block styles: the blocks' contributions gathered across
+    layers (a bypass segment cut by a layer boundary included) decode on the
+    GPU to the original."""
+    img = synth_image(133, 91, 3, 8, seed=style + prog + layers)
+    cs = codec.encode(img, 8, levels=3, cblk_log2=5, reversible=True, cblk_style=style, progression=prog,
+                      layers=layers)
+    np.testing.assert_array_equal(_decoder(gpu_ctx).decode(cs), img)

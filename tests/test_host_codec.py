@@ -620,3 +620,30 @@ def test_unknown_style_bits_are_rejected():
     assert e.value.status == TC_E_UNSUPPORTED
     with pytest.raises(TCError):
         codec.encode(img, 8, cblk_style=0x40)
+
+
+LAYERED = [  # (code-block style, progression, layers)
+    (0, 0, 3), (0, 2, 5), (codec.CBLK_STYLE_BYPASS, 0, 7), (codec.CBLK_STYLE_BYPASS, 1, 3),
+    (codec.CBLK_STYLE_BYPASS, 3, 4), (codec.CBLK_STYLE_BYPASS | codec.CBLK_STYLE_TERMALL, 2, 3),
+    (codec.CBLK_STYLE_TERMALL, 4, 6), (0x3F, 1, 5), (codec.CBLK_STYLE_RESET, 3, 2),
+]
+LAYERED_IDS = [f"style{s:#x}-prog{p}-{n}layers" for s, p, n in LAYERED]
+
+
+@pytest.mark.parametrize("style,prog,layers", LAYERED, ids=LAYERED_IDS)
+def test_layered_streams_through_oracle(style, prog, layers):
+    """Quality layers from the harness encoder, every progression order:
+    each block's passes are spread over the layers, so blocks join in later
+    layers (inclusion tag trees across layers), Lblock grows across
+    contributions, and a bypass block's first ten-pass segment, cut by layer
+    boundaries, continues in the next layer's packet. OpenJPEG and the
+    parser + oracle both give back the original."""
+    from gpu_helpers import oracle_decode_tiled, openjpeg_decode
+    img = synth_image(133, 91, 3, 8, seed=style + prog + layers)
+    cs = codec.encode(img, 8, levels=3, cblk_log2=5, reversible=True, cblk_style=style, progression=prog,
+                      layers=layers)
+    info, _, _ = codec.parse(cs)
+    assert info["layers"] == layers
+    np.testing.assert_array_equal(openjpeg_decode(cs), img)
+    _, out = oracle_decode_tiled(cs)
+    np.testing.assert_array_equal(out, img)

@@ -1781,6 +1781,7 @@ int encode_layout(const tc_encode_params &p, EncodeLayout &L, std::string &err)
     }
     if (!p.reversible && !(p.base_step > 0.0)) { err = "base_step must be positive"; return TC_E_ARG; }
     if (p.cblk_style & ~0x3F) { err = "unknown code-block style bits"; return TC_E_ARG; }
+    if (p.layers < 0 || p.layers > 64) { err = "layers out of range"; return TC_E_ARG; }
     // Per component: code-block size (COC when it differs from COD), step
     // multiplier (QCC when it differs from QCD) and subsampling (SIZ).
     for (int c = 0; c < C; c++) {
@@ -1997,7 +1998,7 @@ int encode_assemble(const tc_encode_params &p, EncodeLayout &L, const std::vecto
     wr.u16(12);
     wr.u8(0);                              // Scod: default precincts, no SOP/EPH
     wr.u8(p.progression);                  // progression order
-    wr.u16(1);                             // layers
+    wr.u16(std::max(1, p.layers));         // layers
     wr.u8(mct ? 1 : 0);
     wr.u8(NL);
     wr.u8(p.cblk_log2 - 2);
@@ -2047,8 +2048,60 @@ int encode_assemble(const tc_encode_params &p, EncodeLayout &L, const std::vecto
     wr.u8(0);
     wr.u8(1);
     wr.u16(M_SOD);
+    // Quality layers: block k's passes [lp(k, l), lp(k, l + 1)) go into
+    // layer l.  A codeword segment that a layer boundary cuts is split by
+    // bytes in proportion to its passes, so a decoder given every layer
+    // reads the whole codeword (the harness computes no rate-distortion
+    // truncation points).
+    const int NLY = std::max(1, p.layers);
+    auto lp = [&](size_t k, int l) { return (int)((int64_t)coded[k].passes * l / NLY); };
+    // bytes of block k's codeword that its first t passes span
+    auto bytes_at = [&](size_t k, int t) -> uint32_t {
+        const CodedBlock &cd = coded[k];
+        if (t >= cd.passes) return cd.len;
+        const std::pair<uint32_t, int> whole(cd.len, cd.passes);
+        const std::pair<uint32_t, int> *sg = cd.nseg ? cd.seg : &whole;
+        const int ns = cd.nseg ? cd.nseg : 1;
+        uint32_t b = 0;
+        int a = 0;  // first pass of segment s
+        for (int s = 0; s < ns; s++) {
+            if (t < a + sg[s].second)
+                return b + (uint32_t)((uint64_t)sg[s].first * (uint64_t)(t - a) / (uint64_t)sg[s].second);
+            b += sg[s].first;
+            a += sg[s].second;
+        }
+        return b;
+    };
+    // Per band: inclusion (first layer with passes) and zero bit-plane tag
+    // trees; per block: Lblock and whether it was included.
+    std::vector<std::vector<std::vector<TagTree>>> incl(C), ztree(C);
+    std::vector<int> lblock(jobs.size(), 3);
+    std::vector<uint8_t> included(jobs.size(), 0);
+    for (int c = 0; c < C; c++) {
+        incl[c].resize(NL + 1);
+        ztree[c].resize(NL + 1);
+        for (int r = 0; r <= NL; r++)
+            for (int bi = 0; bi < (int)geo[c][r].bands.size(); bi++) {
+                const Band &b = geo[c][r].bands[bi];
+                const int n = b.ncbx * b.ncby;
+                incl[c][r].emplace_back(std::max(b.ncbx, 1), std::max(b.ncby, 1));
+                ztree[c][r].emplace_back(std::max(b.ncbx, 1), std::max(b.ncby, 1));
+                if (n == 0) continue;
+                const int k0 = first[c][r][bi];
+                std::vector<int> iv(n), zv(n);
+                for (int i = 0; i < n; i++) {
+                    int fl = NLY;  // never included
+                    for (int l = 0; l < NLY; l++)
+                        if (lp(k0 + i, l + 1) > lp(k0 + i, l)) { fl = l; break; }
+                    iv[i] = fl;
+                    zv[i] = zbps[k0 + i];
+                }
+                incl[c][r][bi].set_leaves(iv);
+                ztree[c][r][bi].set_leaves(zv);
+            }
+    }
     std::vector<uint8_t> hdr;
-    auto write_packet = [&](int r, int c) {
+    auto write_packet = [&](int l, int r, int c) {
         hdr.clear();
         BitWriter bw(hdr);
         bool any = false;
@@ -2056,7 +2109,7 @@ int encode_assemble(const tc_encode_params &p, EncodeLayout &L, const std::vecto
             const Band &b = geo[c][r].bands[bi];
             if (b.ncbx * b.ncby == 0) continue;
             const int k0 = first[c][r][bi];
-            for (int i = 0; i < b.ncbx * b.ncby; i++) any |= coded[k0 + i].passes > 0;
+            for (int i = 0; i < b.ncbx * b.ncby; i++) any |= lp(k0 + i, l + 1) > lp(k0 + i, l);
         }
         if (!any) {
             bw.put(0);
@@ -2065,54 +2118,91 @@ int encode_assemble(const tc_encode_params &p, EncodeLayout &L, const std::vecto
             return;
         }
         bw.put(1);
-        std::vector<int> order;
+        std::vector<std::pair<uint32_t, uint32_t>> body;  // byte ranges of the blocks' codewords
+        std::vector<std::pair<uint32_t, int>> chunks;
         for (int bi = 0; bi < (int)geo[c][r].bands.size(); bi++) {
             const Band &b = geo[c][r].bands[bi];
             const int n = b.ncbx * b.ncby;
             if (n == 0) continue;
             const int k0 = first[c][r][bi];
-            TagTree incl(b.ncbx, b.ncby), zt(b.ncbx, b.ncby);
-            std::vector<int> iv(n), zv(n);
             for (int i = 0; i < n; i++) {
-                iv[i] = coded[k0 + i].passes > 0 ? 0 : 1;
-                zv[i] = zbps[k0 + i];
-            }
-            incl.set_leaves(iv);
-            zt.set_leaves(zv);
-            for (int i = 0; i < n; i++) {
-                const CodedBlock &cd = coded[k0 + i];
-                incl.encode(bw, i, 1);
-                if (cd.passes == 0) continue;
-                zt.encode(bw, i, zbps[k0 + i] + 1);
-                put_num_passes(bw, cd.passes);
-                // One Lblock increment, then each codeword segment's length
-                // in Lblock + floorlog2(its passes) bits (ISO B.10.7).
-                const std::pair<uint32_t, int> whole((uint32_t)cd.len, cd.passes);
-                const std::pair<uint32_t, int> *sg = cd.nseg ? cd.seg : &whole;
-                const int ns = cd.nseg ? cd.nseg : 1;
-                int lblock = 3, incr = 0;
-                for (int s = 0; s < ns; s++)
-                    while (sg[s].first >= (1u << (lblock + incr + floorlog2(sg[s].second)))) incr++;
+                const size_t k = (size_t)k0 + i;
+                const CodedBlock &cd = coded[k];
+                const int t0 = lp(k, l), t1 = lp(k, l + 1);
+                if (!included[k]) incl[c][r][bi].encode(bw, i, l + 1);
+                else bw.put(t1 > t0);
+                if (t1 == t0) continue;
+                if (!included[k]) {
+                    ztree[c][r][bi].encode(bw, i, zbps[k] + 1);
+                    included[k] = 1;
+                }
+                put_num_passes(bw, t1 - t0);
+                // The new passes in codeword-segment chunks (cut at the
+                // segments' last passes), one Lblock increment, then each
+                // chunk's length in Lblock + floorlog2(its passes) bits
+                // (ISO B.10.7).
+                chunks.clear();
+                if (!cd.nseg) {
+                    chunks.emplace_back(bytes_at(k, t1) - bytes_at(k, t0), t1 - t0);
+                } else {
+                    int a = 0;
+                    for (int s = 0; s < cd.nseg; s++) {
+                        const int e = a + cd.seg[s].second;
+                        const int u0 = std::max(a, t0), u1 = std::min(e, t1);
+                        if (u0 < u1) chunks.emplace_back(bytes_at(k, u1) - bytes_at(k, u0), u1 - u0);
+                        a = e;
+                    }
+                }
+                int incr = 0;
+                for (auto &ch : chunks)
+                    while (ch.first >= (1u << (lblock[k] + incr + floorlog2(ch.second)))) incr++;
                 for (int t = 0; t < incr; t++) bw.put(1);
                 bw.put(0);
-                lblock += incr;
-                for (int s = 0; s < ns; s++) bw.put_bits(sg[s].first, lblock + floorlog2(sg[s].second));
-                order.push_back(k0 + i);
+                lblock[k] += incr;
+                for (auto &ch : chunks) bw.put_bits(ch.first, lblock[k] + floorlog2(ch.second));
+                body.emplace_back(bytes_at(k, t0), bytes_at(k, t1));
+                (void)cd;
             }
         }
         bw.flush();
         out.insert(out.end(), hdr.begin(), hdr.end());
-        for (int k : order) out.insert(out.end(), coded[k].data, coded[k].data + coded[k].len);
+        size_t bi = 0;
+        for (int bb = 0; bb < (int)geo[c][r].bands.size(); bb++) {
+            const Band &b = geo[c][r].bands[bb];
+            const int n = b.ncbx * b.ncby;
+            if (n == 0) continue;
+            const int k0 = first[c][r][bb];
+            for (int i = 0; i < n; i++) {
+                const size_t k = (size_t)k0 + i;
+                if (lp(k, l + 1) == lp(k, l)) continue;
+                const auto &rg = body[bi++];
+                out.insert(out.end(), coded[k].data + rg.first, coded[k].data + rg.second);
+            }
+        }
     };
-    // One layer and one precinct per resolution: LRCP, RLCP and RPCL visit
-    // resolution-major, PCRL and CPRL (every precinct starts at the origin)
-    // component-major.
-    if (p.progression >= 3) {
-        for (int c = 0; c < C; c++)
-            for (int r = 0; r <= NL; r++) write_packet(r, c);
-    } else {
+    // One precinct per resolution, all at the origin: LRCP visits (l, r, c),
+    // RLCP (r, l, c), RPCL (r, c, l), PCRL and CPRL (c, r, l).
+    switch (p.progression) {
+    case 0:
+        for (int l = 0; l < NLY; l++)
+            for (int r = 0; r <= NL; r++)
+                for (int c = 0; c < C; c++) write_packet(l, r, c);
+        break;
+    case 1:
         for (int r = 0; r <= NL; r++)
-            for (int c = 0; c < C; c++) write_packet(r, c);
+            for (int l = 0; l < NLY; l++)
+                for (int c = 0; c < C; c++) write_packet(l, r, c);
+        break;
+    case 2:
+        for (int r = 0; r <= NL; r++)
+            for (int c = 0; c < C; c++)
+                for (int l = 0; l < NLY; l++) write_packet(l, r, c);
+        break;
+    default:
+        for (int c = 0; c < C; c++)
+            for (int r = 0; r <= NL; r++)
+                for (int l = 0; l < NLY; l++) write_packet(l, r, c);
+        break;
     }
 
     const uint32_t psot = (uint32_t)(out.size() - sot);
