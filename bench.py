@@ -368,8 +368,46 @@ def kernels_section(ctx, stream, flush, cs, hbm):
     q = Quantizer(ctx)
     out["dequantize_raw"] = entry(timed(lambda: q.dequantize(d_desc, len(desc), raw, deq, 0.5)), 8 * n,
                                   "tc_dequantize_raw over the 4096^2 x 3 workload's 12288 blocks")
+    out["reverse_97_levels"] = dwt_levels(ctx, stream, flush, W, lv, hbm)
     ctx.synchronize()
     return out
+
+
+def dwt_levels(ctx, stream, flush, n, levels, hbm, reps=7):
+    """Per level of tc_dwt_reverse97 on an n x n fp32 plane: the time of each
+    level as the difference of reverses with k and k - 1 levels (CUDA events,
+    median of reps, L2 flushed before each), the full-size level first, with
+    its algorithmic bytes (4 B read + 4 B written per output sample)."""
+    import torch
+    from thousandthchicken_b200.stages import DWTReverse97
+    dev = torch.device("cuda", ctx.device)
+    g = torch.Generator(device=dev).manual_seed(5)
+    x = torch.randn((n, n), generator=g, device=dev) * 30
+    y = torch.empty_like(x)
+    k = DWTReverse97(ctx)
+    med = {}
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            k.run(x, y, n, n, levels)
+        for lv in range(1, levels + 1):
+            ms = []
+            for r in range(reps):
+                flush.fill_(r & 0xFF)
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                k.run(x, y, n, n, lv)
+                b.record(stream)
+                b.synchronize()
+                ms.append(a.elapsed_time(b))
+            med[lv] = sorted(ms)[reps // 2]
+    rows = []
+    for lv, (w_, h_) in enumerate(_level_dims(n, n, levels), start=1):
+        us = (med[lv] - med.get(lv - 1, 0.0)) * 1e3
+        nbytes = 8 * w_ * h_
+        gbs = nbytes / max(us, 1e-3) / 1e3
+        rows.append({"size": w_, "us": round(us, 1), "gbs": round(gbs, 1), "frac": round(gbs / hbm, 4)})
+    return {"plane": n, "levels": rows,
+            "what": "tc_dwt_reverse97 level by level (reverses of k and k-1 levels differenced), full size first"}
 
 
 def _level_dims(w, h, levels):
@@ -609,7 +647,20 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=64)
     ap.add_argument("--size", type=int, default=0,
                     help="square image side for a smaller case of the same workload (profiling)")
+    ap.add_argument("--dwt-levels", type=int, default=0, metavar="N",
+                    help="only time tc_dwt_reverse97 level by level on an N x N plane (profiling)")
+    ap.add_argument("--dwt-depth", type=int, default=6, help="levels for --dwt-levels")
+    ap.add_argument("--dwt-reps", type=int, default=7, help="timed runs per level count for --dwt-levels")
     args = ap.parse_args()
+    if args.dwt_levels:
+        import torch
+        from thousandthchicken_b200.stages import Context
+        ctx = Context(0)
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+        res = dwt_levels(ctx, torch.cuda.current_stream(), flush, args.dwt_levels, args.dwt_depth,
+                         measured_peaks()[0], reps=args.dwt_reps)
+        print(json.dumps(res))
+        return
     if args.size:
         WORKLOAD["width"] = WORKLOAD["height"] = args.size
     rank = int(os.environ.get("RANK", "0"))
