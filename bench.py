@@ -501,7 +501,31 @@ def run_ours(args, rank, world, local_rank):
         t0 = time.perf_counter()
         dec.decode(host_cs, host_out)
         e2e_times.append(time.perf_counter() - t0)
-    e2e_s = max_over_ranks(sum(e2e_times) / e2e_steps, dist, f"cuda:{local_rank}")
+    e2e_seq_s = max_over_ranks(sum(e2e_times) / e2e_steps, dist, f"cuda:{local_rank}")
+    # A stream of images through the same call: two host threads, each with
+    # its own context (stream and buffers) and pinned output, take alternate
+    # images, so one image's parse, upload and read-back overlap the other's
+    # kernels.  Every image still makes its own host->device and
+    # device->host copies; wall time over all images.
+    dec2 = Decoder(Context(local_rank))
+    host_out2 = torch.empty((Cn, H, W), dtype=torch.uint8, pin_memory=True).numpy()
+    dec2.decode(host_cs, host_out2)
+    n_pipe = 2 * max(2, min(args.steps, 6))
+
+    def worker(d, o, n):
+        for _ in range(n):
+            d.decode(host_cs, o)
+
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    th = [threading.Thread(target=worker, args=(d, o, n_pipe // 2)) for d, o in ((dec, host_out), (dec2, host_out2))]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / n_pipe, dist, f"cuda:{local_rank}")
+    same_out = bool(np.array_equal(host_out, host_out2))
 
     batched, served, kernels, encode = None, None, None, None
     if not args.core_only:
@@ -614,7 +638,11 @@ def run_ours(args, rank, world, local_rank):
                              "frac": round(dwt_gbs / hbm, 4), "bytes_per_step": dw_bytes, "peak_kind": peak_kind},
             "e2e": {"value": round(W * H * world / e2e_s / 1e6, 2), "unit": "Mpixel/s",
                     "h2d_bytes_per_step": pool_bytes + 40 * ncblk + 4 * ncblk,
-                    "d2h_bytes_per_step": int(host_out.nbytes), "api": "tc_decode_j2k"},
+                    "d2h_bytes_per_step": int(host_out.nbytes), "api": "tc_decode_j2k",
+                    "mode": f"{n_pipe} images, 2 host threads with a context each (pinned codestream in, pinned "
+                            "samples out per image)",
+                    "sequential_value": round(W * H * world / e2e_seq_s / 1e6, 2),
+                    "outputs_identical": same_out},
             "gpu_launches": int(launches), "clocks": clocks, "psnr_db": round(psnr, 2),
             "wall_s_timed_region": round(wall, 3),
         }
