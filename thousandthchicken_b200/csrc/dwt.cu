@@ -184,13 +184,8 @@ cudaError_t run_fdwt(tc_ctx *ctx, const LevelIO &io)
 {
     using G = FwdGeo<WAVELET>;
     constexpr size_t smem = (size_t)G::NR * G::S * sizeof(T);
-    static bool attr[64] = {};
-    if (!attr[ctx->device & 63]) {
-        cudaError_t e = cudaFuncSetAttribute(fdwt_level_kernel<T, WAVELET, RND>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        attr[ctx->device & 63] = true;
-    }
+    static DeviceFlags attr;
+    if (cudaError_t e = set_smem_once(attr, ctx->device, fdwt_level_kernel<T, WAVELET, RND>, smem)) return e;
     dim3 grid((io.w + G::TX - 1) / G::TX, (io.h + G::TY - 1) / G::TY, io.ncomp);
     fdwt_level_kernel<T, WAVELET, RND><<<grid, kThreads, smem, ctx->stream>>>(io);
     ctx->launches++;

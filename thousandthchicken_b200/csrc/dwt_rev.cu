@@ -343,15 +343,6 @@ constexpr size_t rev_smem()
     return (size_t)(COLOR < 0 ? 1 : NCOMP) * RevGeo<WAVELET>::NR * RevGeo<WAVELET>::S * sizeof(T);
 }
 
-template <typename K>
-cudaError_t set_smem_once(tc_ctx *ctx, K kernel, size_t smem, bool (&done)[64])
-{
-    if (done[ctx->device & 63]) return cudaSuccess;
-    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess) done[ctx->device & 63] = true;
-    return e;
-}
-
 // A launch of one level: a single image (batch == nullptr, io given) or the
 // jobs of a batch (njobs jobs, ntiles tiles in all).
 struct RevLaunch {
@@ -367,16 +358,17 @@ cudaError_t run_rev(tc_ctx *ctx, const RevLaunch &L, int bits)
     constexpr size_t smem = rev_smem<T, WAVELET, NCOMP, COLOR>();
     cudaError_t e;
     if (L.io) {
-        static bool attr[64] = {};
-        if ((e = set_smem_once(ctx, idwt_rev_kernel<T, WAVELET, RND, NCOMP, COLOR, OT>, smem, attr)) != cudaSuccess)
+        static DeviceFlags attr;
+        if ((e = set_smem_once(attr, ctx->device, idwt_rev_kernel<T, WAVELET, RND, NCOMP, COLOR, OT>, smem)) !=
+            cudaSuccess)
             return e;
         const LevelIO &io = *L.io;
         dim3 grid((io.w + G::TX - 1) / G::TX, (io.h + G::TY - 1) / G::TY, COLOR < 0 ? io.ncomp : 1);
         idwt_rev_kernel<T, WAVELET, RND, NCOMP, COLOR, OT><<<grid, kThreads, smem, ctx->stream>>>(io, bits);
     } else {
         if (L.njobs <= 0 || L.ntiles <= 0) return cudaSuccess;
-        static bool attr[64] = {};
-        if ((e = set_smem_once(ctx, idwt_rev_batch_kernel<T, WAVELET, RND, NCOMP, COLOR, OT>, smem, attr)) !=
+        static DeviceFlags attr;
+        if ((e = set_smem_once(attr, ctx->device, idwt_rev_batch_kernel<T, WAVELET, RND, NCOMP, COLOR, OT>, smem)) !=
             cudaSuccess)
             return e;
         idwt_rev_batch_kernel<T, WAVELET, RND, NCOMP, COLOR, OT>

@@ -310,20 +310,11 @@ __global__ void __launch_bounds__(kThreads, 2) idwt97_ict_batch_kernel(const Rev
 
 constexpr size_t kIctSmem = (size_t)NR * S2 * sizeof(float2) + (size_t)NR * S1 * sizeof(float);
 
-template <typename K>
-cudaError_t smem_attr(tc_ctx *ctx, K kernel, size_t smem, bool (&done)[64])
-{
-    if (done[ctx->device & 63]) return cudaSuccess;
-    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess) done[ctx->device & 63] = true;
-    return e;
-}
-
 template <typename OT>
 cudaError_t ict_level(tc_ctx *ctx, const LevelIO &io, int bits)
 {
-    static bool attr[64] = {};
-    cudaError_t e = smem_attr(ctx, idwt97_ict_kernel<OT>, kIctSmem, attr);
+    static DeviceFlags attr;
+    cudaError_t e = set_smem_once(attr, ctx->device, idwt97_ict_kernel<OT>, kIctSmem);
     if (e != cudaSuccess) return e;
     dim3 grid((io.w + TX - 1) / TX, (io.h + TY - 1) / TY);
     idwt97_ict_kernel<OT><<<grid, kThreads, kIctSmem, ctx->stream>>>(io, bits);
@@ -334,8 +325,8 @@ cudaError_t ict_level(tc_ctx *ctx, const LevelIO &io, int bits)
 template <typename OT>
 cudaError_t ict_batch(tc_ctx *ctx, const RevJob *jobs, int njobs, int ntiles, int bits)
 {
-    static bool attr[64] = {};
-    cudaError_t e = smem_attr(ctx, idwt97_ict_batch_kernel<OT>, kIctSmem, attr);
+    static DeviceFlags attr;
+    cudaError_t e = set_smem_once(attr, ctx->device, idwt97_ict_batch_kernel<OT>, kIctSmem);
     if (e != cudaSuccess) return e;
     idwt97_ict_batch_kernel<OT><<<ntiles, kThreads, kIctSmem, ctx->stream>>>(jobs, njobs, bits);
     ctx->launches++;

@@ -629,7 +629,6 @@ __global__ void dequant_raw_kernel(const tc_cblk_desc *__restrict__ desc, int n,
 }
 
 struct LaunchCfg {
-    bool ready = false;
     int per_sm = 1;    // resident CTAs per SM
     int per_cta = 4;   // code-blocks in flight per CTA
     size_t smem = 0;   // dynamic shared memory per CTA
@@ -641,21 +640,21 @@ cudaError_t class_cfg(tc_ctx *ctx, LaunchCfg **out)
 {
     constexpr int kWarps = GroupCfg<MagT, G>::warps;
     static LaunchCfg cfg[64];
+    static DeviceFlags ready;
     LaunchCfg &C = cfg[ctx->device & 63];
-    if (!C.ready) {
+    const cudaError_t e = once_per_device(ready, ctx->device, [&] {
         C.smem = ((sizeof(Tables) + 15) & ~size_t(15)) + kWarps * (32 / G) * sizeof(WarpState<MagT>);
         C.per_cta = kWarps * (32 / G);
-        cudaError_t e = cudaFuncSetAttribute(t1_decode_kernel<MagT, G, Modes>,
+        cudaError_t r = cudaFuncSetAttribute(t1_decode_kernel<MagT, G, Modes>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C.smem);
-        if (e != cudaSuccess) return e;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&C.per_sm, t1_decode_kernel<MagT, G, Modes>, 32 * kWarps,
-                                                          C.smem);
-        if (e != cudaSuccess) return e;
+        if (r == cudaSuccess)
+            r = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&C.per_sm, t1_decode_kernel<MagT, G, Modes>,
+                                                              32 * kWarps, C.smem);
         if (C.per_sm < 1) C.per_sm = 1;
-        C.ready = true;
-    }
+        return r;
+    });
     *out = &C;
-    return cudaSuccess;
+    return e;
 }
 
 // One class launch: a persistent grid pulling the class's blocks from its

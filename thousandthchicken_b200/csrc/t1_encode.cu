@@ -413,12 +413,8 @@ cudaError_t launch_t1_encode(tc_ctx *ctx, const tc_t1_enc_desc *d_desc, int n, c
                              uint32_t cap, tc_t1_enc_result *d_res)
 {
     if (n <= 0) return cudaSuccess;
-    static bool attr[64] = {};
-    if (!attr[ctx->device & 63]) {
-        cudaError_t e = cudaFuncSetAttribute(t1_encode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEncSmem);
-        if (e != cudaSuccess) return e;
-        attr[ctx->device & 63] = true;
-    }
+    static DeviceFlags attr;
+    if (cudaError_t e = set_smem_once(attr, ctx->device, t1_encode_kernel, kEncSmem)) return e;
     t1_encode_kernel<<<(n + kEncWarps - 1) / kEncWarps, 32 * kEncWarps, kEncSmem, ctx->stream>>>(d_desc, n, d_in, d_out,
                                                                                                cap, d_res);
     ctx->launches++;

@@ -3,7 +3,9 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -15,6 +17,35 @@
 #define TC_DERR_STYLE 0x4u    // a styled code-block reached a style-0 launch, or its segment table is bad
 
 namespace tc {
+
+// One-time setup per device shared by every context (kernel attributes,
+// occupancy): fn runs once per device under a lock, and its results are
+// published to the other threads by the release store of the flag.
+inline std::mutex &device_setup_mutex()
+{
+    static std::mutex m;
+    return m;
+}
+using DeviceFlags = std::atomic<bool>[64];
+template <typename F>
+cudaError_t once_per_device(DeviceFlags &done, int device, F &&fn)
+{
+    std::atomic<bool> &d = done[device & 63];
+    if (d.load(std::memory_order_acquire)) return cudaSuccess;
+    std::lock_guard<std::mutex> lock(device_setup_mutex());
+    if (d.load(std::memory_order_relaxed)) return cudaSuccess;
+    const cudaError_t e = fn();
+    if (e == cudaSuccess) d.store(true, std::memory_order_release);
+    return e;
+}
+// cudaFuncSetAttribute(kernel, max dynamic shared memory) once per device.
+template <typename K>
+cudaError_t set_smem_once(DeviceFlags &done, int device, K kernel, size_t smem)
+{
+    return once_per_device(done, device, [&] {
+        return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    });
+}
 
 // Code-block style bits that change decoding (PTERM only constrains the
 // encoder's terminations).
