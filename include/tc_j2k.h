@@ -385,6 +385,10 @@ typedef struct tc_encode_params {
      * split by bytes in proportion, so every layer together gives the whole
      * codeword (no rate-distortion truncation points). */
     int32_t layers;
+    /* Packet headers: 0 in the packets, 1 packed into PPT marker segments of
+     * the tile-part header, 2 packed into PPM marker segments of the main
+     * header (ISO A.7.4-A.7.5). */
+    int32_t packed_headers;
 } tc_encode_params;
 
 /* Encode planar samples (8-bit when bits <= 8, else 16-bit; unsigned, or

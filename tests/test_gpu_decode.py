@@ -6,7 +6,7 @@ import pytest
 
 import oracle as O
 from conftest import golden_cases, load_golden, synth_image
-from test_host_codec import COC_QCC, LAYERED, LAYERED_IDS, PRECINCTS, SIGNED, STYLE_IDS, STYLES, SUBSAMPLED, TILED
+from test_host_codec import COC_QCC, LAYERED, LAYERED_IDS, PACKED, PRECINCTS, SIGNED, STYLE_IDS, STYLES, SUBSAMPLED, TILED
 from thousandthchicken_b200 import codec
 
 pytestmark = pytest.mark.gpu
@@ -477,4 +477,14 @@ def test_layered_streams_decode(gpu_ctx, style, prog, layers):
     img = synth_image(133, 91, 3, 8, seed=style + prog + layers)
     cs = codec.encode(img, 8, levels=3, cblk_log2=5, reversible=True, cblk_style=style, progression=prog,
                       layers=layers)
+    np.testing.assert_array_equal(_decoder(gpu_ctx).decode(cs), img)
+
+
+@pytest.mark.parametrize("where,style,prog,layers", PACKED,
+                         ids=[f"{'ppt' if w == 1 else 'ppm'}-style{s:#x}-prog{p}-{n}layers" for w, s, p, n in PACKED])
+def test_packed_packet_headers_decode(gpu_ctx, where, style, prog, layers):
+    """PPT / PPM streams decode on the GPU to the original."""
+    img = synth_image(133, 91, 3, 8, seed=where + prog)
+    cs = codec.encode(img, 8, levels=3, cblk_log2=5, reversible=True, cblk_style=style, progression=prog,
+                      layers=layers, packed_headers=where)
     np.testing.assert_array_equal(_decoder(gpu_ctx).decode(cs), img)

@@ -647,3 +647,59 @@ def test_layered_streams_through_oracle(style, prog, layers):
     np.testing.assert_array_equal(openjpeg_decode(cs), img)
     _, out = oracle_decode_tiled(cs)
     np.testing.assert_array_equal(out, img)
+
+
+def _header_markers(cs):
+    """Marker codes of the main header and of the first tile-part header."""
+    main, tile, i = [], [], 2
+    while i + 4 <= len(cs):
+        m = int.from_bytes(cs[i:i + 2], "big")
+        if m == 0xFF90:  # SOT: the tile-part header follows its 10-byte segment
+            i += 12
+            while i + 2 <= len(cs):
+                m = int.from_bytes(cs[i:i + 2], "big")
+                if m == 0xFF93:
+                    return main, tile
+                tile.append(m)
+                i += 2 + int.from_bytes(cs[i + 2:i + 4], "big")
+            break
+        main.append(m)
+        i += 2 + int.from_bytes(cs[i + 2:i + 4], "big")
+    return main, tile
+
+
+PACKED = [  # (PPT 1 / PPM 2, code-block style, progression, layers)
+    (1, 0, 0, 1), (1, codec.CBLK_STYLE_BYPASS, 1, 4), (1, 0x3F, 4, 2),
+    (2, 0, 2, 3), (2, codec.CBLK_STYLE_BYPASS | codec.CBLK_STYLE_TERMALL, 3, 5),
+]
+
+
+@pytest.mark.parametrize("where,style,prog,layers", PACKED,
+                         ids=[f"{'ppt' if w == 1 else 'ppm'}-style{s:#x}-prog{p}-{n}layers" for w, s, p, n in PACKED])
+def test_packed_packet_headers_through_oracle(where, style, prog, layers):
+    """Packet headers packed into PPT (tile-part header) or PPM (main
+    header, with each tile-part's Nppm) marker segments, ISO A.7.4-A.7.5:
+    the parser reads the headers from the packed stream and the bodies from
+    the tile-part; OpenJPEG and the oracle give back the original."""
+    from gpu_helpers import oracle_decode_tiled, openjpeg_decode
+    img = synth_image(133, 91, 3, 8, seed=where + prog)
+    cs = codec.encode(img, 8, levels=3, cblk_log2=5, reversible=True, cblk_style=style, progression=prog,
+                      layers=layers, packed_headers=where)
+    main, tile = _header_markers(cs)
+    assert (0xFF61 in tile) == (where == 1) and (0xFF60 in main) == (where == 2)
+    np.testing.assert_array_equal(openjpeg_decode(cs), img)
+    _, out = oracle_decode_tiled(cs)
+    np.testing.assert_array_equal(out, img)
+
+
+@pytest.mark.parametrize("where", [1, 2], ids=["ppt", "ppm"])
+def test_packed_headers_over_several_marker_segments(where):
+    """Headers longer than one marker segment (65532 bytes) continue in the
+    next PPT / PPM segment (Zppt / Zppm incrementing)."""
+    from gpu_helpers import oracle_decode_tiled
+    img = synth_image(700, 500, 3, 8, seed=9)
+    cs = codec.encode(img, 8, levels=5, cblk_log2=2, reversible=True, layers=12, packed_headers=where)
+    main, tile = _header_markers(cs)
+    assert (tile if where == 1 else main).count(0xFF61 if where == 1 else 0xFF60) >= 2
+    _, out = oracle_decode_tiled(cs)
+    np.testing.assert_array_equal(out, img)

@@ -25,6 +25,8 @@ def _bases():
         codec.encode(img, 8, levels=2, cblk_log2=3, reversible=False, cblk_style=0x05, layers=4, progression=4),
         codec.encode(img, 8, levels=2, cblk_log2=4, reversible=True, cblk_style=0x01, layers=5, progression=1),
         codec.encode([img[0], img[1][::2, ::2]], 8, levels=2, mct=False, comp_subsampling=[(1, 1), (2, 2)]),
+        codec.encode(img, 8, levels=2, cblk_log2=4, reversible=True, layers=3, packed_headers=1),
+        codec.encode(img, 8, levels=2, cblk_log2=4, reversible=True, cblk_style=0x01, layers=2, packed_headers=2),
     ]
     bases += [p.read_bytes() for p in sorted(GOLDEN.glob("*.j2k"))[:4]]
     from PIL import Image

@@ -78,7 +78,7 @@ class EncodeParams(C.Structure):
                 ("progression", C.c_int32), ("threads", C.c_int32), ("is_signed", C.c_int32),
                 ("comp_cblk_log2", C.c_int32 * 4), ("comp_step_scale", C.c_double * 4),
                 ("comp_dx", C.c_int32 * 4), ("comp_dy", C.c_int32 * 4), ("cblk_style", C.c_int32),
-                ("layers", C.c_int32)]
+                ("layers", C.c_int32), ("packed_headers", C.c_int32)]
 
 
 assert C.sizeof(CblkDesc) == 40

@@ -140,7 +140,7 @@ def encode_gpu(ctx, planes: np.ndarray, bits: int, levels: int = 5, reversible: 
 def encode(planes: np.ndarray, bits: int, levels: int = 5, reversible: bool = True, mct: bool = True,
            cblk_log2: int = 6, base_step: float = 1.0 / 128, guard_bits: int = 0, progression: int = 0,
            threads: int = 0, comp_cblk_log2=None, comp_step_scale=None, comp_subsampling=None,
-           cblk_style: int = 0, layers: int = 1) -> bytes:
+           cblk_style: int = 0, layers: int = 1, packed_headers: int = 0) -> bytes:
     """Harness encoder: planar samples [ncomp, h, w] -> codestream; signed
     integer arrays (int8 / int16) give signed components (no DC shift).
     comp_cblk_log2 / comp_step_scale: per-component code-block size exponent
@@ -149,11 +149,14 @@ def encode(planes: np.ndarray, bits: int, levels: int = 5, reversible: bool = Tr
     planes is then a list of component arrays of ceil(h/dy) x ceil(w/dx).
     cblk_style: code-block style bits (CBLK_STYLE_*) for every component.
     layers: quality layers; each block's passes are split evenly over them
-    (all layers together give the whole codeword)."""
+    (all layers together give the whole codeword).
+    packed_headers: 0 packet headers in the packets, 1 in PPT marker
+    segments, 2 in PPM marker segments."""
     planes, p = _encode_params(planes, bits, levels, reversible, mct, cblk_log2, base_step, guard_bits, progression,
                                threads, comp_cblk_log2, comp_step_scale, comp_subsampling)
     p.cblk_style = int(cblk_style)
     p.layers = int(layers)
+    p.packed_headers = int(packed_headers)
     cap = planes.nbytes * 3 + 65536
     out = np.empty(cap, np.uint8)
     n = C.c_size_t(0)

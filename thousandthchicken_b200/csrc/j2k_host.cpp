@@ -911,6 +911,9 @@ struct Params {
         int64_t x0, y0, x1, y1;
     };
     std::vector<Tile> tiles;
+    // packed packet headers of the main header (PPM, ISO A.7.4): Zppm and
+    // the segment's Ippm bytes
+    std::vector<std::pair<int, std::vector<uint8_t>>> ppm;
 };
 
 // Precedence of ISO A.6: tile COC > tile COD > main COC > main COD, and
@@ -1143,8 +1146,14 @@ static int parse_main(Reader &rd, Params &P, std::string &err)
             if (rc) return rc;
             break;
         }
-        case M_RGN: case M_PPM: case M_CRG:
-            err = "RGN/PPM/CRG markers are not supported";
+        case M_PPM: {
+            if (seg_end - rd.pos < 1) { err = "bad PPM"; return TC_E_CODESTREAM; }
+            const int z = (int)rd.u8();
+            P.ppm.emplace_back(z, std::vector<uint8_t>(rd.d + rd.pos, rd.d + seg_end));
+            break;
+        }
+        case M_RGN: case M_CRG:
+            err = "RGN/CRG markers are not supported";
             return TC_E_UNSUPPORTED;
         default:
             break;  // COM, TLM, PLM and others carry nothing we need
@@ -1285,7 +1294,7 @@ struct Emit {
 // the tiles (codestream.c:524-527).
 static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Params::Tile &T, const Scope &ts,
                       const std::vector<std::pair<size_t, size_t>> &parts, uint64_t coef_off, Parsed &out,
-                      Emit &em, std::string &err)
+                      Emit &em, std::string &err, const std::vector<uint8_t> *packed = nullptr)
 {
     int rc;
     if ((rc = check_coding(P, &ts, err))) return rc;
@@ -1396,18 +1405,25 @@ static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Para
 
     std::vector<SegNode> arena;
     std::vector<std::pair<CblkState *, uint32_t>> contrib;  // one packet's blocks and lengths
+    // Packed packet headers (PPM / PPT): the headers are read from the
+    // tile's packed stream at hpos, the bodies from the tile-parts.
+    const bool pk = packed != nullptr;
+    size_t hpos = 0;
     // One packet (ISO B.9, B.10): layer, resolution, component, precinct.
     auto read_packet = [&](int layer, int r, int c, int prec) -> int {
         while (part_i < parts.size() && pos >= parts[part_i].second) {
             part_i++;
             if (part_i < parts.size()) pos = parts[part_i].first;
         }
-        if (part_i >= parts.size()) { err = "packet data missing"; return TC_E_CODESTREAM; }
-        const size_t pend = part_end();
-        if (scod & 2) {  // SOP
+        if (part_i >= parts.size() && !pk) { err = "packet data missing"; return TC_E_CODESTREAM; }
+        const size_t pend = part_i < parts.size() ? part_end() : pos;
+        if (scod & 2) {  // SOP, in the body
             if (pos + 6 <= pend && cs[pos] == 0xFF && cs[pos + 1] == 0x91) pos += 6;
         }
-        BitReader br(cs, pos, pend);
+        const uint8_t *hs = pk ? packed->data() : cs;
+        size_t &hp = pk ? hpos : pos;
+        const size_t hend = pk ? packed->size() : pend;
+        BitReader br(hs, hp, hend);
         const int present = br.get();
         contrib.clear();
         ResState &rs = st[c][r];
@@ -1474,10 +1490,10 @@ static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Para
         }
         br.align();
         if (br.overrun) { err = "packet header overrun"; return TC_E_CODESTREAM; }
-        pos = br.pos;
-        if (scod & 4) {  // EPH
-            if (pos + 2 > pend || cs[pos] != 0xFF || cs[pos + 1] != 0x92) { err = "missing EPH"; return TC_E_CODESTREAM; }
-            pos += 2;
+        hp = br.pos;
+        if (scod & 4) {  // EPH, after the header (in the packed stream when headers are packed)
+            if (hp + 2 > hend || hs[hp] != 0xFF || hs[hp + 1] != 0x92) { err = "missing EPH"; return TC_E_CODESTREAM; }
+            hp += 2;
         }
         for (auto &cl : contrib) {
             if (pos + cl.second > pend) { err = "code-block data runs past the tile-part"; return TC_E_CODESTREAM; }
@@ -1671,6 +1687,19 @@ static int parse_raw_codestream(const uint8_t *cs, size_t len, Parsed &out, std:
     std::vector<std::vector<std::pair<size_t, size_t>>> parts(ntiles);
     std::vector<Scope> tscope(ntiles);
     for (Scope &t : tscope) t.init(P.ncomp);
+    // Packed packet headers per tile: PPT segments (Zppt, bytes) from its
+    // tile-part headers, or its tile-parts' shares of the PPM stream, which
+    // gives each tile-part in codestream order Nppm (32 bits) and then Nppm
+    // bytes of headers.
+    std::vector<std::vector<std::pair<int, std::vector<uint8_t>>>> ppt(ntiles);
+    std::vector<std::vector<uint8_t>> packed(ntiles);
+    std::vector<uint8_t> ppm;
+    size_t ppm_pos = 0;
+    if (!P.ppm.empty()) {
+        std::vector<std::pair<int, std::vector<uint8_t>>> segs = P.ppm;
+        std::stable_sort(segs.begin(), segs.end(), [](const auto &a, const auto &b) { return a.first < b.first; });
+        for (auto &sg : segs) ppm.insert(ppm.end(), sg.second.begin(), sg.second.end());
+    }
     for (;;) {
         const uint32_t m = rd.u16();
         if (rd.bad) { err = "truncated codestream"; return TC_E_CODESTREAM; }
@@ -1696,11 +1725,25 @@ static int parse_raw_codestream(const uint8_t *cs, size_t len, Parsed &out, std:
                 if ((rc = read_coding_marker(rd, mm, seg_end, P.ncomp, tscope[isot], err))) return rc;
             } else if (mm == M_POC) {
                 if ((rc = read_poc(rd, seg_end, P.ncomp, tscope[isot].poc, err))) return rc;
-            } else if (mm == M_RGN || mm == M_PPT) {
-                err = "RGN/PPT in a tile-part header are not supported";
+            } else if (mm == M_PPT) {
+                if (!P.ppm.empty()) { err = "PPT with PPM"; return TC_E_CODESTREAM; }
+                if (seg_end - rd.pos < 1) { err = "bad PPT"; return TC_E_CODESTREAM; }
+                const int z = (int)rd.u8();
+                ppt[isot].emplace_back(z, std::vector<uint8_t>(cs + rd.pos, cs + seg_end));
+            } else if (mm == M_RGN) {
+                err = "RGN in a tile-part header is not supported";
                 return TC_E_UNSUPPORTED;
             }
             rd.pos = seg_end;
+        }
+        if (!ppm.empty()) {
+            if (ppm.size() - ppm_pos < 4) { err = "PPM has no headers for a tile-part"; return TC_E_CODESTREAM; }
+            const uint32_t n = (uint32_t)ppm[ppm_pos] << 24 | (uint32_t)ppm[ppm_pos + 1] << 16 |
+                               (uint32_t)ppm[ppm_pos + 2] << 8 | ppm[ppm_pos + 3];
+            ppm_pos += 4;
+            if (n > ppm.size() - ppm_pos) { err = "PPM headers run past the PPM data"; return TC_E_CODESTREAM; }
+            packed[isot].insert(packed[isot].end(), ppm.begin() + ppm_pos, ppm.begin() + ppm_pos + n);
+            ppm_pos += n;
         }
         parts[isot].emplace_back(rd.pos, end);
         rd.pos = end;
@@ -1716,7 +1759,13 @@ static int parse_raw_codestream(const uint8_t *cs, size_t len, Parsed &out, std:
     for (size_t t = 0; t < ntiles; t++) {
         const Params::Tile &T = P.tiles[t];
         if (parts[t].empty()) { err = "tile " + std::to_string(t) + " has no tile-part"; return TC_E_CODESTREAM; }
-        if ((rc = parse_tile(cs, len, P, T, tscope[t], parts[t], coef_off, out, em, err))) return rc;
+        if (!ppt[t].empty()) {
+            std::stable_sort(ppt[t].begin(), ppt[t].end(), [](const auto &a, const auto &b) { return a.first < b.first; });
+            for (auto &sg : ppt[t]) packed[t].insert(packed[t].end(), sg.second.begin(), sg.second.end());
+        }
+        const bool pk = !ppm.empty() || !ppt[t].empty();
+        if ((rc = parse_tile(cs, len, P, T, tscope[t], parts[t], coef_off, out, em, err, pk ? &packed[t] : nullptr)))
+            return rc;
         tc_tile_info ti;
         ti.x0 = (int32_t)(T.x0 - P.xo);
         ti.y0 = (int32_t)(T.y0 - P.yo);
@@ -1782,6 +1831,7 @@ int encode_layout(const tc_encode_params &p, EncodeLayout &L, std::string &err)
     if (!p.reversible && !(p.base_step > 0.0)) { err = "base_step must be positive"; return TC_E_ARG; }
     if (p.cblk_style & ~0x3F) { err = "unknown code-block style bits"; return TC_E_ARG; }
     if (p.layers < 0 || p.layers > 64) { err = "layers out of range"; return TC_E_ARG; }
+    if (p.packed_headers < 0 || p.packed_headers > 2) { err = "packed_headers out of range"; return TC_E_ARG; }
     // Per component: code-block size (COC when it differs from COD), step
     // multiplier (QCC when it differs from QCD) and subsampling (SIZ).
     for (int c = 0; c < C; c++) {
@@ -2040,14 +2090,11 @@ int encode_assemble(const tc_encode_params &p, EncodeLayout &L, const std::vecto
         wr.u8(c);                          // Cqcc
         write_steps(c);
     }
-    const size_t sot = out.size();
-    wr.u16(M_SOT);
-    wr.u16(10);
-    wr.u16(0);
-    wr.u32(0);  // Psot, below
-    wr.u8(0);
-    wr.u8(1);
-    wr.u16(M_SOD);
+    // Packets go to `body`; their headers too, or to `hdrs` when they are
+    // packed into PPT / PPM marker segments (p.packed_headers 1 / 2).
+    std::vector<uint8_t> body, hdrs;
+    body.reserve(total + 8 * jobs.size());
+    std::vector<uint8_t> &hdst = p.packed_headers ? hdrs : body;
     // Quality layers: block k's passes [lp(k, l), lp(k, l + 1)) go into
     // layer l.  A codeword segment that a layer boundary cuts is split by
     // bytes in proportion to its passes, so a decoder given every layer
@@ -2114,11 +2161,11 @@ int encode_assemble(const tc_encode_params &p, EncodeLayout &L, const std::vecto
         if (!any) {
             bw.put(0);
             bw.flush();
-            out.insert(out.end(), hdr.begin(), hdr.end());
+            hdst.insert(hdst.end(), hdr.begin(), hdr.end());
             return;
         }
         bw.put(1);
-        std::vector<std::pair<uint32_t, uint32_t>> body;  // byte ranges of the blocks' codewords
+        std::vector<std::pair<uint32_t, uint32_t>> ranges;  // byte ranges of the blocks' codewords
         std::vector<std::pair<uint32_t, int>> chunks;
         for (int bi = 0; bi < (int)geo[c][r].bands.size(); bi++) {
             const Band &b = geo[c][r].bands[bi];
@@ -2160,12 +2207,12 @@ int encode_assemble(const tc_encode_params &p, EncodeLayout &L, const std::vecto
                 bw.put(0);
                 lblock[k] += incr;
                 for (auto &ch : chunks) bw.put_bits(ch.first, lblock[k] + floorlog2(ch.second));
-                body.emplace_back(bytes_at(k, t0), bytes_at(k, t1));
+                ranges.emplace_back(bytes_at(k, t0), bytes_at(k, t1));
                 (void)cd;
             }
         }
         bw.flush();
-        out.insert(out.end(), hdr.begin(), hdr.end());
+        hdst.insert(hdst.end(), hdr.begin(), hdr.end());
         size_t bi = 0;
         for (int bb = 0; bb < (int)geo[c][r].bands.size(); bb++) {
             const Band &b = geo[c][r].bands[bb];
@@ -2175,8 +2222,8 @@ int encode_assemble(const tc_encode_params &p, EncodeLayout &L, const std::vecto
             for (int i = 0; i < n; i++) {
                 const size_t k = (size_t)k0 + i;
                 if (lp(k, l + 1) == lp(k, l)) continue;
-                const auto &rg = body[bi++];
-                out.insert(out.end(), coded[k].data + rg.first, coded[k].data + rg.second);
+                const auto &rg = ranges[bi++];
+                body.insert(body.end(), coded[k].data + rg.first, coded[k].data + rg.second);
             }
         }
     };
@@ -2205,6 +2252,38 @@ int encode_assemble(const tc_encode_params &p, EncodeLayout &L, const std::vecto
         break;
     }
 
+    // Packed packet headers (ISO A.7.4-A.7.5): PPM in the main header holds,
+    // for the one tile-part, Nppm and the headers; PPT in the tile-part
+    // header holds the headers.  Each marker segment carries at most 65532
+    // bytes after its index.
+    auto put_packed = [&](uint32_t marker, const std::vector<uint8_t> &data) {
+        size_t at = 0;
+        int z = 0;
+        do {
+            const size_t n = std::min<size_t>(data.size() - at, 65532);
+            wr.u16(marker);
+            wr.u16((uint32_t)(n + 3));
+            wr.u8(z++ & 0xFF);
+            out.insert(out.end(), data.begin() + at, data.begin() + at + n);
+            at += n;
+        } while (at < data.size());
+    };
+    if (p.packed_headers == 2) {
+        std::vector<uint8_t> ippm = {(uint8_t)(hdrs.size() >> 24), (uint8_t)(hdrs.size() >> 16),
+                                     (uint8_t)(hdrs.size() >> 8), (uint8_t)hdrs.size()};
+        ippm.insert(ippm.end(), hdrs.begin(), hdrs.end());
+        put_packed(M_PPM, ippm);
+    }
+    const size_t sot = out.size();
+    wr.u16(M_SOT);
+    wr.u16(10);
+    wr.u16(0);
+    wr.u32(0);  // Psot, below
+    wr.u8(0);
+    wr.u8(1);
+    if (p.packed_headers == 1) put_packed(M_PPT, hdrs);
+    wr.u16(M_SOD);
+    out.insert(out.end(), body.begin(), body.end());
     const uint32_t psot = (uint32_t)(out.size() - sot);
     out[sot + 6] = (uint8_t)(psot >> 24);
     out[sot + 7] = (uint8_t)(psot >> 16);
