@@ -96,7 +96,10 @@ typedef struct tc_cblk_desc {
     uint8_t  orient;         /* 0 LL, 1 HL, 2 LH, 3 HH (type_orient) */
     uint8_t  flags;          /* TC_CBLK_* */
     uint8_t  style;          /* code-block style, TC_CBLK_STYLE_* (0: none) */
-    uint8_t  reserved[2];
+    uint8_t  roi_shift;      /* ROI maxshift s (RGN, ISO Annex H; 0: none): mb
+                                counts the s extra bit-planes, and a decoded
+                                magnitude >= 2^s is shifted down by s */
+    uint8_t  reserved[1];
 } tc_cblk_desc;
 
 #define TC_CBLK_IRREVERSIBLE 0x01  /* float output, multiply by step */
@@ -389,6 +392,11 @@ typedef struct tc_encode_params {
      * the tile-part header, 2 packed into PPM marker segments of the main
      * header (ISO A.7.4-A.7.5). */
     int32_t packed_headers;
+    /* Region of interest [roi_x0, roi_x1) x [roi_y0, roi_y1) in image
+     * samples (empty: none), coded with the maxshift method (RGN, ISO
+     * Annex H): per component, the shift is the bit count of the largest
+     * background magnitude. */
+    int32_t roi_x0, roi_y0, roi_x1, roi_y1;
 } tc_encode_params;
 
 /* Encode planar samples (8-bit when bits <= 8, else 16-bit; unsigned, or

@@ -883,6 +883,17 @@ static void or_t1_one(void *arg, int i)
         __atomic_store_n(&J->err, 1, __ATOMIC_RELAXED);
         return;
     }
+    /* ROI maxshift (ISO H.1): a magnitude >= 2^roi belongs to the region and
+     * is scaled down by 2^roi, its undecoded planes with it; the background
+     * keeps its value. */
+    if (c->roi)
+        for (int i = 0; i < c->w * c->h; i++) {
+            const int32_t a = q[i] < 0 ? -q[i] : q[i];
+            if (a >> c->roi) {
+                q[i] = q[i] < 0 ? -(a >> c->roi) : (a >> c->roi);
+                u[i] = (uint8_t)(u[i] > c->roi ? u[i] - c->roi : 0);
+            }
+        }
     for (int y = 0; y < c->h; y++) {
         const size_t o = (size_t)c->comp * np + (size_t)(c->out_y + y) * J->w + c->out_x;
         if (J->reversible) {

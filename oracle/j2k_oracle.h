@@ -138,7 +138,7 @@ typedef struct or_cblk {
     uint32_t seg_len;
     uint16_t w, h;
     uint8_t passes, mb, zero_bitplanes, orient;
-    uint8_t comp, flags, style, pad1;  /* style: OR_STYLE_* */
+    uint8_t comp, flags, style, roi;   /* style: OR_STYLE_*; roi: ROI maxshift (0: none) */
     uint32_t out_x, out_y;   /* position in the component's Mallat plane */
     float step;              /* dequantisation step (irreversible only) */
 } or_cblk;

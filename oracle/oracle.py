@@ -22,7 +22,7 @@ _lib = None
 class OrCblk(C.Structure):
     _fields_ = [("seg_off", C.c_uint64), ("seg_len", C.c_uint32), ("w", C.c_uint16), ("h", C.c_uint16),
                 ("passes", C.c_uint8), ("mb", C.c_uint8), ("zero_bitplanes", C.c_uint8), ("orient", C.c_uint8),
-                ("comp", C.c_uint8), ("flags", C.c_uint8), ("style", C.c_uint8), ("pad1", C.c_uint8),
+                ("comp", C.c_uint8), ("flags", C.c_uint8), ("style", C.c_uint8), ("roi", C.c_uint8),
                 ("out_x", C.c_uint32), ("out_y", C.c_uint32), ("step", C.c_float)]
 
 
@@ -202,6 +202,8 @@ def decode_tile(cblks, pool: np.ndarray, w, h, ncomp, bits, levels, reversible, 
         c.comp = comp
         if "style" in (d.dtype.names or ()):
             c.style = int(d["style"])
+        if "roi_shift" in (d.dtype.names or ()):
+            c.roi = int(d["roi_shift"])
         c.out_x, c.out_y = ox, oy
         c.step = float(d["step"])
     out = np.zeros((ncomp, h, w), np.uint16)

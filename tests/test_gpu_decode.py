@@ -6,7 +6,8 @@ import pytest
 
 import oracle as O
 from conftest import golden_cases, load_golden, synth_image
-from test_host_codec import COC_QCC, LAYERED, LAYERED_IDS, PACKED, PRECINCTS, SIGNED, STYLE_IDS, STYLES, SUBSAMPLED, TILED
+from test_host_codec import (COC_QCC, LAYERED, LAYERED_IDS, PACKED, PRECINCTS, ROI, ROI_IDS, SIGNED, STYLE_IDS, STYLES,
+                             SUBSAMPLED, TILED)
 from thousandthchicken_b200 import codec
 
 pytestmark = pytest.mark.gpu
@@ -488,3 +489,20 @@ def test_packed_packet_headers_decode(gpu_ctx, where, style, prog, layers):
     cs = codec.encode(img, 8, levels=3, cblk_log2=5, reversible=True, cblk_style=style, progression=prog,
                       layers=layers, packed_headers=where)
     np.testing.assert_array_equal(_decoder(gpu_ctx).decode(cs), img)
+
+
+@pytest.mark.parametrize("bits,comps,roi,kw", ROI, ids=ROI_IDS)
+def test_roi_maxshift_decode(gpu_ctx, bits, comps, roi, kw):
+    """ROI maxshift streams on the GPU: the Tier-1 epilogue shifts region
+    magnitudes back down; lossless equals the original, lossy is within 1
+    of the oracle."""
+    from gpu_helpers import oracle_decode_tiled
+    img = synth_image(133, 91, comps, bits, seed=bits + comps)
+    cs = codec.encode(img, bits, levels=3, cblk_log2=5, mct=comps == 3, roi=roi, **kw)
+    got = _decoder(gpu_ctx).decode(cs)
+    if kw["reversible"]:
+        np.testing.assert_array_equal(got, img)
+    else:
+        _, want = oracle_decode_tiled(cs)
+        d = np.abs(got.astype(np.int64) - want.astype(np.int64))
+        assert d.max() <= 1 and (d > 0).mean() < 0.01

@@ -703,3 +703,37 @@ def test_packed_headers_over_several_marker_segments(where):
     assert (tile if where == 1 else main).count(0xFF61 if where == 1 else 0xFF60) >= 2
     _, out = oracle_decode_tiled(cs)
     np.testing.assert_array_equal(out, img)
+
+
+ROI = [  # (bits, components, region, harness options)
+    (8, 3, (30, 20, 90, 60), dict(reversible=True)),
+    (8, 3, (0, 0, 40, 91), dict(reversible=True, layers=3, progression=2)),
+    (12, 1, (10, 10, 70, 70), dict(reversible=True, cblk_style=0x01)),
+    (8, 3, (50, 10, 133, 50), dict(reversible=False, base_step=1 / 256)),
+]
+ROI_IDS = ["rgb-53", "rgb-53-layers-rpcl", "g12-bypass", "rgb-97"]
+
+
+@pytest.mark.parametrize("bits,comps,roi,kw", ROI, ids=ROI_IDS)
+def test_roi_maxshift_through_oracle(bits, comps, roi, kw):
+    """Region of interest with the maxshift method (RGN, ISO Annex H): the
+    region's coefficients are shifted above every background bit-plane, the
+    bands code s more bit-planes, and a decoded magnitude >= 2^s is shifted
+    back down.  Lossless streams give back the original through the parser +
+    oracle and (8-bit) through OpenJPEG; the 9/7 stream stays within the
+    quantiser's error."""
+    from gpu_helpers import oracle_decode_tiled, openjpeg_decode
+    img = synth_image(133, 91, comps, bits, seed=bits + comps)
+    cs = codec.encode(img, bits, levels=3, cblk_log2=5, mct=comps == 3, roi=roi, **kw)
+    main, _ = _header_markers(cs)
+    assert 0xFF5E in main
+    info, desc, pool = codec.parse(cs)
+    assert (desc["roi_shift"] > 0).all()
+    _, out = oracle_decode_tiled(cs)
+    if kw["reversible"]:
+        np.testing.assert_array_equal(out, img)
+        if bits == 8:
+            np.testing.assert_array_equal(openjpeg_decode(cs), img)
+    else:
+        err = out.astype(np.int64) - img
+        assert np.abs(err).max() <= 4 and 10 * np.log10(255 ** 2 / np.mean(err ** 2)) > 45

@@ -27,6 +27,7 @@ def _bases():
         codec.encode([img[0], img[1][::2, ::2]], 8, levels=2, mct=False, comp_subsampling=[(1, 1), (2, 2)]),
         codec.encode(img, 8, levels=2, cblk_log2=4, reversible=True, layers=3, packed_headers=1),
         codec.encode(img, 8, levels=2, cblk_log2=4, reversible=True, cblk_style=0x01, layers=2, packed_headers=2),
+        codec.encode(img, 8, levels=2, cblk_log2=4, reversible=True, roi=(10, 5, 40, 30)),
     ]
     bases += [p.read_bytes() for p in sorted(GOLDEN.glob("*.j2k"))[:4]]
     from PIL import Image

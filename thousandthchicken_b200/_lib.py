@@ -49,7 +49,8 @@ class CblkDesc(C.Structure):
     _fields_ = [("seg_off", C.c_uint64), ("out_off", C.c_uint64), ("seg_len", C.c_uint32),
                 ("out_pitch", C.c_uint32), ("step", C.c_float), ("w", C.c_uint16), ("h", C.c_uint16),
                 ("passes", C.c_uint8), ("mb", C.c_uint8), ("zero_bitplanes", C.c_uint8),
-                ("orient", C.c_uint8), ("flags", C.c_uint8), ("style", C.c_uint8), ("reserved", C.c_uint8 * 2)]
+                ("orient", C.c_uint8), ("flags", C.c_uint8), ("style", C.c_uint8), ("roi_shift", C.c_uint8),
+                ("reserved", C.c_uint8 * 1)]
 
 
 class ImageInfo(C.Structure):
@@ -78,7 +79,8 @@ class EncodeParams(C.Structure):
                 ("progression", C.c_int32), ("threads", C.c_int32), ("is_signed", C.c_int32),
                 ("comp_cblk_log2", C.c_int32 * 4), ("comp_step_scale", C.c_double * 4),
                 ("comp_dx", C.c_int32 * 4), ("comp_dy", C.c_int32 * 4), ("cblk_style", C.c_int32),
-                ("layers", C.c_int32), ("packed_headers", C.c_int32)]
+                ("layers", C.c_int32), ("packed_headers", C.c_int32), ("roi_x0", C.c_int32),
+                ("roi_y0", C.c_int32), ("roi_x1", C.c_int32), ("roi_y1", C.c_int32)]
 
 
 assert C.sizeof(CblkDesc) == 40

@@ -13,7 +13,7 @@ from . import _lib as L
 DESC_DTYPE = np.dtype([("seg_off", "<u8"), ("out_off", "<u8"), ("seg_len", "<u4"), ("out_pitch", "<u4"),
                        ("step", "<f4"), ("w", "<u2"), ("h", "<u2"), ("passes", "u1"), ("mb", "u1"),
                        ("zero_bitplanes", "u1"), ("orient", "u1"), ("flags", "u1"), ("style", "u1"),
-                       ("reserved", "u1", (2,))])
+                       ("roi_shift", "u1"), ("reserved", "u1", (1,))])
 assert DESC_DTYPE.itemsize == 40
 
 INFO_FIELDS = ("width", "height", "ncomp", "bits", "is_signed", "levels", "reversible", "mct", "cblk_w",
@@ -140,7 +140,7 @@ def encode_gpu(ctx, planes: np.ndarray, bits: int, levels: int = 5, reversible: 
 def encode(planes: np.ndarray, bits: int, levels: int = 5, reversible: bool = True, mct: bool = True,
            cblk_log2: int = 6, base_step: float = 1.0 / 128, guard_bits: int = 0, progression: int = 0,
            threads: int = 0, comp_cblk_log2=None, comp_step_scale=None, comp_subsampling=None,
-           cblk_style: int = 0, layers: int = 1, packed_headers: int = 0) -> bytes:
+           cblk_style: int = 0, layers: int = 1, packed_headers: int = 0, roi=None) -> bytes:
     """Harness encoder: planar samples [ncomp, h, w] -> codestream; signed
     integer arrays (int8 / int16) give signed components (no DC shift).
     comp_cblk_log2 / comp_step_scale: per-component code-block size exponent
@@ -151,12 +151,16 @@ def encode(planes: np.ndarray, bits: int, levels: int = 5, reversible: bool = Tr
     layers: quality layers; each block's passes are split evenly over them
     (all layers together give the whole codeword).
     packed_headers: 0 packet headers in the packets, 1 in PPT marker
-    segments, 2 in PPM marker segments."""
+    segments, 2 in PPM marker segments.
+    roi: (x0, y0, x1, y1), a region of interest in image samples coded with
+    the maxshift method (RGN)."""
     planes, p = _encode_params(planes, bits, levels, reversible, mct, cblk_log2, base_step, guard_bits, progression,
                                threads, comp_cblk_log2, comp_step_scale, comp_subsampling)
     p.cblk_style = int(cblk_style)
     p.layers = int(layers)
     p.packed_headers = int(packed_headers)
+    if roi is not None:
+        p.roi_x0, p.roi_y0, p.roi_x1, p.roi_y1 = (int(v) for v in roi)
     cap = planes.nbytes * 3 + 65536
     out = np.empty(cap, np.uint8)
     n = C.c_size_t(0)

@@ -1278,6 +1278,8 @@ int tc_encode_j2k_gpu(tc_ctx *ctx, const tc_encode_params *p, const void *h_plan
             return fail(ctx, TC_E_UNSUPPORTED, "tc_encode_j2k_gpu: subsampled components (use tc_encode_j2k)");
     if (p->cblk_style)
         return fail(ctx, TC_E_UNSUPPORTED, "tc_encode_j2k_gpu: code-block style modes (use tc_encode_j2k)");
+    if (p->roi_x1 > p->roi_x0 || p->roi_y1 > p->roi_y0)
+        return fail(ctx, TC_E_UNSUPPORTED, "tc_encode_j2k_gpu: region of interest (use tc_encode_j2k)");
     const int W = p->width, H = p->height, C = p->ncomp, B = p->bits, NL = p->levels;
     const size_t np = (size_t)W * H;
     const int sb = B <= 8 ? 1 : 2;

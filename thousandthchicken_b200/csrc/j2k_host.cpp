@@ -886,12 +886,16 @@ struct Scope {
     std::vector<char> has_coc, has_qcc;
     std::vector<Coding> coc;
     std::vector<Quant> qcc;
+    std::vector<char> has_roi;  // RGN (ISO A.6.3): maxshift value per component
+    std::vector<int> roi;
     void init(int ncomp)
     {
         has_coc.assign(ncomp, 0);
         has_qcc.assign(ncomp, 0);
         coc.resize(ncomp);
         qcc.resize(ncomp);
+        has_roi.assign(ncomp, 0);
+        roi.assign(ncomp, 0);
     }
 };
 
@@ -932,6 +936,13 @@ const Quant &quant_of(const Params &P, const Scope *t, int c)
     if (t && t->has_qcd) return t->qcd;
     if (P.main.has_qcc[c]) return P.main.qcc[c];
     return P.main.qcd;
+}
+
+// ROI maxshift of component c: a tile's RGN, else the main header's, else 0.
+int roi_of(const Params &P, const Scope *t, int c)
+{
+    if (t && t->has_roi[c]) return t->roi[c];
+    return P.main.has_roi[c] ? P.main.roi[c] : 0;
 }
 
 // Progression, layers, SOP/EPH and the colour transform come from COD only.
@@ -1019,6 +1030,18 @@ static int read_coding_marker(Reader &rd, uint32_t m, size_t seg_end, int ncomp,
 
 // POC (ISO A.6.6): progression volumes appended to `poc`.  The reference
 // reads one progression order from COD (codestream.c:95-136).
+// RGN (ISO A.6.3): Crgn, Srgn (0: the maxshift method of Annex H), SPrgn.
+static int read_rgn(Reader &rd, size_t seg_end, int ncomp, Scope &S, std::string &err)
+{
+    const int c = ncomp < 257 ? (int)rd.u8() : (int)rd.u16();
+    const int style = (int)rd.u8(), shift = (int)rd.u8();
+    if (rd.bad || rd.pos > seg_end || c >= ncomp) { err = "bad RGN"; return TC_E_CODESTREAM; }
+    if (style != 0) { err = "RGN styles other than maxshift"; return TC_E_UNSUPPORTED; }
+    S.has_roi[c] = 1;
+    S.roi[c] = shift;
+    return TC_OK;
+}
+
 static int read_poc(Reader &rd, size_t seg_end, int ncomp, std::vector<PocEntry> &poc, std::string &err)
 {
     const bool wide = ncomp >= 257;
@@ -1152,8 +1175,14 @@ static int parse_main(Reader &rd, Params &P, std::string &err)
             P.ppm.emplace_back(z, std::vector<uint8_t>(rd.d + rd.pos, rd.d + seg_end));
             break;
         }
-        case M_RGN: case M_CRG:
-            err = "RGN/CRG markers are not supported";
+        case M_RGN: {
+            if (!P.have_siz) { err = "RGN before SIZ"; return TC_E_CODESTREAM; }
+            const int rc = read_rgn(rd, seg_end, P.ncomp, P.main, err);
+            if (rc) return rc;
+            break;
+        }
+        case M_CRG:
+            err = "CRG markers are not supported";
             return TC_E_UNSUPPORTED;
         default:
             break;  // COM, TLM, PLM and others carry nothing we need
@@ -1395,6 +1424,14 @@ static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Para
                 }
         }
         if ((rc = assign_quant(quant_of(P, &ts, c), P.bits, NL, geo[c], err))) return rc;
+        // ROI maxshift (ISO H.1): every band codes shift more bit-planes
+        if (const int sh = roi_of(P, &ts, c)) {
+            for (int r = 0; r <= NL; r++)
+                for (Band &b : geo[c][r].bands) {
+                    b.mb += sh;
+                    if (b.mb > 31) { err = "ROI shift leaves more than 31 bit-planes"; return TC_E_UNSUPPORTED; }
+                }
+        }
     }
 
     // The tile-part bodies are read one after the other as one packet
@@ -1638,6 +1675,7 @@ static int parse_tile(const uint8_t *cs, size_t len, const Params &P, const Para
                         d.step = reversible ? 1.0f : b.step;
                         d.flags = reversible ? 0 : TC_CBLK_IRREVERSIBLE;
                         d.style = (uint8_t)style[c];
+                        d.roi_shift = (uint8_t)roi_of(P, &ts, c);
                         em.first.push_back((uint32_t)em.segs.size());
                         if (cb.included && cb.passes > 0) {
                             if (cb.zbp > b.mb) { err = "zero bit-planes exceed Mb"; return TC_E_CODESTREAM; }
@@ -1731,8 +1769,8 @@ static int parse_raw_codestream(const uint8_t *cs, size_t len, Parsed &out, std:
                 const int z = (int)rd.u8();
                 ppt[isot].emplace_back(z, std::vector<uint8_t>(cs + rd.pos, cs + seg_end));
             } else if (mm == M_RGN) {
-                err = "RGN in a tile-part header is not supported";
-                return TC_E_UNSUPPORTED;
+                if (!first_part) { err = "RGN after a tile's first tile-part"; return TC_E_CODESTREAM; }
+                if ((rc = read_rgn(rd, seg_end, P.ncomp, tscope[isot], err))) return rc;
             }
             rd.pos = seg_end;
         }
@@ -1832,6 +1870,11 @@ int encode_layout(const tc_encode_params &p, EncodeLayout &L, std::string &err)
     if (p.cblk_style & ~0x3F) { err = "unknown code-block style bits"; return TC_E_ARG; }
     if (p.layers < 0 || p.layers > 64) { err = "layers out of range"; return TC_E_ARG; }
     if (p.packed_headers < 0 || p.packed_headers > 2) { err = "packed_headers out of range"; return TC_E_ARG; }
+    if ((p.roi_x1 > p.roi_x0 || p.roi_y1 > p.roi_y0) &&
+        (p.roi_x0 < 0 || p.roi_y0 < 0 || p.roi_x1 > W || p.roi_y1 > H || p.roi_x1 <= p.roi_x0 || p.roi_y1 <= p.roi_y0)) {
+        err = "ROI outside the image";
+        return TC_E_ARG;
+    }
     // Per component: code-block size (COC when it differs from COD), step
     // multiplier (QCC when it differs from QCD) and subsampling (SIZ).
     for (int c = 0; c < C; c++) {
@@ -1954,6 +1997,38 @@ int encode_codestream(const tc_encode_params &p, const void *planes, std::vector
                         q[i] = v;
                     }
 
+    // ROI maxshift (ISO Annex H): coefficients whose band cell (scaled by
+    // the band's level) meets the region are shifted up by s, so that every
+    // region bit lies above every background bit; the decoder needs no mask.
+    // s is one more than the bit count of the largest background magnitude:
+    // ISO asks 2^s above the background, and OpenJPEG's decoder compares its
+    // half-bit-scaled values with 2^s, so it needs 2^(s-1) above it.
+    std::vector<uint8_t> in_roi;
+    const bool roi = p.roi_x1 > p.roi_x0 && p.roi_y1 > p.roi_y0;
+    if (roi) {
+        in_roi.assign(ntot, 0);
+        for (int c = 0; c < C; c++) {
+            const int64_t rx0 = p.roi_x0 / L.dx[c], ry0 = p.roi_y0 / L.dy[c];
+            const int64_t rx1 = (p.roi_x1 + L.dx[c] - 1) / L.dx[c], ry1 = (p.roi_y1 + L.dy[c] - 1) / L.dy[c];
+            int bg = 0;
+            for (int r = 0; r <= NL; r++)
+                for (const Band &b : L.geo[c][r].bands)
+                    for (int y = 0; y < b.h; y++)
+                        for (int x = 0; x < b.w; x++) {
+                            const size_t i = L.coff[c] + (size_t)(b.y0 + y) * L.cw[c] + b.x0 + x;
+                            const bool in = ((int64_t)(x + 1) << b.level) > rx0 && ((int64_t)x << b.level) < rx1 &&
+                                            ((int64_t)(y + 1) << b.level) > ry0 && ((int64_t)y << b.level) < ry1;
+                            in_roi[i] = in;
+                            if (!in) bg = std::max(bg, 32 - __builtin_clz((uint32_t)std::abs(q[i]) | 1u) - (q[i] == 0));
+                        }
+            L.roi[c] = bg ? bg + 1 : 0;
+            const int sh = L.roi[c];
+            if (sh)
+                for (size_t i = L.coff[c]; i < L.coff[c + 1]; i++)
+                    if (in_roi[i]) q[i] = q[i] < 0 ? -(-q[i] << sh) : q[i] << sh;
+        }
+    }
+
     // Tier-1: every code-block with all passes; the codeword does not
     // depend on Mb, so the blocks are coded before the guard bits are known.
     std::vector<CodedBlock> coded(L.jobs.size());
@@ -1968,9 +2043,15 @@ int encode_codestream(const tc_encode_params &p, const void *planes, std::vector
         const int cx = jb.i << b.cbw_log2, cy = jb.j << b.cbh_log2;
         const int bw = std::min(1 << b.cbw_log2, b.w - cx), bh = std::min(1 << b.cbh_log2, b.h - cy);
         int32_t blk[64 * 64];
+        uint32_t plain = 0;  // largest magnitude before the ROI shift
         for (int y = 0; y < bh; y++)
-            for (int x = 0; x < bw; x++)
-                blk[y * bw + x] = q[L.coff[jb.c] + (size_t)(b.y0 + cy + y) * L.cw[jb.c] + b.x0 + cx + x];
+            for (int x = 0; x < bw; x++) {
+                const size_t i = L.coff[jb.c] + (size_t)(b.y0 + cy + y) * L.cw[jb.c] + b.x0 + cx + x;
+                blk[y * bw + x] = q[i];
+                const uint32_t a = (uint32_t)std::abs(q[i]);
+                plain = std::max(plain, roi && in_roi[i] ? a >> L.roi[jb.c] : a);
+            }
+        coded[k].numbps_plain = plain ? 32 - __builtin_clz(plain) : 0;
         int zbp = 0;
         if (t1_encode_block(blk, bw, bh, b.orient, 31, 0, words[k], &coded[k].passes, &zbp, style,
                             segmented ? &segs[k] : nullptr))
@@ -2002,7 +2083,7 @@ int encode_assemble(const tc_encode_params &p, EncodeLayout &L, const std::vecto
         for (int r = 0; r <= NL; r++) band_bps[c][r].assign(geo[c][r].bands.size(), 0);
     for (size_t k = 0; k < jobs.size(); k++) {
         int &m = band_bps[jobs[k].c][jobs[k].r][jobs[k].bi];
-        m = std::max(m, coded[k].numbps);
+        m = std::max(m, coded[k].numbps_plain >= 0 ? coded[k].numbps_plain : coded[k].numbps);
     }
     int need_guard = 1;
     for (int c = 0; c < C; c++)
@@ -2015,11 +2096,13 @@ int encode_assemble(const tc_encode_params &p, EncodeLayout &L, const std::vecto
         for (int r = 0; r <= NL; r++)
             for (Band &b : geo[c][r].bands) {
                 b.mb = G + b.eps - 1;
-                if (b.mb > 31) { err = "more than 31 magnitude bit-planes"; return TC_E_ARG; }
+                if (b.mb + L.roi[c] > 31) { err = "more than 31 magnitude bit-planes"; return TC_E_ARG; }
             }
     std::vector<int> zbps(jobs.size());
-    for (size_t k = 0; k < jobs.size(); k++)
-        zbps[k] = geo[jobs[k].c][jobs[k].r].bands[jobs[k].bi].mb - coded[k].numbps;
+    for (size_t k = 0; k < jobs.size(); k++) {
+        zbps[k] = geo[jobs[k].c][jobs[k].r].bands[jobs[k].bi].mb + L.roi[jobs[k].c] - coded[k].numbps;
+        if (zbps[k] < 0) { err = "a block codes more bit-planes than its band"; return TC_E_ARG; }
+    }
 
     // Index jobs by (c, r, bi) for the packet writer.
     std::vector<std::vector<std::vector<int>>> first(C, std::vector<std::vector<int>>(NL + 1));
@@ -2273,6 +2356,15 @@ int encode_assemble(const tc_encode_params &p, EncodeLayout &L, const std::vecto
                                      (uint8_t)(hdrs.size() >> 8), (uint8_t)hdrs.size()};
         ippm.insert(ippm.end(), hdrs.begin(), hdrs.end());
         put_packed(M_PPM, ippm);
+    }
+    // RGN: the maxshift value of each component with a region (ISO A.6.3)
+    for (int c = 0; c < C; c++) {
+        if (!L.roi[c]) continue;
+        wr.u16(M_RGN);
+        wr.u16(5);
+        wr.u8(c);                          // Crgn
+        wr.u8(0);                          // Srgn: maxshift
+        wr.u8(L.roi[c]);                   // SPrgn
     }
     const size_t sot = out.size();
     wr.u16(M_SOT);

@@ -77,6 +77,7 @@ struct EncodeLayout {
     int dx[4] = {1, 1, 1, 1}, dy[4] = {1, 1, 1, 1};  // component subsampling (XRsiz, YRsiz)
     int cw[4] = {0, 0, 0, 0}, ch[4] = {0, 0, 0, 0};  // component sizes ceil(W/dx) x ceil(H/dy)
     size_t coff[5] = {0, 0, 0, 0, 0};                // element offset of each component's plane
+    int roi[4] = {0, 0, 0, 0};                       // ROI maxshift per component (RGN; 0: none)
     std::vector<std::vector<Resolution>> geo;  // per component
     struct Job {
         int c, r, bi, i, j;  // component, resolution, band, block column, block row
@@ -93,6 +94,8 @@ struct CodedBlock {
     // (BYPASS / TERMALL); none: one segment of len bytes.
     const std::pair<uint32_t, int> *seg = nullptr;
     int nseg = 0;
+    // Bit-planes of the block's magnitudes before an ROI shift (-1: numbps).
+    int numbps_plain = -1;
 };
 int encode_layout(const tc_encode_params &p, EncodeLayout &L, std::string &err);
 // Guard bits from the blocks' bit-planes (unless p.guard_bits is set), Mb

@@ -485,8 +485,12 @@ __device__ __forceinline__ void process_block(WarpState<MagT> &S, const Tables &
                                             &last_plane, gl, gmask, gshift, style, lens);
     __syncwarp(gmask);
 
-    // epilogue: reconstruction + inverse quantisation, coalesced rows
+    // epilogue: reconstruction + inverse quantisation, coalesced rows; an
+    // ROI magnitude (>= 2^roi) is shifted down by roi (ISO H.1), and so is
+    // its count of undecoded planes
     const bool irrev = (d.flags & TC_CBLK_IRREVERSIBLE) != 0;
+    const int roi = d.roi_shift < d.mb ? d.roi_shift : 0;
+    const int mb_out = d.mb - roi;  // magnitude bits after the ROI shift
     for (int y = 0; y < h; y++) {
         char *row = out + 4 * (d.out_off + (uint64_t)y * d.out_pitch);
         const int s = y >> 2, k = y & 3;
@@ -499,9 +503,13 @@ __device__ __forceinline__ void process_block(WarpState<MagT> &S, const Tables &
                 neg = (uint32_t)(S.sgn[x + 1] >> y) & 1u;
                 u = (uint32_t)last_plane;
                 if (type == 1 && !(f & pi_bit(k))) u++;
+                if (roi && (mg >> roi)) {
+                    mg >>= roi;
+                    u = u > (uint32_t)roi ? u - roi : 0u;
+                }
             }
             if (out_mode == TC_T1_OUT_RAW) {
-                reinterpret_cast<uint32_t *>(row)[x] = sg ? ((mg << (31 - d.mb)) | (neg << 31)) : 0u;
+                reinterpret_cast<uint32_t *>(row)[x] = sg ? ((mg << (31 - mb_out)) | (neg << 31)) : 0u;
             } else if (irrev) {
                 float v = 0.0f;
                 if (sg) v = ((float)mg + recon_r * (float)(1u << u)) * d.step;
@@ -591,10 +599,13 @@ __global__ void dequant_raw_kernel(const tc_cblk_desc *__restrict__ desc, int n,
         return;
     }
     const int numbps = (int)d.mb - (int)d.zero_bitplanes;
-    // Decoded planes from the pass count: the last pass ran on plane p_last.
+    const int roi = d.roi_shift < d.mb ? d.roi_shift : 0;
+    const int mb = d.mb - roi;  // magnitude bits of the raw words
+    // Decoded planes from the pass count: the last pass ran on plane p_last
+    // (counted in the ROI-shifted domain for an ROI block).
     int u = 0;
     if (numbps > 0 && d.passes > 0) {
-        const int p_last = numbps - 1 - (d.passes + 1) / 3;
+        const int p_last = numbps - 1 - (d.passes + 1) / 3 - roi;
         u = p_last < 0 ? 0 : p_last;
     }
     const bool irrev = (d.flags & TC_CBLK_IRREVERSIBLE) != 0;
@@ -604,7 +615,7 @@ __global__ void dequant_raw_kernel(const tc_cblk_desc *__restrict__ desc, int n,
     // load and store when the block's rows are aligned): whole rows, no
     // index division
     auto one = [&](uint32_t r) -> uint32_t {
-        const uint32_t mg = (r & 0x7FFFFFFFu) >> (31 - d.mb);
+        const uint32_t mg = (r & 0x7FFFFFFFu) >> (31 - mb);
         const bool neg = (r >> 31) != 0;
         if (irrev) {
             const float v = mg ? ((float)mg + fr) * d.step : 0.0f;
