@@ -737,3 +737,16 @@ def test_roi_maxshift_through_oracle(bits, comps, roi, kw):
     else:
         err = out.astype(np.int64) - img
         assert np.abs(err).max() <= 4 and 10 * np.log10(255 ** 2 / np.mean(err ** 2)) > 45
+
+
+def test_crg_marker_is_read_past():
+    """A CRG marker segment (component registration, ISO A.9.1: a display
+    offset per component) changes no decoded sample."""
+    from gpu_helpers import oracle_decode_tiled
+    img = synth_image(64, 48, 3, 8, seed=2)
+    cs = codec.encode(img, 8, levels=2, reversible=True)
+    i = cs.find(b"\xff\x90")  # before SOT
+    crg = b"\xff\x63" + (2 + 4 * 3).to_bytes(2, "big") + b"".join(
+        (0).to_bytes(2, "big") + (32768).to_bytes(2, "big") for _ in range(3))
+    _, out = oracle_decode_tiled(cs[:i] + crg + cs[i:])
+    np.testing.assert_array_equal(out, img)

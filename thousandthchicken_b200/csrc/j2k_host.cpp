@@ -1181,11 +1181,8 @@ static int parse_main(Reader &rd, Params &P, std::string &err)
             if (rc) return rc;
             break;
         }
-        case M_CRG:
-            err = "CRG markers are not supported";
-            return TC_E_UNSUPPORTED;
         default:
-            break;  // COM, TLM, PLM and others carry nothing we need
+            break;  // COM, TLM, PLM, CRG (display registration) and others change no sample
         }
         rd.pos = seg_end;
     }
