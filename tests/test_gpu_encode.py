@@ -19,7 +19,10 @@ torch = pytest.importorskip("torch")
     (1, 1, 1, 8, 0, {}),
     (45, 1, 3, 8, 2, {}),
     (200, 120, 3, 8, 4, dict(comp_cblk_log2=[0, 4, 5])),
-], ids=["rgb8", "rgb8-cb32", "g12", "1x1", "45x1", "coc"])
+    (200, 120, 3, 8, 4, dict(layers=4, progression=2)),
+    (160, 96, 3, 8, 3, dict(layers=3, packed_headers=1)),
+    (160, 96, 1, 12, 3, dict(layers=2, packed_headers=2, progression=4)),
+], ids=["rgb8", "rgb8-cb32", "g12", "1x1", "45x1", "coc", "layers-rpcl", "layers-ppt", "g12-ppm-cprl"])
 def test_lossless_gpu_encode_is_byte_identical(gpu_ctx, w, h, c, bits, levels, kw):
     img = synth_image(w, h, c, bits, seed=w + h)
     cpu = codec.encode(img, bits, levels=levels, reversible=True, mct=c == 3, **kw)

@@ -123,12 +123,15 @@ def _encode_params(planes, bits, levels, reversible, mct, cblk_log2, base_step, 
 
 def encode_gpu(ctx, planes: np.ndarray, bits: int, levels: int = 5, reversible: bool = True, mct: bool = True,
                cblk_log2: int = 6, base_step: float = 1.0 / 128, guard_bits: int = 0, progression: int = 0,
-               comp_cblk_log2=None, comp_step_scale=None) -> bytes:
+               comp_cblk_log2=None, comp_step_scale=None, layers: int = 1, packed_headers: int = 0) -> bytes:
     """The encoder on the GPU (tc_encode_j2k_gpu): colour transform, DWT,
     quantisation and Tier-1 as kernels on ctx's device, packets on the
-    host.  Same parameters as encode; lossless output is byte-identical."""
+    host.  Same parameters as encode (code-block style 0, no region of
+    interest); lossless output is byte-identical."""
     planes, p = _encode_params(planes, bits, levels, reversible, mct, cblk_log2, base_step, guard_bits, progression,
                                0, comp_cblk_log2, comp_step_scale)
+    p.layers = int(layers)
+    p.packed_headers = int(packed_headers)
     cap = planes.nbytes * 3 + 65536
     out = np.empty(cap, np.uint8)
     n = C.c_size_t(0)
