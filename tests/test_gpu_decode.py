@@ -506,3 +506,19 @@ def test_roi_maxshift_decode(gpu_ctx, bits, comps, roi, kw):
         _, want = oracle_decode_tiled(cs)
         d = np.abs(got.astype(np.int64) - want.astype(np.int64))
         assert d.max() <= 1 and (d > 0).mean() < 0.01
+
+
+def test_large_image_round_trip(gpu_ctx):
+    """A 16384 x 16384 x 3 lossless image (3.2 GB of coefficients, byte
+    offsets past 2^31, 196,608 code-blocks, 112k DWT tiles in the last
+    level): GPU encode, then GPU decode, gives back the original."""
+    rng = np.random.default_rng(16384)
+    n = 16384
+    y = (np.arange(n, dtype=np.int32) * 7)[:, None]
+    x = (np.arange(n, dtype=np.int32) * 3)[None, :]
+    base = ((x + y) & 255).astype(np.uint8)
+    img = np.stack([base, base[::-1], base[:, ::-1]])
+    img[:, ::97, ::89] = rng.integers(0, 256, img[:, ::97, ::89].shape, dtype=np.uint8)
+    cs = codec.encode_gpu(gpu_ctx, img, 8, levels=6, reversible=True, mct=True)
+    got = _decoder(gpu_ctx).decode(cs)
+    assert np.array_equal(got, img)
