@@ -197,19 +197,19 @@ static int run_reverse(tc_ctx *ctx, int wavelet, int rounding, const void *const
     return TC_OK;
 }
 
-void t1_class_order(const tc_cblk_desc *h_desc, int n, uint32_t *h_order, int counts[4])
+void t1_class_order(const tc_cblk_desc *h_desc, int n, uint32_t *h_order, int counts[6])
 {
     std::vector<uint32_t> all(n);
     tc_t1_sort_order(h_desc, n, all.data());
-    std::vector<uint32_t> cls[4];
+    std::vector<uint32_t> cls[6];
     for (uint32_t i : all) {
         const tc_cblk_desc &d = h_desc[i];
         const int nb = d.passes ? (int)d.mb - (int)d.zero_bitplanes : 0;
-        const int k = (d.style & kStyleDecodeBits) ? 3 : (nb <= 8 ? 0 : (nb <= 16 ? 1 : 2));
+        const int k = (nb <= 8 ? 0 : (nb <= 16 ? 1 : 2)) + ((d.style & kStyleDecodeBits) ? 3 : 0);
         cls[k].push_back(i);
     }
     int o = 0;
-    for (int k = 0; k < 4; k++) {
+    for (int k = 0; k < 6; k++) {
         counts[k] = (int)cls[k].size();
         for (uint32_t i : cls[k]) h_order[o++] = i;
     }
@@ -259,7 +259,7 @@ struct tc_plan {
     // (tc_decode_j2k): its host address and length
     const void *preloaded = nullptr;
     uint64_t preloaded_len = 0;
-    int class_counts[4] = {0, 0, 0, 0};  // Tier-1 blocks of <= 8, <= 16, <= 31 coded bit-planes, styled
+    int class_counts[6] = {0, 0, 0, 0, 0, 0};  // Tier-1 blocks of <= 8, <= 16, <= 31 coded bit-planes; styled ones alike
     bool profiling = false;
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
     // graph replay of execute (tc_plan_set_graph)
@@ -608,7 +608,7 @@ static int plan_run(tc_plan *P, void *const *d_out)
                                       static_cast<uint32_t *>(P->order.ptr), P->ncblk, P->class_counts[0],
                                       P->class_counts[1], P->class_counts[2],
                                       static_cast<uint8_t *>(P->pool.ptr), P->pool_len, P->coef.ptr,
-                                      TC_T1_OUT_DEQUANT, P->recon_r, P->class_counts[3]);
+                                      TC_T1_OUT_DEQUANT, P->recon_r, P->class_counts + 3);
     if (e != cudaSuccess) return cuda_status(ctx, e, "Tier-1 launch");
     if (P->profiling) cudaEventRecord(P->ev[1], ctx->stream);
     if (plan_batched(P)) {

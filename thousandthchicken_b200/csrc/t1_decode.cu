@@ -716,9 +716,12 @@ cudaError_t launch_t1_decode(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint
                              const uint8_t *d_pool, uint64_t pool_len, void *d_out, int out_mode, float recon_r,
                              int max_bitplanes)
 {
-    if (out_mode & TC_T1_STYLED)
+    if (out_mode & TC_T1_STYLED) {
+        const int s[3] = {max_bitplanes <= 8 ? n : 0, max_bitplanes > 8 && max_bitplanes <= 16 ? n : 0,
+                          max_bitplanes > 16 ? n : 0};
         return launch_t1_classes(ctx, d_desc, d_order, n, 0, 0, 0, d_pool, pool_len, d_out, out_mode & ~TC_T1_STYLED,
-                                 recon_r, n);
+                                 recon_r, s);
+    }
     return launch_t1_classes(ctx, d_desc, d_order, n, max_bitplanes <= 8 ? n : 0,
                              max_bitplanes > 8 && max_bitplanes <= 16 ? n : 0, max_bitplanes > 16 ? n : 0, d_pool,
                              pool_len, d_out, out_mode, recon_r);
@@ -730,19 +733,46 @@ cudaError_t launch_t1_decode(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint
 // class rides in the 8-bit launch (see HeavyQueue), and an 8-bit class at
 // most half the size of the 16-bit class is decoded by the 16-bit launch.
 // Otherwise the classes run as concurrent launches, the 32- and 16-bit ones
-// on side streams.  Styled blocks (nstyled, after the three classes) run in
-// a 32-bit Modes launch on the context's stream.
+// on side streams.  Styled blocks (after the three classes, in the same
+// three widths: nstyled[0..2]) run in Modes launches on the context's stream.
 cudaError_t launch_t1_classes(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint32_t *d_order, int ndesc,
                               int n8, int n16, int n32, const uint8_t *d_pool, uint64_t pool_len, void *d_out,
-                              int out_mode, float recon_r, int nstyled)
+                              int out_mode, float recon_r, const int *nstyled)
 {
-    if (n8 + n16 + n32 + nstyled == 0) return cudaSuccess;
-    cudaError_t e = cudaMemsetAsync(ctx->d_words + 1, 0, 4 * sizeof(uint32_t), ctx->stream);
+    const int ns8 = nstyled ? nstyled[0] : 0, ns16 = nstyled ? nstyled[1] : 0, ns32 = nstyled ? nstyled[2] : 0;
+    if (n8 + n16 + n32 + ns8 + ns16 + ns32 == 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(ctx->d_words + 1, 0, 6 * sizeof(uint32_t), ctx->stream);
     if (e != cudaSuccess) return e;
-    if (nstyled > 0) {
+    if (ns8 + ns16 + ns32 > 0) {
+        // the widths run concurrently (the wider ones on side streams), so
+        // a few deep blocks start with the bulk instead of after it
         const uint32_t *os = d_order ? d_order + n8 + n16 + n32 : nullptr;
-        e = launch_class<uint32_t, 32, true>(ctx, ctx->stream, d_desc, os, nstyled, ndesc, d_pool, pool_len, d_out,
-                                             out_mode, recon_r, 4);
+        const int nl = (ns8 > 0) + (ns16 > 0) + (ns32 > 0);
+        cudaStream_t w8 = ctx->stream, w16 = ctx->stream, w32 = ctx->stream;
+        if (nl > 1) {
+            if ((e = ensure_side_streams(ctx)) != cudaSuccess) return e;
+            if ((e = cudaEventRecord(ctx->ev_fork, ctx->stream)) != cudaSuccess) return e;
+            for (int i = 0; i < 2; i++)
+                if ((e = cudaStreamWaitEvent(ctx->side[i], ctx->ev_fork, 0)) != cudaSuccess) return e;
+            w32 = ctx->side[0];
+            w16 = ctx->side[1];
+        }
+        if (ns32 > 0)
+            e = launch_class<uint32_t, 32, true>(ctx, w32, d_desc, os ? os + ns8 + ns16 : nullptr, ns32, ndesc, d_pool,
+                                                 pool_len, d_out, out_mode, recon_r, 6);
+        if (e == cudaSuccess && ns16 > 0)
+            e = launch_class<uint16_t, 32, true>(ctx, w16, d_desc, os ? os + ns8 : nullptr, ns16, ndesc, d_pool,
+                                                 pool_len, d_out, out_mode, recon_r, 5);
+        if (e == cudaSuccess && ns8 > 0)
+            e = launch_class<uint8_t, 32, true>(ctx, w8, d_desc, os, ns8, ndesc, d_pool, pool_len, d_out, out_mode,
+                                                recon_r, 4);
+        if (nl > 1) {
+            for (int i = 0; i < 2; i++) {
+                cudaError_t e2 = cudaEventRecord(ctx->ev_join[i], ctx->side[i]);
+                if (e2 == cudaSuccess) e2 = cudaStreamWaitEvent(ctx->stream, ctx->ev_join[i], 0);
+                if (e == cudaSuccess) e = e2;
+            }
+        }
         if (e != cudaSuccess || n8 + n16 + n32 == 0) return e;
     }
     const uint32_t *o16 = d_order ? d_order + n8 : nullptr;

@@ -115,7 +115,7 @@ struct tc_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     std::string err;
-    uint32_t *d_words = nullptr;  // [0] error word, [1..4] Tier-1 work counters
+    uint32_t *d_words = nullptr;  // [0] error word, [1..6] Tier-1 work counters
     tc::DevBuf scratch;           // DWT intermediate levels
     tc::DevBuf tmp_pool, tmp_desc, tmp_order, tmp_coef, tmp_out;
     tc::PinBuf stage_pool, stage_desc, stage_order;  // pinned staging of tc_decode_j2k
@@ -160,15 +160,16 @@ int cuda_status(tc_ctx *ctx, cudaError_t e, const char *what);
 cudaError_t launch_t1_decode(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint32_t *d_order,
                              int n, const uint8_t *d_pool, uint64_t pool_len, void *d_out,
                              int out_mode, float recon_r, int max_bitplanes);
-// Up to three persistent launches over an order array partitioned into
-// blocks of at most 8, 16 and 31 coded bit-planes (n8 + n16 + n32 entries),
-// then nstyled blocks with a code-block style.
+// Persistent launches over an order array partitioned into blocks of at
+// most 8, 16 and 31 coded bit-planes (n8 + n16 + n32 entries), then blocks
+// with a code-block style in the same three widths (nstyled[0..2], or none).
 cudaError_t launch_t1_classes(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint32_t *d_order,
                               int ndesc, int n8, int n16, int n32, const uint8_t *d_pool,
-                              uint64_t pool_len, void *d_out, int out_mode, float recon_r, int nstyled = 0);
+                              uint64_t pool_len, void *d_out, int out_mode, float recon_r,
+                              const int *nstyled = nullptr);
 // Host: order longest-first within each class (<= 8, <= 16, <= 31 coded
-// bit-planes, then styled blocks); class sizes out.
-void t1_class_order(const tc_cblk_desc *h_desc, int n, uint32_t *h_order, int counts[4]);
+// bit-planes, then styled blocks of <= 8, <= 16, <= 31); class sizes out.
+void t1_class_order(const tc_cblk_desc *h_desc, int n, uint32_t *h_order, int counts[6]);
 cudaError_t launch_dequant_raw(tc_ctx *ctx, const tc_cblk_desc *d_desc, int n,
                                const uint32_t *d_raw, void *d_out, float recon_r);
 cudaError_t launch_t1_encode(tc_ctx *ctx, const tc_t1_enc_desc *d_desc, int n, const void *d_in, uint8_t *d_out,
