@@ -178,7 +178,9 @@ struct RawBits {
 // Modes: the code-block style `style` applies; lens, when not null, holds
 // the lengths of the codeword's terminated segments (BYPASS / TERMALL),
 // which follow one another from seg.
-template <typename MagT, int G, bool Modes = false>
+// Raw: the block has raw (bypass) passes (BYPASS and more than 10 passes);
+// without them the raw coder and its tests are compiled out.
+template <typename MagT, int G, bool Modes = false, bool Raw = false>
 __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *seg, int len, int w,
                             int h, int orient, int numbps, int passes, int *last_plane, int lane, unsigned gmask,
                             int gshift, int style = 0, const uint32_t *lens = nullptr)
@@ -205,9 +207,14 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
         if constexpr (Modes) {
             if (!lens || (t > 0 && !style_pass_terminates(style, t - 1))) return;
             if (t > 0) segoff += lens[segi++];
-            raw = style_pass_raw(style, t);
-            if (raw) rw.init(seg + segoff, (int)lens[segi]);
-            else mq.init(seg + segoff, (int)lens[segi]);
+            if constexpr (Raw) {
+                raw = style_pass_raw(style, t);
+                if (raw) {
+                    rw.init(seg + segoff, (int)lens[segi]);
+                    return;
+                }
+            }
+            mq.init(seg + segoff, (int)lens[segi]);
         }
     };
     // after a pass: the contexts start over (RESET)
@@ -223,13 +230,13 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
     };
     // one decision of a significance or refinement pass, and a sign
     auto decide = [&](int cx) -> uint32_t {
-        if constexpr (Modes) {
+        if constexpr (Raw) {
             if (raw) return rw.bit();
         }
         return mq.decode(ctx, tbl, cx);
     };
     auto sign = [&](uint32_t si) -> uint32_t {
-        if constexpr (Modes) {
+        if constexpr (Raw) {
             if (raw) return rw.bit();
         }
         return (uint32_t)mq.decode(ctx, tbl, si & 15) ^ (si >> 4);
@@ -480,9 +487,14 @@ __device__ __forceinline__ void process_block(WarpState<MagT> &S, const Tables &
     __syncwarp(gmask);
 
     int type = 0, last_plane = 0;
-    if (coded)
-        type = decode_block<MagT, G, Modes>(S, T, pool + cw_off, (int)d.seg_len, w, h, d.orient, numbps, d.passes,
-                                            &last_plane, gl, gmask, gshift, style, lens);
+    if (coded) {
+        if (Modes && (style & TC_CBLK_STYLE_BYPASS) && d.passes > 10)
+            type = decode_block<MagT, G, Modes, Modes>(S, T, pool + cw_off, (int)d.seg_len, w, h, d.orient, numbps,
+                                                       d.passes, &last_plane, gl, gmask, gshift, style, lens);
+        else
+            type = decode_block<MagT, G, Modes, false>(S, T, pool + cw_off, (int)d.seg_len, w, h, d.orient, numbps,
+                                                       d.passes, &last_plane, gl, gmask, gshift, style, lens);
+    }
     __syncwarp(gmask);
 
     // epilogue: reconstruction + inverse quantisation, coalesced rows; an
