@@ -571,7 +571,7 @@ t1_decode_kernel(const tc_cblk_desc *__restrict__ desc, const uint32_t *__restri
     const int slot = (threadIdx.x >> 5) * (32 / G) + gidx;
     WarpState<MagT> &S = states[slot];
 
-    if constexpr (std::is_same<MagT, uint8_t>::value && G == 32 && !Modes) {
+    if constexpr (std::is_same<MagT, uint8_t>::value && G == 32) {
         static_assert(sizeof(WarpState<uint16_t>) <= 2 * sizeof(WarpState<uint8_t>), "heavy state spans two slots");
         if ((int)blockIdx.x < heavy.ctas && slot < 2) {
             if (slot == 1) return;  // lends its state to warp 0
@@ -581,8 +581,8 @@ t1_decode_kernel(const tc_cblk_desc *__restrict__ desc, const uint32_t *__restri
                 if (wl == 0) idx = (int)atomicAdd(heavy.counter, 1u);
                 idx = __shfl_sync(0xffffffffu, idx, 0);
                 if (idx >= heavy.n) break;
-                process_block<uint16_t, 32>(HS, T, desc, heavy.order[idx], ndesc, pool, pool_len, out, out_mode,
-                                            recon_r, err, gl, gmask, gshift);
+                process_block<uint16_t, 32, Modes>(HS, T, desc, heavy.order[idx], ndesc, pool, pool_len, out,
+                                                   out_mode, recon_r, err, gl, gmask, gshift);
             }
         }
     }
@@ -751,7 +751,7 @@ cudaError_t launch_t1_classes(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uin
                               int n8, int n16, int n32, const uint8_t *d_pool, uint64_t pool_len, void *d_out,
                               int out_mode, float recon_r, const int *nstyled)
 {
-    const int ns8 = nstyled ? nstyled[0] : 0, ns16 = nstyled ? nstyled[1] : 0, ns32 = nstyled ? nstyled[2] : 0;
+    int ns8 = nstyled ? nstyled[0] : 0, ns16 = nstyled ? nstyled[1] : 0, ns32 = nstyled ? nstyled[2] : 0;
     if (n8 + n16 + n32 + ns8 + ns16 + ns32 == 0) return cudaSuccess;
     cudaError_t e = cudaMemsetAsync(ctx->d_words + 1, 0, 6 * sizeof(uint32_t), ctx->stream);
     if (e != cudaSuccess) return e;
@@ -759,6 +759,15 @@ cudaError_t launch_t1_classes(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uin
         // the widths run concurrently (the wider ones on side streams), so
         // a few deep blocks start with the bulk instead of after it
         const uint32_t *os = d_order ? d_order + n8 + n16 + n32 : nullptr;
+        // a short 16-bit class rides in the 8-bit launch, as for unstyled blocks
+        HeavyQueue sheavy;
+        if (ns8 > 0 && ns16 > 0 && ns16 <= kMaxHeavy && 8 * ns16 <= ns8 && os) {
+            sheavy.order = os + ns8;
+            sheavy.n = ns16;
+            sheavy.ctas = ns16;
+            sheavy.counter = ctx->d_words + 5;
+            ns16 = 0;
+        }
         const int nl = (ns8 > 0) + (ns16 > 0) + (ns32 > 0);
         cudaStream_t w8 = ctx->stream, w16 = ctx->stream, w32 = ctx->stream;
         if (nl > 1) {
@@ -777,7 +786,7 @@ cudaError_t launch_t1_classes(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uin
                                                  pool_len, d_out, out_mode, recon_r, 5);
         if (e == cudaSuccess && ns8 > 0)
             e = launch_class<uint8_t, 32, true>(ctx, w8, d_desc, os, ns8, ndesc, d_pool, pool_len, d_out, out_mode,
-                                                recon_r, 4);
+                                                recon_r, 4, sheavy);
         if (nl > 1) {
             for (int i = 0; i < 2; i++) {
                 cudaError_t e2 = cudaEventRecord(ctx->ev_join[i], ctx->side[i]);
