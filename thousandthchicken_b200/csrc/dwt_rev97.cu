@@ -41,7 +41,6 @@ constexpr int SEG = 32, SEGN = SEG + 2 * H;
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 __device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
 __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
-__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
 
 // In-place scaling-free reverse 9/7 lifting of an interleaved signal (v[0]
 // at an even position).  Samples at least H from both ends are exact.
