@@ -522,3 +522,22 @@ def test_large_image_round_trip(gpu_ctx):
     cs = codec.encode_gpu(gpu_ctx, img, 8, levels=6, reversible=True, mct=True)
     got = _decoder(gpu_ctx).decode(cs)
     assert np.array_equal(got, img)
+
+
+def test_styled_deep_blocks_ride_in_the_bulk_launch(gpu_ctx):
+    """A styled lossy image whose blocks mostly code 4 bit-planes, with a few
+    deep low-band blocks: those ride in the styled 8-bit launch with 16-bit
+    state (heavy queue); within 1 of the oracle."""
+    from gpu_helpers import oracle_decode_tiled
+    from thousandthchicken_b200.synth import gradient_noise_image
+    img = gradient_noise_image(1024, 1024, 3, 8, seed=1024)
+    cs = codec.encode(img, 8, levels=6, reversible=False, mct=True, base_step=1 / 128,
+                      cblk_style=codec.CBLK_STYLE_BYPASS | codec.CBLK_STYLE_TERMALL)
+    info, desc, _ = codec.parse(cs)
+    nb = np.where(desc["passes"] > 0, desc["mb"].astype(int) - desc["zero_bitplanes"].astype(int), 0)
+    deep = int(((nb > 8) & (nb <= 16)).sum())
+    assert 0 < deep and 8 * deep <= int((nb <= 8).sum()) and nb.max() <= 16
+    got = _decoder(gpu_ctx).decode(cs).astype(np.int64)
+    _, want = oracle_decode_tiled(cs)
+    d = np.abs(got - want.astype(np.int64))
+    assert d.max() <= 1 and (d > 0).mean() < 0.002
