@@ -192,7 +192,9 @@ int tc_dwt_reverse97(tc_ctx *ctx, const float *d_in, int in_pitch,
  * ceil(w/2) * ceil(h/2) exceeds that size (levels >= 2).  It calls no
  * cudaMalloc, cudaFree or allocating library routine.  Its first call on a
  * device looks up the array's address there (cudaGetSymbolAddress with that
- * device current); make that first call before any stream capture.  Calls
+ * device current, whatever the level count); make that first call before any
+ * stream capture.  The address is cached for the process: do not call this
+ * on a device after cudaDeviceReset on it.  Calls
  * share the array: calls whose work overlaps on the GPU race on it.  The
  * array keeps the last call's contents and nothing in it needs to start at
  * zero. */

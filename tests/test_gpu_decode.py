@@ -536,7 +536,9 @@ def test_styled_deep_blocks_ride_in_the_bulk_launch(gpu_ctx):
     info, desc, _ = codec.parse(cs)
     nb = np.where(desc["passes"] > 0, desc["mb"].astype(int) - desc["zero_bitplanes"].astype(int), 0)
     deep = int(((nb > 8) & (nb <= 16)).sum())
-    assert 0 < deep and 8 * deep <= int((nb <= 8).sum()) and nb.max() <= 16
+    # the heavy queue takes at most one deep block per SM (kMaxHeavy = 148 in
+    # t1_decode.cu); more would go to a separate 16-bit launch
+    assert 0 < deep <= 148 and 8 * deep <= int((nb <= 8).sum()) and nb.max() <= 16
     got = _decoder(gpu_ctx).decode(cs).astype(np.int64)
     _, want = oracle_decode_tiled(cs)
     d = np.abs(got - want.astype(np.int64))

@@ -55,6 +55,26 @@ def test_static_scratch_reverse97_matches_context_entry_point():
     ctx.close()
 
 
+def test_static_scratch_largest_plane_that_fits():
+    """8192 x 8192: the first-level low band is exactly the array's 4 Mi
+    samples, which the size check must accept; same result as the
+    context entry point (random Mallat coefficients, both on the GPU)."""
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from thousandthchicken_b200.stages import Context, DWTReverse97
+    ctx = Context(0)
+    n, levels = 8192, 3
+    g = torch.Generator(device="cuda").manual_seed(8192)
+    inp = torch.randn((n, n), generator=g, device="cuda") * 40
+    want = torch.empty_like(inp)
+    DWTReverse97(ctx).run(inp, want, n, n, levels)
+    got = torch.full_like(inp, float("nan"))
+    assert _call_static(inp, got, n, n, levels) == L.TC_OK
+    torch.cuda.synchronize()
+    assert float((got - want).abs().max()) <= TOL97
+    ctx.close()
+
+
 def test_static_scratch_rejects_planes_beyond_the_array():
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")

@@ -17,8 +17,11 @@
 //    Transforms whose first-level low band, ceil(w/2) * ceil(h/2), is larger
 //    are rejected with TC_E_ARG before any work is issued.
 //  * The first call on a device resolves the array's device address with
-//    cudaGetSymbolAddress (with that device current) and caches it.  Make
-//    that first call outside any stream capture.
+//    cudaGetSymbolAddress (with that device current) and caches it for the
+//    life of the process.  Make that first call outside any stream capture.
+//    The cached address does not survive cudaDeviceReset on that device
+//    (the module, and the array with it, may be reloaded elsewhere): do not
+//    call this entry point on a device after resetting it.
 //  * All calls share the one array.  Two calls whose work overlaps on the
 //    GPU (different streams, or different host threads) race on it; order
 //    them on one stream or serialise them.
@@ -68,15 +71,18 @@ extern "C" int tc_dwt_reverse97_static(const float *d_in, int in_pitch, float *d
     if (levels >= 2 && (size_t)ws[1] * (size_t)hs[1] > (size_t)TC_DWT97_STATIC_SCRATCH_ELEMS)
         return TC_E_ARG;  // the intermediate plane does not fit the static array
     cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
+    // The array's address is resolved on every device's first call, whatever
+    // the level count, so that a caller's first call does the lookup outside
+    // any capture even when it has nothing to transform.
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess) return TC_E_DEVICE;
+    float *scratch = nullptr;
+    if (static_scratch(device, &scratch) != cudaSuccess) return TC_E_DEVICE;
     if (levels == 0) {
         const cudaError_t e = cudaMemcpy2DAsync(d_out, (size_t)out_pitch * 4, d_in, (size_t)in_pitch * 4,
                                                 (size_t)w * 4, h, cudaMemcpyDeviceToDevice, stream);
         return e == cudaSuccess ? TC_OK : TC_E_DEVICE;
     }
-    int device = 0;
-    if (cudaGetDevice(&device) != cudaSuccess) return TC_E_DEVICE;
-    float *scratch = nullptr;
-    if (static_scratch(device, &scratch) != cudaSuccess) return TC_E_DEVICE;
 
     // A context on the stack: the launchers only read its device and
     // stream and count launches; it owns no memory.
