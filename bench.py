@@ -213,43 +213,98 @@ def max_over_ranks(x: float, dist, device) -> float:
     return float(t.item())
 
 
-def run_reference(args, rank):
-    """The reference's CPU implementation of the path (oracle port) on all
-    host cores, on a bounded sample of the workload."""
-    if rank != 0:
-        return
+def _oracle():
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as O
-    from thousandthchicken_b200 import codec
     O.build()
-    w, h = SAMPLE["width"], SAMPLE["height"]
-    img, cs = make_workload(w, h, WORKLOAD["seed"])
-    info, desc, pool = codec.parse(cs)
+    return O
+
+
+def run_reference(args, rank):
+    """The reference arm: the reference's CPU implementation of the path (the
+    oracle port of its algorithm) on all host cores, decoding the workload
+    image itself.  The image is generated and coded here by the oracle's own
+    encoder (byte-identical code-blocks to the harness encoder's, which a
+    CPU test checks), so this process never loads libtc_j2k.so.  A step is
+    one full decode: Tier-1 with dequantisation, reverse 9/7, inverse ICT and
+    DC shift.  When oracle/_ref holds the reference's own Tier-1 kernel
+    (compiled from its OpenCL C, D1/D2 fixed), it is also timed on the same
+    code-blocks."""
+    if rank != 0:
+        return
+    O = _oracle()
+    from thousandthchicken_b200.synth import gradient_noise_image   # numpy only
+    W, H, Cn = WORKLOAD["width"], WORKLOAD["height"], WORKLOAD["ncomp"]
     cores = os.cpu_count() or 1
-
-    def step():
-        return O.decode_tile(desc, pool, w, h, 3, 8, WORKLOAD["levels"], False, True, r=0.5, threads=cores)
-
+    img = gradient_noise_image(W, H, Cn, WORKLOAD["bits"], WORKLOAD["seed"])
+    t0 = time.perf_counter()
+    et = O.encode_tile(img, WORKLOAD["bits"], WORKLOAD["levels"], False, True, WORKLOAD["base_step"],
+                       cblk=WORKLOAD["cblk"], threads=cores)
+    log(f"[reference] oracle encode: {et.n} code-blocks in {time.perf_counter() - t0:.1f}s")
     for _ in range(args.warmup):
-        step()
+        out, _f = et.decode(r=0.5, threads=cores)
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        out = step()
+        out, _f = et.decode(r=0.5, threads=cores)
         times.append(time.perf_counter() - t0)
     total = sum(times)
-    mpx = w * h * args.steps / total / 1e6
-    psnr = _psnr(out, img)
-    sample = f"{w}x{h}x3 image of the same generator and coding parameters ({w * h / 4096 / 4096:.4f} of the workload)"
+    mpx = W * H * args.steps / total / 1e6
+    sample = f"the full {W}x{H}x{Cn} workload image, one oracle decode per step"
     line = {"impl": "reference", "metric": METRIC, "value": round(mpx, 3), "unit": "Mpixel/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * total / args.steps, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": {**WORKLOAD, "sample": sample},
+            "data": "synthetic", "config": workload_config(et.n),
             "cpu_baseline": {"value": round(mpx, 3), "unit": "Mpixel/s", "cores": cores, "kind": "port",
                              "sample": sample},
             "e2e": {"value": round(mpx, 3), "unit": "Mpixel/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "psnr_db": round(psnr, 2)}
+            "psnr_db": round(_psnr(out, img), 2),
+            "input": "coded by the oracle's encoder (ISO C.2/D.3 restatement), code-blocks byte-identical to the "
+                     "harness encoder's"}
+    rk = reference_kernel_tier1(et, cores)
+    if rk:
+        line["reference_kernel_tier1"] = rk
+    line["repo_libraries_mapped"] = repo_libraries_mapped()
     print(json.dumps(line), flush=True)
+
+
+def repo_libraries_mapped():
+    """Shared libraries of this repository mapped into this process."""
+    try:
+        maps = Path("/proc/self/maps").read_text()
+    except OSError:
+        return None
+    root = str(ROOT)
+    return sorted({ln.split()[-1][len(root) + 1:] for ln in maps.splitlines()
+                   if ln.split() and ln.split()[-1].startswith(root) and ".so" in ln.split()[-1]})
+
+
+def reference_kernel_tier1(et, cores):
+    """The reference's own Tier-1 kernel g_decode (coefficient_coder.cl,
+    compiled as host code with its D1/D2 state bugs fixed) on the workload's
+    code-blocks, one work-item per block over all cores: code-blocks/s of
+    one timed run after one warm-up.  None when oracle/_ref is not built."""
+    import ref as R
+    if not R.available():
+        return None
+    blocks = []
+    for i in range(et.n):
+        c = et.arr[i]
+        seg = et.pool[c.seg_off:c.seg_off + c.seg_len].tobytes() + b"\xff"   # D22: one byte read early
+        blocks.append((seg, c.w, c.h, c.orient, c.mb, c.mb - c.zero_bitplanes))
+    R.t1_decode(blocks, patched=True, threads=cores)
+    t0 = time.perf_counter()
+    _, skipped = R.t1_decode(blocks, patched=True, threads=cores)
+    dt = time.perf_counter() - t0
+    return {"cblk_per_s": round(len(blocks) / dt, 1), "ms": round(dt * 1e3, 1), "blocks": len(blocks),
+            "skipped_over_16KiB": int(skipped), "cores": cores,
+            "what": "reference g_decode (coefficient_coder.cl:778-819, D1/D2 fixed) on the workload's code-blocks"}
+
+
+def workload_config(ncblk):
+    """The config object both arms print: the workload and its code-block
+    count, nothing about how either arm times it."""
+    return {**WORKLOAD, "code_blocks": int(ncblk)}
 
 
 def _psnr(a, b):
@@ -258,22 +313,42 @@ def _psnr(a, b):
     return 99.0 if mse == 0 else 10 * np.log10(255.0 ** 2 / mse)
 
 
-def cpu_baseline(cores):
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import oracle as O
+def oracle_check(O, cs, got, img, cores):
+    """The GPU's decode of the workload image against the FP64 oracle: the
+    oracle decodes the same codestream's code-blocks (Tier-1, dequantisation,
+    9/7 in FP64, ISO inverse ICT, DC shift) on all host cores.  Returns
+    (parity, cpu_baseline): the GPU output's difference from the oracle's
+    rounded samples (max, share of samples differing, PSNR) and from its
+    unrounded FP64 samples clamped to the sample range (max and PSNR), the
+    PSNR of both against the original; and the oracle decode's own rate."""
     from thousandthchicken_b200 import codec
-    O.build()
-    w, h = SAMPLE["width"], SAMPLE["height"]
-    img, cs = make_workload(w, h, WORKLOAD["seed"])
+    W, H, Cn, bits = WORKLOAD["width"], WORKLOAD["height"], WORKLOAD["ncomp"], WORKLOAD["bits"]
     info, desc, pool = codec.parse(cs)
-    O.decode_tile(desc, pool, w, h, 3, 8, WORKLOAD["levels"], False, True, r=0.5, threads=cores)
+    arr = O.cblk_array(desc, W, H)
+    args = (arr, len(desc), pool, W, H, Cn, bits, WORKLOAD["levels"], False, True)
     t0 = time.perf_counter()
-    reps = 2
-    for _ in range(reps):
-        O.decode_tile(desc, pool, w, h, 3, 8, WORKLOAD["levels"], False, True, r=0.5, threads=cores)
-    dt = (time.perf_counter() - t0) / reps
-    return {"value": round(w * h / dt / 1e6, 3), "unit": "Mpixel/s", "cores": cores, "kind": "port",
-            "sample": f"{w}x{h}x3 image of the same generator and coding parameters, oracle full decode"}
+    O.decode_cblks(*args, r=0.5, threads=cores)
+    dt = time.perf_counter() - t0
+    want, f64 = O.decode_cblks(*args, r=0.5, threads=cores, f64=True)
+    mx = float((1 << bits) - 1)
+    g = got.astype(np.float64)
+    d = np.abs(g - want.astype(np.float64))
+    e = np.abs(g - np.clip(f64, 0.0, mx))
+
+    def psnr(err):
+        mse = float(np.mean(err * err))
+        return 99.0 if mse == 0 else round(10 * np.log10(mx * mx / mse), 2)
+    parity = {"max_abs": int(d.max()), "frac_differing": round(float((d > 0).mean()), 6),
+              "psnr_vs_oracle_db": psnr(d), "max_abs_vs_fp64": round(float(e.max()), 4),
+              "psnr_vs_fp64_db": psnr(e), "psnr_vs_original_db": psnr(g - img.astype(np.float64)),
+              "oracle_psnr_vs_original_db": psnr(want.astype(np.float64) - img.astype(np.float64)),
+              "ok": bool(d.max() <= 1),
+              "what": f"full {W}x{H}x{Cn} GPU decode vs the FP64 oracle decode of the same code-blocks "
+                      "(max_abs in LSB of the 8-bit output)"}
+    cpu = {"value": round(W * H / dt / 1e6, 3), "unit": "Mpixel/s", "cores": cores, "kind": "port",
+           "sample": f"the full {W}x{H}x{Cn} workload image, one oracle decode (Tier-1, dequantisation, FP64 9/7, "
+                     "inverse ICT, DC shift)"}
+    return parity, cpu
 
 
 def encode_section(ctx, img):
@@ -614,27 +689,43 @@ def run_ours(args, rank, world, local_rank):
         dw_bytes = dwt_bytes(W, H, Cn, WORKLOAD["levels"])
         t1_gbs = t1_bytes / (t1_avg / 1000.0) / 1e9
         dwt_gbs = dw_bytes / (dwt_avg / 1000.0) / 1e9
-        traffic = None
+        prof = {}
         tf = ROOT / "profiles" / "ncu_traffic.json"
         if tf.exists():
-            traffic = json.loads(tf.read_text()).get("t1_decode_kernel_bytes_per_launch")
+            prof = json.loads(tf.read_text())
+        traffic = prof.get("t1_decode_kernel_bytes_per_launch")
+        inst = prof.get("t1_decode_kernel_inst_per_launch")
+        if prof.get("inst_workload") != f"{W}x{H}x{Cn}":
+            inst = None   # counted on another size
+        # Tier-1 is bound by instruction issue: one warp instruction per
+        # cycle per SM sub-partition (148 SMs x 4) at the sampled SM clock
+        sm_mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 1965.0
+        issue_peak = 148 * 4 * sm_mhz * 1e6 / 1e9          # G warp instructions / s
+        issue_achieved = inst / (t1_avg / 1000.0) / 1e9 if inst else None
         srt = sorted(step_ms)
         line = {
             "metric": METRIC, "value": round(value, 2), "unit": "Mpixel/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
-            "config": {**WORKLOAD, "code_blocks": ncblk, "codestream_bytes": pool_bytes,
-                       "l2": "256 MiB flush between steps, outside the timed events",
+            "config": workload_config(ncblk),
+            "timing": {"codestream_bytes": pool_bytes, "l2": "256 MiB flush between steps, outside the timed events",
                        "parallelism": f"replicas x{world} (no collective)"},
             "latency_ms": {"p50": round(srt[len(srt) // 2], 3), "p99": round(srt[min(len(srt) - 1,
                                                                                     int(0.99 * len(srt)))], 3)},
             "stages_ms": {"tier1_dequant": round(t1_avg, 3), "dwt_colour": round(dwt_avg, 3)},
             "code_blocks_per_s": round(ncblk / (t1_avg / 1000.0), 1),
-            "roofline": {"bound": "hbm", "kernel": "t1_decode_kernel", "achieved": round(t1_gbs, 2),
-                         "peak": hbm, "unit": "GB/s", "frac": round(t1_gbs / hbm, 4), "traffic": traffic,
-                         "peak_kind": peak_kind,
-                         "note": "Tier-1 is issue/latency bound (serial MQ decoding); bytes = codestream + 4 B per "
-                                 "coefficient written"},
+            "roofline": {"bound": "issue", "kernel": "t1_decode_kernel",
+                         "achieved": round(issue_achieved, 1) if issue_achieved else None,
+                         "peak": round(issue_peak, 1), "unit": "G warp-instructions/s",
+                         "frac": round(issue_achieved / issue_peak, 4) if issue_achieved else None,
+                         "traffic": traffic, "inst_per_launch": inst,
+                         "hbm": {"achieved": round(t1_gbs, 2), "peak": hbm, "unit": "GB/s",
+                                 "frac": round(t1_gbs / hbm, 4), "peak_kind": peak_kind,
+                                 "bytes": "codestream + 4 B per coefficient written"},
+                         "note": "Tier-1 decodes the serial MQ chain of each code-block and is bound by instruction "
+                                 "issue, not by HBM: achieved = warp instructions per launch (ncu "
+                                 "smsp__inst_executed.sum of this workload, profiles/) / the live CUDA-event Tier-1 "
+                                 "time; peak = 148 SMs x 4 issue slots x the sampled SM clock"},
             "dwt_roofline": {"bound": "hbm", "kernel": "reverse 9/7 levels (idwt_rev_kernel, idwt97_ict_kernel)",
                              "achieved": round(dwt_gbs, 2), "peak": hbm, "unit": "GB/s",
                              "frac": round(dwt_gbs / hbm, 4), "bytes_per_step": dw_bytes, "peak_kind": peak_kind},
@@ -654,7 +745,7 @@ def run_ours(args, rank, world, local_rank):
             line["kernels"] = kernels
             line["encode"] = encode
         if world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(os.cpu_count() or 1)
+            line["parity"], line["cpu_baseline"] = oracle_check(_oracle(), cs, decoded, img, os.cpu_count() or 1)
         print(json.dumps(line), flush=True)
     plan.close()
     ctx.close()

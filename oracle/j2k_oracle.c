@@ -634,76 +634,118 @@ static void idwt97_1d(double *x, int n)
     for (int k = 1; k < n; k += 2) x[k] -= A97 * (x[pse(k - 1, n)] + x[pse(k + 1, n)]);
 }
 
-/* Generic level driver over a strided line: gather -> (de)interleave ->
- * 1-D transform -> scatter.  ELEM/FN choose the sample type and filter. */
-#define DEFINE_LEVEL(NAME, T, BODY_FWD)                                        \
-    static void NAME(T *x, int w, int h, int pitch, int fwd, int rnd)          \
-    {                                                                          \
-        const int nmax = w > h ? w : h;                                        \
-        T *line = malloc(sizeof(T) * nmax), *tmp = malloc(sizeof(T) * nmax);   \
+/* Generic level driver over strided lines: gather -> (de)interleave ->
+ * 1-D transform -> scatter.  The lines of a pass are independent, so a
+ * pass is split into chunks of lines over `threads` workers (the result
+ * does not depend on the split). */
+typedef struct {
+    void *x;
+    int w, h, pitch, fwd, rnd, vertical, elem;
+} or_lvl_job;
+
+enum { LINES_PER_CHUNK = 32 };
+
+#define LEVEL_LINES(T, BODY)                                                   \
+    do {                                                                       \
+        T *x = (T *)J->x;                                                      \
+        const int n = J->vertical ? J->h : J->w;                               \
+        const int lines = J->vertical ? J->w : J->h;                           \
+        const int nl = (n + 1) / 2, fwd = J->fwd, rnd = J->rnd;                \
+        T *line = malloc(sizeof(T) * n), *tmp = malloc(sizeof(T) * n);        \
         (void)rnd;                                                             \
-        for (int pass = 0; pass < 2; pass++) {                                 \
-            /* forward: columns then rows; reverse: rows then columns */       \
-            const int vertical = fwd ? (pass == 0) : (pass == 1);              \
-            const int n = vertical ? h : w, lines = vertical ? w : h;          \
-            const int nl = (n + 1) / 2;                                        \
-            for (int l = 0; l < lines; l++) {                                  \
-                T *base = vertical ? x + l : x + (size_t)l * pitch;            \
-                const size_t step = vertical ? (size_t)pitch : 1;              \
-                for (int i = 0; i < n; i++) line[i] = base[i * step];          \
-                if (fwd) {                                                     \
-                    BODY_FWD(line, n, 1);                                      \
-                    for (int i = 0; i < n; i++)                                \
-                        tmp[(i & 1) ? nl + i / 2 : i / 2] = line[i];           \
-                } else {                                                       \
-                    for (int i = 0; i < n; i++)                                \
-                        tmp[i] = line[(i & 1) ? nl + i / 2 : i / 2];           \
-                    BODY_FWD(tmp, n, 0);                                       \
-                }                                                              \
-                for (int i = 0; i < n; i++) base[i * step] = tmp[i];           \
+        for (int l = chunk * LINES_PER_CHUNK;                                  \
+             l < lines && l < (chunk + 1) * LINES_PER_CHUNK; l++) {            \
+            T *base = J->vertical ? x + l : x + (size_t)l * J->pitch;          \
+            const size_t step = J->vertical ? (size_t)J->pitch : 1;            \
+            for (int i = 0; i < n; i++) line[i] = base[i * step];              \
+            if (fwd) {                                                         \
+                BODY(line, n, 1);                                              \
+                for (int i = 0; i < n; i++)                                    \
+                    tmp[(i & 1) ? nl + i / 2 : i / 2] = line[i];               \
+            } else {                                                           \
+                for (int i = 0; i < n; i++)                                    \
+                    tmp[i] = line[(i & 1) ? nl + i / 2 : i / 2];               \
+                BODY(tmp, n, 0);                                               \
             }                                                                  \
+            for (int i = 0; i < n; i++) base[i * step] = tmp[i];               \
         }                                                                      \
         free(line);                                                            \
         free(tmp);                                                             \
-    }
+    } while (0)
 
 #define F53(v, n, fwd) do { if (fwd) fdwt53_1d(v, n, rnd); else idwt53_1d(v, n, rnd); } while (0)
 #define F97(v, n, fwd) do { if (fwd) fdwt97_1d(v, n); else idwt97_1d(v, n); } while (0)
-DEFINE_LEVEL(level53, int32_t, F53)
-DEFINE_LEVEL(level97, double, F97)
 
-void or_fdwt53(int32_t *x, int w, int h, int pitch, int levels, int rounding)
+static void or_lvl_chunk(void *arg, int chunk)
+{
+    const or_lvl_job *J = (const or_lvl_job *)arg;
+    if (J->elem == 4) LEVEL_LINES(int32_t, F53);
+    else LEVEL_LINES(double, F97);
+}
+
+/* One level: forward = columns then rows (ISO F.4, 2D_SD); reverse = rows
+ * then columns (ISO F.3, 2D_SR). */
+static void level_mt(void *x, int elem, int w, int h, int pitch, int fwd, int rnd, int threads)
+{
+    for (int pass = 0; pass < 2; pass++) {
+        or_lvl_job J = {x, w, h, pitch, fwd, rnd, fwd ? (pass == 0) : (pass == 1), elem};
+        const int lines = J.vertical ? w : h;
+        or_parallel_for((lines + LINES_PER_CHUNK - 1) / LINES_PER_CHUNK, threads, or_lvl_chunk, &J);
+    }
+}
+
+static void fdwt53_mt(int32_t *x, int w, int h, int pitch, int levels, int rounding, int threads)
 {
     for (int l = 0; l < levels; l++) {
-        level53(x, w, h, pitch, 1, rounding);
+        level_mt(x, 4, w, h, pitch, 1, rounding, threads);
         w = (w + 1) / 2;
         h = (h + 1) / 2;
     }
+}
+
+static void idwt53_mt(int32_t *x, int w, int h, int pitch, int levels, int rounding, int threads)
+{
+    int ws[33], hs[33];
+    ws[0] = w; hs[0] = h;
+    for (int l = 1; l <= levels; l++) { ws[l] = (ws[l - 1] + 1) / 2; hs[l] = (hs[l - 1] + 1) / 2; }
+    for (int l = levels - 1; l >= 0; l--) level_mt(x, 4, ws[l], hs[l], pitch, 0, rounding, threads);
+}
+
+static void fdwt97_mt(double *x, int w, int h, int pitch, int levels, int threads)
+{
+    for (int l = 0; l < levels; l++) {
+        level_mt(x, 8, w, h, pitch, 1, 0, threads);
+        w = (w + 1) / 2;
+        h = (h + 1) / 2;
+    }
+}
+
+static void idwt97_mt(double *x, int w, int h, int pitch, int levels, int threads)
+{
+    int ws[33], hs[33];
+    ws[0] = w; hs[0] = h;
+    for (int l = 1; l <= levels; l++) { ws[l] = (ws[l - 1] + 1) / 2; hs[l] = (hs[l - 1] + 1) / 2; }
+    for (int l = levels - 1; l >= 0; l--) level_mt(x, 8, ws[l], hs[l], pitch, 0, 0, threads);
+}
+
+void or_fdwt53(int32_t *x, int w, int h, int pitch, int levels, int rounding)
+{
+    fdwt53_mt(x, w, h, pitch, levels, rounding, 1);
 }
 
 void or_idwt53(int32_t *x, int w, int h, int pitch, int levels, int rounding)
 {
-    int ws[33], hs[33];
-    ws[0] = w; hs[0] = h;
-    for (int l = 1; l <= levels; l++) { ws[l] = (ws[l - 1] + 1) / 2; hs[l] = (hs[l - 1] + 1) / 2; }
-    for (int l = levels - 1; l >= 0; l--) level53(x, ws[l], hs[l], pitch, 0, rounding);
+    idwt53_mt(x, w, h, pitch, levels, rounding, 1);
 }
 
 void or_fdwt97(double *x, int w, int h, int pitch, int levels)
 {
-    for (int l = 0; l < levels; l++) {
-        level97(x, w, h, pitch, 1, 0);
-        w = (w + 1) / 2;
-        h = (h + 1) / 2;
-    }
+    fdwt97_mt(x, w, h, pitch, levels, 1);
 }
 
 void or_idwt97(double *x, int w, int h, int pitch, int levels)
 {
-    int ws[33], hs[33];
-    ws[0] = w; hs[0] = h;
-    for (int l = 1; l <= levels; l++) { ws[l] = (ws[l - 1] + 1) / 2; hs[l] = (hs[l - 1] + 1) / 2; }
-    for (int l = levels - 1; l >= 0; l--) level97(x, ws[l], hs[l], pitch, 0, 0);
+    idwt97_mt(x, w, h, pitch, levels, 1);
 }
 
 /* 1-D synthesis norm of a unit coefficient in the low (high = 0) or high
@@ -906,24 +948,18 @@ static void or_t1_one(void *arg, int i)
     }
 }
 
-typedef struct {
-    int32_t *ip;
-    double *fp;
-    int w, h, levels;
-} or_dwt_job;
-
-static void or_dwt_one(void *arg, int c)
-{
-    or_dwt_job *J = (or_dwt_job *)arg;
-    const size_t np = (size_t)J->w * J->h;
-    if (J->ip) or_idwt53(J->ip + c * np, J->w, J->h, J->w, J->levels, OR_ROUND_FLOOR);
-    else or_idwt97(J->fp + c * np, J->w, J->h, J->w, J->levels);
-}
-
 int or_decode_tile(const or_cblk *cb, int n, const uint8_t *pool,
                    int w, int h, int ncomp, int bits, int levels,
                    int reversible, int mct, float r, int threads,
                    uint16_t *out)
+{
+    return or_decode_tile_f64(cb, n, pool, w, h, ncomp, bits, levels, reversible, mct, r, threads, out, NULL);
+}
+
+int or_decode_tile_f64(const or_cblk *cb, int n, const uint8_t *pool,
+                       int w, int h, int ncomp, int bits, int levels,
+                       int reversible, int mct, float r, int threads,
+                       uint16_t *out, double *out_f64)
 {
     const size_t np = (size_t)w * h;
     int32_t *ip = NULL;
@@ -939,9 +975,9 @@ int or_decode_tile(const or_cblk *cb, int n, const uint8_t *pool,
         or_parallel_for(n, threads, or_t1_one, &J);
         if (J.err) { free(ip); free(fp); return -3; }
     }
-    {
-        or_dwt_job D = {ip, fp, w, h, levels};
-        or_parallel_for(ncomp, threads, or_dwt_one, &D);
+    for (int c = 0; c < ncomp; c++) {
+        if (ip) idwt53_mt(ip + c * np, w, h, w, levels, OR_ROUND_FLOOR, threads);
+        else idwt97_mt(fp + c * np, w, h, w, levels, threads);
     }
     if (reversible) {
         if (mct && ncomp >= 3) or_rct_inverse(ip, ip + np, ip + 2 * np, np, bits);
@@ -951,6 +987,20 @@ int or_decode_tile(const or_cblk *cb, int n, const uint8_t *pool,
     } else {
         int32_t *tmp = malloc(sizeof(int32_t) * np * ncomp);
         if (!tmp) { free(fp); return -2; }
+        if (out_f64) {
+            /* the unrounded samples: ISO G.2 inverse ICT, then the DC shift */
+            int32_t dc, lo, mx;
+            out_range(bits, &dc, &lo, &mx);
+            for (int c = 0; c < ncomp; c++)
+                for (size_t i = 0; i < np; i++) {
+                    double v = fp[c * np + i];
+                    if (mct && ncomp >= 3 && c < 3) {
+                        const double y = fp[i], cb_ = fp[np + i], cr = fp[2 * np + i];
+                        v = c == 0 ? y + 1.402 * cr : (c == 1 ? y - 0.34413 * cb_ - 0.71414 * cr : y + 1.772 * cb_);
+                    }
+                    out_f64[c * np + i] = v + dc;
+                }
+        }
         if (mct && ncomp >= 3) {
             or_ict_inverse(fp, fp + np, fp + 2 * np, tmp, tmp + np, tmp + 2 * np, np, bits);
             for (int c = 3; c < ncomp; c++) or_dc_inverse_float(fp + c * np, tmp + c * np, np, bits);
@@ -963,4 +1013,460 @@ int or_decode_tile(const or_cblk *cb, int n, const uint8_t *pool,
     free(ip);
     free(fp);
     return 0;
+}
+
+/* ===================== MQ encoder (ISO C.2) ============================== */
+/* The reference decodes only and has no encoder; this restates the
+ * normative encoder of ISO/IEC 15444-1 Annex C.2 (INITENC, CODEMPS,
+ * CODELPS, RENORME, BYTEOUT, FLUSH) so that the oracle can generate its own
+ * inputs.  The byte buffer keeps one byte in front of the codeword (the
+ * "B[BPST-1]" of C.2.8), which starts at zero. */
+
+typedef struct {
+    uint8_t *buf;        /* buf[0] precedes the codeword */
+    int cap, bp, ct, overflow;
+    uint32_t a, c;
+    uint8_t idx[NCX], mps[NCX];
+} mqenc;
+
+static void mqe_init(mqenc *e, uint8_t *buf, int cap)
+{
+    memset(e, 0, sizeof *e);
+    e->buf = buf;
+    e->cap = cap;
+    e->buf[0] = 0;
+    e->a = 0x8000;
+    e->ct = 12;
+    e->idx[0] = 4;          /* ISO Table D.7, as mq_reset */
+    e->idx[CX_RUN] = 3;
+    e->idx[CX_UNI] = 46;
+}
+
+static void mqe_put(mqenc *e, uint32_t v)
+{
+    e->bp++;
+    if (e->bp < e->cap) e->buf[e->bp] = (uint8_t)v;
+    else e->overflow = 1;
+}
+
+static uint32_t mqe_last(const mqenc *e) { return e->bp < e->cap ? e->buf[e->bp] : 0; }
+
+/* BYTEOUT with bit stuffing after 0xFF and carry propagation into the
+ * previous byte (ISO Figures C.8 and C.9). */
+static void mqe_byteout(mqenc *e)
+{
+    if (mqe_last(e) == 0xFF) {
+        mqe_put(e, e->c >> 20);
+        e->c &= 0xFFFFF;
+        e->ct = 7;
+        return;
+    }
+    if (e->c < 0x8000000) {
+        mqe_put(e, e->c >> 19);
+        e->c &= 0x7FFFF;
+        e->ct = 8;
+        return;
+    }
+    if (e->bp < e->cap) e->buf[e->bp]++;
+    if (mqe_last(e) == 0xFF) {
+        e->c &= 0x7FFFFFF;
+        mqe_put(e, e->c >> 20);
+        e->c &= 0xFFFFF;
+        e->ct = 7;
+    } else {
+        mqe_put(e, e->c >> 19);
+        e->c &= 0x7FFFF;
+        e->ct = 8;
+    }
+}
+
+static void mqe_renorm(mqenc *e)
+{
+    do {
+        e->a <<= 1;
+        e->c <<= 1;
+        if (--e->ct == 0) mqe_byteout(e);
+    } while ((e->a & 0x8000) == 0);
+}
+
+/* ENCODE (ISO Figure C.3): CODEMPS / CODELPS with conditional exchange. */
+static void mqe_encode(mqenc *e, int d, int cx)
+{
+    const int s = e->idx[cx];
+    const uint32_t qe = kQe[s];
+    e->a -= qe;
+    if (d == e->mps[cx]) {
+        if (e->a & 0x8000) {
+            e->c += qe;
+            return;
+        }
+        if (e->a < qe) e->a = qe;
+        else e->c += qe;
+        e->idx[cx] = kNMPS[s];
+    } else {
+        if (e->a < qe) e->c += qe;
+        else e->a = qe;
+        if (kSWITCH[s]) e->mps[cx] ^= 1;
+        e->idx[cx] = kNLPS[s];
+    }
+    mqe_renorm(e);
+}
+
+/* FLUSH with SETBITS (ISO Figures C.11-C.12); a final 0xFF is dropped.
+ * Returns the codeword length. */
+static int mqe_flush(mqenc *e)
+{
+    const uint32_t tempc = e->c + e->a;
+    e->c |= 0xFFFF;
+    if (e->c >= tempc) e->c -= 0x8000;
+    e->c <<= e->ct;
+    mqe_byteout(e);
+    e->c <<= e->ct;
+    mqe_byteout(e);
+    return mqe_last(e) == 0xFF ? e->bp - 1 : e->bp;
+}
+
+/* ===================== Tier-1 encoder (ISO D) ============================ */
+/* The mirror of the passes above: each decision the decoder reads is the
+ * bit the encoder writes with the same context, in the same scan order. */
+
+static void encode_sign(mqenc *e, const t1st *s, int x, int y, int neg)
+{
+    int hc, vc, cx, xr;
+#define CONTRIB(xx, yy) (AT(s, sig, xx, yy) ? (AT(s, sgn, xx, yy) ? -1 : 1) : 0)
+    hc = CONTRIB(x - 1, y) + CONTRIB(x + 1, y);
+    vc = CONTRIB(x, y - 1) + CONTRIB(x, y + 1);
+#undef CONTRIB
+    hc = hc > 1 ? 1 : (hc < -1 ? -1 : hc);
+    vc = vc > 1 ? 1 : (vc < -1 ? -1 : vc);
+    if (hc == 0) {
+        cx = vc == 0 ? 9 : 10;
+        xr = vc < 0;
+    } else {
+        cx = 12 + hc * vc;
+        xr = hc < 0;
+    }
+    mqe_encode(e, neg ^ xr, cx);
+}
+
+static void enc_significant(mqenc *e, t1st *s, const int32_t *coef, int x, int y)
+{
+    const int neg = coef[y * s->w + x] < 0;
+    encode_sign(e, s, x, y, neg);
+    AT(s, sgn, x, y) = (uint8_t)neg;
+    AT(s, sig, x, y) = 1;
+}
+
+static inline int mag_bit(const int32_t *coef, int w, int x, int y, int p)
+{
+    const int32_t v = coef[y * w + x];
+    return (int)(((uint32_t)(v < 0 ? -v : v) >> p) & 1u);
+}
+
+static void enc_spp(mqenc *e, t1st *s, const int32_t *coef, int orient, int p)
+{
+    for (int y0 = 0; y0 < s->h; y0 += 4)
+        for (int x = 0; x < s->w; x++)
+            for (int y = y0; y < y0 + 4 && y < s->h; y++) {
+                int hh, vv, dd, b;
+                if (AT(s, sig, x, y)) continue;
+                nb_counts(s, x, y, &hh, &vv, &dd);
+                if (hh + vv + dd == 0) continue;
+                AT(s, vis, x, y) = 1;
+                b = mag_bit(coef, s->w, x, y, p);
+                mqe_encode(e, b, zc_context(orient, hh, vv, dd));
+                if (b) enc_significant(e, s, coef, x, y);
+            }
+}
+
+static void enc_mrp(mqenc *e, t1st *s, const int32_t *coef, int p)
+{
+    for (int y0 = 0; y0 < s->h; y0 += 4)
+        for (int x = 0; x < s->w; x++)
+            for (int y = y0; y < y0 + 4 && y < s->h; y++) {
+                int hh, vv, dd;
+                if (!AT(s, sig, x, y) || AT(s, vis, x, y)) continue;
+                nb_counts(s, x, y, &hh, &vv, &dd);
+                mqe_encode(e, mag_bit(coef, s->w, x, y, p), AT(s, ref, x, y) ? 16 : (hh + vv + dd ? 15 : 14));
+                AT(s, ref, x, y) = 1;
+            }
+}
+
+static void enc_cup(mqenc *e, t1st *s, const int32_t *coef, int orient, int p)
+{
+    for (int y0 = 0; y0 < s->h; y0 += 4)
+        for (int x = 0; x < s->w; x++) {
+            int y = y0;
+            if (y0 + 4 <= s->h) {
+                int ok = 1;
+                for (int k = 0; k < 4 && ok; k++) {
+                    int hh, vv, dd;
+                    if (AT(s, sig, x, y0 + k) || AT(s, vis, x, y0 + k)) { ok = 0; break; }
+                    nb_counts(s, x, y0 + k, &hh, &vv, &dd);
+                    if (hh + vv + dd) ok = 0;
+                }
+                if (ok) {
+                    int r = 0;
+                    while (r < 4 && !mag_bit(coef, s->w, x, y0 + r, p)) r++;
+                    if (r == 4) {
+                        mqe_encode(e, 0, CX_RUN);
+                        continue;
+                    }
+                    mqe_encode(e, 1, CX_RUN);
+                    mqe_encode(e, r >> 1, CX_UNI);
+                    mqe_encode(e, r & 1, CX_UNI);
+                    enc_significant(e, s, coef, x, y0 + r);
+                    y = y0 + r + 1;
+                }
+            }
+            for (; y < y0 + 4 && y < s->h; y++) {
+                int hh, vv, dd, b;
+                if (AT(s, sig, x, y) || AT(s, vis, x, y)) continue;
+                nb_counts(s, x, y, &hh, &vv, &dd);
+                b = mag_bit(coef, s->w, x, y, p);
+                mqe_encode(e, b, zc_context(orient, hh, vv, dd));
+                if (b) enc_significant(e, s, coef, x, y);
+            }
+        }
+}
+
+int or_t1_encode(const int32_t *coef, int w, int h, int orient, int passes,
+                 uint8_t *out, int cap, int *len, int *passes_out, int *numbps_out)
+{
+    t1st st;
+    mqenc e;
+    uint32_t mx = 0;
+    int numbps = 0, total, pi = 0;
+    uint8_t *buf;
+    if (!coef || !out || !len || w < 1 || h < 1 || w > 64 || h > 64 || orient < 0 || orient > 3 || cap < 0)
+        return -1;
+    for (int i = 0; i < w * h; i++) {
+        const uint32_t a = (uint32_t)(coef[i] < 0 ? -coef[i] : coef[i]);
+        if (a > mx) mx = a;
+    }
+    while (numbps < 31 && (mx >> numbps)) numbps++;
+    if (mx >> numbps) return -1;   /* magnitude needs more than 31 bit-planes */
+    total = numbps ? 3 * numbps - 2 : 0;
+    if (passes <= 0 || passes > total) passes = total;
+    if (passes_out) *passes_out = passes;
+    if (numbps_out) *numbps_out = numbps;
+    *len = 0;
+    if (passes == 0) return 0;
+    if (t1_alloc(&st, w, h)) { t1_free(&st); return -2; }
+    st.vsc = 0;
+    buf = malloc((size_t)cap + 1);
+    if (!buf) { t1_free(&st); return -2; }
+    mqe_init(&e, buf, cap + 1);
+    for (int p = numbps - 1; p >= 0 && pi < passes; p--) {
+        if (p != numbps - 1) {
+            enc_spp(&e, &st, coef, orient, p);
+            if (++pi >= passes) break;
+            enc_mrp(&e, &st, coef, p);
+            if (++pi >= passes) break;
+        }
+        enc_cup(&e, &st, coef, orient, p);
+        ++pi;
+        memset(st.vis, 0, (size_t)st.W * (st.h + 2));
+    }
+    *len = mqe_flush(&e);
+    t1_free(&st);
+    if (e.overflow || *len > cap) { free(buf); return -3; }
+    memcpy(out, buf + 1, (size_t)*len);
+    free(buf);
+    return 0;
+}
+
+/* ===================== Whole-tile encode ================================= */
+/* The forward pipeline the bench workloads are coded with: DC level shift,
+ * forward RCT or ICT (preprocess_rct.cl:18-31, preprocess_ict.cl:20-37),
+ * multi-level forward 5/3 or 9/7 (dwt_f53.cl, dwt_f97.cl; ISO F.4),
+ * deadzone quantisation with the step of ISO E.1 derived from a base step
+ * scaled by the band's synthesis L2 norm and rounded to its (exponent,
+ * mantissa) code, and Tier-1 per code-block with every pass kept. */
+
+/* log2 of the nominal gain of a band: 0 LL, 1 HL/LH, 2 HH (ISO E.1.1.1). */
+static int band_gain(int orient) { return orient == 0 ? 0 : (orient == 3 ? 2 : 1); }
+
+/* The step a decoder derives from the (exponent, mantissa) pair that codes
+ * delta for a band with rb = bits + gain (ISO E.1, Equation E-3). */
+static double coded_step(double delta, int rb)
+{
+    int ex = rb - (int)floor(log2(delta));
+    int mu = (int)lround((delta / ldexp(1.0, rb - ex) - 1.0) * 2048.0);
+    if (mu >= 2048) { mu = 0; ex--; }
+    if (mu < 0) mu = 0;
+    return ldexp(1.0 + mu / 2048.0, rb - ex);
+}
+
+typedef struct {
+    int comp, orient, level, x0, y0, w, h;
+    double step;
+} or_band;
+
+typedef struct {
+    const or_band *band;
+    int bx, by;           /* block position inside the band */
+} or_blockjob;
+
+typedef struct {
+    const or_blockjob *jobs;
+    const int32_t *q;     /* quantised planes, ncomp * w * h */
+    int w, h, cblk;
+    uint8_t **words;
+    or_cblk *cb;
+    int err;
+} or_enc_job;
+
+static void or_enc_one(void *arg, int k)
+{
+    or_enc_job *J = (or_enc_job *)arg;
+    const or_blockjob *jb = &J->jobs[k];
+    const or_band *b = jb->band;
+    const int bw = (b->w - jb->bx) < J->cblk ? (b->w - jb->bx) : J->cblk;
+    const int bh = (b->h - jb->by) < J->cblk ? (b->h - jb->by) : J->cblk;
+    const int cap = 8 * bw * bh + 64;
+    int32_t blk[64 * 64];
+    int len = 0, passes = 0, numbps = 0;
+    const size_t plane = (size_t)J->w * J->h;
+    or_cblk *c = &J->cb[k];
+    for (int y = 0; y < bh; y++)
+        for (int x = 0; x < bw; x++)
+            blk[y * bw + x] = J->q[(size_t)b->comp * plane + (size_t)(b->y0 + jb->by + y) * J->w + b->x0 + jb->bx + x];
+    J->words[k] = malloc((size_t)cap);
+    if (!J->words[k] || or_t1_encode(blk, bw, bh, b->orient, 0, J->words[k], cap, &len, &passes, &numbps)) {
+        __atomic_store_n(&J->err, 1, __ATOMIC_RELAXED);
+        return;
+    }
+    memset(c, 0, sizeof *c);
+    c->seg_len = (uint32_t)len;
+    c->w = (uint16_t)bw;
+    c->h = (uint16_t)bh;
+    c->passes = (uint8_t)passes;
+    c->mb = 31;
+    c->zero_bitplanes = (uint8_t)(31 - numbps);
+    c->orient = (uint8_t)b->orient;
+    c->comp = (uint8_t)b->comp;
+    c->out_x = (uint32_t)(b->x0 + jb->bx);
+    c->out_y = (uint32_t)(b->y0 + jb->by);
+    c->step = (float)b->step;
+}
+
+int or_encode_tile(const uint16_t *samples, int w, int h, int ncomp, int bits,
+                   int levels, int reversible, int mct, double base_step, int cblk,
+                   int threads, or_cblk **cb_out, int *n_out, uint8_t **pool_out,
+                   size_t *pool_len_out)
+{
+    const size_t np = (size_t)w * h;
+    const int usemct = mct && ncomp >= 3;
+    const int32_t dc = 1 << (bits - 1);
+    int32_t *q = NULL;
+    double *fp = NULL;
+    or_band bands[4 * (3 * 32 + 1)];
+    int nb = 0, nj = 0, lw[34], lh[34];
+    or_blockjob *jobs = NULL;
+    or_cblk *cb = NULL;
+    uint8_t **words = NULL, *pool = NULL;
+    size_t total = 0;
+    int rc = 0;
+    if (!samples || !cb_out || !n_out || !pool_out || !pool_len_out || w < 1 || h < 1 || ncomp < 1 ||
+        ncomp > 4 || bits < 1 || bits > 16 || levels < 0 || levels > 32 || cblk < 4 || cblk > 64 ||
+        (cblk & (cblk - 1)) || (!reversible && !(base_step > 0.0)))
+        return -1;
+    q = malloc(sizeof(int32_t) * np * ncomp);
+    if (!q) return -2;
+    for (size_t i = 0; i < np * ncomp; i++) q[i] = (int32_t)samples[i] - dc;
+    if (reversible) {
+        if (usemct)
+            for (size_t i = 0; i < np; i++) {
+                const int32_t r = q[i], g = q[np + i], b = q[2 * np + i];
+                q[i] = (r + 2 * g + b) >> 2;   /* ISO G.2: floor */
+                q[np + i] = b - g;
+                q[2 * np + i] = r - g;
+            }
+        for (int c = 0; c < ncomp; c++) fdwt53_mt(q + c * np, w, h, w, levels, OR_ROUND_FLOOR, threads);
+    } else {
+        fp = malloc(sizeof(double) * np * ncomp);
+        if (!fp) { free(q); return -2; }
+        for (size_t i = 0; i < np * ncomp; i++) fp[i] = (double)q[i];
+        if (usemct)
+            for (size_t i = 0; i < np; i++) {
+                const double R = fp[i], G = fp[np + i], B = fp[2 * np + i];
+                fp[i] = 0.299 * R + 0.587 * G + 0.114 * B;
+                fp[np + i] = -0.16875 * R - 0.33126 * G + 0.5 * B;
+                fp[2 * np + i] = 0.5 * R - 0.41869 * G - 0.08131 * B;
+            }
+        for (int c = 0; c < ncomp; c++) fdwt97_mt(fp + c * np, w, h, w, levels, threads);
+    }
+    /* band geometry of the Mallat plane (ISO B.5, a tile at the origin) */
+    lw[0] = w; lh[0] = h;
+    for (int l = 1; l <= levels; l++) { lw[l] = (lw[l - 1] + 1) / 2; lh[l] = (lh[l - 1] + 1) / 2; }
+    for (int c = 0; c < ncomp; c++) {
+        bands[nb++] = (or_band){c, 0, levels, 0, 0, lw[levels], lh[levels], 1.0};
+        for (int l = levels; l >= 1; l--)
+            for (int o = 1; o <= 3; o++)
+                bands[nb++] = (or_band){c, o, l, (o & 1) ? lw[l] : 0, (o & 2) ? lh[l] : 0,
+                                        (o & 1) ? lw[l - 1] - lw[l] : lw[l], (o & 2) ? lh[l - 1] - lh[l] : lh[l],
+                                        1.0};
+    }
+    for (int k = 0; k < nb; k++) {
+        or_band *b = &bands[k];
+        if (!reversible)
+            b->step = coded_step(base_step * ldexp(1.0, bits) / or_subband_norm(1, b->level, b->orient),
+                                 bits + band_gain(b->orient));
+        if (b->w > 0 && b->h > 0) nj += ((b->w + cblk - 1) / cblk) * ((b->h + cblk - 1) / cblk);
+    }
+    /* deadzone quantisation (ISO E.1: q = sign(y) floor(|y| / step)) */
+    if (!reversible)
+        for (int k = 0; k < nb; k++) {
+            const or_band *b = &bands[k];
+            for (int y = b->y0; y < b->y0 + b->h; y++)
+                for (int x = b->x0; x < b->x0 + b->w; x++) {
+                    const size_t i = (size_t)b->comp * np + (size_t)y * w + x;
+                    const int32_t v = (int32_t)floor(fabs(fp[i]) / b->step);
+                    q[i] = fp[i] < 0 ? -v : v;
+                }
+        }
+    free(fp);
+    jobs = malloc(sizeof(or_blockjob) * (nj ? nj : 1));
+    cb = calloc(nj ? nj : 1, sizeof(or_cblk));
+    words = calloc(nj ? nj : 1, sizeof(uint8_t *));
+    if (!jobs || !cb || !words) { rc = -2; goto done; }
+    nj = 0;
+    for (int k = 0; k < nb; k++)
+        for (int by = 0; by < bands[k].h; by += cblk)
+            for (int bx = 0; bx < bands[k].w; bx += cblk) jobs[nj++] = (or_blockjob){&bands[k], bx, by};
+    {
+        or_enc_job J = {jobs, q, w, h, cblk, words, cb, 0};
+        or_parallel_for(nj, threads, or_enc_one, &J);
+        if (J.err) { rc = -3; goto done; }
+    }
+    /* segment pool: codewords one after the other, 16-byte aligned */
+    for (int k = 0; k < nj; k++) total += (cb[k].seg_len + 15u) & ~(size_t)15u;
+    pool = calloc(total ? total : 16, 1);
+    if (!pool) { rc = -2; goto done; }
+    total = 0;
+    for (int k = 0; k < nj; k++) {
+        cb[k].seg_off = total;
+        memcpy(pool + total, words[k], cb[k].seg_len);
+        total += (cb[k].seg_len + 15u) & ~(size_t)15u;
+    }
+    *cb_out = cb;
+    *n_out = nj;
+    *pool_out = pool;
+    *pool_len_out = total;
+    cb = NULL;
+done:
+    if (words)
+        for (int k = 0; k < nj; k++) free(words[k]);
+    free(words);
+    free(jobs);
+    free(cb);
+    free(q);
+    return rc;
+}
+
+void or_encoded_free(or_cblk *cb, uint8_t *pool)
+{
+    free(cb);
+    free(pool);
 }

@@ -157,6 +157,40 @@ int or_decode_tile(const or_cblk *cb, int n, const uint8_t *pool,
                    int reversible, int mct, float r, int threads,
                    uint16_t *out);
 
+/* ---- Encoding (the oracle's own inputs) ---------------------------------- */
+
+/* Encode one code-block of quantised coefficients (row-major, w x h) with
+ * the MQ coder of ISO C.2 and the passes of ISO D.3, keeping the first
+ * `passes` coding passes (<= 0 or more than available: all of them) and
+ * terminating the codeword there (FLUSH, ISO C.2.9).  Returns the codeword
+ * length in *len, the passes kept and the coded bit-planes.  0, or -1 for
+ * bad arguments, -2 out of memory, -3 a codeword longer than cap.  The
+ * reference decodes only; this is the standard's encoder. */
+int or_t1_encode(const int32_t *coef, int w, int h, int orient, int passes,
+                 uint8_t *out, int cap, int *len, int *passes_out, int *numbps_out);
+
+/* Encode a w x h tile at the origin from planar unsigned samples
+ * (ncomp * w * h): DC shift, forward RCT (reversible) or ICT (irreversible)
+ * on components 0-2 when mct, `levels` of forward 5/3 or 9/7 (FP64),
+ * deadzone quantisation with the step of each band derived from base_step *
+ * 2^bits / (its 9/7 synthesis L2 norm) and rounded to its ISO E.1 (exponent,
+ * mantissa) code, and cblk x cblk code-blocks with every pass kept.  Returns
+ * malloc'd code-block descriptors (mb = 31) and a 16-byte aligned segment
+ * pool; free both with or_encoded_free.  0, or a negative error. */
+int or_encode_tile(const uint16_t *samples, int w, int h, int ncomp, int bits,
+                   int levels, int reversible, int mct, double base_step, int cblk,
+                   int threads, or_cblk **cb_out, int *n_out, uint8_t **pool_out,
+                   size_t *pool_len_out);
+void or_encoded_free(or_cblk *cb, uint8_t *pool);
+
+/* or_decode_tile, also returning (when out_f64 is not NULL and the tile is
+ * irreversible) the FP64 samples after the inverse colour transform and the
+ * DC shift, before rounding and clamping (ncomp * w * h doubles). */
+int or_decode_tile_f64(const or_cblk *cb, int n, const uint8_t *pool,
+                       int w, int h, int ncomp, int bits, int levels,
+                       int reversible, int mct, float r, int threads,
+                       uint16_t *out, double *out_f64);
+
 #ifdef __cplusplus
 }
 #endif

@@ -60,6 +60,11 @@ def lib():
         L.or_dc_inverse_clamp.argtypes = [P, C.c_size_t, I]
         L.or_dc_inverse_float.argtypes = [P, P, C.c_size_t, I]
         L.or_decode_tile.argtypes = [P, I, P, I, I, I, I, I, I, I, C.c_float, I, P]
+        L.or_decode_tile_f64.argtypes = [P, I, P, I, I, I, I, I, I, I, C.c_float, I, P, P]
+        L.or_t1_encode.argtypes = [P, I, I, I, I, P, I, P, P, P]
+        L.or_encode_tile.argtypes = [P, I, I, I, I, I, I, I, C.c_double, I, I, P, P, P, P]
+        L.or_encoded_free.argtypes = [P, P]
+        L.or_encoded_free.restype = None
         _lib = L
     return _lib
 
@@ -186,6 +191,28 @@ def decode_tile(cblks, pool: np.ndarray, w, h, ncomp, bits, levels, reversible, 
     """Whole-tile decode from parsed code-block descriptors (numpy structured
     rows with the tc_cblk_desc fields of one image).  Returns uint16
     [ncomp, h, w], or int16 for signed samples (no DC level shift)."""
+    arr = cblk_array(cblks, w, h)
+    return decode_cblks(arr, len(cblks), pool, w, h, ncomp, bits, levels, reversible, mct, r, threads, signed)[0]
+
+
+def decode_cblks(arr, n, pool, w, h, ncomp, bits, levels, reversible, mct, r=0.5, threads=0, signed=False,
+                 f64=False):
+    """or_decode_tile(_f64) over an OrCblk array.  Returns (samples, FP64
+    samples before rounding or None): uint16 [ncomp, h, w] (int16 when
+    signed) and, with f64 on an irreversible tile, float64 [ncomp, h, w]."""
+    out = np.zeros((ncomp, h, w), np.uint16)
+    ff = np.zeros((ncomp, h, w), np.float64) if f64 and not reversible else None
+    pool = np.ascontiguousarray(pool, np.uint8)
+    rc = lib().or_decode_tile_f64(arr, n, _p(pool), w, h, ncomp, bits | (0x100 if signed else 0), levels,
+                                  int(reversible), int(mct), r, threads, _p(out),
+                                  _p(ff) if ff is not None else None)
+    if rc:
+        raise ValueError(f"or_decode_tile failed: {rc}")
+    return (out.view(np.int16) if signed else out), ff
+
+
+def cblk_array(cblks, w, h):
+    """OrCblk array from numpy rows with the tc_cblk_desc fields."""
     n = len(cblks)
     arr = (OrCblk * max(n, 1))()
     plane = w * h
@@ -206,10 +233,63 @@ def decode_tile(cblks, pool: np.ndarray, w, h, ncomp, bits, levels, reversible, 
             c.roi = int(d["roi_shift"])
         c.out_x, c.out_y = ox, oy
         c.step = float(d["step"])
-    out = np.zeros((ncomp, h, w), np.uint16)
-    pool = np.ascontiguousarray(pool, np.uint8)
-    rc = lib().or_decode_tile(arr, n, _p(pool), w, h, ncomp, bits | (0x100 if signed else 0), levels,
-                              int(reversible), int(mct), r, threads, _p(out))
+    return arr
+
+
+def t1_encode(coef, orient: int, passes: int = 0):
+    """Encode one code-block (ISO C.2 / D.3 encoder); returns (codeword
+    bytes, passes kept, coded bit-planes)."""
+    coef = np.ascontiguousarray(coef, np.int32)
+    h, w = coef.shape
+    cap = 16 * w * h + 1024
+    out = np.empty(cap, np.uint8)
+    n, np_, nb = C.c_int(0), C.c_int(0), C.c_int(0)
+    rc = lib().or_t1_encode(_p(coef), w, h, orient, passes, _p(out), cap, C.byref(n), C.byref(np_), C.byref(nb))
     if rc:
-        raise ValueError(f"or_decode_tile failed: {rc}")
-    return out.view(np.int16) if signed else out
+        raise ValueError(f"or_t1_encode failed: {rc}")
+    return out[:n.value].tobytes(), np_.value, nb.value
+
+
+class EncodedTile:
+    """The oracle's own encode of a tile: OrCblk descriptors and their pool."""
+
+    def __init__(self, arr, n, pool, w, h, ncomp, bits, levels, reversible, mct):
+        self.arr, self.n, self.pool = arr, n, pool
+        self.w, self.h, self.ncomp, self.bits = w, h, ncomp, bits
+        self.levels, self.reversible, self.mct = levels, reversible, mct
+
+    def decode(self, r=0.5, threads=0, f64=False):
+        return decode_cblks(self.arr, self.n, self.pool, self.w, self.h, self.ncomp, self.bits, self.levels,
+                            self.reversible, self.mct, r, threads, False, f64)
+
+    def blocks(self):
+        """{(comp, out_x, out_y): (codeword bytes, w, h, passes, numbps, orient, step)}"""
+        out = {}
+        for i in range(self.n):
+            c = self.arr[i]
+            seg = self.pool[c.seg_off:c.seg_off + c.seg_len].tobytes()
+            out[(c.comp, c.out_x, c.out_y)] = (seg, c.w, c.h, c.passes, c.mb - c.zero_bitplanes, c.orient, c.step)
+        return out
+
+
+def encode_tile(img, bits, levels, reversible, mct, base_step=1.0 / 128, cblk=64, threads=0) -> EncodedTile:
+    """or_encode_tile on planar unsigned samples [ncomp, h, w]."""
+    a = np.ascontiguousarray(img, np.uint16)
+    if a.ndim == 2:
+        a = a[None]
+    ncomp, h, w = a.shape
+    pc, n, pp, pl = C.c_void_p(), C.c_int(0), C.c_void_p(), C.c_size_t(0)
+    rc = lib().or_encode_tile(_p(a), w, h, ncomp, bits, levels, int(reversible), int(mct), base_step, cblk, threads,
+                              C.byref(pc), C.byref(n), C.byref(pp), C.byref(pl))
+    if rc:
+        raise ValueError(f"or_encode_tile failed: {rc}")
+    try:
+        arr = (OrCblk * max(n.value, 1))()
+        if n.value:
+            C.memmove(arr, pc, C.sizeof(OrCblk) * n.value)
+        pool = np.empty(max(pl.value, 16), np.uint8)
+        if pl.value:
+            C.memmove(pool.ctypes.data, pp, pl.value)
+    finally:
+        lib().or_encoded_free(pc, pp)
+    return EncodedTile(arr, n.value, pool, w, h, ncomp, bits, levels, reversible, mct)

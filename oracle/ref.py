@@ -5,6 +5,7 @@ present; the built libraries travel with the repository snapshot."""
 from __future__ import annotations
 
 import ctypes as C
+import os
 import subprocess
 from pathlib import Path
 
@@ -12,14 +13,15 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
-REF_TREE = Path("/root/reference/ThousandthChicken")
+# the reference project's source directory (TC_REFERENCE_TREE overrides)
+REF_TREE = Path(os.environ.get("TC_REFERENCE_TREE", "/root/reference/ThousandthChicken"))
 _libs: dict = {}
 
 
 def build() -> bool:
     """Build oracle/_ref from the reference sources if they are present."""
     if REF_TREE.exists():
-        subprocess.run(["make", "-s", "-C", str(HERE / "ref_shim")], check=True)
+        subprocess.run(["make", "-s", "-C", str(HERE / "ref_shim"), f"REF={REF_TREE}"], check=True)
     return available()
 
 
