@@ -381,6 +381,97 @@ def encode_section(ctx, img):
                     "codestream out"}
 
 
+def tier1_batched_section(ctx, stream, flush, cores):
+    """The batched Tier-1 workload: 200,000 code-blocks (60% 64x64, 30%
+    32x32, 10% edge blocks 1-64 wide and tall; Laplacian coefficients with
+    4-14 bit-planes and about 15% zeros), each truncated at a seeded pass
+    count, coded by the GPU Tier-1 encoder outside timing.  Decoded in one
+    persistent launch and with one launch per image (groups of 64-4096
+    blocks), each timed with CUDA events (median of 5, L2 flushed before
+    each).  Checked bit for bit against the truncated coefficients (the
+    oracle's ISO D.3 rule on the source coefficients, every block), against
+    the oracle's decode of 5,000 sampled codewords and against the
+    reference's own Tier-1 kernel on the sampled blocks that kept every
+    pass."""
+    import torch
+    from thousandthchicken_b200.blockbatch import BlockBatch
+    from thousandthchicken_b200.synth import c3_coefficients, c3_geometry
+    O = _oracle()
+    dev = torch.device("cuda", ctx.device)
+    t0 = time.perf_counter()
+    geom = c3_geometry(200_000, seed=3)
+    coef = c3_coefficients(geom, dev, seed=3)
+    bb = BlockBatch(ctx, geom, coef)
+    torch.cuda.synchronize()
+    prep_s = time.perf_counter() - t0
+
+    def timed(fn, reps=5):
+        ms = []
+        with torch.cuda.stream(stream):
+            fn()
+            for k in range(reps):
+                flush.fill_(k & 0xFF)
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                fn()
+                b.record(stream)
+                b.synchronize()
+                ms.append(a.elapsed_time(b))
+        return sorted(ms)[reps // 2]
+
+    per_ms = timed(bb.decode_per_image)
+    per_out = bb.out.cpu().numpy()
+    bat_ms = timed(bb.decode_batched)
+    ctx.synchronize()
+    got = bb.out.cpu().numpy()
+    d = bb.desc
+    want = O.t1_truncate_batch(coef.cpu().numpy(), geom["off"], geom["w"], geom["h"], d["passes"], threads=cores)
+    exact = bool(np.array_equal(got, want))
+    pool = bb.pool.cpu().numpy()
+    rng = np.random.default_rng(6)
+    sample = rng.choice(bb.n, 5000, replace=False)
+    oracle_ok, full = True, []
+    for i in sample:
+        w, h, off = int(d["w"][i]), int(d["h"][i]), int(geom["off"][i])
+        seg = pool[i * bb.cap: i * bb.cap + int(d["seg_len"][i])].tobytes()
+        nbp = int(d["mb"][i]) - int(d["zero_bitplanes"][i])
+        mine = got[off: off + w * h].reshape(h, w)
+        q, _ = O.t1_decode(seg, w, h, int(d["orient"][i]), nbp if d["passes"][i] else 0, int(d["passes"][i]))
+        oracle_ok &= bool(np.array_equal(mine, q))
+        if d["passes"][i] and d["passes"][i] == 3 * nbp - 2 and w >= 2:
+            full.append((i, seg + b"\xff", mine))   # the reference kernel reads one byte early (D22)
+    ref_check = None
+    import ref as R
+    if R.available() and full:
+        blocks = [(seg, int(d["w"][i]), int(d["h"][i]), int(d["orient"][i]), int(d["mb"][i]),
+                   int(d["mb"][i]) - int(d["zero_bitplanes"][i])) for i, seg, _ in full]
+        ref_raw, skipped = R.t1_decode(blocks, patched=True, threads=cores)
+        same = 0
+        for k, (i, _, mine) in enumerate(full):
+            h, w = mine.shape
+            mb = int(d["mb"][i])
+            raw = (np.abs(mine).astype(np.uint32) << np.uint32(31 - mb)) | \
+                  ((mine < 0).astype(np.uint32) << np.uint32(31))
+            same += bool(np.array_equal(ref_raw[k, :h, :w], raw))
+        ref_check = {"blocks": len(full), "identical": same, "skipped_over_16KiB": int(skipped)}
+    nbp = d["mb"].astype(int) - d["zero_bitplanes"].astype(int)
+    out = {"blocks": bb.n, "images": len(geom["images"]), "coefficients": geom["elems"],
+           "codeword_bytes": bb.codeword_bytes,
+           "truncated_share": round(float(((d["passes"] > 0) & (d["passes"] < 3 * nbp - 2)).mean()), 4),
+           "batched_ms": round(bat_ms, 3), "per_image_ms": round(per_ms, 3),
+           "cblk_per_s": round(bb.n / (bat_ms / 1000.0), 1), "per_image_cblk_per_s": round(bb.n / (per_ms / 1000.0), 1),
+           "speedup": round(per_ms / bat_ms, 3), "bit_exact": exact,
+           "per_image_identical": bool(np.array_equal(per_out, got)),
+           "oracle_sample": {"blocks": len(sample), "identical": oracle_ok},
+           "reference_kernel_untruncated": ref_check, "prepare_s": round(prep_s, 1),
+           "what": "200,000 uneven code-blocks truncated at seeded pass counts, one persistent Tier-1 launch vs one "
+                   "launch per image; bit_exact against the truncated source coefficients"}
+    bb.close()
+    del coef
+    torch.cuda.empty_cache()
+    return out
+
+
 def kernels_section(ctx, stream, flush, cs, hbm):
     """The stand-alone stage kernels on device-resident 4096x4096 data, each
     timed with CUDA events on the context's stream (median of 5 runs, L2
@@ -604,9 +695,10 @@ def run_ours(args, rank, world, local_rank):
     e2e_s = max_over_ranks((time.perf_counter() - t0) / n_pipe, dist, f"cuda:{local_rank}")
     same_out = bool(np.array_equal(host_out, host_out2))
 
-    batched, served, kernels, encode = None, None, None, None
+    batched, served, kernels, encode, tier1_batched = None, None, None, None, None
     if not args.core_only:
         kernels = kernels_section(ctx, stream, flush, cs, measured_peaks()[0])
+        tier1_batched = tier1_batched_section(ctx, stream, flush, os.cpu_count() or 1)
         encode = encode_section(ctx, img)
         # batched (one plan: one Tier-1 queue over every image) vs per-image plans
         mixed = make_mixed()
@@ -744,6 +836,7 @@ def run_ours(args, rank, world, local_rank):
             line["served"] = served
             line["kernels"] = kernels
             line["encode"] = encode
+            line["tier1_batched"] = tier1_batched
         if world == 1 and not args.no_cpu_baseline:
             line["parity"], line["cpu_baseline"] = oracle_check(_oracle(), cs, decoded, img, os.cpu_count() or 1)
         print(json.dumps(line), flush=True)

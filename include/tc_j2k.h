@@ -343,12 +343,24 @@ int tc_plan_image_info(const tc_plan *plan, int image, tc_image_info *info);
 /* Run the decode of every image in the plan; image i goes to d_out[i]
  * (device memory of tc_plan_output_bytes bytes).  Stream-ordered. */
 int tc_plan_execute(tc_plan *plan, void *const *d_out);
-/* Replay execute as a CUDA graph (on = 1): the first execute with a given
- * set of outputs runs normally and then captures the same work (Tier-1 class
- * launches with their fork/join, counter resets and every DWT level) into a
- * graph; later executes with the same outputs launch the graph.  Other
- * outputs, tc_plan_rebuild or profiling drop or bypass it. */
+/* Replay execute as CUDA graphs (on = 1), one per shape bucket.  In graph
+ * mode the kernels read everything that changes with the images and the
+ * outputs from plan buffers (descriptors, order, segment pool, and a DWT job
+ * table holding the output pointers, uploaded before the launch), so a graph
+ * is keyed by the launch shape: buffer addresses, Tier-1 class sizes and the
+ * list of DWT launches.  The first execute of a new bucket runs normally and
+ * captures the same work (Tier-1 class launches with their fork/join,
+ * counter resets and every DWT level); an execute with the same key, new
+ * outputs included, launches the graph; a batch rebuilt with the same launch
+ * topology (the same Tier-1 classes and DWT launch kinds) updates a cached
+ * graph's parameters (cudaGraphExecUpdate) instead of instantiating one.  Up
+ * to 8 graphs are kept per plan, least recently used dropped; profiling
+ * bypasses them, on = 0 drops them.  No counterpart in the reference. */
 int tc_plan_set_graph(tc_plan *plan, int on);
+/* Graph-mode counters of a plan: graphs captured and instantiated, graphs
+ * updated in place for a batch of the same topology, and replays of a
+ * cached graph. */
+int tc_plan_graph_stats(const tc_plan *plan, uint64_t *captures, uint64_t *updates, uint64_t *replays);
 /* Record CUDA events around the stages of every execute (on = 1): the
  * Tier-1 launch and the DWT/colour launches.  tc_plan_stage_ms waits for the
  * last execute and returns the device time of each stage in milliseconds.
@@ -421,12 +433,14 @@ typedef struct tc_t1_enc_desc {
     uint8_t  mb;         /* magnitude bit-planes Mb of the band (1..31) */
     uint8_t  flags;      /* TC_CBLK_IRREVERSIBLE: float input, quantised
                             floor(|x| / step); else int32 quantised input */
-    uint8_t  reserved;
+    uint8_t  max_passes; /* coding passes to keep, the codeword terminated
+                            after the last (0 or more than the block has:
+                            all of them) */
 } tc_t1_enc_desc;
 
 typedef struct tc_t1_enc_result {
     uint32_t len;            /* codeword bytes */
-    uint32_t passes;         /* coding passes (all of them) */
+    uint32_t passes;         /* coding passes kept */
     uint32_t zero_bitplanes; /* Mb - coded bit-planes */
     uint32_t status;         /* 0 ok, 1 bad descriptor, 2 magnitude above
                                 2^Mb, 3 codeword longer than cap */
@@ -442,10 +456,11 @@ typedef struct tc_t1_enc_result {
 int tc_encode_j2k_gpu(tc_ctx *ctx, const tc_encode_params *p, const void *h_planes,
                       uint8_t *h_out, size_t cap, size_t *out_len);
 
-/* Encode n code-blocks on the GPU, one warp each: block i's codeword (all
- * coding passes, MQ FLUSH termination) goes to d_out + i*cap, its result to
- * d_res[i].  Bit-exact with tc_t1_encode_block on the same quantised
- * coefficients.  Stream-ordered. */
+/* Encode n code-blocks on the GPU, one warp each: block i's codeword (its
+ * first max_passes coding passes, or all, MQ FLUSH termination) goes to
+ * d_out + i*cap, its result to d_res[i].  Bit-exact with
+ * tc_t1_encode_block on the same quantised coefficients and pass count.
+ * Stream-ordered. */
 int tc_t1_encode(tc_ctx *ctx, const tc_t1_enc_desc *d_desc, int n, const void *d_in,
                  uint8_t *d_out, uint32_t cap, tc_t1_enc_result *d_res);
 

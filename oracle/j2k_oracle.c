@@ -1470,3 +1470,93 @@ void or_encoded_free(or_cblk *cb, uint8_t *pool)
     free(cb);
     free(pool);
 }
+
+/* ===================== Truncated coefficients (ISO D.3, E.1.1.2) ========= */
+/* What a decoder reconstructs from the first `passes` coding passes of a
+ * block, computed from the coefficients themselves and the pass structure
+ * of ISO D.3, without any MQ coding: every coefficient is coded once per
+ * bit-plane, so after complete bit-planes it is known down to the last
+ * one.  In a bit-plane cut after its significance-propagation pass only the
+ * coefficients that pass visited (insignificant, with a significant
+ * neighbour at their turn in the scan, ISO D.3.1) carry that plane; cut
+ * after the refinement pass, the coefficients significant before the plane
+ * carry it too (ISO D.3.3).  The value keeps the known bits; the sign
+ * counts once the value is non-zero. */
+void or_t1_truncate(const int32_t *coef, int w, int h, int passes, int32_t *out)
+{
+    uint32_t mx = 0;
+    int nb = 0, total, t, plane, type;
+    for (int i = 0; i < w * h; i++) {
+        const uint32_t a = (uint32_t)(coef[i] < 0 ? -coef[i] : coef[i]);
+        if (a > mx) mx = a;
+    }
+    while (nb < 31 && (mx >> nb)) nb++;
+    total = nb ? 3 * nb - 2 : 0;
+    if (passes <= 0) {
+        for (int i = 0; i < w * h; i++) out[i] = 0;
+        return;
+    }
+    if (passes >= total) {
+        for (int i = 0; i < w * h; i++) out[i] = coef[i];
+        return;
+    }
+    t = passes - 1;                       /* the last pass kept */
+    plane = t == 0 ? nb - 1 : nb - 1 - (t + 2) / 3;
+    type = t == 0 ? 2 : (t - 1) % 3;      /* 0 SPP, 1 MRP, 2 cleanup */
+    {
+        /* low[i]: lowest plane known; 1 + plane unless the cut pass coded it */
+        uint8_t *low = malloc((size_t)w * h), *sig = calloc((size_t)(w + 2) * (h + 2), 1);
+        const int W = w + 2;
+#define SIG(x, y) sig[((y) + 1) * W + (x) + 1]
+        for (int i = 0; i < w * h; i++) low[i] = (uint8_t)(type == 2 ? plane : plane + 1);
+        if (type != 2) {
+            for (int y = 0; y < h; y++)
+                for (int x = 0; x < w; x++) {
+                    const int32_t v = coef[y * w + x];
+                    SIG(x, y) = (((uint32_t)(v < 0 ? -v : v)) >> (plane + 1)) != 0;
+                    if (type == 1 && SIG(x, y)) low[y * w + x] = (uint8_t)plane;
+                }
+            for (int y0 = 0; y0 < h; y0 += 4)
+                for (int x = 0; x < w; x++)
+                    for (int y = y0; y < y0 + 4 && y < h; y++) {
+                        int n;
+                        const int32_t v = coef[y * w + x];
+                        if (SIG(x, y)) continue;
+                        n = SIG(x - 1, y - 1) + SIG(x, y - 1) + SIG(x + 1, y - 1) + SIG(x - 1, y) + SIG(x + 1, y) +
+                            SIG(x - 1, y + 1) + SIG(x, y + 1) + SIG(x + 1, y + 1);
+                        if (!n) continue;
+                        low[y * w + x] = (uint8_t)plane;
+                        if ((((uint32_t)(v < 0 ? -v : v)) >> plane) & 1u) SIG(x, y) = 1;
+                    }
+        }
+#undef SIG
+        for (int i = 0; i < w * h; i++) {
+            const uint32_t a = (uint32_t)(coef[i] < 0 ? -coef[i] : coef[i]);
+            const int32_t k = (int32_t)((a >> low[i]) << low[i]);
+            out[i] = coef[i] < 0 ? -k : k;
+        }
+        free(low);
+        free(sig);
+    }
+}
+
+typedef struct {
+    const int32_t *coef;
+    const uint64_t *off;
+    const uint16_t *w, *h;
+    const uint8_t *passes;
+    int32_t *out;
+} or_trunc_job;
+
+static void or_trunc_one(void *arg, int i)
+{
+    const or_trunc_job *J = (const or_trunc_job *)arg;
+    or_t1_truncate(J->coef + J->off[i], J->w[i], J->h[i], J->passes[i], J->out + J->off[i]);
+}
+
+void or_t1_truncate_batch(const int32_t *coef, const uint64_t *off, const uint16_t *w, const uint16_t *h,
+                          const uint8_t *passes, int n, int threads, int32_t *out)
+{
+    or_trunc_job J = {coef, off, w, h, passes, out};
+    or_parallel_for(n, threads, or_trunc_one, &J);
+}

@@ -191,6 +191,17 @@ int or_decode_tile_f64(const or_cblk *cb, int n, const uint8_t *pool,
                        int reversible, int mct, float r, int threads,
                        uint16_t *out, double *out_f64);
 
+/* The coefficients a decoder reconstructs from the first `passes` coding
+ * passes of a block (row-major w x h, pitch w): derived from the
+ * coefficients and the pass membership rules of ISO D.3 alone, with no MQ
+ * coding, as the independent statement of "the truncated coefficients".
+ * passes <= 0 gives zeros; all passes give the coefficients. */
+void or_t1_truncate(const int32_t *coef, int w, int h, int passes, int32_t *out);
+/* The same over n blocks, block i at element offset off[i] (pitch w[i]) of
+ * coef and of out, on `threads` threads (<= 0: all cores). */
+void or_t1_truncate_batch(const int32_t *coef, const uint64_t *off, const uint16_t *w, const uint16_t *h,
+                          const uint8_t *passes, int n, int threads, int32_t *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -65,6 +65,10 @@ def lib():
         L.or_encode_tile.argtypes = [P, I, I, I, I, I, I, I, C.c_double, I, I, P, P, P, P]
         L.or_encoded_free.argtypes = [P, P]
         L.or_encoded_free.restype = None
+        L.or_t1_truncate.argtypes = [P, I, I, I, P]
+        L.or_t1_truncate.restype = None
+        L.or_t1_truncate_batch.argtypes = [P, P, P, P, P, I, I, P]
+        L.or_t1_truncate_batch.restype = None
         _lib = L
     return _lib
 
@@ -248,6 +252,29 @@ def t1_encode(coef, orient: int, passes: int = 0):
     if rc:
         raise ValueError(f"or_t1_encode failed: {rc}")
     return out[:n.value].tobytes(), np_.value, nb.value
+
+
+def t1_truncate(coef, passes: int):
+    """The coefficients a decoder reconstructs from the first `passes`
+    coding passes (ISO D.3 pass membership, no MQ coding)."""
+    coef = np.ascontiguousarray(coef, np.int32)
+    h, w = coef.shape
+    out = np.empty_like(coef)
+    lib().or_t1_truncate(_p(coef), w, h, passes, _p(out))
+    return out
+
+
+def t1_truncate_batch(coef, off, w, h, passes, threads=0):
+    """t1_truncate over blocks stored one after another in a flat int32
+    array (block i at element off[i], pitch w[i])."""
+    coef = np.ascontiguousarray(coef, np.int32)
+    off = np.ascontiguousarray(off, np.uint64)
+    w = np.ascontiguousarray(w, np.uint16)
+    h = np.ascontiguousarray(h, np.uint16)
+    passes = np.ascontiguousarray(passes, np.uint8)
+    out = np.empty_like(coef)
+    lib().or_t1_truncate_batch(_p(coef), _p(off), _p(w), _p(h), _p(passes), len(off), threads, _p(out))
+    return out
 
 
 class EncodedTile:

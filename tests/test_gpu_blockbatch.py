@@ -1,0 +1,75 @@
+"""Batched Tier-1 over 50,000 uneven code-blocks truncated at seeded pass
+counts (the shape of the 200,000-block workload): one persistent launch and
+one launch per image both give, bit for bit, the truncated coefficients
+(ISO D.3 pass membership applied to the source coefficients by the oracle),
+the oracle's decode of the codewords on a sample, and the reference's own
+Tier-1 kernel on the sampled blocks that kept every pass."""
+import numpy as np
+import pytest
+
+import oracle as O
+import ref as R
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module")
+def batch(gpu_ctx):
+    from thousandthchicken_b200.blockbatch import BlockBatch
+    from thousandthchicken_b200.synth import c3_coefficients, c3_geometry
+    geom = c3_geometry(50_000, seed=4)
+    coef = c3_coefficients(geom, torch.device("cuda", gpu_ctx.device), seed=4)
+    bb = BlockBatch(gpu_ctx, geom, coef)
+    yield bb, coef.cpu().numpy()
+    bb.close()
+
+
+def test_batched_launch_gives_the_truncated_coefficients(gpu_ctx, batch):
+    bb, coef = batch
+    d = bb.desc
+    nbp = d["mb"].astype(int) - d["zero_bitplanes"].astype(int)
+    truncated = (d["passes"] > 0) & (d["passes"] < 3 * nbp - 2)
+    assert truncated.mean() > 0.8 and bb.n == 50_000
+    bb.decode_batched()
+    gpu_ctx.synchronize()
+    got = bb.out.cpu().numpy()
+    g = bb.geom
+    want = O.t1_truncate_batch(coef, g["off"], g["w"], g["h"], d["passes"])
+    np.testing.assert_array_equal(got, want)
+    bb.out.fill_(-1)
+    bb.decode_per_image()
+    gpu_ctx.synchronize()
+    np.testing.assert_array_equal(bb.out.cpu().numpy(), got)
+
+
+def test_sampled_blocks_match_oracle_and_reference_kernel(gpu_ctx, batch):
+    bb, _ = batch
+    bb.decode_batched()
+    gpu_ctx.synchronize()
+    got = bb.out.cpu().numpy()
+    pool = bb.pool.cpu().numpy()
+    d, g = bb.desc, bb.geom
+    rng = np.random.default_rng(5)
+    full = []
+    for i in rng.choice(bb.n, 2000, replace=False):
+        w, h, off = int(d["w"][i]), int(d["h"][i]), int(g["off"][i])
+        seg = pool[i * bb.cap: i * bb.cap + int(d["seg_len"][i])].tobytes()
+        nbp = int(d["mb"][i]) - int(d["zero_bitplanes"][i])
+        mine = got[off: off + w * h].reshape(h, w)
+        q, _ = O.t1_decode(seg, w, h, int(d["orient"][i]), nbp if d["passes"][i] else 0, int(d["passes"][i]))
+        np.testing.assert_array_equal(mine, q, err_msg=f"block {i}")
+        if d["passes"][i] and d["passes"][i] == 3 * nbp - 2 and w >= 2:
+            full.append((i, seg + b"\xff", mine))   # the reference reads one byte early (D22)
+    if not R.available():
+        pytest.skip("oracle/_ref not built")
+    assert len(full) > 20
+    blocks = [(seg, int(d["w"][i]), int(d["h"][i]), int(d["orient"][i]), int(d["mb"][i]),
+               int(d["mb"][i]) - int(d["zero_bitplanes"][i])) for i, seg, _ in full]
+    ref_raw, skipped = R.t1_decode(blocks, patched=True)
+    assert skipped == 0
+    for k, (i, _, mine) in enumerate(full):
+        h, w = mine.shape
+        mb = int(d["mb"][i])
+        raw = (np.abs(mine).astype(np.uint32) << np.uint32(31 - mb)) | ((mine < 0).astype(np.uint32) << np.uint32(31))
+        np.testing.assert_array_equal(ref_raw[k, :h, :w], raw, err_msg=f"block {i}")

@@ -149,6 +149,63 @@ def test_batched_plan_equals_single_decodes(gpu_ctx):
         np.testing.assert_array_equal(got, single)
 
 
+def test_graphs_per_shape_bucket(gpu_ctx):
+    """Graph mode: new outputs replay the bucket's graph (the output
+    pointers sit in the DWT job table); a rebuild with the same images
+    replays it too; a batch of another shape captures or updates a graph;
+    a single-image plan takes the same path.  Every result equals the
+    plain decode."""
+    from thousandthchicken_b200.stages import Plan
+    a = [codec.encode(synth_image(300, 200, 3, 8, 5), 8, levels=5, reversible=True),
+         codec.encode(synth_image(200, 180, 3, 8, 6), 8, levels=4, reversible=False, base_step=1 / 64)]
+    b = [codec.encode(synth_image(160, 96, 1, 12, 7), 12, levels=3, reversible=True, mct=False),
+         codec.encode(synth_image(250, 130, 3, 8, 8), 8, levels=5, reversible=False, base_step=1 / 64)]
+    dec = _decoder(gpu_ctx)
+
+    def check(plan, streams, outs):
+        gpu_ctx.synchronize()
+        for s_, o in zip(streams, outs):
+            single = dec.decode(s_)
+            got = o.cpu().numpy()
+            if single.dtype == np.uint16:
+                got = got.view(np.uint16)
+            np.testing.assert_array_equal(got, single)
+
+    plan = Plan(gpu_ctx, a)
+    plan.set_graph(True)
+    o1, o2 = plan.alloc_outputs(), plan.alloc_outputs()
+    plan.execute(o1)
+    check(plan, a, o1)
+    assert plan.graph_stats()["captures"] == 1
+    for outs in (o2, o1, o2):   # other outputs: the same graph
+        for o in outs:
+            o.zero_()
+        plan.execute(outs)
+        check(plan, a, outs)
+    assert plan.graph_stats() == {"captures": 1, "updates": 0, "replays": 3}
+    plan.rebuild(a)             # same images, same buffers: replayed
+    plan.execute(o2)
+    check(plan, a, o2)
+    assert plan.graph_stats()["replays"] == 4
+    plan.rebuild(b)             # another shape
+    ob = plan.alloc_outputs()
+    plan.execute(ob)
+    check(plan, b, ob)
+    plan.execute(ob)
+    check(plan, b, ob)
+    st = plan.graph_stats()
+    assert st["captures"] + st["updates"] == 2 and st["replays"] == 5
+    plan.close()
+    single = Plan(gpu_ctx, a[1:])
+    single.set_graph(True)
+    for _ in range(2):
+        outs = single.alloc_outputs()
+        single.execute(outs)
+        check(single, a[1:], outs)
+    assert single.graph_stats() == {"captures": 1, "updates": 0, "replays": 1}
+    single.close()
+
+
 def test_decode_file_and_errors(gpu_ctx, tmp_path):
     from thousandthchicken_b200._lib import TCError
     img = synth_image(80, 60, 3, 8, seed=4)

@@ -42,7 +42,7 @@ def read_header(cs) -> dict:
 
 # tc_t1_enc_desc / tc_t1_enc_result (tc_j2k.h)
 ENC_DESC_DTYPE = np.dtype([("in_off", "<u8"), ("in_pitch", "<u4"), ("inv_step", "<f4"), ("w", "<u2"), ("h", "<u2"),
-                           ("orient", "u1"), ("mb", "u1"), ("flags", "u1"), ("reserved", "u1")])
+                           ("orient", "u1"), ("mb", "u1"), ("flags", "u1"), ("max_passes", "u1")])
 ENC_RESULT_DTYPE = np.dtype([("len", "<u4"), ("passes", "<u4"), ("zero_bitplanes", "<u4"), ("status", "<u4")])
 assert ENC_DESC_DTYPE.itemsize == 24 and ENC_RESULT_DTYPE.itemsize == 16
 

@@ -262,13 +262,27 @@ struct tc_plan {
     int class_counts[6] = {0, 0, 0, 0, 0, 0};  // Tier-1 blocks of <= 8, <= 16, <= 31 coded bit-planes; styled ones alike
     bool profiling = false;
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
-    // graph replay of execute (tc_plan_set_graph)
     PinBuf h_pool, h_desc, h_order;  // pinned host staging, alive until the next build
+    // Graph replay of execute (tc_plan_set_graph), one graph per shape
+    // bucket.  A graph's kernels read everything that varies with the
+    // images (descriptors, order, segment pool, DWT job table with the
+    // output pointers) from plan buffers, so it is keyed by its launch
+    // parameters: buffer addresses, Tier-1 class sizes and the DWT launch
+    // list.  Another batch of the same launch topology (same classes and
+    // DWT launch kinds) updates a cached graph's parameters in place
+    // (cudaGraphExecUpdate) instead of instantiating a new one.
+    struct Graph {
+        std::vector<uint64_t> key, topo;
+        cudaGraphExec_t exec = nullptr;
+        uint64_t launches = 0, last_use = 0;
+    };
     bool use_graph = false;
-    cudaGraphExec_t graph = nullptr;
-    std::vector<void *> graph_outs;  // outputs the graph was captured for
-    uint64_t graph_launches = 0;     // kernels per replay
+    std::vector<Graph> graphs;      // at most kMaxGraphs, least recently used dropped
+    uint64_t graph_tick = 0;
+    uint64_t graph_captures = 0, graph_updates = 0, graph_replays = 0;
 };
+
+static constexpr size_t kMaxGraphs = 8;
 
 // Plans of several images or of tiled images run the batched reverse DWT.
 static bool plan_batched(const tc_plan *P)
@@ -277,11 +291,11 @@ static bool plan_batched(const tc_plan *P)
            (P->imgs.size() == 1 && (P->imgs[0].tiles.size() > 1 || subsampled(P->imgs[0].info)));
 }
 
-static void plan_drop_graph(tc_plan *P)
+static void plan_drop_graphs(tc_plan *P)
 {
-    if (P->graph) cudaGraphExecDestroy(P->graph);
-    P->graph = nullptr;
-    P->graph_outs.clear();
+    for (tc_plan::Graph &g : P->graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    P->graphs.clear();
 }
 
 // Lays out and uploads a batch from parsed images: parsed[i] with its
@@ -405,7 +419,7 @@ static int plan_build(tc_ctx *ctx, const uint8_t *const *cs, const size_t *lens,
 // position, by wavelet, colour transform, component count, sample type and
 // bit depth.  The job table is built on the host and uploaded once per set
 // of output buffers (a replayed graph needs no copy).
-static int run_reverse_batched(tc_plan *P, void *const *d_out)
+static int run_reverse_batched(tc_plan *P, void *const *d_out, bool launch = true)
 {
     tc_ctx *ctx = P->ctx;
     const size_t nimg = P->imgs.size();
@@ -471,7 +485,7 @@ static int run_reverse_batched(tc_plan *P, void *const *d_out)
     // images without a transform: colour only
     for (const Unit &u : units) {
         const tc_image_info &inf = *u.inf;
-        if (inf.levels) continue;
+        if (inf.levels || !launch) continue;
         const int ob = sample_bytes(inf.bits);
         e = launch_color_inverse(ctx, u.color, u.ncomp, u.coef, inf.reversible ? TC_INT32 : TC_FLOAT32, u.w, u.out,
                                  ob == 1 ? TC_U8 : TC_U16, u.out_pitch, u.w, u.h, out_bits(inf));
@@ -591,6 +605,7 @@ static int run_reverse_batched(tc_plan *P, void *const *d_out)
         P->dwt_launches = launches;
         P->jobs_outs = outs;
     }
+    if (!launch) return TC_OK;
     const RevJob *dj = static_cast<const RevJob *>(P->jobs.ptr);
     for (const tc_plan::DwtLaunch &L : P->dwt_launches) {
         e = launch_idwt_batch(ctx, dj + L.first, L.njobs, L.ntiles, L.wavelet, TC_ROUND_FLOOR, L.color, L.ncomp,
@@ -600,18 +615,23 @@ static int run_reverse_batched(tc_plan *P, void *const *d_out)
     return TC_OK;
 }
 
-static int plan_run(tc_plan *P, void *const *d_out)
+// One execute's launches.  In graph mode every plan takes the batched
+// reverse DWT (its output pointers then sit in the job table, not in kernel
+// parameters) and Tier-1 bounds codewords by the pool buffer's capacity
+// rather than this batch's exact pool length, so that the launch parameters
+// depend on the batch's shape only.
+static int plan_run(tc_plan *P, void *const *d_out, bool graph_mode = false)
 {
     tc_ctx *ctx = P->ctx;
     if (P->profiling) cudaEventRecord(P->ev[0], ctx->stream);
     cudaError_t e = launch_t1_classes(ctx, static_cast<tc_cblk_desc *>(P->desc.ptr),
                                       static_cast<uint32_t *>(P->order.ptr), P->ncblk, P->class_counts[0],
                                       P->class_counts[1], P->class_counts[2],
-                                      static_cast<uint8_t *>(P->pool.ptr), P->pool_len, P->coef.ptr,
-                                      TC_T1_OUT_DEQUANT, P->recon_r, P->class_counts + 3);
+                                      static_cast<uint8_t *>(P->pool.ptr), graph_mode ? P->pool.size : P->pool_len,
+                                      P->coef.ptr, TC_T1_OUT_DEQUANT, P->recon_r, P->class_counts + 3);
     if (e != cudaSuccess) return cuda_status(ctx, e, "Tier-1 launch");
     if (P->profiling) cudaEventRecord(P->ev[1], ctx->stream);
-    if (plan_batched(P)) {
+    if (graph_mode || plan_batched(P)) {
         const int rc = run_reverse_batched(P, d_out);
         if (rc) return rc;
         if (P->profiling) cudaEventRecord(P->ev[2], ctx->stream);
@@ -1011,7 +1031,8 @@ int tc_plan_rebuild(tc_plan *P, const uint8_t *const *h_cs, const size_t *lens, 
     // wait for the previous execute before its buffers are overwritten
     cudaError_t e = cudaStreamSynchronize(P->ctx->stream);
     if (e != cudaSuccess) return cuda_status(P->ctx, e, "tc_plan_rebuild");
-    plan_drop_graph(P);
+    // cached graphs stay: they are keyed by their launch parameters, so a
+    // batch of the same shape replays or updates one
     return plan_build(P->ctx, h_cs, lens, nimages, P);
 }
 
@@ -1032,7 +1053,6 @@ int tc_plan_rebuild_parsed(tc_plan *P, const tc_j2k_parsed *const *parsed, int n
     }
     cudaError_t e = cudaStreamSynchronize(P->ctx->stream);
     if (e != cudaSuccess) return cuda_status(P->ctx, e, "tc_plan_rebuild_parsed");
-    plan_drop_graph(P);
     return plan_build_parsed(P->ctx, pp.data(), pools.data(), plens.data(), nimages, P);
 }
 
@@ -1056,7 +1076,7 @@ int tc_plan_destroy(tc_plan *P)
     if (P->jobs_uploaded) cudaEventDestroy(P->jobs_uploaded);
     for (auto &e : P->ev)
         if (e) cudaEventDestroy(e);
-    plan_drop_graph(P);
+    plan_drop_graphs(P);
     delete P;
     return TC_OK;
 }
@@ -1100,6 +1120,70 @@ int tc_plan_image_info(const tc_plan *P, int image, tc_image_info *info)
     return TC_OK;
 }
 
+// The launch parameters of a graph-mode execute: equal keys mean the same
+// kernels with the same arguments.  topo keeps only the launch topology.
+static void plan_graph_key(const tc_plan *P, void *const *d_out, std::vector<uint64_t> &key,
+                           std::vector<uint64_t> &topo)
+{
+    const int *cc = P->class_counts;
+    topo = {(uint64_t)P->ctx->t1_group, (uint64_t)P->dwt_launches.size()};
+    for (int k = 0; k < 6; k++) topo.push_back(cc[k] > 0);
+    // the heavy queue and the 8-in-16 merge change the Tier-1 launches
+    topo.push_back(cc[0] > 0 && cc[1] > 0 && cc[1] <= 148 && 8 * cc[1] <= cc[0]);
+    topo.push_back(cc[0] > 0 && cc[1] > 0 && 2 * cc[0] <= cc[1]);
+    topo.push_back(cc[3] > 0 && cc[4] > 0 && cc[4] <= 148 && 8 * cc[4] <= cc[3]);
+    for (const tc_plan::DwtLaunch &L : P->dwt_launches)
+        for (int v : {L.wavelet, L.color, L.ncomp, L.otype, L.bits}) topo.push_back((uint64_t)(int64_t)v);
+    key = topo;
+    uint32_t rbits;
+    std::memcpy(&rbits, &P->recon_r, 4);
+    for (uint64_t v : {(uint64_t)P->ncblk, (uint64_t)(uintptr_t)P->pool.ptr, (uint64_t)P->pool.size,
+                       (uint64_t)(uintptr_t)P->desc.ptr, (uint64_t)(uintptr_t)P->order.ptr,
+                       (uint64_t)(uintptr_t)P->coef.ptr, (uint64_t)(uintptr_t)P->scratch.ptr,
+                       (uint64_t)(uintptr_t)P->jobs.ptr, (uint64_t)rbits})
+        key.push_back(v);
+    for (int k = 0; k < 6; k++) key.push_back((uint64_t)cc[k]);
+    for (const tc_plan::DwtLaunch &L : P->dwt_launches)
+        for (int v : {L.first, L.njobs, L.ntiles}) key.push_back((uint64_t)v);
+    // images without a transform take their colour launch's pointers as
+    // parameters
+    for (size_t i = 0; i < P->imgs.size(); i++)
+        if (P->imgs[i].info.levels == 0) {
+            key.push_back((uint64_t)(uintptr_t)d_out[i]);
+            key.push_back(P->imgs[i].coef_off);
+            topo.push_back(i);
+        }
+}
+
+// Captures one execute's launches on the context's capture stream (the
+// caller's stream may be the legacy default stream, which cannot be
+// captured); the graph is launched on the caller's stream.
+static int plan_capture(tc_plan *P, void *const *d_out, cudaGraph_t *g, uint64_t *launches)
+{
+    tc_ctx *ctx = P->ctx;
+    cudaError_t e = ensure_side_streams(ctx);
+    if (e != cudaSuccess) return cuda_status(ctx, e, "graph capture");
+    const uint64_t l0 = ctx->launches;
+    cudaStream_t caller = ctx->stream;
+    ctx->stream = ctx->capture;
+    e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+        ctx->stream = caller;
+        return cuda_status(ctx, e, "graph capture");
+    }
+    const int rc = plan_run(P, d_out, true);
+    e = cudaStreamEndCapture(ctx->stream, g);
+    ctx->stream = caller;
+    *launches = ctx->launches - l0;
+    ctx->launches = l0;
+    if (rc) {
+        if (*g) cudaGraphDestroy(*g);
+        *g = nullptr;
+        return rc;
+    }
+    return cuda_status(ctx, e, "graph capture");
+}
+
 int tc_plan_execute(tc_plan *P, void *const *d_out)
 {
     if (!P || !d_out) return TC_E_ARG;
@@ -1109,46 +1193,74 @@ int tc_plan_execute(tc_plan *P, void *const *d_out)
         if (!d_out[i]) return fail(P->ctx, TC_E_ARG, "tc_plan_execute: null output");
     if (!P->use_graph || P->profiling) return plan_run(P, d_out);
     tc_ctx *ctx = P->ctx;
-    std::vector<void *> outs(d_out, d_out + P->imgs.size());
-    if (P->graph && outs != P->graph_outs) plan_drop_graph(P);
-    if (!P->graph) {
-        // First execute with these outputs: run normally (kernel attributes
-        // and side streams get set up), then capture the same work.
-        if ((rc = plan_run(P, d_out))) return rc;
-        // Capture on the context's own stream: the caller's stream may be the
-        // legacy default stream, which cannot be captured.  The graph is then
-        // launched on the caller's stream.
+    // the DWT job table for these outputs, uploaded outside any graph
+    if ((rc = run_reverse_batched(P, d_out, false))) return rc;
+    std::vector<uint64_t> key, topo;
+    plan_graph_key(P, d_out, key, topo);
+    tc_plan::Graph *hit = nullptr, *same_topo = nullptr;
+    for (tc_plan::Graph &g : P->graphs) {
+        if (g.key == key) hit = &g;
+        else if (g.topo == topo && !same_topo) same_topo = &g;
+    }
+    cudaError_t e;
+    if (!hit && same_topo) {
+        // same shape bucket: update the cached graph's parameters in place
         cudaGraph_t g = nullptr;
-        const uint64_t l0 = ctx->launches;
-        cudaError_t e = ensure_side_streams(ctx);
-        if (e != cudaSuccess) return cuda_status(ctx, e, "graph capture");
-        cudaStream_t caller = ctx->stream;
-        ctx->stream = ctx->capture;
-        e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
-        if (e != cudaSuccess) {
-            ctx->stream = caller;
-            return cuda_status(ctx, e, "graph capture");
+        uint64_t nl = 0;
+        if ((rc = plan_capture(P, d_out, &g, &nl))) return rc;
+        cudaGraphExecUpdateResultInfo info{};
+        e = cudaGraphExecUpdate(same_topo->exec, g, &info);
+        cudaGraphDestroy(g);
+        if (e == cudaSuccess) {
+            same_topo->key = key;
+            same_topo->launches = nl;
+            hit = same_topo;
+            P->graph_updates++;
+        } else {
+            cudaGetLastError();  // an update refused is not an error: instantiate instead
         }
-        rc = plan_run(P, d_out);
-        e = cudaStreamEndCapture(ctx->stream, &g);
-        ctx->stream = caller;
-        if (rc) {
-            if (g) cudaGraphDestroy(g);
-            return rc;
+    }
+    if (!hit) {
+        // A new bucket: run normally first (kernel attributes, side streams
+        // and the context's one-time set-up), then capture the same work.
+        if ((rc = plan_run(P, d_out, true))) return rc;
+        cudaGraph_t g = nullptr;
+        uint64_t nl = 0;
+        if ((rc = plan_capture(P, d_out, &g, &nl))) return rc;
+        tc_plan::Graph G;
+        e = cudaGraphInstantiate(&G.exec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return cuda_status(ctx, e, "graph instantiate");
+        G.key = key;
+        G.topo = topo;
+        G.launches = nl;
+        G.last_use = ++P->graph_tick;
+        if (P->graphs.size() >= kMaxGraphs) {
+            auto lru = std::min_element(P->graphs.begin(), P->graphs.end(),
+                                        [](const tc_plan::Graph &a, const tc_plan::Graph &b) {
+                                            return a.last_use < b.last_use;
+                                        });
+            cudaGraphExecDestroy(lru->exec);
+            P->graphs.erase(lru);
         }
-        if (e == cudaSuccess) e = cudaGraphInstantiate(&P->graph, g, 0);
-        if (g) cudaGraphDestroy(g);
-        if (e != cudaSuccess) {
-            P->graph = nullptr;
-            return cuda_status(ctx, e, "graph instantiate");
-        }
-        P->graph_outs = outs;
-        P->graph_launches = ctx->launches - l0;
+        P->graphs.push_back(G);
+        P->graph_captures++;
         return TC_OK;
     }
-    cudaError_t e = cudaGraphLaunch(P->graph, ctx->stream);
+    hit->last_use = ++P->graph_tick;
+    e = cudaGraphLaunch(hit->exec, ctx->stream);
     if (e != cudaSuccess) return cuda_status(ctx, e, "graph launch");
-    ctx->launches += P->graph_launches;
+    ctx->launches += hit->launches;
+    P->graph_replays++;
+    return TC_OK;
+}
+
+int tc_plan_graph_stats(const tc_plan *P, uint64_t *captures, uint64_t *updates, uint64_t *replays)
+{
+    if (!P || !captures || !updates || !replays) return TC_E_ARG;
+    *captures = P->graph_captures;
+    *updates = P->graph_updates;
+    *replays = P->graph_replays;
     return TC_OK;
 }
 
@@ -1156,7 +1268,7 @@ int tc_plan_set_graph(tc_plan *P, int on)
 {
     if (!P) return TC_E_ARG;
     P->use_graph = on != 0;
-    if (!on) plan_drop_graph(P);
+    if (!on) plan_drop_graphs(P);
     return TC_OK;
 }
 

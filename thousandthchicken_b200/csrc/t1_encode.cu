@@ -3,8 +3,8 @@
 // The reference has no Tier-1 encoder; this is the GPU half of the forward
 // pipeline (forward colour transform and DWT in color.cu / dwt.cu).  It
 // produces, block for block, the same codeword as the project's host encoder
-// (t1_encode_block in j2k_host.cpp): all coding passes, MQ termination by
-// the FLUSH procedure of ISO C.2.9.
+// (t1_encode_block in j2k_host.cpp): all coding passes, or the first
+// max_passes of them, MQ termination by the FLUSH procedure of ISO C.2.9.
 //
 //   * one warp per code-block, CTAs of kEncWarps blocks; at every bit-plane
 //     the lanes rebuild the plane's bits per column from the input (float
@@ -161,10 +161,11 @@ struct MQEnc {
     }
 };
 
-// All coding passes of a block whose state S holds the magnitudes, signs
-// and a cleared coding state (the lanes in lock-step).
+// The first `limit` coding passes of a block whose state S holds the signs
+// and a cleared coding state (the lanes in lock-step; limit is the same in
+// every lane, so the early exits are uniform).
 __device__ void encode_block(EncState &S, const Tables &T, MQEnc &mq, const tc_t1_enc_desc &d, const void *in,
-                             int numbps, int lane)
+                             int numbps, int limit, int lane)
 {
     const int w = d.w, h = d.h, orient = d.orient;
     uint32_t *ctx = S.ctx;
@@ -177,7 +178,8 @@ __device__ void encode_block(EncState &S, const Tables &T, MQEnc &mq, const tc_t
     auto bit = [&](int y, int c, int) -> uint32_t { return (uint32_t)(S.bits[c] >> y) & 1u; };
     auto sign_bit = [&](int y, int c) -> uint32_t { return (uint32_t)(S.neg[c] >> y) & 1u; };
 
-    for (int p = numbps - 1; p >= 0; --p) {
+    int done = 0;  // coding passes emitted
+    for (int p = numbps - 1; p >= 0 && done < limit; --p) {
         // this bit-plane's bits, the lanes' columns
 #pragma unroll
         for (int j = 0; j < CPL; j++) {
@@ -230,6 +232,7 @@ __device__ void encode_block(EncState &S, const Tables &T, MQEnc &mq, const tc_t
                     if (f != f0) F[s * 64 + c] = f;
                 }
             }
+            if (++done >= limit) break;
 
             // ---- magnitude refinement pass (ISO D.3.3) ----
             for (int s = 0; s < nstripes; s++) {
@@ -269,6 +272,7 @@ __device__ void encode_block(EncState &S, const Tables &T, MQEnc &mq, const tc_t
                     }
                 }
             }
+            if (++done >= limit) break;
         }
 
         // ---- cleanup pass (ISO D.3.4) ----
@@ -333,6 +337,7 @@ __device__ void encode_block(EncState &S, const Tables &T, MQEnc &mq, const tc_t
                 if (f != f0) F[s * 64 + c] = f;
             }
         }
+        ++done;
         __syncwarp();
         for (int i = lane; i < nstripes * 64; i += G) F[i] &= ~0x3C0000u;  // clear pi
         __syncwarp();
@@ -391,11 +396,14 @@ __global__ void __launch_bounds__(32 * kEncWarps)
     if (numbps > d.mb) {
         r.status = 2;  // the magnitudes need more bit-planes than the band has
     } else if (numbps > 0) {
+        // passes kept: d.max_passes (0 or more than the block has: all)
+        const int total = 3 * numbps - 2;
+        const int limit = d.max_passes && d.max_passes < total ? (int)d.max_passes : total;
         MQEnc mq;
         mq.init(out + (size_t)bi * cap, cap, lane == 0);
-        encode_block(S, T, mq, d, in, numbps, lane);
+        encode_block(S, T, mq, d, in, numbps, limit, lane);
         r.len = mq.flush();
-        r.passes = 3 * numbps - 2;
+        r.passes = (uint32_t)limit;
         if (mq.overflow || r.len > cap) {
             r.status = 3;
             r.len = 0;

@@ -166,6 +166,27 @@ class T1Encoder:
         return [(data[i * cap:i * cap + int(r["len"][i])].tobytes(), int(r["passes"][i]), int(r["zero_bitplanes"][i]))
                 for i in range(n)]
 
+    def encode_device(self, desc: np.ndarray, planes, cap: int):
+        """Encode on the device and keep the codewords there: returns (a
+        uint8 device tensor holding block i's codeword at i * cap, the
+        ENC_RESULT_DTYPE results on the host).  desc may set max_passes per
+        block to truncate its codeword."""
+        from .codec import ENC_DESC_DTYPE, ENC_RESULT_DTYPE
+        dev = torch.device("cuda", self.ctx.device)
+        desc = np.ascontiguousarray(desc, ENC_DESC_DTYPE)
+        n = len(desc)
+        d_desc = _dev_bytes(desc, dev)
+        out = torch.empty(max(n, 1) * cap, dtype=torch.uint8, device=dev)
+        res = torch.empty(max(n, 1) * ENC_RESULT_DTYPE.itemsize, dtype=torch.uint8, device=dev)
+        self.ctx.check(L.lib().tc_t1_encode(self.ctx.handle, _ptr(d_desc), n, _ptr(planes), _ptr(out), cap,
+                                            _ptr(res)), "tc_t1_encode")
+        self.ctx.synchronize()
+        r = res.cpu().numpy().view(ENC_RESULT_DTYPE)[:n].copy()
+        if (r["status"] != 0).any():
+            bad = int(np.nonzero(r["status"])[0][0])
+            raise L.TCError(L.TC_E_ARG, f"tc_t1_encode: block {bad} status {int(r['status'][bad])}")
+        return out, r
+
 
 class Quantizer:
     """Standalone inverse quantiser over raw Tier-1 words
@@ -309,15 +330,18 @@ class Plan:
         ctx.check(L.lib().tc_plan_create(ctx.handle, ptrs, lens, n, C.byref(h)), "tc_plan_create")
         self.handle = h
         ctx._plans.add(self)  # destroyed before the context (a plan uses its context's stream and pool)
+        self._read_infos(n)
+
+    def _read_infos(self, n):
+        from .codec import _info_dict
         self.infos = []
         self.out_bytes = []
         for i in range(n):
             info = L.ImageInfo()
-            L.check(L.lib().tc_plan_image_info(h, i, C.byref(info)))
-            from .codec import _info_dict
+            L.check(L.lib().tc_plan_image_info(self.handle, i, C.byref(info)))
             self.infos.append(_info_dict(info))
             nb = C.c_size_t(0)
-            L.check(L.lib().tc_plan_output_bytes(h, i, C.byref(nb)))
+            L.check(L.lib().tc_plan_output_bytes(self.handle, i, C.byref(nb)))
             self.out_bytes.append(nb.value)
 
     def alloc_outputs(self):
@@ -341,8 +365,26 @@ class Plan:
         return outs
 
     def set_graph(self, on: bool = True):
-        """Replay execute as a captured CUDA graph (per set of outputs)."""
+        """Replay execute as captured CUDA graphs, one per shape bucket (new
+        outputs replay the same graph)."""
         L.check(L.lib().tc_plan_set_graph(self.handle, int(on)), self.ctx.handle, "tc_plan_set_graph")
+
+    def graph_stats(self) -> dict:
+        """{"captures", "updates", "replays"} of graph mode."""
+        a, b, c = C.c_uint64(0), C.c_uint64(0), C.c_uint64(0)
+        L.check(L.lib().tc_plan_graph_stats(self.handle, C.byref(a), C.byref(b), C.byref(c)), self.ctx.handle,
+                "tc_plan_graph_stats")
+        return {"captures": a.value, "updates": b.value, "replays": c.value}
+
+    def rebuild(self, codestreams):
+        """Re-parse for new codestreams, keeping the device buffers (and, in
+        graph mode, the cached graphs of earlier shape buckets)."""
+        self._bufs = [np.frombuffer(bytes(c), np.uint8) for c in codestreams]
+        n = len(self._bufs)
+        ptrs = (C.c_void_p * n)(*[b.ctypes.data for b in self._bufs])
+        lens = (C.c_size_t * n)(*[b.size for b in self._bufs])
+        self.ctx.check(L.lib().tc_plan_rebuild(self.handle, ptrs, lens, n), "tc_plan_rebuild")
+        self._read_infos(n)
 
     def set_profiling(self, on: bool = True):
         L.check(L.lib().tc_plan_set_profiling(self.handle, int(on)), self.ctx.handle, "tc_plan_set_profiling")

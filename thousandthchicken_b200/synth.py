@@ -39,3 +39,54 @@ def laplacian_block(rng, w: int, h: int, bitplanes: int, zero_frac: float = 0.15
     v[rng.random((h, w)) < zero_frac] = 0
     lim = (1 << bitplanes) - 1
     return np.clip(v, -lim, lim).astype(np.int32)
+
+
+def c3_geometry(n: int = 200_000, seed: int = 3, min_image: int = 64, max_image: int = 4096) -> dict:
+    """Code-block geometry of the batched Tier-1 workload: n blocks, 60%
+    64x64, 30% 32x32 and 10% edge blocks with width and height uniform in
+    1..64; each with a subband orientation, a magnitude bit-plane count
+    uniform in 4..14 (its subband's scale) and a seeded pass count at which
+    its codeword is truncated, uniform in 1..3*planes-2.  Blocks are stored
+    one after another (block i at element off[i], pitch w[i]) and grouped in
+    order into "images" of min_image..max_image blocks for the per-image
+    comparison."""
+    rng = np.random.default_rng(seed)
+    kind = rng.choice(3, size=n, p=[0.6, 0.3, 0.1])
+    w = np.where(kind == 0, 64, np.where(kind == 1, 32, rng.integers(1, 65, n))).astype(np.uint16)
+    h = np.where(kind == 0, 64, np.where(kind == 1, 32, rng.integers(1, 65, n))).astype(np.uint16)
+    nb = rng.integers(4, 15, n).astype(np.uint8)
+    orient = rng.integers(0, 4, n).astype(np.uint8)
+    max_passes = (1 + (rng.random(n) * (3 * nb.astype(np.int64) - 2)).astype(np.int64)).astype(np.uint8)
+    size = w.astype(np.int64) * h.astype(np.int64)
+    off = np.concatenate([[0], np.cumsum(size)[:-1]]).astype(np.uint64)
+    images, s = [], 0
+    while s < n:
+        k = int(rng.integers(min_image, max_image + 1))
+        images.append((s, min(k, n - s)))
+        s += k
+    return {"w": w, "h": h, "nb": nb, "orient": orient, "max_passes": max_passes, "off": off,
+            "elems": int(size.sum()), "images": images}
+
+
+def c3_coefficients(geom: dict, device, seed: int = 3, zero_frac: float = 0.15, chunk: int = 1 << 26):
+    """The blocks' int32 coefficients on `device` (a torch tensor of
+    geom["elems"] values): Laplacian with scale 2^(planes-1)/4 per block,
+    rounded, about zero_frac exact zeros, clipped to the block's bit-plane
+    count.  Generated in chunks with a seeded torch generator."""
+    import torch
+    n = len(geom["w"])
+    size = torch.from_numpy((geom["w"].astype(np.int64) * geom["h"].astype(np.int64))).to(device)
+    nb = torch.from_numpy(geom["nb"].astype(np.int64)).to(device)
+    g = torch.Generator(device=device).manual_seed(seed)
+    out = torch.empty(geom["elems"], dtype=torch.int32, device=device)
+    block_of = torch.repeat_interleave(torch.arange(n, device=device), size)
+    for a in range(0, geom["elems"], chunk):
+        b = min(a + chunk, geom["elems"])
+        planes = nb[block_of[a:b]]
+        scale = torch.exp2((planes - 1).to(torch.float32)) / 4.0
+        u = torch.rand(b - a, generator=g, device=device) - 0.5
+        v = torch.round(-scale * torch.sign(u) * torch.log1p(-2.0 * u.abs().clamp(max=0.4999999)))
+        v = torch.where(torch.rand(b - a, generator=g, device=device) < zero_frac, torch.zeros_like(v), v)
+        lim = (torch.exp2(planes.to(torch.float32)) - 1.0)
+        out[a:b] = torch.maximum(torch.minimum(v, lim), -lim).to(torch.int32)
+    return out
