@@ -58,32 +58,6 @@ def make_workload(w, h, seed):
     return img, cs
 
 
-MIXED = dict(images=16, min_side=256, max_side=2048, step=16, seed=11)
-
-
-def make_mixed(n=None, seed=None):
-    """Mixed-size batch with the distribution of the mixed workload, scaled
-    down in image count and side length so the harness encoder finishes in
-    seconds: W, H uniform in [256, 2048] step 16, 1 or 3 components, 8- or
-    12-bit, half lossless (RCT + 5-level 5/3) and half lossy (ICT + 5-level
-    9/7, base step 1/64), 64x64 code-blocks."""
-    from thousandthchicken_b200 import codec
-    from thousandthchicken_b200.synth import gradient_noise_image
-    n = n or MIXED["images"]
-    rng = np.random.default_rng(seed if seed is not None else MIXED["seed"])
-    out = []
-    for i in range(n):
-        w = int(rng.integers(MIXED["min_side"] // 16, MIXED["max_side"] // 16 + 1)) * 16
-        h = int(rng.integers(MIXED["min_side"] // 16, MIXED["max_side"] // 16 + 1)) * 16
-        c = int(rng.choice([1, 3]))
-        bits = int(rng.choice([8, 12]))
-        rev = i % 2 == 0
-        img = gradient_noise_image(w, h, c, bits, seed=1000 + i)
-        cs = codec.encode(img, bits, levels=5, reversible=rev, mct=c == 3, base_step=1.0 / 64)
-        out.append((img, cs))
-    return out
-
-
 def serve_section(args, mixed, device):
     """Served decode: requests drawn from the mixed batch plus 20% 16-bit
     2048x2048 lossless images (radial field + N(0, 40^2) noise) arrive as a
@@ -472,6 +446,132 @@ def tier1_batched_section(ctx, stream, flush, cores):
     return out
 
 
+WAVE_BYTES = 24 << 30   # device memory of one wave of the mixed batch (plans + outputs)
+
+
+def encode_mixed(ctx, specs):
+    """The mixed batch's codestreams: each image generated on the device
+    (seeded), read back and coded by the GPU encoder (tc_encode_j2k_gpu),
+    outside any timing."""
+    import torch
+    from thousandthchicken_b200 import codec
+    from thousandthchicken_b200.synth import gradient_noise_image_device
+    dev = torch.device("cuda", ctx.device)
+    out = []
+    for sp in specs:
+        img = gradient_noise_image_device(sp["w"], sp["h"], sp["c"], sp["bits"], sp["seed"], dev).cpu().numpy()
+        if img.dtype == np.int16:
+            img = img.view(np.uint16)
+        out.append(codec.encode_gpu(ctx, img, sp["bits"], levels=sp["levels"], reversible=sp["reversible"],
+                                    mct=sp["c"] == 3, base_step=sp["base_step"]))
+    return out
+
+
+def mixed_waves(specs, streams, budget=WAVE_BYTES):
+    """Consecutive images grouped so that each group's device memory
+    (coefficients, DWT scratch, outputs, codestreams, descriptors) stays
+    under the budget."""
+    from thousandthchicken_b200.codec import read_header
+    from thousandthchicken_b200.serve import request_device_bytes
+    waves, cur, used = [], [], 0
+    for i, cs in enumerate(streams):
+        b = request_device_bytes(read_header(cs), len(cs))
+        if cur and used + b > budget:
+            waves.append(cur)
+            cur, used = [], 0
+        cur.append(i)
+        used += b
+    if cur:
+        waves.append(cur)
+    return waves
+
+
+def mixed_section(ctx, stream, specs, streams, cores):
+    """Mixed-size batch: 256 images of 256-8192 per side decoded in waves
+    under a device-memory budget, (a) batched: one plan per wave (one Tier-1
+    queue over all its code-blocks, DWT levels of all its images in shared
+    launches) replayed as a CUDA graph per shape bucket, and (b) per image:
+    one plan per image executed one after another, the plain per-image GPU
+    path.  Each is timed with CUDA events on the context's stream over one
+    execute of every image after one untimed execute (the waves are larger
+    than L2).  Lossless outputs are compared with the source image
+    regenerated on the device; lossy ones give their PSNR against it, and
+    the two smallest lossy images are compared with the FP64 oracle."""
+    import torch
+    from thousandthchicken_b200 import codec
+    from thousandthchicken_b200.stages import Plan
+    from thousandthchicken_b200.synth import gradient_noise_image_device
+    dev = torch.device("cuda", ctx.device)
+    waves = mixed_waves(specs, streams)
+    mpx = sum(sp["w"] * sp["h"] for sp in specs) / 1e6
+    lossy_small = sorted([i for i, sp in enumerate(specs) if not sp["reversible"]],
+                         key=lambda i: specs[i]["w"] * specs[i]["h"])[:2]
+    kept = {}
+    res = {"per_image": 0.0, "batched": 0.0}
+    exact, psnrs, graphs = True, [], {"captures": 0, "updates": 0, "replays": 0}
+    for path in ("per_image", "batched"):
+        for wave in waves:
+            ws = [streams[i] for i in wave]
+            plans = [Plan(ctx, ws)] if path == "batched" else [Plan(ctx, [s_]) for s_ in ws]
+            if path == "batched":
+                plans[0].set_graph(True)
+            outs = [p_.alloc_outputs() for p_ in plans]
+            with torch.cuda.stream(stream):
+                for p_, o_ in zip(plans, outs):
+                    p_.execute(o_)
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                for p_, o_ in zip(plans, outs):
+                    p_.execute(o_)
+                b.record(stream)
+            b.synchronize()
+            ctx.synchronize()
+            res[path] += a.elapsed_time(b)
+            if path == "batched":
+                for k, v in plans[0].graph_stats().items():
+                    graphs[k] += v
+                for i, o_ in zip(wave, outs[0]):
+                    sp = specs[i]
+                    ref = gradient_noise_image_device(sp["w"], sp["h"], sp["c"], sp["bits"], sp["seed"], dev)
+                    if sp["reversible"]:
+                        exact &= bool(torch.equal(o_, ref))
+                    else:
+                        mx = float((1 << sp["bits"]) - 1)
+                        d = o_.float() - ref.float()
+                        mse = float((d * d).mean())
+                        psnrs.append(99.0 if mse == 0 else 10 * np.log10(mx * mx / mse))
+                    if i in lossy_small:
+                        kept[i] = o_.cpu().numpy()
+                    del ref
+            for p_ in plans:
+                p_.close()
+            del outs, plans
+            torch.cuda.empty_cache()
+    # the two smallest lossy images against the FP64 oracle
+    O = _oracle()
+    orc = []
+    for i in lossy_small:
+        sp = specs[i]
+        info, desc, pool = codec.parse(streams[i])
+        want = O.decode_tile(desc, pool, sp["w"], sp["h"], sp["c"], sp["bits"], sp["levels"], False, sp["c"] == 3,
+                             r=0.5, threads=cores)
+        got = kept[i].view(np.uint16) if kept[i].dtype == np.int16 else kept[i]
+        d = np.abs(got.astype(np.int64) - want.astype(np.int64))
+        orc.append({"image": i, "size": f"{sp['w']}x{sp['h']}x{sp['c']}", "bits": sp["bits"],
+                    "max_abs": int(d.max()), "frac_differing": round(float((d > 0).mean()), 6)})
+    return {"images": len(specs), "mpixels": round(mpx, 1), "waves": len(waves),
+            "wave_budget_bytes": WAVE_BYTES,
+            "codestream_bytes": int(sum(len(s_) for s_ in streams)),
+            "batched_ms": round(res["batched"], 2), "per_image_ms": round(res["per_image"], 2),
+            "batched_mpix_s": round(mpx / (res["batched"] / 1000.0), 2),
+            "per_image_mpix_s": round(mpx / (res["per_image"] / 1000.0), 2),
+            "speedup": round(res["per_image"] / res["batched"], 3),
+            "lossless_bit_exact": exact, "lossy_min_psnr_db": round(min(psnrs), 2), "graphs": graphs,
+            "oracle_sample": orc,
+            "workload": "256 images, W and H uniform 256-8192 step 16, 1/3 comps, 8/12-bit, half RCT + 5-level 5/3, "
+                        "half ICT + 5-level 9/7 step 1/64, 64x64 blocks"}
+
+
 def kernels_section(ctx, stream, flush, cs, hbm):
     """The stand-alone stage kernels on device-resident 4096x4096 data, each
     timed with CUDA events on the context's stream (median of 5 runs, L2
@@ -700,75 +800,17 @@ def run_ours(args, rank, world, local_rank):
         kernels = kernels_section(ctx, stream, flush, cs, measured_peaks()[0])
         tier1_batched = tier1_batched_section(ctx, stream, flush, os.cpu_count() or 1)
         encode = encode_section(ctx, img)
-        # batched (one plan: one Tier-1 queue over every image) vs per-image plans
-        mixed = make_mixed()
-        streams = [cs_ for _, cs_ in mixed]
-        mpx_mixed = sum(im.shape[1] * im.shape[2] for im, _ in mixed) / 1e6
-        bplan = Plan(ctx, streams)
-        bouts = bplan.alloc_outputs()
-        bplan.set_graph(True)   # the batched path replays one captured graph per shape bucket
-        pplans = [Plan(ctx, [s_]) for s_ in streams]
-        pouts = [p_.alloc_outputs() for p_ in pplans]
-        mixed_steps = max(3, min(args.steps, 10))
-
-        def timed(fn, steps):
-            ms, lat = [], []
-            with torch.cuda.stream(stream):
-                for _ in range(2):
-                    fn(None)
-                for k in range(steps):
-                    flush.fill_(k & 0xFF)
-                    a_, b_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                    a_.record(stream)
-                    fn(lat)
-                    b_.record(stream)
-                    ms.append((a_, b_))
-            torch.cuda.synchronize()
-            return sum(x.elapsed_time(y) for x, y in ms) / steps, lat
-
-        def run_batched(lat):
-            bplan.execute(bouts)
-
-        def run_per_image(lat):
-            for p_, o_ in zip(pplans, pouts):
-                if lat is not None:
-                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                    e0.record(stream)
-                    p_.execute(o_)
-                    e1.record(stream)
-                    lat.append((e0, e1))
-                else:
-                    p_.execute(o_)
-
-        b_ms, _ = timed(run_batched, mixed_steps)
-        p_ms, p_lat = timed(run_per_image, mixed_steps)
-        lat_ms = sorted(x.elapsed_time(y) for x, y in p_lat)
-        ctx.synchronize()
-        lossless_exact, lossy_psnr = True, []
-        for i, ((im, _), o_) in enumerate(zip(mixed, bouts)):
-            got = o_.cpu().numpy()
-            if im.dtype == np.uint16:
-                got = got.view(np.uint16)
-            if i % 2 == 0:
-                lossless_exact &= bool(np.array_equal(got, im))
-            else:
-                mx_ = float((1 << (12 if im.dtype == np.uint16 else 8)) - 1)
-                d_ = got.astype(np.float64) - im.astype(np.float64)
-                lossy_psnr.append(10 * np.log10(mx_ * mx_ / max(float(np.mean(d_ * d_)), 1e-12)))
-        batched = {"images": len(mixed), "mpixels": round(mpx_mixed, 3),
-                   "batched_mpix_s": round(mpx_mixed / (b_ms / 1000.0), 2),
-                   "per_image_mpix_s": round(mpx_mixed / (p_ms / 1000.0), 2),
-                   "speedup": round(p_ms / b_ms, 3),
-                   "per_image_latency_ms": {"p50": round(lat_ms[len(lat_ms) // 2], 3),
-                                            "p99": round(lat_ms[min(len(lat_ms) - 1, int(0.99 * len(lat_ms)))], 3)},
-                   "lossless_bit_exact": lossless_exact, "lossy_min_psnr_db": round(min(lossy_psnr), 2),
-                   "workload": "mixed sizes 256-2048 step 16, 1/3 comps, 8/12-bit, half 5/3 lossless, half 9/7 lossy"}
-        bplan.close()
-        for p_ in pplans:
-            p_.close()
+        # the mixed-size batch at its stated size: batched waves vs per-image plans
+        from thousandthchicken_b200.synth import c4_specs
+        t0 = time.perf_counter()
+        specs = c4_specs()
+        mixed_streams = encode_mixed(ctx, specs)
+        log(f"[rank {rank}] mixed batch: {len(specs)} images, {sum(map(len, mixed_streams)) / 1e9:.2f} GB of "
+            f"codestreams in {time.perf_counter() - t0:.1f}s")
+        batched = mixed_section(ctx, stream, specs, mixed_streams, os.cpu_count() or 1)
 
         # served decode: Poisson arrivals, continuous batching vs the per-image path
-        served = serve_section(args, mixed, local_rank)
+        served = serve_section(args, specs, mixed_streams, local_rank)
 
     if rank == 0:
         px = W * H

@@ -361,6 +361,11 @@ int tc_plan_set_graph(tc_plan *plan, int on);
  * updated in place for a batch of the same topology, and replays of a
  * cached graph. */
 int tc_plan_graph_stats(const tc_plan *plan, uint64_t *captures, uint64_t *updates, uint64_t *replays);
+/* Device memory the plan holds now (segment pool, descriptors, order,
+ * coefficient arena, DWT scratch, job table; the buffers only grow).  A
+ * serving loop checks its admission estimates against it.  No counterpart
+ * in the reference, which allocates per call. */
+int tc_plan_device_bytes(const tc_plan *plan, size_t *bytes);
 /* Record CUDA events around the stages of every execute (on = 1): the
  * Tier-1 launch and the DWT/colour launches.  tc_plan_stage_ms waits for the
  * last execute and returns the device time of each stage in milliseconds.

@@ -44,10 +44,32 @@ def test_budget_limits_batches(gpu_ctx):
     server = Server(0, budget_bytes=biggest, max_batch=8, inflight=2)
     done, _ = server.run(reqs, realtime=False)
     server.close()
-    assert len(done) == len(reqs)
-    with pytest.raises(ValueError):
-        Server(0, budget_bytes=biggest - 1).run([Request(0, streams[np.argmax([len(s) for s in streams])], 0.0)],
-                                                 realtime=False)
+    assert len(done) == len(reqs) and not any(r.error for r in done)
+    assert server.stats["peak_admitted_bytes"] <= biggest
+    # a request above the whole budget fails alone, with an error
+    big = int(np.argmax([request_device_bytes(codec.read_header(s), len(s)) for s in streams]))
+    server = Server(0, budget_bytes=biggest - 1)
+    done, _ = server.run([Request(0, streams[big], 0.0)], realtime=False)
+    server.close()
+    assert done[0].error and "budget" in done[0].error
+
+
+def test_corrupt_request_fails_alone_on_the_gpu(gpu_ctx):
+    """One truncated codestream among good ones: one error, the others
+    decode to the same samples as alone."""
+    from thousandthchicken_b200.serve import Request, Server
+    from thousandthchicken_b200.stages import Decoder
+    streams = _streams()
+    alone = [Decoder(gpu_ctx).decode(s) for s in streams]
+    bad = streams[2][: len(streams[2]) // 2]
+    reqs = [Request(i, s, 0.0) for i, s in enumerate(streams)] + [Request(77, bad, 0.0)]
+    server = Server(0, budget_bytes=1 << 30, max_batch=4, inflight=2)
+    done, _ = server.run(reqs, realtime=False, keep_outputs=True)
+    server.close()
+    assert [r.rid for r in done if r.error] == [77]
+    for r in done:
+        if r.rid != 77:
+            np.testing.assert_array_equal(r.output, alone[r.rid])
 
 
 def test_poisson_arrivals_report_latency(gpu_ctx):

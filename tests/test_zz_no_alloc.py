@@ -56,15 +56,15 @@ def test_static_scratch_reverse97_matches_context_entry_point():
 
 
 def test_static_scratch_largest_plane_that_fits():
-    """8192 x 8192: the first-level low band is exactly the array's 4 Mi
-    samples, which the size check must accept; same result as the
-    context entry point (random Mallat coefficients, both on the GPU)."""
+    """4096 x 4096: the first-level low band (2048 x 2048) is exactly the
+    array's 4 Mi samples, which the size check must accept; same result as
+    the context entry point (random Mallat coefficients, both on the GPU)."""
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
     from thousandthchicken_b200.stages import Context, DWTReverse97
     ctx = Context(0)
-    n, levels = 8192, 3
-    g = torch.Generator(device="cuda").manual_seed(8192)
+    n, levels = 4096, 3
+    g = torch.Generator(device="cuda").manual_seed(4096)
     inp = torch.randn((n, n), generator=g, device="cuda") * 40
     want = torch.empty_like(inp)
     DWTReverse97(ctx).run(inp, want, n, n, levels)
@@ -80,7 +80,8 @@ def test_static_scratch_rejects_planes_beyond_the_array():
         pytest.skip("no CUDA device")
     inp = torch.empty(1, dtype=torch.float32, device="cuda")
     out = torch.empty(1, dtype=torch.float32, device="cuda")
-    # first-level low band 4097 x 4096 samples > TC_DWT97_STATIC_SCRATCH_ELEMS (4 Mi)
-    w, h = 8194, 8192
+    # first-level low band 2049 x 2048 samples, one row over
+    # TC_DWT97_STATIC_SCRATCH_ELEMS (4 Mi)
+    w, h = 4098, 4096
     rc = L.lib().tc_dwt_reverse97_static(inp.data_ptr(), w, out.data_ptr(), w, w, h, 3, None)
     assert rc == L.TC_E_ARG

@@ -122,6 +122,7 @@ _PROTOS = {
     "tc_plan_execute": (_I, [_VP, _VP]),
     "tc_plan_set_profiling": (_I, [_VP, _I]),
     "tc_plan_set_graph": (_I, [_VP, _I]),
+    "tc_plan_device_bytes": (_I, [_VP, C.POINTER(C.c_size_t)]),
     "tc_plan_graph_stats": (_I, [_VP, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "tc_plan_stage_ms": (_I, [_VP, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "tc_encode_j2k": (_I, [C.POINTER(EncodeParams), _VP, _VP, C.c_size_t, C.POINTER(C.c_size_t)]),

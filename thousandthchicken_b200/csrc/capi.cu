@@ -1255,6 +1255,13 @@ int tc_plan_execute(tc_plan *P, void *const *d_out)
     return TC_OK;
 }
 
+int tc_plan_device_bytes(const tc_plan *P, size_t *bytes)
+{
+    if (!P || !bytes) return TC_E_ARG;
+    *bytes = P->pool.size + P->desc.size + P->order.size + P->coef.size + P->scratch.size + P->jobs.size;
+    return TC_OK;
+}
+
 int tc_plan_graph_stats(const tc_plan *P, uint64_t *captures, uint64_t *updates, uint64_t *replays)
 {
     if (!P || !captures || !updates || !replays) return TC_E_ARG;

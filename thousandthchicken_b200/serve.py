@@ -10,9 +10,20 @@ next free slot, so arrivals overlap with decoding.  Each request's latency is
 its completion time minus its arrival time.
 
 Each request's codestream is parsed (Tier-2: packet headers, segment
-gathering, descriptors) on a worker thread as soon as it is admitted, while
+gathering, descriptors) on a worker thread as soon as it arrives, while
 earlier batches decode; a batch is then built from the parsed requests with
 `tc_plan_rebuild_parsed`, which only lays out and uploads.
+
+Failures stay with their request.  A request whose header or codestream does
+not parse, or whose estimated device memory is above the whole budget,
+finishes at once with `error` set and never holds budget.  A batch that fails
+on the device (a kernel flagged bad code-block data) is split: each of its
+requests is run again alone, and only the ones that fail alone finish with an
+error.  Budget is released whenever a request finishes, failed or not.
+
+The GPU side of a slot is an executor object (`_Slot` by default); tests pass
+a CPU fake through `slot_factory` to drive admission, failures and latency
+without a device.
 
 Results are deterministic per code-block, so a request decoded in a mix is
 bit-identical to the same request decoded alone.
@@ -46,6 +57,8 @@ class Request:
     done: float = -1.0
     output: object = None               # numpy array when keep_outputs
     parsed: object = None               # future of the tc_j2k_parse result
+    error: str | None = None            # set when the request failed
+    alone: bool = False                 # re-run alone after its batch failed
 
 
 def _parse(cs: bytes):
@@ -80,7 +93,9 @@ def request_device_bytes(info: dict, cs_len: int) -> int:
 
 
 class _Slot:
-    def __init__(self, server, device):
+    """One batch in flight on its own CUDA stream and resident plan."""
+
+    def __init__(self, device):
         self.stream = torch.cuda.Stream(device)
         from .stages import Context
         self.ctx = Context(device, self.stream)
@@ -91,8 +106,13 @@ class _Slot:
         self.keep = []
 
     def launch(self, batch, keep_outputs):
+        """Build the slot's plan for `batch` and start its decode; raises on
+        a host-side failure (a request that does not parse)."""
         lib = L.lib()
+        self.batch = []
         try:
+            parsed = [r.parsed.result() for r in batch]
+            arr = (C.POINTER(L.Parsed) * len(parsed))(*parsed)
             if self.plan is None:
                 bufs = [np.frombuffer(r.cs, np.uint8) for r in batch]
                 ptrs = (C.c_void_p * len(bufs))(*[b.ctypes.data for b in bufs])
@@ -102,8 +122,6 @@ class _Slot:
                                "tc_plan_create")
                 self.plan = h
             else:
-                parsed = [r.parsed.result() for r in batch]
-                arr = (C.POINTER(L.Parsed) * len(parsed))(*parsed)
                 self.ctx.check(lib.tc_plan_rebuild_parsed(self.plan, arr, len(parsed)), "tc_plan_rebuild_parsed")
         finally:
             for r in batch:
@@ -126,21 +144,36 @@ class _Slot:
         return bool(self.batch)
 
     def poll(self, now_fn):
+        """The finished batch's requests, or []; raises when the device
+        flagged the batch (the slot is free again either way)."""
         if not self.batch or not self.event.query():
             return []
         t = now_fn()
-        self.ctx.synchronize()  # reads the device error word
         done = self.batch
-        for r, o in zip(done, self.outs):
-            r.done = t
-            if self.keep:
-                a = o.cpu().numpy()
-                if r.info["bits"] > 8:
-                    a = a.view(np.int16 if r.info.get("is_signed") else np.uint16)
-                r.output = a
         self.batch = []
-        self.outs = None
+        try:
+            self.ctx.synchronize()  # reads and clears the device error word
+            for r, o in zip(done, self.outs):
+                r.done = t
+                if self.keep:
+                    a = o.cpu().numpy()
+                    if r.info["bits"] > 8:
+                        a = a.view(np.int16 if r.info.get("is_signed") else np.uint16)
+                    r.output = a
+        finally:
+            self.outs = None
         return done
+
+    def device_bytes(self) -> int:
+        """Device memory of the slot's plan and its batch's outputs now."""
+        n = 0
+        if self.plan is not None:
+            b = C.c_size_t(0)
+            if L.lib().tc_plan_device_bytes(self.plan, C.byref(b)) == L.TC_OK:
+                n += b.value
+        for o in self.outs or []:
+            n += o.numel() * o.element_size()
+        return n
 
     def close(self):
         if self.plan is not None:
@@ -150,70 +183,142 @@ class _Slot:
 
 
 class Server:
-    """Continuous-batching decoder.  `budget_bytes` bounds the device memory
-    of the requests in flight; `max_batch` bounds a batch's request count."""
+    """Continuous-batching decoder.  `budget_bytes` bounds the estimated
+    device memory of the requests in flight; `max_batch` bounds a batch's
+    request count.  `slot_factory(i)` makes the executor of slot i (default:
+    a GPU slot on `device`)."""
 
-    def __init__(self, device: int = 0, budget_bytes: int = 40 << 30, max_batch: int = 32, inflight: int = 2):
-        if torch is None or not torch.cuda.is_available():
-            raise L.LibraryMissing("a CUDA device is required (no CPU fallback)")
+    def __init__(self, device: int = 0, budget_bytes: int = 40 << 30, max_batch: int = 32, inflight: int = 2,
+                 slot_factory=None):
+        if slot_factory is None:
+            if torch is None or not torch.cuda.is_available():
+                raise L.LibraryMissing("a CUDA device is required (no CPU fallback)")
+            slot_factory = lambda i: _Slot(device)  # noqa: E731
         self.budget = budget_bytes
         self.max_batch = max_batch
-        self.slots = [_Slot(self, device) for _ in range(inflight)]
+        self.slots = [slot_factory(i) for i in range(inflight)]
         self.parser = ThreadPoolExecutor(max_workers=max(1, min(8, os.cpu_count() or 1)))
+        self.stats = {}
 
     def close(self):
         for s in self.slots:
             s.close()
         self.parser.shutdown(wait=True)
 
-    def run(self, requests, realtime: bool = True, keep_outputs: bool = False):
+    def run(self, requests, realtime: bool = True, keep_outputs: bool = False, stop_backlog_s: float = 0.0):
         """Serve `requests` (Request objects with arrival times in seconds
         from the start).  With realtime, a request becomes visible only once
         the clock passes its arrival; otherwise all are visible at once.
-        Returns (requests with done times, wall seconds)."""
-        for r in requests:
-            if not r.info:
-                r.info = read_header(r.cs)
-                r.device_bytes = request_device_bytes(r.info, len(r.cs))
-            if r.device_bytes > self.budget:
-                raise ValueError(f"request {r.rid} needs {r.device_bytes} B, above the budget")
-        pending = sorted(requests, key=lambda r: r.arrival)
+        stop_backlog_s > 0 ends an overloaded run early: once the oldest
+        waiting request has waited that long, no further arrivals are
+        admitted and the run finishes what it holds (the rest are returned
+        unserved, done < 0).  Returns (finished requests, wall seconds);
+        failed requests are among them with `error` set.  self.stats then
+        holds the peak admitted and measured device bytes and the counts of
+        failed and unserved requests."""
         t0 = time.perf_counter()
-        now = (lambda: time.perf_counter() - t0) if realtime else (lambda: time.perf_counter() - t0)
-        if not realtime:
-            for r in pending:
+        now = lambda: time.perf_counter() - t0  # noqa: E731
+        finished = []
+
+        def fail(r, msg):
+            r.error = msg
+            r.done = now()
+            _free_parsed(r)
+            finished.append(r)
+
+        pending = []
+        for r in sorted(requests, key=lambda r: r.arrival):
+            if not realtime:
                 r.arrival = 0.0
-        queue, finished = [], []
+            r.error, r.done, r.alone = None, -1.0, False
+            pending.append(r)
+        queue, retry = [], []
         nxt = 0
         in_flight_bytes = 0
-        while len(finished) < len(requests):
+        peak_admitted = peak_measured = 0
+        stopped = False
+        unserved = []
+        while True:
             t = now()
-            while nxt < len(pending) and pending[nxt].arrival <= t:
+            while not stopped and nxt < len(pending) and pending[nxt].arrival <= t:
                 r = pending[nxt]
+                nxt += 1
+                try:
+                    if not r.info:
+                        r.info = read_header(r.cs)
+                        r.device_bytes = request_device_bytes(r.info, len(r.cs))
+                except Exception as ex:  # noqa: BLE001 - a bad header fails its request only
+                    fail(r, f"header: {ex}")
+                    continue
+                if r.device_bytes > self.budget:
+                    fail(r, f"needs {r.device_bytes} B of device memory, above the budget")
+                    continue
                 r.parsed = self.parser.submit(_parse, r.cs)  # Tier-2 overlaps the decodes in flight
                 queue.append(r)
-                nxt += 1
+            if stop_backlog_s > 0 and not stopped and queue and t - queue[0].arrival > stop_backlog_s:
+                stopped = True          # overloaded: stop admitting, drain what is held
+                unserved = pending[nxt:]
+                nxt = len(pending)
             for s in self.slots:
-                for r in s.poll(now):
+                batch = s.batch if s.busy() else []
+                try:
+                    done = s.poll(now)
+                except Exception as ex:  # noqa: BLE001 - the device flagged this batch
+                    for r in batch:
+                        in_flight_bytes -= r.device_bytes
+                        if len(batch) == 1 or r.alone:
+                            fail(r, f"decode: {ex}")
+                        else:
+                            r.alone = True
+                            r.parsed = self.parser.submit(_parse, r.cs)
+                            retry.append(r)
+                    continue
+                for r in done:
                     in_flight_bytes -= r.device_bytes
                     finished.append(r)
             for s in self.slots:
-                if s.busy() or not queue:
+                if s.busy():
                     continue
                 batch = []
-                while queue and len(batch) < self.max_batch and \
-                        in_flight_bytes + queue[0].device_bytes <= self.budget:
-                    r = queue.pop(0)
+                src = retry if retry else queue
+                while src and len(batch) < (1 if src is retry else self.max_batch) and \
+                        in_flight_bytes + src[0].device_bytes <= self.budget:
+                    r = src[0]
+                    if r.parsed is not None and r.parsed.done() and r.parsed.exception() is not None:
+                        src.pop(0)
+                        fail(r, f"parse: {r.parsed.exception()}")
+                        continue
+                    src.pop(0)
                     batch.append(r)
                     in_flight_bytes += r.device_bytes
-                if batch:
+                if not batch:
+                    continue
+                peak_admitted = max(peak_admitted, in_flight_bytes)
+                try:
                     s.launch(batch, keep_outputs)
-            if not any(s.busy() for s in self.slots) and not queue and nxt < len(pending):
-                # idle until the next arrival
-                wait = pending[nxt].arrival - now()
+                except Exception as ex:  # noqa: BLE001 - host-side failure of the batch
+                    for r in batch:
+                        in_flight_bytes -= r.device_bytes
+                        if len(batch) == 1 or r.alone:
+                            fail(r, f"launch: {ex}")
+                        else:
+                            r.alone = True
+                            r.parsed = self.parser.submit(_parse, r.cs)
+                            retry.append(r)
+                    continue
+                peak_measured = max(peak_measured, sum(x.device_bytes() for x in self.slots))
+            if nxt >= len(pending) and not queue and not retry and not any(s.busy() for s in self.slots):
+                break
+            if not any(s.busy() for s in self.slots) and not queue and not retry and nxt < len(pending):
+                wait = pending[nxt].arrival - now()   # idle until the next arrival
                 if wait > 0:
                     time.sleep(min(wait, 0.001))
-        return finished, now()
+            elif any(s.busy() for s in self.slots):
+                time.sleep(0)
+        wall = now()
+        self.stats = {"peak_admitted_bytes": int(peak_admitted), "peak_device_bytes": int(peak_measured),
+                      "failed": sum(1 for r in finished if r.error), "unserved": len(unserved)}
+        return finished, wall
 
 
 def poisson_arrivals(n: int, rate_per_s: float, seed: int = 0):
@@ -222,6 +327,9 @@ def poisson_arrivals(n: int, rate_per_s: float, seed: int = 0):
 
 
 def latency_stats(reqs):
-    lat = np.array([(r.done - r.arrival) * 1000.0 for r in reqs])
+    ok = [r for r in reqs if r.error is None and r.done >= 0]
+    if not ok:
+        return {"p50_ms": float("nan"), "p99_ms": float("nan"), "mean_ms": float("nan")}
+    lat = np.array([(r.done - r.arrival) * 1000.0 for r in ok])
     return {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
             "mean_ms": float(lat.mean())}

@@ -90,3 +90,41 @@ def c3_coefficients(geom: dict, device, seed: int = 3, zero_frac: float = 0.15, 
         lim = (torch.exp2(planes.to(torch.float32)) - 1.0)
         out[a:b] = torch.maximum(torch.minimum(v, lim), -lim).to(torch.int32)
     return out
+
+
+def c4_specs(n: int = 256, seed: int = 11, min_side: int = 256, max_side: int = 8192, step: int = 16) -> list:
+    """The mixed-size batch: n images with width and height each uniform in
+    min_side..max_side (multiples of step), 1 or 3 components, 8- or 12-bit
+    samples; even-numbered images lossless (RCT + 5-level 5/3), odd ones
+    lossy (ICT + 5-level 9/7, base step 1/64)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        w = int(rng.integers(min_side // step, max_side // step + 1)) * step
+        h = int(rng.integers(min_side // step, max_side // step + 1)) * step
+        c = int(rng.choice([1, 3]))
+        bits = int(rng.choice([8, 12]))
+        out.append({"w": w, "h": h, "c": c, "bits": bits, "reversible": i % 2 == 0, "levels": 5,
+                    "base_step": 1.0 / 64, "seed": 1000 + i})
+    return out
+
+
+def gradient_noise_image_device(w: int, h: int, c: int, bits: int, seed: int, device, sigma: float = 8.0):
+    """The gradient_noise_image family generated on a CUDA device with a
+    seeded torch generator: per-channel bilinear gradients plus N(0, sigma^2)
+    noise (sigma in 8-bit units, scaled to the bit depth), rounded and
+    clipped; [c, h, w] uint8 (bits <= 8) or int16 holding the unsigned
+    samples.  The same seed gives the same image on the same device."""
+    import torch
+    g = torch.Generator(device=device).manual_seed(seed)
+    mx = float((1 << bits) - 1)
+    gx = torch.linspace(0.0, 1.0, w, device=device)[None, :]
+    gy = torch.linspace(0.0, 1.0, h, device=device)[:, None]
+    out = torch.empty((c, h, w), dtype=torch.uint8 if bits <= 8 else torch.int16, device=device)
+    for k in range(c):
+        a, b, off = (torch.rand(3, generator=g, device=device) * torch.tensor([0.8, 0.8, 0.2], device=device) +
+                     torch.tensor([0.2, 0.2, 0.0], device=device)).tolist()
+        base = mx * (off + (1 - off) * (a * gx + b * gy) / (a + b))
+        noise = torch.randn((h, w), generator=g, device=device) * (sigma * mx / 255.0)
+        out[k] = torch.clamp(torch.round(base + noise), 0, mx).to(out.dtype)
+    return out
