@@ -71,6 +71,13 @@ uint64_t tc_ctx_launch_count(const tc_ctx *ctx);
  * and caches the choice.  Default 32. */
 int tc_ctx_set_t1_group(tc_ctx *ctx, int lanes);
 int tc_ctx_t1_group(const tc_ctx *ctx);
+/* Device memory the ctx's memory pool reserves now: the buffers of its
+ * plans plus freed blocks the pool keeps mapped for regrowth.  A serving
+ * loop admits work against it.  No counterpart in the reference. */
+int tc_ctx_pool_bytes(tc_ctx *ctx, size_t *reserved);
+/* Wait for the ctx's stream, then return the pool's unused blocks to the
+ * device (after a plan is destroyed, its memory leaves the pool). */
+int tc_ctx_trim(tc_ctx *ctx);
 
 /* ---- Tier-1 code-block decode (CoefficientCoder) ------------------------- */
 

@@ -25,6 +25,8 @@ class FakeSlot:
         self.t_end = 0.0
         self.watch = watch if watch is not None else {}
         self.watch.setdefault("batches", [])
+        self.plan = None        # a plan's buffers: grow-only, by at least half again
+        self.held = 0
 
     def launch(self, batch, keep_outputs):
         for r in batch:
@@ -32,6 +34,11 @@ class FakeSlot:
         if any(r.rid in self.launch_fails for r in batch):
             raise RuntimeError("plan build failed")
         self.batch = list(batch)
+        need = sum(r.device_bytes for r in batch)
+        if self.plan is None:
+            self.plan, self.held = object(), need
+        elif need > self.held:
+            self.held = max(need, int(1.5 * self.held))
         self.watch["batches"].append([r.rid for r in batch])
         self.t_end = time.perf_counter() + self.latency_s * len(batch)
 
@@ -50,7 +57,10 @@ class FakeSlot:
         return done
 
     def device_bytes(self):
-        return sum(r.device_bytes for r in self.batch)
+        return self.held
+
+    def shrink(self):
+        self.plan, self.held = None, 0
 
     def close(self):
         pass
@@ -107,6 +117,7 @@ def test_budget_bounds_requests_in_flight_and_is_released():
     srv.close()
     assert len(done) == len(reqs) and not any(r.error for r in done)
     assert srv.stats["peak_admitted_bytes"] <= budget
+    assert srv.stats["peak_device_bytes"] <= budget
     for b in watch["batches"]:
         assert sum(sizes[i % len(streams)] if i < 50 else sizes[0] for i in b) <= budget
     # a request larger than the whole budget fails without blocking the others

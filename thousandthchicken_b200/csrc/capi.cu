@@ -773,6 +773,28 @@ int tc_ctx_set_t1_group(tc_ctx *ctx, int lanes)
 
 int tc_ctx_t1_group(const tc_ctx *ctx) { return ctx ? ctx->t1_group : TC_E_ARG; }
 
+int tc_ctx_pool_bytes(tc_ctx *ctx, size_t *reserved)
+{
+    if (!ctx || !reserved) return TC_E_ARG;
+    *reserved = 0;
+    if (!ctx->pool) return TC_OK;
+    uint64_t v = 0;
+    const cudaError_t e = cudaMemPoolGetAttribute(ctx->pool, cudaMemPoolAttrReservedMemCurrent, &v);
+    if (e != cudaSuccess) return cuda_status(ctx, e, "tc_ctx_pool_bytes");
+    *reserved = (size_t)v;
+    return TC_OK;
+}
+
+int tc_ctx_trim(tc_ctx *ctx)
+{
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!ctx->pool) return TC_OK;
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e == cudaSuccess) e = cudaMemPoolTrimTo(ctx->pool, 0);
+    return cuda_status(ctx, e, "tc_ctx_trim");
+}
+
 int tc_t1_decode(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint32_t *d_order, int n, const uint8_t *d_pool,
                  uint64_t pool_len, void *d_out, int out_mode, float recon_r, int max_bitplanes)
 {

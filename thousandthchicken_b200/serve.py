@@ -165,15 +165,20 @@ class _Slot:
         return done
 
     def device_bytes(self) -> int:
-        """Device memory of the slot's plan and its batch's outputs now."""
-        n = 0
+        """Device memory the slot holds now: what its context's memory pool
+        reserves (its plan's buffers and blocks kept for regrowth) and its
+        batch's outputs."""
+        b = C.c_size_t(0)
+        L.check(L.lib().tc_ctx_pool_bytes(self.ctx.handle, C.byref(b)), self.ctx.handle, "tc_ctx_pool_bytes")
+        return b.value + sum(o.numel() * o.element_size() for o in self.outs or [])
+
+    def shrink(self):
+        """Give the slot's device memory back (idle slots only): destroy its
+        plan and return the pool's blocks; the next batch builds a new plan."""
         if self.plan is not None:
-            b = C.c_size_t(0)
-            if L.lib().tc_plan_device_bytes(self.plan, C.byref(b)) == L.TC_OK:
-                n += b.value
-        for o in self.outs or []:
-            n += o.numel() * o.element_size()
-        return n
+            L.lib().tc_plan_destroy(self.plan)
+            self.plan = None
+        L.check(L.lib().tc_ctx_trim(self.ctx.handle), self.ctx.handle, "tc_ctx_trim")
 
     def close(self):
         if self.plan is not None:
@@ -211,8 +216,9 @@ class Server:
         the clock passes its arrival; otherwise all are visible at once.
         stop_backlog_s > 0 ends an overloaded run early: once the oldest
         waiting request has waited that long, no further arrivals are
-        admitted and the run finishes what it holds (the rest are returned
-        unserved, done < 0).  Returns (finished requests, wall seconds);
+        admitted, waiting requests are dropped and the run finishes the
+        batches in flight (the dropped and unarrived requests are left
+        unserved, done < 0, and not returned).  Returns (finished requests, wall seconds);
         failed requests are among them with `error` set.  self.stats then
         holds the peak admitted and measured device bytes and the counts of
         failed and unserved requests."""
@@ -256,8 +262,11 @@ class Server:
                 r.parsed = self.parser.submit(_parse, r.cs)  # Tier-2 overlaps the decodes in flight
                 queue.append(r)
             if stop_backlog_s > 0 and not stopped and queue and t - queue[0].arrival > stop_backlog_s:
-                stopped = True          # overloaded: stop admitting, drain what is held
-                unserved = pending[nxt:]
+                stopped = True          # overloaded: stop admitting, finish the batches in flight
+                unserved = pending[nxt:] + queue
+                for r in queue:
+                    _free_parsed(r)
+                queue = []
                 nxt = len(pending)
             for s in self.slots:
                 batch = s.batch if s.busy() else []
@@ -279,10 +288,33 @@ class Server:
             for s in self.slots:
                 if s.busy():
                     continue
-                batch = []
                 src = retry if retry else queue
+                if not src:
+                    continue
+                # Measured memory: the other slots hold `others`, so this slot
+                # may hold `room`.  A slot with a plan grows its buffers by up
+                # to half again to fit a batch; a fresh one allocates exactly.
+                # An idle slot that keeps more than the head request leaves
+                # room for gives its memory back, then the other idle ones.
+                head = src[0].device_bytes
+                others = sum(x.device_bytes() for x in self.slots if x is not s)
+
+                def fits(n, s=s, others=others):
+                    held = n if s.plan is None else max(s.device_bytes(), 1.5 * n)
+                    return held <= self.budget - others
+
+                if not fits(head):
+                    s.shrink()
+                    if self.budget - others < head:
+                        for x in self.slots:
+                            if x is not s and not x.busy():
+                                x.shrink()
+                        others = sum(x.device_bytes() for x in self.slots if x is not s)
+                batch = []
+                need = 0
                 while src and len(batch) < (1 if src is retry else self.max_batch) and \
-                        in_flight_bytes + src[0].device_bytes <= self.budget:
+                        in_flight_bytes + src[0].device_bytes <= self.budget and \
+                        fits(need + src[0].device_bytes, s, others):
                     r = src[0]
                     if r.parsed is not None and r.parsed.done() and r.parsed.exception() is not None:
                         src.pop(0)
@@ -290,6 +322,7 @@ class Server:
                         continue
                     src.pop(0)
                     batch.append(r)
+                    need += r.device_bytes
                     in_flight_bytes += r.device_bytes
                 if not batch:
                     continue
@@ -317,7 +350,8 @@ class Server:
                 time.sleep(0)
         wall = now()
         self.stats = {"peak_admitted_bytes": int(peak_admitted), "peak_device_bytes": int(peak_measured),
-                      "failed": sum(1 for r in finished if r.error), "unserved": len(unserved)}
+                      "failed": sum(1 for r in finished if r.error), "unserved": len(unserved),
+                      "stopped_at_s": round(wall, 3) if stopped else None}
         return finished, wall
 
 
