@@ -61,6 +61,7 @@ def make_workload(w, h, seed):
 SERVE_RATES = "50,100,200,500,1000,2000"
 SERVE_BUDGET = 40 << 30
 SERVE_BACKLOG_S = 2.0    # a rate is not sustained once a request waits this long unbatched
+SERVE_BATCH_SAMPLES = 128 << 20   # samples per batch (about 50 ms of decode)
 
 
 def serve_section(args, specs, streams, device):
@@ -70,7 +71,8 @@ def serve_section(args, specs, streams, device):
     40 GB.  First the capacity of each path (every request available at
     once).  Then, for each rate of --serve-rates and at 80% of the
     continuous-batching capacity, min(1000, 5 s x rate) arrivals served by
-    the continuous-batching server (batches of up to 16, two in flight) and
+    the continuous-batching server (batches of up to 16 requests and 128 Mi
+    samples, two in flight) and
     by the per-image path (one request per batch, one in flight) on the same
     arrivals.  A rate is sustained when no request waits more than 2 s
     before its batch starts; otherwise the run stops admitting there and the
@@ -90,14 +92,16 @@ def serve_section(args, specs, streams, device):
         return [nmix + int(r.integers(len(radial))) if r.random() < 0.2 else int(r.integers(nmix))
                 for _ in range(n)]
 
-    paths = {"continuous_batching": dict(max_batch=16, inflight=2), "per_image": dict(max_batch=1, inflight=1)}
+    paths = {"continuous_batching": dict(max_batch=16, inflight=2, max_batch_samples=SERVE_BATCH_SAMPLES),
+             "per_image": dict(max_batch=1, inflight=1)}
     servers = {k: Server(device, budget_bytes=SERVE_BUDGET, **kw) for k, kw in paths.items()}
     # warm-up: the largest requests once, so plan buffers and pinned staging
     # reach their working size before any timed run
     big = sorted(range(len(pool)), key=lambda i: -len(pool[i][0]))[:16]
     for srv in servers.values():
         srv.run([Request(k, pool[i][0], 0.0) for k, i in enumerate(big)], realtime=False)
-    out = {"budget_bytes": SERVE_BUDGET, "pool_images": len(pool), "radial_share": 0.2, "capacity": {}, "by_rate": []}
+    out = {"budget_bytes": SERVE_BUDGET, "batch_samples_cap": SERVE_BATCH_SAMPLES, "pool_images": len(pool),
+           "radial_share": 0.2, "capacity": {}, "by_rate": []}
     cap_ids = picks(48, 7)
     mpx = sum(pool[i][1] for i in cap_ids) / 1e6
     for name, srv in servers.items():

@@ -151,3 +151,18 @@ def test_overloaded_run_stops_admitting():
     srv.close()
     assert srv.stats["unserved"] > 0 and len(done) + srv.stats["unserved"] == len(reqs)
     assert wall < 400 * 0.01
+
+
+def test_batch_sample_cap():
+    streams = _streams()
+    sizes = {i: codec.read_header(s) for i, s in enumerate(streams)}
+    cap = max(v["width"] * v["height"] * v["ncomp"] for v in sizes.values())
+    watch = {}
+    srv = Server(budget_bytes=1 << 30, max_batch=8, inflight=1, max_batch_samples=cap,
+                 slot_factory=lambda i: FakeSlot(watch=watch))
+    done, _ = srv.run([Request(i, s, 0.0) for i, s in enumerate(streams)], realtime=False)
+    srv.close()
+    assert len(done) == len(streams)
+    for b in watch["batches"]:
+        assert len(b) == 1 or sum(sizes[i]["width"] * sizes[i]["height"] * sizes[i]["ncomp"] for i in b) <= cap
+    assert any(len(b) > 1 for b in watch["batches"])

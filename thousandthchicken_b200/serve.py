@@ -194,13 +194,17 @@ class Server:
     a GPU slot on `device`)."""
 
     def __init__(self, device: int = 0, budget_bytes: int = 40 << 30, max_batch: int = 32, inflight: int = 2,
-                 slot_factory=None):
+                 slot_factory=None, max_batch_samples: int = 0):
         if slot_factory is None:
             if torch is None or not torch.cuda.is_available():
                 raise L.LibraryMissing("a CUDA device is required (no CPU fallback)")
             slot_factory = lambda i: _Slot(device)  # noqa: E731
         self.budget = budget_bytes
         self.max_batch = max_batch
+        # samples (width x height x components) per batch, 0: no cap.  Large
+        # images fill the GPU alone; batching pays for small ones, and a cap
+        # keeps a batch's decode, and so its requests' latency, short.
+        self.max_batch_samples = max_batch_samples
         self.slots = [slot_factory(i) for i in range(inflight)]
         self.parser = ThreadPoolExecutor(max_workers=max(1, min(8, os.cpu_count() or 1)))
         self.stats = {}
@@ -311,10 +315,12 @@ class Server:
                                 x.shrink()
                         others = sum(x.device_bytes() for x in self.slots if x is not s)
                 batch = []
-                need = 0
+                need = samples = 0
+                cap = self.max_batch_samples or float("inf")
                 while src and len(batch) < (1 if src is retry else self.max_batch) and \
                         in_flight_bytes + src[0].device_bytes <= self.budget and \
-                        fits(need + src[0].device_bytes, s, others):
+                        fits(need + src[0].device_bytes, s, others) and \
+                        (not batch or samples + _samples(src[0]) <= cap):
                     r = src[0]
                     if r.parsed is not None and r.parsed.done() and r.parsed.exception() is not None:
                         src.pop(0)
@@ -323,6 +329,7 @@ class Server:
                     src.pop(0)
                     batch.append(r)
                     need += r.device_bytes
+                    samples += _samples(r)
                     in_flight_bytes += r.device_bytes
                 if not batch:
                     continue
@@ -353,6 +360,11 @@ class Server:
                       "failed": sum(1 for r in finished if r.error), "unserved": len(unserved),
                       "stopped_at_s": round(wall, 3) if stopped else None}
         return finished, wall
+
+
+def _samples(r) -> int:
+    i = r.info
+    return i["width"] * i["height"] * i["ncomp"]
 
 
 def poisson_arrivals(n: int, rate_per_s: float, seed: int = 0):
