@@ -140,12 +140,16 @@ typedef struct tc_cblk_desc {
  * only for truncated blocks; 0 = truncated value).  max_bitplanes bounds
  * Mb - zero_bitplanes over the blocks (0 = up to 31); it sizes the
  * magnitude storage, and a block above it is flagged as out of range.
+ * d_out holds out_elems 4-byte elements: a block whose last sample,
+ * out_off + (h-1)*out_pitch + w - 1, is not below out_elems is skipped before
+ * anything is written and reported by tc_ctx_synchronize (the reference
+ * trusts d_coefficientsOffset, coefficientcoder_common.h:5-24).
  * Replaces CoefficientCoder::decode_tile/decodeInit/decode
  * (CoefficientCoder.cpp:62-252) plus Quantizer::dequantize_tile
  * (Quantizer.cpp:181-216). */
 int tc_t1_decode(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint32_t *d_order,
                  int n, const uint8_t *d_pool, uint64_t pool_len, void *d_out,
-                 int out_mode, float recon_r, int max_bitplanes);
+                 uint64_t out_elems, int out_mode, float recon_r, int max_bitplanes);
 
 /* Host helper: write into h_order a permutation of 0..n-1 sorted by
  * decreasing estimated work (passes x area, then codeword length). */
@@ -157,9 +161,10 @@ int tc_t1_sort_order(const tc_cblk_desc *h_desc, int n, uint32_t *h_order);
  * bit-planes is taken from the pass count.  Replaces Quantizer::dequantization
  * and the subband_dequantization_lossless/lossy kernels
  * (Quantizer.cpp:126-175, quantizer_*_inverse.cl:16-44), with the sign
- * handled (defect D4 fixed). */
+ * handled (defect D4 fixed).  d_raw and d_out each hold `elems` elements;
+ * blocks placed beyond them are skipped and reported, as in tc_t1_decode. */
 int tc_dequantize_raw(tc_ctx *ctx, const tc_cblk_desc *d_desc, int n,
-                      const uint32_t *d_raw, void *d_out, float recon_r);
+                      const uint32_t *d_raw, void *d_out, uint64_t elems, float recon_r);
 
 /* ---- DWT (DWTForward53/97, DWTReverse53/97, DWTKernel<T>::run) ----------- */
 

@@ -206,3 +206,43 @@ def test_gpu_encoder_flags_a_short_buffer(gpu_ctx):
     desc, plane, _ = _enc_blocks(seed=42, n=8)
     with pytest.raises(TCError):
         T1Encoder(gpu_ctx).encode(desc, torch.from_numpy(plane.reshape(-1)).cuda(), cap=16)
+
+
+def test_block_placed_past_the_output_is_skipped_and_reported(gpu_ctx):
+    """A caller-built descriptor whose block would run past the output
+    (out_off + (h-1)*out_pitch + w > out_elems) is skipped before any write
+    and reported; the other blocks decode as usual and the memory after the
+    output is untouched.  The same for the standalone dequantiser."""
+    from thousandthchicken_b200.stages import CoefficientCoder, Quantizer, _dev_bytes
+    desc, pool, _ = make_blocks(seed=61, n=24, mix="full", truncate=False)
+    n = len(desc)
+    elems = n * 4096
+    dev = torch.device("cuda")
+    want = _coder(gpu_ctx).decode_blocks(desc, pool, elems, recon_r=0.0).cpu().numpy()
+    bad = desc.copy()
+    bad["out_off"][5] = elems - 64 * 3          # three rows left, the block has 64
+    guard = 0x5A5A5A5A
+    buf = torch.full((elems + 8192,), guard, dtype=torch.int32, device=dev)
+    out = buf[:elems]
+    out[: n * 4096].zero_()
+    cc = CoefficientCoder(gpu_ctx)
+    d_desc = _dev_bytes(np.ascontiguousarray(bad, codec.DESC_DTYPE), dev)
+    d_pool = _dev_bytes(pool, dev)
+    cc.decode(d_desc, d_pool, out, n, None, raw=False, recon_r=0.0, max_bitplanes=16)
+    with pytest.raises(TCError) as ei:
+        gpu_ctx.synchronize()
+    assert ei.value.status == TC_E_CODESTREAM and "past the output" in str(ei.value)
+    got = buf.cpu().numpy()
+    assert (got[elems:] == guard).all()
+    keep = np.ones(elems, bool)
+    keep[5 * 4096: 6 * 4096] = False    # block 5's own slot stays as it was (zero)
+    np.testing.assert_array_equal(got[:elems][keep], want[keep])
+    assert (got[5 * 4096: 6 * 4096] == 0).all()
+    # the standalone dequantiser over raw words
+    raw = _coder(gpu_ctx).decode_blocks(desc, pool, elems, raw=True)
+    buf2 = torch.full((elems + 8192,), guard, dtype=torch.int32, device=dev)
+    Quantizer(gpu_ctx).dequantize(d_desc, n, raw, buf2[:elems], 0.0)
+    with pytest.raises(TCError):
+        gpu_ctx.synchronize()
+    assert (buf2[elems:].cpu().numpy() == guard).all()
+    gpu_ctx.synchronize()   # the error word was cleared by the report

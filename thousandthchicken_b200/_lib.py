@@ -100,9 +100,9 @@ _PROTOS = {
     "tc_ctx_t1_group": (_I, [_VP]),
     "tc_ctx_pool_bytes": (_I, [_VP, C.POINTER(C.c_size_t)]),
     "tc_ctx_trim": (_I, [_VP]),
-    "tc_t1_decode": (_I, [_VP, _VP, _VP, _I, _VP, C.c_uint64, _VP, _I, C.c_float, _I]),
+    "tc_t1_decode": (_I, [_VP, _VP, _VP, _I, _VP, C.c_uint64, _VP, C.c_uint64, _I, C.c_float, _I]),
     "tc_t1_sort_order": (_I, [_VP, _I, _VP]),
-    "tc_dequantize_raw": (_I, [_VP, _VP, _I, _VP, _VP, C.c_float]),
+    "tc_dequantize_raw": (_I, [_VP, _VP, _I, _VP, _VP, C.c_uint64, C.c_float]),
     "tc_dwt_forward53": (_I, [_VP, _VP, _I, _VP, _I, _I, _I, _I, _I]),
     "tc_dwt_forward97": (_I, [_VP, _VP, _I, _VP, _I, _I, _I, _I]),
     "tc_dwt_reverse53": (_I, [_VP, _VP, _I, _VP, _I, _I, _I, _I, _I]),

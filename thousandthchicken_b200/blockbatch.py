@@ -79,7 +79,7 @@ class BlockBatch:
         base = _ptr(self.d_desc)
         for (s, k), order in zip(self.geom["images"], self.image_orders):
             self.ctx.check(lib.tc_t1_decode(self.ctx.handle, base + s * DESC_DTYPE.itemsize, _ptr(order), k,
-                                            _ptr(self.pool), self.pool.numel(), _ptr(self.out),
+                                            _ptr(self.pool), self.pool.numel(), _ptr(self.out), self.out.numel(),
                                             L.TC_T1_OUT_DEQUANT, 0.0, self.max_bitplanes), "tc_t1_decode")
 
     def close(self):

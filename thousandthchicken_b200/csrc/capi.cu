@@ -628,7 +628,8 @@ static int plan_run(tc_plan *P, void *const *d_out, bool graph_mode = false)
                                       static_cast<uint32_t *>(P->order.ptr), P->ncblk, P->class_counts[0],
                                       P->class_counts[1], P->class_counts[2],
                                       static_cast<uint8_t *>(P->pool.ptr), graph_mode ? P->pool.size : P->pool_len,
-                                      P->coef.ptr, TC_T1_OUT_DEQUANT, P->recon_r, P->class_counts + 3);
+                                      P->coef.ptr, P->coef.size / 4, TC_T1_OUT_DEQUANT, P->recon_r,
+                                      P->class_counts + 3);
     if (e != cudaSuccess) return cuda_status(ctx, e, "Tier-1 launch");
     if (P->profiling) cudaEventRecord(P->ev[1], ctx->stream);
     if (graph_mode || plan_batched(P)) {
@@ -753,7 +754,8 @@ int tc_ctx_synchronize(tc_ctx *ctx)
     if (w) {
         cudaMemset(ctx->d_words, 0, sizeof w);
         return fail(ctx, TC_E_CODESTREAM,
-                    (w & TC_DERR_POOL)    ? "a code-block codeword runs past the segment pool"
+                    (w & TC_DERR_OUT)     ? "a code-block's place runs past the output (the block was skipped)"
+                    : (w & TC_DERR_POOL)  ? "a code-block codeword runs past the segment pool"
                     : (w & TC_DERR_STYLE) ? "a code-block style this launch does not decode, or a bad segment table"
                                           : "a code-block descriptor is out of range");
     }
@@ -796,7 +798,7 @@ int tc_ctx_trim(tc_ctx *ctx)
 }
 
 int tc_t1_decode(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint32_t *d_order, int n, const uint8_t *d_pool,
-                 uint64_t pool_len, void *d_out, int out_mode, float recon_r, int max_bitplanes)
+                 uint64_t pool_len, void *d_out, uint64_t out_elems, int out_mode, float recon_r, int max_bitplanes)
 {
     int rc = check_ctx(ctx);
     if (rc) return rc;
@@ -806,8 +808,8 @@ int tc_t1_decode(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint32_t *d_orde
         return fail(ctx, TC_E_ARG, "tc_t1_decode: bad argument");
     if (max_bitplanes <= 0 || max_bitplanes > 31) max_bitplanes = 31;
     return cuda_status(ctx,
-                       launch_t1_decode(ctx, d_desc, d_order, n, d_pool, pool_len, d_out, out_mode, recon_r,
-                                        max_bitplanes),
+                       launch_t1_decode(ctx, d_desc, d_order, n, d_pool, pool_len, d_out, out_elems, out_mode,
+                                        recon_r, max_bitplanes),
                        "tc_t1_decode");
 }
 
@@ -826,13 +828,13 @@ int tc_t1_sort_order(const tc_cblk_desc *h_desc, int n, uint32_t *h_order)
 }
 
 int tc_dequantize_raw(tc_ctx *ctx, const tc_cblk_desc *d_desc, int n, const uint32_t *d_raw, void *d_out,
-                      float recon_r)
+                      uint64_t elems, float recon_r)
 {
     int rc = check_ctx(ctx);
     if (rc) return rc;
     if (n < 0 || (n > 0 && (!d_desc || !d_raw || !d_out)) || !(recon_r >= 0.0f && recon_r < 1.0f))
         return fail(ctx, TC_E_ARG, "tc_dequantize_raw: bad argument");
-    return cuda_status(ctx, launch_dequant_raw(ctx, d_desc, n, d_raw, d_out, recon_r), "tc_dequantize_raw");
+    return cuda_status(ctx, launch_dequant_raw(ctx, d_desc, n, d_raw, d_out, elems, recon_r), "tc_dequantize_raw");
 }
 
 static int dwt_args_ok(const void *in, int ip, const void *out, int op, int w, int h, int levels)

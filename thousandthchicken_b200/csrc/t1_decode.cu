@@ -425,8 +425,9 @@ struct GroupCfg {
 template <typename MagT, int G, bool Modes = false>
 __device__ __forceinline__ void process_block(WarpState<MagT> &S, const Tables &T, const tc_cblk_desc *__restrict__ desc,
                                               uint32_t bi, int ndesc, const uint8_t *__restrict__ pool,
-                                              uint64_t pool_len, char *__restrict__ out, int out_mode, float recon_r,
-                                              uint32_t *__restrict__ err, int gl, unsigned gmask, int gshift)
+                                              uint64_t pool_len, char *__restrict__ out, uint64_t out_elems, int out_mode,
+                                              float recon_r, uint32_t *__restrict__ err, int gl, unsigned gmask,
+                                              int gshift)
 {
     if (bi >= (uint32_t)ndesc) {
         if (gl == 0) atomicOr(err, TC_DERR_DESC);
@@ -441,6 +442,12 @@ __device__ __forceinline__ void process_block(WarpState<MagT> &S, const Tables &
     const bool pool_ok = d.seg_off <= pool_len && (uint64_t)d.seg_len <= pool_len - d.seg_off;
     if (!geom_ok) {
         if (gl == 0) atomicOr(err, TC_DERR_DESC);
+        return;
+    }
+    // the block's last sample, out_off + (h-1) * out_pitch + w - 1, must lie
+    // inside the output; a block that does not is skipped before any write
+    if (d.out_off > out_elems || (uint64_t)(h - 1) * d.out_pitch + (uint64_t)w > out_elems - d.out_off) {
+        if (gl == 0) atomicOr(err, TC_DERR_OUT);
         return;
     }
     if (!ok || !pool_ok) {
@@ -554,8 +561,8 @@ struct HeavyQueue {
 template <typename MagT, int G, bool Modes = false>
 __global__ void __launch_bounds__(32 * GroupCfg<MagT, G>::warps)
 t1_decode_kernel(const tc_cblk_desc *__restrict__ desc, const uint32_t *__restrict__ order, int n, int ndesc,
-                 const uint8_t *__restrict__ pool, uint64_t pool_len, char *__restrict__ out, int out_mode,
-                 float recon_r, uint32_t *__restrict__ counter, uint32_t *__restrict__ err, HeavyQueue heavy)
+                 const uint8_t *__restrict__ pool, uint64_t pool_len, char *__restrict__ out, uint64_t out_elems,
+                 int out_mode, float recon_r, uint32_t *__restrict__ counter, uint32_t *__restrict__ err, HeavyQueue heavy)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     Tables &T = *reinterpret_cast<Tables *>(smem);
@@ -582,7 +589,7 @@ t1_decode_kernel(const tc_cblk_desc *__restrict__ desc, const uint32_t *__restri
                 idx = __shfl_sync(0xffffffffu, idx, 0);
                 if (idx >= heavy.n) break;
                 process_block<uint16_t, 32, Modes>(HS, T, desc, heavy.order[idx], ndesc, pool, pool_len, out,
-                                                   out_mode, recon_r, err, gl, gmask, gshift);
+                                                   out_elems, out_mode, recon_r, err, gl, gmask, gshift);
             }
         }
     }
@@ -593,14 +600,14 @@ t1_decode_kernel(const tc_cblk_desc *__restrict__ desc, const uint32_t *__restri
         idx = __shfl_sync(gmask, idx, gshift);
         if (idx >= n) break;
         const uint32_t bi = order ? order[idx] : (uint32_t)idx;
-        process_block<MagT, G, Modes>(S, T, desc, bi, ndesc, pool, pool_len, out, out_mode, recon_r, err, gl,
+        process_block<MagT, G, Modes>(S, T, desc, bi, ndesc, pool, pool_len, out, out_elems, out_mode, recon_r, err, gl,
                                       gmask, gshift);
     }
 }
 
 // Standalone inverse quantiser over raw sign-magnitude words.
 __global__ void dequant_raw_kernel(const tc_cblk_desc *__restrict__ desc, int n,
-                                   const uint32_t *__restrict__ raw, char *__restrict__ out,
+                                   const uint32_t *__restrict__ raw, char *__restrict__ out, uint64_t elems,
                                    float recon_r, uint32_t *words, bool base16)
 {
     const int b = blockIdx.x;
@@ -608,6 +615,11 @@ __global__ void dequant_raw_kernel(const tc_cblk_desc *__restrict__ desc, int n,
     const tc_cblk_desc d = desc[b];
     if (d.w < 1 || d.w > 64 || d.h < 1 || d.h > 64 || d.mb < 1 || d.mb > 31) {
         if (threadIdx.x == 0) atomicOr(&words[0], TC_DERR_DESC);
+        return;
+    }
+    // raw words and output share the block's place: both hold `elems`
+    if (d.out_off > elems || (uint64_t)(d.h - 1) * d.out_pitch + (uint64_t)d.w > elems - d.out_off) {
+        if (threadIdx.x == 0) atomicOr(&words[0], TC_DERR_OUT);
         return;
     }
     const int numbps = (int)d.mb - (int)d.zero_bitplanes;
@@ -684,7 +696,7 @@ cudaError_t class_cfg(tc_ctx *ctx, LaunchCfg **out)
 // work counter d_words[slot] (zeroed beforehand).
 template <typename MagT, int G, bool Modes = false>
 cudaError_t launch_class(tc_ctx *ctx, cudaStream_t stream, const tc_cblk_desc *d_desc, const uint32_t *d_order,
-                         int n, int ndesc, const uint8_t *d_pool, uint64_t pool_len, void *d_out, int out_mode,
+                         int n, int ndesc, const uint8_t *d_pool, uint64_t pool_len, void *d_out, uint64_t out_elems, int out_mode,
                          float recon_r, int slot, const HeavyQueue &heavy = HeavyQueue())
 {
     LaunchCfg *C = nullptr;
@@ -693,7 +705,7 @@ cudaError_t launch_class(tc_ctx *ctx, cudaStream_t stream, const tc_cblk_desc *d
     const int want = std::max((n + C->per_cta - 1) / C->per_cta, heavy.ctas);
     const int grid = std::max(1, std::min(want, C->per_sm * num_sms(ctx->device)));
     t1_decode_kernel<MagT, G, Modes><<<grid, 32 * GroupCfg<MagT, G>::warps, C->smem, stream>>>(
-        d_desc, d_order, n, ndesc, d_pool, pool_len, static_cast<char *>(d_out), out_mode, recon_r,
+        d_desc, d_order, n, ndesc, d_pool, pool_len, static_cast<char *>(d_out), out_elems, out_mode, recon_r,
         ctx->d_words + slot, ctx->d_words, heavy);
     ctx->launches++;
     return cudaGetLastError();
@@ -701,18 +713,18 @@ cudaError_t launch_class(tc_ctx *ctx, cudaStream_t stream, const tc_cblk_desc *d
 
 template <typename MagT>
 cudaError_t launch_class_g(tc_ctx *ctx, cudaStream_t stream, const tc_cblk_desc *d_desc, const uint32_t *d_order,
-                           int n, int ndesc, const uint8_t *d_pool, uint64_t pool_len, void *d_out, int out_mode,
+                           int n, int ndesc, const uint8_t *d_pool, uint64_t pool_len, void *d_out, uint64_t out_elems, int out_mode,
                            float recon_r, int slot)
 {
     switch (ctx->t1_group) {
     case 8:
-        return launch_class<MagT, 8>(ctx, stream, d_desc, d_order, n, ndesc, d_pool, pool_len, d_out, out_mode,
+        return launch_class<MagT, 8>(ctx, stream, d_desc, d_order, n, ndesc, d_pool, pool_len, d_out, out_elems, out_mode,
                                      recon_r, slot);
     case 16:
-        return launch_class<MagT, 16>(ctx, stream, d_desc, d_order, n, ndesc, d_pool, pool_len, d_out, out_mode,
+        return launch_class<MagT, 16>(ctx, stream, d_desc, d_order, n, ndesc, d_pool, pool_len, d_out, out_elems, out_mode,
                                       recon_r, slot);
     default:
-        return launch_class<MagT, 32>(ctx, stream, d_desc, d_order, n, ndesc, d_pool, pool_len, d_out, out_mode,
+        return launch_class<MagT, 32>(ctx, stream, d_desc, d_order, n, ndesc, d_pool, pool_len, d_out, out_elems, out_mode,
                                       recon_r, slot);
     }
 }
@@ -725,18 +737,18 @@ constexpr int kMaxHeavy = 148;
 }  // namespace
 
 cudaError_t launch_t1_decode(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint32_t *d_order, int n,
-                             const uint8_t *d_pool, uint64_t pool_len, void *d_out, int out_mode, float recon_r,
+                             const uint8_t *d_pool, uint64_t pool_len, void *d_out, uint64_t out_elems, int out_mode, float recon_r,
                              int max_bitplanes)
 {
     if (out_mode & TC_T1_STYLED) {
         const int s[3] = {max_bitplanes <= 8 ? n : 0, max_bitplanes > 8 && max_bitplanes <= 16 ? n : 0,
                           max_bitplanes > 16 ? n : 0};
-        return launch_t1_classes(ctx, d_desc, d_order, n, 0, 0, 0, d_pool, pool_len, d_out, out_mode & ~TC_T1_STYLED,
+        return launch_t1_classes(ctx, d_desc, d_order, n, 0, 0, 0, d_pool, pool_len, d_out, out_elems, out_mode & ~TC_T1_STYLED,
                                  recon_r, s);
     }
     return launch_t1_classes(ctx, d_desc, d_order, n, max_bitplanes <= 8 ? n : 0,
                              max_bitplanes > 8 && max_bitplanes <= 16 ? n : 0, max_bitplanes > 16 ? n : 0, d_pool,
-                             pool_len, d_out, out_mode, recon_r);
+                             pool_len, d_out, out_elems, out_mode, recon_r);
 }
 
 // Classes: blocks of <= 8, <= 16 and <= 31 coded bit-planes, in that order in
@@ -749,7 +761,7 @@ cudaError_t launch_t1_decode(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint
 // three widths: nstyled[0..2]) run in Modes launches on the context's stream.
 cudaError_t launch_t1_classes(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint32_t *d_order, int ndesc,
                               int n8, int n16, int n32, const uint8_t *d_pool, uint64_t pool_len, void *d_out,
-                              int out_mode, float recon_r, const int *nstyled)
+                              uint64_t out_elems, int out_mode, float recon_r, const int *nstyled)
 {
     int ns8 = nstyled ? nstyled[0] : 0, ns16 = nstyled ? nstyled[1] : 0, ns32 = nstyled ? nstyled[2] : 0;
     if (n8 + n16 + n32 + ns8 + ns16 + ns32 == 0) return cudaSuccess;
@@ -780,12 +792,12 @@ cudaError_t launch_t1_classes(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uin
         }
         if (ns32 > 0)
             e = launch_class<uint32_t, 32, true>(ctx, w32, d_desc, os ? os + ns8 + ns16 : nullptr, ns32, ndesc, d_pool,
-                                                 pool_len, d_out, out_mode, recon_r, 6);
+                                                 pool_len, d_out, out_elems, out_mode, recon_r, 6);
         if (e == cudaSuccess && ns16 > 0)
             e = launch_class<uint16_t, 32, true>(ctx, w16, d_desc, os ? os + ns8 : nullptr, ns16, ndesc, d_pool,
-                                                 pool_len, d_out, out_mode, recon_r, 5);
+                                                 pool_len, d_out, out_elems, out_mode, recon_r, 5);
         if (e == cudaSuccess && ns8 > 0)
-            e = launch_class<uint8_t, 32, true>(ctx, w8, d_desc, os, ns8, ndesc, d_pool, pool_len, d_out, out_mode,
+            e = launch_class<uint8_t, 32, true>(ctx, w8, d_desc, os, ns8, ndesc, d_pool, pool_len, d_out, out_elems, out_mode,
                                                 recon_r, 4, sheavy);
         if (nl > 1) {
             for (int i = 0; i < 2; i++) {
@@ -823,17 +835,17 @@ cudaError_t launch_t1_classes(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uin
         s16 = ctx->side[1];
     }
     if (n32 > 0)
-        e = launch_class_g<uint32_t>(ctx, s32, d_desc, o32, n32, ndesc, d_pool, pool_len, d_out, out_mode,
+        e = launch_class_g<uint32_t>(ctx, s32, d_desc, o32, n32, ndesc, d_pool, pool_len, d_out, out_elems, out_mode,
                                      recon_r, 3);
     if (e == cudaSuccess && n16 > 0)
-        e = launch_class_g<uint16_t>(ctx, s16, d_desc, o16, n16, ndesc, d_pool, pool_len, d_out, out_mode,
+        e = launch_class_g<uint16_t>(ctx, s16, d_desc, o16, n16, ndesc, d_pool, pool_len, d_out, out_elems, out_mode,
                                      recon_r, 2);
     if (e == cudaSuccess && n8 > 0) {
         if (heavy.n > 0)
-            e = launch_class<uint8_t, 32>(ctx, s8, d_desc, d_order, n8, ndesc, d_pool, pool_len, d_out, out_mode,
+            e = launch_class<uint8_t, 32>(ctx, s8, d_desc, d_order, n8, ndesc, d_pool, pool_len, d_out, out_elems, out_mode,
                                           recon_r, 1, heavy);
         else
-            e = launch_class_g<uint8_t>(ctx, s8, d_desc, d_order, n8, ndesc, d_pool, pool_len, d_out, out_mode,
+            e = launch_class_g<uint8_t>(ctx, s8, d_desc, d_order, n8, ndesc, d_pool, pool_len, d_out, out_elems, out_mode,
                                         recon_r, 1);
     }
     if (nlaunch > 1) {
@@ -847,11 +859,11 @@ cudaError_t launch_t1_classes(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uin
 }
 
 cudaError_t launch_dequant_raw(tc_ctx *ctx, const tc_cblk_desc *d_desc, int n, const uint32_t *d_raw,
-                               void *d_out, float recon_r)
+                               void *d_out, uint64_t elems, float recon_r)
 {
     if (n <= 0) return cudaSuccess;
     const bool base16 = ((reinterpret_cast<uintptr_t>(d_raw) | reinterpret_cast<uintptr_t>(d_out)) & 15) == 0;
-    dequant_raw_kernel<<<n, 256, 0, ctx->stream>>>(d_desc, n, d_raw, static_cast<char *>(d_out), recon_r,
+    dequant_raw_kernel<<<n, 256, 0, ctx->stream>>>(d_desc, n, d_raw, static_cast<char *>(d_out), elems, recon_r,
                                                    ctx->d_words, base16);
     ctx->launches++;
     return cudaGetLastError();

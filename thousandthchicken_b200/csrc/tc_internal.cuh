@@ -15,6 +15,7 @@
 #define TC_DERR_DESC 0x1u     // a code-block descriptor was out of range
 #define TC_DERR_POOL 0x2u     // a codeword ran past the segment pool
 #define TC_DERR_STYLE 0x4u    // a styled code-block reached a style-0 launch, or its segment table is bad
+#define TC_DERR_OUT 0x8u      // a code-block's place ran past the output (block skipped, nothing written)
 
 namespace tc {
 
@@ -159,19 +160,19 @@ int cuda_status(tc_ctx *ctx, cudaError_t e, const char *what);
 // max_bitplanes (selects the magnitude storage width: 8, 16 or 32 bits).
 cudaError_t launch_t1_decode(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint32_t *d_order,
                              int n, const uint8_t *d_pool, uint64_t pool_len, void *d_out,
-                             int out_mode, float recon_r, int max_bitplanes);
+                             uint64_t out_elems, int out_mode, float recon_r, int max_bitplanes);
 // Persistent launches over an order array partitioned into blocks of at
 // most 8, 16 and 31 coded bit-planes (n8 + n16 + n32 entries), then blocks
 // with a code-block style in the same three widths (nstyled[0..2], or none).
 cudaError_t launch_t1_classes(tc_ctx *ctx, const tc_cblk_desc *d_desc, const uint32_t *d_order,
                               int ndesc, int n8, int n16, int n32, const uint8_t *d_pool,
-                              uint64_t pool_len, void *d_out, int out_mode, float recon_r,
-                              const int *nstyled = nullptr);
+                              uint64_t pool_len, void *d_out, uint64_t out_elems, int out_mode,
+                              float recon_r, const int *nstyled = nullptr);
 // Host: order longest-first within each class (<= 8, <= 16, <= 31 coded
 // bit-planes, then styled blocks of <= 8, <= 16, <= 31); class sizes out.
 void t1_class_order(const tc_cblk_desc *h_desc, int n, uint32_t *h_order, int counts[6]);
 cudaError_t launch_dequant_raw(tc_ctx *ctx, const tc_cblk_desc *d_desc, int n,
-                               const uint32_t *d_raw, void *d_out, float recon_r);
+                               const uint32_t *d_raw, void *d_out, uint64_t elems, float recon_r);
 cudaError_t launch_t1_encode(tc_ctx *ctx, const tc_t1_enc_desc *d_desc, int n, const void *d_in, uint8_t *d_out,
                              uint32_t cap, tc_t1_enc_result *d_res);
 // Packs n codewords (block k: res[k].len bytes at src + k * cap) to dst + off[k].

@@ -96,8 +96,8 @@ class CoefficientCoder:
         mode = (L.TC_T1_OUT_RAW if raw else L.TC_T1_OUT_DEQUANT) | (L.TC_T1_STYLED if styled else 0)
         self.ctx.check(L.lib().tc_t1_decode(self.ctx.handle, _ptr(desc_dev),
                                             _ptr(order_dev) if order_dev is not None else None, n,
-                                            _ptr(pool_dev), pool_dev.numel(), _ptr(out), mode, recon_r,
-                                            max_bitplanes),
+                                            _ptr(pool_dev), pool_dev.numel(), _ptr(out),
+                                            out.numel() * out.element_size() // 4, mode, recon_r, max_bitplanes),
                        "tc_t1_decode")
 
     def decode_blocks(self, desc: np.ndarray, pool: np.ndarray, out_elems: int, raw: bool = False,
@@ -196,8 +196,9 @@ class Quantizer:
         self.ctx = ctx
 
     def dequantize(self, desc_dev, n: int, raw, out, recon_r: float = 0.5):
+        elems = min(raw.numel() * raw.element_size(), out.numel() * out.element_size()) // 4
         self.ctx.check(L.lib().tc_dequantize_raw(self.ctx.handle, _ptr(desc_dev), n, _ptr(raw), _ptr(out),
-                                                 recon_r), "tc_dequantize_raw")
+                                                 elems, recon_r), "tc_dequantize_raw")
 
 
 class _DWTKernel:
