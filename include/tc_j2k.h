@@ -71,6 +71,8 @@ uint64_t tc_ctx_launch_count(const tc_ctx *ctx);
  * and caches the choice.  Default 32. */
 int tc_ctx_set_t1_group(tc_ctx *ctx, int lanes);
 int tc_ctx_t1_group(const tc_ctx *ctx);
+/* The CUDA stream (cudaStream_t) the ctx issues its work on. */
+void *tc_ctx_stream(const tc_ctx *ctx);
 /* Device memory the ctx's memory pool reserves now: the buffers of its
  * plans plus freed blocks the pool keeps mapped for regrowth.  A serving
  * loop admits work against it.  No counterpart in the reference. */

@@ -1,0 +1,95 @@
+"""The reference-named C++ classes of include/tc_j2k.hpp (CoefficientCoder,
+Quantizer, DWTKernel<T> / DWTForward53/97 / DWTReverse53/97, DWT,
+Preprocessor, Decoder): they compile against the reference's own
+codestream_image_types.h (when its tree is present) and link against
+libtc_j2k.so (CPU), and a C++ program driving decode_tile ->
+dequantize_tile -> iwt -> colour over a decode tree decodes images to the
+same samples as the C ABI's Decoder (GPU)."""
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, synth_image
+from thousandthchicken_b200 import codec
+
+REF_TREE = Path(os.environ.get("TC_REFERENCE_TREE", "/root/reference/ThousandthChicken"))
+PKG = ROOT / "thousandthchicken_b200"
+CUDA_INC = "/usr/local/cuda/include"
+CUDA_LIB = "/usr/local/cuda/lib64"
+
+
+def _gxx(src, out, extra=()):
+    cmd = ["g++", "-std=c++17", "-O1", "-Wall", f"-I{ROOT / 'include'}", f"-I{CUDA_INC}", *extra, str(src), "-o",
+           str(out), f"-L{PKG}", "-ltc_j2k", f"-L{CUDA_LIB}", "-lcudart", f"-Wl,-rpath,{PKG}"]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    assert res.returncode == 0, res.stderr
+    return out
+
+
+def test_classes_compile_and_link(tmp_path):
+    _gxx(ROOT / "tests" / "cpp" / "ref_classes.cpp", tmp_path / "ref_classes")
+
+
+def test_classes_compile_against_reference_types(tmp_path):
+    if not (REF_TREE / "codestream_image_types.h").exists():
+        pytest.skip("reference tree not present")
+    src = tmp_path / "ref_types.cpp"
+    src.write_text('''
+#include "codestream_image_types.h"
+#include "tc_j2k.hpp"
+void drive(tc_ctx *ctx, type_image *img) {
+    tc::CoefficientCoder coder(ctx);
+    tc::Quantizer quant(ctx);
+    tc::DWT dwt(ctx);
+    tc::Preprocessor pre(ctx);
+    coder.decode_tile(&img->tile[0]);
+    quant.dequantize_tile(&img->tile[0]);
+    dwt.iwt(&img->tile[0]);
+    if (img->wavelet_type) pre.color_decoder_lossy(img); else pre.color_decoder_lossless(img);
+    pre.idc_level_shifting(img);
+    tc::DWTForward53 f53(ctx); tc::DWTForward97 f97(ctx); tc::DWTReverse53 r53(ctx); tc::DWTReverse97 r97(ctx);
+    tc::DWTKernel<int> &k = r53; (void)k; (void)f53; (void)f97; (void)r97;
+    tc::Decoder dec(ctx);
+    (void)dec.decode(std::string("missing.j2k"));
+}
+int main() { return 0; }
+''')
+    _gxx(src, tmp_path / "ref_types", extra=(f"-I{REF_TREE}",))
+
+
+def _write_input(path, cs):
+    info, desc, pool = codec.parse(cs)
+    W, H, C = info["width"], info["height"], info["ncomp"]
+    hdr = np.array([W, H, C, info["bits"], info["levels"], info["reversible"], info["mct"], len(desc), len(pool)],
+                   np.int32)
+    rec = np.zeros(len(desc), np.dtype([("i", "<i4", (11,)), ("step", "<f4")]))
+    comp, rem = np.divmod(desc["out_off"].astype(np.int64), W * H)
+    y, x = np.divmod(rem, W)
+    sig = desc["mb"].astype(np.int32) - desc["zero_bitplanes"].astype(np.int32)
+    rec["i"] = np.stack([comp, x, y, desc["w"], desc["h"], desc["seg_off"], desc["seg_len"], sig, desc["passes"],
+                         desc["mb"], desc["orient"]], axis=1).astype(np.int32)
+    rec["step"] = desc["step"]
+    with open(path, "wb") as f:
+        f.write(hdr.tobytes())
+        f.write(rec.tobytes())
+        f.write(np.ascontiguousarray(pool, np.uint8).tobytes())
+    return W, H, C
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("rev,comps,bits", [(True, 3, 8), (False, 3, 8), (True, 1, 12), (False, 1, 8)])
+def test_classes_decode_like_the_c_abi(gpu_ctx, tmp_path, rev, comps, bits):
+    from thousandthchicken_b200.stages import Decoder
+    exe = _gxx(ROOT / "tests" / "cpp" / "ref_classes.cpp", tmp_path / "ref_classes")
+    img = synth_image(203, 141, comps, bits, seed=comps + bits)
+    cs = codec.encode(img, bits, levels=4, reversible=rev, mct=comps == 3, base_step=1 / 64)
+    W, H, C = _write_input(tmp_path / "in.bin", cs)
+    res = subprocess.run([str(exe), str(tmp_path / "in.bin"), str(tmp_path / "out.bin")], capture_output=True,
+                         text=True, timeout=120)
+    assert res.returncode == 0, res.stderr
+    got = np.fromfile(tmp_path / "out.bin", np.int32).reshape(C, H, W)
+    want = Decoder(gpu_ctx).decode(cs).astype(np.int32)
+    np.testing.assert_array_equal(got, want)

@@ -100,6 +100,7 @@ _PROTOS = {
     "tc_ctx_t1_group": (_I, [_VP]),
     "tc_ctx_pool_bytes": (_I, [_VP, C.POINTER(C.c_size_t)]),
     "tc_ctx_trim": (_I, [_VP]),
+    "tc_ctx_stream": (_VP, [_VP]),
     "tc_t1_decode": (_I, [_VP, _VP, _VP, _I, _VP, C.c_uint64, _VP, C.c_uint64, _I, C.c_float, _I]),
     "tc_t1_sort_order": (_I, [_VP, _I, _VP]),
     "tc_dequantize_raw": (_I, [_VP, _VP, _I, _VP, _VP, C.c_uint64, C.c_float]),

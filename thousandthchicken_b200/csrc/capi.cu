@@ -775,6 +775,8 @@ int tc_ctx_set_t1_group(tc_ctx *ctx, int lanes)
 
 int tc_ctx_t1_group(const tc_ctx *ctx) { return ctx ? ctx->t1_group : TC_E_ARG; }
 
+void *tc_ctx_stream(const tc_ctx *ctx) { return ctx ? static_cast<void *>(ctx->stream) : nullptr; }
+
 int tc_ctx_pool_bytes(tc_ctx *ctx, size_t *reserved)
 {
     if (!ctx || !reserved) return TC_E_ARG;
