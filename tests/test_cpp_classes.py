@@ -92,4 +92,10 @@ def test_classes_decode_like_the_c_abi(gpu_ctx, tmp_path, rev, comps, bits):
     assert res.returncode == 0, res.stderr
     got = np.fromfile(tmp_path / "out.bin", np.int32).reshape(C, H, W)
     want = Decoder(gpu_ctx).decode(cs).astype(np.int32)
-    np.testing.assert_array_equal(got, want)
+    if rev:
+        np.testing.assert_array_equal(got, want)
+    else:
+        # separate stages (standalone dequantiser, plane DWT, colour kernel)
+        # round in other places than the fused decode: within 1 of it
+        d = np.abs(got - want)
+        assert d.max() <= 1 and (d > 0).mean() < 1e-3
