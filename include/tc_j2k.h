@@ -71,6 +71,16 @@ uint64_t tc_ctx_launch_count(const tc_ctx *ctx);
  * and caches the choice.  Default 32. */
 int tc_ctx_set_t1_group(tc_ctx *ctx, int lanes);
 int tc_ctx_t1_group(const tc_ctx *ctx);
+/* How the fused last reverse 9/7 level of three-component images stages
+ * its subband tiles: TC_DWT_TMA (default) with 2-D tensor copies (TMA) on
+ * an mbarrier, where the level's band width, row pitches and addresses are
+ * multiples of 16 bytes (others fall back), or TC_DWT_CPASYNC with one
+ * 4-byte asynchronous copy per sample.  Same results either way; the
+ * package's autotuner times both per shape bucket. */
+#define TC_DWT_CPASYNC 0
+#define TC_DWT_TMA     1
+int tc_ctx_set_dwt_variant(tc_ctx *ctx, int variant);
+int tc_ctx_dwt_variant(const tc_ctx *ctx);
 /* The CUDA stream (cudaStream_t) the ctx issues its work on. */
 void *tc_ctx_stream(const tc_ctx *ctx);
 /* Device memory the ctx's memory pool reserves now: the buffers of its

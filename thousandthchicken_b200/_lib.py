@@ -26,6 +26,7 @@ TC_CBLK_IRREVERSIBLE = 1
 TC_T1_OUT_DEQUANT, TC_T1_OUT_RAW, TC_T1_STYLED = 0, 1, 0x10
 TC_ROUND_FLOOR, TC_ROUND_TRUNC = 0, 1
 TC_COLOR_DC, TC_COLOR_RCT, TC_COLOR_ICT = 0, 1, 2
+TC_DWT_CPASYNC, TC_DWT_TMA = 0, 1
 
 
 class LibraryMissing(RuntimeError):
@@ -98,6 +99,8 @@ _PROTOS = {
     "tc_ctx_launch_count": (C.c_uint64, [_VP]),
     "tc_ctx_set_t1_group": (_I, [_VP, _I]),
     "tc_ctx_t1_group": (_I, [_VP]),
+    "tc_ctx_set_dwt_variant": (_I, [_VP, _I]),
+    "tc_ctx_dwt_variant": (_I, [_VP]),
     "tc_ctx_pool_bytes": (_I, [_VP, C.POINTER(C.c_size_t)]),
     "tc_ctx_trim": (_I, [_VP]),
     "tc_ctx_stream": (_VP, [_VP]),

@@ -753,8 +753,9 @@ int tc_ctx_synchronize(tc_ctx *ctx)
     if (e != cudaSuccess) return cuda_status(ctx, e, "read device error word");
     if (w) {
         cudaMemset(ctx->d_words, 0, sizeof w);
-        return fail(ctx, TC_E_CODESTREAM,
-                    (w & TC_DERR_OUT)     ? "a code-block's place runs past the output (the block was skipped)"
+        return fail(ctx, (w & TC_DERR_TIMEOUT) ? TC_E_TIMEOUT : TC_E_CODESTREAM,
+                    (w & TC_DERR_TIMEOUT) ? "a bounded device wait for a TMA copy gave up"
+                    : (w & TC_DERR_OUT)   ? "a code-block's place runs past the output (the block was skipped)"
                     : (w & TC_DERR_POOL)  ? "a code-block codeword runs past the segment pool"
                     : (w & TC_DERR_STYLE) ? "a code-block style this launch does not decode, or a bad segment table"
                                           : "a code-block descriptor is out of range");
@@ -774,6 +775,15 @@ int tc_ctx_set_t1_group(tc_ctx *ctx, int lanes)
 }
 
 int tc_ctx_t1_group(const tc_ctx *ctx) { return ctx ? ctx->t1_group : TC_E_ARG; }
+
+int tc_ctx_set_dwt_variant(tc_ctx *ctx, int variant)
+{
+    if (!ctx || (variant != TC_DWT_CPASYNC && variant != TC_DWT_TMA)) return TC_E_ARG;
+    ctx->dwt_variant = variant;
+    return TC_OK;
+}
+
+int tc_ctx_dwt_variant(const tc_ctx *ctx) { return ctx ? ctx->dwt_variant : TC_E_ARG; }
 
 void *tc_ctx_stream(const tc_ctx *ctx) { return ctx ? static_cast<void *>(ctx->stream) : nullptr; }
 

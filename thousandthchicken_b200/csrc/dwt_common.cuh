@@ -2,10 +2,41 @@
 // symmetric extension (ISO F.3.7) and the lifting constants and roundings.
 #pragma once
 
+#include <cuda_runtime.h>
+
 #include "tc_j2k.h"
 
 namespace tc {
 namespace dwt {
+
+// Programmatic dependent launch between the reverse levels: a level's grid
+// lets the next level's grid be scheduled once all its CTAs have started
+// (launch_dependents), and a level waits for the previous one to complete
+// and flush before it reads that level's output (wait).  Without a
+// programmatic predecessor the wait returns at once.
+__device__ __forceinline__ void pdl_allow_next() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait_prev() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+// Launches kernel<<<grid, block, smem, stream>>>(args...) with programmatic
+// stream serialisation allowed, so its CTAs may be scheduled while the
+// previous kernel on the stream finishes (the kernel must pdl_wait_prev()
+// before it reads what that kernel wrote).
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
+                       Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
 
 __device__ __forceinline__ int pse(int i, int n)
 {

@@ -314,6 +314,8 @@ __device__ __forceinline__ void rev_tile(const LevelIO &io, int bits, int bx, in
 template <typename T, int WAVELET, int RND, int NCOMP, int COLOR, typename OT>
 __global__ void __launch_bounds__(kThreads) idwt_rev_kernel(LevelIO io, int bits)
 {
+    pdl_allow_next();
+    pdl_wait_prev();
     rev_tile<T, WAVELET, RND, NCOMP, COLOR, OT>(io, bits, blockIdx.x, blockIdx.y, COLOR < 0 ? blockIdx.z : 0);
 }
 
@@ -325,8 +327,9 @@ template <typename T, int WAVELET, int RND, int NCOMP, int COLOR, typename OT>
 __global__ void __launch_bounds__(kThreads) idwt_rev_batch_kernel(const RevJob *__restrict__ jobs, int njobs,
                                                                   int bits)
 {
+    pdl_allow_next();
     const int b = blockIdx.x;
-    int lo = 0, hi = njobs - 1;
+    int lo = 0, hi = njobs - 1;   // the job table is written by the host before any level runs
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
         if (jobs[mid].tile0 <= b) lo = mid;
@@ -334,6 +337,7 @@ __global__ void __launch_bounds__(kThreads) idwt_rev_batch_kernel(const RevJob *
     }
     const RevJob &J = jobs[lo];
     const int t = b - J.tile0;
+    pdl_wait_prev();
     rev_tile<T, WAVELET, RND, NCOMP, COLOR, OT>(J.io, bits, t % J.tiles_x, t / J.tiles_x, 0);
 }
 
@@ -364,15 +368,18 @@ cudaError_t run_rev(tc_ctx *ctx, const RevLaunch &L, int bits)
             return e;
         const LevelIO &io = *L.io;
         dim3 grid((io.w + G::TX - 1) / G::TX, (io.h + G::TY - 1) / G::TY, COLOR < 0 ? io.ncomp : 1);
-        idwt_rev_kernel<T, WAVELET, RND, NCOMP, COLOR, OT><<<grid, kThreads, smem, ctx->stream>>>(io, bits);
+        if ((e = launch_pdl(idwt_rev_kernel<T, WAVELET, RND, NCOMP, COLOR, OT>, grid, dim3(kThreads), smem,
+                            ctx->stream, io, bits)) != cudaSuccess)
+            return e;
     } else {
         if (L.njobs <= 0 || L.ntiles <= 0) return cudaSuccess;
         static DeviceFlags attr;
         if ((e = set_smem_once(attr, ctx->device, idwt_rev_batch_kernel<T, WAVELET, RND, NCOMP, COLOR, OT>, smem)) !=
             cudaSuccess)
             return e;
-        idwt_rev_batch_kernel<T, WAVELET, RND, NCOMP, COLOR, OT>
-            <<<L.ntiles, kThreads, smem, ctx->stream>>>(L.jobs, L.njobs, bits);
+        if ((e = launch_pdl(idwt_rev_batch_kernel<T, WAVELET, RND, NCOMP, COLOR, OT>, dim3(L.ntiles),
+                            dim3(kThreads), smem, ctx->stream, L.jobs, L.njobs, bits)) != cudaSuccess)
+            return e;
     }
     ctx->launches++;
     return cudaGetLastError();
@@ -430,7 +437,11 @@ cudaError_t launch_idwt_last_color(tc_ctx *ctx, const LevelIO &io, int wavelet, 
 {
     if (io.w <= 0 || io.h <= 0) return cudaSuccess;
     if (color != TC_COLOR_DC && io.ncomp < 3) color = TC_COLOR_DC;
-    if (wavelet && rev97_handles(color, io.ncomp, out_type)) return launch_rev97_level(ctx, io, out_type, bits);
+    if (wavelet && rev97_handles(color, io.ncomp, out_type)) {
+        if (ctx->dwt_variant == TC_DWT_TMA && rev97_tma_handles(io, out_type))
+            return launch_rev97_tma(ctx, io, out_type, bits);
+        return launch_rev97_level(ctx, io, out_type, bits);
+    }
     RevLaunch L;
     L.io = &io;
     return last_level(ctx, L, io.ncomp, wavelet, color, out_type, bits);

@@ -288,6 +288,8 @@ __device__ __forceinline__ void ict_tile(const LevelIO &io, int bx, int by, int 
 template <typename OT>
 __global__ void __launch_bounds__(kThreads, 2) idwt97_ict_kernel(LevelIO io, int bits)
 {
+    pdl_allow_next();
+    pdl_wait_prev();
     ict_tile<OT>(io, blockIdx.x, blockIdx.y, bits);
 }
 
@@ -295,6 +297,7 @@ template <typename OT>
 __global__ void __launch_bounds__(kThreads, 2) idwt97_ict_batch_kernel(const RevJob *__restrict__ jobs, int njobs,
                                                                       int bits)
 {
+    pdl_allow_next();
     const int b = blockIdx.x;
     int lo = 0, hi = njobs - 1;
     while (lo < hi) {
@@ -304,6 +307,7 @@ __global__ void __launch_bounds__(kThreads, 2) idwt97_ict_batch_kernel(const Rev
     }
     const RevJob &J = jobs[lo];
     const int t = b - J.tile0;
+    pdl_wait_prev();
     ict_tile<OT>(J.io, t % J.tiles_x, t / J.tiles_x, bits);
 }
 
@@ -316,9 +320,9 @@ cudaError_t ict_level(tc_ctx *ctx, const LevelIO &io, int bits)
     cudaError_t e = set_smem_once(attr, ctx->device, idwt97_ict_kernel<OT>, kIctSmem);
     if (e != cudaSuccess) return e;
     dim3 grid((io.w + TX - 1) / TX, (io.h + TY - 1) / TY);
-    idwt97_ict_kernel<OT><<<grid, kThreads, kIctSmem, ctx->stream>>>(io, bits);
+    e = launch_pdl(idwt97_ict_kernel<OT>, grid, dim3(kThreads), kIctSmem, ctx->stream, io, bits);
     ctx->launches++;
-    return cudaGetLastError();
+    return e;
 }
 
 template <typename OT>
@@ -327,9 +331,10 @@ cudaError_t ict_batch(tc_ctx *ctx, const RevJob *jobs, int njobs, int ntiles, in
     static DeviceFlags attr;
     cudaError_t e = set_smem_once(attr, ctx->device, idwt97_ict_batch_kernel<OT>, kIctSmem);
     if (e != cudaSuccess) return e;
-    idwt97_ict_batch_kernel<OT><<<ntiles, kThreads, kIctSmem, ctx->stream>>>(jobs, njobs, bits);
+    e = launch_pdl(idwt97_ict_batch_kernel<OT>, dim3(ntiles), dim3(kThreads), kIctSmem, ctx->stream, jobs, njobs,
+                   bits);
     ctx->launches++;
-    return cudaGetLastError();
+    return e;
 }
 
 }  // namespace

@@ -16,6 +16,7 @@
 #define TC_DERR_POOL 0x2u     // a codeword ran past the segment pool
 #define TC_DERR_STYLE 0x4u    // a styled code-block reached a style-0 launch, or its segment table is bad
 #define TC_DERR_OUT 0x8u      // a code-block's place ran past the output (block skipped, nothing written)
+#define TC_DERR_TIMEOUT 0x10u // a bounded device wait (an mbarrier of a TMA copy) gave up
 
 namespace tc {
 
@@ -131,6 +132,7 @@ struct tc_ctx {
     cudaEvent_t jobs_uploaded = nullptr;
     uint64_t launches = 0;
     int t1_group = 32;            // lanes per code-block in the Tier-1 kernel (8, 16 or 32)
+    int dwt_variant = TC_DWT_TMA; // staging of the fused last reverse 9/7 level (TC_DWT_*)
     // side streams for concurrent Tier-1 class launches (created on first use)
     cudaStream_t side[2] = {nullptr, nullptr};
     cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
@@ -216,6 +218,11 @@ cudaError_t launch_fdwt_level(tc_ctx *ctx, const LevelIO &io, int wavelet, int r
 bool rev97_handles(int color, int ncomp, int out_type);
 cudaError_t launch_rev97_level(tc_ctx *ctx, const LevelIO &io, int out_type, int bits);
 cudaError_t launch_rev97_batch(tc_ctx *ctx, const RevJob *d_jobs, int njobs, int ntiles, int out_type, int bits);
+// The same last level with its subband tiles staged by TMA (dwt_tma.cu), for
+// levels whose band width, pitches and addresses suit 2-D tensor copies
+// (rev97_tma_handles).
+bool rev97_tma_handles(const LevelIO &io, int out_type);
+cudaError_t launch_rev97_tma(tc_ctx *ctx, const LevelIO &io, int out_type, int bits);
 
 // Last reverse level fused with the inverse colour transform, DC shift,
 // rounding and clamping; writes out_type samples (TC_U8/TC_U16/TC_INT32).
