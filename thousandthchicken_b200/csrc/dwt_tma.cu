@@ -31,6 +31,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <mutex>
 #include <type_traits>
@@ -245,86 +246,110 @@ __device__ __forceinline__ void extend_borders(float *comps, int x0, int y0, int
     __syncthreads();
 }
 
+// Thread 0: the twelve box copies of tile (bx, by) onto `bar`.
+__device__ __forceinline__ void issue_tile(const IctMaps &maps, float *comps, uint32_t bar, int bx, int by, int wl,
+                                           int hl)
+{
+    // order this CTA's earlier shared-memory accesses (generic proxy) before
+    // the copies' writes (async proxy) into the same buffer
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(bar, kTileBytes);
+    const int xl = bx * (TX / 2) - 4, yl = by * (TY / 2) - 2;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        const uint32_t base = smem_addr(comps + c * COMPF);
+        tma_load_2d(base + 0 * kBoxBytes, &maps.ll[c], xl, yl, bar);
+        tma_load_2d(base + 1 * kBoxBytes, &maps.coef[c], wl + xl, yl, bar);
+        tma_load_2d(base + 2 * kBoxBytes, &maps.coef[c], xl, hl + yl, bar);
+        tma_load_2d(base + 3 * kBoxBytes, &maps.coef[c], wl + xl, hl + yl, bar);
+    }
+}
+
+// Persistent CTAs (two per SM) walk the tiles t = blockIdx.x, blockIdx.x +
+// gridDim.x, ...  Once the vertical pass has read its columns into
+// registers the staging buffer is free, and thread 0 starts the next tile's
+// copies, which land while this tile is lifted, colour-transformed and
+// stored.
 template <typename OT>
 __global__ void __launch_bounds__(kThreads, 2)
-    idwt97_ict_tma_kernel(const __grid_constant__ IctMaps maps, TileArgs a, uint32_t *err)
+    idwt97_ict_tma_kernel(const __grid_constant__ IctMaps maps, TileArgs a, uint32_t *err, int ntx, int ntiles)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     float *comps = reinterpret_cast<float *>(smem_raw);
     const uint32_t bar = smem_addr(smem_raw + (size_t)3 * COMPF * 4);
     const int tid = threadIdx.x;
-    const int bx = blockIdx.x, by = blockIdx.y, x0 = bx * TX, y0 = by * TY;
     const int w = a.w, h = a.h, wl = (w + 1) >> 1, hl = (h + 1) >> 1;
+    float *Y = comps, *Cb = comps + COMPF, *Cr = comps + 2 * COMPF;
+    const int col = tid % TX, half = tid / TX;
+    const int vbase = half ? 32 - H : 0, obase = half ? OUTR : 0;
+    const int p = col & 1, j = (col >> 1) + 4;   // extended column col + 4
+    const float fa = sf_factor(0, p, true, true), fb = sf_factor(1, p, true, true);  // obase and y0 are even
+    const OutRange R = out_range(a.bits);
+    const bool sgn = a.bits & TC_SIGNED;
+    const float dc = (float)R.dc;
 
     pdl_allow_next();
     if (tid == 0) mbar_init(bar, 1);
     __syncthreads();
     pdl_wait_prev();   // the LL input is the previous level's output
-    if (tid == 0) {
-        mbar_expect_tx(bar, kTileBytes);
-        const int xl = x0 / 2 - 4, yl = y0 / 2 - 2;
-#pragma unroll
-        for (int c = 0; c < 3; c++) {
-            const uint32_t base = smem_addr(comps + c * COMPF);
-            tma_load_2d(base + 0 * kBoxBytes, &maps.ll[c], xl, yl, bar);
-            tma_load_2d(base + 1 * kBoxBytes, &maps.coef[c], wl + xl, yl, bar);
-            tma_load_2d(base + 2 * kBoxBytes, &maps.coef[c], xl, hl + yl, bar);
-            tma_load_2d(base + 3 * kBoxBytes, &maps.coef[c], wl + xl, hl + yl, bar);
+    int t = blockIdx.x;
+    if (t >= ntiles) return;
+    if (tid == 0) issue_tile(maps, comps, bar, t % ntx, t / ntx, wl, hl);
+    uint32_t phase = 0;
+    for (; t < ntiles; t += gridDim.x) {
+        const int bx = t % ntx, by = t / ntx, x0 = bx * TX, y0 = by * TY;
+        // every thread waits (bounded); all leave together if any gave up
+        const bool landed = mbar_wait(bar, phase);
+        if (__syncthreads_or(!landed)) {
+            if (tid == 0) atomicOr(err, TC_DERR_TIMEOUT);
+            return;
         }
-    }
-    // every thread waits (bounded); all leave together if any gave up
-    const bool landed = mbar_wait(bar, 0);
-    if (__syncthreads_or(!landed)) {
-        if (tid == 0) atomicOr(err, TC_DERR_TIMEOUT);
-        return;
-    }
-    const bool interior = x0 >= H && x0 + TX + H <= w && y0 >= H && y0 + NR - H <= h;
-    if (!interior) extend_borders(comps, x0, y0, w, h);
+        phase ^= 1u;
+        const bool interior = x0 >= H && x0 + TX + H <= w && y0 >= H && y0 + NR - H <= h;
+        if (!interior) extend_borders(comps, x0, y0, w, h);
+        hpass<true>(Y, Cb, tid & 63, tid >> 6);
+        hpass<false>(Cr, Cr, tid & 63, tid >> 6);
+        __syncthreads();
 
-    float *Y = comps, *Cb = comps + COMPF, *Cr = comps + 2 * COMPF;
-    hpass<true>(Y, Cb, tid & 63, tid >> 6);
-    hpass<false>(Cr, Cr, tid & 63, tid >> 6);
-    __syncthreads();
-
-    const int col = tid % TX, half = tid / TX;
-    const int vbase = half ? 32 - H : 0, obase = half ? OUTR : 0;
-    const int x = x0 + col, y = y0 + obase;
-    const int p = col & 1, j = (col >> 1) + 4;   // extended column col + 4
-    float2 yc[OUTR];
-    {
-        float2 v[VN];
+        float2 yc[OUTR];
+        {
+            float2 v[VN];
 #pragma unroll
-        for (int k = 0; k < VN; k++) v[k] = f2(band_row(Y, vbase + k, p)[j], band_row(Cb, vbase + k, p)[j]);
-        lift2<VN>(v);
+            for (int k = 0; k < VN; k++) v[k] = f2(band_row(Y, vbase + k, p)[j], band_row(Cb, vbase + k, p)[j]);
+            lift2<VN>(v);
 #pragma unroll
-        for (int r = 0; r < OUTR; r++) yc[r] = v[H + r];
-    }
-    float u[VN];
+            for (int r = 0; r < OUTR; r++) yc[r] = v[H + r];
+        }
+        float u[VN];
 #pragma unroll
-    for (int k = 0; k < VN; k++) u[k] = band_row(Cr, vbase + k, p)[j];
-    lift1<VN>(u);
-    if (x >= w) return;
-    const bool full = y + OUTR <= h;
-    const float fa = sf_factor(0, p, true, true), fb = sf_factor(1, p, true, true);  // obase and y0 are even
-    const OutRange R = out_range(a.bits);
-    const bool sgn = a.bits & TC_SIGNED;
-    const float dc = (float)R.dc;
-    const size_t o = (size_t)y * a.out_pitch + x;
-    OT *o0 = static_cast<OT *>(a.out[0]) + o, *o1 = static_cast<OT *>(a.out[1]) + o,
-       *o2 = static_cast<OT *>(a.out[2]) + o;
+        for (int k = 0; k < VN; k++) u[k] = band_row(Cr, vbase + k, p)[j];
+        __syncthreads();   // every read of this tile is done: the buffer takes the next one
+        if (tid == 0 && t + (int)gridDim.x < ntiles) {
+            const int tn = t + gridDim.x;
+            issue_tile(maps, comps, bar, tn % ntx, tn / ntx, wl, hl);
+        }
+        lift1<VN>(u);
+        const int x = x0 + col, y = y0 + obase;
+        if (x < w) {
+            const bool full = y + OUTR <= h;
+            const size_t o = (size_t)y * a.out_pitch + x;
+            OT *o0 = static_cast<OT *>(a.out[0]) + o, *o1 = static_cast<OT *>(a.out[1]) + o,
+               *o2 = static_cast<OT *>(a.out[2]) + o;
 #pragma unroll
-    for (int r = 0; r < OUTR; r++) {
-        if (!(full || y + r < h)) continue;
-        const float f = (r & 1) ? fb : fa;
-        const float Yv = yc[r].x, Cbv = yc[r].y, Crv = u[H + r];
-        const float yf = fmaf(f, Yv, dc);
-        const float Rc = fmaf(1.402f * f, Crv, yf);
-        const float Gc = fmaf(-0.71414f * f, Crv, fmaf(-0.34413f * f, Cbv, yf));
-        const float B = fmaf(1.772f * f, Cbv, yf);
-        const size_t ro = (size_t)r * a.out_pitch;
-        o0[ro] = to_out<OT>(Rc, R, sgn);
-        o1[ro] = to_out<OT>(Gc, R, sgn);
-        o2[ro] = to_out<OT>(B, R, sgn);
+            for (int r = 0; r < OUTR; r++) {
+                if (!(full || y + r < h)) continue;
+                const float f = (r & 1) ? fb : fa;
+                const float Yv = yc[r].x, Cbv = yc[r].y, Crv = u[H + r];
+                const float yf = fmaf(f, Yv, dc);
+                const float Rc = fmaf(1.402f * f, Crv, yf);
+                const float Gc = fmaf(-0.71414f * f, Crv, fmaf(-0.34413f * f, Cbv, yf));
+                const float B = fmaf(1.772f * f, Cbv, yf);
+                const size_t ro = (size_t)r * a.out_pitch;
+                o0[ro] = to_out<OT>(Rc, R, sgn);
+                o1[ro] = to_out<OT>(Gc, R, sgn);
+                o2[ro] = to_out<OT>(B, R, sgn);
+            }
+        }
     }
 }
 
@@ -393,18 +418,20 @@ cudaError_t launch_rev97_tma(tc_ctx *ctx, const LevelIO &io, int out_type, int b
     a.out_pitch = io.out_pitch;
     a.bits = bits;
     for (int c = 0; c < 3; c++) a.out[c] = io.out[c];
-    const dim3 grid((io.w + TX - 1) / TX, (io.h + TY - 1) / TY);
+    const int ntx = (io.w + TX - 1) / TX, ntiles = ntx * ((io.h + TY - 1) / TY);
+    // two persistent CTAs per SM (the shared memory of one tile each)
+    const dim3 grid(std::min(ntiles, 2 * num_sms(ctx->device)));
     cudaError_t e;
     if (out_type == TC_U8) {
         static DeviceFlags attr;
         if ((e = set_smem_once(attr, ctx->device, idwt97_ict_tma_kernel<uint8_t>, kSmem)) != cudaSuccess) return e;
         e = launch_pdl(idwt97_ict_tma_kernel<uint8_t>, grid, dim3(kThreads), kSmem, ctx->stream, maps, a,
-                       ctx->d_words);
+                       ctx->d_words, ntx, ntiles);
     } else {
         static DeviceFlags attr;
         if ((e = set_smem_once(attr, ctx->device, idwt97_ict_tma_kernel<uint16_t>, kSmem)) != cudaSuccess) return e;
         e = launch_pdl(idwt97_ict_tma_kernel<uint16_t>, grid, dim3(kThreads), kSmem, ctx->stream, maps, a,
-                       ctx->d_words);
+                       ctx->d_words, ntx, ntiles);
     }
     ctx->launches++;
     return e;
