@@ -280,9 +280,13 @@ __global__ void __launch_bounds__(kThreads, 2)
     const int tid = threadIdx.x;
     const int w = a.w, h = a.h, wl = (w + 1) >> 1, hl = (h + 1) >> 1;
     float *Y = comps, *Cb = comps + COMPF, *Cr = comps + 2 * COMPF;
-    const int col = tid % TX, half = tid / TX;
+    // Vertical pass: warp w takes one half of the rows (w / 4) and 32
+    // columns of one parity (w & 1: the low or the high band array), so its
+    // lanes read 32 consecutive cells of one array, free of bank conflicts.
+    const int vw = tid >> 5, lane = tid & 31;
+    const int half = vw >> 2, p = vw & 1, col = 64 * ((vw >> 1) & 1) + 2 * lane + p;
     const int vbase = half ? 32 - H : 0, obase = half ? OUTR : 0;
-    const int p = col & 1, j = (col >> 1) + 4;   // extended column col + 4
+    const int j = (col >> 1) + 4;   // band column of extended column col + 4
     const float fa = sf_factor(0, p, true, true), fb = sf_factor(1, p, true, true);  // obase and y0 are even
     const OutRange R = out_range(a.bits);
     const bool sgn = a.bits & TC_SIGNED;
