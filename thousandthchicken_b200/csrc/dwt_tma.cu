@@ -175,23 +175,30 @@ __device__ __forceinline__ void hpass(float *c0, float *c1, int r, int s)
     const int j0 = 16 * s + 2;   // band column of the segment's first input
     V v[SEGN];
     {
-        const float *al = band_row(c0, r, 0) + j0, *ah = band_row(c0, r, 1) + j0;
-        const float *bl = band_row(c1, r, 0) + j0, *bh = band_row(c1, r, 1) + j0;
+        // 16-byte loads from band column j0 - 2 (a multiple of 4): 24 cells
+        // per array, of which cells 2 .. 21 are the segment's inputs
+        const float *al = band_row(c0, r, 0) + j0 - 2, *ah = band_row(c0, r, 1) + j0 - 2;
+        const float *bl = band_row(c1, r, 0) + j0 - 2, *bh = band_row(c1, r, 1) + j0 - 2;
+        float L0[24], H0[24], L1[PAIR ? 24 : 1], H1[PAIR ? 24 : 1];
 #pragma unroll
-        for (int k = 0; k < SEGN / 2; k += 2) {
-            const float2 l0 = *reinterpret_cast<const float2 *>(al + k), h0 = *reinterpret_cast<const float2 *>(ah + k);
+        for (int k = 0; k < 24; k += 4) {
+            const float4 a = *reinterpret_cast<const float4 *>(al + k), b = *reinterpret_cast<const float4 *>(ah + k);
+            L0[k] = a.x, L0[k + 1] = a.y, L0[k + 2] = a.z, L0[k + 3] = a.w;
+            H0[k] = b.x, H0[k + 1] = b.y, H0[k + 2] = b.z, H0[k + 3] = b.w;
             if constexpr (PAIR) {
-                const float2 l1 = *reinterpret_cast<const float2 *>(bl + k);
-                const float2 h1 = *reinterpret_cast<const float2 *>(bh + k);
-                v[2 * k] = f2(l0.x, l1.x);
-                v[2 * k + 1] = f2(h0.x, h1.x);
-                v[2 * k + 2] = f2(l0.y, l1.y);
-                v[2 * k + 3] = f2(h0.y, h1.y);
+                const float4 c = *reinterpret_cast<const float4 *>(bl + k), d = *reinterpret_cast<const float4 *>(bh + k);
+                L1[k] = c.x, L1[k + 1] = c.y, L1[k + 2] = c.z, L1[k + 3] = c.w;
+                H1[k] = d.x, H1[k + 1] = d.y, H1[k + 2] = d.z, H1[k + 3] = d.w;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < SEGN / 2; k++) {
+            if constexpr (PAIR) {
+                v[2 * k] = f2(L0[k + 2], L1[k + 2]);
+                v[2 * k + 1] = f2(H0[k + 2], H1[k + 2]);
             } else {
-                v[2 * k] = l0.x;
-                v[2 * k + 1] = h0.x;
-                v[2 * k + 2] = l0.y;
-                v[2 * k + 3] = h0.y;
+                v[2 * k] = L0[k + 2];
+                v[2 * k + 1] = H0[k + 2];
             }
         }
     }
