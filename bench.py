@@ -541,8 +541,27 @@ def mixed_section(ctx, stream, specs, streams, cores):
     from thousandthchicken_b200.stages import Plan
     from thousandthchicken_b200.synth import gradient_noise_image_device
     dev = torch.device("cuda", ctx.device)
+    from thousandthchicken_b200 import autotune
     waves = mixed_waves(specs, streams)
     mpx = sum(sp["w"] * sp["h"] for sp in specs) / 1e6
+    # autotune a few shape buckets on single images of the batch (smallest,
+    # median and largest lossy RGB image, a median lossless RGB one); the
+    # per-image path then applies each plan's bucket choice
+    rgb_lossy = sorted([i for i, sp in enumerate(specs) if sp["c"] == 3 and not sp["reversible"]],
+                       key=lambda i: specs[i]["w"] * specs[i]["h"])
+    rgb_lossless = sorted([i for i, sp in enumerate(specs) if sp["c"] == 3 and sp["reversible"]],
+                          key=lambda i: specs[i]["w"] * specs[i]["h"])
+    tuned = {}
+    for i in [rgb_lossy[0], rgb_lossy[len(rgb_lossy) // 2], rgb_lossy[-1], rgb_lossless[len(rgb_lossless) // 2]]:
+        tp = Plan(ctx, [streams[i]])
+        to = tp.alloc_outputs()
+        with torch.cuda.stream(stream):
+            r_ = autotune.tune_plan(tp, to, trials=2, use_cache=False)
+        tuned[r_["bucket"]] = {k: r_[k] for k in ("lanes", "dwt", "tier1_ms", "dwt_ms")}
+        tuned[r_["bucket"]]["image"] = f"{specs[i]['w']}x{specs[i]['h']}x{specs[i]['c']}"
+        tp.close()
+        del to
+    autotune._set(ctx, 32, autotune.L.TC_DWT_TMA)
     lossy_small = sorted([i for i, sp in enumerate(specs) if not sp["reversible"]],
                          key=lambda i: specs[i]["w"] * specs[i]["h"])[:2]
     kept = {}
@@ -553,14 +572,19 @@ def mixed_section(ctx, stream, specs, streams, cores):
             ws = [streams[i] for i in wave]
             plans = [Plan(ctx, ws)] if path == "batched" else [Plan(ctx, [s_]) for s_ in ws]
             if path == "batched":
+                autotune._set(ctx, 32, autotune.L.TC_DWT_TMA)
                 plans[0].set_graph(True)
             outs = [p_.alloc_outputs() for p_ in plans]
             with torch.cuda.stream(stream):
                 for p_, o_ in zip(plans, outs):
+                    if path == "per_image":
+                        autotune.apply(p_, tuned)
                     p_.execute(o_)
                 a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 a.record(stream)
                 for p_, o_ in zip(plans, outs):
+                    if path == "per_image":
+                        autotune.apply(p_, tuned)
                     p_.execute(o_)
                 b.record(stream)
             b.synchronize()
@@ -606,6 +630,7 @@ def mixed_section(ctx, stream, specs, streams, cores):
             "per_image_mpix_s": round(mpx / (res["per_image"] / 1000.0), 2),
             "speedup": round(res["per_image"] / res["batched"], 3),
             "lossless_bit_exact": exact, "lossy_min_psnr_db": round(min(psnrs), 2), "graphs": graphs,
+            "autotune": tuned,
             "oracle_sample": orc,
             "workload": "256 images, W and H uniform 256-8192 step 16, 1/3 comps, 8/12-bit, half RCT + 5-level 5/3, "
                         "half ICT + 5-level 9/7 step 1/64, 64x64 blocks"}

@@ -249,10 +249,42 @@ def test_graph_replay_and_autotune(gpu_ctx):
             np.testing.assert_array_equal(o.cpu().numpy(), w)
     assert gpu_ctx.launches > n0
     plan.set_graph(False)
-    g = tune_plan(plan, outs, trials=1, use_cache=False)
-    assert g in (8, 16, 32)
+    res = tune_plan(plan, outs, trials=1, use_cache=False)
+    assert res["lanes"] in (8, 16, 32) and res["dwt"] in ("tma", "cp.async")
     L.lib().tc_ctx_set_t1_group(gpu_ctx.handle, 32)
+    L.lib().tc_ctx_set_dwt_variant(gpu_ctx.handle, L.TC_DWT_TMA)
     plan.close()
+
+
+@pytest.mark.parametrize("size", [(264, 136), (2048, 1024)])
+def test_autotuned_choices_decode_like_the_defaults(gpu_ctx, size, tmp_path, monkeypatch):
+    """The tuner's choices (Tier-1 lane width, last-level DWT staging) for a
+    single lossy RGB image: the tuned decode equals the default decode bit
+    for bit, and the cache returns the same choice without searching."""
+    from thousandthchicken_b200 import _lib as L
+    from thousandthchicken_b200 import autotune
+    from thousandthchicken_b200.stages import Plan
+    monkeypatch.setattr(autotune, "CACHE", tmp_path / "tune.json")
+    w, h = size
+    cs = codec.encode(synth_image(w, h, 3, 8, seed=w), 8, levels=5, reversible=False, base_step=1 / 128)
+    plan = Plan(gpu_ctx, [cs])
+    outs = plan.alloc_outputs()
+    plan.execute(outs)
+    gpu_ctx.synchronize()
+    want = outs[0].cpu().numpy().copy()
+    try:
+        res = autotune.tune_plan(plan, outs, trials=1)
+        assert not res["cached"] and set(res["dwt_ms"]) == {"tma", "cp.async"}
+        outs[0].zero_()
+        plan.execute(outs)
+        gpu_ctx.synchronize()
+        np.testing.assert_array_equal(outs[0].cpu().numpy(), want)
+        again = autotune.tune_plan(plan, outs)
+        assert again["cached"] and (again["lanes"], again["dwt"]) == (res["lanes"], res["dwt"])
+    finally:
+        L.lib().tc_ctx_set_t1_group(gpu_ctx.handle, 32)
+        L.lib().tc_ctx_set_dwt_variant(gpu_ctx.handle, L.TC_DWT_TMA)
+        plan.close()
 
 
 def test_jp2_files_decode(gpu_ctx, tmp_path):
