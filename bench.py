@@ -110,9 +110,10 @@ def serve_section(args, specs, streams, device):
                                  "req_s": round(len(cap_ids) / wall, 2)}
     rates = [float(r) for r in str(args.serve_rates).split(",") if r]
     sustained_rate = round(0.8 * out["capacity"]["continuous_batching"]["req_s"], 1)
+    seq = picks(1000, 13)   # one request sequence for every rate (its first n)
     for rate in sorted(set(rates + [sustained_rate])):
         n = int(min(1000, max(20, 5 * rate)))
-        ids = picks(n, int(rate * 10))
+        ids = seq[:n]
         arr = poisson_arrivals(n, rate, seed=9)
         row = {"rate_per_s": rate, "requests": n, "arrival_span_s": round(float(arr[-1]), 3)}
         for name, srv in servers.items():
