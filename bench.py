@@ -70,10 +70,10 @@ def serve_section(args, specs, streams, device):
     lossless images (radial field + N(0, 40^2) noise), device-memory budget
     40 GB.  First the capacity of each path (every request available at
     once).  Then, for each rate of --serve-rates and at 80% of the
-    continuous-batching capacity, min(1000, 5 s x rate) arrivals served by
-    the continuous-batching server (batches of up to 16 requests and 128 Mi
-    samples, two in flight) and
-    by the per-image path (one request per batch, one in flight) on the same
+    continuous-batching capacity, min(1000, 5 s x rate) arrivals (the first
+    requests of one fixed sequence) served by the continuous-batching server
+    (batches of up to 16 requests and 128 Mi samples, two in flight) and by
+    the per-image path (one request per batch, one in flight) on the same
     arrivals.  A rate is sustained when no request waits more than 2 s
     before its batch starts; otherwise the run stops admitting there and the
     rate is reported as overloaded with the throughput reached.  p50/p99 are
