@@ -46,7 +46,15 @@ static inline size_t get_group_id(uint d) { return shim_grp[d]; }
 
 #define CLK_LOCAL_MEM_FENCE 1
 #define CLK_GLOBAL_MEM_FENCE 2
+#ifdef SHIM_WORKGROUP_BARRIER
+/* Kernels with work-group barriers: every work-item of a group runs on a
+ * host thread of its own, and barrier() waits for the whole group (the
+ * driver provides shim_group_barrier). */
+void shim_group_barrier(void);
+static inline void barrier(int flags) { (void)flags; shim_group_barrier(); }
+#else
 static inline void barrier(int flags) { (void)flags; }
+#endif
 
 static inline int clamp(int x, int lo, int hi) { return x < lo ? lo : (x > hi ? hi : x); }
 

@@ -1,7 +1,7 @@
 """Generate golden vectors from the reference's own kernels run on the CPU.
 
 The reference's OpenCL C (coefficient_coder.cl, preprocess_*.cl,
-quantizer_lossless_inverse.cl) is compiled as host code by
+quantizer_lossless_inverse.cl, dwt_f53.cl, dwt_r53.cl) is compiled as host code by
 oracle/ref_shim/Makefile into oracle/_ref/ and driven by oracle/ref.py.
 Tier-1 vectors use the build with the state-update helpers passing their
 register by reference (defects D1/D2 fixed); each codeword is followed by
@@ -76,12 +76,38 @@ def colour_vectors(seed=7):
     return out
 
 
+# widths that are multiples of the kernels' window (64 columns below 480, 128
+# below 960, 192 from there): at other widths the kernels read local memory
+# that no work-item wrote
+DWT_SIZES = [(64, 64), (128, 61), (192, 66), (256, 40), (512, 24), (960, 16)]
+
+
+def dwt53_vectors(seed=11):
+    """One level of the reference's 5/3 kernels (dwt_f53.cl / dwt_r53.cl,
+    truncating division) per size; the window width follows the image width
+    as DWTForward53::dwt chooses it (64, 128 or 192 columns).  The reverse
+    runs on the oracle's forward coefficients (truncating mode, packed)."""
+    import oracle as O
+    rng = np.random.default_rng(seed)
+    out = {}
+    for w, h in DWT_SIZES:
+        x = rng.integers(-128, 128, (h, w)).astype(np.int32)
+        k = f"{w}x{h}"
+        out[f"x_{k}"] = x
+        out[f"fwd_{k}"] = R.dwt53_forward(x, 1)
+        rev_in = R.mallat_to_packed(O.fdwt53(x, 1, rounding=1), 1)
+        out[f"revin_{k}"] = rev_in
+        out[f"rev_{k}"] = R.dwt53_reverse(rev_in, w, h, 1)
+    return out
+
+
 def main():
-    if not R.build():
+    if not R.build() or not R.dwt_available():
         raise SystemExit("oracle/_ref could not be built (reference sources missing)")
     np.savez_compressed(HERE / "ref_t1_blocks.npz", **t1_vectors())
     np.savez_compressed(HERE / "ref_colour.npz", **colour_vectors())
-    print("written ref_t1_blocks.npz, ref_colour.npz")
+    np.savez_compressed(HERE / "ref_dwt53.npz", **dwt53_vectors())
+    print("written ref_t1_blocks.npz, ref_colour.npz, ref_dwt53.npz")
 
 
 if __name__ == "__main__":

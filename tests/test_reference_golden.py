@@ -86,3 +86,57 @@ def test_live_reference_kernels_when_built():
     for i, (b, (seg, zbp, passes)) in enumerate(zip(blocks, truth)):
         want = O.t1_decode_raw(seg, b[1], b[2], b[3], 15, zbp, passes)
         np.testing.assert_array_equal(raw[i, :b[2], :b[1]], want)
+
+
+def _dwt_cases():
+    import ref as R
+    z = np.load(GOLDEN / "ref_dwt53.npz")
+    for k in sorted({f[2:] for f in z.files if f.startswith("x_")}):
+        w, h = map(int, k.split("x"))
+        yield w, h, z[f"x_{k}"], z[f"fwd_{k}"], z[f"revin_{k}"], z[f"rev_{k}"], R
+
+
+def test_oracle_53_trunc_equals_reference_kernels():
+    """One level of the reference's own 5/3 kernels (dwt_f53.cl, dwt_r53.cl;
+    truncating division, defect D13) against the oracle's truncating mode:
+    equal on every sample outside the rows the kernels get wrong (D24: the
+    forward kernel's top rows; D25: the reverse kernel's last row at even
+    heights), and those rows do differ."""
+    n = 0
+    for w, h, x, fwd, revin, rev, R in _dwt_cases():
+        mine = R.mallat_to_packed(O.fdwt53(x, 1, rounding=1), 1)
+        mk = R.dwt53_defect_mask(w, h, True)
+        np.testing.assert_array_equal(mine[~mk], fwd[~mk], err_msg=f"{w}x{h} forward")
+        assert (mine[mk] != fwd[mk]).mean() > 0.9
+        back = O.idwt53(R.packed_to_mallat(revin, w, h, 1), 1, rounding=1)
+        mr = R.dwt53_defect_mask(w, h, False)
+        np.testing.assert_array_equal(back[~mr], rev[~mr], err_msg=f"{w}x{h} reverse")
+        np.testing.assert_array_equal(back, x)   # the oracle's own round trip is exact
+        if h % 2 == 0:
+            assert (back[mr] != rev[mr]).mean() > 0.9
+        n += 1
+    assert n >= 6
+
+
+def test_packed_layout_round_trip():
+    import ref as R
+    rng = np.random.default_rng(3)
+    for w, h, lv in [(64, 64, 3), (97, 61, 4), (33, 17, 2)]:
+        m = rng.integers(-100, 100, (h, w)).astype(np.int32)
+        np.testing.assert_array_equal(R.packed_to_mallat(R.mallat_to_packed(m, lv), w, h, lv), m)
+
+
+def test_live_reference_53_kernels_match_oracle():
+    """With oracle/_ref built: the reference kernels on a fresh 512 x 64
+    image (window 128), forward and reverse, against the oracle."""
+    import ref as R
+    if not R.dwt_available():
+        pytest.skip("oracle/_ref not built")
+    rng = np.random.default_rng(99)
+    w, h = 512, 64
+    x = rng.integers(-255, 256, (h, w)).astype(np.int32)
+    mine = R.mallat_to_packed(O.fdwt53(x, 1, rounding=1), 1)
+    mk = R.dwt53_defect_mask(w, h, True)
+    np.testing.assert_array_equal(R.dwt53_forward(x, 1)[~mk], mine[~mk])
+    mr = R.dwt53_defect_mask(w, h, False)
+    np.testing.assert_array_equal(R.dwt53_reverse(mine, w, h, 1)[~mr], x[~mr])
