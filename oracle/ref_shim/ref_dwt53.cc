@@ -14,6 +14,12 @@
  * sliding-window step count divRndUp(sy, 15 * WIN_SY), and the local buffer
  * size of calcTransformDataBufferSize (DWTKernel.cpp:193-201).  The
  * multi-level recursion with copyLLBandToSrc runs in the caller.
+ *
+ * OpenCL local memory starts undefined; here every group's buffer starts
+ * filled with REF_DWT53_FILL (default 0).  At image widths that are not a
+ * multiple of the window the kernels read cells no work-item wrote, and
+ * their output changes with the fill; at window-multiple widths it does not
+ * (the tests compare only those).
  */
 // the standard headers first: the shim's address-space macros (local,
 // global, kernel) would break them
