@@ -10,7 +10,8 @@ but which the reference needs to consume the codeword's real last byte (its
 bytein stops one byte early).  Blocks one column wide are excluded (the
 reference's window scan leaves the block when width == 1).
 
-Run from the repository root: ``python tests/golden/make_ref_golden.py``.
+Run from the repository root: ``python tests/golden/make_ref_golden.py
+[fixture ...]`` (every fixture when none is named).
 """
 from __future__ import annotations
 
@@ -59,6 +60,46 @@ def t1_vectors(seed=123, n=160, mb=14):
                 ref_raw=flat, unpatched_mismatches=unpatched_diff)
 
 
+def t1_trunc_vectors(seed=321, n=160, mb=14):
+    """Blocks truncated after P whole bit-planes (3P - 2 coding passes, the
+    oracle's encoder terminating the codeword there).  The reference kernel
+    decodes every plane it is told a block has (significantBits,
+    coefficient_coder.cl:797-815) and ignores pass counts (defect D3), so it
+    is given significantBits = P: it then decodes exactly those passes and
+    writes the P planes as the top planes of a P-plane block.  The stored
+    `ref_raw` words are its own output; a decoder of the same block with its
+    nb coded planes puts them nb - P bits higher."""
+    import oracle as O
+    rng = np.random.default_rng(seed)
+    segs, meta = [], []
+    while len(meta) < n:
+        i = len(meta)
+        kind = i % 4
+        if kind == 0:
+            w = h = 64
+        elif kind == 1:
+            w = h = 32
+        else:
+            w, h = int(rng.integers(2, 65)), int(rng.integers(1, 65))
+        orient = int(rng.integers(0, 4))
+        coef = laplacian_block(rng, w, h, bitplanes=int(rng.integers(2, 14)))
+        _, _, nb = O.t1_encode(coef, orient, 0)
+        if nb < 2:
+            continue
+        planes = int(rng.integers(1, nb))
+        seg, passes, nb2 = O.t1_encode(coef, orient, 3 * planes - 2)
+        assert passes == 3 * planes - 2 and nb2 == nb
+        segs.append(seg)
+        meta.append((w, h, orient, mb, mb - nb, passes, planes))
+    blocks = [(s + b"\xff", m[0], m[1], m[2], m[3], m[6]) for s, m in zip(segs, meta)]
+    raw, skipped = R.t1_decode(blocks, patched=True)
+    assert skipped == 0
+    off = np.cumsum([0] + [len(s) for s in segs])
+    flat = np.concatenate([raw[i, :m[1], :m[0]].ravel() for i, m in enumerate(meta)])
+    return dict(pool=np.frombuffer(b"".join(segs), np.uint8), seg_off=off[:-1].astype(np.int64),
+                seg_len=np.array([len(s) for s in segs], np.int32), meta=np.array(meta, np.int32), ref_raw=flat)
+
+
 def colour_vectors(seed=7):
     rng = np.random.default_rng(seed)
     out = {}
@@ -101,14 +142,18 @@ def dwt53_vectors(seed=11):
     return out
 
 
-def main():
+FIXTURES = {"ref_t1_blocks": t1_vectors, "ref_t1_trunc": t1_trunc_vectors, "ref_colour": colour_vectors,
+            "ref_dwt53": dwt53_vectors}
+
+
+def main(names=None):
+    """Write the named fixtures (all when none are named)."""
     if not R.build() or not R.dwt_available():
         raise SystemExit("oracle/_ref could not be built (reference sources missing)")
-    np.savez_compressed(HERE / "ref_t1_blocks.npz", **t1_vectors())
-    np.savez_compressed(HERE / "ref_colour.npz", **colour_vectors())
-    np.savez_compressed(HERE / "ref_dwt53.npz", **dwt53_vectors())
-    print("written ref_t1_blocks.npz, ref_colour.npz, ref_dwt53.npz")
+    for name in names or FIXTURES:
+        np.savez_compressed(HERE / f"{name}.npz", **FIXTURES[name]())
+        print(f"written {name}.npz")
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

@@ -42,7 +42,7 @@ def test_53_forward_reverse_bit_exact(gpu_ctx, w, h, levels, rounding):
 
 
 @pytest.mark.parametrize("w,h,levels", SIZES)
-def test_97_forward_reverse_within_tolerance(gpu_ctx, w, h, levels):
+def test_97_forward_reverse_within_tolerance(gpu_ctx, w, h, levels, record_property):
     from thousandthchicken_b200.stages import DWTForward97, DWTReverse97
     x = _rand(w, h, w * 17 + h, -128, 128).astype(np.float64)
     want_f = O.fdwt97(x, levels)
@@ -54,6 +54,8 @@ def test_97_forward_reverse_within_tolerance(gpu_ctx, w, h, levels):
     got_r = torch.empty((h, w), dtype=torch.float32, device="cuda")
     DWTReverse97(gpu_ctx).run(_dev(want_f, torch.float32), got_r, w, h, levels)
     err_r = np.abs(got_r.cpu().numpy().astype(np.float64) - x).max()
+    record_property("forward_max_abs_vs_fp64", float(err_f))
+    record_property("reverse_max_abs_vs_fp64", float(err_r))
     assert err_r <= TOL97, err_r
 
 

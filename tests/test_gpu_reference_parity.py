@@ -31,6 +31,33 @@ def test_gpu_t1_equals_reference_kernel(gpu_ctx):
         pos += w * h
 
 
+def test_gpu_t1_truncated_equals_reference_kernel(gpu_ctx):
+    """Blocks truncated after P whole bit-planes, in one launch: the GPU's raw
+    words equal the reference kernel's output for a P-plane block moved up by
+    the planes left undecoded (tests/golden/make_ref_golden.py,
+    t1_trunc_vectors)."""
+    from test_reference_golden import ref_planes_to_coded
+    from thousandthchicken_b200.stages import CoefficientCoder
+    z = np.load(GOLDEN / "ref_t1_trunc.npz")
+    meta = z["meta"]
+    n = len(meta)
+    desc = np.zeros(n, codec.DESC_DTYPE)
+    desc["seg_off"] = z["seg_off"]
+    desc["seg_len"] = z["seg_len"]
+    desc["w"], desc["h"], desc["orient"], desc["mb"] = meta[:, 0], meta[:, 1], meta[:, 2], meta[:, 3]
+    desc["zero_bitplanes"], desc["passes"] = meta[:, 4], meta[:, 5]
+    desc["out_off"] = np.arange(n) * 4096
+    desc["out_pitch"] = 64
+    got = CoefficientCoder(gpu_ctx).decode_blocks(desc, z["pool"], n * 4096, raw=True).cpu().numpy()
+    got = got.view(np.uint32).reshape(n, 64, 64)
+    flat, pos = z["ref_raw"], 0
+    for i, (w, h, _o, mb, zbp, _p, planes) in enumerate(meta):
+        ref = flat[pos: pos + w * h].reshape(h, w)
+        np.testing.assert_array_equal(got[i, :h, :w], ref_planes_to_coded(ref, int(planes), int(mb - zbp)),
+                                      err_msg=f"block {i}")
+        pos += w * h
+
+
 @pytest.mark.parametrize("bits", [8, 12])
 def test_gpu_colour_equals_reference_kernels(gpu_ctx, bits):
     from thousandthchicken_b200.stages import Preprocessor

@@ -34,6 +34,34 @@ def test_oracle_t1_equals_reference_kernel():
     assert n >= 100
 
 
+def ref_planes_to_coded(ref, planes, nb):
+    """The reference's raw words of a block decoded as a `planes`-plane block
+    (significantBits = planes) in the layout of a decoder that knows the
+    block has nb coded planes and decoded the first `planes`: magnitude bits
+    nb - planes higher, sign bit unchanged."""
+    ref = ref.astype(np.uint64)
+    mag = ((ref & 0x7FFFFFFF) << np.uint64(nb - planes)) & 0x7FFFFFFF
+    return (mag | (ref & 0x80000000)).astype(np.uint32)
+
+
+def test_oracle_t1_truncated_equals_reference_kernel():
+    """Blocks truncated after whole bit-planes (3P - 2 passes): the oracle's
+    raw decode equals the reference kernel's own output for a P-plane block,
+    moved up by the planes left undecoded."""
+    z = np.load(GOLDEN / "ref_t1_trunc.npz")
+    pool, off, ln, flat = z["pool"], z["seg_off"], z["seg_len"], z["ref_raw"]
+    pos = n = 0
+    for i, (w, h, orient, mb, zbp, passes, planes) in enumerate(z["meta"]):
+        seg = pool[off[i]: off[i] + ln[i]].tobytes()
+        ref = flat[pos: pos + w * h].reshape(h, w)
+        pos += w * h
+        got = O.t1_decode_raw(seg, int(w), int(h), int(orient), int(mb), int(zbp), int(passes))
+        np.testing.assert_array_equal(got, ref_planes_to_coded(ref, int(planes), int(mb - zbp)), err_msg=f"block {i}")
+        assert (got != 0).any() or not ln[i]
+        n += 1
+    assert n == 160
+
+
 def test_unpatched_reference_kernel_is_defective():
     """Defects D1/D2 (state helpers take their register by value): the
     reference kernel as written decodes wrong coefficients."""
