@@ -21,6 +21,7 @@ constexpr int kSgnCols = 66;       // 64 columns + a zero column on each side
 //              (j = 0..5, rows -1..4) and col 0 = left, 1 = this, 2 = right
 //   bits 18-21 pi: coded in this plane's significance propagation pass
 //   bits 22-25 sigma': refined at least once
+//   bits 26-31 (decoder only) sign of row j-1 at bit 26 + j, j = 0..5
 constexpr uint32_t kSigMask = 0x3FFFFu;
 __device__ __forceinline__ uint32_t self_bit(int k) { return 1u << (3 * k + 4); }
 __device__ __forceinline__ uint32_t pi_bit(int k) { return 1u << (18 + k); }
@@ -46,6 +47,10 @@ struct Tables {
     uint32_t mq[48];          // packed states: Qe << 16 | NMPS << 1 | NLPS << 7 | SWITCH << 13 (bit 0: MPS)
     uint8_t zc[4][512];       // zero-coding label per orientation and 3x3 neighbourhood
     uint8_t sc[256];          // sign label | XOR bit << 4
+    // Decoder context words by 2 * state + MPS: Qe << 16, the entry after an
+    // LPS << 7 (NLPS, MPS switched where SWITCH is set), the entry after an
+    // MPS (NMPS, same MPS) in bits 0-6, whose bit 0 is the MPS.
+    uint32_t mqd[96];
 };
 
 // Zero-coding label from neighbour counts, ISO Table D.1 (the reference's
@@ -72,6 +77,11 @@ __device__ void build_tables(Tables &t)
     for (int i = threadIdx.x; i < 47; i += blockDim.x)
         t.mq[i] = ((uint32_t)c_qe[i] << 16) | ((uint32_t)c_nmps[i] << 1) | ((uint32_t)c_nlps[i] << 7) |
                   ((uint32_t)(i == 0 || i == 6 || i == 14) << 13);
+    for (int i = threadIdx.x; i < 94; i += blockDim.x) {
+        const int st = i >> 1, mps = i & 1, sw = st == 0 || st == 6 || st == 14;
+        t.mqd[i] = ((uint32_t)c_qe[st] << 16) | ((uint32_t)(2 * c_nlps[st] + (mps ^ sw)) << 7) |
+                   (uint32_t)(2 * c_nmps[st] + mps);
+    }
     // 3x3 neighbourhood bits: 0 up-left 1 up 2 up-right 3 left 4 self
     // 5 right 6 down-left 7 down 8 down-right.
     for (int i = threadIdx.x; i < 4 * 512; i += blockDim.x) {

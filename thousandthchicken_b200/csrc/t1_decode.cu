@@ -10,11 +10,16 @@
 //     as concurrent launches, heaviest first;
 //   * the code-block state is one 32-bit flag word per stripe column: the
 //     significance of its 3x6 neighbourhood interleaved so that row k's 3x3
-//     neighbourhood is (F >> 3k) & 0x1FF, plus the visited (pi) and refined
-//     (sigma') bits of its four rows.  A context label is one shift, one mask
-//     and one table lookup; a coefficient that becomes significant updates the
-//     words of its neighbours.  (The reference rebuilds a 3x3 window of packed
-//     words from global memory at every step, coefficient_coder.cl:271-298.)
+//     neighbourhood is (F >> 3k) & 0x1FF, the visited (pi) and refined
+//     (sigma') bits of its four rows, and the signs of its six rows (-1..4).
+//     A context label is one shift, one mask and one table lookup, a sign
+//     context reads the column's word and its two neighbours'; a coefficient
+//     that becomes significant updates the words of its neighbours.  (The
+//     reference rebuilds a 3x3 window of packed words from global memory at
+//     every step, coefficient_coder.cl:271-298.)
+//   * the MQ context words carry both successor states whole (Qe, both
+//     successors, MPS), so a state change is one table load;
+//   * the candidate columns of a stripe are scanned as two 32-bit masks;
 //   * all 32 lanes run the decoder in lock-step (replicated MQ state,
 //     broadcast shared-memory accesses); at every stripe the lanes find the
 //     candidate columns of the pass with __ballot_sync and the serial loop
@@ -49,21 +54,67 @@ constexpr int kBlocks8 = TC_T1_BLOCKS8;  // code-blocks per CTA of the 8-bit cla
 
 template <typename MagT>
 struct WarpState {
-    uint32_t F[kMaxStripes * 64];          // flag word per stripe column
-    unsigned long long sgn[kSgnCols];      // sign per column (bit y = row y), zero guard columns
+    uint32_t F[kMaxStripes * 64];          // flag word per stripe column (with signs, bits 26-31)
     uint32_t ctx[20];                      // packed probability state per context
     uint8_t mrow[64];                      // refinement pass: rows of the stripe to refine
     uint8_t mctx[64];                      // refinement pass: 2-bit context code per row
     MagT mag[64 * 64];                     // magnitude bits decoded so far
 };
 
+// Signs in the decoder's flag word: bit 26 + j holds the sign of row j - 1 of
+// the stripe column (j = 0..5, rows -1..4), set when that row becomes
+// significant; rows -1 and 4 belong to the stripes above and below.
+constexpr int kSignShift = 26;
+
+// Sign-coding index (ISO Table D.3 neighbourhood) of row k of the column at
+// F[i], whose flag word is f and 3x3 neighbourhood n9: the signs of the rows
+// above and below come from f, those of the left and right neighbours from
+// their own words.  Bits: up sign 0, up 1, left sign 2, left 3, right sign 4,
+// right 5, down sign 6, down 7.
+__device__ __forceinline__ uint32_t dec_sign_index(const uint32_t *F, uint32_t f, uint32_t n9, int i, int k, int c,
+                                                   int w)
+{
+    const uint32_t lf = c > 0 ? F[i - 1] : 0u, rt = c + 1 < w ? F[i + 1] : 0u;
+    const int own = kSignShift + 1 + k;  // this row's sign bit in a word of its stripe
+    return (n9 & 0xAAu) | ((f >> (own - 1)) & 1u) | (((lf >> own) & 1u) << 2) | (((rt >> own) & 1u) << 4) |
+           (((f >> (own + 1)) & 1u) << 6);
+}
+
+// Row k of stripe s in column c became significant with sign neg: the flag
+// words of the neighbouring columns see its significance, and those of the
+// stripes above and below also its sign.  The caller sets the column's own
+// significance and sign bits.  With vertically causal contexts (vsc, ISO
+// D.7) the stripe above does not see it: its last row's neighbourhood then
+// leaves out the row below for every context.
+__device__ __forceinline__ void dec_mark_significant(uint32_t *F, int s, int k, int c, int w, int nstripes,
+                                                     uint32_t neg, bool vsc)
+{
+    const int i = s * 64 + c;
+    if (c > 0) F[i - 1] |= 1u << (3 * k + 5);
+    if (c + 1 < w) F[i + 1] |= 1u << (3 * k + 3);
+    if (k == 0 && s > 0 && !vsc) {
+        const int u = i - 64;
+        F[u] |= (1u << 16) | (neg << (kSignShift + 5));
+        if (c > 0) F[u - 1] |= 1u << 17;
+        if (c + 1 < w) F[u + 1] |= 1u << 15;
+    }
+    if (k == 3 && s + 1 < nstripes) {
+        const int d = i + 64;
+        F[d] |= (1u << 1) | (neg << kSignShift);
+        if (c > 0) F[d - 1] |= 1u << 2;
+        if (c + 1 < w) F[d + 1] |= 1u << 0;
+    }
+}
+
 // MQ decoder (ISO C.3; bytein/renormd/mqDecode, coefficient_coder.cl:121-252).
 // The interval register A is kept scaled by 2^16 so that it lives in the same
 // bit positions as C's upper half: the Qe comparison against C, the
 // "A < 0x8000" test (sign bit of the scaled A) and the renormalisation shift
-// (count of leading zeros) need no extra shifts.  Each context word holds
-// Qe << 16 plus its transition indices and MPS.  The byte after the current
-// one is loaded ahead of use.
+// (count of leading zeros) need no extra shifts.  Each context word is an
+// entry of Tables::mqd: Qe << 16, the entries of its two successor states
+// (after an MPS, after an LPS with the MPS switched where ISO Table C.2 says
+// so) and the MPS in bit 0.  The byte after the current one is loaded ahead
+// of use.
 struct MQ {
     const uint8_t *p;
     int len, bp, ct;
@@ -130,7 +181,7 @@ struct MQ {
         c = lower ? c : c - qs;
         a = lower ? qs : a1;
         if (lower || (int)a1 >= 0) {
-            ctx[cx] = d != mps ? (tbl[(w >> 7) & 63] | (mps ^ ((w >> 13) & 1u))) : (tbl[(w >> 1) & 63] | mps);
+            ctx[cx] = tbl[d != mps ? (w >> 7) & 127u : w & 127u];
             renorm();
         }
         return d;
@@ -193,7 +244,7 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
     const bool vsc = Modes && (style & TC_CBLK_STYLE_VSC);
     if (!Modes || !lens) mq.init(seg, len);
     uint32_t *ctx = S.ctx;
-    const uint32_t *tbl = T.mq;
+    const uint32_t *tbl = T.mqd;
     const uint8_t *zc = T.zc[orient];
     uint32_t *F = S.F;
     const int nstripes = (h + 3) >> 2;
@@ -223,7 +274,7 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
             if (style & TC_CBLK_STYLE_RESET) {
                 __syncwarp(gmask);
                 for (int i = lane; i < 19; i += G)
-                    ctx[i] = tbl[i == 0 ? 4 : (i == 17 ? 46 : (i == 18 ? 3 : 0))];
+                    ctx[i] = tbl[2 * (i == 0 ? 4 : (i == 17 ? 46 : (i == 18 ? 3 : 0)))];
                 __syncwarp(gmask);
             }
         }
@@ -262,28 +313,35 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
                     }
                     any[j] = a;
                 }
-                unsigned long long cand = group_ballot<G>(any, gmask, gshift);
-                while (cand) {
-                    const int c = __ffsll((long long)cand) - 1;
-                    cand &= cand - 1;
-                    uint32_t f = F[s * 64 + c];
-                    const uint32_t f0 = f;
-                    for (int k = 0; k < rows; k++) {
-                        if (f & self_bit(k)) continue;
-                        const uint32_t n9 = (f >> (3 * k)) & 0x1FFu;
-                        if (!(n9 & 0x1EFu)) continue;
-                        f |= pi_bit(k);
-                        if (decide(zc[n9])) {
-                            const int y = 4 * s + k;
-                            const uint32_t si = T.sc[sign_index(S.sgn, n9, c, y)];
-                            const uint32_t neg = sign(si);
-                            f |= self_bit(k);
-                            mark_significant(S.F, S.sgn, s, k, c, w, nstripes, neg, vsc);
-                            S.mag[y * 64 + c] = pbit;
-                            if (c + 1 < w) cand |= 1ull << (c + 1);  // the next column gained a neighbour
+                const unsigned long long cand64 = group_ballot<G>(any, gmask, gshift);
+                uint32_t chi = (uint32_t)(cand64 >> 32);  // columns 32-63
+#pragma unroll 1
+                for (int half = 0; half < 2; half++) {
+                    uint32_t cand = half ? chi : (uint32_t)cand64;
+                    while (cand) {
+                        const int c = 32 * half + __ffs(cand) - 1;
+                        cand &= cand - 1;
+                        uint32_t f = F[s * 64 + c];
+                        const uint32_t f0 = f;
+                        for (int k = 0; k < rows; k++) {
+                            if (f & self_bit(k)) continue;
+                            const uint32_t n9 = (f >> (3 * k)) & 0x1FFu;
+                            if (!(n9 & 0x1EFu)) continue;
+                            f |= pi_bit(k);
+                            if (decide(zc[n9])) {
+                                const uint32_t si = T.sc[dec_sign_index(F, f, n9, s * 64 + c, k, c, w)];
+                                const uint32_t neg = sign(si);
+                                f |= self_bit(k) | (neg << (kSignShift + 1 + k));
+                                dec_mark_significant(F, s, k, c, w, nstripes, neg, vsc);
+                                S.mag[(4 * s + k) * 64 + c] = pbit;
+                                if (c + 1 < w) {  // the next column gained a neighbour
+                                    cand |= 2u << (c & 31);
+                                    chi |= (uint32_t)(c == 31);
+                                }
+                            }
                         }
+                        if (f != f0) F[s * 64 + c] = f;
                     }
-                    if (f != f0) F[s * 64 + c] = f;
                 }
             }
             end_pass();
@@ -318,17 +376,21 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
                     }
                     any[j] = rr != 0;
                 }
-                unsigned long long cand = group_ballot<G>(any, gmask, gshift);
+                const unsigned long long cand64 = group_ballot<G>(any, gmask, gshift);
                 __syncwarp(gmask);
-                while (cand) {
-                    const int c = __ffsll((long long)cand) - 1;
-                    cand &= cand - 1;
-                    uint32_t rr = S.mrow[c];
-                    const uint32_t codes = S.mctx[c];
-                    while (rr) {
-                        const int k = __ffs(rr) - 1;
-                        rr &= rr - 1;
-                        if (decide(14 + ((codes >> (2 * k)) & 3u))) S.mag[(4 * s + k) * 64 + c] |= pbit;
+#pragma unroll 1
+                for (int half = 0; half < 2; half++) {
+                    uint32_t cand = half ? (uint32_t)(cand64 >> 32) : (uint32_t)cand64;
+                    while (cand) {
+                        const int c = 32 * half + __ffs(cand) - 1;
+                        cand &= cand - 1;
+                        uint32_t rr = S.mrow[c];
+                        const uint32_t codes = S.mctx[c];
+                        while (rr) {
+                            const int k = __ffs(rr) - 1;
+                            rr &= rr - 1;
+                            if (decide(14 + ((codes >> (2 * k)) & 3u))) S.mag[(4 * s + k) * 64 + c] |= pbit;
+                        }
                     }
                 }
             }
@@ -357,39 +419,41 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
                 }
                 any[j] = a;
             }
-            unsigned long long cand = group_ballot<G>(any, gmask, gshift);
-            while (cand) {
-                const int c = __ffsll((long long)cand) - 1;
-                cand &= cand - 1;
-                uint32_t f = F[s * 64 + c];
-                const uint32_t f0 = f;
-                int k = 0;
-                if (rows == 4 && (f & kSigMask) == 0u) {
-                    // run-length mode: four rows with an all-zero neighbourhood
-                    if (!mq.decode(ctx, tbl, 18)) continue;
-                    int r = mq.decode(ctx, tbl, 17) << 1;
-                    r |= mq.decode(ctx, tbl, 17);
-                    const int y = 4 * s + r;
-                    const uint32_t si = T.sc[sign_index(S.sgn, (f >> (3 * r)) & 0x1FFu, c, y)];
-                    const uint32_t neg = (uint32_t)mq.decode(ctx, tbl, si & 15) ^ (si >> 4);
-                    f |= self_bit(r);
-                    mark_significant(S.F, S.sgn, s, r, c, w, nstripes, neg, vsc);
-                    S.mag[y * 64 + c] = pbit;
-                    k = r + 1;
-                }
-                for (; k < rows; k++) {
-                    if (f & (self_bit(k) | pi_bit(k))) continue;
-                    const uint32_t n9 = (f >> (3 * k)) & 0x1FFu;
-                    if (mq.decode(ctx, tbl, zc[n9])) {
-                        const int y = 4 * s + k;
-                        const uint32_t si = T.sc[sign_index(S.sgn, n9, c, y)];
+            const unsigned long long cand64 = group_ballot<G>(any, gmask, gshift);
+#pragma unroll 1
+            for (int half = 0; half < 2; half++) {
+                uint32_t cand = half ? (uint32_t)(cand64 >> 32) : (uint32_t)cand64;
+                while (cand) {
+                    const int c = 32 * half + __ffs(cand) - 1;
+                    cand &= cand - 1;
+                    uint32_t f = F[s * 64 + c];
+                    const uint32_t f0 = f;
+                    int k = 0;
+                    if (rows == 4 && (f & kSigMask) == 0u) {
+                        // run-length mode: four rows with an all-zero neighbourhood
+                        if (!mq.decode(ctx, tbl, 18)) continue;
+                        int r = mq.decode(ctx, tbl, 17) << 1;
+                        r |= mq.decode(ctx, tbl, 17);
+                        const uint32_t si = T.sc[dec_sign_index(F, f, (f >> (3 * r)) & 0x1FFu, s * 64 + c, r, c, w)];
                         const uint32_t neg = (uint32_t)mq.decode(ctx, tbl, si & 15) ^ (si >> 4);
-                        f |= self_bit(k);
-                        mark_significant(S.F, S.sgn, s, k, c, w, nstripes, neg, vsc);
-                        S.mag[y * 64 + c] = pbit;
+                        f |= self_bit(r) | (neg << (kSignShift + 1 + r));
+                        dec_mark_significant(F, s, r, c, w, nstripes, neg, vsc);
+                        S.mag[(4 * s + r) * 64 + c] = pbit;
+                        k = r + 1;
                     }
+                    for (; k < rows; k++) {
+                        if (f & (self_bit(k) | pi_bit(k))) continue;
+                        const uint32_t n9 = (f >> (3 * k)) & 0x1FFu;
+                        if (mq.decode(ctx, tbl, zc[n9])) {
+                            const uint32_t si = T.sc[dec_sign_index(F, f, n9, s * 64 + c, k, c, w)];
+                            const uint32_t neg = (uint32_t)mq.decode(ctx, tbl, si & 15) ^ (si >> 4);
+                            f |= self_bit(k) | (neg << (kSignShift + 1 + k));
+                            dec_mark_significant(F, s, k, c, w, nstripes, neg, vsc);
+                            S.mag[(4 * s + k) * 64 + c] = pbit;
+                        }
+                    }
+                    if (f != f0) F[s * 64 + c] = f;
                 }
-                if (f != f0) F[s * 64 + c] = f;
             }
         }
         if constexpr (Modes) {
@@ -486,10 +550,9 @@ __device__ __forceinline__ void process_block(WarpState<MagT> &S, const Tables &
 
     // clear the state (the group's lanes)
     for (int i = gl; i < nstripes * 64; i += G) S.F[i] = 0u;
-    for (int i = gl; i < kSgnCols; i += G) S.sgn[i] = 0ull;
     for (int i = gl; i < 19; i += G) {
         const int st = i == 0 ? 4 : (i == 17 ? 46 : (i == 18 ? 3 : 0));
-        S.ctx[i] = T.mq[st];
+        S.ctx[i] = T.mqd[2 * st];   // MPS 0
     }
     __syncwarp(gmask);
 
@@ -519,7 +582,7 @@ __device__ __forceinline__ void process_block(WarpState<MagT> &S, const Tables &
             uint32_t mg = 0, neg = 0, u = 0;
             if (sg) {
                 mg = (uint32_t)S.mag[y * 64 + x];
-                neg = (uint32_t)(S.sgn[x + 1] >> y) & 1u;
+                neg = (f >> (kSignShift + 1 + k)) & 1u;
                 u = (uint32_t)last_plane;
                 if (type == 1 && !(f & pi_bit(k))) u++;
                 if (roi && (mg >> roi)) {
