@@ -307,9 +307,12 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
                     const int c = lane + G * j;
                     bool a = false;
                     if (c < w) {
+                        // bit 3j of g: a significant sample in row j - 1 of
+                        // the three columns; bit 3k of the test: row k is not
+                        // significant and has a significant neighbour
                         const uint32_t f = F[s * 64 + c];
-                        for (int k = 0; k < rows; k++)
-                            a |= !(f & self_bit(k)) && ((f >> (3 * k)) & 0x1EFu);
+                        const uint32_t g = (f | (f >> 1) | (f >> 2)) & 0x9249u;
+                        a = ((g | (g >> 3) | (g >> 6)) & ~(f >> 4) & (0x249u >> (3 * (4 - rows)))) != 0u;
                     }
                     any[j] = a;
                 }
@@ -322,7 +325,6 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
                         const int c = 32 * half + __ffs(cand) - 1;
                         cand &= cand - 1;
                         uint32_t f = F[s * 64 + c];
-                        const uint32_t f0 = f;
                         for (int k = 0; k < rows; k++) {
                             if (f & self_bit(k)) continue;
                             const uint32_t n9 = (f >> (3 * k)) & 0x1FFu;
@@ -340,7 +342,9 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
                                 }
                             }
                         }
-                        if (f != f0) F[s * 64 + c] = f;
+                        // stored unconditionally: a visited column nearly
+                        // always had a row coded (its pi bit set)
+                        F[s * 64 + c] = f;
                     }
                 }
             }
