@@ -137,8 +137,7 @@ struct MQ {
         }
         bp++;
         cur = nxt;
-        nxt = byte_at(bp + 1);
-        if ((bp & 63) == 0 && bp + 256 < len) asm volatile("prefetch.global.L1 [%0];" ::"l"(p + bp + 256));
+        nxt = byte_at(bp + 1);   // used about nine decisions later: no prefetch needed
     }
     __device__ __forceinline__ void init(const uint8_t *d, int n)
     {
@@ -326,8 +325,9 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
                         cand &= cand - 1;
                         uint32_t f = F[s * 64 + c];
                         for (int k = 0; k < rows; k++) {
-                            if (f & self_bit(k)) continue;
-                            const uint32_t n9 = (f >> (3 * k)) & 0x1FFu;
+                            const uint32_t fk = f >> (3 * k);   // row k's window at bit 0, self at bit 4
+                            if (fk & 0x10u) continue;
+                            const uint32_t n9 = fk & 0x1FFu;
                             if (!(n9 & 0x1EFu)) continue;
                             f |= pi_bit(k);
                             if (decide(zc[n9])) {
