@@ -52,13 +52,26 @@ namespace {
 #endif
 constexpr int kBlocks8 = TC_T1_BLOCKS8;  // code-blocks per CTA of the 8-bit class
 
+// Blocks of more than 8 coded bit-planes keep their magnitude bits in their
+// own output words instead of shared memory, so their state is as small as
+// an 8-bit block's and as many of them reside per SM (24 warps instead of
+// 16: lossless 12-bit 4096^2 Tier-1 48.7 -> 46.3 ms).  8-bit blocks keep
+// them in shared memory, which is faster for them.
+// (OM, "output magnitudes", true.)  A launch too small to fill the GPU keeps
+// them in shared memory instead (OM false): each of its warps then runs
+// nearly alone, and the output-word path's longer per-block latency would
+// show (the 200,000-block workload decoded one launch per image: 1366 ms
+// against 1007 ms).
 template <typename MagT>
+constexpr bool kOutMag = sizeof(MagT) > 1;
+
+template <typename MagT, bool OM = kOutMag<MagT>>
 struct WarpState {
     uint32_t F[kMaxStripes * 64];          // flag word per stripe column (with signs, bits 26-31)
     uint32_t ctx[20];                      // packed probability state per context
     uint8_t mrow[64];                      // refinement pass: rows of the stripe to refine
     uint8_t mctx[64];                      // refinement pass: 2-bit context code per row
-    MagT mag[64 * 64];                     // magnitude bits decoded so far
+    MagT mag[OM ? 4 : 64 * 64];            // magnitude bits decoded so far (unless OM)
 };
 
 // Signs in the decoder's flag word: bit 26 + j holds the sign of row j - 1 of
@@ -230,11 +243,29 @@ struct RawBits {
 // which follow one another from seg.
 // Raw: the block has raw (bypass) passes (BYPASS and more than 10 passes);
 // without them the raw coder and its tests are compiled out.
-template <typename MagT, int G, bool Modes = false, bool Raw = false>
-__device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *seg, int len, int w,
+template <typename MagT, int G, bool Modes = false, bool Raw = false, bool OM = kOutMag<MagT>>
+__device__ int decode_block(WarpState<MagT, OM> &S, const Tables &T, const uint8_t *seg, int len, int w,
                             int h, int orient, int numbps, int passes, int *last_plane, int lane, unsigned gmask,
-                            int gshift, int style = 0, const uint32_t *lens = nullptr)
+                            int gshift, uint32_t *ob, uint32_t pitch, int style = 0, const uint32_t *lens = nullptr)
 {
+    // magnitude bits: in shared memory, or (deep blocks) in the block's own
+    // output words ob (row pitch `pitch`), where lane 0 of the group stores a
+    // sample's first bit and ORs refinement bits in with fire-and-forget
+    // atomics; the epilogue reads them back
+    auto mag_set = [&](int y, int c, uint32_t v) {
+        if constexpr (OM) {
+            if (lane == 0) ob[(size_t)y * pitch + c] = v;
+        } else {
+            S.mag[y * 64 + c] = (MagT)v;
+        }
+    };
+    auto mag_or = [&](int y, int c, uint32_t v) {
+        if constexpr (OM) {
+            if (lane == 0) atomicOr(ob + (size_t)y * pitch + c, v);
+        } else {
+            S.mag[y * 64 + c] |= (MagT)v;
+        }
+    };
     MQ mq;
     RawBits rw;
     bool raw = false;      // the current segment is raw-coded
@@ -293,7 +324,7 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
     };
 
     for (int p = numbps - 1; p >= 0; --p) {
-        const MagT pbit = (MagT)(1u << p);
+        const uint32_t pbit = 1u << p;
         if (p != numbps - 1) {
             // ---- significance propagation pass (ISO D.3.1; SigPropPassFunctor) ----
             begin_pass(pass);
@@ -335,7 +366,7 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
                                 const uint32_t neg = sign(si);
                                 f |= self_bit(k) | (neg << (kSignShift + 1 + k));
                                 dec_mark_significant(F, s, k, c, w, nstripes, neg, vsc);
-                                S.mag[(4 * s + k) * 64 + c] = pbit;
+                                mag_set(4 * s + k, c, pbit);
                                 if (c + 1 < w) {  // the next column gained a neighbour
                                     cand |= 2u << (c & 31);
                                     chi |= (uint32_t)(c == 31);
@@ -393,7 +424,7 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
                         while (rr) {
                             const int k = __ffs(rr) - 1;
                             rr &= rr - 1;
-                            if (decide(14 + ((codes >> (2 * k)) & 3u))) S.mag[(4 * s + k) * 64 + c] |= pbit;
+                            if (decide(14 + ((codes >> (2 * k)) & 3u))) mag_or(4 * s + k, c, pbit);
                         }
                     }
                 }
@@ -442,7 +473,7 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
                         const uint32_t neg = (uint32_t)mq.decode(ctx, tbl, si & 15) ^ (si >> 4);
                         f |= self_bit(r) | (neg << (kSignShift + 1 + r));
                         dec_mark_significant(F, s, r, c, w, nstripes, neg, vsc);
-                        S.mag[(4 * s + r) * 64 + c] = pbit;
+                        mag_set(4 * s + r, c, pbit);
                         k = r + 1;
                     }
                     for (; k < rows; k++) {
@@ -453,7 +484,7 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
                             const uint32_t neg = (uint32_t)mq.decode(ctx, tbl, si & 15) ^ (si >> 4);
                             f |= self_bit(k) | (neg << (kSignShift + 1 + k));
                             dec_mark_significant(F, s, k, c, w, nstripes, neg, vsc);
-                            S.mag[(4 * s + k) * 64 + c] = pbit;
+                            mag_set(4 * s + k, c, pbit);
                         }
                     }
                     if (f != f0) F[s * 64 + c] = f;
@@ -489,20 +520,22 @@ __device__ int decode_block(WarpState<MagT> &S, const Tables &T, const uint8_t *
 // 4096^2 workload (and 12 blocks per CTA beat 8 at the same count by 5%).
 // The styled instantiations use more registers, so they are told how many
 // CTAs their shared memory lets reside, which keeps that occupancy.
-template <typename MagT, int G>
+template <typename MagT, int G, bool OM = kOutMag<MagT>>
 struct GroupCfg {
-    static constexpr int blocks = sizeof(MagT) == 1 ? kBlocks8 : (sizeof(MagT) == 2 ? 4 : 2);
+    static constexpr int blocks = sizeof(MagT) == 1 ? kBlocks8 : 4;
     static constexpr int warps = blocks * G / 32 > 0 ? blocks * G / 32 : 1;
-    static constexpr size_t smem = ((sizeof(Tables) + 15) & ~size_t(15)) + (size_t)blocks * sizeof(WarpState<MagT>);
+    static constexpr size_t smem =
+        ((sizeof(Tables) + 15) & ~size_t(15)) + (size_t)blocks * sizeof(WarpState<MagT, OM>);
     static constexpr int by_smem = (int)((228u * 1024u) / (smem + 1024u));
+    static constexpr int by_warps = 24 / warps < 1 ? 1 : 24 / warps;   // 24 warps per SM
     template <bool Modes>
-    static constexpr int min_ctas() { return Modes ? (by_smem < 1 ? 1 : (by_smem > 8 ? 8 : by_smem)) : 1; }
+    static constexpr int min_ctas() { return Modes ? (by_smem < 1 ? 1 : (by_smem > by_warps ? by_warps : by_smem)) : 1; }
 };
 
 // Decode code-block `bi` with the state S and write it out (the group's
 // lanes, in lock-step).  MagT bounds the coded bit-planes it accepts.
-template <typename MagT, int G, bool Modes = false>
-__device__ __forceinline__ void process_block(WarpState<MagT> &S, const Tables &T, const tc_cblk_desc *__restrict__ desc,
+template <typename MagT, int G, bool Modes = false, bool OM = kOutMag<MagT>>
+__device__ __forceinline__ void process_block(WarpState<MagT, OM> &S, const Tables &T, const tc_cblk_desc *__restrict__ desc,
                                               uint32_t bi, int ndesc, const uint8_t *__restrict__ pool,
                                               uint64_t pool_len, char *__restrict__ out, uint64_t out_elems, int out_mode,
                                               float recon_r, uint32_t *__restrict__ err, int gl, unsigned gmask,
@@ -572,14 +605,18 @@ __device__ __forceinline__ void process_block(WarpState<MagT> &S, const Tables &
     __syncwarp(gmask);
 
     int type = 0, last_plane = 0;
+    uint32_t *ob = reinterpret_cast<uint32_t *>(out) + d.out_off;   // the block's output words
     if (coded) {
         if (Modes && (style & TC_CBLK_STYLE_BYPASS) && d.passes > 10)
-            type = decode_block<MagT, G, Modes, Modes>(S, T, pool + cw_off, (int)d.seg_len, w, h, d.orient, numbps,
-                                                       d.passes, &last_plane, gl, gmask, gshift, style, lens);
+            type = decode_block<MagT, G, Modes, Modes, OM>(S, T, pool + cw_off, (int)d.seg_len, w, h, d.orient, numbps,
+                                                       d.passes, &last_plane, gl, gmask, gshift, ob, d.out_pitch, style,
+                                                       lens);
         else
-            type = decode_block<MagT, G, Modes, false>(S, T, pool + cw_off, (int)d.seg_len, w, h, d.orient, numbps,
-                                                       d.passes, &last_plane, gl, gmask, gshift, style, lens);
+            type = decode_block<MagT, G, Modes, false, OM>(S, T, pool + cw_off, (int)d.seg_len, w, h, d.orient, numbps,
+                                                       d.passes, &last_plane, gl, gmask, gshift, ob, d.out_pitch, style,
+                                                       lens);
     }
+    if constexpr (OM) __threadfence();   // lane 0's magnitude writes, before the group reads them
     __syncwarp(gmask);
 
     // epilogue: reconstruction + inverse quantisation, coalesced rows; an
@@ -596,7 +633,10 @@ __device__ __forceinline__ void process_block(WarpState<MagT> &S, const Tables &
             const bool sg = (f & self_bit(k)) != 0u;
             uint32_t mg = 0, neg = 0, u = 0;
             if (sg) {
-                mg = (uint32_t)S.mag[y * 64 + x];
+                if constexpr (OM)
+                    mg = __ldcg(reinterpret_cast<const uint32_t *>(row) + x);
+                else
+                    mg = (uint32_t)S.mag[y * 64 + x];
                 neg = (f >> (kSignShift + 1 + k)) & 1u;
                 u = (uint32_t)last_plane;
                 if (type == 1 && !(f & pi_bit(k))) u++;
@@ -623,9 +663,9 @@ __device__ __forceinline__ void process_block(WarpState<MagT> &S, const Tables &
 
 // Persistent Tier-1 launch over one magnitude class.  The 8-bit class with
 // 32-lane groups can also take a short queue of 16-bit blocks (`heavy`): in
-// each of the first `heavy_ctas` CTAs warp 0 becomes a 16-bit decoder that
-// uses its own and warp 1's state memory (warp 1 stands down), drains the
-// heavy queue first and then joins the 8-bit queue.  A few blocks with many
+// each of the first `heavy_ctas` CTAs warp 0 becomes a 16-bit decoder in
+// its own state slot (a deep block's magnitudes live in its output words),
+// drains the heavy queue first and then joins the 8-bit queue.  A few blocks with many
 // bit-planes thus start at once, one per CTA, in the same longest-first
 // launch as the bulk, instead of running as a separate class whose warps
 // share SMs with the bulk and become the launch's longest chain.
@@ -636,16 +676,16 @@ struct HeavyQueue {
     uint32_t *counter = nullptr;
 };
 
-template <typename MagT, int G, bool Modes = false>
-__global__ void __launch_bounds__(32 * GroupCfg<MagT, G>::warps, GroupCfg<MagT, G>::template min_ctas<Modes>())
+template <typename MagT, int G, bool Modes = false, bool OM = kOutMag<MagT>>
+__global__ void __launch_bounds__(32 * GroupCfg<MagT, G, OM>::warps, GroupCfg<MagT, G, OM>::template min_ctas<Modes>())
 t1_decode_kernel(const tc_cblk_desc *__restrict__ desc, const uint32_t *__restrict__ order, int n, int ndesc,
                  const uint8_t *__restrict__ pool, uint64_t pool_len, char *__restrict__ out, uint64_t out_elems,
                  int out_mode, float recon_r, uint32_t *__restrict__ counter, uint32_t *__restrict__ err, HeavyQueue heavy)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     Tables &T = *reinterpret_cast<Tables *>(smem);
-    WarpState<MagT> *states =
-        reinterpret_cast<WarpState<MagT> *>(smem + ((sizeof(Tables) + 15) & ~size_t(15)));
+    WarpState<MagT, OM> *states =
+        reinterpret_cast<WarpState<MagT, OM> *>(smem + ((sizeof(Tables) + 15) & ~size_t(15)));
     build_tables(T);
     __syncthreads();
 
@@ -654,12 +694,11 @@ t1_decode_kernel(const tc_cblk_desc *__restrict__ desc, const uint32_t *__restri
     const int gshift = gidx * G;
     const unsigned gmask = G == 32 ? 0xffffffffu : (((1u << G) - 1u) << gshift);
     const int slot = (threadIdx.x >> 5) * (32 / G) + gidx;
-    WarpState<MagT> &S = states[slot];
+    WarpState<MagT, OM> &S = states[slot];
 
     if constexpr (std::is_same<MagT, uint8_t>::value && G == 32) {
-        static_assert(sizeof(WarpState<uint16_t>) <= 2 * sizeof(WarpState<uint8_t>), "heavy state spans two slots");
-        if ((int)blockIdx.x < heavy.ctas && slot < 2) {
-            if (slot == 1) return;  // lends its state to warp 0
+        static_assert(sizeof(WarpState<uint16_t>) <= sizeof(WarpState<uint8_t>), "heavy state fits a slot");
+        if ((int)blockIdx.x < heavy.ctas && slot == 0) {
             WarpState<uint16_t> &HS = *reinterpret_cast<WarpState<uint16_t> *>(&states[0]);
             for (;;) {
                 int idx = 0;
@@ -678,7 +717,7 @@ t1_decode_kernel(const tc_cblk_desc *__restrict__ desc, const uint32_t *__restri
         idx = __shfl_sync(gmask, idx, gshift);
         if (idx >= n) break;
         const uint32_t bi = order ? order[idx] : (uint32_t)idx;
-        process_block<MagT, G, Modes>(S, T, desc, bi, ndesc, pool, pool_len, out, out_elems, out_mode, recon_r, err, gl,
+        process_block<MagT, G, Modes, OM>(S, T, desc, bi, ndesc, pool, pool_len, out, out_elems, out_mode, recon_r, err, gl,
                                       gmask, gshift);
     }
 }
@@ -748,20 +787,20 @@ struct LaunchCfg {
 };
 
 // Kernel attributes and occupancy of one class variant, set up once per device.
-template <typename MagT, int G, bool Modes = false>
+template <typename MagT, int G, bool Modes = false, bool OM = kOutMag<MagT>>
 cudaError_t class_cfg(tc_ctx *ctx, LaunchCfg **out)
 {
-    constexpr int kWarps = GroupCfg<MagT, G>::warps;
+    constexpr int kWarps = GroupCfg<MagT, G, OM>::warps;
     static LaunchCfg cfg[64];
     static DeviceFlags ready;
     LaunchCfg &C = cfg[ctx->device & 63];
     const cudaError_t e = once_per_device(ready, ctx->device, [&] {
-        C.smem = ((sizeof(Tables) + 15) & ~size_t(15)) + kWarps * (32 / G) * sizeof(WarpState<MagT>);
+        C.smem = ((sizeof(Tables) + 15) & ~size_t(15)) + kWarps * (32 / G) * sizeof(WarpState<MagT, OM>);
         C.per_cta = kWarps * (32 / G);
-        cudaError_t r = cudaFuncSetAttribute(t1_decode_kernel<MagT, G, Modes>,
+        cudaError_t r = cudaFuncSetAttribute(t1_decode_kernel<MagT, G, Modes, OM>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C.smem);
         if (r == cudaSuccess)
-            r = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&C.per_sm, t1_decode_kernel<MagT, G, Modes>,
+            r = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&C.per_sm, t1_decode_kernel<MagT, G, Modes, OM>,
                                                               32 * kWarps, C.smem);
         if (C.per_sm < 1) C.per_sm = 1;
         return r;
@@ -772,21 +811,38 @@ cudaError_t class_cfg(tc_ctx *ctx, LaunchCfg **out)
 
 // One class launch: a persistent grid pulling the class's blocks from its
 // work counter d_words[slot] (zeroed beforehand).
-template <typename MagT, int G, bool Modes = false>
-cudaError_t launch_class(tc_ctx *ctx, cudaStream_t stream, const tc_cblk_desc *d_desc, const uint32_t *d_order,
-                         int n, int ndesc, const uint8_t *d_pool, uint64_t pool_len, void *d_out, uint64_t out_elems, int out_mode,
-                         float recon_r, int slot, const HeavyQueue &heavy = HeavyQueue())
+template <typename MagT, int G, bool Modes = false, bool OM = kOutMag<MagT>>
+cudaError_t launch_class_om(tc_ctx *ctx, cudaStream_t stream, const tc_cblk_desc *d_desc, const uint32_t *d_order,
+                            int n, int ndesc, const uint8_t *d_pool, uint64_t pool_len, void *d_out, uint64_t out_elems,
+                            int out_mode, float recon_r, int slot, const HeavyQueue &heavy = HeavyQueue())
 {
     LaunchCfg *C = nullptr;
-    cudaError_t e = class_cfg<MagT, G, Modes>(ctx, &C);
+    cudaError_t e = class_cfg<MagT, G, Modes, OM>(ctx, &C);
     if (e != cudaSuccess) return e;
     const int want = std::max((n + C->per_cta - 1) / C->per_cta, heavy.ctas);
     const int grid = std::max(1, std::min(want, C->per_sm * num_sms(ctx->device)));
-    t1_decode_kernel<MagT, G, Modes><<<grid, 32 * GroupCfg<MagT, G>::warps, C->smem, stream>>>(
+    t1_decode_kernel<MagT, G, Modes, OM><<<grid, 32 * GroupCfg<MagT, G, OM>::warps, C->smem, stream>>>(
         d_desc, d_order, n, ndesc, d_pool, pool_len, static_cast<char *>(d_out), out_elems, out_mode, recon_r,
         ctx->d_words + slot, ctx->d_words, heavy);
     ctx->launches++;
     return cudaGetLastError();
+}
+
+// A plain 32-lane launch of a deep class keeps its magnitudes in the output
+// words only when its blocks fill the GPU (one block for each of 24 warps on
+// every SM); a smaller one keeps them in shared memory.
+template <typename MagT, int G, bool Modes = false>
+cudaError_t launch_class(tc_ctx *ctx, cudaStream_t stream, const tc_cblk_desc *d_desc, const uint32_t *d_order,
+                         int n, int ndesc, const uint8_t *d_pool, uint64_t pool_len, void *d_out, uint64_t out_elems,
+                         int out_mode, float recon_r, int slot, const HeavyQueue &heavy = HeavyQueue())
+{
+    if constexpr (kOutMag<MagT> && G == 32 && !Modes) {
+        if (n < 24 * num_sms(ctx->device))
+            return launch_class_om<MagT, G, Modes, false>(ctx, stream, d_desc, d_order, n, ndesc, d_pool, pool_len, d_out,
+                                                          out_elems, out_mode, recon_r, slot, heavy);
+    }
+    return launch_class_om<MagT, G, Modes>(ctx, stream, d_desc, d_order, n, ndesc, d_pool, pool_len, d_out, out_elems,
+                                           out_mode, recon_r, slot, heavy);
 }
 
 template <typename MagT>
