@@ -5,9 +5,10 @@
 //   * one warp per code-block; warps pull block indices from a device work
 //     queue (an atomic counter over a longest-first order), so blocks of
 //     uneven size and pass count from many tiles and images share a launch;
-//   * blocks are split by coded bit-planes (<= 8, <= 16, <= 31) into classes
-//     whose magnitudes are stored as 8-, 16- or 32-bit values; the classes run
-//     as concurrent launches, heaviest first;
+//   * blocks are split by coded bit-planes (<= 8, <= 16, <= 31) into classes:
+//     8-bit magnitudes in shared memory, deeper ones in the block's output
+//     words (or as 16- or 32-bit values in shared memory when the launch is
+//     small); the classes run as concurrent launches, heaviest first;
 //   * the code-block state is one 32-bit flag word per stripe column: the
 //     significance of its 3x6 neighbourhood interleaved so that row k's 3x3
 //     neighbourhood is (F >> 3k) & 0x1FF, the visited (pi) and refined
@@ -53,15 +54,14 @@ namespace {
 constexpr int kBlocks8 = TC_T1_BLOCKS8;  // code-blocks per CTA of the 8-bit class
 
 // Blocks of more than 8 coded bit-planes keep their magnitude bits in their
-// own output words instead of shared memory, so their state is as small as
-// an 8-bit block's and as many of them reside per SM (24 warps instead of
-// 16: lossless 12-bit 4096^2 Tier-1 48.7 -> 46.3 ms).  8-bit blocks keep
-// them in shared memory, which is faster for them.
-// (OM, "output magnitudes", true.)  A launch too small to fill the GPU keeps
-// them in shared memory instead (OM false): each of its warps then runs
-// nearly alone, and the output-word path's longer per-block latency would
-// show (the 200,000-block workload decoded one launch per image: 1366 ms
-// against 1007 ms).
+// own output words instead of shared memory (OM, "output magnitudes"), so
+// their state is smaller than an 8-bit block's and 24 warps of them reside
+// per SM instead of 16 (with 4-block CTAs: lossless 12-bit 4096^2 Tier-1
+// 48.7 -> 42.0 ms).  8-bit blocks keep them in shared memory, which is
+// faster for them.  A launch too small to fill the GPU keeps them in shared
+// memory too (OM false): each of its warps then runs nearly alone, and the
+// output-word path's longer per-block latency would show (the 200,000-block
+// workload decoded one launch per image: 1366 ms against 1049 ms).
 template <typename MagT>
 constexpr bool kOutMag = sizeof(MagT) > 1;
 
