@@ -934,7 +934,7 @@ def run_ours(args, rank, world, local_rank):
                                  "issue, not by HBM: achieved = warp instructions per launch (ncu "
                                  "smsp__inst_executed.sum of this workload, profiles/) / the live CUDA-event Tier-1 "
                                  "time; peak = 148 SMs x 4 issue slots x the sampled SM clock"},
-            "dwt_roofline": {"bound": "hbm", "kernel": "reverse 9/7 levels (idwt_rev_kernel, idwt97_ict_kernel)",
+            "dwt_roofline": {"bound": "hbm", "kernel": "reverse 9/7 levels (idwt_rev_kernel plane levels, idwt97_ict_tma_kernel last level)",
                              "achieved": round(dwt_gbs, 2), "peak": hbm, "unit": "GB/s",
                              "frac": round(dwt_gbs / hbm, 4), "bytes_per_step": dw_bytes, "peak_kind": peak_kind},
             "e2e": {"value": round(W * H * world / e2e_s / 1e6, 2), "unit": "Mpixel/s",
