@@ -43,6 +43,25 @@ def test_batched_launch_gives_the_truncated_coefficients(gpu_ctx, batch):
     np.testing.assert_array_equal(bb.out.cpu().numpy(), got)
 
 
+def test_repeated_launches_are_identical(gpu_ctx, batch):
+    """The deep blocks of this batch fill the GPU, so their magnitudes go
+    through the output words (lane 0's stores and atomic ORs, then the
+    group's read-back after a fence and a warp barrier); the output must be
+    the same on every run, from any starting contents of the output."""
+    bb, _ = batch
+    d = bb.desc
+    nbp = d["mb"].astype(int) - d["zero_bitplanes"].astype(int)
+    assert (nbp > 8).sum() > 24 * 148   # a deep class large enough for output-word magnitudes
+    bb.decode_batched()
+    gpu_ctx.synchronize()
+    first = bb.out.cpu().numpy()
+    for fill in (0, -1, 0x5A5A5A5A):
+        bb.out.fill_(fill)
+        bb.decode_batched()
+        gpu_ctx.synchronize()
+        np.testing.assert_array_equal(bb.out.cpu().numpy(), first)
+
+
 def test_sampled_blocks_match_oracle_and_reference_kernel(gpu_ctx, batch):
     bb, _ = batch
     bb.decode_batched()
