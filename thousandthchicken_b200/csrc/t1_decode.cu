@@ -828,15 +828,15 @@ cudaError_t launch_class_om(tc_ctx *ctx, cudaStream_t stream, const tc_cblk_desc
     return cudaGetLastError();
 }
 
-// A plain 32-lane launch of a deep class keeps its magnitudes in the output
-// words only when its blocks fill the GPU (one block for each of 24 warps on
-// every SM); a smaller one keeps them in shared memory.
+// A 32-lane launch of a deep class keeps its magnitudes in the output words
+// only when its blocks fill the GPU (one block for each of 24 warps on every
+// SM); a smaller one keeps them in shared memory.
 template <typename MagT, int G, bool Modes = false>
 cudaError_t launch_class(tc_ctx *ctx, cudaStream_t stream, const tc_cblk_desc *d_desc, const uint32_t *d_order,
                          int n, int ndesc, const uint8_t *d_pool, uint64_t pool_len, void *d_out, uint64_t out_elems,
                          int out_mode, float recon_r, int slot, const HeavyQueue &heavy = HeavyQueue())
 {
-    if constexpr (kOutMag<MagT> && G == 32 && !Modes) {
+    if constexpr (kOutMag<MagT> && G == 32) {
         if (n < 24 * num_sms(ctx->device))
             return launch_class_om<MagT, G, Modes, false>(ctx, stream, d_desc, d_order, n, ndesc, d_pool, pool_len, d_out,
                                                           out_elems, out_mode, recon_r, slot, heavy);
