@@ -744,6 +744,44 @@ def dwt_levels(ctx, stream, flush, n, levels, hbm, reps=7):
             "what": "tc_dwt_reverse97 level by level (reverses of k and k-1 levels differenced), full size first"}
 
 
+def tier1_only(kind, n, reps=12):
+    """Tier-1 time (CUDA events on the plan's stream, L2 flushed before each
+    run; min and median of `reps`) of one n x n x 3 image: the bench's lossy
+    coding, or 12-bit samples coded losslessly (RCT, 5-level 5/3), with a
+    hash of the decoded samples."""
+    import hashlib
+    import torch
+    from thousandthchicken_b200 import codec
+    from thousandthchicken_b200.stages import Context, Plan
+    from thousandthchicken_b200.synth import gradient_noise_image
+    if kind == "lossy":
+        _, cs = make_workload(n, n, WORKLOAD["seed"])
+    else:
+        img = gradient_noise_image(n, n, 3, 12, WORKLOAD["seed"])
+        cs = codec.encode(img, 12, levels=5, reversible=True, mct=True)
+    stream = torch.cuda.Stream(0)
+    ctx = Context(0, stream)
+    plan = Plan(ctx, [cs])
+    outs = plan.alloc_outputs()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda:0")
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            plan.execute(outs)
+    ctx.synchronize()
+    digest = hashlib.sha1(outs[0].cpu().numpy().tobytes()).hexdigest()[:12]
+    plan.set_profiling(True)
+    t1 = []
+    with torch.cuda.stream(stream):
+        for k in range(reps):
+            flush.fill_(k & 0xFF)
+            plan.execute(outs)
+            t1.append(plan.stage_ms()[0])
+    plan.set_profiling(False)
+    t1.sort()
+    return {"tier1": kind, "size": n, "code_blocks": plan.infos[0]["ncblk"], "tier1_ms_min": round(t1[0], 3),
+            "tier1_ms_median": round(t1[len(t1) // 2], 3), "samples_sha1": digest}
+
+
 def _level_dims(w, h, levels):
     """(width, height) of each level's region, the full size first."""
     dims = []
@@ -980,7 +1018,13 @@ def main():
                     help="only time tc_dwt_reverse97 level by level on an N x N plane (profiling)")
     ap.add_argument("--dwt-depth", type=int, default=6, help="levels for --dwt-levels")
     ap.add_argument("--dwt-reps", type=int, default=7, help="timed runs per level count for --dwt-levels")
+    ap.add_argument("--tier1", choices=["lossy", "lossless12"], default=None,
+                    help="only time Tier-1 of one image of --size (default 4096): the bench's lossy coding, or "
+                         "12-bit RCT + 5-level 5/3 (profiling)")
     args = ap.parse_args()
+    if args.tier1:
+        print(json.dumps(tier1_only(args.tier1, args.size or 4096)))
+        return
     if args.dwt_levels:
         import torch
         from thousandthchicken_b200.stages import Context
